@@ -1,0 +1,140 @@
+"""ctypes mirror of include/flash_hy.h and the loader of the CUDA library.
+
+The structs here are the C-ABI parameter and grid descriptors; the library
+itself is ``flash5_b200/_flash_hy.so`` built from ``flash5_b200/csrc`` by
+``flash5_b200.build``.  Loading fails loudly when the library is missing:
+there is no CPU fallback on the product path.
+"""
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_flash_hy.so")
+
+# status bits
+OK = 0
+ERR_NEG_SOUNDSPEED = 1 << 0
+ERR_NONPOS_DT = 1 << 1
+ERR_NEWTON_NOCONV = 1 << 2
+ERR_NAN = 1 << 3
+ERR_TIMEOUT = 1 << 4
+ERR_BAD_ARG = 1 << 5
+ERR_CUDA = 1 << 6
+ERR_UNSUPPORTED = 1 << 7
+
+RS_HLLC = 4
+RS_EXACT = 100
+LIM_MINMOD, LIM_MC, LIM_HYBRID, LIM_VANLEER, LIM_LIMITED = 1, 2, 3, 4, 5
+BC_REFLECTING, BC_OUTFLOW, BC_PERIODIC = -31, -32, -135
+PREC_FP64, PREC_FP64_FMA, PREC_MIXED = 0, 1, 2
+LAYOUT_VAR_FASTEST, LAYOUT_XYZ_FASTEST = 0, 1
+UPDATE_NONE, UPDATE_ALL = 0, 3
+
+
+class VarMap(C.Structure):
+    _fields_ = [(n, C.c_int) for n in
+                ("dens", "eint", "ener", "gamc", "game", "pres", "temp", "velx", "vely", "velz")]
+
+
+# FLASH's alphabetical +uhd / gamma-EOS UNK ordering (1-based *_VAR).
+FLASH_UHD_VARS = ("dens", "eint", "ener", "gamc", "game", "pres", "shok", "temp", "velx", "vely", "velz")
+
+
+def flash_varmap():
+    vm = VarMap()
+    for i, n in enumerate(FLASH_UHD_VARS):
+        if hasattr(vm, n):
+            setattr(vm, n, i + 1)
+    return vm
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("order", C.c_int), ("riemann_solver", C.c_int), ("slope_limiter", C.c_int),
+        ("char_limiting", C.c_int), ("use_flattening", C.c_int), ("use_steepening", C.c_int),
+        ("use_aux_eint", C.c_int), ("use_3d_full_ctu", C.c_int), ("precision", C.c_int),
+        ("learned_guess", C.c_int),
+        ("limited_slope_beta", C.c_double), ("f_pres_in_mom_flux", C.c_double), ("cfl", C.c_double),
+        ("eint_switch", C.c_double), ("smlrho", C.c_double), ("smallp", C.c_double),
+        ("smalle", C.c_double), ("tiny", C.c_double), ("gamma", C.c_double),
+        ("gas_constant", C.c_double), ("single_species_a", C.c_double),
+    ]
+
+
+def default_params(**kw):
+    """Runtime parameters with FLASH5's unsplit defaults (unsplit/Config:105-159,
+    HydroMain/Config:26, Eos/EosMain/Config:49-56) except order=3 (PPM) and
+    flattening on, the settings of the benchmark configurations."""
+    p = Params()
+    p.order = 3
+    p.riemann_solver = RS_HLLC
+    p.slope_limiter = LIM_VANLEER
+    p.char_limiting = 1
+    p.use_flattening = 1
+    p.use_steepening = 0
+    p.use_aux_eint = 1
+    p.use_3d_full_ctu = 1
+    p.precision = PREC_FP64
+    p.learned_guess = 0
+    p.limited_slope_beta = 1.0
+    p.f_pres_in_mom_flux = 1.0
+    p.cfl = 0.8
+    p.eint_switch = 0.0
+    p.smlrho = 1e-10
+    p.smallp = 1e-10
+    p.smalle = 1e-10
+    p.tiny = 1e-16
+    p.gamma = 1.4
+    p.gas_constant = 8.3144598e7
+    p.single_species_a = 1.0
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v)
+    return p
+
+
+class GridDesc(C.Structure):
+    _fields_ = [
+        ("ndim", C.c_int), ("nxb", C.c_int), ("nyb", C.c_int), ("nzb", C.c_int),
+        ("nguard", C.c_int), ("nblocks", C.c_int), ("nblk_l1", C.c_int * 3), ("max_level", C.c_int),
+        ("block_coords", C.POINTER(C.c_int)), ("block_level", C.POINTER(C.c_int)),
+        ("domain_lo", C.c_double * 3), ("domain_hi", C.c_double * 3), ("bc", C.c_int * 6),
+    ]
+
+
+def _set_sigs(lib):
+    P, G, V = C.POINTER(Params), C.POINTER(GridDesc), C.POINTER(VarMap)
+    dp, ip, vp = C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_void_p
+    sigs = {
+        "flash_hy_create": (C.c_int, [P, G, C.c_int, C.POINTER(vp)]),
+        "flash_hy_destroy": (C.c_int, [vp]),
+        "flash_hy_upload": (C.c_int, [vp, dp, C.c_int, C.c_int, V]),
+        "flash_hy_download": (C.c_int, [vp, dp, C.c_int, C.c_int, V]),
+        "flash_hy_step": (C.c_int, [vp, C.c_double, C.c_double, C.c_double, C.c_int]),
+        "flash_hy_step_blocks": (C.c_int, [vp, C.c_int, ip, C.c_double, C.c_double, C.c_double, C.c_int]),
+        "flash_hy_compute_dt": (C.c_int, [vp, dp, ip]),
+        "flash_hy_sync": (C.c_int, [vp]),
+        "flash_hy_stream": (vp, [vp]),
+        "flash_hy_last_error": (C.c_int, [vp, C.c_char_p, C.c_int]),
+        "flash_hy_last_launch_count": (C.c_int, [vp]),
+    }
+    for name, (res, args) in sigs.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+_LIB = None
+
+
+def load_library(path=LIB_PATH):
+    """Load the CUDA C-ABI library; raise if it was not built."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(path):
+            raise RuntimeError(
+                f"CUDA library {path} not found: build it with `python -c 'import __graft_entry__ as g; g.build()'`")
+        _LIB = _set_sigs(C.CDLL(path))
+    return _LIB

@@ -1,0 +1,496 @@
+// hy_kernels.cuh -- kernels of one unsplit hydro step on a uniform block grid.
+//
+// Device state: five block-major SoA arrays (dens, velx, vely, velz, eint) of
+// the block interiors only.  Everything else FLASH keeps in UNK (PRES, GAMC,
+// GAME, ENER, TEMP) is the gamma-law EOS of these five after every step
+// (Eos_wrapped MODE_DENS_EI, eos_idealGamma.F90:323-335, Eos_putData.F90:
+// 95-106), so it is recomputed where needed.  Guard cells are not stored: the
+// kernels gather them from the neighbouring blocks (or the boundary
+// condition) and apply the EOS to them, which is Grid_fillGuardCells with
+// doEos (paramesh4/Grid_fillGuardCells.F90:227-569, Hydro.F90:121-123).
+//
+// One step = k_sig (transverse fluxes of every direction on the box of
+// cells [-1, N]^d of every block) followed by one k_dir launch per direction
+// (PPM + transverse + CTU corrections, HLLC, accumulation of the
+// conservative update).  The last direction also finalises the update,
+// applies hy_energyFix and the EOS, writes the new state and reduces the CFL
+// time step per block.
+#pragma once
+#include "hy_core.cuh"
+#include <float.h>
+
+namespace fhy {
+
+struct CflPart {          // per-block CFL reduction result
+  double dt;              // cfl / max (|u_d| + c_s)/dx_d, DBL_MAX if 0
+  int i, j, k, blk;       // 0-based interior cell of the winning cell
+};
+
+__device__ __forceinline__ int map_axis(int g, int n, int bclo, int bchi, int &flip) {
+  if (g < 0) {
+    if (bclo == -135) return ((g % n) + n) % n;
+    if (bclo == -31) { flip = 1; return -1 - g; }
+    return 0;
+  }
+  if (g >= n) {
+    if (bchi == -135) return g % n;
+    if (bchi == -31) { flip = 1; return 2 * n - 1 - g; }
+    return n - 1;
+  }
+  return g;
+}
+
+// Offset of the stored cell that provides local cell (li,lj,lk) of block b.
+template <int NDIM, int NX, int NY, int NZ>
+__device__ __forceinline__ size_t cell_src(const DevParams &P, int b, int3 bc, int li, int lj, int lk,
+                                           bool &inside, int &fx, int &fy, int &fz) {
+  constexpr int NCB = NX * NY * NZ;
+  inside = (li >= 0 && li < NX) && (NDIM < 2 || (lj >= 0 && lj < NY)) && (NDIM < 3 || (lk >= 0 && lk < NZ));
+  fx = fy = fz = 0;
+  if (inside) return (size_t)b * NCB + (size_t)((lk * NY + lj) * NX + li);
+  int gx = map_axis(bc.x * NX + li, P.nbx * NX, P.bc[0], P.bc[1], fx);
+  int gy = NDIM > 1 ? map_axis(bc.y * NY + lj, P.nby * NY, P.bc[2], P.bc[3], fy) : 0;
+  int gz = NDIM > 2 ? map_axis(bc.z * NZ + lk, P.nbz * NZ, P.bc[4], P.bc[5], fz) : 0;
+  int sb = P.blk_at[((gz / NZ) * P.nby + gy / NY) * P.nbx + gx / NX];
+  return (size_t)sb * NCB + (size_t)(((gz % NZ) * NY + (gy % NY)) * NX + (gx % NX));
+}
+
+// Primitive slots of a cell as hy_getRiemannState sees it: interior cells
+// straight from the state, guard cells after the guard-cell EOS.
+template <int NDIM, int NX, int NY, int NZ>
+__device__ __forceinline__ void load_prim(const DevParams &P, int b, int3 bc, int li, int lj, int lk, double V[8]) {
+  bool inside; int fx, fy, fz;
+  size_t o = cell_src<NDIM, NX, NY, NZ>(P, b, bc, li, lj, lk, inside, fx, fy, fz);
+  double rho = __ldg(P.s_in[0] + o), vx = __ldg(P.s_in[1] + o), vy = __ldg(P.s_in[2] + o);
+  double vz = __ldg(P.s_in[3] + o), e = __ldg(P.s_in[4] + o);
+  if (fx) vx = -vx;
+  if (fy) vy = -vy;
+  if (fz) vz = -vz;
+  double eg = e;
+  if (!inside) {   // Eos_getData.F90:80-96 on ENER = eint + ekin of the source cell
+    double ekin = 0.5 * (vx * vx + vy * vy + vz * vz);
+    double ener = e + ekin;
+    if (ener - ekin > rmax(P.smalle, P.eswitch * ekin)) eg = ener - ekin;
+  }
+  double p = rho * eg * P.gam1inv;
+  V[HD] = rho; V[HVX] = vx; V[HVY] = vy; V[HVZ] = vz; V[HP] = p;
+  V[HGC] = P.gamma; V[HGE] = p / (eg * rho) + 1; V[HEI] = eg;
+}
+
+// Pressure only (flattening stencil ends).
+template <int NDIM, int NX, int NY, int NZ>
+__device__ __forceinline__ double load_pres(const DevParams &P, int b, int3 bc, int li, int lj, int lk) {
+  bool inside; int fx, fy, fz;
+  size_t o = cell_src<NDIM, NX, NY, NZ>(P, b, bc, li, lj, lk, inside, fx, fy, fz);
+  double rho = __ldg(P.s_in[0] + o), e = __ldg(P.s_in[4] + o);
+  double eg = e;
+  if (!inside) {
+    double vx = __ldg(P.s_in[1] + o), vy = __ldg(P.s_in[2] + o), vz = __ldg(P.s_in[3] + o);
+    double ekin = 0.5 * (vx * vx + vy * vy + vz * vz);
+    double ener = e + ekin;
+    if (ener - ekin > rmax(P.smalle, P.eswitch * ekin)) eg = ener - ekin;
+  }
+  return rho * eg * P.gam1inv;
+}
+
+template <int NDIM, int NX, int NY, int NZ> struct Box {
+  static constexpr int bx = NX + 2, by = NDIM > 1 ? NY + 2 : 1, bz = NDIM > 2 ? NZ + 2 : 1;
+  static constexpr int n = bx * by * bz;
+  __device__ static __forceinline__ int idx(int i, int j, int k) {
+    return ((k + (NDIM > 2)) * by + (j + (NDIM > 1))) * bx + (i + 1);
+  }
+};
+
+__device__ __forceinline__ int3 blk_coords(const DevParams &P, int b) {
+  return make_int3(P.blk_coord[3 * b], P.blk_coord[3 * b + 1], P.blk_coord[3 * b + 2]);
+}
+
+template <class R, int DIR>
+__device__ __forceinline__ void sig_dir(const DevParams &P, const double *Vm, const double *Vc, const double *Vp,
+                                        R sig[8], unsigned &st) {
+  R m[8], c[8], p[8];
+#pragma unroll
+  for (int n = 0; n < 8; ++n) { m[n] = R(Vm[n]); c[n] = R(Vc[n]); p[n] = R(Vp[n]); }
+  Eig<R> e;
+  eigen<R, DIR>(c, e, st);
+  upwind_tflux<R, DIR>(P, m, c, p, e, sig);
+}
+
+// sig components kept in memory: dens, velx, vely, velz, pres, eint
+__device__ __forceinline__ int sig_slot(int q) { return q < 5 ? q : HEI; }
+
+// ---------------------------------------------------------------------------
+// k_sig: transverse flux "sig" of every direction for the box cells
+// (hy_DataReconstructNormalDir_PPM.F90:351-371 via hy_getRiemannState.F90:
+// 471-637, which evaluates it for every cell of [lo-1, hi+1]^d)
+// ---------------------------------------------------------------------------
+template <int NDIM, int NX, int NY, int NZ, class R>
+__global__ void __launch_bounds__(256) k_sig(const DevParams P, R *__restrict__ SIG) {
+  using B = Box<NDIM, NX, NY, NZ>;
+  const int b = P.blk_list ? P.blk_list[blockIdx.x] : blockIdx.x;
+  const int3 bc = blk_coords(P, b);
+  unsigned st = 0;
+  for (int t = threadIdx.x; t < B::n; t += blockDim.x) {
+    int i = t % B::bx - 1, j = NDIM > 1 ? (t / B::bx) % B::by - 1 : 0, k = NDIM > 2 ? t / (B::bx * B::by) - 1 : 0;
+    double Vc[8], Vm[8], Vp[8];
+    load_prim<NDIM, NX, NY, NZ>(P, b, bc, i, j, k, Vc);
+#pragma unroll
+    for (int d = 1; d <= NDIM; ++d) {
+      load_prim<NDIM, NX, NY, NZ>(P, b, bc, i - (d == 1), j - (d == 2), k - (d == 3), Vm);
+      load_prim<NDIM, NX, NY, NZ>(P, b, bc, i + (d == 1), j + (d == 2), k + (d == 3), Vp);
+      R s[8];
+      if (d == 1) sig_dir<R, 1>(P, Vm, Vc, Vp, s, st);
+      else if (d == 2) sig_dir<R, 2>(P, Vm, Vc, Vp, s, st);
+      else sig_dir<R, 3>(P, Vm, Vc, Vp, s, st);
+      R *dst = SIG + ((size_t)blockIdx.x * NDIM + (d - 1)) * 6 * B::n + t;
+#pragma unroll
+      for (int q = 0; q < 6; ++q) dst[(size_t)q * B::n] = s[sig_slot(q)];
+    }
+  }
+  if (st) atomicOr(P.status, st);
+}
+
+__device__ __forceinline__ void load_sig(const float *p, size_t stride, float s[8]) {
+#pragma unroll
+  for (int q = 0; q < 6; ++q) s[sig_slot(q)] = p[q * stride];
+  s[HGC] = 0.f; s[HGE] = 0.f;
+}
+__device__ __forceinline__ void load_sig(const double *p, size_t stride, double s[8]) {
+#pragma unroll
+  for (int q = 0; q < 6; ++q) s[sig_slot(q)] = p[q * stride];
+  s[HGC] = 0.; s[HGE] = 0.;
+}
+
+// deterministic (max key, first index) reduction for the CFL step
+struct CflCand { double key, val; int idx; };
+__device__ __forceinline__ void cfl_merge(CflCand &a, const CflCand &b) {
+  if (b.key > a.key || (b.key == a.key && b.idx < a.idx)) a = b;
+}
+
+template <int NX, int NY, int NZ>
+__device__ void cfl_block_reduce(CflCand c, int blk, double cfl, CflPart *part) {
+  __shared__ CflCand red[32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    CflCand b;
+    b.key = __shfl_down_sync(0xffffffffu, c.key, o);
+    b.val = __shfl_down_sync(0xffffffffu, c.val, o);
+    b.idx = __shfl_down_sync(0xffffffffu, c.idx, o);
+    if (lane + o < 32) cfl_merge(c, b);
+  }
+  if (lane == 0) red[w] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    CflCand a = red[0];
+    for (int q = 1; q < (int)(blockDim.x + 31) / 32; ++q) cfl_merge(a, red[q]);
+    CflPart r;
+    // Hydro_computeDt.F90:265-284: the winner is the first cell whose
+    // dt_ltemp*cfl exceeds every earlier one; dt = cfl / dt_ltemp
+    if (a.key > 0.0) {
+      r.dt = cfl / a.val;
+      r.i = a.idx % NX; r.j = (a.idx / NX) % NY; r.k = a.idx / (NX * NY);
+    } else {
+      r.dt = DBL_MAX; r.i = r.j = r.k = -1;
+    }
+    r.blk = blk;
+    part[blk] = r;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// k_dir: one direction of the unsplit update for one block per CTA.
+//   phase 1: face states W-/W+ of the line cells (c_DIR in [-1, N], other
+//            coordinates interior) -- PPM (hy_dataReconstOneStep.F90:485-
+//            716), transverse corrections (:918-951), last negativity
+//            check (:1120-1154), 3D full-CTU cross terms and positivity
+//            fallback (hy_getRiemannState.F90:956-1313)
+//   phase 2: HLLC at the N+1 faces of every line plus the auxiliary
+//            internal-energy and volume fluxes (hy_getFaceFlux.F90:283-442)
+//   phase 3: accumulation of the conservative update in direction order
+//            x, y, z (updateConservedVariable, hy_unsplitUpdate.F90:1187-
+//            1242); the last direction finishes the cell: internal-energy
+//            update with the n+1/2 pressure (:657-672, hy_getFaceFlux.F90:
+//            551-557 and y/z analogues), hy_energyFix (:188-253), the EOS
+//            and the CFL reduction (Hydro_computeDt.F90:186-290).
+// ---------------------------------------------------------------------------
+template <int NDIM, int NX, int NY, int NZ, class R, int DIR>
+struct DirGeom {
+  static constexpr int rx = DIR == 1 ? NX + 2 : NX;
+  static constexpr int ry = NDIM > 1 ? (DIR == 2 ? NY + 2 : NY) : 1;
+  static constexpr int rz = NDIM > 2 ? (DIR == 3 ? NZ + 2 : NZ) : 1;
+  static constexpr int n = rx * ry * rz;
+  static constexpr int stride = DIR == 1 ? 1 : (DIR == 2 ? rx : rx * ry);
+  static constexpr int nd = DIR == 1 ? NX : (DIR == 2 ? NY : NZ);
+  __device__ static __forceinline__ void decode(int t, int &i, int &j, int &k) {
+    i = t % rx - (DIR == 1);
+    j = NDIM > 1 ? (t / rx) % ry - (DIR == 2) : 0;
+    k = NDIM > 2 ? t / (rx * ry) - (DIR == 3) : 0;
+  }
+  __device__ static __forceinline__ int along(int i, int j, int k) { return DIR == 1 ? i : (DIR == 2 ? j : k); }
+  static constexpr size_t smem_bytes() { return (size_t)n * (14 + NFLX) * sizeof(R); }
+};
+
+// slots stored for the face states: dens, velx, vely, velz, pres, game, eint
+__device__ __forceinline__ int wslot(int q) { return q < 5 ? q : q + 1; }
+
+template <int NDIM, int NX, int NY, int NZ, class R, int DIR, bool FIRST, bool LAST>
+__global__ void __launch_bounds__(256) k_dir(const DevParams P, const R *__restrict__ SIG, double *__restrict__ ACC,
+                                             double *__restrict__ AUX, size_t ncells, CflPart *part) {
+  using G = DirGeom<NDIM, NX, NY, NZ, R, DIR>;
+  using B = Box<NDIM, NX, NY, NZ>;
+  constexpr int NCB = NX * NY * NZ;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R *sWp = reinterpret_cast<R *>(smem_raw);     // [7][n]
+  R *sWm = sWp + 7 * G::n;                       // [7][n]
+  R *sF = sWm + 7 * G::n;                        // [8][n]
+  const int b = P.blk_list ? P.blk_list[blockIdx.x] : blockIdx.x;
+  const int3 bc = blk_coords(P, b);
+  unsigned st = 0;
+  const double dt = P.dt;
+  const double delta = P.del[DIR - 1];
+  const R dtn = R(dt / delta);
+  const R hdtx = R(0.5 * dt / P.del[0]), hdty = R(0.5 * dt / P.del[1]), hdtz = R(0.5 * dt / P.del[2]);
+  const R *sigb = SIG + (size_t)blockIdx.x * NDIM * 6 * B::n;
+
+  // ---------------- phase 1: face states of the line cells ----------------
+  for (int t = threadIdx.x; t < G::n; t += blockDim.x) {
+    int i, j, k;
+    G::decode(t, i, j, k);
+    const int di = DIR == 1, dj = DIR == 2, dk = DIR == 3;
+    R V5[5][8];
+    double Vd[8];
+#pragma unroll
+    for (int s = -2; s <= 2; ++s) {
+      load_prim<NDIM, NX, NY, NZ>(P, b, bc, i + s * di, j + s * dj, k + s * dk, Vd);
+#pragma unroll
+      for (int n = 0; n < 8; ++n) V5[s + 2][n] = R(Vd[n]);
+    }
+    R flat = R(0);
+    if (P.use_flattening) {
+      R p7[7], u7[7];
+      p7[0] = R(load_pres<NDIM, NX, NY, NZ>(P, b, bc, i - 3 * di, j - 3 * dj, k - 3 * dk));
+      p7[6] = R(load_pres<NDIM, NX, NY, NZ>(P, b, bc, i + 3 * di, j + 3 * dj, k + 3 * dk));
+#pragma unroll
+      for (int s = 0; s < 5; ++s) { p7[s + 1] = V5[s][HP]; u7[s + 1] = V5[s][Slots<DIR>::v1]; }
+      u7[0] = R(0); u7[6] = R(0);
+      flat = flat_coeff(p7, u7);
+    }
+    R Wp[8], Wm[8];
+    ppm_cell<R, DIR>(P, V5, flat, dtn, R(delta), Wp, Wm, st);
+    const R *Vc = V5[2];
+    // transverse corrections with the sig of the other directions (same cell)
+    const int bi = B::idx(i, j, k);
+    R sx[8], sy[8], sz[8];
+    if (DIR != 1) load_sig(sigb + 0 * 6 * B::n + bi, B::n, sx);
+    if (NDIM > 1 && DIR != 2) load_sig(sigb + 1 * 6 * B::n + bi, B::n, sy);
+    if (NDIM > 2 && DIR != 3) load_sig(sigb + 2 * 6 * B::n + bi, B::n, sz);
+    const int sl[6] = {0, 1, 2, 3, 4, 7};
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      int n = sl[q];
+      if (NDIM == 2) {
+        if (DIR == 1) { Wm[n] = Wm[n] - hdty * sy[n]; Wp[n] = Wp[n] - hdty * sy[n]; }
+        else          { Wm[n] = Wm[n] - hdtx * sx[n]; Wp[n] = Wp[n] - hdtx * sx[n]; }
+      } else {
+        if (DIR == 1)      { Wm[n] = Wm[n] - hdty * sy[n] - hdtz * sz[n]; Wp[n] = Wp[n] - hdty * sy[n] - hdtz * sz[n]; }
+        else if (DIR == 2) { Wm[n] = Wm[n] - hdtx * sx[n] - hdtz * sz[n]; Wp[n] = Wp[n] - hdtx * sx[n] - hdtz * sz[n]; }
+        else               { Wm[n] = Wm[n] - hdtx * sx[n] - hdty * sy[n]; Wp[n] = Wp[n] - hdtx * sx[n] - hdty * sy[n]; }
+      }
+    }
+    if (Wm[HD] < R(0) || Wp[HD] < R(0) || Wm[HP] < R(0) || Wp[HP] < R(0)) {
+#pragma unroll
+      for (int n = 0; n < 8; ++n) { Wm[n] = Vc[n]; Wp[n] = Vc[n]; }
+    }
+    if (NDIM == 3 && P.use_ctu) {
+      // axis / sig direction pairs of hy_getRiemannState.F90:999-1022,
+      // 1101-1124, 1204-1227
+      constexpr int A1 = DIR == 1 ? 2 : (DIR == 2 ? 3 : 1), S1 = DIR == 1 ? 3 : (DIR == 2 ? 1 : 2);
+      constexpr int A2 = DIR == 1 ? 3 : (DIR == 2 ? 1 : 2), S2 = DIR == 1 ? 2 : (DIR == 2 ? 3 : 1);
+      const double dA = P.del[A1 - 1], dB = P.del[A2 - 1];
+      const R fac = R(dt * dt / (6. * (DIR == 1 ? P.del[1] : (DIR == 2 ? P.del[2] : P.del[0])) *
+                                 (DIR == 1 ? P.del[2] : (DIR == 2 ? P.del[0] : P.del[1]))));
+      (void)dA; (void)dB;
+      R T1[8], T2[8];
+      {
+        R sm[8], s0[8], sp[8];
+        const R *base = sigb + (size_t)(S1 - 1) * 6 * B::n;
+        load_sig(base + B::idx(i - (A1 == 1), j - (A1 == 2), k - (A1 == 3)), B::n, sm);
+        load_sig(base + bi, B::n, s0);
+        load_sig(base + B::idx(i + (A1 == 1), j + (A1 == 2), k + (A1 == 3)), B::n, sp);
+        Eig<R> e;
+        eigen<R, A1>(Vc, e, st);
+        upwind_tflux<R, A1>(P, sm, s0, sp, e, T1);
+      }
+      {
+        R sm[8], s0[8], sp[8];
+        const R *base = sigb + (size_t)(S2 - 1) * 6 * B::n;
+        load_sig(base + B::idx(i - (A2 == 1), j - (A2 == 2), k - (A2 == 3)), B::n, sm);
+        load_sig(base + bi, B::n, s0);
+        load_sig(base + B::idx(i + (A2 == 1), j + (A2 == 2), k + (A2 == 3)), B::n, sp);
+        Eig<R> e;
+        eigen<R, A2>(Vc, e, st);
+        upwind_tflux<R, A2>(P, sm, s0, sp, e, T2);
+      }
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        int n = sl[q];
+        Wp[n] = Wp[n] + (T1[n] + T2[n]) * fac;
+        Wm[n] = Wm[n] + (T1[n] + T2[n]) * fac;
+      }
+      if (Wp[HD] <= R(0) || Wm[HD] <= R(0) || Wp[HP] <= R(0) || Wm[HP] <= R(0)) {
+#pragma unroll
+        for (int n = 0; n < 8; ++n) { Wm[n] = Vc[n]; Wp[n] = Vc[n]; }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 7; ++q) {
+      sWp[q * G::n + t] = Wp[wslot(q)];
+      sWm[q * G::n + t] = Wm[wslot(q)];
+    }
+  }
+  __syncthreads();
+
+  // ---------------- phase 2: Riemann problems at the faces ----------------
+  const R gam = R(P.gamma);
+  for (int t = threadIdx.x; t < G::n; t += blockDim.x) {
+    int i, j, k;
+    G::decode(t, i, j, k);
+    if (G::along(i, j, k) < 0) continue;
+    R VL[8], VR[8];
+#pragma unroll
+    for (int q = 0; q < 7; ++q) {
+      VL[wslot(q)] = sWp[q * G::n + t - G::stride];
+      VR[wslot(q)] = sWm[q * G::n + t];
+    }
+    VL[HGC] = gam; VR[HGC] = gam;
+    R F[6];
+    hllc<R, DIR>(P, VL, VR, F, st);
+#pragma unroll
+    for (int n = 0; n < 6; ++n) sF[n * G::n + t] = F[n];
+    R fv = R(0), fe = R(0);
+    if (P.use_aux_eint) {                         // hy_getFaceFlux.F90:433-442
+      if (F[FDENS] > R(0)) { fv = F[FDENS] / VL[HD]; fe = F[FDENS] * VL[HEI]; }
+      else { fv = F[FDENS] / VR[HD]; fe = F[FDENS] * VR[HEI]; }
+    }
+    sF[FEINT * G::n + t] = fe;
+    sF[FVOLU * G::n + t] = fv;
+  }
+  __syncthreads();
+
+  // ---------------- phase 3: conservative update ----------------
+  const double dtd = dt / delta;
+  CflCand cand; cand.key = 0.0; cand.val = 0.0; cand.idx = 0x7fffffff;
+  for (int t = threadIdx.x; t < G::n; t += blockDim.x) {
+    int i, j, k;
+    G::decode(t, i, j, k);
+    int a = G::along(i, j, k);
+    if (a < 0 || a >= G::nd) continue;
+    const int loc = (k * NY + j) * NX + i;
+    const size_t off = (size_t)b * NCB + loc;
+    double FL[NFLX], FR[NFLX];
+#pragma unroll
+    for (int n = 0; n < NFLX; ++n) { FL[n] = double(sF[n * G::n + t]); FR[n] = double(sF[n * G::n + t + G::stride]); }
+    double U[5];
+    if (FIRST) {
+      double rho = P.s_in[0][off], vx = P.s_in[1][off], vy = P.s_in[2][off], vz = P.s_in[3][off], e = P.s_in[4][off];
+      double ekin = 0.5 * (vx * vx + vy * vy + vz * vz);
+      U[0] = rho; U[1] = vx * rho; U[2] = vy * rho; U[3] = vz * rho; U[4] = rho * (e + ekin);
+    } else {
+#pragma unroll
+      for (int n = 0; n < 5; ++n) U[n] = ACC[n * ncells + off];
+    }
+#pragma unroll
+    for (int n = 0; n < 5; ++n) U[n] = U[n] - dtd * (FR[n] - FL[n]);
+    const double ea = FL[FEINT] - FR[FEINT], eb = FL[FVOLU] - FR[FVOLU];
+    const double sp = double(sWm[4 * G::n + t]) + double(sWp[4 * G::n + t]);   // N05 + P05
+    if (!LAST) {
+#pragma unroll
+      for (int n = 0; n < 5; ++n) ACC[n * ncells + off] = U[n];
+      double *ax = AUX + (size_t)(DIR - 1) * 3 * ncells;
+      ax[off] = ea; ax[ncells + off] = eb; ax[2 * ncells + off] = sp;
+    } else {
+#pragma unroll
+      for (int n = 0; n < 5; ++n) U[n] = U[n] + 0.0;       // + dt*(Sgeo + Sphys), both +0 here
+      const double rho0 = P.s_in[0][off], e0 = P.s_in[4][off];
+      double IntEner = 0.0;
+      if (P.use_aux_eint) {
+        // n+1/2 pressure: scrch_Ptr(1) of hy_getFaceFlux.F90:551-557 and the
+        // y/z averages
+        double pb;
+        const double sx = AUX[2 * ncells + off];
+        if (NDIM == 2) {
+          pb = (0.5 * sx) * 0.5 + sp * 0.25;
+        } else {
+          const double sy = AUX[3 * ncells + 2 * ncells + off];
+          pb = ((0.5 * sx) * 0.5 + sy * 0.25) * 4.0;
+          pb = (pb + sp) / 6.0;
+        }
+        IntEner = rho0 * e0;
+        {
+          const double *ax = AUX;
+          IntEner = IntEner + dt / P.del[0] * (ax[off] + pb * ax[ncells + off]);
+        }
+        if (NDIM == 2) {
+          IntEner = IntEner + dt / P.del[1] * (ea + pb * eb);
+        } else {
+          const double *ay = AUX + 3 * ncells;
+          IntEner = IntEner + dt / P.del[1] * (ay[off] + pb * ay[ncells + off]);
+          IntEner = IntEner + dt / P.del[2] * (ea + pb * eb);
+        }
+        IntEner = IntEner + dt * 0.;
+      }
+      // hy_unsplitUpdate.F90:811-893
+      double dens = rmax(U[0], P.smlrho);
+      double vx = U[1] / dens, vy = U[2] / dens, vz = U[3] / dens;
+      double ener = U[4] / dens;
+      double eaux = IntEner / dens;
+      // hy_energyFix.F90:188-253
+      double ekin = 0.5 * (vx * vx + vy * vy + vz * vz);
+      double eint = ener - ekin - 0.0;
+      double newE;
+      if (!P.use_aux_eint || eint > P.eswitch * (ekin + 0.0)) newE = rmax(P.smalle, eint);
+      else newE = rmax(P.smalle, eaux);
+      ener = newE + ekin;
+      // Eos_wrapped(MODE_DENS_EI)
+      double e = newE;
+      if (ener - ekin > rmax(P.smalle, P.eswitch * ekin)) e = ener - ekin;
+      P.s_out[0][off] = dens; P.s_out[1][off] = vx; P.s_out[2][off] = vy; P.s_out[3][off] = vz;
+      P.s_out[4][off] = e;
+      if (!(isfinite(dens) && isfinite(vx) && isfinite(vy) && isfinite(vz) && isfinite(e))) st |= ST_NAN;
+      // CFL: Hydro_computeDt.F90:260-284 on the new state
+      double pres = dens * e * P.gam1inv;
+      double c2 = P.gamma * pres / dens;
+      double cs = sqrt(c2);
+      double dtl = (fabs(vx - 0.) + cs) * (1.0 / P.del[0]);
+      if (NDIM > 1) dtl = rmax(dtl, (fabs(vy - 0.) + cs) * (1.0 / P.del[1]));
+      if (NDIM > 2) dtl = rmax(dtl, (fabs(vz - 0.) + cs) * (1.0 / P.del[2]));
+      CflCand c; c.key = dtl * P.cfl; c.val = dtl; c.idx = loc;
+      cfl_merge(cand, c);
+    }
+  }
+  if (LAST) cfl_block_reduce<NX, NY, NZ>(cand, b, P.cfl, part);
+  if (st) atomicOr(P.status, st);
+}
+
+// CFL reduction of a stored state (Hydro_computeDt on its own).
+template <int NDIM, int NX, int NY, int NZ>
+__global__ void __launch_bounds__(256) k_cfl(const DevParams P, CflPart *part) {
+  constexpr int NCB = NX * NY * NZ;
+  const int b = blockIdx.x;
+  CflCand cand; cand.key = 0.0; cand.val = 0.0; cand.idx = 0x7fffffff;
+  for (int loc = threadIdx.x; loc < NCB; loc += blockDim.x) {
+    size_t off = (size_t)b * NCB + loc;
+    double dens = P.s_in[0][off], vx = P.s_in[1][off], vy = P.s_in[2][off], vz = P.s_in[3][off], e = P.s_in[4][off];
+    double pres = dens * e * P.gam1inv;
+    double cs = sqrt(P.gamma * pres / dens);
+    double dtl = (fabs(vx - 0.) + cs) * (1.0 / P.del[0]);
+    if (NDIM > 1) dtl = rmax(dtl, (fabs(vy - 0.) + cs) * (1.0 / P.del[1]));
+    if (NDIM > 2) dtl = rmax(dtl, (fabs(vz - 0.) + cs) * (1.0 / P.del[2]));
+    CflCand c; c.key = dtl * P.cfl; c.val = dtl; c.idx = loc;
+    cfl_merge(cand, c);
+  }
+  cfl_block_reduce<NX, NY, NZ>(cand, b, P.cfl, part);
+}
+
+}  // namespace fhy

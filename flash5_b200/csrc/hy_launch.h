@@ -1,0 +1,29 @@
+// hy_launch.h -- interface between the C-ABI (flash_hy.cu) and the kernel
+// variants (hy_variant.cu, compiled once per arithmetic variant).
+#pragma once
+#include "hy_kernels.cuh"
+
+namespace fhy {
+
+struct StepArgs {
+  DevParams P;
+  void *sig;          // transverse-flux scratch, sizeof(R) * 6 * ndim * box * nlaunch
+  double *acc;        // [5][ncells] conservative-update accumulator
+  double *aux;        // [ndim-1][3][ncells] eint-update terms of the earlier directions
+  size_t ncells;
+  CflPart *part;      // per-block CFL results
+  int nlaunch;        // CTAs (blocks updated)
+  int threads;        // threads per CTA
+  cudaStream_t stream;
+};
+
+// Enqueue one hydro step; returns the number of kernel launches, or -1 for an
+// unsupported block shape, or -2 for a launch error.
+int step_fp64_exact(const StepArgs &a, int ndim, int nx, int ny, int nz);
+int step_fp64_fma(const StepArgs &a, int ndim, int nx, int ny, int nz);
+int step_mixed(const StepArgs &a, int ndim, int nx, int ny, int nz);
+// CFL reduction of the stored state (one launch).
+int cfl_state(const StepArgs &a, int ndim, int nx, int ny, int nz);
+size_t sig_bytes_per_block(int ndim, int nx, int ny, int nz, int real_bytes);
+
+}  // namespace fhy

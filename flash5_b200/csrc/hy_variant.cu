@@ -1,0 +1,70 @@
+// hy_variant.cu -- instantiates the step kernels for one arithmetic variant.
+// Compiled three times (see flash5_b200/build.py):
+//   FHY_VARIANT=1  FP64, no FMA contraction (--fmad=false): the parity path
+//   FHY_VARIANT=2  FP64 with FMA contraction
+//   FHY_VARIANT=3  FP32 reconstruction / Riemann solve, FP64 update
+#include "hy_launch.h"
+
+#if FHY_VARIANT == 3
+typedef float Real;
+#define FHY_ENTRY step_mixed
+#elif FHY_VARIANT == 2
+typedef double Real;
+#define FHY_ENTRY step_fp64_fma
+#else
+typedef double Real;
+#define FHY_ENTRY step_fp64_exact
+#endif
+
+namespace fhy {
+
+template <int NDIM, int NX, int NY, int NZ, int DIR, bool FIRST, bool LAST>
+static bool launch_dir(const StepArgs &a) {
+  using G = DirGeom<NDIM, NX, NY, NZ, Real, DIR>;
+  auto kern = k_dir<NDIM, NX, NY, NZ, Real, DIR, FIRST, LAST>;
+  const size_t smem = G::smem_bytes();
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return false;
+  kern<<<a.nlaunch, a.threads, smem, a.stream>>>(a.P, (const Real *)a.sig, a.acc, a.aux, a.ncells, a.part);
+  return cudaGetLastError() == cudaSuccess;
+}
+
+template <int NDIM, int NX, int NY, int NZ>
+static int run(const StepArgs &a) {
+  k_sig<NDIM, NX, NY, NZ, Real><<<a.nlaunch, a.threads, 0, a.stream>>>(a.P, (Real *)a.sig);
+  if (cudaGetLastError() != cudaSuccess) return -2;
+  bool ok;
+  if (NDIM == 2) {
+    ok = launch_dir<NDIM, NX, NY, NZ, 1, true, false>(a) && launch_dir<NDIM, NX, NY, NZ, 2, false, true>(a);
+    return ok ? 3 : -2;
+  }
+  ok = launch_dir<NDIM, NX, NY, NZ, 1, true, false>(a) && launch_dir<NDIM, NX, NY, NZ, 2, false, false>(a) &&
+       launch_dir<NDIM, NX, NY, NZ, 3, false, true>(a);
+  return ok ? 4 : -2;
+}
+
+int FHY_ENTRY(const StepArgs &a, int ndim, int nx, int ny, int nz) {
+  if (ndim == 2 && nx == 8 && ny == 8) return run<2, 8, 8, 1>(a);
+  if (ndim == 2 && nx == 16 && ny == 16) return run<2, 16, 16, 1>(a);
+  if (ndim == 3 && nx == 8 && ny == 8 && nz == 8) return run<3, 8, 8, 8>(a);
+  return -1;
+}
+
+#if FHY_VARIANT == 1
+template <int NDIM, int NX, int NY, int NZ>
+static int run_cfl(const StepArgs &a) {
+  k_cfl<NDIM, NX, NY, NZ><<<a.nlaunch, a.threads, 0, a.stream>>>(a.P, a.part);
+  return cudaGetLastError() == cudaSuccess ? 1 : -2;
+}
+int cfl_state(const StepArgs &a, int ndim, int nx, int ny, int nz) {
+  if (ndim == 2 && nx == 8 && ny == 8) return run_cfl<2, 8, 8, 1>(a);
+  if (ndim == 2 && nx == 16 && ny == 16) return run_cfl<2, 16, 16, 1>(a);
+  if (ndim == 3 && nx == 8 && ny == 8 && nz == 8) return run_cfl<3, 8, 8, 8>(a);
+  return -1;
+}
+size_t sig_bytes_per_block(int ndim, int nx, int ny, int nz, int real_bytes) {
+  size_t box = (size_t)(nx + 2) * (ndim > 1 ? ny + 2 : 1) * (ndim > 2 ? nz + 2 : 1);
+  return box * 6 * ndim * real_bytes;
+}
+#endif
+
+}  // namespace fhy

@@ -1,0 +1,109 @@
+"""Host-side mirror of FLASH5's Hydro interface over the CUDA C-ABI.
+
+``Hydro`` mirrors ``Hydro_init`` / ``Hydro(simTime, dt, dtOld, sweepOrder)``
+/ ``Hydro_computeDt`` (source/physics/Hydro/Hydro_interface.F90:12-137,
+HydroMain/unsplit/Hydro.F90:6-343) and the FLASH4-style
+``Hydro(blockCount, blockList, timeEndAdv, dt, dtOld, sweepOrder)``.
+Errors come back as ``HydroError`` with the C-ABI status bits; FLASH aborts
+the run in the same situations (Driver_abortFlash).
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+
+
+class HydroError(RuntimeError):
+    def __init__(self, status, msg=""):
+        self.status = status
+        names = [n for n in dir(abi) if n.startswith("ERR_") and getattr(abi, n) & status]
+        super().__init__(f"flash_hy status {status:#x} {names} {msg}")
+
+
+class Hydro:
+    """One device context holding the block store of a grid."""
+
+    def __init__(self, params, grid, device=0):
+        self.lib = abi.load_library()
+        self.params = params
+        self.grid = grid
+        self._gdesc = grid.desc()
+        self.ctx = C.c_void_p()
+        st = self.lib.flash_hy_create(C.byref(params), C.byref(self._gdesc), device, C.byref(self.ctx))
+        if st:
+            msg = self.last_error() if self.ctx else ""
+            if self.ctx:
+                self.lib.flash_hy_destroy(self.ctx)
+                self.ctx = C.c_void_p()
+            raise HydroError(st, msg)
+        self.varmap = abi.flash_varmap()
+
+    # -- lifecycle -------------------------------------------------------
+    def close(self):
+        if self.ctx:
+            self.lib.flash_hy_destroy(self.ctx)
+            self.ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def last_error(self):
+        buf = C.create_string_buffer(512)
+        self.lib.flash_hy_last_error(self.ctx, buf, 512)
+        return buf.value.decode()
+
+    def _check(self, st):
+        if st:
+            raise HydroError(st, self.last_error())
+
+    # -- Grid data --------------------------------------------------------
+    def upload(self, unk, layout=abi.LAYOUT_VAR_FASTEST):
+        unk = np.ascontiguousarray(unk, dtype=np.float64)
+        self._check(self.lib.flash_hy_upload(self.ctx, unk.ctypes.data_as(C.POINTER(C.c_double)), layout,
+                                             unk.shape[-1] if layout == abi.LAYOUT_VAR_FASTEST else unk.shape[1],
+                                             C.byref(self.varmap)))
+
+    def download(self, unk, layout=abi.LAYOUT_VAR_FASTEST):
+        assert unk.dtype == np.float64 and unk.flags.c_contiguous
+        self._check(self.lib.flash_hy_download(self.ctx, unk.ctypes.data_as(C.POINTER(C.c_double)), layout,
+                                               unk.shape[-1] if layout == abi.LAYOUT_VAR_FASTEST else unk.shape[1],
+                                               C.byref(self.varmap)))
+        return unk
+
+    # -- the hot path -----------------------------------------------------
+    def __call__(self, simTime, dt, dtOld, sweepOrder=0):
+        """Hydro(simTime, dt, dtOld, sweepOrder): enqueue one step (async)."""
+        self._check(self.lib.flash_hy_step(self.ctx, simTime, dt, dtOld, sweepOrder))
+
+    def step_blocks(self, blockList, timeEndAdv, dt, dtOld, sweepOrder=0):
+        bl = np.ascontiguousarray(blockList, dtype=np.int32)
+        self._check(self.lib.flash_hy_step_blocks(self.ctx, len(bl), bl.ctypes.data_as(C.POINTER(C.c_int)),
+                                                  timeEndAdv, dt, dtOld, sweepOrder))
+
+    def compute_dt(self):
+        """Hydro_computeDt + the MINLOC reduction: (dt, (i, j, k, level, block))."""
+        dt = C.c_double()
+        loc = (C.c_int * 5)()
+        self._check(self.lib.flash_hy_compute_dt(self.ctx, C.byref(dt), loc))
+        return dt.value, tuple(loc)
+
+    def sync(self):
+        self._check(self.lib.flash_hy_sync(self.ctx))
+
+    @property
+    def stream(self):
+        return self.lib.flash_hy_stream(self.ctx)
+
+    @property
+    def last_launch_count(self):
+        return self.lib.flash_hy_last_launch_count(self.ctx)
+
+
+def next_dt(dt_cfl, dt_old, tstep_change_factor=2.0, dtmin=1e-10, dtmax=1e5):
+    """Driver_computeDt.F90:431-447: limit the growth and clamp."""
+    dt = min(dt_cfl, dt_old * tstep_change_factor)
+    return min(max(dt, dtmin), dtmax)

@@ -1,0 +1,164 @@
+/*
+ * flash_hy.h -- C ABI of the B200 unsplit-hydro block update.
+ *
+ * Drop-in boundary for FLASH5's directionally unsplit hydro step over the leaf
+ * blocks of a block-structured grid.  Every entry point takes plain pointers
+ * and sizes, returns an int status (0 = OK, otherwise FLASH_HY_ERR_* bit
+ * flags) and never aborts the process.  The library owns device memory; the
+ * caller owns host memory.  One context per GPU; calls on one context are not
+ * thread-safe.
+ *
+ * Reference interfaces replaced (paths inside mbdevpl/FLASH5):
+ *   Hydro(simTime, dt, dtOld, sweepOrder)
+ *       source/physics/Hydro/Hydro_interface.F90:52-57,
+ *       source/physics/Hydro/HydroMain/unsplit/Hydro.F90:6-343
+ *   Hydro_init            source/physics/Hydro/HydroMain/unsplit/Hydro_init.F90:60-688
+ *   Hydro_computeDt       source/physics/Hydro/Hydro_interface.F90:12-32,
+ *                         source/physics/Hydro/HydroMain/unsplit/Hydro_computeDt.F90:63-328
+ *   hy_computeFluxes / hy_updateSolution (per-block API)
+ *                         source/physics/Hydro/localAPI/hy_interface.F90:969,982
+ *   Grid UNK ownership    source/Grid/GridMain/UG/gr_createDomain.F90:127-147,
+ *                         source/Grid/GridMain/AMR/paramesh/Grid_tile.F90:157-182
+ */
+#ifndef FLASH_HY_H
+#define FLASH_HY_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status bits (0 = success) --------------------------------------- */
+#define FLASH_HY_OK                 0
+#define FLASH_HY_ERR_NEG_SOUNDSPEED (1 << 0) /* a^2 <= 0 (hy_eigenParameters.F90:83-86, hy_HLLC.F90:125-127) */
+#define FLASH_HY_ERR_NONPOS_DT      (1 << 1) /* Hydro_computeDt.F90:321-323 */
+#define FLASH_HY_ERR_NEWTON_NOCONV  (1 << 2) /* exact Riemann solver gave up */
+#define FLASH_HY_ERR_NAN            (1 << 3) /* non-finite value in the updated state */
+#define FLASH_HY_ERR_TIMEOUT        (1 << 4) /* a bounded device wait expired */
+#define FLASH_HY_ERR_BAD_ARG        (1 << 5)
+#define FLASH_HY_ERR_CUDA           (1 << 6)
+#define FLASH_HY_ERR_UNSUPPORTED    (1 << 7)
+
+/* ---- enumerations (numeric values follow FLASH's own headers) ---------- */
+/* Riemann solvers: UHD.h:366-372 numbering; EXACT has no FLASH counterpart */
+#define FLASH_HY_RS_HLLC   4
+#define FLASH_HY_RS_EXACT  100
+/* slope limiters: UHD.h:15-19 */
+#define FLASH_HY_LIM_MINMOD  1
+#define FLASH_HY_LIM_MC      2
+#define FLASH_HY_LIM_HYBRID  3
+#define FLASH_HY_LIM_VANLEER 4
+#define FLASH_HY_LIM_LIMITED 5
+/* boundary conditions: source/Simulation/constants.h:62-64 */
+#define FLASH_HY_BC_REFLECTING (-31)
+#define FLASH_HY_BC_OUTFLOW    (-32)
+#define FLASH_HY_BC_PERIODIC   (-135)
+/* arithmetic of the reconstruction + flux stage */
+#define FLASH_HY_PREC_FP64   0  /* FP64 everywhere, no FMA contraction   */
+#define FLASH_HY_PREC_FP64_FMA 1 /* FP64 everywhere, FMA contraction on  */
+#define FLASH_HY_PREC_MIXED  2  /* FP32 reconstruction/flux, FP64 update */
+/* host UNK layouts: default FLASH unk(var,i,j,k,blk) and --index-reorder
+ * unk(i,j,k,var,blk) (gr_createDomain.F90:133-135, bin/Readme.Reorder) */
+#define FLASH_HY_LAYOUT_VAR_FASTEST 0
+#define FLASH_HY_LAYOUT_XYZ_FASTEST 1
+/* update modes of hy_computeFluxes (UHD.h:24-27) */
+#define FLASH_HY_UPDATE_NONE 0
+#define FLASH_HY_UPDATE_ALL  3
+
+/* ---- variable map: 1-based *_VAR indices of the caller's UNK ---------- */
+/* FLASH sorts VARIABLE declarations alphabetically (bin/unitCfg.py:713-714);
+ * for +uhd with the gamma EOS: DENS=1 EINT=2 ENER=3 GAMC=4 GAME=5 PRES=6
+ * SHOK=7 TEMP=8 VELX=9 VELY=10 VELZ=11.  0 = variable absent.           */
+typedef struct flash_hy_varmap {
+  int dens, eint, ener, gamc, game, pres, temp, velx, vely, velz;
+} flash_hy_varmap;
+
+/* ---- runtime parameters (names follow unsplit/Config:105-159) ---------- */
+typedef struct flash_hy_params {
+  int    order;            /* 3 = PPM (the only order on this path)       */
+  int    riemann_solver;   /* FLASH_HY_RS_*                               */
+  int    slope_limiter;    /* FLASH_HY_LIM_*                              */
+  int    char_limiting;    /* charLimiting                                */
+  int    use_flattening;   /* use_flattening                              */
+  int    use_steepening;   /* use_steepening                              */
+  int    use_aux_eint;     /* use_auxEintEqn                              */
+  int    use_3d_full_ctu;  /* use_3dFullCTU                               */
+  int    precision;        /* FLASH_HY_PREC_*                             */
+  int    learned_guess;    /* exact solver: seed Newton with the MLP      */
+  double limited_slope_beta;  /* LimitedSlopeBeta                         */
+  double f_pres_in_mom_flux;  /* hy_fPresInMomFlux                        */
+  double cfl;
+  double eint_switch;      /* eintSwitch                                  */
+  double smlrho, smallp, smalle, tiny;
+  double gamma;            /* eos_gamma                                   */
+  double gas_constant;     /* eos_gasConstant (PhysicalConstants "ideal gas constant") */
+  double single_species_a; /* eos_singleSpeciesA                          */
+} flash_hy_params;
+
+/* ---- grid descriptor ---------------------------------------------------
+ * Blocks of nxb x nyb x nzb interior cells.  FLASH keeps NGUARD=4 guard
+ * layers (unsplit/Config:209-211); the device keeps none and fills halos
+ * inside the kernels.  Block b sits at integer block coordinates
+ * block_coords[3*b .. 3*b+2] of its refinement level block_level[b]
+ * (1-based, as tileDesc%level); level L has 2^(L-1) times the level-1 block
+ * count per axis (nblk_l1[]).  A uniform grid uses one level.           */
+typedef struct flash_hy_grid_desc {
+  int ndim;
+  int nxb, nyb, nzb;
+  int nguard;              /* guard layers of the host UNK arrays (0 or 4) */
+  int nblocks;
+  int nblk_l1[3];          /* level-1 blocks per axis                       */
+  int max_level;
+  const int *block_coords; /* [3*nblocks]                                   */
+  const int *block_level;  /* [nblocks]                                     */
+  double domain_lo[3], domain_hi[3];
+  int bc[6];               /* xl, xr, yl, yr, zl, zr: FLASH_HY_BC_*         */
+} flash_hy_grid_desc;
+
+typedef struct flash_hy_ctx flash_hy_ctx;
+
+/* Hydro_init + Grid block storage allocation.  device: CUDA ordinal. */
+int flash_hy_create(const flash_hy_params *params, const flash_hy_grid_desc *grid,
+                    int device, flash_hy_ctx **ctx_out);
+int flash_hy_destroy(flash_hy_ctx *ctx);
+
+/* Copy the caller's UNK (host memory, nunk variables per cell, guard layers
+ * as grid->nguard) into the device block store and apply the gamma-law EOS
+ * in MODE_DENS_EI to every interior cell, as Grid_initDomain does after
+ * Simulation_initBlock (GridMain/UG/Grid_initDomain.F90:85).             */
+int flash_hy_upload(flash_hy_ctx *ctx, const double *unk, int layout, int nunk,
+                    const flash_hy_varmap *vars);
+/* Write the device state back into the caller's UNK interiors: DENS, VEL*,
+ * EINT plus the EOS outputs PRES, TEMP, GAMC, GAME, ENER
+ * (Eos_putData semantics).  Guard cells are left untouched.             */
+int flash_hy_download(flash_hy_ctx *ctx, double *unk, int layout, int nunk,
+                      const flash_hy_varmap *vars);
+
+/* Hydro(simTime, dt, dtOld, sweepOrder): guard-cell fill (with EOS on the
+ * guard cells), reconstruction, Riemann solve, conservative update, energy
+ * fix and EOS on every leaf block, one launch sequence on the context's
+ * stream.  sweepOrder is accepted and ignored, as in the unsplit solver
+ * (unsplit/Hydro.F90:45-48).  The CFL reduction of the new state is fused
+ * into the update and cached for flash_hy_compute_dt.                    */
+int flash_hy_step(flash_hy_ctx *ctx, double simTime, double dt, double dtOld,
+                  int sweepOrder);
+/* FLASH4-style Hydro(blockCount, blockList, timeEndAdv, dt, dtOld,
+ * sweepOrder) / hy_uhd_unsplit: update only the listed blocks (0-based
+ * indices into the descriptor's block order).                           */
+int flash_hy_step_blocks(flash_hy_ctx *ctx, int blockCount, const int *blockList,
+                         double timeEndAdv, double dt, double dtOld, int sweepOrder);
+/* Hydro_computeDt + the MPI_MINLOC reduction of Driver_computeDt.F90:376-377:
+ * dt_out = cfl / max_cells max_d (|u_d| + c_s)/dx_d; minloc_out = (i, j, k,
+ * level, block) with FLASH's 1-based guard-inclusive cell indices.      */
+int flash_hy_compute_dt(flash_hy_ctx *ctx, double *dt_out, int minloc_out[5]);
+
+/* Device-side access for callers that keep the state resident. */
+int flash_hy_sync(flash_hy_ctx *ctx);
+void *flash_hy_stream(flash_hy_ctx *ctx);        /* cudaStream_t of the context */
+int flash_hy_last_error(flash_hy_ctx *ctx, char *buf, int len);
+/* Number of kernel launches issued by the last flash_hy_step call. */
+int flash_hy_last_launch_count(flash_hy_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FLASH_HY_H */

@@ -1,0 +1,990 @@
+/*
+ * flash_hy_oracle.c -- TEST INFRASTRUCTURE ONLY (the oracle).
+ *
+ * A plain-C FP64 CPU restatement of FLASH5's directionally unsplit hydro
+ * block update for pure hydrodynamics on a Cartesian uniform block grid:
+ * guard-cell fill with EOS on the guard cells, PPM reconstruction with
+ * characteristic limiting / flattening / optional steepening, transverse and
+ * 3D full-CTU corrections, HLLC fluxes with the auxiliary internal-energy
+ * fluxes, the conservative update, the energy fix, the gamma-law EOS and the
+ * CFL time step.  Every routine cites the Fortran it follows (paths inside
+ * mbdevpl/FLASH5, source/physics/Hydro/HydroMain/unsplit unless stated).
+ *
+ * It is only ever used as the checker: by tests/, by __graft_entry__.smoke()
+ * and by bench.py's CPU-baseline leg.  The product path never calls it.
+ *
+ * PARITY STATUS: unpinned against the reference's own outputs.  The
+ * reference is Fortran + MPI and cannot be compiled in this environment (no
+ * Fortran compiler), and its repository holds no golden outputs for this
+ * path.  The only known answer the reference ships is the analytic Sod
+ * shock-tube solution (Simulation/SimulationMain/Sod/shocktube.pro), which
+ * the tests use to check this restatement's physics.
+ *
+ * Build: gcc -O2 -std=c11 -ffp-contract=off -fno-fast-math -fopenmp -fPIC
+ * -shared (no FMA contraction, IEEE division and sqrt), see oracle/Makefile.
+ *
+ * UNK layout: unk[(((blk*NZT + k)*NYT + j)*NXT + i)*NUNK + var], the default
+ * FLASH unk(var,i,j,k,blk) ordering with NGUARD guard layers, variables in
+ * FLASH's alphabetical order for +uhd with the gamma EOS (bin/unitCfg.py:713).
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include <float.h>
+#include "../include/flash_hy.h"
+
+/* ---- UNK variables, 0-based (DENS_VAR=1 ... VELZ_VAR=11 in Flash.h) ---- */
+enum { DENS_V = 0, EINT_V, ENER_V, GAMC_V, GAME_V, PRES_V, SHOK_V, TEMP_V,
+       VELX_V, VELY_V, VELZ_V, NUNK = 11 };
+/* ---- primitive slots of UHD.h:374-383 (HY_DENS=1..HY_EINT=8), 0-based -- */
+enum { HD = 0, HVX, HVY, HVZ, HP, HGC, HGE, HEI, NSLOT = 9 };
+/* ---- flux slots of OnlyHydro/Config:6-13 (F01Dens..F08VOLU), 0-based --- */
+enum { FDENS = 0, FXMOM, FYMOM, FZMOM, FENER, FPRES, FEINT, FVOLU, NFLX = 8 };
+#define NGUARD 4
+#define NWAVE 5
+
+typedef struct {
+  const flash_hy_params *p;
+  int ndim, nxb, nyb, nzb, nxt, nyt, nzt;
+  int k2, k3;               /* 1 if the dimension exists (y, z)            */
+  double gam1inv;           /* 1/eos_gammam1, eos_idealGamma.F90:323-326   */
+  double ggprodinv;         /* 1/(eos_gammam1*R), eos_idealGamma.F90:262   */
+  int status;
+} ctx_t;
+
+static inline size_t cidx(const ctx_t *c, int i, int j, int k) {
+  return ((size_t)k * c->nyt + j) * c->nxt + i;
+}
+
+/* ===================================================================== */
+/* Slope limiters: hy_slopeLimiters.F90:38-60                             */
+/* ===================================================================== */
+static inline double f_sign(double a, double b) { return copysign(fabs(a), b); }
+static double lim_vanleer(double a, double b) {           /* :38-46 */
+  if (a * b <= 0.) return 0.;
+  return 2. * a * b / (a + b);
+}
+static double lim_mc(double a, double b) {                /* :49-53 */
+  double m = fabs(a);
+  double t = .25 * fabs(a + b);
+  if (t < m) m = t;
+  if (fabs(b) < m) m = fabs(b);
+  return (f_sign(1., a) + f_sign(1., b)) * m;
+}
+static double lim_minmod(double a, double b) {            /* :56-60 */
+  double m = fabs(a) < fabs(b) ? fabs(a) : fabs(b);
+  return .5 * (f_sign(1., a) + f_sign(1., b)) * m;
+}
+static inline double fmax2(double a, double b) { return a > b ? a : b; }
+static inline double fmin2(double a, double b) { return a < b ? a : b; }
+
+/* ===================================================================== */
+/* Eigen system in primitive variables                                   */
+/* ===================================================================== */
+/* hy_eigenParameters.F90:71-89 (pure hydro branch) */
+static void eigen_parameters(ctx_t *c, const double *V, int dir, double *un, double *cf) {
+  *un = V[HVX + dir - 1];
+  double a2 = V[HGC] * V[HP] / V[HD];
+  if (a2 <= 0.) c->status |= FLASH_HY_ERR_NEG_SOUNDSPEED;  /* Driver_abortFlash in FLASH */
+  *cf = sqrt(a2);
+}
+/* hy_eigenValue.F90:46-50 */
+static void eigen_value(double lam[NWAVE], double un, double cf) {
+  lam[0] = un - cf; lam[1] = un; lam[2] = un; lam[3] = un; lam[4] = un + cf;
+}
+/* OnlyHydro/hy_eigenVector.F90:95-152, primitive (cons=.false.) branch.
+ * leig[var][wave], reig[var][wave] as LeftEigvec(var,wave). */
+static void eigen_vector(double leig[5][5], double reig[5][5], const double *V, int dir, double cf) {
+  int v1, v2, v3;
+  if (dir == 1) { v1 = HVX; v2 = HVY; v3 = HVZ; }
+  else if (dir == 2) { v1 = HVY; v2 = HVZ; v3 = HVX; }
+  else { v1 = HVZ; v2 = HVX; v3 = HVY; }
+  memset(leig, 0, sizeof(double) * 25);
+  memset(reig, 0, sizeof(double) * 25);
+  double dinv = 1. / V[HD];
+  double a2 = cf * cf;
+  double a2inv = 1. / a2;
+  double ahinv = 0.5 / cf;
+  double Na = 0.5 * a2inv;
+  leig[v1][0] = -ahinv;
+  leig[HP][0] = dinv * Na;
+  leig[v2][1] = 1.;
+  leig[HD][2] = 1.;
+  leig[HP][2] = -a2inv;
+  leig[v3][3] = 1.;
+  leig[v1][4] = ahinv;
+  leig[HP][4] = leig[HP][0];
+  reig[HD][0] = V[HD];
+  reig[v1][0] = -cf;
+  reig[HP][0] = V[HD] * a2;
+  reig[v2][1] = 1.;
+  reig[HD][2] = 1.;
+  reig[v3][3] = 1.;
+  reig[HD][4] = V[HD];
+  reig[v1][4] = cf;
+  reig[HP][4] = reig[HP][0];
+}
+/* Fortran dot_product, summed in index order */
+static inline double dot5(const double a[5][5], int col, const double *b, int n) {
+  double s = 0.;
+  for (int v = 0; v < n; ++v) s = s + a[v][col] * b[v];
+  return s;
+}
+
+/* ===================================================================== */
+/* hy_TVDslope.F90:76-246 (characteristic or primitive limited slopes)   */
+/* ===================================================================== */
+static double limit2(int lim, double beta, double d1, double d2) {
+  switch (lim) {
+    case FLASH_HY_LIM_MINMOD:  return lim_minmod(d1, d2);
+    case FLASH_HY_LIM_MC:      return lim_mc(d1, d2);
+    case FLASH_HY_LIM_VANLEER: return lim_vanleer(d1, d2);
+    case FLASH_HY_LIM_LIMITED: /* :213-245 */
+      if (d2 > 0.) return fmax2(0., fmax2(fmin2(beta * d1, d2), fmin2(d1, beta * d2)));
+      return fmin2(0., fmin2(fmax2(beta * d1, d2), fmax2(d1, beta * d2)));
+  }
+  return 0.;
+}
+static void tvd_slope(const ctx_t *c, const double *VL, const double *V0, const double *VR,
+                      double leig[5][5], double delbar[NSLOT]) {
+  const flash_hy_params *p = c->p;
+  double dL[NSLOT], dR[NSLOT];
+  for (int n = 0; n < NSLOT; ++n) { delbar[n] = 0.; dL[n] = V0[n] - VL[n]; dR[n] = VR[n] - V0[n]; }
+  int lim = p->slope_limiter;
+  if (p->char_limiting) {
+    for (int k = 0; k < NWAVE; ++k) {
+      double a = dot5(leig, k, dL, 5), b = dot5(leig, k, dR, 5);
+      int lk = lim;
+      if (lim == FLASH_HY_LIM_HYBRID) lk = (k == 2) ? FLASH_HY_LIM_MC : FLASH_HY_LIM_MINMOD; /* :128-147 */
+      delbar[k] = limit2(lk, p->limited_slope_beta, a, b);
+    }
+    for (int k = HGC; k <= HEI; ++k) {
+      int lk = (lim == FLASH_HY_LIM_HYBRID) ? FLASH_HY_LIM_MC : lim;
+      delbar[k] = limit2(lk, p->limited_slope_beta, dL[k], dR[k]);
+    }
+  } else {
+    for (int k = 0; k <= HEI; ++k) {
+      int lk = lim;
+      /* hybrid: mc for DENS, GAMC, GAME; minmod for the velocities and PRES; EINT is in
+       * neither case list and keeps delbar = 0 (:188-196) */
+      if (lim == FLASH_HY_LIM_HYBRID) {
+        if (k == HEI) continue;
+        lk = (k == HD || k == HGC || k == HGE) ? FLASH_HY_LIM_MC : FLASH_HY_LIM_MINMOD;
+      }
+      delbar[k] = limit2(lk, p->limited_slope_beta, dL[k], dR[k]);
+    }
+  }
+}
+
+/* ===================================================================== */
+/* hy_upwindTransverseFlux.F90:75-207 (transOrder = 1)                   */
+/* ===================================================================== */
+static void upwind_transverse_flux(const ctx_t *c, const double *vm1, const double *vc0, const double *vp1,
+                                   const double lam[NWAVE], double leig[5][5], double reig[5][5],
+                                   double sig[8]) {
+  double tf[8];
+  for (int n = 0; n < 8; ++n) sig[n] = 0.;
+  for (int n = 0; n < NWAVE; ++n) {
+    if (lam[n] > 0.) for (int v = 0; v < 5; ++v) tf[v] = vc0[v] - vm1[v];
+    else             for (int v = 0; v < 5; ++v) tf[v] = vp1[v] - vc0[v];
+    double delbar = dot5(leig, n, tf, 5);
+    for (int v = 0; v < 5; ++v) tf[v] = lam[n] * reig[v][n] * delbar;
+    for (int v = 0; v < 5; ++v) sig[v] = sig[v] + tf[v];
+  }
+  if (c->p->use_aux_eint) {   /* :174-188, entropy-wave upwinding of EINT */
+    double t;
+    if (lam[2] > 0.) t = vc0[HEI] - vm1[HEI]; else t = vp1[HEI] - vc0[HEI];
+    sig[HEI] = lam[2] * t;
+  }
+}
+
+/* ===================================================================== */
+/* hy_DataReconstructNormalDir_PPM.F90:181-842                           */
+/* V5: five stencil cells Vmm..Vpp (only Vm,Vc,Vp when transUpdateOnly)  */
+/* ===================================================================== */
+static void ppm(ctx_t *c, int dir, double dt, double delta, const double V5[5][NSLOT],
+                double flat_coeff, int trans_update_only,
+                double lambda0[NWAVE], double leig0[5][5], double reig0[5][5],
+                double Wp[NSLOT], double Wm[NSLOT], double sig[8]) {
+  const flash_hy_params *p = c->p;
+  const int hyEndPrimVar = 5;                         /* HY_ENER          */
+  const int hyEndVar = p->use_aux_eint ? 8 : 5;       /* :197-199          */
+  const double *Vmm = V5[0], *Vm = V5[1], *Vc = V5[2], *Vp = V5[3], *Vpp = V5[4];
+  double un, cf;
+  double dtn = dt / delta, hdtn = 0.5 * dtn;
+  for (int n = 0; n < NSLOT; ++n) { Wp[n] = 0.; Wm[n] = 0.; }
+  /* eigen system at Vc, :319-345 */
+  eigen_parameters(c, Vc, dir, &un, &cf);
+  eigen_value(lambda0, un, cf);
+  eigen_vector(leig0, reig0, Vc, dir, cf);
+  /* transverse flux sig for the other directions, :351-371 */
+  upwind_transverse_flux(c, Vm, Vc, Vp, lambda0, leig0, reig0, sig);
+  if (trans_update_only) return;
+
+  double lambdaP[NWAVE], lambdaN[NWAVE], leigP[5][5], reigP[5][5], leigN[5][5], reigN[5][5];
+  eigen_parameters(c, Vp, dir, &un, &cf);                     /* :380-405 */
+  eigen_value(lambdaP, un, cf);
+  eigen_vector(leigP, reigP, Vp, dir, cf);
+  eigen_parameters(c, Vm, dir, &un, &cf);                     /* :409-435 */
+  eigen_value(lambdaN, un, cf);
+  eigen_vector(leigN, reigN, Vm, dir, cf);
+
+  double delbarN[NSLOT], delbar0[NSLOT], delbarP[NSLOT];     /* :438-441 */
+  tvd_slope(c, Vmm, Vm, Vc, leigN, delbarN);
+  tvd_slope(c, Vm, Vc, Vp, leig0, delbar0);
+  tvd_slope(c, Vc, Vp, Vpp, leigP, delbarP);
+
+  double Flattening = p->use_flattening ? flat_coeff : 0.;    /* :520-524 */
+
+  if (p->char_limiting) {                                     /* :528-570 */
+    double t0[NSLOT], tP[NSLOT], tN[NSLOT];
+    for (int v = 0; v < hyEndPrimVar; ++v) {
+      t0[v] = reig0[v][0] * delbar0[0] + reig0[v][1] * delbar0[1] + reig0[v][2] * delbar0[2]
+            + reig0[v][3] * delbar0[3] + reig0[v][4] * delbar0[4];
+      tP[v] = reigP[v][0] * delbarP[0] + reigP[v][1] * delbarP[1] + reigP[v][2] * delbarP[2]
+            + reigP[v][3] * delbarP[3] + reigP[v][4] * delbarP[4];
+      tN[v] = reigN[v][0] * delbarN[0] + reigN[v][1] * delbarN[1] + reigN[v][2] * delbarN[2]
+            + reigN[v][3] * delbarN[3] + reigN[v][4] * delbarN[4];
+    }
+    for (int v = 0; v < hyEndPrimVar; ++v) { delbar0[v] = t0[v]; delbarP[v] = tP[v]; delbarN[v] = tN[v]; }
+  }
+
+  double vecL[NSLOT], vecR[NSLOT], delW[NSLOT], W6[NSLOT];
+  for (int n = 0; n < NSLOT; ++n) { vecL[n] = 0.; vecR[n] = 0.; delW[n] = 0.; W6[n] = 0.; }
+  for (int n = 0; n < hyEndVar; ++n) {                        /* :579-582 */
+    vecL[n] = 0.5 * (Vc[n] + Vm[n]) - (delbar0[n] - delbarN[n]) / 6.;
+    vecR[n] = 0.5 * (Vc[n] + Vp[n]) - (delbarP[n] - delbar0[n]) / 6.;
+  }
+  if (p->use_steepening) {                                    /* :639-670 */
+    const double eta1 = 20.E0, eta2 = 0.05E0, epsln = 0.01E0, K0 = 0.1E0;
+    double temp1 = Vp[HD] - Vm[HD];
+    if (fabs(temp1) > p->tiny) {
+      double del2rhoR = (Vpp[HD] - 2. * Vp[HD] + Vc[HD]) / (6. * delta * delta);
+      double del2rhoL = (Vc[HD] - 2. * Vm[HD] + Vmm[HD]) / (6. * delta * delta);
+      double eta_steep = (del2rhoL - del2rhoR) * (delta * delta) / temp1;
+      if (del2rhoR * del2rhoL >= 0.) eta_steep = 0.;
+      if (epsln * fmin2(Vp[HD], Vm[HD]) - fabs(Vp[HD] - Vm[HD]) >= 0.) eta_steep = 0.;
+      eta_steep = fmax2(0., fmin2(1., eta1 * (eta_steep - eta2)));
+      double temp2 = fabs(Vp[HP] - Vm[HP]) / fmin2(Vp[HP], Vm[HP]);
+      double temp3 = fabs(Vp[HD] - Vm[HD]) / fmin2(Vp[HD], Vm[HD]);
+      if (Vc[HGE] * K0 * temp3 - temp2 < 0.0) eta_steep = 0.;
+      vecL[HD] = vecL[HD] * (1. - eta_steep) + (Vm[HD] + 0.5 * delbarN[HD]) * eta_steep;
+      vecR[HD] = vecR[HD] * (1. - eta_steep) + (Vp[HD] - 0.5 * delbarP[HD]) * eta_steep;
+    }
+  }
+  if (p->use_flattening) {                                    /* :676-679 */
+    for (int n = 0; n < NSLOT; ++n) {
+      vecL[n] = Flattening * Vc[n] + (1.0 - Flattening) * vecL[n];
+      vecR[n] = Flattening * Vc[n] + (1.0 - Flattening) * vecR[n];
+    }
+  }
+  for (int n = 0; n < hyEndVar; ++n) {                        /* :686-697 */
+    if ((vecR[n] - Vc[n]) * (Vc[n] - vecL[n]) <= 0.) { vecL[n] = Vc[n]; vecR[n] = Vc[n]; }
+    if (6. * (vecR[n] - vecL[n]) * (Vc[n] - 0.5 * (vecL[n] + vecR[n])) > (vecR[n] - vecL[n]) * (vecR[n] - vecL[n]))
+      vecL[n] = 3. * Vc[n] - 2. * vecR[n];
+    if (6. * (vecR[n] - vecL[n]) * (Vc[n] - 0.5 * (vecL[n] + vecR[n])) < -((vecR[n] - vecL[n]) * (vecR[n] - vecL[n])))
+      vecR[n] = 3. * Vc[n] - 2. * vecL[n];
+  }
+  for (int n = 0; n < hyEndVar; ++n) {                        /* :704-706 */
+    delW[n] = vecR[n] - vecL[n];
+    W6[n] = 6. * (Vc[n] - 0.5 * (vecR[n] + vecL[n]));
+  }
+  /* [7] initial guesses, :710-727 */
+  double lambdaMax = fmax2(lambda0[4], 0.);
+  for (int n = 0; n < hyEndPrimVar; ++n)
+    Wp[n] = vecR[n] - lambdaMax * hdtn * (delW[n] - (1.0 - lambdaMax * hdtn * 4. / 3.) * W6[n]);
+  lambdaMax = fmax2(lambda0[2], 0.);
+  for (int n = hyEndPrimVar; n < hyEndVar; ++n)
+    Wp[n] = vecR[n] - lambdaMax * hdtn * (delW[n] - (1.0 - lambdaMax * hdtn * 4. / 3.) * W6[n]);
+  double lambdaMin = -fmin2(lambda0[0], 0.);
+  for (int n = 0; n < hyEndPrimVar; ++n)
+    Wm[n] = vecL[n] + lambdaMin * hdtn * (delW[n] + (1.0 - lambdaMin * hdtn * 4. / 3.) * W6[n]);
+  lambdaMin = -fmin2(lambda0[2], 0.);
+  for (int n = hyEndPrimVar; n < hyEndVar; ++n)
+    Wm[n] = vecL[n] + lambdaMin * hdtn * (delW[n] + (1.0 - lambdaMin * hdtn * 4. / 3.) * W6[n]);
+  /* FLASH_EOS_GAMMA: constant gammas, :733-736 */
+  Wp[HGC] = Vc[HGC]; Wp[HGE] = Vc[HGE];
+  Wm[HGC] = Vc[HGC]; Wm[HGE] = Vc[HGE];
+
+  /* [8] characteristic tracing, HLL-type branch sums over all waves, :753-800 */
+  double sigL[NSLOT], sigR[NSLOT], mW6[NSLOT];
+  for (int n = 0; n < NSLOT; ++n) { sigL[n] = 0.; sigR[n] = 0.; mW6[n] = -W6[n]; }
+  for (int n = 0; n < NWAVE; ++n) {
+    double constA = dot5(leig0, n, delW, hyEndPrimVar);
+    double constB = dot5(leig0, n, mW6, hyEndPrimVar);
+    double x = dtn * lambda0[n];
+    if (p->riemann_solver == 1 /* ROE */) {
+      /* not reachable: this path supports HLLC and the exact solver only */
+    }
+    for (int v = 0; v < hyEndPrimVar; ++v) {
+      vecL[v] = .5 * (-1. - dtn * lambda0[n]) * reig0[v][n] * constA
+              + .25 * (1. + 2. * dtn * lambda0[n] + 4. / 3. * (x * x)) * reig0[v][n] * constB;
+      sigL[v] = sigL[v] + vecL[v];
+      vecR[v] = .5 * (1. - dtn * lambda0[n]) * reig0[v][n] * constA
+              + .25 * (1. - 2. * dtn * lambda0[n] + 4. / 3. * (x * x)) * reig0[v][n] * constB;
+      sigR[v] = sigR[v] + vecR[v];
+    }
+  }
+  /* [10] finalize, :841-842 */
+  for (int n = 0; n < hyEndPrimVar; ++n) {
+    Wm[n] = Vc[n] + W6[n] / 12. + sigL[n];
+    Wp[n] = Vc[n] + W6[n] / 12. + sigR[n];
+  }
+}
+
+/* Primitive slots of a UNK cell (the Data1D extraction of PPM.F90:209-240) */
+static inline void prim_of(const double *u, double V[NSLOT]) {
+  V[HD] = u[DENS_V]; V[HVX] = u[VELX_V]; V[HVY] = u[VELY_V]; V[HVZ] = u[VELZ_V];
+  V[HP] = u[PRES_V]; V[HGC] = u[GAMC_V]; V[HGE] = u[GAME_V]; V[HEI] = u[EINT_V];
+  V[8] = 0.;
+}
+
+/* ===================================================================== */
+/* Per-block work arrays of hy_computeFluxes / hy_getRiemannState         */
+/* ===================================================================== */
+typedef struct {
+  double *flat_coeff, *flat_tilde;       /* [NDIM][cells]                 */
+  double *sig;                            /* [cells][NDIM][8]               */
+  double *lambda;                         /* [cells][NDIM][5]               */
+  double *leig, *reig;                    /* [cells][NDIM][5][5]            */
+  double *face[3];                        /* [cells][16]: P01..P08,N01..N08 */
+  double *flux[3];                        /* [cells][8]                     */
+  double *scrch;                          /* [cells][2]                     */
+} work_t;
+
+static void work_alloc(const ctx_t *c, work_t *w) {
+  size_t nc = (size_t)c->nxt * c->nyt * c->nzt;
+  w->flat_coeff = calloc(3 * nc, sizeof(double));
+  w->flat_tilde = calloc(3 * nc, sizeof(double));
+  w->sig = calloc(nc * 3 * 8, sizeof(double));
+  w->lambda = calloc(nc * 3 * 5, sizeof(double));
+  w->leig = calloc(nc * 3 * 25, sizeof(double));
+  w->reig = calloc(nc * 3 * 25, sizeof(double));
+  for (int d = 0; d < 3; ++d) {
+    w->face[d] = calloc(nc * 16, sizeof(double));
+    w->flux[d] = calloc(nc * NFLX, sizeof(double));
+  }
+  w->scrch = calloc(nc * 2, sizeof(double));
+}
+static void work_free(work_t *w) {
+  free(w->flat_coeff); free(w->flat_tilde); free(w->sig); free(w->lambda);
+  free(w->leig); free(w->reig);
+  for (int d = 0; d < 3; ++d) { free(w->face[d]); free(w->flux[d]); }
+  free(w->scrch);
+}
+
+/* ===================================================================== */
+/* hy_dataReconstOneStep.F90:246-1154 for one cell (order = 3, PPM)       */
+/* ===================================================================== */
+static void data_reconst_one_step(ctx_t *c, const double *U, work_t *w, int ix, int iy, int iz,
+                                  double dt, const double del[3], const int trans_only[3],
+                                  double Wp[3][NSLOT], double Wn[3][NSLOT]) {
+  const int nd = c->ndim;
+  size_t cc = cidx(c, ix, iy, iz);
+  double hdtx = 0.5 * dt / del[0], hdty = 0.5 * dt / del[1], hdtz = 0.5 * dt / del[2];
+  for (int d = 0; d < nd; ++d) {
+    /* Data1D => U(:, ix-kOrder:ix+kOrder), kOrder = 2 (PPM, NGUARD=4) or 1
+     * when only the transverse quantities are needed (:285-301, :485-513) */
+    int kOrder = trans_only[d] ? 1 : 2;
+    double V5[5][NSLOT];
+    memset(V5, 0, sizeof V5);
+    for (int s = -kOrder; s <= kOrder; ++s) {
+      int ii = ix + (d == 0 ? s : 0), jj = iy + (d == 1 ? s : 0), kk = iz + (d == 2 ? s : 0);
+      prim_of(&U[cidx(c, ii, jj, kk) * NUNK], V5[s + 2]);
+    }
+    double fc = c->p->use_flattening ? w->flat_coeff[d * (size_t)(c->nxt * c->nyt * c->nzt) + cc] : 0.;
+    ppm(c, d + 1, dt, del[d], (const double (*)[NSLOT])V5, fc, trans_only[d],
+        &w->lambda[(cc * 3 + d) * 5],
+        (double (*)[5]) & w->leig[(cc * 3 + d) * 25], (double (*)[5]) & w->reig[(cc * 3 + d) * 25],
+        Wp[d], Wn[d], &w->sig[(cc * 3 + d) * 8]);
+  }
+  const double *sx = &w->sig[(cc * 3 + 0) * 8], *sy = &w->sig[(cc * 3 + 1) * 8], *sz = &w->sig[(cc * 3 + 2) * 8];
+  /* (II) transverse contributions, :918-951 (HY_DENS:HY_END_VARS) */
+  for (int n = 0; n < 8; ++n) {
+    Wn[0][n] = Wn[0][n] - hdty * sy[n];
+    Wp[0][n] = Wp[0][n] - hdty * sy[n];
+    Wn[1][n] = Wn[1][n] - hdtx * sx[n];
+    Wp[1][n] = Wp[1][n] - hdtx * sx[n];
+  }
+  if (nd == 3) {
+    for (int n = 0; n < 8; ++n) {
+      Wn[0][n] = Wn[0][n] - hdtz * sz[n];
+      Wp[0][n] = Wp[0][n] - hdtz * sz[n];
+      Wn[1][n] = Wn[1][n] - hdtz * sz[n];
+      Wp[1][n] = Wp[1][n] - hdtz * sz[n];
+      Wn[2][n] = Wn[2][n] - hdtx * sx[n] - hdty * sy[n];
+      Wp[2][n] = Wp[2][n] - hdtx * sx[n] - hdty * sy[n];
+    }
+  }
+  /* (IV) last negativity check, :1120-1154 */
+  const double *u = &U[cc * NUNK];
+  for (int d = 0; d < nd; ++d) {
+    if (Wn[d][HD] < 0. || Wp[d][HD] < 0. || Wn[d][HP] < 0. || Wp[d][HP] < 0.) {
+      double V[NSLOT];
+      prim_of(u, V);
+      for (int n = 0; n < 8; ++n) { Wn[d][n] = V[n]; Wp[d][n] = V[n]; }
+    }
+  }
+}
+
+/* ===================================================================== */
+/* hy_getRiemannState.F90:356-1475 (pure hydro, Cartesian, no gravity)    */
+/* ===================================================================== */
+static void get_riemann_state(ctx_t *c, const double *U, work_t *w, double dt, const double del[3]) {
+  const int nd = c->ndim, ng = NGUARD;
+  const size_t nc = (size_t)c->nxt * c->nyt * c->nzt;
+  int lo[3] = {ng, c->k2 ? ng : 0, c->k3 ? ng : 0};
+  int hi[3] = {ng + c->nxb - 1, c->k2 ? ng + c->nyb - 1 : 0, c->k3 ? ng + c->nzb - 1 : 0};
+  int kk2 = c->k2, kk3 = c->k3;
+
+  /* (3) flattening, :356-454 */
+  if (c->p->use_flattening) {
+    memset(w->flat_tilde, 0, 3 * nc * sizeof(double));
+    memset(w->flat_coeff, 0, 3 * nc * sizeof(double));
+    for (int k = lo[2] - 2 * kk3; k <= hi[2] + 2 * kk3; ++k)
+      for (int j = lo[1] - 2 * kk2; j <= hi[1] + 2 * kk2; ++j)
+        for (int i = lo[0] - 2; i <= hi[0] + 2; ++i)
+          for (int d = 0; d < nd; ++d) {
+            int di = d == 0, dj = d == 1, dk = d == 2;
+            const double *um1 = &U[cidx(c, i - di, j - dj, k - dk) * NUNK];
+            const double *up1 = &U[cidx(c, i + di, j + dj, k + dk) * NUNK];
+            const double *um2 = &U[cidx(c, i - 2 * di, j - 2 * dj, k - 2 * dk) * NUNK];
+            const double *up2 = &U[cidx(c, i + 2 * di, j + 2 * dj, k + 2 * dk) * NUNK];
+            double dp1 = (up1[PRES_V] - um1[PRES_V]);
+            double dp2 = (up2[PRES_V] - um2[PRES_V]);
+            double dv1 = up1[VELX_V + d] - um1[VELX_V + d];
+            double presL = um1[PRES_V], presR = up1[PRES_V];
+            double Sp = (fabs(dp2) > 1.e-15) ? dp1 / dp2 - 0.75 : 0.;
+            double ft = fmax2(0.0, fmin2(1.0, 10.0 * Sp));
+            if ((fabs(dp1) / fmin2(presL, presR) < 1. / 3.) || dv1 > 0.) ft = 0.;
+            w->flat_tilde[d * nc + cidx(c, i, j, k)] = ft;
+          }
+    for (int k = lo[2] - kk3; k <= hi[2] + kk3; ++k)
+      for (int j = lo[1] - kk2; j <= hi[1] + kk2; ++j)
+        for (int i = lo[0] - 1; i <= hi[0] + 1; ++i)
+          for (int d = 0; d < nd; ++d) {
+            int di = d == 0, dj = d == 1, dk = d == 2;
+            size_t c0 = cidx(c, i, j, k);
+            double dp1 = U[cidx(c, i + di, j + dj, k + dk) * NUNK + PRES_V] - U[cidx(c, i - di, j - dj, k - dk) * NUNK + PRES_V];
+            double t0 = w->flat_tilde[d * nc + c0];
+            double fc;
+            if (dp1 < 0.0) fc = fmax2(t0, w->flat_tilde[d * nc + cidx(c, i + di, j + dj, k + dk)]);
+            else if (dp1 == 0.) fc = t0;
+            else fc = fmax2(t0, w->flat_tilde[d * nc + cidx(c, i - di, j - dj, k - dk)]);
+            w->flat_coeff[d * nc + c0] = fc;
+          }
+  }
+
+  /* (4) per-cell reconstruction over [lo-1, hi+1], :471-901 */
+  for (int k = lo[2] - kk3; k <= hi[2] + kk3; ++k)
+    for (int j = lo[1] - kk2; j <= hi[1] + kk2; ++j)
+      for (int i = lo[0] - 1; i <= hi[0] + 1; ++i) {
+        int tx = 0, ty = 0, tz = 0;                              /* :553-591 */
+        if (i > hi[0] + 1 || i < lo[0] - 1) tx = 1;
+        if (i > hi[0] || i < lo[0]) { ty = 1; tz = 1; }
+        if (nd > 1) {
+          if (j > hi[1] + 1 || j < lo[1] - 1) ty = 1;
+          if (j > hi[1] || j < lo[1]) { tx = 1; tz = 1; }
+          if (nd > 2) {
+            if (k > hi[2] + 1 || k < lo[2] - 1) tz = 1;
+            if (k > hi[2] || k < lo[2]) { tx = 1; ty = 1; }
+          }
+        }
+        int tonly[3] = {tx, ty, tz};
+        double Wp[3][NSLOT], Wn[3][NSLOT];
+        data_reconst_one_step(c, U, w, i, j, k, dt, del, tonly, Wp, Wn);
+        size_t cc = cidx(c, i, j, k);
+        for (int d = 0; d < nd; ++d) {                           /* :843-880 */
+          if (tonly[d]) continue;
+          double *f = &w->face[d][cc * 16];
+          for (int n = 0; n < 8; ++n) { f[n] = Wp[d][n]; f[8 + n] = Wn[d][n]; }
+        }
+      }
+
+  /* (5) 3D full CTU cross terms, :956-1313 */
+  if (nd == 3 && c->p->use_3d_full_ctu) {
+    double dt2dxdy6 = dt * dt / (6. * del[0] * del[1]);
+    double dt2dydz6 = dt * dt / (6. * del[1] * del[2]);
+    double dt2dzdx6 = dt * dt / (6. * del[2] * del[0]);
+    for (int k = lo[2] - 1; k <= hi[2] + 1; ++k)
+      for (int j = lo[1] - 1; j <= hi[1] + 1; ++j)
+        for (int i = lo[0] - 1; i <= hi[0] + 1; ++i) {
+          size_t cc = cidx(c, i, j, k);
+          double Vc[NSLOT];
+          prim_of(&U[cc * NUNK], Vc);
+          for (int d = 0; d < 3; ++d) {
+            /* d-states need the d index in [lo-1,hi+1] and the others interior */
+            int ok = 1;
+            int idx[3] = {i, j, k};
+            for (int e = 0; e < 3; ++e) {
+              if (e == d) continue;
+              if (idx[e] < lo[e] || idx[e] > hi[e]) ok = 0;
+            }
+            if (!ok) continue;
+            /* X: (YZ: sig_z along y, eig_y) + (ZY: sig_y along z, eig_z)
+             * Y: (ZX: sig_x along z, eig_z) + (XZ: sig_z along x, eig_x)
+             * Z: (XY: sig_y along x, eig_x) + (YX: sig_x along y, eig_y) */
+            int a1, s1, a2, s2; double fac;
+            if (d == 0)      { a1 = 1; s1 = 2; a2 = 2; s2 = 1; fac = dt2dydz6; }
+            else if (d == 1) { a1 = 2; s1 = 0; a2 = 0; s2 = 2; fac = dt2dzdx6; }
+            else             { a1 = 0; s1 = 1; a2 = 1; s2 = 0; fac = dt2dxdy6; }
+            double T1[8], T2[8];
+            for (int t = 0; t < 2; ++t) {
+              int ax = t ? a2 : a1, sd = t ? s2 : s1;
+              int oi = ax == 0, oj = ax == 1, ok2 = ax == 2;
+              const double *sm = &w->sig[(cidx(c, i - oi, j - oj, k - ok2) * 3 + sd) * 8];
+              const double *s0 = &w->sig[(cc * 3 + sd) * 8];
+              const double *sp = &w->sig[(cidx(c, i + oi, j + oj, k + ok2) * 3 + sd) * 8];
+              upwind_transverse_flux(c, sm, s0, sp, &w->lambda[(cc * 3 + ax) * 5],
+                                     (double (*)[5]) & w->leig[(cc * 3 + ax) * 25],
+                                     (double (*)[5]) & w->reig[(cc * 3 + ax) * 25], t ? T2 : T1);
+            }
+            double *f = &w->face[d][cc * 16];
+            for (int n = 0; n < 8; ++n) {
+              f[n] = f[n] + (T1[n] + T2[n]) * fac;
+              f[8 + n] = f[8 + n] + (T1[n] + T2[n]) * fac;
+            }
+            if (f[HD] <= 0. || f[8 + HD] <= 0. || f[HP] <= 0. || f[8 + HP] <= 0.) {
+              for (int n = 0; n < 8; ++n) { f[n] = Vc[n]; f[8 + n] = Vc[n]; }
+            }
+          }
+        }
+  }
+}
+
+/* ===================================================================== */
+/* hy_prim2con.F90:37-54, hy_prim2flx.F90:49-123, hy_HLLC.F90:94-311      */
+/* ===================================================================== */
+static void prim2con(const double *V, double CU[5]) {
+  double u2 = V[HVX] * V[HVX] + V[HVY] * V[HVY] + V[HVZ] * V[HVZ];
+  CU[0] = V[HD];
+  CU[1] = V[HD] * V[HVX]; CU[2] = V[HD] * V[HVY]; CU[3] = V[HD] * V[HVZ];
+  CU[4] = 0.5 * V[HD] * u2 + V[HP] / (V[HGE] - 1.) + 0.5 * 0.;
+}
+static void prim2flx(const ctx_t *c, int dir, const double *V, double F[6]) {
+  double fP = c->p->f_pres_in_mom_flux;
+  double u2 = V[HVX] * V[HVX] + V[HVY] * V[HVY] + V[HVZ] * V[HVZ];
+  double E = 0.5 * V[HD] * u2 + V[HP] / (V[HGE] - 1.);
+  F[5] = V[HP];
+  double un = V[HVX + dir - 1];
+  F[0] = V[HD] * un;
+  F[1] = F[0] * V[HVX];
+  F[2] = F[0] * V[HVY];
+  F[3] = F[0] * V[HVZ];
+  F[dir] = F[dir] + fP * V[HP];
+  F[4] = (E + V[HP]) * un;
+}
+static void hllc(ctx_t *c, int dir, const double *Vm, const double *Vp, double Fstar[6]) {
+  const double fP = c->p->f_pres_in_mom_flux, tiny = c->p->tiny;
+  double velNL = Vm[HVX + dir - 1], velNR = Vp[HVX + dir - 1];
+  double aL2 = Vm[HGC] * Vm[HP] / Vm[HD];
+  double aR2 = Vp[HGC] * Vp[HP] / Vp[HD];
+  if ((Vm[HD] < tiny && Vm[HD] > 0.) || (Vp[HD] < tiny && Vp[HD] > 0.) ||
+      (Vm[HP] < tiny && Vm[HP] > 0.) || (Vp[HP] < tiny && Vp[HP] > 0.)) {
+    for (int n = 0; n < 6; ++n) Fstar[n] = 0.;                 /* :118-124 */
+    return;
+  }
+  if (aL2 < 0. || aR2 < 0.) {                                  /* :125-127 */
+    c->status |= FLASH_HY_ERR_NEG_SOUNDSPEED;
+    for (int n = 0; n < 6; ++n) Fstar[n] = 0.;
+    return;
+  }
+  double cfL = sqrt(aL2), cfR = sqrt(aR2);
+  double SL = fmin2(velNL - cfL, velNR - cfR);                 /* :141-142 */
+  double SR = fmax2(velNL + cfL, velNR + cfR);
+  double totalPresL = Vm[HP], totalPresR = Vp[HP];
+  double UL[5], UR[5], FL[6], FR[6], UCL[5], UCR[5];
+  prim2con(Vm, UL); prim2con(Vp, UR);
+  prim2flx(c, dir, Vm, FL); prim2flx(c, dir, Vp, FR);
+  /* Uhll (:154-175) is only used by the MHD variant; not needed here */
+  double qStar = (Vp[HD] * velNR * (SR - velNR) - Vm[HD] * velNL * (SL - velNL)
+                  + totalPresL - totalPresR - 0. * 0. + 0. * 0.);      /* :189-193 */
+  qStar = qStar / (Vp[HD] * (SR - velNR) - Vm[HD] * (SL - velNL));
+  double numerL = SL - velNL, denomL = SL - qStar;
+  double numerR = SR - velNR, denomR = SR - qStar;
+  double pStar = Vm[HD] * numerL * (qStar - velNL) + totalPresL;        /* :203 */
+  double dStarL = UL[0] * numerL / denomL;
+  double dStarR = UR[0] * numerR / denomR;
+  UCL[0] = dStarL;
+  UCL[4] = UL[4] * numerL / denomL + ((pStar * qStar - totalPresL * velNL)) / denomL;
+  UCR[0] = dStarR;
+  UCR[4] = UR[4] * numerR / denomR + ((pStar * qStar - totalPresR * velNR)) / denomR;
+  for (int m = 1; m <= 3; ++m) {
+    if (m == dir) { UCL[m] = dStarL * qStar; UCR[m] = dStarR * qStar; }
+    else { UCL[m] = UL[m] * numerL / denomL; UCR[m] = UR[m] * numerR / denomR; }
+  }
+  if (SL >= 0.) {                                                      /* :295-311 */
+    for (int n = 0; n < 6; ++n) Fstar[n] = FL[n];
+  } else if ((SL < 0.) && (qStar >= 0.)) {
+    for (int n = 0; n < 5; ++n) Fstar[n] = FL[n] + SL * (UCL[n] - UL[n]);
+    Fstar[5] = FL[5];
+  } else if ((qStar < 0.) && (SR >= 0.)) {
+    for (int n = 0; n < 5; ++n) Fstar[n] = FR[n] + SR * (UCR[n] - UR[n]);
+    Fstar[5] = FR[5];
+  } else {
+    for (int n = 0; n < 6; ++n) Fstar[n] = FR[n];
+  }
+  (void)fP;
+}
+
+/* Exact Riemann solver face flux (no FLASH counterpart); defined in
+ * oracle_exact.c.  Returns 0 on convergence. */
+int orc_exact_flux(int dir, const double *VL, const double *VR, double gamma, double tol,
+                   int max_iter, double F[6], int *iters);
+
+/* ===================================================================== */
+/* hy_getFaceFlux.F90:283-570 (x), y and z analogues                      */
+/* ===================================================================== */
+static void get_face_flux(ctx_t *c, work_t *w) {
+  const int nd = c->ndim, ng = NGUARD;
+  int lo[3] = {ng, c->k2 ? ng : 0, c->k3 ? ng : 0};
+  int hi[3] = {ng + c->nxb - 1, c->k2 ? ng + c->nyb - 1 : 0, c->k3 ? ng + c->nzb - 1 : 0};
+  for (int d = 0; d < nd; ++d) {
+    int di = d == 0, dj = d == 1, dk = d == 2;
+    for (int k = lo[2]; k <= hi[2] + dk; ++k)
+      for (int j = lo[1]; j <= hi[1] + dj; ++j)
+        for (int i = lo[0]; i <= hi[0] + di; ++i) {
+          size_t cc = cidx(c, i, j, k), cm = cidx(c, i - di, j - dj, k - dk);
+          const double *VL = &w->face[d][cm * 16];          /* P-state of i-1 */
+          const double *VR = &w->face[d][cc * 16 + 8];      /* N-state of i   */
+          double *F = &w->flux[d][cc * NFLX];
+          double Fs[6];
+          if (c->p->riemann_solver == FLASH_HY_RS_EXACT) {
+            int it;
+            if (orc_exact_flux(d + 1, VL, VR, c->p->gamma, 1e-12, 50, Fs, &it) != 0)
+              c->status |= FLASH_HY_ERR_NEWTON_NOCONV;
+          } else {
+            hllc(c, d + 1, VL, VR, Fs);
+          }
+          for (int n = 0; n < 6; ++n) F[n] = Fs[n];
+          if (c->p->use_aux_eint) {                          /* :433-442 */
+            if (F[FDENS] > 0.) { F[FVOLU] = F[FDENS] / VL[HD]; F[FEINT] = F[FDENS] * VL[HEI]; }
+            else               { F[FVOLU] = F[FDENS] / VR[HD]; F[FEINT] = F[FDENS] * VR[HEI]; }
+          } else { F[FVOLU] = 0.; F[FEINT] = 0.; }
+        }
+    /* n+1/2 pressure average into scrch_Ptr, :551-557 and y/z analogues */
+    if (c->p->use_aux_eint) {
+      for (int k = lo[2]; k <= hi[2]; ++k)
+        for (int j = lo[1]; j <= hi[1]; ++j)
+          for (int i = lo[0]; i <= hi[0]; ++i) {
+            size_t cc = cidx(c, i, j, k);
+            const double *f = &w->face[d][cc * 16];
+            double *s = &w->scrch[cc * 2];
+            if (d == 0) { s[1] = 0.5 * (f[8 + HP] + f[HP]); s[0] = s[1]; }
+            else if (d == 1) s[0] = s[0] * 0.5 + (f[8 + HP] + f[HP]) * 0.25;
+            else s[0] = (s[0] * 4.0 + (f[8 + HP] + f[HP])) / 6.0;
+          }
+    }
+  }
+}
+
+/* ===================================================================== */
+/* hy_unsplitUpdate.F90:442-925, updateConservedVariable :1187-1242,      */
+/* updateInternalEnergy :1279-1298 (Cartesian, no gravity)               */
+/* ===================================================================== */
+static void unsplit_update(ctx_t *c, double *U, work_t *w, double dt, const double del[3]) {
+  const flash_hy_params *p = c->p;
+  const int nd = c->ndim, ng = NGUARD;
+  int lo[3] = {ng, c->k2 ? ng : 0, c->k3 ? ng : 0};
+  int hi[3] = {ng + c->nxb - 1, c->k2 ? ng + c->nyb - 1 : 0, c->k3 ? ng + c->nzb - 1 : 0};
+  double dx = del[0], dy = nd > 1 ? del[1] : 1., dz = nd > 2 ? del[2] : 1.;
+  double fP = p->f_pres_in_mom_flux;
+  for (int k = lo[2]; k <= hi[2]; ++k)
+    for (int j = lo[1]; j <= hi[1]; ++j)
+      for (int i = lo[0]; i <= hi[0]; ++i) {
+        size_t cc = cidx(c, i, j, k);
+        double FL[8], FR[8], GL[8], GR[8], HL[8], HR[8];
+        for (int n = 0; n < 8; ++n) {
+          FL[n] = w->flux[0][cc * 8 + n];
+          FR[n] = w->flux[0][cidx(c, i + 1, j, k) * 8 + n];
+          GL[n] = nd > 1 ? w->flux[1][cc * 8 + n] * 1. : 0.;
+          GR[n] = nd > 1 ? w->flux[1][cidx(c, i, j + 1, k) * 8 + n] * 1. : 0.;
+          HL[n] = nd > 2 ? w->flux[2][cc * 8 + n] * 1. : 0.;
+          HR[n] = nd > 2 ? w->flux[2][cidx(c, i, j, k + 1) * 8 + n] * 1. : 0.;
+        }
+        double Sphys[5] = {0., 0., 0., 0., 0.};
+        Sphys[1] = (FL[FPRES] - FR[FPRES]) * (1.0 - fP) / dx;
+        if (nd >= 2) Sphys[2] = (GL[FPRES] - GR[FPRES]) * (1.0 - fP) / dy;
+        if (nd == 3) Sphys[3] = (HL[FPRES] - HR[FPRES]) * (1.0 - fP) / dz;
+        double *u = &U[cc * NUNK];
+        double U0[5];
+        U0[0] = u[DENS_V];
+        double IntEner = 0.;
+        if (p->use_aux_eint) {
+          IntEner = u[DENS_V] * u[EINT_V];
+          double pres = w->scrch[cc * 2];
+          IntEner = IntEner + dt / dx * (FL[FEINT] - FR[FEINT] + pres * (FL[FVOLU] - FR[FVOLU]));
+          if (nd > 1) IntEner = IntEner + dt / dy * (GL[FEINT] - GR[FEINT] + pres * (GL[FVOLU] - GR[FVOLU]));
+          if (nd > 2) IntEner = IntEner + dt / dz * (HL[FEINT] - HR[FEINT] + pres * (HL[FVOLU] - HR[FVOLU]));
+          IntEner = IntEner + dt * 0.;
+        }
+        U0[1] = u[VELX_V] * u[DENS_V];
+        U0[2] = u[VELY_V] * u[DENS_V];
+        U0[3] = u[VELZ_V] * u[DENS_V];
+        U0[4] = u[DENS_V] * u[ENER_V];
+        for (int n = 0; n < 5; ++n) U0[n] = U0[n] - dt / dx * (FR[n] - FL[n]);
+        if (nd > 1) for (int n = 0; n < 5; ++n) U0[n] = U0[n] - dt / dy * (GR[n] - GL[n]);
+        if (nd > 2) for (int n = 0; n < 5; ++n) U0[n] = U0[n] - dt / dz * (HR[n] - HL[n]);
+        for (int n = 0; n < 5; ++n) U0[n] = U0[n] + dt * (0. + Sphys[n]);
+        u[DENS_V] = fmax2(U0[0], p->smlrho);
+        u[ENER_V] = U0[4];
+        u[VELX_V] = U0[1] / u[DENS_V];
+        u[VELY_V] = U0[2] / u[DENS_V];
+        u[VELZ_V] = U0[3] / u[DENS_V];
+        u[ENER_V] = U0[4] / u[DENS_V];
+        if (p->use_aux_eint) {
+          IntEner = IntEner / u[DENS_V];
+          u[EINT_V] = IntEner;
+        }
+      }
+}
+
+/* hy_energyFix.F90:188-253 (pure hydro) */
+static void energy_fix(ctx_t *c, double *U) {
+  const flash_hy_params *p = c->p;
+  const int ng = NGUARD;
+  for (int k = c->k3 ? ng : 0; k <= (c->k3 ? ng + c->nzb - 1 : 0); ++k)
+    for (int j = c->k2 ? ng : 0; j <= (c->k2 ? ng + c->nyb - 1 : 0); ++j)
+      for (int i = ng; i <= ng + c->nxb - 1; ++i) {
+        double *u = &U[cidx(c, i, j, k) * NUNK];
+        double ekin = 0.5 * (u[VELX_V] * u[VELX_V] + u[VELY_V] * u[VELY_V] + u[VELZ_V] * u[VELZ_V]);
+        double eint = u[ENER_V] - ekin - 0.0;
+        double IntEner = u[EINT_V];
+        double newEint;
+        if (!p->use_aux_eint || eint > p->eint_switch * (ekin + 0.0)) newEint = fmax2(p->smalle, eint);
+        else newEint = fmax2(p->smalle, IntEner);
+        u[ENER_V] = newEint + ekin;
+        u[EINT_V] = newEint;
+      }
+}
+
+/* Eos_wrapped(MODE_DENS_EI) on one cell: Eos_getData (Eos_getData.F90:80-110),
+ * eos_idealGamma MODE_DENS_EI (eos_idealGamma.F90:323-335), Eos_putData
+ * (Eos_putData.F90:95-106). */
+static void eos_dens_ei_cell(const ctx_t *c, double *u) {
+  const flash_hy_params *p = c->p;
+  double ekin = 0.5 * (u[VELX_V] * u[VELX_V] + u[VELY_V] * u[VELY_V] + u[VELZ_V] * u[VELZ_V]);
+  double eint = u[EINT_V];
+  if (u[ENER_V] - ekin > fmax2(p->smalle, p->eint_switch * ekin)) eint = u[ENER_V] - ekin;
+  double dens = u[DENS_V];
+  double pres = dens * eint * c->gam1inv;
+  double temp = eint * c->ggprodinv * p->single_species_a;
+  u[PRES_V] = pres;
+  u[TEMP_V] = temp;
+  u[GAMC_V] = p->gamma;
+  u[EINT_V] = eint;
+  u[ENER_V] = eint + ekin;
+  u[GAME_V] = pres / (eint * dens) + 1;
+}
+
+/* ===================================================================== */
+/* Guard-cell fill on a uniform block grid (Grid_fillGuardCells with      */
+/* doEos, paramesh4/Grid_fillGuardCells.F90:227-569; UG gr_shiftData)     */
+/* ===================================================================== */
+static int map_axis(int g, int n, int bclo, int bchi, int *flip) {
+  if (g < 0) {
+    if (bclo == FLASH_HY_BC_PERIODIC) return ((g % n) + n) % n;
+    if (bclo == FLASH_HY_BC_REFLECTING) { *flip = 1; return -1 - g; }
+    return 0;                                     /* OUTFLOW: zero gradient */
+  }
+  if (g >= n) {
+    if (bchi == FLASH_HY_BC_PERIODIC) return g % n;
+    if (bchi == FLASH_HY_BC_REFLECTING) { *flip = 1; return 2 * n - 1 - g; }
+    return n - 1;
+  }
+  return g;
+}
+
+static void ctx_init(ctx_t *c, const flash_hy_params *p, const flash_hy_grid_desc *g) {
+  memset(c, 0, sizeof *c);
+  c->p = p;
+  c->ndim = g->ndim;
+  c->nxb = g->nxb; c->nyb = g->ndim > 1 ? g->nyb : 1; c->nzb = g->ndim > 2 ? g->nzb : 1;
+  c->k2 = g->ndim > 1; c->k3 = g->ndim > 2;
+  c->nxt = c->nxb + 2 * NGUARD;
+  c->nyt = c->k2 ? c->nyb + 2 * NGUARD : 1;
+  c->nzt = c->k3 ? c->nzb + 2 * NGUARD : 1;
+  double gammam1 = 1.0 / (p->gamma - 1.0);          /* eos_initGamma.F90:32 */
+  c->gam1inv = 1. / gammam1;
+  double ggprod = gammam1 * p->gas_constant;        /* eos_idealGamma.F90:262 */
+  c->ggprodinv = 1. / ggprod;
+}
+
+static int check_grid(const flash_hy_grid_desc *g) {
+  if (g->ndim < 2 || g->ndim > 3) return FLASH_HY_ERR_UNSUPPORTED;
+  if (g->nguard != NGUARD) return FLASH_HY_ERR_BAD_ARG;
+  if (g->max_level > 1) return FLASH_HY_ERR_UNSUPPORTED;
+  return 0;
+}
+
+/* Fill every guard cell of every block from the block that owns the cell
+ * (same refinement level) or from the boundary condition, then apply the
+ * EOS to the guard cells.  Blocks are located through block_coords. */
+int orc_fill_guardcells(const flash_hy_params *p, const flash_hy_grid_desc *g, double *unk) {
+  int st = check_grid(g);
+  if (st) return st;
+  ctx_t c; ctx_init(&c, p, g);
+  int nbx = g->nblk_l1[0], nby = g->ndim > 1 ? g->nblk_l1[1] : 1, nbz = g->ndim > 2 ? g->nblk_l1[2] : 1;
+  int *owner = malloc(sizeof(int) * nbx * nby * nbz);
+  for (int b = 0; b < g->nblocks; ++b) {
+    const int *bc = &g->block_coords[3 * b];
+    owner[((g->ndim > 2 ? bc[2] : 0) * nby + (g->ndim > 1 ? bc[1] : 0)) * nbx + bc[0]] = b;
+  }
+  size_t bsz = (size_t)c.nxt * c.nyt * c.nzt * NUNK;
+  int NX = nbx * c.nxb, NY = nby * c.nyb, NZ = nbz * c.nzb;
+  #pragma omp parallel for schedule(dynamic)
+  for (int b = 0; b < g->nblocks; ++b) {
+    const int *bc = &g->block_coords[3 * b];
+    for (int k = 0; k < c.nzt; ++k)
+      for (int j = 0; j < c.nyt; ++j)
+        for (int i = 0; i < c.nxt; ++i) {
+          int li = i - NGUARD, lj = c.k2 ? j - NGUARD : 0, lk = c.k3 ? k - NGUARD : 0;
+          if (li >= 0 && li < c.nxb && lj >= 0 && lj < c.nyb && lk >= 0 && lk < c.nzb) continue;
+          int fx = 0, fy = 0, fz = 0;
+          int gx = map_axis(bc[0] * c.nxb + li, NX, g->bc[0], g->bc[1], &fx);
+          int gy = c.k2 ? map_axis(bc[1] * c.nyb + lj, NY, g->bc[2], g->bc[3], &fy) : 0;
+          int gz = c.k3 ? map_axis(bc[2] * c.nzb + lk, NZ, g->bc[4], g->bc[5], &fz) : 0;
+          int sb = owner[((gz / c.nzb) * nby + gy / c.nyb) * nbx + gx / c.nxb];
+          int si = gx % c.nxb + NGUARD, sj = c.k2 ? gy % c.nyb + NGUARD : 0, sk = c.k3 ? gz % c.nzb + NGUARD : 0;
+          const double *src = &unk[sb * bsz + cidx(&c, si, sj, sk) * NUNK];
+          double *dst = &unk[b * bsz + cidx(&c, i, j, k) * NUNK];
+          memcpy(dst, src, sizeof(double) * NUNK);
+          if (fx) dst[VELX_V] = -dst[VELX_V];
+          if (fy) dst[VELY_V] = -dst[VELY_V];
+          if (fz) dst[VELZ_V] = -dst[VELZ_V];
+        }
+  }
+  /* EOS on the guard cells (Eos_guardCells, doEos=.true., Hydro.F90:121-123) */
+  #pragma omp parallel for schedule(dynamic)
+  for (int b = 0; b < g->nblocks; ++b)
+    for (int k = 0; k < c.nzt; ++k)
+      for (int j = 0; j < c.nyt; ++j)
+        for (int i = 0; i < c.nxt; ++i) {
+          int li = i - NGUARD, lj = c.k2 ? j - NGUARD : 0, lk = c.k3 ? k - NGUARD : 0;
+          if (li >= 0 && li < c.nxb && lj >= 0 && lj < c.nyb && lk >= 0 && lk < c.nzb) continue;
+          eos_dens_ei_cell(&c, &unk[b * bsz + cidx(&c, i, j, k) * NUNK]);
+        }
+  free(owner);
+  return 0;
+}
+
+/* Eos_wrapped(MODE_DENS_EI) on every block interior. */
+int orc_eos_interior(const flash_hy_params *p, const flash_hy_grid_desc *g, double *unk) {
+  int st = check_grid(g);
+  if (st) return st;
+  ctx_t c; ctx_init(&c, p, g);
+  size_t bsz = (size_t)c.nxt * c.nyt * c.nzt * NUNK;
+  #pragma omp parallel for schedule(static)
+  for (int b = 0; b < g->nblocks; ++b)
+    for (int k = c.k3 ? NGUARD : 0; k < (c.k3 ? NGUARD + c.nzb : 1); ++k)
+      for (int j = c.k2 ? NGUARD : 0; j < (c.k2 ? NGUARD + c.nyb : 1); ++j)
+        for (int i = NGUARD; i < NGUARD + c.nxb; ++i)
+          eos_dens_ei_cell(&c, &unk[b * bsz + cidx(&c, i, j, k) * NUNK]);
+  return 0;
+}
+
+/* hy_computeFluxes.F90:156-375 with Uout => Uin (UPDATE_ALL) for one block:
+ * Riemann states, face fluxes, unsplit update, energy fix, EOS. */
+static int compute_fluxes_block(ctx_t *c, double *U, double dt, const double del[3]) {
+  work_t w;
+  work_alloc(c, &w);
+  get_riemann_state(c, U, &w, dt, del);
+  get_face_flux(c, &w);
+  unsplit_update(c, U, &w, dt, del);
+  energy_fix(c, U);
+  for (int k = c->k3 ? NGUARD : 0; k < (c->k3 ? NGUARD + c->nzb : 1); ++k)
+    for (int j = c->k2 ? NGUARD : 0; j < (c->k2 ? NGUARD + c->nyb : 1); ++j)
+      for (int i = NGUARD; i < NGUARD + c->nxb; ++i) {
+        double *u = &U[cidx(c, i, j, k) * NUNK];
+        eos_dens_ei_cell(c, u);
+        for (int n = 0; n < NUNK; ++n) if (!isfinite(u[n]) && n != SHOK_V) c->status |= FLASH_HY_ERR_NAN;
+      }
+  work_free(&w);
+  return c->status;
+}
+
+static void block_deltas(const flash_hy_grid_desc *g, double del[3]) {
+  int nb[3] = {g->nxb, g->nyb, g->nzb};
+  for (int d = 0; d < 3; ++d) {
+    if (d < g->ndim) del[d] = (g->domain_hi[d] - g->domain_lo[d]) / (double)(g->nblk_l1[d] * nb[d]);
+    else del[d] = 1.;
+  }
+}
+
+/* Hydro(simTime, dt, dtOld, sweepOrder) over a list of blocks (all blocks
+ * when block_list is NULL): unsplit/Hydro.F90:121-229 on a single level. */
+int orc_hydro(const flash_hy_params *p, const flash_hy_grid_desc *g, double *unk,
+              double sim_time, double dt, double dt_old, int nlist, const int *block_list) {
+  (void)sim_time; (void)dt_old;
+  int st = check_grid(g);
+  if (st) return st;
+  if (p->order != 3) return FLASH_HY_ERR_UNSUPPORTED;
+  st = orc_fill_guardcells(p, g, unk);
+  if (st) return st;
+  ctx_t c0; ctx_init(&c0, p, g);
+  double del[3];
+  block_deltas(g, del);
+  size_t bsz = (size_t)c0.nxt * c0.nyt * c0.nzt * NUNK;
+  int n = block_list ? nlist : g->nblocks;
+  int status = 0;
+  #pragma omp parallel for schedule(dynamic) reduction(| : status)
+  for (int ib = 0; ib < n; ++ib) {
+    int b = block_list ? block_list[ib] : ib;
+    ctx_t c; ctx_init(&c, p, g);
+    status |= compute_fluxes_block(&c, &unk[b * bsz], dt, del);
+  }
+  return status;
+}
+
+/* Hydro_computeDt.F90:186-290 per block, then the MINLOC reduction of
+ * Driver_computeDt.F90:376-377 across blocks (first block wins ties).
+ * minloc = (i, j, k, level, block) with 1-based guard-inclusive indices. */
+int orc_compute_dt(const flash_hy_params *p, const flash_hy_grid_desc *g, const double *unk,
+                   double *dt_out, int minloc[5]) {
+  int st = check_grid(g);
+  if (st) return st;
+  ctx_t c; ctx_init(&c, p, g);
+  double del[3];
+  block_deltas(g, del);
+  size_t bsz = (size_t)c.nxt * c.nyt * c.nzt * NUNK;
+  double dt_check = DBL_MAX;
+  int best[5] = {0, 0, 0, 0, -1};
+  double delxinv = 1.0 / del[0], delyinv = 1.0 / del[1], delzinv = 1.0 / del[2];
+  for (int b = 0; b < g->nblocks; ++b) {
+    double dt_temp = 0.;
+    int temploc[5] = {0, 0, 0, 0, 0};
+    double tempCfl = p->cfl, localCfl = p->cfl;
+    for (int k = c.k3 ? NGUARD : 0; k < (c.k3 ? NGUARD + c.nzb : 1); ++k)
+      for (int j = c.k2 ? NGUARD : 0; j < (c.k2 ? NGUARD + c.nyb : 1); ++j)
+        for (int i = NGUARD; i < NGUARD + c.nxb; ++i) {
+          const double *u = &unk[b * bsz + cidx(&c, i, j, k) * NUNK];
+          double sndspd2 = u[GAMC_V] * u[PRES_V] / u[DENS_V];
+          double dt_ltemp = (fabs(u[VELX_V] - 0.) + sqrt(sndspd2)) * delxinv;
+          if (g->ndim > 1) dt_ltemp = fmax2(dt_ltemp, (fabs(u[VELY_V] - 0.) + sqrt(sndspd2)) * delyinv);
+          if (g->ndim > 2) dt_ltemp = fmax2(dt_ltemp, (fabs(u[VELZ_V] - 0.) + sqrt(sndspd2)) * delzinv);
+          if (dt_ltemp * tempCfl > dt_temp * localCfl) {
+            dt_temp = dt_ltemp;
+            tempCfl = localCfl;
+            temploc[0] = i + 1; temploc[1] = j + 1; temploc[2] = k + 1;
+            temploc[3] = g->block_level ? g->block_level[b] : 1;
+            temploc[4] = b;
+          }
+        }
+    if (dt_temp != 0.0) dt_temp = tempCfl / dt_temp;
+    else dt_temp = DBL_MAX;
+    if (dt_temp < dt_check) {
+      dt_check = dt_temp;
+      memcpy(best, temploc, sizeof best);
+    }
+  }
+  *dt_out = dt_check;
+  memcpy(minloc, best, sizeof best);
+  return dt_check <= 0.0 ? FLASH_HY_ERR_NONPOS_DT : 0;
+}
+
+/* Single-interface HLLC flux (for unit tests of the Riemann stage). */
+int orc_hllc(const flash_hy_params *p, int dir, const double *VL, const double *VR, double F[6]) {
+  ctx_t c; memset(&c, 0, sizeof c); c.p = p;
+  hllc(&c, dir, VL, VR, F);
+  return c.status;
+}

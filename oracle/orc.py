@@ -1,0 +1,109 @@
+"""ctypes wrapper of the CPU oracle (test infrastructure only).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use
+this module, always as the checker.  The oracle library is built by
+``oracle/Makefile`` (``make -C oracle``).
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from flash5_b200 import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liborc_hy.so")
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = C.CDLL(LIB)
+        P, G = C.POINTER(abi.Params), C.POINTER(abi.GridDesc)
+        dp, ip = C.POINTER(C.c_double), C.POINTER(C.c_int)
+        L.orc_fill_guardcells.argtypes = [P, G, dp]
+        L.orc_eos_interior.argtypes = [P, G, dp]
+        L.orc_hydro.argtypes = [P, G, dp, C.c_double, C.c_double, C.c_double, C.c_int, ip]
+        L.orc_compute_dt.argtypes = [P, G, dp, dp, ip]
+        L.orc_hllc.argtypes = [P, C.c_int, dp, dp, dp]
+        L.orc_exact_flux.argtypes = [C.c_int, dp, dp, C.c_double, C.c_double, C.c_int, dp, ip]
+        L.orc_star_state.argtypes = [C.c_double] * 8 + [C.c_double, C.c_int, dp, dp, ip]
+        L.orc_two_rarefaction_guess.argtypes = [C.c_double] * 7
+        L.orc_two_rarefaction_guess.restype = C.c_double
+        L.orc_star_batch.argtypes = [C.c_long] + [dp] * 8 + [C.c_double, C.c_int, dp, dp, ip, ip]
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Oracle:
+    """FLASH-like driver over host UNK arrays: eos_init, hydro step, dt."""
+
+    def __init__(self, params, grid):
+        self.p = params
+        self.grid = grid
+        self.g = grid.desc()
+
+    def eos_init(self, unk):
+        st = lib().orc_eos_interior(C.byref(self.p), C.byref(self.g), _dp(unk))
+        assert st == 0, st
+        return unk
+
+    def fill_guardcells(self, unk):
+        return lib().orc_fill_guardcells(C.byref(self.p), C.byref(self.g), _dp(unk))
+
+    def hydro(self, unk, sim_time, dt, dt_old, blocks=None):
+        if blocks is None:
+            return lib().orc_hydro(C.byref(self.p), C.byref(self.g), _dp(unk), sim_time, dt, dt_old, 0, None)
+        bl = np.ascontiguousarray(blocks, dtype=np.int32)
+        return lib().orc_hydro(C.byref(self.p), C.byref(self.g), _dp(unk), sim_time, dt, dt_old, len(bl),
+                               bl.ctypes.data_as(C.POINTER(C.c_int)))
+
+    def compute_dt(self, unk):
+        dt = C.c_double()
+        loc = (C.c_int * 5)()
+        st = lib().orc_compute_dt(C.byref(self.p), C.byref(self.g), _dp(unk), C.byref(dt), loc)
+        return st, dt.value, tuple(loc)
+
+
+def hllc(params, dirn, VL, VR):
+    VL = np.ascontiguousarray(VL, dtype=np.float64)
+    VR = np.ascontiguousarray(VR, dtype=np.float64)
+    F = np.zeros(6)
+    st = lib().orc_hllc(C.byref(params), dirn, _dp(VL), _dp(VR), _dp(F))
+    return st, F
+
+
+def star_state(dl, ul, pl, dr, ur, pr, gamma, p0=0.0, tol=1e-12, max_iter=50):
+    ps, us, it = C.c_double(), C.c_double(), C.c_int()
+    st = lib().orc_star_state(dl, ul, pl, dr, ur, pr, gamma, p0, tol, max_iter, C.byref(ps), C.byref(us),
+                              C.byref(it))
+    return st, ps.value, us.value, it.value
+
+
+def star_batch(dl, ul, pl, dr, ur, pr, gam, p0=None, tol=1e-12, max_iter=50):
+    n = len(dl)
+    arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (dl, ul, pl, dr, ur, pr, gam)]
+    p0a = None if p0 is None else np.ascontiguousarray(p0, dtype=np.float64)
+    ps, us = np.zeros(n), np.zeros(n)
+    it, st = np.zeros(n, np.int32), np.zeros(n, np.int32)
+    lib().orc_star_batch(n, *[_dp(a) for a in arrs], None if p0a is None else _dp(p0a), tol, max_iter,
+                         _dp(ps), _dp(us), it.ctypes.data_as(C.POINTER(C.c_int)),
+                         st.ctypes.data_as(C.POINTER(C.c_int)))
+    return ps, us, it, st
+
+
+def two_rarefaction_guess(dl, ul, pl, dr, ur, pr, gamma):
+    return lib().orc_two_rarefaction_guess(dl, ul, pl, dr, ur, pr, gamma)
