@@ -1,0 +1,368 @@
+"""Benchmark of the unsplit hydro step (zone-updates/s).
+
+Workload: 3D Kelvin-Helmholtz, 256^3 cells as 32^3 blocks of 8^3 interior
+cells (FLASH's 4 guard layers are filled inside the kernels), gamma = 5/3,
+periodic boundaries, PPM + HLLC with characteristic limiting and
+flattening, CFL 0.8, the time step recomputed every step (Hydro_computeDt
+reduction + Driver_computeDt growth limit).  Inputs are synthetic (seeded
+noise, numpy PCG64 seed 12345).
+
+One step = the device pass of the hot path over all blocks (k_sig + one
+fused kernel per direction) plus the CFL reduction read back to the host.
+``value`` is the mixed path (FP32 reconstruction and Riemann solve, FP64
+update) with the state resident in HBM; the plain FP64 path is reported
+beside it, and the mixed path's L1 error against the FP64 path (which
+matches the CPU oracle bit for bit in the tests) is measured on the same
+run.  ``e2e`` is the same metric through the C-ABI with host UNK buffers
+(interior-only FLASH UNK, 11 variables, pinned): upload, step, dt, download
+every step.
+
+``--impl reference`` times the CPU oracle (the C restatement of the
+reference's Fortran; the Fortran itself cannot be built here) on a bounded
+64^3 sample of the same workload with all host threads.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "zone-updates/s on 1 B200: batched mixed+learned vs plain FP64, rel L1<=1e-6"
+UNIT = "zone-updates/s"
+BYTES_PER_ZONE = 80.0          # read + write of 5 FP64 state variables
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        load = [s for s in sm if s > 500] or sm
+        return {"sm_mhz": float(np.median(load)) if load else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def kh_workload(nblk=32, nguard=0):
+    from flash5_b200 import abi, setups
+    from flash5_b200.grid import UniformGrid
+    g = UniformGrid(3, (8, 8, 8), (nblk, nblk, nblk), bc="periodic", nguard=nguard)
+    unk = setups.kelvin_helmholtz(g)
+    return g, unk, abi
+
+
+def run_device(h, steps, warmup, dts=None, sampler=None, dist=None):
+    """Time `steps` hydro steps with the state resident on the device.
+    Returns (ms_per_step, dt list, launches per step)."""
+    import torch
+    from flash5_b200.hydro import next_dt
+    stream = torch.cuda.ExternalStream(h.stream)
+    dt, _ = h.compute_dt()
+    if dist is not None:
+        dt = dist_min(dist, dt)
+    dt_old = dt
+    used = []
+    t = 0.0
+
+    def one(i):
+        nonlocal dt, dt_old, t
+        d = dts[i] if dts is not None else dt
+        h(t + d, d, dt_old)
+        used.append(d)
+        t += d
+        dcfl, _ = h.compute_dt()
+        if dist is not None:
+            dcfl = dist_min(dist, dcfl)
+        dt_old, dt = d, next_dt(dcfl, d)
+
+    for i in range(warmup):
+        one(i)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ctx = sampler if sampler is not None else _null()
+    with ctx:
+        e0.record(stream)
+        for i in range(warmup, warmup + steps):
+            one(i)
+        e1.record(stream)
+        e1.synchronize()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    ms = e0.elapsed_time(e1) / steps
+    return ms, used, h.last_launch_count + 1
+
+
+class _null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        pass
+
+
+def dist_min(dist, x):
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MIN)
+    return float(t.item())
+
+
+def dist_max(dist, x):
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_e2e(h, unk_host, steps, warmup):
+    """upload -> step -> dt -> download per step through the C-ABI, host buffers."""
+    import torch
+    from flash5_b200.hydro import next_dt
+    stream = torch.cuda.ExternalStream(h.stream)
+    h.upload(unk_host)
+    dt, _ = h.compute_dt()
+    dt_old, t = dt, 0.0
+
+    def one():
+        nonlocal dt, dt_old, t
+        h.upload(unk_host)
+        h(t + dt, dt, dt_old)
+        dcfl, _ = h.compute_dt()
+        h.download(unk_host)
+        t += dt
+        dt_old, dt = dt, next_dt(dcfl, dt)
+
+    for _ in range(warmup):
+        one()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        one()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def cpu_baseline(seconds=12.0, steps=None, warmup=0):
+    """Oracle (C restatement of the reference) on a 64^3 sample, all threads."""
+    from flash5_b200 import abi, setups
+    from flash5_b200.grid import UniformGrid
+    from flash5_b200.hydro import next_dt
+    from oracle import orc
+    g = UniformGrid(3, (8, 8, 8), (8, 8, 8), bc="periodic")
+    p = abi.default_params(gamma=5.0 / 3.0)
+    unk = setups.kelvin_helmholtz(g)
+    o = orc.Oracle(p, g)
+    o.eos_init(unk)
+    _, dt, _ = o.compute_dt(unk)
+    dt_old, t = dt, 0.0
+
+    def one():
+        nonlocal dt, dt_old, t
+        o.hydro(unk, t + dt, dt, dt_old)
+        _, dcfl, _ = o.compute_dt(unk)
+        t += dt
+        dt_old, dt = dt, next_dt(dcfl, dt)
+
+    for _ in range(warmup):
+        one()
+    n = 0
+    t0 = time.perf_counter()
+    while (steps is None and (n < 2 or time.perf_counter() - t0 < seconds)) or (steps is not None and n < steps):
+        one()
+        n += 1
+    el = time.perf_counter() - t0
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
+    return {"value": g.ncells * n / el, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"3D KH 64^3 (512 blocks of 8^3), {n} steps, {el:.1f} s, oracle C port, OpenMP"}
+
+
+def conserved_l1(a, b, var):
+    from oracle import sfocu
+    ca = sfocu.conserved(a, var)
+    cb = sfocu.conserved(b, var)
+    return {k: sfocu.l1_rel(ca[k], cb[k]) for k in sfocu.CONSERVED}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nblk", type=int, default=32, help="blocks per axis (32 -> 256^3)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--paths", default="fp64,fp64_fma,mixed",
+                    help="comma list of paths to time; profiling runs use one")
+    args = ap.parse_args()
+    paths = args.paths.split(",")
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    warmup = max(3, args.warmup)
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        r = cpu_baseline(steps=args.steps, warmup=warmup)
+        ms = 1000.0 / (r["value"] / (64 ** 3))
+        line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+                "warmup": warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": "3D Kelvin-Helmholtz 64^3 sample (512 blocks of 8^3), periodic, PPM+HLLC, CFL 0.8",
+                           "l2": "CPU"},
+                "impl": "reference", "cpu_baseline": r,
+                "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    import torch
+    dist = None
+    if world > 1:
+        import torch.distributed as tdist
+        import datetime
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    else:
+        torch.cuda.set_device(0)
+    dev = local if world > 1 else 0
+
+    from flash5_b200.hydro import Hydro
+    from flash5_b200.grid import VAR
+    g, unk, abi = kh_workload(args.nblk, nguard=0)
+    zones = g.ncells
+    peak, peak_kind = measured_peaks()
+
+    prec = {"fp64": abi.PREC_FP64, "fp64_fma": abi.PREC_FP64_FMA, "mixed": abi.PREC_MIXED}
+    ms, outs, dts, launches, clocks, e2e_ms, hb = {}, {}, None, 0, None, None, None
+    for name in ["fp64", "fp64_fma", "mixed"]:
+        if name not in paths:
+            continue
+        h = Hydro(abi.default_params(gamma=5.0 / 3.0, precision=prec[name]), g, device=dev)
+        h.upload(unk)
+        headline = name == paths[-1]
+        sampler = ClockSampler(dev) if headline else None
+        ms[name], used, launches = run_device(h, args.steps, warmup, dts=dts, sampler=sampler, dist=dist)
+        if dts is None:
+            dts = used            # later paths replay the first path's dt sequence
+        if headline:
+            clocks = sampler.summary()
+        outs[name] = np.empty_like(unk)
+        h.download(outs[name])
+        if headline and not args.no_e2e:
+            pinned = torch.empty(unk.shape, dtype=torch.float64, pin_memory=True)
+            host = pinned.numpy()
+            host[...] = unk
+            e2e_ms = run_e2e(h, host, max(3, min(args.steps, 8)), 3)
+            hb = host.nbytes
+        h.close()
+    head = paths[-1]
+    errs = {n: conserved_l1(outs[n], outs["fp64"], VAR) for n in outs if n != "fp64" and "fp64" in outs}
+    if dist is not None:
+        for n in ms:
+            ms[n] = dist_max(dist, ms[n])
+        if e2e_ms is not None:
+            e2e_ms = dist_max(dist, e2e_ms)
+    total = zones * world
+    value = total / (ms[head] * 1e-3)
+    if rank == 0:
+        cpu = None if (args.no_cpu or world > 1) else cpu_baseline()
+        achieved = zones * BYTES_PER_ZONE / (ms[head] * 1e-3) / 1e9
+        notes = {"fp64": "FP64, no FMA contraction; bit-identical to the CPU oracle in the tests",
+                 "fp64_fma": "FP64 with FMA contraction", "mixed": "FP32 reconstruction + Riemann solve, FP64 update"}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": warmup,
+            "ms_per_step": ms[head], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": {"mixed": "f32 reconstruction/flux, f64 update"}.get(head, "f64"),
+            "data": "synthetic (seeded KH noise)",
+            "config": {"workload": f"3D Kelvin-Helmholtz {8 * args.nblk}^3 as {args.nblk}^3 blocks of 8^3 (+4 guard "
+                                   "filled in-kernel), gamma 5/3, periodic, PPM+HLLC, CFL 0.8, dt from the CFL reduction "
+                                   "every step" + (", independent replica per GPU + NCCL dt min" if world > 1 else ""),
+                       "zones_per_gpu": zones, "l2": f"inputs larger than L2 (state {zones * 40 / 1e6:.0f} MB)",
+                       "path": head},
+            "paths": {n: {"value": total / (ms[n] * 1e-3), "ms_per_step": ms[n], "note": notes[n],
+                          **({"rel_l1_vs_fp64": errs[n]} if n in errs else {})} for n in ms},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "peak_kind": peak_kind,
+                         "kernel": "one hydro step (k_sig + k_dir x,y,z), 80 B/zone algorithmic"},
+            "clocks": clocks,
+            "gpu_launches": launches * args.steps,
+        }
+        if "fp64" in ms and head != "fp64":
+            line["speedup_vs_fp64"] = ms["fp64"] / ms[head]
+        if e2e_ms is not None:
+            line["e2e"] = {"value": total / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": hb,
+                           "d2h_bytes_per_step": hb, "ms_per_step": e2e_ms,
+                           "path": "flash_hy_upload + flash_hy_step + flash_hy_compute_dt + flash_hy_download, "
+                                   "interior-only FLASH UNK (11 vars), pinned host memory"}
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -18,7 +18,8 @@ VAR = {n: i for i, n in enumerate(abi.FLASH_UHD_VARS)}
 
 
 class UniformGrid:
-    def __init__(self, ndim, nb, nblk, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), bc="outflow", order="lex"):
+    def __init__(self, ndim, nb, nblk, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), bc="outflow", order="lex",
+                 nguard=NGUARD):
         self.ndim = ndim
         nb = tuple(nb) + (1,) * (3 - len(nb))
         nblk = tuple(nblk) + (1,) * (3 - len(nblk))
@@ -42,7 +43,8 @@ class UniformGrid:
         self.coords = np.array(coords, dtype=np.int32)
         self.nblocks = len(coords)
         self.levels = np.ones(self.nblocks, dtype=np.int32)
-        self.ng = (NGUARD, NGUARD if ndim > 1 else 0, NGUARD if ndim > 2 else 0)
+        self.nguard = nguard
+        self.ng = (nguard, nguard if ndim > 1 else 0, nguard if ndim > 2 else 0)
         self.nt = tuple(self.nb[d] + 2 * self.ng[d] for d in range(3))
         self.delta = tuple((self.hi[d] - self.lo[d]) / (self.nblk[d] * self.nb[d]) if d < ndim else 1.0
                            for d in range(3))
@@ -55,7 +57,7 @@ class UniformGrid:
         g = abi.GridDesc()
         g.ndim = self.ndim
         g.nxb, g.nyb, g.nzb = self.nb
-        g.nguard = NGUARD
+        g.nguard = self.nguard
         g.nblocks = self.nblocks
         for d in range(3):
             g.nblk_l1[d] = self.nblk[d]

@@ -75,10 +75,11 @@ def kelvin_helmholtz(grid, gamma=5.0 / 3.0, seed=12345, noise=1e-3):
     nx, ny, nz = (grid.nblk[d] * grid.nb[d] for d in range(3))
     rng = np.random.default_rng(seed)
     glob = rng.uniform(-noise, noise, size=(nz, ny, nx))
-    pert = np.empty_like(rho)
-    for b, (bx, by, bz) in enumerate(grid.coords):
-        pert[b] = glob[bz * grid.nb[2]:(bz + 1) * grid.nb[2], by * grid.nb[1]:(by + 1) * grid.nb[1],
-                       bx * grid.nb[0]:(bx + 1) * grid.nb[0]]
+    # global (z, y, x) -> per-block (nzb, nyb, nxb) tiles in block order
+    tiles = glob.reshape(grid.nblk[2], grid.nb[2], grid.nblk[1], grid.nb[1], grid.nblk[0], grid.nb[0])
+    tiles = tiles.transpose(0, 2, 4, 1, 3, 5)
+    c = grid.coords
+    pert = tiles[c[:, 2], c[:, 1], c[:, 0]]
     vy = 0.01 * np.sin(4.0 * np.pi * x) + pert
     vz = np.zeros_like(rho)
     p = np.full_like(rho, 2.5)
