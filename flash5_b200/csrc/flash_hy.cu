@@ -131,7 +131,7 @@ extern "C" int flash_hy_create(const flash_hy_params *params, const flash_hy_gri
   c->ncb = (size_t)g->nxb * ny * nz;
   c->ncells = c->ncb * g->nblocks;
   c->device = device;
-  c->threads = 256;
+  c->threads = g->ndim == 3 ? 320 : (g->nxb == 8 ? 96 : 288);  // line cells split evenly
   c->host_ng = g->nguard;
   *out = c;
   int rc = 0;

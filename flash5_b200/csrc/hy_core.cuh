@@ -146,12 +146,8 @@ __device__ __forceinline__ void rproject(const Eig<R> &e, const R db[5], R t[5])
 // under FLASH_EOS_GAMMA (PPM.F90:733-736) and are not computed.
 // ---------------------------------------------------------------------------
 template <class R, int DIR>
-__device__ __forceinline__ void tvd_slope(const DevParams &P, const R *VL, const R *V0, const R *VR,
-                                          const Eig<R> &e, R db[8]) {
-  R dL[5], dR[5];
-#pragma unroll
-  for (int n = 0; n < 5; ++n) { dL[n] = V0[n] - VL[n]; dR[n] = VR[n] - V0[n]; }
-  R dLe = V0[HEI] - VL[HEI], dRe = VR[HEI] - V0[HEI];
+__device__ __forceinline__ void tvd_slope_d(const DevParams &P, const R *dL, const R *dR, R dLe, R dRe,
+                                            const Eig<R> &e, R db[8]) {
   const int lim = P.limiter;
   const R beta = R(P.lim_beta);
   if (P.char_limiting) {
@@ -177,16 +173,23 @@ __device__ __forceinline__ void tvd_slope(const DevParams &P, const R *VL, const
   db[HGC] = R(0); db[HGE] = R(0);
 }
 
+template <class R, int DIR>
+__device__ __forceinline__ void tvd_slope(const DevParams &P, const R *VL, const R *V0, const R *VR,
+                                          const Eig<R> &e, R db[8]) {
+  R dL[5], dR[5];
+#pragma unroll
+  for (int n = 0; n < 5; ++n) { dL[n] = V0[n] - VL[n]; dR[n] = VR[n] - V0[n]; }
+  tvd_slope_d<R, DIR>(P, dL, dR, V0[HEI] - VL[HEI], VR[HEI] - V0[HEI], e, db);
+}
+
 // ---------------------------------------------------------------------------
 // hy_upwindTransverseFlux.F90:75-207 (transOrder = 1), sparse reig terms
 // ---------------------------------------------------------------------------
 template <class R, int DIR>
-__device__ __forceinline__ void upwind_tflux(const DevParams &P, const R *vm1, const R *vc0, const R *vp1,
-                                             const Eig<R> &e, R sig[8]) {
+__device__ __forceinline__ void upwind_tflux_d(const DevParams &P, const R *dl, const R *dr, R dle, R dre,
+                                               const Eig<R> &e, R sig[8]) {
   constexpr int v1 = Slots<DIR>::v1, v2 = Slots<DIR>::v2, v3 = Slots<DIR>::v3;
-  R dl[5], dr[5], dn[5];
-#pragma unroll
-  for (int v = 0; v < 5; ++v) { dl[v] = vc0[v] - vm1[v]; dr[v] = vp1[v] - vc0[v]; }
+  R dn[5];
 #pragma unroll
   for (int n = 0; n < 5; ++n) dn[n] = ldot<R, DIR>(e, n, e.lam[n] > R(0) ? dl : dr);
   const R *lam = e.lam;
@@ -196,12 +199,17 @@ __device__ __forceinline__ void upwind_tflux(const DevParams &P, const R *vm1, c
   sig[v3] = lam[3] * dn[3];
   sig[HP] = (lam[0] * e.rp) * dn[0] + (lam[4] * e.rp) * dn[4];
   sig[HGC] = R(0); sig[HGE] = R(0);
-  if (P.use_aux_eint) {
-    R t = lam[2] > R(0) ? vc0[HEI] - vm1[HEI] : vp1[HEI] - vc0[HEI];
-    sig[HEI] = lam[2] * t;
-  } else {
-    sig[HEI] = R(0);
-  }
+  sig[HEI] = P.use_aux_eint ? lam[2] * (lam[2] > R(0) ? dle : dre) : R(0);
+}
+
+// upwind differences dl = vc0 - vm1, dr = vp1 - vc0 of the three cells
+template <class R, int DIR>
+__device__ __forceinline__ void upwind_tflux(const DevParams &P, const R *vm1, const R *vc0, const R *vp1,
+                                             const Eig<R> &e, R sig[8]) {
+  R dl[5], dr[5];
+#pragma unroll
+  for (int v = 0; v < 5; ++v) { dl[v] = vc0[v] - vm1[v]; dr[v] = vp1[v] - vc0[v]; }
+  upwind_tflux_d<R, DIR>(P, dl, dr, vc0[HEI] - vm1[HEI], vp1[HEI] - vc0[HEI], e, sig);
 }
 
 // ---------------------------------------------------------------------------

@@ -57,7 +57,7 @@ __device__ __forceinline__ size_t cell_src(const DevParams &P, int b, int3 bc, i
 
 // Primitive slots of a cell as hy_getRiemannState sees it: interior cells
 // straight from the state, guard cells after the guard-cell EOS.
-template <int NDIM, int NX, int NY, int NZ>
+template <int NDIM, int NX, int NY, int NZ, bool GAME = true>
 __device__ __forceinline__ void load_prim(const DevParams &P, int b, int3 bc, int li, int lj, int lk, double V[8]) {
   bool inside; int fx, fy, fz;
   size_t o = cell_src<NDIM, NX, NY, NZ>(P, b, bc, li, lj, lk, inside, fx, fy, fz);
@@ -74,7 +74,9 @@ __device__ __forceinline__ void load_prim(const DevParams &P, int b, int3 bc, in
   }
   double p = rho * eg * P.gam1inv;
   V[HD] = rho; V[HVX] = vx; V[HVY] = vy; V[HVZ] = vz; V[HP] = p;
-  V[HGC] = P.gamma; V[HGE] = p / (eg * rho) + 1; V[HEI] = eg;
+  // GAME (Eos_putData.F90:105-106) is only read for the cell's own face
+  // states; stencil neighbours skip the division
+  V[HGC] = P.gamma; V[HGE] = GAME ? p / (eg * rho) + 1 : 0.0; V[HEI] = eg;
 }
 
 // Pressure only (flattening stencil ends).
@@ -105,15 +107,19 @@ __device__ __forceinline__ int3 blk_coords(const DevParams &P, int b) {
   return make_int3(P.blk_coord[3 * b], P.blk_coord[3 * b + 1], P.blk_coord[3 * b + 2]);
 }
 
+// Differences are taken in FP64 before any conversion to R, so the FP32
+// path carries the relative precision of the differences, not of the values.
 template <class R, int DIR>
 __device__ __forceinline__ void sig_dir(const DevParams &P, const double *Vm, const double *Vc, const double *Vp,
                                         R sig[8], unsigned &st) {
-  R m[8], c[8], p[8];
+  R c[8], dl[5], dr[5];
 #pragma unroll
-  for (int n = 0; n < 8; ++n) { m[n] = R(Vm[n]); c[n] = R(Vc[n]); p[n] = R(Vp[n]); }
+  for (int n = 0; n < 8; ++n) c[n] = R(Vc[n]);
+#pragma unroll
+  for (int n = 0; n < 5; ++n) { dl[n] = R(Vc[n] - Vm[n]); dr[n] = R(Vp[n] - Vc[n]); }
   Eig<R> e;
   eigen<R, DIR>(c, e, st);
-  upwind_tflux<R, DIR>(P, m, c, p, e, sig);
+  upwind_tflux_d<R, DIR>(P, dl, dr, R(Vc[HEI] - Vm[HEI]), R(Vp[HEI] - Vc[HEI]), e, sig);
 }
 
 // sig components kept in memory: dens, velx, vely, velz, pres, eint
@@ -124,8 +130,8 @@ __device__ __forceinline__ int sig_slot(int q) { return q < 5 ? q : HEI; }
 // (hy_DataReconstructNormalDir_PPM.F90:351-371 via hy_getRiemannState.F90:
 // 471-637, which evaluates it for every cell of [lo-1, hi+1]^d)
 // ---------------------------------------------------------------------------
-template <int NDIM, int NX, int NY, int NZ, class R>
-__global__ void __launch_bounds__(256) k_sig(const DevParams P, R *__restrict__ SIG) {
+template <int NDIM, int NX, int NY, int NZ, class R, int VAR>
+__global__ void __launch_bounds__(320) k_sig(const DevParams P, R *__restrict__ SIG) {
   using B = Box<NDIM, NX, NY, NZ>;
   const int b = P.blk_list ? P.blk_list[blockIdx.x] : blockIdx.x;
   const int3 bc = blk_coords(P, b);
@@ -133,11 +139,11 @@ __global__ void __launch_bounds__(256) k_sig(const DevParams P, R *__restrict__ 
   for (int t = threadIdx.x; t < B::n; t += blockDim.x) {
     int i = t % B::bx - 1, j = NDIM > 1 ? (t / B::bx) % B::by - 1 : 0, k = NDIM > 2 ? t / (B::bx * B::by) - 1 : 0;
     double Vc[8], Vm[8], Vp[8];
-    load_prim<NDIM, NX, NY, NZ>(P, b, bc, i, j, k, Vc);
+    load_prim<NDIM, NX, NY, NZ, false>(P, b, bc, i, j, k, Vc);
 #pragma unroll
     for (int d = 1; d <= NDIM; ++d) {
-      load_prim<NDIM, NX, NY, NZ>(P, b, bc, i - (d == 1), j - (d == 2), k - (d == 3), Vm);
-      load_prim<NDIM, NX, NY, NZ>(P, b, bc, i + (d == 1), j + (d == 2), k + (d == 3), Vp);
+      load_prim<NDIM, NX, NY, NZ, false>(P, b, bc, i - (d == 1), j - (d == 2), k - (d == 3), Vm);
+      load_prim<NDIM, NX, NY, NZ, false>(P, b, bc, i + (d == 1), j + (d == 2), k + (d == 3), Vp);
       R s[8];
       if (d == 1) sig_dir<R, 1>(P, Vm, Vc, Vp, s, st);
       else if (d == 2) sig_dir<R, 2>(P, Vm, Vc, Vp, s, st);
@@ -234,8 +240,8 @@ struct DirGeom {
 // slots stored for the face states: dens, velx, vely, velz, pres, game, eint
 __device__ __forceinline__ int wslot(int q) { return q < 5 ? q : q + 1; }
 
-template <int NDIM, int NX, int NY, int NZ, class R, int DIR, bool FIRST, bool LAST>
-__global__ void __launch_bounds__(256) k_dir(const DevParams P, const R *__restrict__ SIG, double *__restrict__ ACC,
+template <int NDIM, int NX, int NY, int NZ, class R, int DIR, bool FIRST, bool LAST, int VAR>
+__global__ void __launch_bounds__(320) k_dir(const DevParams P, const R *__restrict__ SIG, double *__restrict__ ACC,
                                              double *__restrict__ AUX, size_t ncells, CflPart *part) {
   using G = DirGeom<NDIM, NX, NY, NZ, R, DIR>;
   using B = Box<NDIM, NX, NY, NZ>;
@@ -262,7 +268,8 @@ __global__ void __launch_bounds__(256) k_dir(const DevParams P, const R *__restr
     double Vd[8];
 #pragma unroll
     for (int s = -2; s <= 2; ++s) {
-      load_prim<NDIM, NX, NY, NZ>(P, b, bc, i + s * di, j + s * dj, k + s * dk, Vd);
+      if (s == 0) load_prim<NDIM, NX, NY, NZ, true>(P, b, bc, i, j, k, Vd);
+      else load_prim<NDIM, NX, NY, NZ, false>(P, b, bc, i + s * di, j + s * dj, k + s * dk, Vd);
 #pragma unroll
       for (int n = 0; n < 8; ++n) V5[s + 2][n] = R(Vd[n]);
     }
@@ -475,7 +482,7 @@ __global__ void __launch_bounds__(256) k_dir(const DevParams P, const R *__restr
 
 // CFL reduction of a stored state (Hydro_computeDt on its own).
 template <int NDIM, int NX, int NY, int NZ>
-__global__ void __launch_bounds__(256) k_cfl(const DevParams P, CflPart *part) {
+__global__ void __launch_bounds__(320) k_cfl(const DevParams P, CflPart *part) {
   constexpr int NCB = NX * NY * NZ;
   const int b = blockIdx.x;
   CflCand cand; cand.key = 0.0; cand.val = 0.0; cand.idx = 0x7fffffff;

@@ -1,0 +1,482 @@
+// hy_mixed.cuh -- the mixed-precision direction kernel.
+//
+// Same algorithm as k_dir (PPM with characteristic limiting / flattening /
+// steepening, transverse and 3D CTU corrections, HLLC, unsplit update), with
+// three changes that do not exist in the FP64 parity path:
+//  * the reconstruction runs in FP32 in "delta form": every quantity is an
+//    increment relative to the cell value (differences of neighbours are
+//    taken in FP64 and then rounded), and the face states are assembled as
+//    W = V_cell (FP64) + dW (FP32).  FP32 rounding then scales with the
+//    increments instead of the values, e.g. the 1e-3 pressure variations of
+//    a p = 2.5 background keep ~1e-10 absolute precision instead of 1.5e-7;
+//  * the primitive stencil of every line is staged once in shared memory
+//    and the limited slopes of each cell are computed once and shared by
+//    its neighbours (the reference recomputes three per cell,
+//    hy_DataReconstructNormalDir_PPM.F90:438-441);
+//  * the Riemann solve, the fluxes and the update run in FP64 (HLLC with
+//    shared reciprocals instead of the reference's repeated divisions).
+#pragma once
+#include "hy_kernels.cuh"
+
+namespace fhy {
+
+// FP64 HLLC (hy_HLLC.F90:94-311) with one division per star state; igm1 =
+// 1/(game - 1) of the cell the face state belongs to.
+template <int DIR>
+__device__ __forceinline__ void hllc_fp64(const DevParams &P, const double *Vm, const double *Vp, double igL,
+                                          double igR, double Fs[6], unsigned &st) {
+  constexpr int v1 = Slots<DIR>::v1;
+  const double tiny = P.tiny;
+  if ((Vm[HD] < tiny && Vm[HD] > 0.) || (Vp[HD] < tiny && Vp[HD] > 0.) || (Vm[HP] < tiny && Vm[HP] > 0.) ||
+      (Vp[HP] < tiny && Vp[HP] > 0.)) {
+#pragma unroll
+    for (int n = 0; n < 6; ++n) Fs[n] = 0.;
+    return;
+  }
+  const double uL = Vm[v1], uR = Vp[v1], dL = Vm[HD], dR = Vp[HD], pL = Vm[HP], pR = Vp[HP];
+  const double aL2 = P.gamma * pL / dL, aR2 = P.gamma * pR / dR;
+  if (aL2 < 0. || aR2 < 0.) {
+    st |= ST_NEG_SOUND;
+#pragma unroll
+    for (int n = 0; n < 6; ++n) Fs[n] = 0.;
+    return;
+  }
+  const double cL = sqrt(aL2), cR = sqrt(aR2);
+  const double SL = fmin(uL - cL, uR - cR), SR = fmax(uL + cL, uR + cR);
+  double qStar = (dR * uR * (SR - uR) - dL * uL * (SL - uL) + pL - pR) / (dR * (SR - uR) - dL * (SL - uL));
+  // side whose flux (and star state) is used
+  const bool useL = SL >= 0. || qStar >= 0.;
+  const double *V = useL ? Vm : Vp;
+  const double d = useL ? dL : dR, u = useL ? uL : uR, p = useL ? pL : pR, S = useL ? SL : SR;
+  const double ig = useL ? igL : igR;
+  const double u2 = V[HVX] * V[HVX] + V[HVY] * V[HVY] + V[HVZ] * V[HVZ];
+  const double E = 0.5 * d * u2 + p * ig;
+  double F[5], U[5];
+  F[0] = d * u;
+  F[1] = F[0] * V[HVX]; F[2] = F[0] * V[HVY]; F[3] = F[0] * V[HVZ];
+  F[DIR] += p;
+  F[4] = (E + p) * u;
+  Fs[5] = p;
+  const bool outside = useL ? (SL >= 0.) : (SR < 0.);
+  if (outside) {
+#pragma unroll
+    for (int n = 0; n < 5; ++n) Fs[n] = F[n];
+    return;
+  }
+  U[0] = d; U[1] = d * V[HVX]; U[2] = d * V[HVY]; U[3] = d * V[HVZ]; U[4] = E;
+  const double num = S - u, rden = 1.0 / (S - qStar);
+  const double r = num * rden;
+  const double pStar = dL * (SL - uL) * (qStar - uL) + pL;
+  double UC[5];
+  UC[0] = d * r;
+#pragma unroll
+  for (int m = 1; m <= 3; ++m) UC[m] = (m == DIR) ? UC[0] * qStar : U[m] * r;
+  UC[4] = U[4] * r + (pStar * qStar - p * u) * rden;
+#pragma unroll
+  for (int n = 0; n < 5; ++n) Fs[n] = F[n] + S * (UC[n] - U[n]);
+}
+
+template <int NDIM, int NX, int NY, int NZ, int DIR>
+struct MxGeom {
+  static constexpr int ND = DIR == 1 ? NX : (DIR == 2 ? NY : NZ);
+  static constexpr int C = DIR == 1 ? NY * NZ : (DIR == 2 ? NX * NZ : NX * NY);   // lines
+  static constexpr int L4 = ND + 8, LS = ND + 4, LC = ND + 2;                      // staged, slope, line cells
+  static constexpr int SA = L4 * C, SB = LS * C, SC = LC * C;
+  // index of position x on line l in a space of length L with offset o
+  __device__ static __forceinline__ int at(int x, int l, int L, int o) { return DIR == 1 ? l * L + (x + o) : (x + o) * C + l; }
+  __device__ static __forceinline__ void dec(int s, int L, int o, int &x, int &l) {
+    if (DIR == 1) { l = s / L; x = s % L - o; } else { l = s % C; x = s / C - o; }
+  }
+  static constexpr int step = DIR == 1 ? 1 : C;      // +1 along the line
+  __device__ static __forceinline__ void cell(int x, int l, int &i, int &j, int &k) {
+    if (DIR == 1) { i = x; j = l % NY; k = l / NY; }
+    else if (DIR == 2) { j = x; i = l % NX; k = l / NX; }
+    else { k = x; i = l % NX; j = l / NX; }
+    if (NDIM < 3) k = (DIR == 3) ? k : 0;
+  }
+  // shared memory: staged prims (FP64), then a region used first for the
+  // reconstruction scratch and then for the face fluxes
+  static constexpr size_t prim_bytes = (size_t)6 * SA * 8;
+  static constexpr size_t recon_bytes = (size_t)SB * 4 + (size_t)SB * 6 * 4 + (size_t)2 * SC * 6 * 4 + (size_t)SC * 8;
+  static constexpr size_t flux_bytes = (size_t)SC * 9 * 8;
+  static constexpr size_t smem_bytes() { return prim_bytes + (recon_bytes > flux_bytes ? recon_bytes : flux_bytes); }
+};
+
+template <int NDIM, int NX, int NY, int NZ> struct MxThreads {
+  static constexpr int n = NDIM == 3 ? 320 : (NX == 8 ? 96 : 288);
+};
+
+template <int NDIM, int NX, int NY, int NZ, int DIR, bool FIRST, bool LAST>
+__global__ void __launch_bounds__(MxThreads<NDIM, NX, NY, NZ>::n, NDIM == 3 ? 2 : 1)
+k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ ACC, double *__restrict__ AUX,
+         size_t ncells, CflPart *part) {
+  using G = MxGeom<NDIM, NX, NY, NZ, DIR>;
+  using B = Box<NDIM, NX, NY, NZ>;
+  constexpr int NCB = NX * NY * NZ;
+  constexpr int NT = MxThreads<NDIM, NX, NY, NZ>::n;
+  constexpr int NIT = (G::SC + NT - 1) / NT;
+  constexpr int v1 = Slots<DIR>::v1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double *sV = reinterpret_cast<double *>(smem_raw);                     // [6][SA]: rho,u,v,w,p,e
+  unsigned char *reg = smem_raw + G::prim_bytes;
+  float *sFlat = reinterpret_cast<float *>(reg);                          // [SB]
+  float *sDb = sFlat + G::SB;                                             // [6][SB]
+  float *sWp = sDb + 6 * G::SB;                                           // [6][SC] increments
+  float *sWm = sWp + 6 * G::SC;                                           // [6][SC]
+  double *sIg = reinterpret_cast<double *>(sWm + 6 * G::SC);              // [SC] 1/(game-1)
+  double *sF = reinterpret_cast<double *>(reg);                           // [9][SC] (after phase D)
+
+  const int b = P.blk_list ? P.blk_list[blockIdx.x] : blockIdx.x;
+  const int3 bc = blk_coords(P, b);
+  unsigned st = 0;
+  const double dt = P.dt, delta = P.del[DIR - 1];
+  const float dtn = float(dt / delta), hdtn = 0.5f * dtn;
+  const float hdtx = float(0.5 * dt / P.del[0]), hdty = float(0.5 * dt / P.del[1]), hdtz = float(0.5 * dt / P.del[2]);
+  const float *sigb = SIG + (size_t)blockIdx.x * NDIM * 6 * B::n;
+
+  // ---- A: stage the primitive stencil of every line (guard cells get the EOS)
+  for (int s = threadIdx.x; s < G::SA; s += NT) {
+    int x, l, i, j, k;
+    G::dec(s, G::L4, 4, x, l);
+    G::cell(x, l, i, j, k);
+    double V[8];
+    load_prim<NDIM, NX, NY, NZ, false>(P, b, bc, i, j, k, V);
+    sV[0 * G::SA + s] = V[HD]; sV[1 * G::SA + s] = V[HVX]; sV[2 * G::SA + s] = V[HVY];
+    sV[3 * G::SA + s] = V[HVZ]; sV[4 * G::SA + s] = V[HP]; sV[5 * G::SA + s] = V[HEI];
+  }
+  __syncthreads();
+  auto Vs = [&](int q, int s) -> double { return sV[q * G::SA + s]; };   // q: 0..5 (5 = eint)
+
+  // ---- B: limited slopes and flattening switches of cells [-2, N+1]
+  for (int q = threadIdx.x; q < G::SB; q += NT) {
+    int x, l;
+    G::dec(q, G::LS, 2, x, l);
+    const int s = G::at(x, l, G::L4, 4);
+    float Vc[8], dL[5], dR[5];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) {
+      Vc[n] = float(Vs(n, s));
+      dL[n] = float(Vs(n, s) - Vs(n, s - G::step));
+      dR[n] = float(Vs(n, s + G::step) - Vs(n, s));
+    }
+    Vc[HGC] = float(P.gamma); Vc[HGE] = 0.f; Vc[HEI] = float(Vs(5, s));
+    Eig<float> e;
+    eigen<float, DIR>(Vc, e, st);
+    float db[8];
+    tvd_slope_d<float, DIR>(P, dL, dR, float(Vs(5, s) - Vs(5, s - G::step)), float(Vs(5, s + G::step) - Vs(5, s)), e,
+                            db);
+#pragma unroll
+    for (int n = 0; n < 5; ++n) sDb[n * G::SB + q] = db[n];
+    sDb[5 * G::SB + q] = db[HEI];
+    if (P.use_flattening) {
+      const int st1 = G::step, st2 = 2 * G::step;
+      float dp1 = float(Vs(4, s + st1) - Vs(4, s - st1));
+      float dp2 = float(Vs(4, s + st2) - Vs(4, s - st2));
+      float dv1 = float(Vs(v1, s + st1) - Vs(v1, s - st1));
+      float pmin = float(fmin(Vs(4, s - st1), Vs(4, s + st1)));
+      float Sp = fabsf(dp2) > 1.e-15f ? dp1 / dp2 - 0.75f : 0.f;
+      float ft = fmaxf(0.f, fminf(1.f, 10.f * Sp));
+      if ((fabsf(dp1) / pmin < 1.f / 3.f) || dv1 > 0.f) ft = 0.f;
+      sFlat[q] = ft;
+    }
+  }
+  __syncthreads();
+
+  // ---- C: face states of the line cells [-1, N] as increments
+  for (int t = threadIdx.x; t < G::SC; t += NT) {
+    int x, l, i, j, k;
+    G::dec(t, G::LC, 1, x, l);
+    G::cell(x, l, i, j, k);
+    const int s = G::at(x, l, G::L4, 4), q = G::at(x, l, G::LS, 2);
+    const int qs = G::step;
+    float Vc[8], dL[8], dR[8];
+#pragma unroll
+    for (int n = 0; n < 5; ++n) {
+      Vc[n] = float(Vs(n, s));
+      dL[n] = float(Vs(n, s) - Vs(n, s - G::step));
+      dR[n] = float(Vs(n, s + G::step) - Vs(n, s));
+    }
+    Vc[HGC] = float(P.gamma); Vc[HEI] = float(Vs(5, s));
+    dL[HEI] = float(Vs(5, s) - Vs(5, s - G::step));
+    dR[HEI] = float(Vs(5, s + G::step) - Vs(5, s));
+    Eig<float> e0;
+    eigen<float, DIR>(Vc, e0, st);
+    float flat = 0.f;
+    if (P.use_flattening) {
+      float t0 = sFlat[q];
+      double dp1 = Vs(4, s + G::step) - Vs(4, s - G::step);
+      if (dp1 < 0.) flat = fmaxf(t0, sFlat[q + qs]);
+      else if (dp1 == 0.) flat = t0;
+      else flat = fmaxf(t0, sFlat[q - qs]);
+    }
+    const int sl[6] = {0, 1, 2, 3, 4, 7};
+    float lft[8], rgt[8], delW[8], W6[8];
+#pragma unroll
+    for (int qq = 0; qq < 6; ++qq) {
+      int n = sl[qq], m = qq < 5 ? qq : 5;
+      float dbN = sDb[m * G::SB + q - qs], db0 = sDb[m * G::SB + q], dbP = sDb[m * G::SB + q + qs];
+      lft[n] = -0.5f * dL[n] - (db0 - dbN) / 6.f;
+      rgt[n] = 0.5f * dR[n] - (dbP - db0) / 6.f;
+    }
+    if (P.use_steepening) {
+      const float eta1 = 20.f, eta2 = 0.05f, epsln = 0.01f, K0 = 0.1f;
+      double rm = Vs(0, s - G::step), rp = Vs(0, s + G::step), rc = Vs(0, s);
+      double rmm = Vs(0, s - 2 * G::step), rpp = Vs(0, s + 2 * G::step);
+      float temp1 = float(rp - rm);
+      if (fabsf(temp1) > float(P.tiny)) {
+        float dd = float(delta);
+        float d2R = float((rpp - rp) - (rp - rc)) / (6.f * dd * dd);
+        float d2L = float((rc - rm) - (rm - rmm)) / (6.f * dd * dd);
+        float eta = (d2L - d2R) * (dd * dd) / temp1;
+        if (d2R * d2L >= 0.f) eta = 0.f;
+        if (epsln * float(fmin(rp, rm)) - fabsf(temp1) >= 0.f) eta = 0.f;
+        eta = fmaxf(0.f, fminf(1.f, eta1 * (eta - eta2)));
+        double pm = Vs(4, s - G::step), pp = Vs(4, s + G::step);
+        float temp2 = float(fabs(pp - pm) / fmin(pp, pm));
+        float temp3 = fabsf(temp1) / float(fmin(rp, rm));
+        double game_c = Vs(4, s) / (Vs(5, s) * rc) + 1;
+        if (float(game_c) * K0 * temp3 - temp2 < 0.f) eta = 0.f;
+        float dbN = sDb[q - qs], dbP = sDb[q + qs];
+        lft[HD] = lft[HD] * (1.f - eta) + (-dL[HD] + 0.5f * dbN) * eta;
+        rgt[HD] = rgt[HD] * (1.f - eta) + (dR[HD] - 0.5f * dbP) * eta;
+      }
+    }
+#pragma unroll
+    for (int qq = 0; qq < 6; ++qq) {
+      int n = sl[qq];
+      if (P.use_flattening) { lft[n] = (1.f - flat) * lft[n]; rgt[n] = (1.f - flat) * rgt[n]; }
+      if (rgt[n] * (-lft[n]) <= 0.f) { lft[n] = 0.f; rgt[n] = 0.f; }
+      float dw = rgt[n] - lft[n];
+      if (6.f * dw * (-0.5f * (lft[n] + rgt[n])) > dw * dw) lft[n] = -2.f * rgt[n];
+      dw = rgt[n] - lft[n];
+      if (6.f * dw * (-0.5f * (lft[n] + rgt[n])) < -(dw * dw)) rgt[n] = -2.f * lft[n];
+      delW[n] = rgt[n] - lft[n];
+      W6[n] = -3.f * (lft[n] + rgt[n]);
+    }
+    float dWp[8], dWm[8];
+    {
+      float lmax = fmaxf(e0.lam[2], 0.f);
+      dWp[HEI] = rgt[HEI] - lmax * hdtn * (delW[HEI] - (1.f - lmax * hdtn * 4.f / 3.f) * W6[HEI]);
+      float lmin = -fminf(e0.lam[2], 0.f);
+      dWm[HEI] = lft[HEI] + lmin * hdtn * (delW[HEI] + (1.f - lmin * hdtn * 4.f / 3.f) * W6[HEI]);
+    }
+    {
+      constexpr int u1 = Slots<DIR>::v1, u2 = Slots<DIR>::v2, u3 = Slots<DIR>::v3;
+      float mW6[5];
+#pragma unroll
+      for (int n = 0; n < 5; ++n) mW6[n] = -W6[n];
+      float sL[5] = {0.f, 0.f, 0.f, 0.f, 0.f}, sR[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+      for (int n = 0; n < 5; ++n) {
+        float cA = ldot<float, DIR>(e0, n, delW), cB = ldot<float, DIR>(e0, n, mW6);
+        float lam = e0.lam[n], xx = dtn * lam;
+        float AL = 0.5f * (-1.f - xx), BL = 0.25f * (1.f + 2.f * xx + (4.f / 3.f) * (xx * xx));
+        float AR = 0.5f * (1.f - xx), BR = 0.25f * (1.f - 2.f * xx + (4.f / 3.f) * (xx * xx));
+        float tL = AL * cA + BL * cB, tR = AR * cA + BR * cB;
+        if (n == 0 || n == 4) {
+          float rv = n == 0 ? -e0.cf : e0.cf;
+          sL[HD] += e0.rho * tL; sR[HD] += e0.rho * tR;
+          sL[u1] += rv * tL; sR[u1] += rv * tR;
+          sL[HP] += e0.rp * tL; sR[HP] += e0.rp * tR;
+        } else if (n == 1) { sL[u2] += tL; sR[u2] += tR; }
+        else if (n == 2) { sL[HD] += tL; sR[HD] += tR; }
+        else { sL[u3] += tL; sR[u3] += tR; }
+      }
+#pragma unroll
+      for (int n = 0; n < 5; ++n) {
+        dWm[n] = W6[n] / 12.f + sL[n];
+        dWp[n] = W6[n] / 12.f + sR[n];
+      }
+    }
+    // transverse corrections
+    const int bi = B::idx(i, j, k);
+    float sx[8], sy[8], sz[8];
+    if (DIR != 1) load_sig(sigb + 0 * 6 * B::n + bi, B::n, sx);
+    if (NDIM > 1 && DIR != 2) load_sig(sigb + 1 * 6 * B::n + bi, B::n, sy);
+    if (NDIM > 2 && DIR != 3) load_sig(sigb + 2 * 6 * B::n + bi, B::n, sz);
+#pragma unroll
+    for (int qq = 0; qq < 6; ++qq) {
+      int n = sl[qq];
+      float c = 0.f;
+      if (NDIM == 2) c = DIR == 1 ? hdty * sy[n] : hdtx * sx[n];
+      else c = DIR == 1 ? hdty * sy[n] + hdtz * sz[n] : (DIR == 2 ? hdtx * sx[n] + hdtz * sz[n] : hdtx * sx[n] + hdty * sy[n]);
+      dWm[n] -= c;
+      dWp[n] -= c;
+    }
+    const double rc = Vs(0, s), pc = Vs(4, s);
+    if (rc + dWm[HD] < 0. || rc + dWp[HD] < 0. || pc + dWm[HP] < 0. || pc + dWp[HP] < 0.) {
+#pragma unroll
+      for (int n = 0; n < 8; ++n) { dWm[n] = 0.f; dWp[n] = 0.f; }
+    }
+    if (NDIM == 3 && P.use_ctu) {
+      constexpr int A1 = DIR == 1 ? 2 : (DIR == 2 ? 3 : 1), S1 = DIR == 1 ? 3 : (DIR == 2 ? 1 : 2);
+      constexpr int A2 = DIR == 1 ? 3 : (DIR == 2 ? 1 : 2), S2 = DIR == 1 ? 2 : (DIR == 2 ? 3 : 1);
+      const float fac = float(dt * dt / (6. * (DIR == 1 ? P.del[1] : (DIR == 2 ? P.del[2] : P.del[0])) *
+                                         (DIR == 1 ? P.del[2] : (DIR == 2 ? P.del[0] : P.del[1]))));
+      float T1[8], T2[8];
+      {
+        float sm[8], s0[8], sp[8];
+        const float *base = sigb + (size_t)(S1 - 1) * 6 * B::n;
+        load_sig(base + B::idx(i - (A1 == 1), j - (A1 == 2), k - (A1 == 3)), B::n, sm);
+        load_sig(base + bi, B::n, s0);
+        load_sig(base + B::idx(i + (A1 == 1), j + (A1 == 2), k + (A1 == 3)), B::n, sp);
+        Eig<float> e;
+        eigen<float, A1>(Vc, e, st);
+        upwind_tflux<float, A1>(P, sm, s0, sp, e, T1);
+      }
+      {
+        float sm[8], s0[8], sp[8];
+        const float *base = sigb + (size_t)(S2 - 1) * 6 * B::n;
+        load_sig(base + B::idx(i - (A2 == 1), j - (A2 == 2), k - (A2 == 3)), B::n, sm);
+        load_sig(base + bi, B::n, s0);
+        load_sig(base + B::idx(i + (A2 == 1), j + (A2 == 2), k + (A2 == 3)), B::n, sp);
+        Eig<float> e;
+        eigen<float, A2>(Vc, e, st);
+        upwind_tflux<float, A2>(P, sm, s0, sp, e, T2);
+      }
+#pragma unroll
+      for (int qq = 0; qq < 6; ++qq) {
+        int n = sl[qq];
+        float c = (T1[n] + T2[n]) * fac;
+        dWp[n] += c;
+        dWm[n] += c;
+      }
+      if (rc + dWp[HD] <= 0. || rc + dWm[HD] <= 0. || pc + dWp[HP] <= 0. || pc + dWm[HP] <= 0.) {
+#pragma unroll
+        for (int n = 0; n < 8; ++n) { dWm[n] = 0.f; dWp[n] = 0.f; }
+      }
+    }
+#pragma unroll
+    for (int qq = 0; qq < 6; ++qq) {
+      sWp[qq * G::SC + t] = dWp[sl[qq]];
+      sWm[qq * G::SC + t] = dWm[sl[qq]];
+    }
+    // 1/(game-1) of the cell: game - 1 = p/(e rho) (Eos_putData.F90:105-106)
+    sIg[t] = (Vs(5, s) * rc) / pc;
+  }
+  __syncthreads();
+
+  // ---- D: Riemann problems at the faces, FP64
+  double Fr[NIT][9];
+#pragma unroll
+  for (int it = 0; it < NIT; ++it) {
+    const int t = threadIdx.x + it * NT;
+    if (t >= G::SC) break;
+    int x, l;
+    G::dec(t, G::LC, 1, x, l);
+    if (x < 0) continue;
+    const int s = G::at(x, l, G::L4, 4);
+    const int tl = t - G::step, sL = s - G::step;
+    double VL[8], VR[8];
+#pragma unroll
+    for (int qq = 0; qq < 6; ++qq) {
+      int n = qq < 5 ? qq : HEI;
+      VL[n] = Vs(qq, sL) + double(sWp[qq * G::SC + tl]);
+      VR[n] = Vs(qq, s) + double(sWm[qq * G::SC + t]);
+    }
+    double F[6];
+    hllc_fp64<DIR>(P, VL, VR, sIg[tl], sIg[t], F, st);
+#pragma unroll
+    for (int n = 0; n < 6; ++n) Fr[it][n] = F[n];
+    double fv = 0., fe = 0.;
+    if (P.use_aux_eint) {
+      if (F[FDENS] > 0.) { fv = F[FDENS] / VL[HD]; fe = F[FDENS] * VL[HEI]; }
+      else { fv = F[FDENS] / VR[HD]; fe = F[FDENS] * VR[HEI]; }
+    }
+    Fr[it][FEINT] = fe;
+    Fr[it][FVOLU] = fv;
+    // N05 + P05 of this cell (n+1/2 pressure sum)
+    Fr[it][8] = (Vs(4, s) + double(sWm[4 * G::SC + t])) + (Vs(4, s) + double(sWp[4 * G::SC + t]));
+  }
+  __syncthreads();
+#pragma unroll
+  for (int it = 0; it < NIT; ++it) {
+    const int t = threadIdx.x + it * NT;
+    if (t >= G::SC) break;
+    int x, l;
+    G::dec(t, G::LC, 1, x, l);
+    if (x < 0) continue;
+#pragma unroll
+    for (int n = 0; n < 9; ++n) sF[n * G::SC + t] = Fr[it][n];
+  }
+  __syncthreads();
+
+  // ---- E: conservative update
+  const double dtd = dt / delta;
+  CflCand cand; cand.key = 0.0; cand.val = 0.0; cand.idx = 0x7fffffff;
+  for (int t = threadIdx.x; t < G::SC; t += NT) {
+    int x, l, i, j, k;
+    G::dec(t, G::LC, 1, x, l);
+    if (x < 0 || x >= G::ND) continue;
+    G::cell(x, l, i, j, k);
+    const int loc = (k * NY + j) * NX + i;
+    const size_t off = (size_t)b * NCB + loc;
+    double FL[NFLX], FR[NFLX];
+#pragma unroll
+    for (int n = 0; n < NFLX; ++n) { FL[n] = sF[n * G::SC + t]; FR[n] = sF[n * G::SC + t + G::step]; }
+    const double sp = sF[8 * G::SC + t];
+    double U[5];
+    if (FIRST) {
+      double rho = P.s_in[0][off], vx = P.s_in[1][off], vy = P.s_in[2][off], vz = P.s_in[3][off], e = P.s_in[4][off];
+      double ekin = 0.5 * (vx * vx + vy * vy + vz * vz);
+      U[0] = rho; U[1] = vx * rho; U[2] = vy * rho; U[3] = vz * rho; U[4] = rho * (e + ekin);
+    } else {
+#pragma unroll
+      for (int n = 0; n < 5; ++n) U[n] = ACC[n * ncells + off];
+    }
+#pragma unroll
+    for (int n = 0; n < 5; ++n) U[n] = U[n] - dtd * (FR[n] - FL[n]);
+    const double ea = FL[FEINT] - FR[FEINT], eb = FL[FVOLU] - FR[FVOLU];
+    if (!LAST) {
+#pragma unroll
+      for (int n = 0; n < 5; ++n) ACC[n * ncells + off] = U[n];
+      double *ax = AUX + (size_t)(DIR - 1) * 3 * ncells;
+      ax[off] = ea; ax[ncells + off] = eb; ax[2 * ncells + off] = sp;
+    } else {
+      const double rho0 = P.s_in[0][off], e0 = P.s_in[4][off];
+      double IntEner = 0.0;
+      if (P.use_aux_eint) {
+        double pb;
+        const double sx = AUX[2 * ncells + off];
+        if (NDIM == 2) {
+          pb = (0.5 * sx) * 0.5 + sp * 0.25;
+        } else {
+          const double sy = AUX[5 * ncells + off];
+          pb = (((0.5 * sx) * 0.5 + sy * 0.25) * 4.0 + sp) / 6.0;
+        }
+        IntEner = rho0 * e0 + dt / P.del[0] * (AUX[off] + pb * AUX[ncells + off]);
+        if (NDIM == 2) {
+          IntEner += dt / P.del[1] * (ea + pb * eb);
+        } else {
+          IntEner += dt / P.del[1] * (AUX[3 * ncells + off] + pb * AUX[4 * ncells + off]);
+          IntEner += dt / P.del[2] * (ea + pb * eb);
+        }
+      }
+      double dens = fmax(U[0], P.smlrho);
+      double rinv = 1.0 / dens;
+      double vx = U[1] * rinv, vy = U[2] * rinv, vz = U[3] * rinv;
+      double ener = U[4] * rinv;
+      double eaux = IntEner * rinv;
+      double ekin = 0.5 * (vx * vx + vy * vy + vz * vz);
+      double eint = ener - ekin;
+      double newE = (!P.use_aux_eint || eint > P.eswitch * ekin) ? fmax(P.smalle, eint) : fmax(P.smalle, eaux);
+      ener = newE + ekin;
+      double e = newE;
+      if (ener - ekin > fmax(P.smalle, P.eswitch * ekin)) e = ener - ekin;
+      P.s_out[0][off] = dens; P.s_out[1][off] = vx; P.s_out[2][off] = vy; P.s_out[3][off] = vz;
+      P.s_out[4][off] = e;
+      if (!(isfinite(dens) && isfinite(vx) && isfinite(vy) && isfinite(vz) && isfinite(e))) st |= ST_NAN;
+      double pres = dens * e * P.gam1inv;
+      double cs = sqrt(P.gamma * pres * rinv);
+      double dtl = (fabs(vx) + cs) * (1.0 / P.del[0]);
+      if (NDIM > 1) dtl = fmax(dtl, (fabs(vy) + cs) * (1.0 / P.del[1]));
+      if (NDIM > 2) dtl = fmax(dtl, (fabs(vz) + cs) * (1.0 / P.del[2]));
+      CflCand c; c.key = dtl * P.cfl; c.val = dtl; c.idx = loc;
+      cfl_merge(cand, c);
+    }
+  }
+  if (LAST) cfl_block_reduce<NX, NY, NZ>(cand, b, P.cfl, part);
+  if (st) atomicOr(P.status, st);
+}
+
+}  // namespace fhy

@@ -4,6 +4,9 @@
 //   FHY_VARIANT=2  FP64 with FMA contraction
 //   FHY_VARIANT=3  FP32 reconstruction / Riemann solve, FP64 update
 #include "hy_launch.h"
+#if FHY_VARIANT == 3
+#include "hy_mixed.cuh"
+#endif
 
 #if FHY_VARIANT == 3
 typedef float Real;
@@ -20,17 +23,24 @@ namespace fhy {
 
 template <int NDIM, int NX, int NY, int NZ, int DIR, bool FIRST, bool LAST>
 static bool launch_dir(const StepArgs &a) {
+#if FHY_VARIANT == 3
+  using G = MxGeom<NDIM, NX, NY, NZ, DIR>;
+  auto kern = k_dir_mx<NDIM, NX, NY, NZ, DIR, FIRST, LAST>;
+  const int threads = MxThreads<NDIM, NX, NY, NZ>::n;
+#else
   using G = DirGeom<NDIM, NX, NY, NZ, Real, DIR>;
-  auto kern = k_dir<NDIM, NX, NY, NZ, Real, DIR, FIRST, LAST>;
+  auto kern = k_dir<NDIM, NX, NY, NZ, Real, DIR, FIRST, LAST, FHY_VARIANT>;
+  const int threads = a.threads;
+#endif
   const size_t smem = G::smem_bytes();
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return false;
-  kern<<<a.nlaunch, a.threads, smem, a.stream>>>(a.P, (const Real *)a.sig, a.acc, a.aux, a.ncells, a.part);
+  kern<<<a.nlaunch, threads, smem, a.stream>>>(a.P, (const Real *)a.sig, a.acc, a.aux, a.ncells, a.part);
   return cudaGetLastError() == cudaSuccess;
 }
 
 template <int NDIM, int NX, int NY, int NZ>
 static int run(const StepArgs &a) {
-  k_sig<NDIM, NX, NY, NZ, Real><<<a.nlaunch, a.threads, 0, a.stream>>>(a.P, (Real *)a.sig);
+  k_sig<NDIM, NX, NY, NZ, Real, FHY_VARIANT><<<a.nlaunch, a.threads, 0, a.stream>>>(a.P, (Real *)a.sig);
   if (cudaGetLastError() != cudaSuccess) return -2;
   bool ok;
   if (NDIM == 2) {

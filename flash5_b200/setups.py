@@ -65,6 +65,19 @@ def sod(grid, gamma=1.4, rho_l=1.0, rho_r=0.125, p_l=1.0, p_r=0.1, u_l=0.0, u_r=
     return _fill(grid, unk, rho, u * xcos, u * ycos, u * zcos, p, gamma)
 
 
+def sod_axis(grid, axis=0, gamma=1.4, rho_l=1.0, rho_r=0.125, p_l=1.0, p_r=0.1, posn=0.5):
+    """Planar Sod problem with its interface normal along ``axis`` (the
+    angled form of ``sod`` divides by cos(xangle) and cannot express an
+    interface normal to y or z)."""
+    unk = grid.new_unk()
+    c = grid.cell_centers()[axis]
+    left = c < posn
+    rho = np.where(left, rho_l, rho_r)
+    p = np.where(left, p_l, p_r)
+    z = np.zeros_like(rho)
+    return _fill(grid, unk, rho, z, z, z, p, gamma)
+
+
 def kelvin_helmholtz(grid, gamma=5.0 / 3.0, seed=12345, noise=1e-3):
     """3D (or 2D) Kelvin-Helmholtz shear layer with seeded noise."""
     unk = grid.new_unk()

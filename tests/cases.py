@@ -12,7 +12,7 @@ def make_case(name, **pkw):
         return g, setups.sod(g), abi.default_params(**pkw)
     if name == "sod2d_y":       # interface normal along y
         g = UniformGrid(2, (8, 8), (2, 6), bc="outflow")
-        return g, setups.sod(g, xangle=90.0), abi.default_params(**pkw)
+        return g, setups.sod_axis(g, axis=1), abi.default_params(**pkw)
     if name == "sod2d_rot":     # 45 degree interface, block order Morton
         g = UniformGrid(2, (8, 8), (4, 4), bc="outflow", order="morton")
         return g, setups.sod(g, xangle=45.0), abi.default_params(**pkw)
