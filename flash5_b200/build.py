@@ -23,6 +23,7 @@ UNITS = [
     ("hy_fp64_fma.o", "hy_variant.cu", ["-DFHY_VARIANT=2", "--fmad=true"]),
     ("hy_mixed.o", "hy_variant.cu", ["-DFHY_VARIANT=3", "--fmad=true"]),
     ("flash_hy.o", "flash_hy.cu", ["--fmad=false"]),
+    ("riemann_exact.o", "riemann_exact.cu", ["--fmad=true"]),
 ]
 
 

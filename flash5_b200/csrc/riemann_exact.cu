@@ -1,0 +1,709 @@
+// riemann_exact.cu -- exact ideal-gas Riemann solver with a learned initial
+// guess for the star pressure (no counterpart in FLASH5, whose unsplit path
+// only has approximate solvers, hy_getFaceFlux.F90:324-372).
+//
+// Method: E. F. Toro, "Riemann Solvers and Numerical Methods for Fluid
+// Dynamics", 3rd ed., ch. 4 -- pressure functions f_K(p) (eqs. 4.6-4.7),
+// two-rarefaction guess (eq. 4.46), Newton iteration on
+// f(p) = f_L(p) + f_R(p) + (u_R - u_L) = 0.  Newton is kept inside a bracket
+// [pa, pb] with f(pa) < 0 < f(pb), so every solve terminates within
+// max_iter; steps leaving the bracket are replaced by bisection.
+//
+// The learned guess is an 8-64-64-1 MLP with BF16 weights and activations
+// and FP32 accumulation, evaluated on the tensor cores with warp-level
+// mma.sync (m16n8k16).  It predicts ln(p*/p_TR) from eight scale-free
+// features of the two states; Newton starts from p_TR*exp(y).  If that
+// Newton run does not converge within three iterations, the solve restarts
+// from the two-rarefaction guess (fallback), so the converged p* never
+// depends on the network.
+//
+// Training: hand-written FP32 forward/backward kernels (mean-squared error
+// on ln(p*/p_TR)) and an Adam update, on interface states harvested from
+// the solver's own runs.
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include "../../include/flash_hy.h"
+
+namespace rx {
+
+constexpr int NIN = 8, NH = 64;
+// parameter layout (FP32 master copy): W1[64][8], b1[64], W2[64][64], b2[64], w3[64], b3
+constexpr int OFF_W1 = 0, OFF_B1 = OFF_W1 + NH * NIN, OFF_W2 = OFF_B1 + NH, OFF_B2 = OFF_W2 + NH * NH,
+              OFF_W3 = OFF_B2 + NH, OFF_B3 = OFF_W3 + NH, NPARAM = OFF_B3 + 1;
+
+// ---------------------------------------------------------------------------
+// pressure functions and the star state
+// ---------------------------------------------------------------------------
+struct Side { double d, u, p, c; };
+
+__device__ __forceinline__ void pres_fn(double p, const Side &s, double g, double &f, double &fd) {
+  if (p <= s.p) {
+    double prat = p / s.p;
+    double ex = (g - 1.0) / (2.0 * g);
+    double q = pow(prat, ex);
+    f = 2.0 * s.c / (g - 1.0) * (q - 1.0);
+    fd = q / (prat * s.d * s.c);                  // (p/pK)^(-(g+1)/2g) / (dK cK)
+  } else {
+    double A = 2.0 / ((g + 1.0) * s.d);
+    double B = (g - 1.0) / (g + 1.0) * s.p;
+    double q = sqrt(A / (B + p));
+    f = (p - s.p) * q;
+    fd = (1.0 - 0.5 * (p - s.p) / (B + p)) * q;
+  }
+}
+
+__device__ __forceinline__ double tr_guess(const Side &L, const Side &R, double g) {
+  double z = (g - 1.0) / (2.0 * g);
+  double num = L.c + R.c - 0.5 * (g - 1.0) * (R.u - L.u);
+  if (num <= 0.0) return 0.0;
+  return pow(num / (L.c / pow(L.p, z) + R.c / pow(R.p, z)), 1.0 / z);
+}
+
+// Bracketed Newton from p0.  Returns iterations used (>= 1), or -iterations
+// when it did not converge within max_iter.
+__device__ int newton(const Side &L, const Side &R, double g, double p0, double tol, int max_iter, double &pout) {
+  double du = R.u - L.u;
+  double fl, fdl, fr, fdr;
+  double pa = 0.0, pb = fmax(L.p, R.p);
+  for (int k = 0; k < 200; ++k) {
+    pres_fn(pb, L, g, fl, fdl); pres_fn(pb, R, g, fr, fdr);
+    if (fl + fr + du > 0.0) break;
+    pa = pb;
+    pb *= 4.0;
+  }
+  double p = (p0 > pa && p0 < pb) ? p0 : 0.5 * (pa + pb);
+  for (int it = 0; it < max_iter; ++it) {
+    pres_fn(p, L, g, fl, fdl); pres_fn(p, R, g, fr, fdr);
+    double f = fl + fr + du;
+    if (f < 0.0) pa = p; else pb = p;
+    double pn = p - f / (fdl + fdr);
+    if (!(pn > pa && pn < pb)) pn = 0.5 * (pa + pb);
+    double change = fabs(pn - p) / (0.5 * (pn + p));
+    p = pn;
+    if (change < tol) { pout = p; return it + 1; }
+  }
+  pout = p;
+  return -max_iter;
+}
+
+__device__ __forceinline__ double star_u(const Side &L, const Side &R, double g, double p) {
+  double fl, fdl, fr, fdr;
+  pres_fn(p, L, g, fl, fdl); pres_fn(p, R, g, fr, fdr);
+  return 0.5 * (L.u + R.u) + 0.5 * (fr - fl);
+}
+
+// ---------------------------------------------------------------------------
+// features (scale free, ~O(1)); target = ln(p*/p_TR)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void features(const Side &L, const Side &R, double g, double ptr, float f[NIN]) {
+  const float i4 = 1.0f / 9.2103404f, i3 = 1.0f / 6.9077553f;   // 1/ln(1e4), 1/ln(1e3)
+  f[0] = float(log(R.p / L.p)) * i4;
+  f[1] = float(log(R.d / L.d)) * i3;
+  f[2] = float(L.u / L.c) * 0.2f;
+  f[3] = float(R.u / R.c) * 0.2f;
+  f[4] = float((g - 1.5333333333333333) * 7.5);
+  f[5] = float((R.u - L.u) / (L.c + R.c));
+  f[6] = float(log(ptr / L.p)) * i4;
+  f[7] = float(log(fmax(L.p, R.p) / L.p)) * i4;
+}
+
+// ---------------------------------------------------------------------------
+// tensor-core MLP inference for the 32 interfaces of a warp
+// ---------------------------------------------------------------------------
+struct MlpSmem {
+  __nv_bfloat16 W1[NH][16];      // K padded 8 -> 16
+  __nv_bfloat16 W2[NH][NH];
+  float b1[NH], b2[NH], w3[NH], b3;
+};
+
+__device__ __forceinline__ void mma_bf16(float d[4], const uint32_t a[4], const uint32_t b[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<uint32_t *>(&v);
+}
+
+// xin: this warp's feature rows in shared memory, [32][16] bf16 (cols 8..15
+// zero).  Returns y for row (lane) through yout[32] in shared memory.
+__device__ void mlp_warp(const MlpSmem &M, const __nv_bfloat16 (*xin)[16], float *yout) {
+  const int lane = threadIdx.x & 31, r = lane >> 2, q = lane & 3;
+#pragma unroll
+  for (int tile = 0; tile < 2; ++tile) {
+    const int row0 = tile * 16;
+    // layer 1: [16 x 16] x [16 x 64]
+    uint32_t a[4];
+    a[0] = *reinterpret_cast<const uint32_t *>(&xin[row0 + r][2 * q]);
+    a[1] = *reinterpret_cast<const uint32_t *>(&xin[row0 + r + 8][2 * q]);
+    a[2] = *reinterpret_cast<const uint32_t *>(&xin[row0 + r][2 * q + 8]);
+    a[3] = *reinterpret_cast<const uint32_t *>(&xin[row0 + r + 8][2 * q + 8]);
+    float h1[8][4];
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+      uint32_t bb[2];
+      bb[0] = *reinterpret_cast<const uint32_t *>(&M.W1[nt * 8 + r][2 * q]);
+      bb[1] = *reinterpret_cast<const uint32_t *>(&M.W1[nt * 8 + r][2 * q + 8]);
+      h1[nt][0] = h1[nt][1] = h1[nt][2] = h1[nt][3] = 0.f;
+      mma_bf16(h1[nt], a, bb);
+      // bias + relu; columns of this thread: nt*8 + 2q, +1
+      float c0 = M.b1[nt * 8 + 2 * q], c1 = M.b1[nt * 8 + 2 * q + 1];
+      h1[nt][0] = fmaxf(h1[nt][0] + c0, 0.f); h1[nt][1] = fmaxf(h1[nt][1] + c1, 0.f);
+      h1[nt][2] = fmaxf(h1[nt][2] + c0, 0.f); h1[nt][3] = fmaxf(h1[nt][3] + c1, 0.f);
+    }
+    // layer 2: [16 x 64] x [64 x 64]; the C fragments of layer 1 are the A
+    // fragments of layer 2 (k-step kk = n-tiles 2kk and 2kk+1)
+    float h2[8][4];
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) h2[nt][0] = h2[nt][1] = h2[nt][2] = h2[nt][3] = 0.f;
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk) {
+      uint32_t a2[4];
+      a2[0] = pack_bf16(h1[2 * kk][0], h1[2 * kk][1]);
+      a2[1] = pack_bf16(h1[2 * kk][2], h1[2 * kk][3]);
+      a2[2] = pack_bf16(h1[2 * kk + 1][0], h1[2 * kk + 1][1]);
+      a2[3] = pack_bf16(h1[2 * kk + 1][2], h1[2 * kk + 1][3]);
+#pragma unroll
+      for (int nt = 0; nt < 8; ++nt) {
+        uint32_t bb[2];
+        bb[0] = *reinterpret_cast<const uint32_t *>(&M.W2[nt * 8 + r][kk * 16 + 2 * q]);
+        bb[1] = *reinterpret_cast<const uint32_t *>(&M.W2[nt * 8 + r][kk * 16 + 2 * q + 8]);
+        mma_bf16(h2[nt], a2, bb);
+      }
+    }
+    // layer 3 on the CUDA cores: y = relu(h2 + b2) . w3 + b3
+    float y0 = 0.f, y1 = 0.f;
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+      int c = nt * 8 + 2 * q;
+      float v0 = __bfloat162float(__float2bfloat16(fmaxf(h2[nt][0] + M.b2[c], 0.f)));
+      float v1 = __bfloat162float(__float2bfloat16(fmaxf(h2[nt][1] + M.b2[c + 1], 0.f)));
+      float v2 = __bfloat162float(__float2bfloat16(fmaxf(h2[nt][2] + M.b2[c], 0.f)));
+      float v3 = __bfloat162float(__float2bfloat16(fmaxf(h2[nt][3] + M.b2[c + 1], 0.f)));
+      y0 += v0 * M.w3[c] + v1 * M.w3[c + 1];
+      y1 += v2 * M.w3[c] + v3 * M.w3[c + 1];
+    }
+    y0 += __shfl_xor_sync(0xffffffffu, y0, 1); y0 += __shfl_xor_sync(0xffffffffu, y0, 2);
+    y1 += __shfl_xor_sync(0xffffffffu, y1, 1); y1 += __shfl_xor_sync(0xffffffffu, y1, 2);
+    if (q == 0) { yout[row0 + r] = y0 + M.b3; yout[row0 + r + 8] = y1 + M.b3; }
+  }
+  __syncwarp();
+}
+
+__device__ void load_mlp(MlpSmem &M, const float *__restrict__ w) {
+  for (int t = threadIdx.x; t < NH * 16; t += blockDim.x) {
+    int n = t / 16, k = t % 16;
+    M.W1[n][k] = __float2bfloat16(k < NIN ? w[OFF_W1 + n * NIN + k] : 0.f);
+  }
+  for (int t = threadIdx.x; t < NH * NH; t += blockDim.x) M.W2[t / NH][t % NH] = __float2bfloat16(w[OFF_W2 + t]);
+  for (int t = threadIdx.x; t < NH; t += blockDim.x) {
+    M.b1[t] = w[OFF_B1 + t]; M.b2[t] = w[OFF_B2 + t]; M.w3[t] = w[OFF_W3 + t];
+  }
+  if (threadIdx.x == 0) M.b3 = w[OFF_B3];
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// isolated solves: states[7][n] = (dl, ul, pl, dr, ur, pr, gamma)
+// out[2][n] = (p*, u*); iters[n] = Newton iterations (incl. fallback);
+// flags bit0: fell back to the two-rarefaction guess, bit1: vacuum,
+// bit2: not converged
+// ---------------------------------------------------------------------------
+constexpr int SOLVE_THREADS = 256;
+
+__global__ void __launch_bounds__(SOLVE_THREADS) k_solve(const double *__restrict__ S, long n, double *__restrict__ out,
+                                                         unsigned char *__restrict__ iters, unsigned char *__restrict__ flags,
+                                                         const float *__restrict__ w, int learned, double tol,
+                                                         int max_iter, unsigned *status) {
+  __shared__ MlpSmem M;
+  __shared__ __align__(16) __nv_bfloat16 X[SOLVE_THREADS / 32][32][16];
+  __shared__ float Y[SOLVE_THREADS / 32][32];
+  if (learned) load_mlp(M, w);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long stride = (long)gridDim.x * blockDim.x;
+  unsigned st = 0;
+  // grid-stride loop whose trip count is uniform across a warp
+  for (long base = (long)blockIdx.x * blockDim.x; base < n; base += stride) {
+    const long i = base + threadIdx.x;
+    const bool valid = i < n;
+    Side L, R;
+    double g = 1.4;
+    if (valid) {
+      L.d = S[i]; L.u = S[n + i]; L.p = S[2 * n + i];
+      R.d = S[3 * n + i]; R.u = S[4 * n + i]; R.p = S[5 * n + i];
+      g = S[6 * n + i];
+    } else {
+      L.d = R.d = 1.0; L.u = R.u = 0.0; L.p = R.p = 1.0;
+    }
+    L.c = sqrt(g * L.p / L.d); R.c = sqrt(g * R.p / R.d);
+    const bool vacuum = 2.0 * (L.c + R.c) / (g - 1.0) <= R.u - L.u;
+    double ptr = vacuum ? 0.0 : tr_guess(L, R, g);
+    double p0 = ptr;
+    if (learned) {
+      float f[NIN];
+      if (!vacuum) features(L, R, g, ptr, f);
+      else for (int k = 0; k < NIN; ++k) f[k] = 0.f;
+#pragma unroll
+      for (int k = 0; k < 16; k += 2)
+        *reinterpret_cast<uint32_t *>(&X[warp][lane][k]) = pack_bf16(k < NIN ? f[k] : 0.f, k + 1 < NIN ? f[k + 1] : 0.f);
+      __syncwarp();
+      mlp_warp(M, X[warp], Y[warp]);
+      float y = fminf(fmaxf(Y[warp][lane], -20.f), 20.f);
+      p0 = ptr * exp((double)y);
+    }
+    unsigned char fl = 0;
+    int its = 0;
+    double ps = 0.0, us = 0.5 * (L.u + R.u);
+    if (vacuum) {
+      fl |= 2;
+    } else if (learned) {
+      int k = newton(L, R, g, p0, tol, 3, ps);
+      if (k > 0) {
+        its = k;
+      } else {             // judge: restart from the two-rarefaction guess
+        its = 3;
+        fl |= 1;
+        int k2 = newton(L, R, g, ptr, tol, max_iter, ps);
+        if (k2 > 0) its += k2;
+        else { its += max_iter; fl |= 4; st |= FLASH_HY_ERR_NEWTON_NOCONV; }
+      }
+    } else {
+      int k = newton(L, R, g, ptr, tol, max_iter, ps);
+      if (k > 0) its = k;
+      else { its = max_iter; fl |= 4; st |= FLASH_HY_ERR_NEWTON_NOCONV; }
+    }
+    if (!vacuum) us = star_u(L, R, g, ps);
+    if (valid) {
+      out[i] = ps; out[n + i] = us;
+      if (iters) iters[i] = (unsigned char)(its > 255 ? 255 : its);
+      if (flags) flags[i] = fl;
+    }
+  }
+  if (st) atomicOr(status, st);
+}
+
+// network output y = MLP(features) for every interface (0 for vacuum cases)
+__global__ void __launch_bounds__(SOLVE_THREADS) k_predict(const double *__restrict__ S, long n, float *__restrict__ y,
+                                                           const float *__restrict__ w) {
+  __shared__ MlpSmem M;
+  __shared__ __align__(16) __nv_bfloat16 X[SOLVE_THREADS / 32][32][16];
+  __shared__ float Y[SOLVE_THREADS / 32][32];
+  load_mlp(M, w);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (long base = (long)blockIdx.x * blockDim.x; base < n; base += (long)gridDim.x * blockDim.x) {
+    const long i = base + threadIdx.x;
+    float f[NIN];
+    for (int k = 0; k < NIN; ++k) f[k] = 0.f;
+    bool vac = true;
+    if (i < n) {
+      Side L{S[i], S[n + i], S[2 * n + i], 0.}, R{S[3 * n + i], S[4 * n + i], S[5 * n + i], 0.};
+      double g = S[6 * n + i];
+      L.c = sqrt(g * L.p / L.d); R.c = sqrt(g * R.p / R.d);
+      vac = 2.0 * (L.c + R.c) / (g - 1.0) <= R.u - L.u;
+      if (!vac) features(L, R, g, tr_guess(L, R, g), f);
+    }
+#pragma unroll
+    for (int k = 0; k < 16; k += 2)
+      *reinterpret_cast<uint32_t *>(&X[warp][lane][k]) = pack_bf16(k < NIN ? f[k] : 0.f, k + 1 < NIN ? f[k + 1] : 0.f);
+    __syncwarp();
+    mlp_warp(M, X[warp], Y[warp]);
+    if (i < n) y[i] = vac ? 0.f : Y[warp][lane];
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// config-4 input generator: splitmix64 of (seed, index, stream)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+__device__ __forceinline__ double uni(uint64_t seed, long i, int k) {
+  uint64_t h = splitmix64(seed ^ splitmix64((uint64_t)i * 8 + (uint64_t)k));
+  return (double)(h >> 11) * (1.0 / 9007199254740992.0);     // [0, 1)
+}
+
+__global__ void k_generate(uint64_t seed, long n, double *S) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    double g = uni(seed, i, 0) < 0.5 ? 1.4 : 5.0 / 3.0;
+    double pr = exp(log(1e-4) + uni(seed, i, 1) * (log(1e4) - log(1e-4)));     // pR/pL log-uniform
+    double dr = exp(log(1e-3) + uni(seed, i, 2) * (log(1e3) - log(1e-3)));     // rhoR/rhoL log-uniform
+    double cl = sqrt(g), cr = sqrt(g * pr / dr);
+    double ul = (2.0 * uni(seed, i, 3) - 1.0) * 5.0 * cl;
+    double ur = (2.0 * uni(seed, i, 4) - 1.0) * 5.0 * cr;
+    S[i] = 1.0; S[n + i] = ul; S[2 * n + i] = 1.0;
+    S[3 * n + i] = dr; S[4 * n + i] = ur; S[5 * n + i] = pr; S[6 * n + i] = g;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// training set: features and targets ln(p*/p_TR) of non-vacuum solves
+// ---------------------------------------------------------------------------
+__global__ void k_make_samples(const double *S, const double *out, long n, float *X, float *T, int *count, long cap) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    Side L{S[i], S[n + i], S[2 * n + i], 0.}, R{S[3 * n + i], S[4 * n + i], S[5 * n + i], 0.};
+    double g = S[6 * n + i];
+    L.c = sqrt(g * L.p / L.d); R.c = sqrt(g * R.p / R.d);
+    if (2.0 * (L.c + R.c) / (g - 1.0) <= R.u - L.u) continue;
+    double ps = out[i];
+    if (!(ps > 0.0)) continue;
+    double ptr = tr_guess(L, R, g);
+    int k = atomicAdd(count, 1);
+    if (k >= cap) continue;
+    float f[NIN];
+    features(L, R, g, ptr, f);
+    for (int q = 0; q < NIN; ++q) X[(long)k * NIN + q] = f[q];
+    T[k] = float(log(ps / ptr));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FP32 forward/backward of one minibatch (MSE, mean over the batch); each
+// CTA handles TS samples and adds its gradient into G (atomics)
+// ---------------------------------------------------------------------------
+constexpr int TS = 32, TRAIN_THREADS = 256;
+
+__global__ void __launch_bounds__(TRAIN_THREADS) k_grad(const float *__restrict__ w, const float *__restrict__ X,
+                                                        const float *__restrict__ T, const int *__restrict__ idx, int nb,
+                                                        float inv_batch, float *__restrict__ G, float *__restrict__ loss) {
+  __shared__ float sW1[NH * NIN], sB1[NH], sW2[NH * NH], sB2[NH], sW3[NH];
+  __shared__ float sX[TS][NIN], sH1[TS][NH + 1], sH2[TS][NH + 1], sD[TS];
+  __shared__ float gW1[NH * NIN], gB1[NH], gW3[NH], gB2[NH];
+  const int tid = threadIdx.x;
+  for (int t = tid; t < NH * NIN; t += TRAIN_THREADS) { sW1[t] = w[OFF_W1 + t]; gW1[t] = 0.f; }
+  for (int t = tid; t < NH * NH; t += TRAIN_THREADS) sW2[t] = w[OFF_W2 + t];
+  for (int t = tid; t < NH; t += TRAIN_THREADS) {
+    sB1[t] = w[OFF_B1 + t]; sB2[t] = w[OFF_B2 + t]; sW3[t] = w[OFF_W3 + t];
+    gB1[t] = 0.f; gW3[t] = 0.f; gB2[t] = 0.f;
+  }
+  const float b3 = w[OFF_B3];
+  const int s0 = blockIdx.x * TS;
+  const int ns = min(TS, nb - s0);
+  for (int t = tid; t < TS * NIN; t += TRAIN_THREADS) {
+    int s = t / NIN, k = t % NIN;
+    sX[s][k] = s < ns ? X[(long)idx[s0 + s] * NIN + k] : 0.f;
+  }
+  __syncthreads();
+  // forward
+  for (int t = tid; t < TS * NH; t += TRAIN_THREADS) {
+    int s = t / NH, u = t % NH;
+    float a = sB1[u];
+#pragma unroll
+    for (int k = 0; k < NIN; ++k) a += sW1[u * NIN + k] * sX[s][k];
+    sH1[s][u] = fmaxf(a, 0.f);
+  }
+  __syncthreads();
+  for (int t = tid; t < TS * NH; t += TRAIN_THREADS) {
+    int s = t / NH, u = t % NH;
+    float a = sB2[u];
+    for (int j = 0; j < NH; ++j) a += sW2[u * NH + j] * sH1[s][j];
+    sH2[s][u] = fmaxf(a, 0.f);
+  }
+  __syncthreads();
+  // output and dL/dy per sample (one warp per group of samples)
+  float lsum = 0.f;
+  for (int s = tid >> 5; s < TS; s += TRAIN_THREADS / 32) {
+    float a = 0.f;
+    for (int u = tid & 31; u < NH; u += 32) a += sW3[u] * sH2[s][u];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if ((tid & 31) == 0) {
+      float y = a + b3;
+      float r = s < ns ? y - T[idx[s0 + s]] : 0.f;
+      sD[s] = 2.f * r * inv_batch;
+      lsum += r * r;
+    }
+  }
+  __syncthreads();
+  // dH2 (in place over sH2 after using it for dW3)
+  for (int u = tid; u < NH; u += TRAIN_THREADS) {
+    float gw = 0.f;
+    for (int s = 0; s < TS; ++s) gw += sD[s] * sH2[s][u];
+    gW3[u] = gw;
+  }
+  __syncthreads();
+  for (int t = tid; t < TS * NH; t += TRAIN_THREADS) {
+    int s = t / NH, u = t % NH;
+    sH2[s][u] = sH2[s][u] > 0.f ? sD[s] * sW3[u] : 0.f;
+  }
+  __syncthreads();
+  // dW2[u][j] = sum_s dH2[s][u] H1[s][j], db2
+  for (int t = tid; t < NH * NH; t += TRAIN_THREADS) {
+    int u = t / NH, j = t % NH;
+    float a = 0.f;
+    for (int s = 0; s < TS; ++s) a += sH2[s][u] * sH1[s][j];
+    atomicAdd(&G[OFF_W2 + t], a);
+  }
+  for (int u = tid; u < NH; u += TRAIN_THREADS) {
+    float a = 0.f;
+    for (int s = 0; s < TS; ++s) a += sH2[s][u];
+    gB2[u] = a;
+  }
+  // dH1 = (dH2 W2) relu'(H1), written into a register pass then sH1
+  __syncthreads();
+  float dh1[TS * NH / TRAIN_THREADS];
+#pragma unroll
+  for (int q = 0; q < TS * NH / TRAIN_THREADS; ++q) {
+    int t = tid + q * TRAIN_THREADS;
+    int s = t / NH, j = t % NH;
+    float a = 0.f;
+    for (int u = 0; u < NH; ++u) a += sH2[s][u] * sW2[u * NH + j];
+    dh1[q] = sH1[s][j] > 0.f ? a : 0.f;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < TS * NH / TRAIN_THREADS; ++q) {
+    int t = tid + q * TRAIN_THREADS;
+    sH1[t / NH][t % NH] = dh1[q];
+  }
+  __syncthreads();
+  for (int t = tid; t < NH * NIN; t += TRAIN_THREADS) {
+    int j = t / NIN, k = t % NIN;
+    float a = 0.f;
+    for (int s = 0; s < TS; ++s) a += sH1[s][j] * sX[s][k];
+    gW1[t] = a;
+  }
+  for (int j = tid; j < NH; j += TRAIN_THREADS) {
+    float a = 0.f;
+    for (int s = 0; s < TS; ++s) a += sH1[s][j];
+    gB1[j] = a;
+  }
+  __syncthreads();
+  for (int t = tid; t < NH * NIN; t += TRAIN_THREADS) atomicAdd(&G[OFF_W1 + t], gW1[t]);
+  for (int t = tid; t < NH; t += TRAIN_THREADS) {
+    atomicAdd(&G[OFF_B1 + t], gB1[t]);
+    atomicAdd(&G[OFF_B2 + t], gB2[t]);
+    atomicAdd(&G[OFF_W3 + t], gW3[t]);
+  }
+  if (tid == 0) {
+    float a = 0.f;
+    for (int s = 0; s < TS; ++s) a += sD[s];
+    atomicAdd(&G[OFF_B3], a);
+  }
+  // loss (sum of squared residuals of this CTA)
+  if ((tid & 31) == 0) atomicAdd(loss, lsum);
+}
+
+__global__ void k_adam(float *w, float *m, float *v, const float *G, int step, float lr, float b1, float b2, float eps) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= NPARAM) return;
+  float g = G[t];
+  m[t] = b1 * m[t] + (1.f - b1) * g;
+  v[t] = b2 * v[t] + (1.f - b2) * g * g;
+  float mh = m[t] / (1.f - powf(b1, (float)step));
+  float vh = v[t] / (1.f - powf(b2, (float)step));
+  w[t] -= lr * mh / (sqrtf(vh) + eps);
+}
+
+__global__ void k_shuffle_idx(int *idx, int n, uint64_t seed) {
+  // one random key per sample, then the host sorts nothing: a multiplicative
+  // permutation (a*i + c) mod n with a coprime to n visits every sample once
+  long a = 1 + 2 * (long)(splitmix64(seed) % (uint64_t)(n > 2 ? n / 2 : 1));
+  while (true) {
+    long x = a, y = n, t;
+    while (y) { t = x % y; x = y; y = t; }
+    if (x == 1) break;
+    a += 2;
+  }
+  long c = (long)(splitmix64(seed + 1) % (uint64_t)n);
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    idx[i] = (int)((a * i + c) % n);
+}
+
+}  // namespace rx
+
+using namespace rx;
+
+struct flash_hy_rsolver {
+  int device;
+  cudaStream_t stream;
+  float *w, *m, *v, *G, *loss;
+  unsigned *status;
+  int step;
+  char err[256];
+};
+
+#define RS_CUDA(call)                                                                    \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess) { snprintf(r->err, sizeof r->err, "CUDA: %s", cudaGetErrorString(e_)); return FLASH_HY_ERR_CUDA; } \
+  } while (0)
+
+static int grid_for(long n, int threads) {
+  long g = (n + threads - 1) / threads;
+  if (g > 148L * 16) g = 148L * 16;
+  return (int)(g > 0 ? g : 1);
+}
+
+extern "C" int flash_hy_rsolver_create(int device, flash_hy_rsolver **out) {
+  if (!out) return FLASH_HY_ERR_BAD_ARG;
+  flash_hy_rsolver *r = (flash_hy_rsolver *)calloc(1, sizeof *r);
+  *out = r;
+  r->device = device;
+  RS_CUDA(cudaSetDevice(device));
+  RS_CUDA(cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking));
+  RS_CUDA(cudaMalloc(&r->w, NPARAM * sizeof(float)));
+  RS_CUDA(cudaMalloc(&r->m, NPARAM * sizeof(float)));
+  RS_CUDA(cudaMalloc(&r->v, NPARAM * sizeof(float)));
+  RS_CUDA(cudaMalloc(&r->G, NPARAM * sizeof(float)));
+  RS_CUDA(cudaMalloc(&r->loss, sizeof(float)));
+  RS_CUDA(cudaMalloc(&r->status, sizeof(unsigned)));
+  RS_CUDA(cudaMemset(r->m, 0, NPARAM * sizeof(float)));
+  RS_CUDA(cudaMemset(r->v, 0, NPARAM * sizeof(float)));
+  RS_CUDA(cudaMemset(r->status, 0, sizeof(unsigned)));
+  // He-style initialisation from a fixed seed (host side, deterministic)
+  float *h = (float *)malloc(NPARAM * sizeof(float));
+  uint64_t s = 12345;
+  auto rnd = [&]() { s = s * 6364136223846793005ull + 1442695040888963407ull; return ((s >> 11) * (1.0 / 9007199254740992.0)) * 2.0 - 1.0; };
+  for (int t = 0; t < NPARAM; ++t) h[t] = 0.f;
+  for (int t = 0; t < NH * NIN; ++t) h[OFF_W1 + t] = (float)(rnd() * sqrt(6.0 / NIN));
+  for (int t = 0; t < NH * NH; ++t) h[OFF_W2 + t] = (float)(rnd() * sqrt(6.0 / NH));
+  for (int t = 0; t < NH; ++t) h[OFF_W3 + t] = (float)(rnd() * sqrt(3.0 / NH) * 0.1);
+  cudaError_t e = cudaMemcpy(r->w, h, NPARAM * sizeof(float), cudaMemcpyHostToDevice);
+  free(h);
+  if (e != cudaSuccess) return FLASH_HY_ERR_CUDA;
+  return 0;
+}
+
+extern "C" int flash_hy_rsolver_destroy(flash_hy_rsolver *r) {
+  if (!r) return FLASH_HY_ERR_BAD_ARG;
+  cudaSetDevice(r->device);
+  if (r->stream) cudaStreamSynchronize(r->stream);
+  cudaFree(r->w); cudaFree(r->m); cudaFree(r->v); cudaFree(r->G); cudaFree(r->loss); cudaFree(r->status);
+  if (r->stream) cudaStreamDestroy(r->stream);
+  free(r);
+  return 0;
+}
+
+extern "C" void *flash_hy_rsolver_stream(flash_hy_rsolver *r) { return r ? (void *)r->stream : nullptr; }
+
+extern "C" int flash_hy_rsolver_generate(flash_hy_rsolver *r, unsigned long long seed, long n, double *d_states) {
+  if (!r || !d_states || n <= 0) return FLASH_HY_ERR_BAD_ARG;
+  RS_CUDA(cudaSetDevice(r->device));
+  k_generate<<<grid_for(n, 256), 256, 0, r->stream>>>(seed, n, d_states);
+  RS_CUDA(cudaGetLastError());
+  return 0;
+}
+
+extern "C" int flash_hy_rsolver_solve(flash_hy_rsolver *r, const double *d_states, long n, double *d_star,
+                                      unsigned char *d_iters, unsigned char *d_flags, int learned, double tol,
+                                      int max_iter) {
+  if (!r || !d_states || !d_star || n <= 0 || max_iter <= 0 || max_iter > 200) return FLASH_HY_ERR_BAD_ARG;
+  RS_CUDA(cudaSetDevice(r->device));
+  k_solve<<<grid_for(n, SOLVE_THREADS), SOLVE_THREADS, 0, r->stream>>>(d_states, n, d_star, d_iters, d_flags, r->w,
+                                                                      learned, tol, max_iter, r->status);
+  RS_CUDA(cudaGetLastError());
+  return 0;
+}
+
+extern "C" int flash_hy_rsolver_predict(flash_hy_rsolver *r, const double *d_states, long n, float *d_y) {
+  if (!r || !d_states || !d_y || n <= 0) return FLASH_HY_ERR_BAD_ARG;
+  RS_CUDA(cudaSetDevice(r->device));
+  k_predict<<<grid_for(n, SOLVE_THREADS), SOLVE_THREADS, 0, r->stream>>>(d_states, n, d_y, r->w);
+  RS_CUDA(cudaGetLastError());
+  return 0;
+}
+
+extern "C" int flash_hy_rsolver_make_samples(flash_hy_rsolver *r, const double *d_states, const double *d_star, long n,
+                                             float *d_x, float *d_t, long cap, long *count_out) {
+  if (!r || !d_states || !d_star || !d_x || !d_t || !count_out) return FLASH_HY_ERR_BAD_ARG;
+  RS_CUDA(cudaSetDevice(r->device));
+  int *cnt;
+  RS_CUDA(cudaMalloc(&cnt, sizeof(int)));
+  RS_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int), r->stream));
+  k_make_samples<<<grid_for(n, 256), 256, 0, r->stream>>>(d_states, d_star, n, d_x, d_t, cnt, cap);
+  int h = 0;
+  RS_CUDA(cudaMemcpyAsync(&h, cnt, sizeof(int), cudaMemcpyDeviceToHost, r->stream));
+  RS_CUDA(cudaStreamSynchronize(r->stream));
+  cudaFree(cnt);
+  *count_out = h < cap ? h : cap;
+  return 0;
+}
+
+// Gradient of the mean-squared loss on samples idx[0..nb) (device arrays);
+// writes the FP32 gradient (NPARAM floats) and the loss to host memory.
+extern "C" int flash_hy_rsolver_grad(flash_hy_rsolver *r, const float *d_x, const float *d_t, const int *d_idx, int nb,
+                                     float *h_grad, float *h_loss) {
+  if (!r || !d_x || !d_t || !d_idx || nb <= 0) return FLASH_HY_ERR_BAD_ARG;
+  RS_CUDA(cudaSetDevice(r->device));
+  RS_CUDA(cudaMemsetAsync(r->G, 0, NPARAM * sizeof(float), r->stream));
+  RS_CUDA(cudaMemsetAsync(r->loss, 0, sizeof(float), r->stream));
+  k_grad<<<(nb + TS - 1) / TS, TRAIN_THREADS, 0, r->stream>>>(r->w, d_x, d_t, d_idx, nb, 1.f / nb, r->G, r->loss);
+  RS_CUDA(cudaGetLastError());
+  if (h_grad) RS_CUDA(cudaMemcpyAsync(h_grad, r->G, NPARAM * sizeof(float), cudaMemcpyDeviceToHost, r->stream));
+  if (h_loss) RS_CUDA(cudaMemcpyAsync(h_loss, r->loss, sizeof(float), cudaMemcpyDeviceToHost, r->stream));
+  RS_CUDA(cudaStreamSynchronize(r->stream));
+  if (h_loss) *h_loss /= nb;
+  return 0;
+}
+
+// Adam training over ns samples (device arrays from make_samples): epochs x
+// minibatches of `batch`; returns the mean loss of the last epoch.
+extern "C" int flash_hy_rsolver_train(flash_hy_rsolver *r, const float *d_x, const float *d_t, long ns, int epochs,
+                                      int batch, float lr, float *loss_out) {
+  if (!r || !d_x || !d_t || ns < batch || batch <= 0 || epochs <= 0) return FLASH_HY_ERR_BAD_ARG;
+  RS_CUDA(cudaSetDevice(r->device));
+  int *idx;
+  RS_CUDA(cudaMalloc(&idx, ns * sizeof(int)));
+  float last = 0.f;
+  long nbat = ns / batch;
+  for (int ep = 0; ep < epochs; ++ep) {
+    k_shuffle_idx<<<grid_for(ns, 256), 256, 0, r->stream>>>(idx, (int)ns, 0x5eedull + ep);
+    RS_CUDA(cudaMemsetAsync(r->loss, 0, sizeof(float), r->stream));
+    for (long bi = 0; bi < nbat; ++bi) {
+      RS_CUDA(cudaMemsetAsync(r->G, 0, NPARAM * sizeof(float), r->stream));
+      k_grad<<<(batch + TS - 1) / TS, TRAIN_THREADS, 0, r->stream>>>(r->w, d_x, d_t, idx + bi * batch, batch,
+                                                                      1.f / batch, r->G, r->loss);
+      r->step++;
+      k_adam<<<(NPARAM + 255) / 256, 256, 0, r->stream>>>(r->w, r->m, r->v, r->G, r->step, lr, 0.9f, 0.999f, 1e-8f);
+    }
+    float h = 0.f;
+    RS_CUDA(cudaMemcpyAsync(&h, r->loss, sizeof(float), cudaMemcpyDeviceToHost, r->stream));
+    RS_CUDA(cudaStreamSynchronize(r->stream));
+    last = h / (float)(nbat * batch);
+  }
+  cudaFree(idx);
+  RS_CUDA(cudaGetLastError());
+  if (loss_out) *loss_out = last;
+  return 0;
+}
+
+extern "C" int flash_hy_rsolver_get_weights(flash_hy_rsolver *r, float *h_w, int n) {
+  if (!r || !h_w || n < NPARAM) return FLASH_HY_ERR_BAD_ARG;
+  RS_CUDA(cudaSetDevice(r->device));
+  RS_CUDA(cudaMemcpy(h_w, r->w, NPARAM * sizeof(float), cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+extern "C" int flash_hy_rsolver_set_weights(flash_hy_rsolver *r, const float *h_w, int n) {
+  if (!r || !h_w || n < NPARAM) return FLASH_HY_ERR_BAD_ARG;
+  RS_CUDA(cudaSetDevice(r->device));
+  RS_CUDA(cudaMemcpy(r->w, h_w, NPARAM * sizeof(float), cudaMemcpyHostToDevice));
+  RS_CUDA(cudaMemset(r->m, 0, NPARAM * sizeof(float)));
+  RS_CUDA(cudaMemset(r->v, 0, NPARAM * sizeof(float)));
+  r->step = 0;
+  return 0;
+}
+
+extern "C" int flash_hy_rsolver_num_params(void) { return NPARAM; }
+
+extern "C" int flash_hy_rsolver_sync(flash_hy_rsolver *r) {
+  if (!r) return FLASH_HY_ERR_BAD_ARG;
+  unsigned h = 0;
+  RS_CUDA(cudaSetDevice(r->device));
+  RS_CUDA(cudaMemcpyAsync(&h, r->status, sizeof(unsigned), cudaMemcpyDeviceToHost, r->stream));
+  RS_CUDA(cudaMemsetAsync(r->status, 0, sizeof(unsigned), r->stream));
+  RS_CUDA(cudaStreamSynchronize(r->stream));
+  return (int)h;
+}

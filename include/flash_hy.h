@@ -158,6 +158,34 @@ int flash_hy_last_error(flash_hy_ctx *ctx, char *buf, int len);
 /* Number of kernel launches issued by the last flash_hy_step call. */
 int flash_hy_last_launch_count(flash_hy_ctx *ctx);
 
+/* ---- exact Riemann solver with a learned star-pressure guess ----------
+ * No counterpart in FLASH5 (its unsplit solvers are approximate:
+ * source/physics/Hydro/HydroMain/unsplit/hy_getFaceFlux.F90:324-372); the
+ * hydro step uses it when riemann_solver = FLASH_HY_RS_EXACT.  Arrays are
+ * DEVICE pointers.  states = SoA [7][n] of (rho_L, u_L, p_L, rho_R, u_R,
+ * p_R, gamma) with u the face-normal velocity; star = SoA [2][n] (p*, u*);
+ * iters[n] = Newton iterations (fallback included); flags[n]: bit 0 fell
+ * back to the two-rarefaction guess, bit 1 vacuum, bit 2 not converged.  */
+typedef struct flash_hy_rsolver flash_hy_rsolver;
+int flash_hy_rsolver_create(int device, flash_hy_rsolver **out);
+int flash_hy_rsolver_destroy(flash_hy_rsolver *r);
+void *flash_hy_rsolver_stream(flash_hy_rsolver *r);
+int flash_hy_rsolver_generate(flash_hy_rsolver *r, unsigned long long seed, long n, double *d_states);
+int flash_hy_rsolver_solve(flash_hy_rsolver *r, const double *d_states, long n, double *d_star,
+                           unsigned char *d_iters, unsigned char *d_flags, int learned, double tol, int max_iter);
+/* network output: the estimate of ln(pstar / p_TR) per interface (d_y[n] floats) */
+int flash_hy_rsolver_predict(flash_hy_rsolver *r, const double *d_states, long n, float *d_y);
+int flash_hy_rsolver_make_samples(flash_hy_rsolver *r, const double *d_states, const double *d_star, long n,
+                                  float *d_x, float *d_t, long cap, long *count_out);
+int flash_hy_rsolver_grad(flash_hy_rsolver *r, const float *d_x, const float *d_t, const int *d_idx, int nb,
+                          float *h_grad, float *h_loss);
+int flash_hy_rsolver_train(flash_hy_rsolver *r, const float *d_x, const float *d_t, long ns, int epochs, int batch,
+                           float lr, float *loss_out);
+int flash_hy_rsolver_get_weights(flash_hy_rsolver *r, float *h_w, int n);
+int flash_hy_rsolver_set_weights(flash_hy_rsolver *r, const float *h_w, int n);
+int flash_hy_rsolver_num_params(void);
+int flash_hy_rsolver_sync(flash_hy_rsolver *r);
+
 #ifdef __cplusplus
 }
 #endif

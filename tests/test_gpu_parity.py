@@ -78,19 +78,33 @@ def test_fp64_bitwise_options(case, opts):
         assert dtg == dto and tuple(locg) == tuple(loco)
 
 
+def momentum_normalised_l1(out, ref, grid):
+    """sfocu L1 per conserved variable; a momentum component whose own L1
+    norm is below 1e-3 of the total momentum norm (e.g. rho*w of a 2D-like
+    flow) is normalised by the total momentum norm instead of its own."""
+    ca = sfocu.conserved(grid.interior(out), VAR)
+    cb = sfocu.conserved(grid.interior(ref), VAR)
+    mom = sum(np.abs(cb[k]).sum() for k in ("xmom", "ymom", "zmom"))
+    res = {}
+    for k in sfocu.CONSERVED:
+        den = np.abs(cb[k]).sum()
+        if k != "dens" and k != "ener":
+            den = max(den, 1e-3 * mom)
+        res[k] = float(np.abs(ca[k] - cb[k]).sum() / den)
+    return res
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("case", ["sod2d_rot", "kh2d_16", "kh3d"])
 def test_fp64_fma_close(case):
     grid, ref, out, _ = run_pair(case, precision=abi.PREC_FP64_FMA)
-    for k, (l1, mag) in sfocu.compare(out, ref, grid).items():
-        assert l1 <= 1e-12, (k, l1, mag)
+    for k, l1 in momentum_normalised_l1(out, ref, grid).items():
+        assert l1 <= 1e-12, (k, l1)
 
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("case", ["sod2d_rot", "kh2d_16", "quad2d_16", "kh3d", "sod3d_rot"])
 def test_mixed_close(case):
     grid, ref, out, _ = run_pair(case, precision=abi.PREC_MIXED)
-    for k, (l1, mag) in sfocu.compare(out, ref, grid).items():
-        if k == "zmom" and grid.ndim == 2:
-            continue
-        assert l1 <= 1e-6, (k, l1, mag)
+    for k, l1 in momentum_normalised_l1(out, ref, grid).items():
+        assert l1 <= 1e-6, (k, l1)
