@@ -243,6 +243,64 @@ def conserved_l1(a, b, var):
     return {k: sfocu.l1_rel(ca[k], cb[k]) for k in sfocu.CONSERVED}
 
 
+def riemann_workload(args):
+    """Isolated exact Riemann solves (1e8 interface pairs): two-rarefaction
+    guess vs the learned guess trained on solver-harvested states."""
+    import torch
+    from flash5_b200.riemann import ExactRiemann
+    torch.cuda.set_device(0)
+    n = args.riemann_n
+    r = ExactRiemann(0)
+    stream = r.stream
+    # training set harvested from the solver's own solves of another seed
+    Str = r.generate(1, 2_000_000)
+    otr, _, _ = r.solve(Str, learned=False)
+    X, T, ns = r.make_samples(Str, otr)
+    t0 = time.perf_counter()
+    loss = r.train(X, T, ns, epochs=8, batch=4096, lr=2e-3)
+    train_s = time.perf_counter() - t0
+    del Str, otr, X, T
+    S = r.generate(20251203, n)
+    out = r.empty(2, n)
+    its = r.empty(n, dtype=torch.uint8)
+    flg = r.empty(n, dtype=torch.uint8)
+    res = {}
+    for learned in (False, True):
+        for _ in range(max(1, args.warmup)):
+            r.solve(S, learned, out=out, iters=its, flags=flg)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            r.solve(S, learned, out=out, iters=its, flags=flg)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        it = its.cpu().numpy()
+        fl = flg.cpu().numpy()
+        ok = (fl & 2) == 0
+        hist = np.bincount(it[ok], minlength=12)[:12].tolist()
+        res["learned" if learned else "two_rarefaction"] = {
+            "solves_per_s": n / (ms * 1e-3), "ms": ms, "mean_iters": float(it[ok].mean()), "iter_hist": hist,
+            "fallback_frac": float(((fl & 1) != 0)[ok].mean()), "nonconverged": int(((fl & 4) != 0).sum()),
+            "vacuum": int((~ok).sum()), "pstar": out[0].clone()}
+    p0, p1 = res["two_rarefaction"].pop("pstar"), res["learned"].pop("pstar")
+    okd = torch.tensor(ok, device=p0.device)
+    rel = ((p1 - p0).abs() / p0.clamp_min(1e-300))[okd].max().item()
+    line = {"metric": "exact Riemann star-pressure solves/s (Newton to 1e-12, FP64)", "value": res["learned"]["solves_per_s"],
+            "unit": "solves/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["learned"]["ms"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64 Newton, bf16 MLP (f32 acc)",
+            "data": "synthetic (splitmix64 seed 20251203)",
+            "config": {"workload": f"{n:.0e} isolated interface pairs: p ratio log-uniform 1e-4..1e4, rho ratio 1e-3..1e3, "
+                                   "u uniform +-5 c, gamma in {1.4, 5/3}; MLP 8-64-64-1 BF16 on tensor cores (mma.sync)"},
+            "paths": res, "speedup_vs_two_rarefaction": res["two_rarefaction"]["ms"] / res["learned"]["ms"],
+            "max_rel_pstar_diff_learned_vs_tr": rel, "training": {"samples": ns, "epochs": 8, "final_mse": loss,
+                                                                  "seconds": train_s}}
+    print(json.dumps(line))
+    r.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -252,6 +310,8 @@ def main():
     ap.add_argument("--nblk", type=int, default=32, help="blocks per axis (32 -> 256^3)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="kh", choices=["kh", "riemann"])
+    ap.add_argument("--riemann-n", type=int, default=100_000_000)
     ap.add_argument("--paths", default="fp64,fp64_fma,mixed",
                     help="comma list of paths to time; profiling runs use one")
     args = ap.parse_args()
@@ -260,6 +320,11 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     warmup = max(3, args.warmup)
+    if args.workload == "riemann" and args.impl == "ours":
+        if rank != 0:
+            return 0
+        args.warmup = warmup
+        return riemann_workload(args)
 
     if args.impl == "reference":
         if rank != 0:
