@@ -13,7 +13,7 @@
 // and FP32 accumulation, evaluated on the tensor cores with warp-level
 // mma.sync (m16n8k16).  It predicts ln(p*/p_TR) from eight scale-free
 // features of the two states; Newton starts from p_TR*exp(y).  If that
-// Newton run does not converge within three iterations, the solve restarts
+// Newton run does not converge within three evaluations, the solve restarts
 // from the two-rarefaction guess (fallback), so the converged p* never
 // depends on the network.
 //
@@ -64,8 +64,11 @@ __device__ __forceinline__ double tr_guess(const Side &L, const Side &R, double 
   return pow(num / (L.c / pow(L.p, z) + R.c / pow(R.p, z)), 1.0 / z);
 }
 
-// Bracketed Newton from p0.  Returns iterations used (>= 1), or -iterations
-// when it did not converge within max_iter.
+// Bracketed Newton from p0.  Converged when the Newton step is below
+// tol * p or, in the quadratic regime, when the predicted next step is below
+// tol * p / 100; the returned count is the number of function evaluations.  Steps
+// leaving [pa, pb] are replaced by a geometric (pa > 0) or decimating
+// (pa = 0, near vacuum) bisection.  Returns -max_iter when not converged.
 __device__ int newton(const Side &L, const Side &R, double g, double p0, double tol, int max_iter, double &pout) {
   double du = R.u - L.u;
   double fl, fdl, fr, fdr;
@@ -76,16 +79,27 @@ __device__ int newton(const Side &L, const Side &R, double g, double p0, double 
     pa = pb;
     pb *= 4.0;
   }
-  double p = (p0 > pa && p0 < pb) ? p0 : 0.5 * (pa + pb);
+  double p = (p0 > pa && p0 < pb) ? p0 : (pa > 0.0 ? sqrt(pa * pb) : 0.5 * pb);
+  double prev = -1.0;                 // previous Newton step (-1: none / bisection)
   for (int it = 0; it < max_iter; ++it) {
     pres_fn(p, L, g, fl, fdl); pres_fn(p, R, g, fr, fdr);
     double f = fl + fr + du;
+    if (f == 0.0) { pout = p; return it + 1; }
     if (f < 0.0) pa = p; else pb = p;
-    double pn = p - f / (fdl + fdr);
-    if (!(pn > pa && pn < pb)) pn = 0.5 * (pa + pb);
-    double change = fabs(pn - p) / (0.5 * (pn + p));
+    double step = f / (fdl + fdr);
+    double pn = p - step;
+    double as = fabs(step);
+    bool inside = pn > pa && pn < pb;
+    // converged: the step itself is below tol, or -- once the last two
+    // steps show the quadratic regime -- the predicted next step
+    // |step|^3 / prev^2 is below tol/100
+    if (as <= tol * p || (inside && prev > 0.0 && as < prev && as * (as / prev) * (as / prev) <= 0.01 * tol * p)) {
+      pout = (pn > 0.0) ? pn : p;
+      return it + 1;
+    }
+    if (!inside) { pn = pa > 0.0 ? sqrt(pa * pb) : 0.01 * pb; prev = -1.0; }
+    else prev = as;
     p = pn;
-    if (change < tol) { pout = p; return it + 1; }
   }
   pout = p;
   return -max_iter;
@@ -100,17 +114,31 @@ __device__ __forceinline__ double star_u(const Side &L, const Side &R, double g,
 // ---------------------------------------------------------------------------
 // features (scale free, ~O(1)); target = ln(p*/p_TR)
 // ---------------------------------------------------------------------------
+// Computed in FP32: the network needs about three significant digits.
 __device__ __forceinline__ void features(const Side &L, const Side &R, double g, double ptr, float f[NIN]) {
   const float i4 = 1.0f / 9.2103404f, i3 = 1.0f / 6.9077553f;   // 1/ln(1e4), 1/ln(1e3)
-  f[0] = float(log(R.p / L.p)) * i4;
-  f[1] = float(log(R.d / L.d)) * i3;
-  f[2] = float(L.u / L.c) * 0.2f;
-  f[3] = float(R.u / R.c) * 0.2f;
-  f[4] = float((g - 1.5333333333333333) * 7.5);
-  f[5] = float((R.u - L.u) / (L.c + R.c));
-  f[6] = float(log(ptr / L.p)) * i4;
-  f[7] = float(log(fmax(L.p, R.p) / L.p)) * i4;
+  const float dl = float(L.d), dr = float(R.d), pl = float(L.p), pr = float(R.p);
+  const float ul = float(L.u), ur = float(R.u), cl = float(L.c), cr = float(R.c), gf = float(g);
+  const float du = ur - ul;
+  // two-shock estimate (Toro eq. 4.47) around the PVRS pressure
+  float ppv = fmaxf(0.5f * (pl + pr) - 0.125f * du * (dl + dr) * (cl + cr), 1e-6f * fminf(pl, pr));
+  float gL = sqrtf(2.0f / ((gf + 1.0f) * dl) / (ppv + (gf - 1.0f) / (gf + 1.0f) * pl));
+  float gR = sqrtf(2.0f / ((gf + 1.0f) * dr) / (ppv + (gf - 1.0f) / (gf + 1.0f) * pr));
+  float pts = fmaxf((gL * pl + gR * pr - du) / (gL + gR), 1e-30f);
+  float ptrf = float(ptr);
+  f[0] = logf(pr / pl) * i4;
+  f[1] = logf(dr / dl) * i3;
+  f[2] = ul / cl * 0.2f;
+  f[3] = ur / cr * 0.2f;
+  f[4] = (gf - 1.5333333f) * 7.5f;
+  f[5] = du / (cl + cr);
+  f[6] = logf(ptrf / pl) * i4;
+  f[7] = logf(pts / ptrf) * i4;
 }
+
+// The two-rarefaction guess is the exact root when it does not exceed
+// min(p_L, p_R) (both waves are rarefactions, Toro section 4.3.2).
+__device__ __forceinline__ bool tr_exact(const Side &L, const Side &R, double ptr) { return ptr <= fmin(L.p, R.p); }
 
 // ---------------------------------------------------------------------------
 // tensor-core MLP inference for the 32 interfaces of a warp
@@ -257,7 +285,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_solve(const double *__restric
       __syncwarp();
       mlp_warp(M, X[warp], Y[warp]);
       float y = fminf(fmaxf(Y[warp][lane], -20.f), 20.f);
-      p0 = ptr * exp((double)y);
+      if (!vacuum && !tr_exact(L, R, ptr)) p0 = ptr * (double)expf(y);
     }
     unsigned char fl = 0;
     int its = 0;
@@ -359,6 +387,7 @@ __global__ void k_make_samples(const double *S, const double *out, long n, float
     double ps = out[i];
     if (!(ps > 0.0)) continue;
     double ptr = tr_guess(L, R, g);
+    if (tr_exact(L, R, ptr)) continue;          // the guess is only used where TR is inexact
     int k = atomicAdd(count, 1);
     if (k >= cap) continue;
     float f[NIN];
@@ -666,7 +695,8 @@ extern "C" int flash_hy_rsolver_train(flash_hy_rsolver *r, const float *d_x, con
       k_grad<<<(batch + TS - 1) / TS, TRAIN_THREADS, 0, r->stream>>>(r->w, d_x, d_t, idx + bi * batch, batch,
                                                                       1.f / batch, r->G, r->loss);
       r->step++;
-      k_adam<<<(NPARAM + 255) / 256, 256, 0, r->stream>>>(r->w, r->m, r->v, r->G, r->step, lr, 0.9f, 0.999f, 1e-8f);
+      float lr_ep = lr * powf(0.05f, (float)ep / (float)epochs);   // exponential decay to lr/20
+      k_adam<<<(NPARAM + 255) / 256, 256, 0, r->stream>>>(r->w, r->m, r->v, r->G, r->step, lr_ep, 0.9f, 0.999f, 1e-8f);
     }
     float h = 0.f;
     RS_CUDA(cudaMemcpyAsync(&h, r->loss, sizeof(float), cudaMemcpyDeviceToHost, r->stream));

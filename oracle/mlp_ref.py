@@ -90,13 +90,18 @@ def two_rarefaction(L, R, g):
 
 
 def features(S):
-    """Feature map of riemann_exact.cu for states S[7][n] (non-vacuum)."""
+    """Feature map of riemann_exact.cu for states S[7][n] (non-vacuum),
+    evaluated in float64 (the device evaluates it in FP32)."""
     dl, ul, pl, dr, ur, pr, g = S
     cl, cr = np.sqrt(g * pl / dl), np.sqrt(g * pr / dr)
     ptr = two_rarefaction((dl, ul, pl, cl), (dr, ur, pr, cr), g)
+    ppv = np.maximum(0.5 * (pl + pr) - 0.125 * (ur - ul) * (dl + dr) * (cl + cr), 1e-6 * np.minimum(pl, pr))
+    gL = np.sqrt(2.0 / ((g + 1.0) * dl) / (ppv + (g - 1.0) / (g + 1.0) * pl))
+    gR = np.sqrt(2.0 / ((g + 1.0) * dr) / (ppv + (g - 1.0) / (g + 1.0) * pr))
+    pts = np.maximum((gL * pl + gR * pr - (ur - ul)) / (gL + gR), 1e-30)
     f = np.stack([np.log(pr / pl) / np.log(1e4), np.log(dr / dl) / np.log(1e3), ul / cl * 0.2, ur / cr * 0.2,
                   (g - 1.5333333333333333) * 7.5, (ur - ul) / (cl + cr), np.log(ptr / pl) / np.log(1e4),
-                  np.log(np.maximum(pl, pr) / pl) / np.log(1e4)], axis=1)
+                  np.log(pts / ptr) / np.log(1e4)], axis=1)
     return f, ptr
 
 

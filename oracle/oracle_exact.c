@@ -15,8 +15,9 @@
  * (lines 15-33, 90-120), is the cross-check used by the tests.
  *
  * Newton here is safeguarded by a bracket [pa, pb] with f(pa) < 0 < f(pb):
- * a step that leaves the bracket is replaced by bisection, so the iteration
- * always terminates within max_iter.
+ * a step that leaves the bracket is replaced by a geometric bisection (or a
+ * decimation towards zero while pa = 0), and the iteration stops when the
+ * Newton step is below tol * p, so it always terminates within max_iter.
  */
 #include <math.h>
 
@@ -71,18 +72,29 @@ int orc_star_state(double dl, double ul, double pl, double dr, double ur, double
     pb *= 4.0;
   }
   double p = p0 > 0.0 ? p0 : orc_two_rarefaction_guess(dl, ul, pl, dr, ur, pr, g);
-  if (!(p > pa && p < pb)) p = 0.5 * (pa + pb);
+  if (!(p > pa && p < pb)) p = pa > 0.0 ? sqrt(pa * pb) : 0.5 * pb;
   int status = 1;
+  double prev = -1.0;
   for (int it = 0; it < max_iter; ++it) {
     pres_fn(p, &L, g, &fl, &fdl); pres_fn(p, &R, g, &fr, &fdr);
     double f = fl + fr + du;
-    if (f < 0.0) pa = p; else pb = p;
-    double pn = p - f / (fdl + fdr);
-    if (!(pn > pa && pn < pb)) pn = 0.5 * (pa + pb);
     *iters = it + 1;
-    double change = fabs(pn - p) / (0.5 * (pn + p));
+    if (f == 0.0) { status = 0; break; }
+    if (f < 0.0) pa = p; else pb = p;
+    double step = f / (fdl + fdr);
+    double pn = p - step;
+    double as = fabs(step);
+    int inside = pn > pa && pn < pb;
+    /* converged: step below tol, or the predicted next step of the
+     * quadratic regime, |step|^3/prev^2, below tol/100 */
+    if (as <= tol * p || (inside && prev > 0.0 && as < prev && as * (as / prev) * (as / prev) <= 0.01 * tol * p)) {
+      if (pn > 0.0) p = pn;
+      status = 0;
+      break;
+    }
+    if (!inside) { pn = pa > 0.0 ? sqrt(pa * pb) : 0.01 * pb; prev = -1.0; }
+    else prev = as;
     p = pn;
-    if (change < tol) { status = 0; break; }
   }
   pres_fn(p, &L, g, &fl, &fdl); pres_fn(p, &R, g, &fr, &fdr);
   *pstar = p;
