@@ -24,6 +24,7 @@ UNITS = [
     ("hy_mixed.o", "hy_variant.cu", ["-DFHY_VARIANT=3", "--fmad=true"]),
     ("flash_hy.o", "flash_hy.cu", ["--fmad=false"]),
     ("riemann_exact.o", "riemann_exact.cu", ["--fmad=true"]),
+    ("cfl_noalloc.o", "cfl_noalloc.cu", ["--fmad=false"]),
 ]
 
 

@@ -158,6 +158,26 @@ int flash_hy_last_error(flash_hy_ctx *ctx, char *buf, int len);
 /* Number of kernel launches issued by the last flash_hy_step call. */
 int flash_hy_last_launch_count(flash_hy_ctx *ctx);
 
+/* ---- CFL time step without any device allocation ------------------------
+ * No counterpart in the reference: FLASH5's Hydro_computeDt runs on host
+ * arrays.  This entry point is for callers that cannot call cudaMalloc
+ * (device memory owned by another framework's pool, a fixed allocation
+ * budget, or work issued while a stream is being captured into a graph).  It
+ * computes the time step of flash_hy_compute_dt from caller-owned DEVICE
+ * arrays (block-major SoA: dens, velx, vely, velz, eint of the interiors,
+ * nblocks x nzb x nyb x nxb each, all EOS-consistent) and writes dt and the
+ * minloc (i, j, k, level, block) to HOST memory.  Its scratch is a fixed
+ * file-scope device array of FLASH_HY_NOALLOC_MAX_BLOCKS entries (1.5 MiB,
+ * held by every GPU that loads the library until exit); larger grids are
+ * rejected with FLASH_HY_ERR_BAD_ARG.  The first call on a device resolves
+ * the scratch address and should precede any stream capture.  All calls
+ * share the scratch: calls that overlap on the GPU race.  stream may be NULL. */
+#define FLASH_HY_NOALLOC_MAX_BLOCKS 65536
+int flash_hy_compute_dt_noalloc(const double *d_dens, const double *d_velx, const double *d_vely,
+                                const double *d_velz, const double *d_eint, int ndim, int nxb, int nyb, int nzb,
+                                int nblocks, const double deltas[3], double gamma, double cfl, void *stream,
+                                double *dt_out, int minloc_out[5]);
+
 /* ---- exact Riemann solver with a learned star-pressure guess ----------
  * No counterpart in FLASH5 (its unsplit solvers are approximate:
  * source/physics/Hydro/HydroMain/unsplit/hy_getFaceFlux.F90:324-372); the
