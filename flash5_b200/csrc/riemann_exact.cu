@@ -69,7 +69,8 @@ __device__ __forceinline__ double tr_guess(const Side &L, const Side &R, double 
 // tol * p / 100; the returned count is the number of function evaluations.  Steps
 // leaving [pa, pb] are replaced by a geometric (pa > 0) or decimating
 // (pa = 0, near vacuum) bisection.  Returns -max_iter when not converged.
-__device__ int newton(const Side &L, const Side &R, double g, double p0, double tol, int max_iter, double &pout) {
+__device__ __forceinline__ int newton(const Side &L, const Side &R, double g, double p0, double tol, int max_iter,
+                                      double &pout) {
   double du = R.u - L.u;
   double fl, fdl, fr, fdr;
   double pa = 0.0, pb = fmax(L.p, R.p);
@@ -247,10 +248,22 @@ __device__ void load_mlp(MlpSmem &M, const float *__restrict__ w) {
 // ---------------------------------------------------------------------------
 constexpr int SOLVE_THREADS = 256;
 
+__device__ __forceinline__ void load_state(const double *__restrict__ S, long n, long i, Side &L, Side &R, double &g) {
+  L.d = S[i]; L.u = S[n + i]; L.p = S[2 * n + i];
+  R.d = S[3 * n + i]; R.u = S[4 * n + i]; R.p = S[5 * n + i];
+  g = S[6 * n + i];
+  L.c = sqrt(g * L.p / L.d); R.c = sqrt(g * R.p / R.d);
+}
+
+// learned != 0: Newton gets three evaluations from the network's guess
+// (or from the two-rarefaction guess where that guess is exact); lanes that
+// have not converged are appended to `queue` (warp-aggregated atomics) and
+// re-solved from the two-rarefaction guess by k_fallback, so no warp waits
+// for a fallback lane.
 __global__ void __launch_bounds__(SOLVE_THREADS) k_solve(const double *__restrict__ S, long n, double *__restrict__ out,
                                                          unsigned char *__restrict__ iters, unsigned char *__restrict__ flags,
                                                          const float *__restrict__ w, int learned, double tol,
-                                                         int max_iter, unsigned *status) {
+                                                         int max_iter, int *queue, int *qcount, unsigned *status) {
   __shared__ MlpSmem M;
   __shared__ __align__(16) __nv_bfloat16 X[SOLVE_THREADS / 32][32][16];
   __shared__ float Y[SOLVE_THREADS / 32][32];
@@ -265,13 +278,10 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_solve(const double *__restric
     Side L, R;
     double g = 1.4;
     if (valid) {
-      L.d = S[i]; L.u = S[n + i]; L.p = S[2 * n + i];
-      R.d = S[3 * n + i]; R.u = S[4 * n + i]; R.p = S[5 * n + i];
-      g = S[6 * n + i];
+      load_state(S, n, i, L, R, g);
     } else {
-      L.d = R.d = 1.0; L.u = R.u = 0.0; L.p = R.p = 1.0;
+      L.d = R.d = 1.0; L.u = R.u = 0.0; L.p = R.p = 1.0; L.c = R.c = sqrt(1.4);
     }
-    L.c = sqrt(g * L.p / L.d); R.c = sqrt(g * R.p / R.d);
     const bool vacuum = 2.0 * (L.c + R.c) / (g - 1.0) <= R.u - L.u;
     double ptr = vacuum ? 0.0 : tr_guess(L, R, g);
     double p0 = ptr;
@@ -289,31 +299,56 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_solve(const double *__restric
     }
     unsigned char fl = 0;
     int its = 0;
+    bool pending = false;
     double ps = 0.0, us = 0.5 * (L.u + R.u);
     if (vacuum) {
       fl |= 2;
-    } else if (learned) {
-      int k = newton(L, R, g, p0, tol, 3, ps);
-      if (k > 0) {
-        its = k;
-      } else {             // judge: restart from the two-rarefaction guess
-        its = 3;
-        fl |= 1;
-        int k2 = newton(L, R, g, ptr, tol, max_iter, ps);
-        if (k2 > 0) its += k2;
-        else { its += max_iter; fl |= 4; st |= FLASH_HY_ERR_NEWTON_NOCONV; }
-      }
     } else {
-      int k = newton(L, R, g, ptr, tol, max_iter, ps);
+      int k = newton(L, R, g, p0, tol, learned ? 3 : max_iter, ps);
       if (k > 0) its = k;
+      else if (learned) pending = true;
       else { its = max_iter; fl |= 4; st |= FLASH_HY_ERR_NEWTON_NOCONV; }
     }
-    if (!vacuum) us = star_u(L, R, g, ps);
-    if (valid) {
+    if (learned) {
+      const unsigned m = __ballot_sync(0xffffffffu, pending && valid);
+      if (m) {
+        int base_q = 0;
+        if (lane == __ffs(m) - 1) base_q = atomicAdd(qcount, __popc(m));
+        base_q = __shfl_sync(0xffffffffu, base_q, __ffs(m) - 1);
+        if (pending && valid) queue[base_q + __popc(m & ((1u << lane) - 1))] = (int)i;
+      }
+    }
+    if (valid && !pending) {
+      if (!vacuum) us = star_u(L, R, g, ps);
       out[i] = ps; out[n + i] = us;
       if (iters) iters[i] = (unsigned char)(its > 255 ? 255 : its);
       if (flags) flags[i] = fl;
     }
+  }
+  if (st) atomicOr(status, st);
+}
+
+// the judge: queued solves restart from the two-rarefaction guess
+__global__ void __launch_bounds__(SOLVE_THREADS) k_fallback(const double *__restrict__ S, long n,
+                                                            double *__restrict__ out, unsigned char *__restrict__ iters,
+                                                            unsigned char *__restrict__ flags, const int *queue,
+                                                            const int *qcount, double tol, int max_iter,
+                                                            unsigned *status) {
+  const int nq = *qcount;
+  unsigned st = 0;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+    const long i = queue[q];
+    Side L, R;
+    double g;
+    load_state(S, n, i, L, R, g);
+    double ps;
+    unsigned char fl = 1;
+    int k = newton(L, R, g, tr_guess(L, R, g), tol, max_iter, ps);
+    int its = 3 + (k > 0 ? k : max_iter);
+    if (k <= 0) { fl |= 4; st |= FLASH_HY_ERR_NEWTON_NOCONV; }
+    out[i] = ps; out[n + i] = star_u(L, R, g, ps);
+    if (iters) iters[i] = (unsigned char)(its > 255 ? 255 : its);
+    if (flags) flags[i] = fl;
   }
   if (st) atomicOr(status, st);
 }
@@ -558,6 +593,8 @@ struct flash_hy_rsolver {
   int device;
   cudaStream_t stream;
   float *w, *m, *v, *G, *loss;
+  int *queue, *qcount;          // fallback queue of the learned path
+  long qcap;
   unsigned *status;
   int step;
   char err[256];
@@ -588,6 +625,7 @@ extern "C" int flash_hy_rsolver_create(int device, flash_hy_rsolver **out) {
   RS_CUDA(cudaMalloc(&r->G, NPARAM * sizeof(float)));
   RS_CUDA(cudaMalloc(&r->loss, sizeof(float)));
   RS_CUDA(cudaMalloc(&r->status, sizeof(unsigned)));
+  RS_CUDA(cudaMalloc(&r->qcount, sizeof(int)));
   RS_CUDA(cudaMemset(r->m, 0, NPARAM * sizeof(float)));
   RS_CUDA(cudaMemset(r->v, 0, NPARAM * sizeof(float)));
   RS_CUDA(cudaMemset(r->status, 0, sizeof(unsigned)));
@@ -610,6 +648,7 @@ extern "C" int flash_hy_rsolver_destroy(flash_hy_rsolver *r) {
   cudaSetDevice(r->device);
   if (r->stream) cudaStreamSynchronize(r->stream);
   cudaFree(r->w); cudaFree(r->m); cudaFree(r->v); cudaFree(r->G); cudaFree(r->loss); cudaFree(r->status);
+  cudaFree(r->queue); cudaFree(r->qcount);
   if (r->stream) cudaStreamDestroy(r->stream);
   free(r);
   return 0;
@@ -628,11 +667,24 @@ extern "C" int flash_hy_rsolver_generate(flash_hy_rsolver *r, unsigned long long
 extern "C" int flash_hy_rsolver_solve(flash_hy_rsolver *r, const double *d_states, long n, double *d_star,
                                       unsigned char *d_iters, unsigned char *d_flags, int learned, double tol,
                                       int max_iter) {
-  if (!r || !d_states || !d_star || n <= 0 || max_iter <= 0 || max_iter > 200) return FLASH_HY_ERR_BAD_ARG;
+  if (!r || !d_states || !d_star || n <= 0 || n > 0x7fffffffL || max_iter <= 0 || max_iter > 200)
+    return FLASH_HY_ERR_BAD_ARG;
   RS_CUDA(cudaSetDevice(r->device));
+  if (learned && r->qcap < n) {
+    if (r->queue) { cudaStreamSynchronize(r->stream); cudaFree(r->queue); r->queue = nullptr; r->qcap = 0; }
+    RS_CUDA(cudaMalloc(&r->queue, n * sizeof(int)));
+    r->qcap = n;
+  }
+  if (learned) RS_CUDA(cudaMemsetAsync(r->qcount, 0, sizeof(int), r->stream));
   k_solve<<<grid_for(n, SOLVE_THREADS), SOLVE_THREADS, 0, r->stream>>>(d_states, n, d_star, d_iters, d_flags, r->w,
-                                                                      learned, tol, max_iter, r->status);
+                                                                      learned, tol, max_iter, r->queue, r->qcount,
+                                                                      r->status);
   RS_CUDA(cudaGetLastError());
+  if (learned) {
+    k_fallback<<<148 * 4, SOLVE_THREADS, 0, r->stream>>>(d_states, n, d_star, d_iters, d_flags, r->queue, r->qcount,
+                                                         tol, max_iter, r->status);
+    RS_CUDA(cudaGetLastError());
+  }
   return 0;
 }
 

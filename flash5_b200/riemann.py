@@ -68,12 +68,21 @@ class ExactRiemann:
         if st:
             raise RiemannError(f"status {st:#x}")
 
+    def _enter(self):
+        # the library works on its own stream: order it after torch's work
+        self.stream.wait_stream(self.torch.cuda.current_stream())
+
+    def _leave(self):
+        self.torch.cuda.current_stream().wait_stream(self.stream)
+
     def empty(self, *shape, dtype=None):
         return self.torch.empty(*shape, dtype=dtype or self.torch.float64, device=f"cuda:{self.device}")
 
     def generate(self, seed, n):
         S = self.empty(7, n)
+        self._enter()
         self._check(self.L.flash_hy_rsolver_generate(self.h, seed, n, S.data_ptr()))
+        self._leave()
         return S
 
     def solve(self, S, learned, tol=1e-12, max_iter=50, out=None, iters=None, flags=None):
@@ -81,14 +90,18 @@ class ExactRiemann:
         out = self.empty(2, n) if out is None else out
         iters = self.empty(n, dtype=self.torch.uint8) if iters is None else iters
         flags = self.empty(n, dtype=self.torch.uint8) if flags is None else flags
+        self._enter()
         self._check(self.L.flash_hy_rsolver_solve(self.h, S.data_ptr(), n, out.data_ptr(), iters.data_ptr(),
                                                   flags.data_ptr(), int(learned), tol, max_iter))
+        self._leave()
         return out, iters, flags
 
     def predict(self, S):
         n = S.shape[1]
         y = self.empty(n, dtype=self.torch.float32)
+        self._enter()
         self._check(self.L.flash_hy_rsolver_predict(self.h, S.data_ptr(), n, y.data_ptr()))
+        self._leave()
         return y
 
     def make_samples(self, S, star, cap=None):
@@ -97,6 +110,7 @@ class ExactRiemann:
         X = self.empty(cap, 8, dtype=self.torch.float32)
         T = self.empty(cap, dtype=self.torch.float32)
         cnt = C.c_long()
+        self._enter()
         self._check(self.L.flash_hy_rsolver_make_samples(self.h, S.data_ptr(), star.data_ptr(), n, X.data_ptr(),
                                                          T.data_ptr(), cap, C.byref(cnt)))
         return X, T, cnt.value
@@ -104,12 +118,14 @@ class ExactRiemann:
     def grad(self, X, T, idx):
         g = np.zeros(self.nparam, np.float32)
         loss = C.c_float()
+        self._enter()
         self._check(self.L.flash_hy_rsolver_grad(self.h, X.data_ptr(), T.data_ptr(), idx.data_ptr(), idx.numel(),
                                                  g.ctypes.data_as(C.POINTER(C.c_float)), C.byref(loss)))
         return g, loss.value
 
     def train(self, X, T, ns, epochs=4, batch=4096, lr=2e-3):
         loss = C.c_float()
+        self._enter()
         self._check(self.L.flash_hy_rsolver_train(self.h, X.data_ptr(), T.data_ptr(), ns, epochs, batch, lr,
                                                   C.byref(loss)))
         return loss.value
