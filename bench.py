@@ -2,20 +2,26 @@
 
 Workload: 3D Kelvin-Helmholtz, 256^3 cells as 32^3 blocks of 8^3 interior
 cells (FLASH's 4 guard layers are filled inside the kernels), gamma = 5/3,
-periodic boundaries, PPM + HLLC with characteristic limiting and
-flattening, CFL 0.8, the time step recomputed every step (Hydro_computeDt
-reduction + Driver_computeDt growth limit).  Inputs are synthetic (seeded
-noise, numpy PCG64 seed 12345).
+periodic boundaries, PPM with characteristic limiting and flattening, CFL
+0.8, the time step recomputed every step (Hydro_computeDt reduction +
+Driver_computeDt growth limit).  Inputs are synthetic (seeded noise, numpy
+PCG64 seed 12345).
 
 One step = the device pass of the hot path over all blocks (k_sig + one
 fused kernel per direction) plus the CFL reduction read back to the host.
-``value`` is the mixed path (FP32 reconstruction and Riemann solve, FP64
-update) with the state resident in HBM; the plain FP64 path is reported
-beside it, and the mixed path's L1 error against the FP64 path (which
-matches the CPU oracle bit for bit in the tests) is measured on the same
-run.  ``e2e`` is the same metric through the C-ABI with host UNK buffers
-(interior-only FLASH UNK, 11 variables, pinned): upload, step, dt, download
-every step.
+Paths (all replay the dt sequence of the first):
+  fp64           plain FP64 HLLC (bit-identical to the CPU oracle)
+  fp64_exact     FP64 with the exact Riemann solver (FP64 reference of the
+                 exact-solver paths)
+  mixed          FP32 reconstruction, FP64 HLLC and update
+  mixed_exact    FP32 reconstruction, FP64 exact solver and update
+  mixed_learned  as mixed_exact, Newton started from the tensor-core MLP
+                 guess trained on this run's harvested face states
+``value`` is the last path (by default mixed_learned, the metric's
+"batched mixed+learned") with the state resident in HBM; each path's L1
+error is measured against its FP64 reference on the same run.  ``e2e`` is
+the same metric through the C-ABI with host UNK buffers (interior-only
+FLASH UNK, 11 variables, pinned): upload, step, dt, download every step.
 
 ``--impl reference`` times the CPU oracle (the C restatement of the
 reference's Fortran; the Fortran itself cannot be built here) on a bounded
@@ -236,6 +242,42 @@ def cpu_baseline(seconds=12.0, steps=None, warmup=0):
             "sample": f"3D KH 64^3 (512 blocks of 8^3), {n} steps, {el:.1f} s, oracle C port, OpenMP"}
 
 
+def train_guess(g, unk, abi, dev, dts):
+    """Learned star-pressure guess for the hydro faces: run two steps of the
+    mixed exact-solver path with face-state harvesting on (the faces where
+    the network is consulted: strong waves, inexact two-rarefaction guess),
+    top the sample up with the solver's own isolated solves when the flow
+    has few such faces, and train the network with the library's training
+    kernels.  Returns the FP32 weights (outside the timed region)."""
+    import torch
+    from flash5_b200.hydro import Hydro
+    from flash5_b200.riemann import ExactRiemann
+    t0 = time.perf_counter()
+    h = Hydro(abi.default_params(gamma=5.0 / 3.0, precision=abi.PREC_MIXED, riemann_solver=abi.RS_EXACT), g,
+              device=dev)
+    h.upload(unk)
+    dt, _ = h.compute_dt()
+    h.harvest(2_000_000, keep_log2=0)
+    t = 0.0
+    for i in range(2):
+        d = dts[i] if dts is not None else dt
+        h(t + d, d, d)
+        t += d
+    S = h.harvest_fetch(torch)
+    h.close()
+    r = ExactRiemann(dev)
+    nh = int(S.shape[1])
+    if nh < 1_000_000:
+        S = torch.cat([S, r.generate(7, 1_000_000 - nh)], dim=1).contiguous()
+    loss, ns = r.fit(S, epochs=8, batch=4096, lr=2e-3)
+    w = r.weights()
+    r.close()
+    return w, {"hydro_face_states": nh, "isolated_states": int(S.shape[1]) - nh, "samples": ns, "epochs": 8,
+               "final_mse": loss, "seconds": time.perf_counter() - t0,
+               "source": "2 steps of the mixed exact path (faces with strong waves), topped up with isolated "
+                         "solves of the 1e8-pair distribution"}
+
+
 def conserved_l1(a, b, var):
     from oracle import sfocu
     ca = sfocu.conserved(a, var)
@@ -312,7 +354,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", default="kh", choices=["kh", "riemann"])
     ap.add_argument("--riemann-n", type=int, default=100_000_000)
-    ap.add_argument("--paths", default="fp64,fp64_fma,mixed",
+    ap.add_argument("--paths", default="fp64,fp64_exact,mixed,mixed_exact,mixed_learned",
                     help="comma list of paths to time; profiling runs use one")
     args = ap.parse_args()
     paths = args.paths.split(",")
@@ -359,16 +401,27 @@ def main():
     zones = g.ncells
     peak, peak_kind = measured_peaks()
 
-    prec = {"fp64": abi.PREC_FP64, "fp64_fma": abi.PREC_FP64_FMA, "mixed": abi.PREC_MIXED}
-    ms, outs, dts, launches, clocks, e2e_ms, hb = {}, {}, None, 0, None, None, None
-    for name in ["fp64", "fp64_fma", "mixed"]:
-        if name not in paths:
-            continue
-        h = Hydro(abi.default_params(gamma=5.0 / 3.0, precision=prec[name]), g, device=dev)
+    # path -> (precision, Riemann solver, learned guess, error reference path)
+    spec = {"fp64": (abi.PREC_FP64, abi.RS_HLLC, 0, None),
+            "fp64_fma": (abi.PREC_FP64_FMA, abi.RS_HLLC, 0, "fp64"),
+            "fp64_exact": (abi.PREC_FP64, abi.RS_EXACT, 0, None),
+            "mixed": (abi.PREC_MIXED, abi.RS_HLLC, 0, "fp64"),
+            "mixed_exact": (abi.PREC_MIXED, abi.RS_EXACT, 0, "fp64_exact"),
+            "mixed_learned": (abi.PREC_MIXED, abi.RS_EXACT, 1, "fp64_exact")}
+    ms, outs, dts, launches, clocks, e2e_ms, hb, training = {}, {}, None, {}, None, None, None, None
+    for name in paths:
+        pr, rsv, learned, _ = spec[name]
+        params = abi.default_params(gamma=5.0 / 3.0, precision=pr, riemann_solver=rsv, learned_guess=learned)
+        weights = None
+        if learned:
+            weights, training = train_guess(g, unk, abi, dev, dts)
+        h = Hydro(params, g, device=dev)
+        if weights is not None:
+            h.set_guess_weights(weights)
         h.upload(unk)
         headline = name == paths[-1]
         sampler = ClockSampler(dev) if headline else None
-        ms[name], used, launches = run_device(h, args.steps, warmup, dts=dts, sampler=sampler, dist=dist)
+        ms[name], used, launches[name] = run_device(h, args.steps, warmup, dts=dts, sampler=sampler, dist=dist)
         if dts is None:
             dts = used            # later paths replay the first path's dt sequence
         if headline:
@@ -383,7 +436,7 @@ def main():
             hb = host.nbytes
         h.close()
     head = paths[-1]
-    errs = {n: conserved_l1(outs[n], outs["fp64"], VAR) for n in outs if n != "fp64" and "fp64" in outs}
+    errs = {n: conserved_l1(outs[n], outs[spec[n][3]], VAR) for n in outs if spec[n][3] in outs}
     if dist is not None:
         for n in ms:
             ms[n] = dist_max(dist, ms[n])
@@ -394,26 +447,36 @@ def main():
     if rank == 0:
         cpu = None if (args.no_cpu or world > 1) else cpu_baseline()
         achieved = zones * BYTES_PER_ZONE / (ms[head] * 1e-3) / 1e9
-        notes = {"fp64": "FP64, no FMA contraction; bit-identical to the CPU oracle in the tests",
-                 "fp64_fma": "FP64 with FMA contraction", "mixed": "FP32 reconstruction + Riemann solve, FP64 update"}
+        notes = {"fp64": "plain FP64 HLLC, no FMA contraction; bit-identical to the CPU oracle in the tests",
+                 "fp64_fma": "FP64 HLLC with FMA contraction",
+                 "fp64_exact": "FP64, exact Riemann solver (two-rarefaction start, Newton to 1e-12); the FP64 "
+                               "reference of the exact-solver paths, matches the CPU oracle to 1e-10 in the tests",
+                 "mixed": "FP32 reconstruction, FP64 HLLC and update",
+                 "mixed_exact": "FP32 reconstruction, FP64 exact Riemann (two-rarefaction start) and update",
+                 "mixed_learned": "FP32 reconstruction, FP64 exact Riemann started from the BF16 tensor-core MLP "
+                                  "guess (trained on this run's harvested face states), FP64 update"}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": warmup,
             "ms_per_step": ms[head], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": {"mixed": "f32 reconstruction/flux, f64 update"}.get(head, "f64"),
+            "dtype": "f32 reconstruction, f64 Riemann/update" + (", bf16 MLP guess" if head == "mixed_learned" else "")
+                     if head.startswith("mixed") else "f64",
             "data": "synthetic (seeded KH noise)",
             "config": {"workload": f"3D Kelvin-Helmholtz {8 * args.nblk}^3 as {args.nblk}^3 blocks of 8^3 (+4 guard "
-                                   "filled in-kernel), gamma 5/3, periodic, PPM+HLLC, CFL 0.8, dt from the CFL reduction "
+                                   "filled in-kernel), gamma 5/3, periodic, PPM, CFL 0.8, dt from the CFL reduction "
                                    "every step" + (", independent replica per GPU + NCCL dt min" if world > 1 else ""),
+                       "riemann": "exact (Newton 1e-12)" if spec[head][1] == abi.RS_EXACT else "HLLC",
                        "zones_per_gpu": zones, "l2": f"inputs larger than L2 (state {zones * 40 / 1e6:.0f} MB)",
                        "path": head},
             "paths": {n: {"value": total / (ms[n] * 1e-3), "ms_per_step": ms[n], "note": notes[n],
-                          **({"rel_l1_vs_fp64": errs[n]} if n in errs else {})} for n in ms},
+                          **({f"rel_l1_vs_{spec[n][3]}": errs[n]} if n in errs else {})} for n in ms},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": None, "peak_kind": peak_kind,
                          "kernel": "one hydro step (k_sig + k_dir x,y,z), 80 B/zone algorithmic"},
             "clocks": clocks,
-            "gpu_launches": launches * args.steps,
+            "gpu_launches": launches[head] * args.steps,
         }
+        if training is not None:
+            line["training"] = training
         if "fp64" in ms and head != "fp64":
             line["speedup_vs_fp64"] = ms["fp64"] / ms[head]
         if e2e_ms is not None:

@@ -118,6 +118,9 @@ def _set_sigs(lib):
         "flash_hy_stream": (vp, [vp]),
         "flash_hy_last_error": (C.c_int, [vp, C.c_char_p, C.c_int]),
         "flash_hy_last_launch_count": (C.c_int, [vp]),
+        "flash_hy_set_guess_weights": (C.c_int, [vp, C.POINTER(C.c_float), C.c_int]),
+        "flash_hy_harvest": (C.c_int, [vp, C.c_longlong, C.c_int]),
+        "flash_hy_harvest_fetch": (C.c_int, [vp, vp, C.c_longlong, C.POINTER(C.c_longlong)]),
     }
     for name, (res, args) in sigs.items():
         f = getattr(lib, name)

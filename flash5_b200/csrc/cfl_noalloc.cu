@@ -121,6 +121,7 @@ extern "C" int flash_hy_compute_dt_noalloc(const double *d_dens, const double *d
   a.nlaunch = nblocks;
   a.threads = 320;
   a.stream = static_cast<cudaStream_t>(stream);
+  a.set_attr = true;
   int n = cfl_state(a, ndim, nxb, ndim > 1 ? nyb : 1, ndim > 2 ? nzb : 1);
   if (n == -1) return FLASH_HY_ERR_UNSUPPORTED;
   if (n < 0) return FLASH_HY_ERR_CUDA;

@@ -38,8 +38,32 @@ struct flash_hy_ctx {
   int launches;
   int threads;
   int host_ng;         // guard layers of the caller's UNK arrays
+  float *d_wmaster;    // learned guess: FP32 master weights
+  void *d_mlp;         // learned guess: packed BF16 inference copy (xrs::MlpPacked)
+  int mlp_set;
+  double *d_harvest;   // [7][harvest_cap] face states kept for training
+  unsigned long long *d_harvest_n;
+  long long harvest_cap;
+  unsigned harvest_mask;
+  // graph replay of flash_hy_step: one executable graph per state-buffer
+  // parity (the step reads buffer cur and writes 1 - cur); dt is written to
+  // d_stepdt by a one-thread kernel launched before the replay
+  bool use_graph;
+  cudaGraphExec_t gexec[2];
+  int glaunches[2];
+  int plain_steps[2];
+  double *d_stepdt;
   char err[512];
 };
+
+static void drop_graphs(flash_hy_ctx *c) {
+  for (int q = 0; q < 2; ++q) {
+    if (c->gexec[q]) cudaGraphExecDestroy(c->gexec[q]);
+    c->gexec[q] = nullptr;
+  }
+}
+
+__global__ void k_set_dt(double *d, double dt) { *d = dt; }
 
 static int fail(flash_hy_ctx *c, int code, const char *fmt, const char *detail) {
   if (c) snprintf(c->err, sizeof c->err, fmt, detail ? detail : "");
@@ -69,6 +93,15 @@ static void fill_devparams(const flash_hy_ctx *c, DevParams &P) {
   P.use_ctu = c->p.use_3d_full_ctu;
   P.riemann = c->p.riemann_solver;
   P.learned = c->p.learned_guess;
+  P.mlp = (c->p.learned_guess && c->mlp_set) ? c->d_mlp : nullptr;
+  P.rs_tol = 1e-12;
+  P.rs_max_iter = 50;
+  if (c->harvest_cap > 0) {
+    P.harvest = c->d_harvest;
+    P.harvest_n = c->d_harvest_n;
+    P.harvest_cap = c->harvest_cap;
+    P.harvest_mask = c->harvest_mask;
+  }
   P.lim_beta = c->p.limited_slope_beta;
   P.gamma = c->p.gamma;
   double gammam1 = 1.0 / (c->p.gamma - 1.0);            // eos_initGamma.F90:32
@@ -94,8 +127,13 @@ extern "C" int flash_hy_create(const flash_hy_params *params, const flash_hy_gri
                                flash_hy_ctx **out) {
   if (!params || !g || !out) return FLASH_HY_ERR_BAD_ARG;
   *out = nullptr;
-  if (params->order != 3 || params->riemann_solver != FLASH_HY_RS_HLLC || params->f_pres_in_mom_flux != 1.0 ||
-      params->precision < 0 || params->precision > 2)
+  if (params->order != 3 ||
+      (params->riemann_solver != FLASH_HY_RS_HLLC && params->riemann_solver != FLASH_HY_RS_EXACT) ||
+      params->f_pres_in_mom_flux != 1.0 || params->precision < 0 || params->precision > 2)
+    return FLASH_HY_ERR_UNSUPPORTED;
+  // the learned guess belongs to the exact solver and to the mixed path
+  if (params->learned_guess &&
+      (params->riemann_solver != FLASH_HY_RS_EXACT || params->precision != FLASH_HY_PREC_MIXED))
     return FLASH_HY_ERR_UNSUPPORTED;
   if (params->gamma <= 1.0 || params->cfl <= 0.0) return FLASH_HY_ERR_BAD_ARG;
   int nz = g->ndim > 2 ? g->nzb : 1, ny = g->ndim > 1 ? g->nyb : 1;
@@ -157,6 +195,11 @@ extern "C" int flash_hy_create(const flash_hy_params *params, const flash_hy_gri
   ALLOC(c->d_part, g->nblocks * sizeof(CflPart));
   ALLOC(c->d_dt, sizeof(DtInfo));
   ALLOC(c->d_status, sizeof(unsigned));
+  ALLOC(c->d_stepdt, sizeof(double));
+  {
+    const char *e = getenv("FLASH_HY_GRAPH");
+    c->use_graph = !(e && e[0] == '0');
+  }
   if (cudaMallocHost((void **)&c->h_dt, sizeof(DtInfo)) != cudaSuccess ||
       cudaMallocHost((void **)&c->h_status, sizeof(unsigned)) != cudaSuccess) {
     rc = fail(c, FLASH_HY_ERR_CUDA, "cudaMallocHost%s", ""); goto bad;
@@ -181,6 +224,9 @@ extern "C" int flash_hy_destroy(flash_hy_ctx *c) {
   cudaFree(c->acc); cudaFree(c->aux); cudaFree(c->sig);
   cudaFree(c->d_blk_at); cudaFree(c->d_blk_coord); cudaFree(c->d_list);
   cudaFree(c->d_part); cudaFree(c->d_dt); cudaFree(c->d_status); cudaFree(c->d_stage);
+  cudaFree(c->d_wmaster); cudaFree(c->d_mlp); cudaFree(c->d_harvest); cudaFree(c->d_harvest_n);
+  drop_graphs(c);
+  cudaFree(c->d_stepdt);
   if (c->h_dt) cudaFreeHost(c->h_dt);
   if (c->h_status) cudaFreeHost(c->h_status);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -312,10 +358,13 @@ extern "C" int flash_hy_download(flash_hy_ctx *c, double *unk, int layout, int n
 // ---------------------------------------------------------------------------
 // step
 // ---------------------------------------------------------------------------
-static int enqueue_step(flash_hy_ctx *c, double dt, const int *d_list, int nlaunch) {
+static int enqueue_step(flash_hy_ctx *c, double dt, const int *d_list, int nlaunch, const double *dt_dev = nullptr,
+                        bool set_attr = true) {
   StepArgs a;
   fill_devparams(c, a.P);
   a.P.dt = dt;
+  a.P.dt_dev = dt_dev;
+  a.set_attr = set_attr;
   a.P.blk_list = d_list;
   a.sig = c->sig;
   a.acc = c->acc;
@@ -342,8 +391,40 @@ extern "C" int flash_hy_step(flash_hy_ctx *c, double simTime, double dt, double 
   if (!c) return FLASH_HY_ERR_BAD_ARG;
   if (!(dt > 0.0)) return fail(c, FLASH_HY_ERR_NONPOS_DT, "dt must be positive%s", "");
   CUDA_OK(c, cudaSetDevice(c->device));
-  int rc = enqueue_step(c, dt, nullptr, c->nblocks);
-  if (rc) return rc;
+  if (!c->use_graph) {
+    int rc = enqueue_step(c, dt, nullptr, c->nblocks);
+    if (rc) return rc;
+  } else {
+    const int q = c->cur;
+    k_set_dt<<<1, 1, 0, c->stream>>>(c->d_stepdt, dt);
+    CUDA_OK(c, cudaGetLastError());
+    if (!c->gexec[q] && c->plain_steps[q] == 0) {
+      // first step of this parity runs uncaptured (it also sets the kernels'
+      // shared-memory attributes, which are not stream work)
+      int rc = enqueue_step(c, dt, nullptr, c->nblocks, c->d_stepdt, true);
+      if (rc) return rc;
+      c->plain_steps[q]++;
+      c->launches = c->launches + 1;
+    } else {
+      if (!c->gexec[q]) {
+        cudaGraph_t g = nullptr;
+        CUDA_OK(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = enqueue_step(c, dt, nullptr, c->nblocks, c->d_stepdt, false);
+        cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
+        if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+        if (ec != cudaSuccess) return fail(c, FLASH_HY_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ec));
+        ec = cudaGraphInstantiate(&c->gexec[q], g, 0);
+        cudaGraphDestroy(g);
+        if (ec != cudaSuccess) {
+          c->gexec[q] = nullptr;
+          return fail(c, FLASH_HY_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ec));
+        }
+        c->glaunches[q] = c->launches;
+      }
+      CUDA_OK(c, cudaGraphLaunch(c->gexec[q], c->stream));
+      c->launches = c->glaunches[q] + 1;
+    }
+  }
   c->cur = 1 - c->cur;
   c->dt_valid = 1;
   return 0;
@@ -427,6 +508,7 @@ extern "C" int flash_hy_compute_dt(flash_hy_ctx *c, double *dt_out, int minloc_o
     a.nlaunch = c->nblocks;
     a.threads = c->threads;
     a.stream = c->stream;
+    a.set_attr = true;
     if (cfl_state(a, c->ndim, c->nx, c->ny, c->nz) < 0) return fail(c, FLASH_HY_ERR_CUDA, "cfl launch%s", "");
     c->dt_valid = 1;
   }
@@ -464,3 +546,60 @@ extern "C" int flash_hy_last_error(flash_hy_ctx *c, char *buf, int len) {
 }
 
 extern "C" int flash_hy_last_launch_count(flash_hy_ctx *c) { return c ? c->launches : -1; }
+
+// ---------------------------------------------------------------------------
+// exact Riemann solver: learned initial guess and face-state harvesting
+// ---------------------------------------------------------------------------
+extern "C" int flash_hy_set_guess_weights(flash_hy_ctx *c, const float *w, int n) {
+  if (!c || !w || n != xrs::NPARAM) return fail(c, FLASH_HY_ERR_BAD_ARG, "set_guess_weights: %s", "bad arguments");
+  CUDA_OK(c, cudaSetDevice(c->device));
+  if (!c->d_wmaster) {
+    CUDA_OK(c, cudaMalloc((void **)&c->d_wmaster, xrs::NPARAM * sizeof(float)));
+    CUDA_OK(c, cudaMalloc(&c->d_mlp, sizeof(xrs::MlpPacked)));
+  }
+  CUDA_OK(c, cudaMemcpyAsync(c->d_wmaster, w, xrs::NPARAM * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  xrs::k_pack_mlp<<<1, 256, 0, c->stream>>>(c->d_wmaster, static_cast<xrs::MlpPacked *>(c->d_mlp));
+  CUDA_OK(c, cudaGetLastError());
+  CUDA_OK(c, cudaStreamSynchronize(c->stream));     // the host copy may go away after return
+  c->mlp_set = 1;
+  drop_graphs(c);                                   // captured steps hold the old kernel parameters
+  return 0;
+}
+
+extern "C" int flash_hy_harvest(flash_hy_ctx *c, long long cap, int keep_log2) {
+  if (!c || cap < 0 || keep_log2 < 0 || keep_log2 > 30) return fail(c, FLASH_HY_ERR_BAD_ARG, "harvest: %s", "bad arguments");
+  if (c->p.riemann_solver != FLASH_HY_RS_EXACT || c->p.precision != FLASH_HY_PREC_MIXED)
+    return fail(c, FLASH_HY_ERR_UNSUPPORTED, "harvest: %s", "needs the exact solver on the mixed path");
+  CUDA_OK(c, cudaSetDevice(c->device));
+  CUDA_OK(c, cudaStreamSynchronize(c->stream));
+  cudaFree(c->d_harvest); c->d_harvest = nullptr;
+  c->harvest_cap = 0;
+  drop_graphs(c);
+  if (cap == 0) return 0;
+  CUDA_OK(c, cudaMalloc((void **)&c->d_harvest, (size_t)7 * cap * sizeof(double)));
+  if (!c->d_harvest_n) CUDA_OK(c, cudaMalloc((void **)&c->d_harvest_n, sizeof(unsigned long long)));
+  CUDA_OK(c, cudaMemsetAsync(c->d_harvest_n, 0, sizeof(unsigned long long), c->stream));
+  c->harvest_cap = cap;
+  c->harvest_mask = (1u << keep_log2) - 1u;
+  return 0;
+}
+
+extern "C" int flash_hy_harvest_fetch(flash_hy_ctx *c, double *d_states, long long n_max, long long *n_out) {
+  if (!c || !n_out || n_max < 0) return fail(c, FLASH_HY_ERR_BAD_ARG, "harvest_fetch: %s", "bad arguments");
+  *n_out = 0;
+  if (c->harvest_cap == 0) return 0;
+  CUDA_OK(c, cudaSetDevice(c->device));
+  unsigned long long h = 0;
+  CUDA_OK(c, cudaMemcpyAsync(&h, c->d_harvest_n, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_OK(c, cudaStreamSynchronize(c->stream));
+  long long n = (long long)h < c->harvest_cap ? (long long)h : c->harvest_cap;
+  if (!d_states) { *n_out = n; return 0; }       // query only
+  if (n > n_max) n = n_max;
+  for (int k = 0; k < 7 && n > 0; ++k)
+    CUDA_OK(c, cudaMemcpyAsync(d_states + (size_t)k * n, c->d_harvest + (size_t)k * c->harvest_cap, n * sizeof(double),
+                               cudaMemcpyDeviceToDevice, c->stream));
+  CUDA_OK(c, cudaMemsetAsync(c->d_harvest_n, 0, sizeof(unsigned long long), c->stream));
+  CUDA_OK(c, cudaStreamSynchronize(c->stream));
+  *n_out = n;
+  return 0;
+}

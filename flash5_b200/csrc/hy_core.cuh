@@ -35,13 +35,20 @@ struct DevParams {
   double lim_beta, gamma, gam1inv, ggprodinv, abar, smalle, smlrho, eswitch, tiny, cfl;
   double del[3];
   double dt;
+  const double *dt_dev;       // when set, dt is read from device memory (graph-replayed steps)
   const int *blk_at;          // block index at block coordinates
   const int *blk_coord;       // 3 ints per block
   const int *blk_list;        // optional list of blocks to update (NULL = all)
   const double *s_in[5];      // dens, velx, vely, velz, eint (block-major SoA)
   double *s_out[5];
   unsigned *status;
-  const float *mlp;           // learned-guess network weights (exact solver)
+  const void *mlp;            // learned-guess network, xrs::MlpPacked (exact solver; NULL = off)
+  double *harvest;            // optional face-state sample, [7][harvest_cap] (dl,ul,pl,dr,ur,pr,gamma)
+  unsigned long long *harvest_n;
+  long long harvest_cap;
+  unsigned harvest_mask;      // a face is kept when its hash & mask == 0
+  double rs_tol;              // exact solver: relative tolerance of p*
+  int rs_max_iter;
 };
 
 template <class R> __device__ __forceinline__ R rmax(R a, R b) { return a > b ? a : b; }

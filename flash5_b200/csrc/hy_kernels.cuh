@@ -17,6 +17,7 @@
 // time step per block.
 #pragma once
 #include "hy_core.cuh"
+#include "exact_rs.cuh"
 #include <float.h>
 
 namespace fhy {
@@ -205,13 +206,51 @@ __device__ void cfl_block_reduce(CflCand c, int blk, double cfl, CflPart *part) 
 }
 
 // ---------------------------------------------------------------------------
+// exact Riemann face flux (no FLASH5 counterpart; Toro ch. 4, exact_rs.cuh)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ xrs::Side side_of(const double *V, int n, double g, unsigned &st) {
+  const double c2 = g * V[HP] / V[HD];
+  if (!(c2 > 0.0)) st |= ST_NEG_SOUND;
+  return xrs::Side{V[HD], V[n], V[HP], sqrt(c2)};
+}
+
+// keep a hashed sample of the face states (two-rarefaction guess inexact) for
+// training the learned guess
+__device__ __forceinline__ void harvest_face(const DevParams &P, const xrs::Side &L, const xrs::Side &R, double g,
+                                             unsigned key) {
+  unsigned h = key * 2654435761u;
+  h ^= h >> 15; h *= 2246822519u; h ^= h >> 13;
+  if (h & P.harvest_mask) return;
+  const unsigned long long k = atomicAdd(P.harvest_n, 1ull);
+  if ((long long)k >= P.harvest_cap) return;
+  const long long c = P.harvest_cap;
+  double *S = P.harvest;
+  S[k] = L.d; S[c + k] = L.u; S[2 * c + k] = L.p;
+  S[3 * c + k] = R.d; S[4 * c + k] = R.u; S[5 * c + k] = R.p; S[6 * c + k] = g;
+}
+
+// Godunov flux from the exact solution with the two-rarefaction guess
+template <int DIR>
+__device__ __forceinline__ void exact_face(const DevParams &P, const double *VL, const double *VR, double F[6],
+                                           unsigned &st) {
+  const double g = P.gamma;
+  const xrs::Side L = side_of(VL, DIR, g, st), R = side_of(VR, DIR, g, st);
+  const bool vac = xrs::vacuum(L, R, g);
+  double ps = 0.0, us = 0.5 * (L.u + R.u);
+  if (!vac && xrs::newton(L, R, g, xrs::tr_guess(L, R, g), P.rs_tol, P.rs_max_iter, ps, us, xrs::strong_waves(L, R)) < 0)
+    st |= ST_NEWTON;
+  xrs::godunov_flux<DIR>(VL, VR, L, R, g, ps, us, vac, F);
+}
+
+// ---------------------------------------------------------------------------
 // k_dir: one direction of the unsplit update for one block per CTA.
 //   phase 1: face states W-/W+ of the line cells (c_DIR in [-1, N], other
 //            coordinates interior) -- PPM (hy_dataReconstOneStep.F90:485-
 //            716), transverse corrections (:918-951), last negativity
 //            check (:1120-1154), 3D full-CTU cross terms and positivity
 //            fallback (hy_getRiemannState.F90:956-1313)
-//   phase 2: HLLC at the N+1 faces of every line plus the auxiliary
+//   phase 2: HLLC (RS = 0) or the exact solver (RS = 1) at the N+1 faces
+//            of every line plus the auxiliary
 //            internal-energy and volume fluxes (hy_getFaceFlux.F90:283-442)
 //   phase 3: accumulation of the conservative update in direction order
 //            x, y, z (updateConservedVariable, hy_unsplitUpdate.F90:1187-
@@ -240,7 +279,7 @@ struct DirGeom {
 // slots stored for the face states: dens, velx, vely, velz, pres, game, eint
 __device__ __forceinline__ int wslot(int q) { return q < 5 ? q : q + 1; }
 
-template <int NDIM, int NX, int NY, int NZ, class R, int DIR, bool FIRST, bool LAST, int VAR>
+template <int NDIM, int NX, int NY, int NZ, class R, int DIR, bool FIRST, bool LAST, int VAR, int RS>
 __global__ void __launch_bounds__(320) k_dir(const DevParams P, const R *__restrict__ SIG, double *__restrict__ ACC,
                                              double *__restrict__ AUX, size_t ncells, CflPart *part) {
   using G = DirGeom<NDIM, NX, NY, NZ, R, DIR>;
@@ -253,7 +292,7 @@ __global__ void __launch_bounds__(320) k_dir(const DevParams P, const R *__restr
   const int b = P.blk_list ? P.blk_list[blockIdx.x] : blockIdx.x;
   const int3 bc = blk_coords(P, b);
   unsigned st = 0;
-  const double dt = P.dt;
+  const double dt = P.dt_dev ? *P.dt_dev : P.dt;
   const double delta = P.del[DIR - 1];
   const R dtn = R(dt / delta);
   const R hdtx = R(0.5 * dt / P.del[0]), hdty = R(0.5 * dt / P.del[1]), hdtz = R(0.5 * dt / P.del[2]);
@@ -372,7 +411,8 @@ __global__ void __launch_bounds__(320) k_dir(const DevParams P, const R *__restr
     }
     VL[HGC] = gam; VR[HGC] = gam;
     R F[6];
-    hllc<R, DIR>(P, VL, VR, F, st);
+    if constexpr (RS == 1) exact_face<DIR>(P, VL, VR, F, st);
+    else hllc<R, DIR>(P, VL, VR, F, st);
 #pragma unroll
     for (int n = 0; n < 6; ++n) sF[n * G::n + t] = F[n];
     R fv = R(0), fe = R(0);

@@ -15,6 +15,7 @@ struct StepArgs {
   int nlaunch;        // CTAs (blocks updated)
   int threads;        // threads per CTA
   cudaStream_t stream;
+  bool set_attr;      // raise the kernels' dynamic shared-memory limit (not while capturing a graph)
 };
 
 // Enqueue one hydro step; returns the number of kernel launches, or -1 for an

@@ -76,7 +76,7 @@ __device__ __forceinline__ void hllc_fp64(const DevParams &P, const double *Vm, 
   for (int n = 0; n < 5; ++n) Fs[n] = F[n] + S * (UC[n] - U[n]);
 }
 
-template <int NDIM, int NX, int NY, int NZ, int DIR>
+template <int NDIM, int NX, int NY, int NZ, int DIR, int RS = 0>
 struct MxGeom {
   static constexpr int ND = DIR == 1 ? NX : (DIR == 2 ? NY : NZ);
   static constexpr int C = DIR == 1 ? NY * NZ : (DIR == 2 ? NX * NZ : NX * NY);   // lines
@@ -96,8 +96,13 @@ struct MxGeom {
   }
   // shared memory: staged prims (FP64), then a region used first for the
   // reconstruction scratch and then for the face fluxes
+  // (with the exact solver the slope scratch, dead during the Riemann
+  // phase, also holds the learned-guess network, so it is at least that big)
   static constexpr size_t prim_bytes = (size_t)6 * SA * 8;
-  static constexpr size_t recon_bytes = (size_t)SB * 4 + (size_t)SB * 6 * 4 + (size_t)2 * SC * 6 * 4 + (size_t)SC * 8;
+  static constexpr size_t slope_bytes = (size_t)SB * 4 + (size_t)SB * 6 * 4;
+  static constexpr size_t wp_off =
+      (RS == 1 && slope_bytes < sizeof(xrs::MlpPacked)) ? sizeof(xrs::MlpPacked) : slope_bytes;
+  static constexpr size_t recon_bytes = wp_off + (size_t)2 * SC * 6 * 4 + (size_t)SC * 8;
   static constexpr size_t flux_bytes = (size_t)SC * 9 * 8;
   static constexpr size_t smem_bytes() { return prim_bytes + (recon_bytes > flux_bytes ? recon_bytes : flux_bytes); }
 };
@@ -106,11 +111,11 @@ template <int NDIM, int NX, int NY, int NZ> struct MxThreads {
   static constexpr int n = NDIM == 3 ? 320 : (NX == 8 ? 96 : 288);
 };
 
-template <int NDIM, int NX, int NY, int NZ, int DIR, bool FIRST, bool LAST>
+template <int NDIM, int NX, int NY, int NZ, int DIR, bool FIRST, bool LAST, int RS>
 __global__ void __launch_bounds__(MxThreads<NDIM, NX, NY, NZ>::n, NDIM == 3 ? 2 : 1)
 k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ ACC, double *__restrict__ AUX,
          size_t ncells, CflPart *part) {
-  using G = MxGeom<NDIM, NX, NY, NZ, DIR>;
+  using G = MxGeom<NDIM, NX, NY, NZ, DIR, RS>;
   using B = Box<NDIM, NX, NY, NZ>;
   constexpr int NCB = NX * NY * NZ;
   constexpr int NT = MxThreads<NDIM, NX, NY, NZ>::n;
@@ -121,7 +126,7 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
   unsigned char *reg = smem_raw + G::prim_bytes;
   float *sFlat = reinterpret_cast<float *>(reg);                          // [SB]
   float *sDb = sFlat + G::SB;                                             // [6][SB]
-  float *sWp = sDb + 6 * G::SB;                                           // [6][SC] increments
+  float *sWp = reinterpret_cast<float *>(reg + G::wp_off);                // [6][SC] increments
   float *sWm = sWp + 6 * G::SC;                                           // [6][SC]
   double *sIg = reinterpret_cast<double *>(sWm + 6 * G::SC);              // [SC] 1/(game-1)
   double *sF = reinterpret_cast<double *>(reg);                           // [9][SC] (after phase D)
@@ -129,7 +134,7 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
   const int b = P.blk_list ? P.blk_list[blockIdx.x] : blockIdx.x;
   const int3 bc = blk_coords(P, b);
   unsigned st = 0;
-  const double dt = P.dt, delta = P.del[DIR - 1];
+  const double dt = P.dt_dev ? *P.dt_dev : P.dt, delta = P.del[DIR - 1];
   const float dtn = float(dt / delta), hdtn = 0.5f * dtn;
   const float hdtx = float(0.5 * dt / P.del[0]), hdty = float(0.5 * dt / P.del[1]), hdtz = float(0.5 * dt / P.del[2]);
   const float *sigb = SIG + (size_t)blockIdx.x * NDIM * 6 * B::n;
@@ -358,6 +363,122 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
 
   // ---- D: Riemann problems at the faces, FP64
   double Fr[NIT][9];
+  if constexpr (RS == 1) {
+    // exact solver.  With a network attached, pass 1 evaluates its
+    // tensor-core guess for the faces with strong waves (the network sits
+    // over the slope scratch, dead from here on) and leaves the start value
+    // in sP0 (over the unused 1/(game-1) array; negative = network start,
+    // limited to three evaluations; 0 = two-rarefaction start); pass 2 runs
+    // Newton and the Godunov flux.  Each thread reads back only its own
+    // entries.
+    double *sP0 = sIg;
+    const bool learned = P.mlp != nullptr;
+    const double g = P.gamma;
+    auto face = [&](int qq, bool left, int s, int t) -> double {
+      return left ? Vs(qq, s - G::step) + double(sWp[qq * G::SC + t - G::step])
+                  : Vs(qq, s) + double(sWm[qq * G::SC + t]);
+    };
+    auto sides = [&](int s, int t, xrs::Side &L, xrs::Side &R) {
+      const double dl = face(0, true, s, t), ul = face(DIR, true, s, t), pl = face(4, true, s, t);
+      const double dr = face(0, false, s, t), ur = face(DIR, false, s, t), pr = face(4, false, s, t);
+      const double c2l = g * pl / dl, c2r = g * pr / dr;
+      if (!(c2l > 0.0) || !(c2r > 0.0)) st |= ST_NEG_SOUND;
+      L = xrs::Side{dl, ul, pl, sqrt(c2l)};
+      R = xrs::Side{dr, ur, pr, sqrt(c2r)};
+    };
+    if (learned) {
+      // pass 1a: faces with strong waves and an inexact two-rarefaction
+      // guess get sP0 = p_TR > 0, all others 0 (two-rarefaction start)
+      int need = 0;
+#pragma unroll
+      for (int it = 0; it < NIT; ++it) {
+        const int t = threadIdx.x + it * NT;
+        if (t >= G::SC) break;
+        int x, l;
+        G::dec(t, G::LC, 1, x, l);
+        if (x < 0) continue;
+        xrs::Side L, R;
+        sides(G::at(x, l, G::L4, 4), t, L, R);
+        double q = 0.0;
+        if (!xrs::vacuum(L, R, g) && xrs::strong_waves(L, R)) {
+          const double ptr = xrs::tr_guess(L, R, g);
+          if (!xrs::tr_exact(L, R, ptr)) q = ptr;
+        }
+        sP0[t] = q;
+        need |= q > 0.0;
+      }
+      // pass 1b: the network's start for those faces (negative: limited to
+      // three evaluations); skipped by CTAs and warps without such faces
+      if (__syncthreads_or(need)) {
+        xrs::MlpPacked *sM = reinterpret_cast<xrs::MlpPacked *>(reg);
+        xrs::load_packed(*sM, static_cast<const xrs::MlpPacked *>(P.mlp));
+        __syncthreads();
+#pragma unroll
+        for (int it = 0; it < NIT; ++it) {
+          const int t = threadIdx.x + it * NT;
+          if (t - (int)(threadIdx.x & 31) >= G::SC) break;    // warp-uniform: NT is a multiple of 32
+          int x = -1, l = 0;
+          if (t < G::SC) G::dec(t, G::LC, 1, x, l);
+          const double q = (t < G::SC && x >= 0) ? sP0[t] : 0.0;
+          const bool net = q > 0.0;
+          if (!__any_sync(0xffffffffu, net)) continue;
+          xrs::Side L{1.0, 0.0, 1.0, 1.0}, R{1.0, 0.0, 1.0, 1.0};
+          if (net) sides(G::at(x, l, G::L4, 4), t, L, R);
+          float f[xrs::NIN];
+          if (net) xrs::features(L, R, g, q, f);
+          else {
+#pragma unroll
+            for (int k = 0; k < xrs::NIN; ++k) f[k] = 0.f;
+          }
+          const float y = fminf(fmaxf(xrs::mlp_lane(*sM, f), -20.f), 20.f);
+          if (net) sP0[t] = -(q * (double)expf(y));
+        }
+      }
+    }
+#pragma unroll
+    for (int it = 0; it < NIT; ++it) {
+      const int t = threadIdx.x + it * NT;
+      if (t >= G::SC) break;
+      int x, l;
+      G::dec(t, G::LC, 1, x, l);
+      if (x < 0) continue;
+      const int s = G::at(x, l, G::L4, 4);
+      xrs::Side L, R;
+      sides(s, t, L, R);
+      const bool vac = xrs::vacuum(L, R, g);
+      double ps = 0.0, us = 0.5 * (L.u + R.u);
+      if (!vac) {
+        const double q = learned ? sP0[t] : 0.0;
+        const double p0 = q < 0.0 ? -q : xrs::tr_guess(L, R, g);
+        const bool strong = xrs::strong_waves(L, R);
+        int k = xrs::newton(L, R, g, p0, P.rs_tol, q < 0.0 ? 3 : P.rs_max_iter, ps, us, q >= 0.0 && strong);
+        if (k < 0 && q < 0.0)
+          k = xrs::newton(L, R, g, xrs::tr_guess(L, R, g), P.rs_tol, P.rs_max_iter, ps, us, strong);
+        if (k < 0) st |= ST_NEWTON;
+        if (P.harvest && (q < 0.0 || (strong && !xrs::tr_exact(L, R, p0))))
+          harvest_face(P, L, R, g, (unsigned)(blockIdx.x * 4 + DIR) * 2048u + (unsigned)t);
+      }
+      double VL[8], VR[8];
+#pragma unroll
+      for (int qq = 0; qq < 6; ++qq) {
+        const int n = qq < 5 ? qq : HEI;
+        VL[n] = face(qq, true, s, t);
+        VR[n] = face(qq, false, s, t);
+      }
+      double F[6];
+      xrs::godunov_flux<DIR>(VL, VR, L, R, g, ps, us, vac, F);
+#pragma unroll
+      for (int n = 0; n < 6; ++n) Fr[it][n] = F[n];
+      double fv = 0., fe = 0.;
+      if (P.use_aux_eint) {
+        if (F[FDENS] > 0.) { fv = F[FDENS] / VL[HD]; fe = F[FDENS] * VL[HEI]; }
+        else { fv = F[FDENS] / VR[HD]; fe = F[FDENS] * VR[HEI]; }
+      }
+      Fr[it][FEINT] = fe;
+      Fr[it][FVOLU] = fv;
+      Fr[it][8] = (Vs(4, s) + double(sWm[4 * G::SC + t])) + (Vs(4, s) + double(sWp[4 * G::SC + t]));
+    }
+  } else {
 #pragma unroll
   for (int it = 0; it < NIT; ++it) {
     const int t = threadIdx.x + it * NT;
@@ -387,6 +508,7 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
     Fr[it][FVOLU] = fv;
     // N05 + P05 of this cell (n+1/2 pressure sum)
     Fr[it][8] = (Vs(4, s) + double(sWm[4 * G::SC + t])) + (Vs(4, s) + double(sWp[4 * G::SC + t]));
+  }
   }
   __syncthreads();
 #pragma unroll

@@ -4,6 +4,7 @@
 //   FHY_VARIANT=2  FP64 with FMA contraction
 //   FHY_VARIANT=3  FP32 reconstruction / Riemann solve, FP64 update
 #include "hy_launch.h"
+#include "../../include/flash_hy.h"
 #if FHY_VARIANT == 3
 #include "hy_mixed.cuh"
 #endif
@@ -21,35 +22,44 @@ typedef double Real;
 
 namespace fhy {
 
-template <int NDIM, int NX, int NY, int NZ, int DIR, bool FIRST, bool LAST>
+template <int NDIM, int NX, int NY, int NZ, int DIR, bool FIRST, bool LAST, int RS>
 static bool launch_dir(const StepArgs &a) {
 #if FHY_VARIANT == 3
-  using G = MxGeom<NDIM, NX, NY, NZ, DIR>;
-  auto kern = k_dir_mx<NDIM, NX, NY, NZ, DIR, FIRST, LAST>;
+  using G = MxGeom<NDIM, NX, NY, NZ, DIR, RS>;
+  auto kern = k_dir_mx<NDIM, NX, NY, NZ, DIR, FIRST, LAST, RS>;
   const int threads = MxThreads<NDIM, NX, NY, NZ>::n;
 #else
   using G = DirGeom<NDIM, NX, NY, NZ, Real, DIR>;
-  auto kern = k_dir<NDIM, NX, NY, NZ, Real, DIR, FIRST, LAST, FHY_VARIANT>;
+  auto kern = k_dir<NDIM, NX, NY, NZ, Real, DIR, FIRST, LAST, FHY_VARIANT, RS>;
   const int threads = a.threads;
 #endif
   const size_t smem = G::smem_bytes();
-  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return false;
+  if (a.set_attr && cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return false;
   kern<<<a.nlaunch, threads, smem, a.stream>>>(a.P, (const Real *)a.sig, a.acc, a.aux, a.ncells, a.part);
   return cudaGetLastError() == cudaSuccess;
 }
 
-template <int NDIM, int NX, int NY, int NZ>
-static int run(const StepArgs &a) {
+// RS: 0 = HLLC, 1 = exact Riemann solver
+template <int NDIM, int NX, int NY, int NZ, int RS>
+static int run_rs(const StepArgs &a) {
   k_sig<NDIM, NX, NY, NZ, Real, FHY_VARIANT><<<a.nlaunch, a.threads, 0, a.stream>>>(a.P, (Real *)a.sig);
   if (cudaGetLastError() != cudaSuccess) return -2;
-  bool ok;
-  if (NDIM == 2) {
-    ok = launch_dir<NDIM, NX, NY, NZ, 1, true, false>(a) && launch_dir<NDIM, NX, NY, NZ, 2, false, true>(a);
+  if constexpr (NDIM == 2) {
+    const bool ok =
+        launch_dir<NDIM, NX, NY, NZ, 1, true, false, RS>(a) && launch_dir<NDIM, NX, NY, NZ, 2, false, true, RS>(a);
     return ok ? 3 : -2;
+  } else {
+    const bool ok = launch_dir<NDIM, NX, NY, NZ, 1, true, false, RS>(a) &&
+                    launch_dir<NDIM, NX, NY, NZ, 2, false, false, RS>(a) &&
+                    launch_dir<NDIM, NX, NY, NZ, 3, false, true, RS>(a);
+    return ok ? 4 : -2;
   }
-  ok = launch_dir<NDIM, NX, NY, NZ, 1, true, false>(a) && launch_dir<NDIM, NX, NY, NZ, 2, false, false>(a) &&
-       launch_dir<NDIM, NX, NY, NZ, 3, false, true>(a);
-  return ok ? 4 : -2;
+}
+
+template <int NDIM, int NX, int NY, int NZ>
+static int run(const StepArgs &a) {
+  return a.P.riemann == FLASH_HY_RS_EXACT ? run_rs<NDIM, NX, NY, NZ, 1>(a) : run_rs<NDIM, NX, NY, NZ, 0>(a);
 }
 
 int FHY_ENTRY(const StepArgs &a, int ndim, int nx, int ny, int nz) {

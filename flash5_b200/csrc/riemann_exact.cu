@@ -1,25 +1,17 @@
-// riemann_exact.cu -- exact ideal-gas Riemann solver with a learned initial
-// guess for the star pressure (no counterpart in FLASH5, whose unsplit path
-// only has approximate solvers, hy_getFaceFlux.F90:324-372).
+// riemann_exact.cu -- batched isolated exact Riemann solves with a learned
+// initial guess for the star pressure, and the hand-written training of that
+// guess (no counterpart in FLASH5, whose unsplit path only has approximate
+// solvers, hy_getFaceFlux.F90:324-372).  The solver itself (Toro ch. 4) and
+// the tensor-core network inference live in exact_rs.cuh, shared with the
+// hydro face fluxes.
 //
-// Method: E. F. Toro, "Riemann Solvers and Numerical Methods for Fluid
-// Dynamics", 3rd ed., ch. 4 -- pressure functions f_K(p) (eqs. 4.6-4.7),
-// two-rarefaction guess (eq. 4.46), Newton iteration on
-// f(p) = f_L(p) + f_R(p) + (u_R - u_L) = 0.  Newton is kept inside a bracket
-// [pa, pb] with f(pa) < 0 < f(pb), so every solve terminates within
-// max_iter; steps leaving the bracket are replaced by bisection.
-//
-// The learned guess is an 8-64-64-1 MLP with BF16 weights and activations
-// and FP32 accumulation, evaluated on the tensor cores with warp-level
-// mma.sync (m16n8k16).  It predicts ln(p*/p_TR) from eight scale-free
-// features of the two states; Newton starts from p_TR*exp(y).  If that
-// Newton run does not converge within three evaluations, the solve restarts
-// from the two-rarefaction guess (fallback), so the converged p* never
-// depends on the network.
+// Learned path: Newton gets three evaluations from the network's guess; if
+// that does not converge, the solve restarts from the two-rarefaction guess
+// (fallback), so the converged p* never depends on the network.
 //
 // Training: hand-written FP32 forward/backward kernels (mean-squared error
 // on ln(p*/p_TR)) and an Adam update, on interface states harvested from
-// the solver's own runs.
+// the solver's own runs (isolated solves or hydro face states).
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
 #include <stdint.h>
@@ -28,221 +20,15 @@
 #include <stdlib.h>
 #include <string.h>
 #include "../../include/flash_hy.h"
+#include "exact_rs.cuh"
 
 namespace rx {
 
-constexpr int NIN = 8, NH = 64;
-// parameter layout (FP32 master copy): W1[64][8], b1[64], W2[64][64], b2[64], w3[64], b3
-constexpr int OFF_W1 = 0, OFF_B1 = OFF_W1 + NH * NIN, OFF_W2 = OFF_B1 + NH, OFF_B2 = OFF_W2 + NH * NH,
-              OFF_W3 = OFF_B2 + NH, OFF_B3 = OFF_W3 + NH, NPARAM = OFF_B3 + 1;
-
-// ---------------------------------------------------------------------------
-// pressure functions and the star state
-// ---------------------------------------------------------------------------
-struct Side { double d, u, p, c; };
-
-__device__ __forceinline__ void pres_fn(double p, const Side &s, double g, double &f, double &fd) {
-  if (p <= s.p) {
-    double prat = p / s.p;
-    double ex = (g - 1.0) / (2.0 * g);
-    double q = pow(prat, ex);
-    f = 2.0 * s.c / (g - 1.0) * (q - 1.0);
-    fd = q / (prat * s.d * s.c);                  // (p/pK)^(-(g+1)/2g) / (dK cK)
-  } else {
-    double A = 2.0 / ((g + 1.0) * s.d);
-    double B = (g - 1.0) / (g + 1.0) * s.p;
-    double q = sqrt(A / (B + p));
-    f = (p - s.p) * q;
-    fd = (1.0 - 0.5 * (p - s.p) / (B + p)) * q;
-  }
-}
-
-__device__ __forceinline__ double tr_guess(const Side &L, const Side &R, double g) {
-  double z = (g - 1.0) / (2.0 * g);
-  double num = L.c + R.c - 0.5 * (g - 1.0) * (R.u - L.u);
-  if (num <= 0.0) return 0.0;
-  return pow(num / (L.c / pow(L.p, z) + R.c / pow(R.p, z)), 1.0 / z);
-}
-
-// Bracketed Newton from p0.  Converged when the Newton step is below
-// tol * p or, in the quadratic regime, when the predicted next step is below
-// tol * p / 100; the returned count is the number of function evaluations.  Steps
-// leaving [pa, pb] are replaced by a geometric (pa > 0) or decimating
-// (pa = 0, near vacuum) bisection.  Returns -max_iter when not converged.
-__device__ __forceinline__ int newton(const Side &L, const Side &R, double g, double p0, double tol, int max_iter,
-                                      double &pout) {
-  double du = R.u - L.u;
-  double fl, fdl, fr, fdr;
-  double pa = 0.0, pb = fmax(L.p, R.p);
-  for (int k = 0; k < 200; ++k) {
-    pres_fn(pb, L, g, fl, fdl); pres_fn(pb, R, g, fr, fdr);
-    if (fl + fr + du > 0.0) break;
-    pa = pb;
-    pb *= 4.0;
-  }
-  double p = (p0 > pa && p0 < pb) ? p0 : (pa > 0.0 ? sqrt(pa * pb) : 0.5 * pb);
-  double prev = -1.0;                 // previous Newton step (-1: none / bisection)
-  for (int it = 0; it < max_iter; ++it) {
-    pres_fn(p, L, g, fl, fdl); pres_fn(p, R, g, fr, fdr);
-    double f = fl + fr + du;
-    if (f == 0.0) { pout = p; return it + 1; }
-    if (f < 0.0) pa = p; else pb = p;
-    double step = f / (fdl + fdr);
-    double pn = p - step;
-    double as = fabs(step);
-    bool inside = pn > pa && pn < pb;
-    // converged: the step itself is below tol, or -- once the last two
-    // steps show the quadratic regime -- the predicted next step
-    // |step|^3 / prev^2 is below tol/100
-    if (as <= tol * p || (inside && prev > 0.0 && as < prev && as * (as / prev) * (as / prev) <= 0.01 * tol * p)) {
-      pout = (pn > 0.0) ? pn : p;
-      return it + 1;
-    }
-    if (!inside) { pn = pa > 0.0 ? sqrt(pa * pb) : 0.01 * pb; prev = -1.0; }
-    else prev = as;
-    p = pn;
-  }
-  pout = p;
-  return -max_iter;
-}
-
-__device__ __forceinline__ double star_u(const Side &L, const Side &R, double g, double p) {
-  double fl, fdl, fr, fdr;
-  pres_fn(p, L, g, fl, fdl); pres_fn(p, R, g, fr, fdr);
-  return 0.5 * (L.u + R.u) + 0.5 * (fr - fl);
-}
-
-// ---------------------------------------------------------------------------
-// features (scale free, ~O(1)); target = ln(p*/p_TR)
-// ---------------------------------------------------------------------------
-// Computed in FP32: the network needs about three significant digits.
-__device__ __forceinline__ void features(const Side &L, const Side &R, double g, double ptr, float f[NIN]) {
-  const float i4 = 1.0f / 9.2103404f, i3 = 1.0f / 6.9077553f;   // 1/ln(1e4), 1/ln(1e3)
-  const float dl = float(L.d), dr = float(R.d), pl = float(L.p), pr = float(R.p);
-  const float ul = float(L.u), ur = float(R.u), cl = float(L.c), cr = float(R.c), gf = float(g);
-  const float du = ur - ul;
-  // two-shock estimate (Toro eq. 4.47) around the PVRS pressure
-  float ppv = fmaxf(0.5f * (pl + pr) - 0.125f * du * (dl + dr) * (cl + cr), 1e-6f * fminf(pl, pr));
-  float gL = sqrtf(2.0f / ((gf + 1.0f) * dl) / (ppv + (gf - 1.0f) / (gf + 1.0f) * pl));
-  float gR = sqrtf(2.0f / ((gf + 1.0f) * dr) / (ppv + (gf - 1.0f) / (gf + 1.0f) * pr));
-  float pts = fmaxf((gL * pl + gR * pr - du) / (gL + gR), 1e-30f);
-  float ptrf = float(ptr);
-  f[0] = logf(pr / pl) * i4;
-  f[1] = logf(dr / dl) * i3;
-  f[2] = ul / cl * 0.2f;
-  f[3] = ur / cr * 0.2f;
-  f[4] = (gf - 1.5333333f) * 7.5f;
-  f[5] = du / (cl + cr);
-  f[6] = logf(ptrf / pl) * i4;
-  f[7] = logf(pts / ptrf) * i4;
-}
-
-// The two-rarefaction guess is the exact root when it does not exceed
-// min(p_L, p_R) (both waves are rarefactions, Toro section 4.3.2).
-__device__ __forceinline__ bool tr_exact(const Side &L, const Side &R, double ptr) { return ptr <= fmin(L.p, R.p); }
-
-// ---------------------------------------------------------------------------
-// tensor-core MLP inference for the 32 interfaces of a warp
-// ---------------------------------------------------------------------------
-struct MlpSmem {
-  __nv_bfloat16 W1[NH][16];      // K padded 8 -> 16
-  __nv_bfloat16 W2[NH][NH];
-  float b1[NH], b2[NH], w3[NH], b3;
-};
-
-__device__ __forceinline__ void mma_bf16(float d[4], const uint32_t a[4], const uint32_t b[2]) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-      "{%0,%1,%2,%3};\n"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
-}
-__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
-  __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
-  return *reinterpret_cast<uint32_t *>(&v);
-}
-
-// xin: this warp's feature rows in shared memory, [32][16] bf16 (cols 8..15
-// zero).  Returns y for row (lane) through yout[32] in shared memory.
-__device__ void mlp_warp(const MlpSmem &M, const __nv_bfloat16 (*xin)[16], float *yout) {
-  const int lane = threadIdx.x & 31, r = lane >> 2, q = lane & 3;
-#pragma unroll
-  for (int tile = 0; tile < 2; ++tile) {
-    const int row0 = tile * 16;
-    // layer 1: [16 x 16] x [16 x 64]
-    uint32_t a[4];
-    a[0] = *reinterpret_cast<const uint32_t *>(&xin[row0 + r][2 * q]);
-    a[1] = *reinterpret_cast<const uint32_t *>(&xin[row0 + r + 8][2 * q]);
-    a[2] = *reinterpret_cast<const uint32_t *>(&xin[row0 + r][2 * q + 8]);
-    a[3] = *reinterpret_cast<const uint32_t *>(&xin[row0 + r + 8][2 * q + 8]);
-    float h1[8][4];
-#pragma unroll
-    for (int nt = 0; nt < 8; ++nt) {
-      uint32_t bb[2];
-      bb[0] = *reinterpret_cast<const uint32_t *>(&M.W1[nt * 8 + r][2 * q]);
-      bb[1] = *reinterpret_cast<const uint32_t *>(&M.W1[nt * 8 + r][2 * q + 8]);
-      h1[nt][0] = h1[nt][1] = h1[nt][2] = h1[nt][3] = 0.f;
-      mma_bf16(h1[nt], a, bb);
-      // bias + relu; columns of this thread: nt*8 + 2q, +1
-      float c0 = M.b1[nt * 8 + 2 * q], c1 = M.b1[nt * 8 + 2 * q + 1];
-      h1[nt][0] = fmaxf(h1[nt][0] + c0, 0.f); h1[nt][1] = fmaxf(h1[nt][1] + c1, 0.f);
-      h1[nt][2] = fmaxf(h1[nt][2] + c0, 0.f); h1[nt][3] = fmaxf(h1[nt][3] + c1, 0.f);
-    }
-    // layer 2: [16 x 64] x [64 x 64]; the C fragments of layer 1 are the A
-    // fragments of layer 2 (k-step kk = n-tiles 2kk and 2kk+1)
-    float h2[8][4];
-#pragma unroll
-    for (int nt = 0; nt < 8; ++nt) h2[nt][0] = h2[nt][1] = h2[nt][2] = h2[nt][3] = 0.f;
-#pragma unroll
-    for (int kk = 0; kk < 4; ++kk) {
-      uint32_t a2[4];
-      a2[0] = pack_bf16(h1[2 * kk][0], h1[2 * kk][1]);
-      a2[1] = pack_bf16(h1[2 * kk][2], h1[2 * kk][3]);
-      a2[2] = pack_bf16(h1[2 * kk + 1][0], h1[2 * kk + 1][1]);
-      a2[3] = pack_bf16(h1[2 * kk + 1][2], h1[2 * kk + 1][3]);
-#pragma unroll
-      for (int nt = 0; nt < 8; ++nt) {
-        uint32_t bb[2];
-        bb[0] = *reinterpret_cast<const uint32_t *>(&M.W2[nt * 8 + r][kk * 16 + 2 * q]);
-        bb[1] = *reinterpret_cast<const uint32_t *>(&M.W2[nt * 8 + r][kk * 16 + 2 * q + 8]);
-        mma_bf16(h2[nt], a2, bb);
-      }
-    }
-    // layer 3 on the CUDA cores: y = relu(h2 + b2) . w3 + b3
-    float y0 = 0.f, y1 = 0.f;
-#pragma unroll
-    for (int nt = 0; nt < 8; ++nt) {
-      int c = nt * 8 + 2 * q;
-      float v0 = __bfloat162float(__float2bfloat16(fmaxf(h2[nt][0] + M.b2[c], 0.f)));
-      float v1 = __bfloat162float(__float2bfloat16(fmaxf(h2[nt][1] + M.b2[c + 1], 0.f)));
-      float v2 = __bfloat162float(__float2bfloat16(fmaxf(h2[nt][2] + M.b2[c], 0.f)));
-      float v3 = __bfloat162float(__float2bfloat16(fmaxf(h2[nt][3] + M.b2[c + 1], 0.f)));
-      y0 += v0 * M.w3[c] + v1 * M.w3[c + 1];
-      y1 += v2 * M.w3[c] + v3 * M.w3[c + 1];
-    }
-    y0 += __shfl_xor_sync(0xffffffffu, y0, 1); y0 += __shfl_xor_sync(0xffffffffu, y0, 2);
-    y1 += __shfl_xor_sync(0xffffffffu, y1, 1); y1 += __shfl_xor_sync(0xffffffffu, y1, 2);
-    if (q == 0) { yout[row0 + r] = y0 + M.b3; yout[row0 + r + 8] = y1 + M.b3; }
-  }
-  __syncwarp();
-}
-
-__device__ void load_mlp(MlpSmem &M, const float *__restrict__ w) {
-  for (int t = threadIdx.x; t < NH * 16; t += blockDim.x) {
-    int n = t / 16, k = t % 16;
-    M.W1[n][k] = __float2bfloat16(k < NIN ? w[OFF_W1 + n * NIN + k] : 0.f);
-  }
-  for (int t = threadIdx.x; t < NH * NH; t += blockDim.x) M.W2[t / NH][t % NH] = __float2bfloat16(w[OFF_W2 + t]);
-  for (int t = threadIdx.x; t < NH; t += blockDim.x) {
-    M.b1[t] = w[OFF_B1 + t]; M.b2[t] = w[OFF_B2 + t]; M.w3[t] = w[OFF_W3 + t];
-  }
-  if (threadIdx.x == 0) M.b3 = w[OFF_B3];
-  __syncthreads();
-}
+using namespace xrs;
 
 // ---------------------------------------------------------------------------
 // isolated solves: states[7][n] = (dl, ul, pl, dr, ur, pr, gamma)
-// out[2][n] = (p*, u*); iters[n] = Newton iterations (incl. fallback);
+// out[2][n] = (p*, u*); iters[n] = Newton evaluations (incl. fallback);
 // flags bit0: fell back to the two-rarefaction guess, bit1: vacuum,
 // bit2: not converged
 // ---------------------------------------------------------------------------
@@ -255,20 +41,22 @@ __device__ __forceinline__ void load_state(const double *__restrict__ S, long n,
   L.c = sqrt(g * L.p / L.d); R.c = sqrt(g * R.p / R.d);
 }
 
-// learned != 0: Newton gets three evaluations from the network's guess
-// (or from the two-rarefaction guess where that guess is exact); lanes that
-// have not converged are appended to `queue` (warp-aggregated atomics) and
-// re-solved from the two-rarefaction guess by k_fallback, so no warp waits
-// for a fallback lane.
-__global__ void __launch_bounds__(SOLVE_THREADS) k_solve(const double *__restrict__ S, long n, double *__restrict__ out,
-                                                         unsigned char *__restrict__ iters, unsigned char *__restrict__ flags,
-                                                         const float *__restrict__ w, int learned, double tol,
-                                                         int max_iter, int *queue, int *qcount, unsigned *status) {
-  __shared__ MlpSmem M;
-  __shared__ __align__(16) __nv_bfloat16 X[SOLVE_THREADS / 32][32][16];
-  __shared__ float Y[SOLVE_THREADS / 32][32];
-  if (learned) load_mlp(M, w);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+// learned != 0: Newton gets three evaluations from the network's guess where
+// the network is consulted (strong waves, inexact two-rarefaction guess;
+// elsewhere the two-rarefaction start with the full iteration budget);
+// lanes that have not converged are appended to `queue` (warp-aggregated
+// atomics) and re-solved from the two-rarefaction guess by k_fallback, so no
+// warp waits for a fallback lane.
+// One instantiation per path, so that the two-rarefaction path does not
+// carry the network's register footprint.
+template <bool learned>
+__global__ void __launch_bounds__(SOLVE_THREADS, learned ? 2 : 1)
+k_solve(const double *__restrict__ S, long n, double *__restrict__ out, unsigned char *__restrict__ iters,
+        unsigned char *__restrict__ flags, const MlpPacked *__restrict__ w, double tol, int max_iter, int *queue,
+        int *qcount, unsigned *status) {
+  __shared__ __align__(16) MlpPacked M;
+  if (learned) { load_packed(M, w); __syncthreads(); }
+  const int lane = threadIdx.x & 31;
   const long stride = (long)gridDim.x * blockDim.x;
   unsigned st = 0;
   // grid-stride loop whose trip count is uniform across a warp
@@ -282,31 +70,32 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_solve(const double *__restric
     } else {
       L.d = R.d = 1.0; L.u = R.u = 0.0; L.p = R.p = 1.0; L.c = R.c = sqrt(1.4);
     }
-    const bool vacuum = 2.0 * (L.c + R.c) / (g - 1.0) <= R.u - L.u;
-    double ptr = vacuum ? 0.0 : tr_guess(L, R, g);
+    const bool vac = vacuum(L, R, g);
+    const double ptr = vac ? 0.0 : tr_guess(L, R, g);
     double p0 = ptr;
+    bool net = false;
     if (learned) {
-      float f[NIN];
-      if (!vacuum) features(L, R, g, ptr, f);
-      else for (int k = 0; k < NIN; ++k) f[k] = 0.f;
-#pragma unroll
-      for (int k = 0; k < 16; k += 2)
-        *reinterpret_cast<uint32_t *>(&X[warp][lane][k]) = pack_bf16(k < NIN ? f[k] : 0.f, k + 1 < NIN ? f[k + 1] : 0.f);
-      __syncwarp();
-      mlp_warp(M, X[warp], Y[warp]);
-      float y = fminf(fmaxf(Y[warp][lane], -20.f), 20.f);
-      if (!vacuum && !tr_exact(L, R, ptr)) p0 = ptr * (double)expf(y);
+      // the network is consulted for strong waves with an inexact
+      // two-rarefaction guess; warps without such a lane skip it
+      net = valid && !vac && !tr_exact(L, R, ptr) && strong_waves(L, R);
+      if (__any_sync(0xffffffffu, net)) {
+        float f[NIN];
+        if (net) features(L, R, g, ptr, f);
+        else for (int k = 0; k < NIN; ++k) f[k] = 0.f;
+        float y = fminf(fmaxf(mlp_lane(M, f), -20.f), 20.f);
+        if (net) p0 = ptr * (double)expf(y);
+      }
     }
     unsigned char fl = 0;
     int its = 0;
     bool pending = false;
     double ps = 0.0, us = 0.5 * (L.u + R.u);
-    if (vacuum) {
+    if (vac) {
       fl |= 2;
     } else {
-      int k = newton(L, R, g, p0, tol, learned ? 3 : max_iter, ps);
+      int k = newton(L, R, g, p0, tol, net ? 3 : max_iter, ps, us, !net && strong_waves(L, R));
       if (k > 0) its = k;
-      else if (learned) pending = true;
+      else if (net) pending = true;
       else { its = max_iter; fl |= 4; st |= FLASH_HY_ERR_NEWTON_NOCONV; }
     }
     if (learned) {
@@ -319,7 +108,6 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_solve(const double *__restric
       }
     }
     if (valid && !pending) {
-      if (!vacuum) us = star_u(L, R, g, ps);
       out[i] = ps; out[n + i] = us;
       if (iters) iters[i] = (unsigned char)(its > 255 ? 255 : its);
       if (flags) flags[i] = fl;
@@ -341,12 +129,12 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_fallback(const double *__rest
     Side L, R;
     double g;
     load_state(S, n, i, L, R, g);
-    double ps;
+    double ps, us;
     unsigned char fl = 1;
-    int k = newton(L, R, g, tr_guess(L, R, g), tol, max_iter, ps);
+    int k = newton(L, R, g, tr_guess(L, R, g), tol, max_iter, ps, us, strong_waves(L, R));
     int its = 3 + (k > 0 ? k : max_iter);
     if (k <= 0) { fl |= 4; st |= FLASH_HY_ERR_NEWTON_NOCONV; }
-    out[i] = ps; out[n + i] = star_u(L, R, g, ps);
+    out[i] = ps; out[n + i] = us;
     if (iters) iters[i] = (unsigned char)(its > 255 ? 255 : its);
     if (flags) flags[i] = fl;
   }
@@ -355,31 +143,24 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_fallback(const double *__rest
 
 // network output y = MLP(features) for every interface (0 for vacuum cases)
 __global__ void __launch_bounds__(SOLVE_THREADS) k_predict(const double *__restrict__ S, long n, float *__restrict__ y,
-                                                           const float *__restrict__ w) {
-  __shared__ MlpSmem M;
-  __shared__ __align__(16) __nv_bfloat16 X[SOLVE_THREADS / 32][32][16];
-  __shared__ float Y[SOLVE_THREADS / 32][32];
-  load_mlp(M, w);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+                                                           const MlpPacked *__restrict__ w) {
+  __shared__ __align__(16) MlpPacked M;
+  load_packed(M, w);
+  __syncthreads();
   for (long base = (long)blockIdx.x * blockDim.x; base < n; base += (long)gridDim.x * blockDim.x) {
     const long i = base + threadIdx.x;
     float f[NIN];
     for (int k = 0; k < NIN; ++k) f[k] = 0.f;
     bool vac = true;
     if (i < n) {
-      Side L{S[i], S[n + i], S[2 * n + i], 0.}, R{S[3 * n + i], S[4 * n + i], S[5 * n + i], 0.};
-      double g = S[6 * n + i];
-      L.c = sqrt(g * L.p / L.d); R.c = sqrt(g * R.p / R.d);
-      vac = 2.0 * (L.c + R.c) / (g - 1.0) <= R.u - L.u;
+      Side L, R;
+      double g;
+      load_state(S, n, i, L, R, g);
+      vac = vacuum(L, R, g);
       if (!vac) features(L, R, g, tr_guess(L, R, g), f);
     }
-#pragma unroll
-    for (int k = 0; k < 16; k += 2)
-      *reinterpret_cast<uint32_t *>(&X[warp][lane][k]) = pack_bf16(k < NIN ? f[k] : 0.f, k + 1 < NIN ? f[k + 1] : 0.f);
-    __syncwarp();
-    mlp_warp(M, X[warp], Y[warp]);
-    if (i < n) y[i] = vac ? 0.f : Y[warp][lane];
-    __syncwarp();
+    const float yy = mlp_lane(M, f);
+    if (i < n) y[i] = vac ? 0.f : yy;
   }
 }
 
@@ -422,7 +203,7 @@ __global__ void k_make_samples(const double *S, const double *out, long n, float
     double ps = out[i];
     if (!(ps > 0.0)) continue;
     double ptr = tr_guess(L, R, g);
-    if (tr_exact(L, R, ptr)) continue;          // the guess is only used where TR is inexact
+    if (tr_exact(L, R, ptr) || !strong_waves(L, R)) continue;   // where the network is consulted
     int k = atomicAdd(count, 1);
     if (k >= cap) continue;
     float f[NIN];
@@ -593,6 +374,7 @@ struct flash_hy_rsolver {
   int device;
   cudaStream_t stream;
   float *w, *m, *v, *G, *loss;
+  MlpPacked *packed;            // BF16 inference copy of w
   int *queue, *qcount;          // fallback queue of the learned path
   long qcap;
   unsigned *status;
@@ -612,6 +394,12 @@ static int grid_for(long n, int threads) {
   return (int)(g > 0 ? g : 1);
 }
 
+static int repack(flash_hy_rsolver *r) {
+  k_pack_mlp<<<1, 256, 0, r->stream>>>(r->w, r->packed);
+  RS_CUDA(cudaGetLastError());
+  return 0;
+}
+
 extern "C" int flash_hy_rsolver_create(int device, flash_hy_rsolver **out) {
   if (!out) return FLASH_HY_ERR_BAD_ARG;
   flash_hy_rsolver *r = (flash_hy_rsolver *)calloc(1, sizeof *r);
@@ -626,6 +414,7 @@ extern "C" int flash_hy_rsolver_create(int device, flash_hy_rsolver **out) {
   RS_CUDA(cudaMalloc(&r->loss, sizeof(float)));
   RS_CUDA(cudaMalloc(&r->status, sizeof(unsigned)));
   RS_CUDA(cudaMalloc(&r->qcount, sizeof(int)));
+  RS_CUDA(cudaMalloc(&r->packed, sizeof(MlpPacked)));
   RS_CUDA(cudaMemset(r->m, 0, NPARAM * sizeof(float)));
   RS_CUDA(cudaMemset(r->v, 0, NPARAM * sizeof(float)));
   RS_CUDA(cudaMemset(r->status, 0, sizeof(unsigned)));
@@ -640,7 +429,7 @@ extern "C" int flash_hy_rsolver_create(int device, flash_hy_rsolver **out) {
   cudaError_t e = cudaMemcpy(r->w, h, NPARAM * sizeof(float), cudaMemcpyHostToDevice);
   free(h);
   if (e != cudaSuccess) return FLASH_HY_ERR_CUDA;
-  return 0;
+  return repack(r);
 }
 
 extern "C" int flash_hy_rsolver_destroy(flash_hy_rsolver *r) {
@@ -648,7 +437,7 @@ extern "C" int flash_hy_rsolver_destroy(flash_hy_rsolver *r) {
   cudaSetDevice(r->device);
   if (r->stream) cudaStreamSynchronize(r->stream);
   cudaFree(r->w); cudaFree(r->m); cudaFree(r->v); cudaFree(r->G); cudaFree(r->loss); cudaFree(r->status);
-  cudaFree(r->queue); cudaFree(r->qcount);
+  cudaFree(r->queue); cudaFree(r->qcount); cudaFree(r->packed);
   if (r->stream) cudaStreamDestroy(r->stream);
   free(r);
   return 0;
@@ -676,9 +465,12 @@ extern "C" int flash_hy_rsolver_solve(flash_hy_rsolver *r, const double *d_state
     r->qcap = n;
   }
   if (learned) RS_CUDA(cudaMemsetAsync(r->qcount, 0, sizeof(int), r->stream));
-  k_solve<<<grid_for(n, SOLVE_THREADS), SOLVE_THREADS, 0, r->stream>>>(d_states, n, d_star, d_iters, d_flags, r->w,
-                                                                      learned, tol, max_iter, r->queue, r->qcount,
-                                                                      r->status);
+  if (learned)
+    k_solve<true><<<grid_for(n, SOLVE_THREADS), SOLVE_THREADS, 0, r->stream>>>(
+        d_states, n, d_star, d_iters, d_flags, r->packed, tol, max_iter, r->queue, r->qcount, r->status);
+  else
+    k_solve<false><<<grid_for(n, SOLVE_THREADS), SOLVE_THREADS, 0, r->stream>>>(
+        d_states, n, d_star, d_iters, d_flags, r->packed, tol, max_iter, r->queue, r->qcount, r->status);
   RS_CUDA(cudaGetLastError());
   if (learned) {
     k_fallback<<<148 * 4, SOLVE_THREADS, 0, r->stream>>>(d_states, n, d_star, d_iters, d_flags, r->queue, r->qcount,
@@ -691,7 +483,7 @@ extern "C" int flash_hy_rsolver_solve(flash_hy_rsolver *r, const double *d_state
 extern "C" int flash_hy_rsolver_predict(flash_hy_rsolver *r, const double *d_states, long n, float *d_y) {
   if (!r || !d_states || !d_y || n <= 0) return FLASH_HY_ERR_BAD_ARG;
   RS_CUDA(cudaSetDevice(r->device));
-  k_predict<<<grid_for(n, SOLVE_THREADS), SOLVE_THREADS, 0, r->stream>>>(d_states, n, d_y, r->w);
+  k_predict<<<grid_for(n, SOLVE_THREADS), SOLVE_THREADS, 0, r->stream>>>(d_states, n, d_y, r->packed);
   RS_CUDA(cudaGetLastError());
   return 0;
 }
@@ -758,7 +550,7 @@ extern "C" int flash_hy_rsolver_train(flash_hy_rsolver *r, const float *d_x, con
   cudaFree(idx);
   RS_CUDA(cudaGetLastError());
   if (loss_out) *loss_out = last;
-  return 0;
+  return repack(r);
 }
 
 extern "C" int flash_hy_rsolver_get_weights(flash_hy_rsolver *r, float *h_w, int n) {
@@ -775,7 +567,7 @@ extern "C" int flash_hy_rsolver_set_weights(flash_hy_rsolver *r, const float *h_
   RS_CUDA(cudaMemset(r->m, 0, NPARAM * sizeof(float)));
   RS_CUDA(cudaMemset(r->v, 0, NPARAM * sizeof(float)));
   r->step = 0;
-  return 0;
+  return repack(r);
 }
 
 extern "C" int flash_hy_rsolver_num_params(void) { return NPARAM; }

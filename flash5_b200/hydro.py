@@ -26,6 +26,7 @@ class Hydro:
 
     def __init__(self, params, grid, device=0):
         self.lib = abi.load_library()
+        self.device = device
         self.params = params
         self.grid = grid
         self._gdesc = grid.desc()
@@ -93,6 +94,30 @@ class Hydro:
 
     def sync(self):
         self._check(self.lib.flash_hy_sync(self.ctx))
+
+    # -- exact Riemann solver: learned guess and its training data ---------
+    def set_guess_weights(self, w):
+        """Attach the learned star-pressure guess (FP32 master weights, the
+        layout of ExactRiemann.get_weights) to the exact-solver faces."""
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        self._check(self.lib.flash_hy_set_guess_weights(self.ctx, w.ctypes.data_as(C.POINTER(C.c_float)), w.size))
+
+    def harvest(self, cap, keep_log2=6):
+        """Keep about one face in 2**keep_log2 (where the two-rarefaction guess
+        is inexact) of the following steps' face states, at most cap."""
+        self._check(self.lib.flash_hy_harvest(self.ctx, int(cap), int(keep_log2)))
+
+    def harvest_fetch(self, torch, n_max=None):
+        """The harvested face states as a [7, n] float64 CUDA tensor
+        (rho_L, u_L, p_L, rho_R, u_R, p_R, gamma); starts a new sample."""
+        n = C.c_longlong()
+        self._check(self.lib.flash_hy_harvest_fetch(self.ctx, None, 0, C.byref(n)))
+        k = n.value if n_max is None else min(n.value, int(n_max))
+        out = torch.empty(7 * max(k, 1), dtype=torch.float64, device=torch.device("cuda", self.device))
+        torch.cuda.current_stream(out.device).synchronize()   # the library writes on its own stream
+        got = C.c_longlong()
+        self._check(self.lib.flash_hy_harvest_fetch(self.ctx, C.c_void_p(out.data_ptr()), k, C.byref(got)))
+        return out[:7 * got.value].view(7, got.value)
 
     @property
     def stream(self):

@@ -130,6 +130,18 @@ class ExactRiemann:
                                                   C.byref(loss)))
         return loss.value
 
+    def fit(self, S, epochs=8, batch=4096, lr=2e-3):
+        """Train the guess on interface states S ([7, n] CUDA tensor, e.g. the
+        face states harvested by Hydro.harvest_fetch): solve them from the
+        two-rarefaction guess, build (features, ln(p*/p_TR)) samples where
+        that guess is inexact, run the Adam training kernels.  Returns
+        (final loss, number of samples)."""
+        out, _, _ = self.solve(S, learned=False)
+        X, T, ns = self.make_samples(S, out)
+        if ns < batch:
+            raise RiemannError(f"only {ns} training samples (batch {batch})")
+        return self.train(X, T, ns, epochs=epochs, batch=batch, lr=lr), ns
+
     def weights(self):
         w = np.zeros(self.nparam, np.float32)
         self._check(self.L.flash_hy_rsolver_get_weights(self.h, w.ctypes.data_as(C.POINTER(C.c_float)), self.nparam))

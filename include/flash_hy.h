@@ -158,6 +158,26 @@ int flash_hy_last_error(flash_hy_ctx *ctx, char *buf, int len);
 /* Number of kernel launches issued by the last flash_hy_step call. */
 int flash_hy_last_launch_count(flash_hy_ctx *ctx);
 
+/* ---- exact solver inside the hydro step (riemann_solver = FLASH_HY_RS_EXACT)
+ * No counterpart in FLASH5 (see the exact-solver section below).  With
+ * learned_guess = 1 (mixed precision only) the face solves start Newton
+ * from the network's estimate of p* once weights are attached; until then,
+ * and wherever the network's start does not converge within three
+ * evaluations, they start from the two-rarefaction guess, so the converged
+ * fluxes do not depend on the network.  w = FP32 master weights in the
+ * layout of flash_hy_rsolver_get_weights (n = flash_hy_rsolver_num_params()),
+ * host memory.                                                          */
+int flash_hy_set_guess_weights(flash_hy_ctx *ctx, const float *w, int n);
+/* Keep a hashed sample (about one face in 2^keep_log2 where the
+ * two-rarefaction guess is not exact) of the face states the mixed exact
+ * path solves, up to cap states, as training data for the guess; cap = 0
+ * stops.  fetch copies the states kept so far into the DEVICE array
+ * d_states as SoA [7][n] (rho_L, u_L, p_L, rho_R, u_R, p_R, gamma; u normal
+ * to the face), n = min(kept, n_max), and starts a new sample; d_states =
+ * NULL only reports the count.                                          */
+int flash_hy_harvest(flash_hy_ctx *ctx, long long cap, int keep_log2);
+int flash_hy_harvest_fetch(flash_hy_ctx *ctx, double *d_states, long long n_max, long long *n_out);
+
 /* ---- CFL time step without any device allocation ------------------------
  * No counterpart in the reference: FLASH5's Hydro_computeDt runs on host
  * arrays.  This entry point is for callers that cannot call cudaMalloc

@@ -14,11 +14,11 @@
  * Sod shock-tube secant solve of Simulation/SimulationMain/Sod/shocktube.pro
  * (lines 15-33, 90-120), is the cross-check used by the tests.
  *
- * Newton here is safeguarded by a bracket [pa, pb] with f(pa) < 0 < f(pb):
- * a step that leaves the bracket is replaced by a geometric bisection (or a
- * decimation towards zero while pa = 0), and the iteration stops when the
- * Newton step is below tol * p, so it always terminates within max_iter.
+ * Newton is safeguarded by the bracket of evaluated signs (see
+ * orc_star_state), so it always terminates within max_iter.  The vacuum-
+ * generating case is sampled as in Toro section 4.6.
  */
+#include <float.h>
 #include <math.h>
 
 typedef struct { double d, u, p, c; } side_t;
@@ -28,8 +28,9 @@ static void pres_fn(double p, const side_t *s, double g, double *f, double *fd) 
   if (p <= s->p) {                                   /* rarefaction */
     double prat = p / s->p;
     double ex = (g - 1.0) / (2.0 * g);
-    *f = 2.0 * s->c / (g - 1.0) * (pow(prat, ex) - 1.0);
-    *fd = (1.0 / (s->d * s->c)) * pow(prat, -(g + 1.0) / (2.0 * g));
+    double q = pow(prat, ex);
+    *f = 2.0 * s->c / (g - 1.0) * (q - 1.0);
+    *fd = q / (prat * s->d * s->c);                  /* (p/pK)^(-(g+1)/2g) / (dK cK) */
   } else {                                           /* shock */
     double A = 2.0 / ((g + 1.0) * s->d);
     double B = (g - 1.0) / (g + 1.0) * s->p;
@@ -48,9 +49,31 @@ double orc_two_rarefaction_guess(double dl, double ul, double pl, double dr, dou
   return pow(num / (cl / pow(pl, z) + cr / pow(pr, z)), 1.0 / z);
 }
 
-/* Solve for p* and u*.  p0 > 0 is the initial guess (<= 0: two-rarefaction).
- * Returns 0 on convergence to |dp|/p < tol, 1 when max_iter was hit, 2 when
- * the data generate vacuum (p* = 0).  *iters = Newton/bisection steps. */
+/* Strong waves (the network is consulted and the bracket probed only
+ * there): the pressure range of p_L, p_R and the PVRS estimate covers a
+ * factor of two or more, with the PVRS estimate above min(p_L, p_R). */
+int orc_strong_waves(double dl, double ul, double pl, double dr, double ur, double pr, double g) {
+  double cl = sqrt(g * pl / dl), cr = sqrt(g * pr / dr);
+  double pmin = fmin(pl, pr), pmax = fmax(pl, pr);
+  double ppv = 0.5 * (pl + pr) - 0.125 * (ur - ul) * (dl + dr) * (cl + cr);
+  return ppv > pmin && fmax(pmax, ppv) >= 2.0 * pmin;
+}
+
+/* Solve for p* and u*.  p0 > 0 is the initial guess; p0 <= 0 starts from
+ * the two-rarefaction guess and, for strong waves, first probes the bracket:
+ * [pa, pb] = [p/4, p] with f(pb) > 0, from p = max(p_L, p_R) growing by 4,
+ * and a start outside it is replaced by sqrt(pa * pb).  Returns 0 on
+ * convergence, 1 when max_iter evaluations were used, 2 when the data
+ * generate vacuum (p* = 0).  *iters = pressure-function evaluations.
+ *
+ * f is increasing and concave (Toro 4.3.1), so an iterate at or left of
+ * the root stays there.  The iterate is kept inside the bracket of
+ * evaluated signs (pb = DBL_MAX until a positive f is seen): a step leaving
+ * it is replaced by a geometric bisection, a decimation towards zero
+ * (pa = 0) or a growth by 4 (no upper end yet).  Converged when the step is
+ * below tol * p or the predicted next step of the quadratic regime,
+ * |step|^3/prev^2, is below tol * p / 100.  u* uses f_L, f_R linearised
+ * from the last evaluation to the returned p*. */
 int orc_star_state(double dl, double ul, double pl, double dr, double ur, double pr, double g,
                    double p0, double tol, int max_iter, double *pstar, double *ustar, int *iters) {
   side_t L = {dl, ul, pl, sqrt(g * pl / dl)}, R = {dr, ur, pr, sqrt(g * pr / dr)};
@@ -62,92 +85,117 @@ int orc_star_state(double dl, double ul, double pl, double dr, double ur, double
     *ustar = 0.5 * (ul + ur);
     return 2;
   }
-  double fl, fdl, fr, fdr;
-  /* bracket: f is increasing in p; f(0+) < 0 here, find pb with f(pb) > 0 */
-  double pa = 0.0, pb = fmax(pl, pr);
-  for (int k = 0; k < 200; ++k) {
-    pres_fn(pb, &L, g, &fl, &fdl); pres_fn(pb, &R, g, &fr, &fdr);
-    if (fl + fr + du > 0.0) break;
-    pa = pb;
-    pb *= 4.0;
-  }
+  double fl = 0., fdl = 0., fr = 0., fdr = 0.;
+  double pa = 0.0, pb = DBL_MAX;
+  int probe = p0 <= 0.0 && orc_strong_waves(dl, ul, pl, dr, ur, pr, g);
   double p = p0 > 0.0 ? p0 : orc_two_rarefaction_guess(dl, ul, pl, dr, ur, pr, g);
-  if (!(p > pa && p < pb)) p = pa > 0.0 ? sqrt(pa * pb) : 0.5 * pb;
-  int status = 1;
-  double prev = -1.0;
-  for (int it = 0; it < max_iter; ++it) {
+  int evals = 0;
+  if (probe) {
+    double q = fmax(pl, pr);
+    for (int k = 0; k < 64 && evals < max_iter; ++k) {
+      pres_fn(q, &L, g, &fl, &fdl); pres_fn(q, &R, g, &fr, &fdr);
+      ++evals;
+      if (fl + fr + du > 0.0) { pb = q; break; }
+      pa = q;
+      q *= 4.0;
+    }
+    if (!(p > pa && p < pb)) p = (pa > 0.0 && pb < DBL_MAX) ? sqrt(pa * pb) : (pb < DBL_MAX ? 0.5 * pb : 4.0 * pa);
+  }
+  double pe = p, prev = -1.0;
+  for (; evals < max_iter;) {
     pres_fn(p, &L, g, &fl, &fdl); pres_fn(p, &R, g, &fr, &fdr);
+    ++evals;
+    *iters = evals;
+    pe = p;
     double f = fl + fr + du;
-    *iters = it + 1;
-    if (f == 0.0) { status = 0; break; }
+    if (f == 0.0) {
+      *pstar = p;
+      *ustar = 0.5 * (ul + ur) + 0.5 * (fr - fl);
+      return 0;
+    }
     if (f < 0.0) pa = p; else pb = p;
     double step = f / (fdl + fdr);
     double pn = p - step;
     double as = fabs(step);
     int inside = pn > pa && pn < pb;
-    /* converged: step below tol, or the predicted next step of the
-     * quadratic regime, |step|^3/prev^2, below tol/100 */
     if (as <= tol * p || (inside && prev > 0.0 && as < prev && as * (as / prev) * (as / prev) <= 0.01 * tol * p)) {
-      if (pn > 0.0) p = pn;
-      status = 0;
-      break;
+      *pstar = pn > 0.0 ? pn : p;
+      double dp = *pstar - pe;
+      *ustar = 0.5 * (ul + ur) + 0.5 * ((fr + fdr * dp) - (fl + fdl * dp));
+      return 0;
     }
-    if (!inside) { pn = pa > 0.0 ? sqrt(pa * pb) : 0.01 * pb; prev = -1.0; }
+    if (!inside) { pn = pb == DBL_MAX ? 4.0 * p : (pa > 0.0 ? sqrt(pa * pb) : 0.01 * pb); prev = -1.0; }
     else prev = as;
     p = pn;
   }
-  pres_fn(p, &L, g, &fl, &fdl); pres_fn(p, &R, g, &fr, &fdr);
+  *iters = evals;
   *pstar = p;
-  *ustar = 0.5 * (ul + ur) + 0.5 * (fr - fl);
-  return status;
+  double dp = p - pe;
+  *ustar = 0.5 * (ul + ur) + 0.5 * ((fr + fdr * dp) - (fl + fdl * dp));
+  return 1;
 }
 
-/* Sample the exact solution at x/t = 0 (Toro section 4.5); returns the
- * density, normal velocity and pressure there and which side (0 = left,
- * 1 = right) supplies the transverse velocities. */
-static void sample0(const side_t *L, const side_t *R, double g, double ps, double us,
+/* Sample the exact solution at x/t = 0 (Toro section 4.5; vacuum
+ * generation, section 4.6); returns the density, normal velocity and
+ * pressure there and which side (0 = left, 1 = right) supplies the
+ * transverse velocities. */
+static void fan_left(const side_t *L, double g, double *d, double *u, double *p) {
+  double c = 2.0 / (g + 1.0) * (L->c + 0.5 * (g - 1.0) * L->u);
+  double r = c / L->c;
+  *u = c;
+  *d = L->d * pow(r, 2.0 / (g - 1.0));
+  *p = L->p * pow(r, 2.0 * g / (g - 1.0));
+}
+static void fan_right(const side_t *R, double g, double *d, double *u, double *p) {
+  double c = 2.0 / (g + 1.0) * (R->c - 0.5 * (g - 1.0) * R->u);
+  double r = c / R->c;
+  *u = -c;
+  *d = R->d * pow(r, 2.0 / (g - 1.0));
+  *p = R->p * pow(r, 2.0 * g / (g - 1.0));
+}
+
+static void sample0(const side_t *L, const side_t *R, double g, double ps, double us, int vac,
                     double *d, double *u, double *p, int *from_right) {
+  if (vac) {
+    double sl = L->u + 2.0 * L->c / (g - 1.0), sr = R->u - 2.0 * R->c / (g - 1.0);
+    if (0.0 <= L->u - L->c) { *from_right = 0; *d = L->d; *u = L->u; *p = L->p; }
+    else if (0.0 < sl) { *from_right = 0; fan_left(L, g, d, u, p); }
+    else if (0.0 >= R->u + R->c) { *from_right = 1; *d = R->d; *u = R->u; *p = R->p; }
+    else if (0.0 > sr) { *from_right = 1; fan_right(R, g, d, u, p); }
+    else { *from_right = 0; *d = 0.0; *u = 0.0; *p = 0.0; }
+    return;
+  }
   double g1 = (g - 1.0) / (2.0 * g), g2 = (g + 1.0) / (2.0 * g), g6 = (g - 1.0) / (g + 1.0);
   if (0.0 <= us) {                                   /* left of contact */
     *from_right = 0;
     if (ps > L->p) {                                 /* left shock */
-      double sl = L->u - L->c * sqrt(g2 * ps / L->p + g1);
+      double pr = ps / L->p;
+      double sl = L->u - L->c * sqrt(g2 * pr + g1);
       if (0.0 <= sl) { *d = L->d; *u = L->u; *p = L->p; }
-      else { *d = L->d * (ps / L->p + g6) / (ps / L->p * g6 + 1.0); *u = us; *p = ps; }
+      else { *d = L->d * (pr + g6) / (pr * g6 + 1.0); *u = us; *p = ps; }
     } else {                                         /* left rarefaction */
-      double shl = L->u - L->c;
-      if (0.0 <= shl) { *d = L->d; *u = L->u; *p = L->p; }
+      if (0.0 <= L->u - L->c) { *d = L->d; *u = L->u; *p = L->p; }
       else {
-        double cml = L->c * pow(ps / L->p, g1);
-        double stl = us - cml;
-        if (0.0 > stl) { *d = L->d * pow(ps / L->p, 1.0 / g); *u = us; *p = ps; }
-        else {
-          double c = 2.0 / (g + 1.0) * (L->c + 0.5 * (g - 1.0) * L->u);
-          *u = c;
-          *d = L->d * pow(c / L->c, 2.0 / (g - 1.0));
-          *p = L->p * pow(c / L->c, 2.0 * g / (g - 1.0));
-        }
+        double pr = ps / L->p;
+        double cml = L->c * pow(pr, g1);
+        if (0.0 > us - cml) { *d = L->d * pow(pr, 1.0 / g); *u = us; *p = ps; }
+        else fan_left(L, g, d, u, p);
       }
     }
   } else {                                           /* right of contact */
     *from_right = 1;
     if (ps > R->p) {
-      double sr = R->u + R->c * sqrt(g2 * ps / R->p + g1);
+      double pr = ps / R->p;
+      double sr = R->u + R->c * sqrt(g2 * pr + g1);
       if (0.0 >= sr) { *d = R->d; *u = R->u; *p = R->p; }
-      else { *d = R->d * (ps / R->p + g6) / (ps / R->p * g6 + 1.0); *u = us; *p = ps; }
+      else { *d = R->d * (pr + g6) / (pr * g6 + 1.0); *u = us; *p = ps; }
     } else {
-      double shr = R->u + R->c;
-      if (0.0 >= shr) { *d = R->d; *u = R->u; *p = R->p; }
+      if (0.0 >= R->u + R->c) { *d = R->d; *u = R->u; *p = R->p; }
       else {
-        double cmr = R->c * pow(ps / R->p, g1);
-        double str = us + cmr;
-        if (0.0 <= str) { *d = R->d * pow(ps / R->p, 1.0 / g); *u = us; *p = ps; }
-        else {
-          double c = 2.0 / (g + 1.0) * (R->c - 0.5 * (g - 1.0) * R->u);
-          *u = -c;
-          *d = R->d * pow(c / R->c, 2.0 / (g - 1.0));
-          *p = R->p * pow(c / R->c, 2.0 * g / (g - 1.0));
-        }
+        double pr = ps / R->p;
+        double cmr = R->c * pow(pr, g1);
+        if (0.0 <= us + cmr) { *d = R->d * pow(pr, 1.0 / g); *u = us; *p = ps; }
+        else fan_right(R, g, d, u, p);
       }
     }
   }
@@ -166,7 +214,7 @@ int orc_exact_flux(int dir, const double *VL, const double *VR, double gamma, do
   side_t R = {VR[0], VR[n], VR[4], sqrt(gamma * VR[4] / VR[0])};
   double d, u, p;
   int fr;
-  sample0(&L, &R, gamma, ps, us, &d, &u, &p, &fr);
+  sample0(&L, &R, gamma, ps, us, st == 2, &d, &u, &p, &fr);
   const double *Vt = fr ? VR : VL;
   double v[3] = {Vt[1], Vt[2], Vt[3]};
   v[dir - 1] = u;

@@ -39,6 +39,10 @@ def lib():
         L.orc_two_rarefaction_guess.argtypes = [C.c_double] * 7
         L.orc_two_rarefaction_guess.restype = C.c_double
         L.orc_star_batch.argtypes = [C.c_long] + [dp] * 8 + [C.c_double, C.c_int, dp, dp, ip, ip]
+        L.orc_amr_fill_guardcells.argtypes = [P, G, dp]
+        L.orc_amr_hydro.argtypes = [P, G, dp, C.c_double, C.c_double, C.c_double]
+        L.orc_amr_compute_dt.argtypes = [P, G, dp, dp, ip]
+        L.orc_amr_restrict.argtypes = [P, G, dp]
         _lib = L
     return _lib
 
@@ -49,32 +53,47 @@ def _dp(a):
 
 
 class Oracle:
-    """FLASH-like driver over host UNK arrays: eos_init, hydro step, dt."""
+    """FLASH-like driver over host UNK arrays: eos_init, hydro step, dt.
+    Grids with max_level > 1 (AmrGrid) use the AMR restatement."""
 
     def __init__(self, params, grid):
         self.p = params
         self.grid = grid
         self.g = grid.desc()
+        self.amr = self.g.max_level > 1
 
     def eos_init(self, unk):
         st = lib().orc_eos_interior(C.byref(self.p), C.byref(self.g), _dp(unk))
         assert st == 0, st
+        if self.amr:
+            st = lib().orc_amr_restrict(C.byref(self.p), C.byref(self.g), _dp(unk))
+            assert st == 0, st
         return unk
 
     def fill_guardcells(self, unk):
+        if self.amr:
+            return lib().orc_amr_fill_guardcells(C.byref(self.p), C.byref(self.g), _dp(unk))
         return lib().orc_fill_guardcells(C.byref(self.p), C.byref(self.g), _dp(unk))
 
     def hydro(self, unk, sim_time, dt, dt_old, blocks=None):
+        if self.amr:
+            assert blocks is None
+            return lib().orc_amr_hydro(C.byref(self.p), C.byref(self.g), _dp(unk), sim_time, dt, dt_old)
         if blocks is None:
             return lib().orc_hydro(C.byref(self.p), C.byref(self.g), _dp(unk), sim_time, dt, dt_old, 0, None)
         bl = np.ascontiguousarray(blocks, dtype=np.int32)
         return lib().orc_hydro(C.byref(self.p), C.byref(self.g), _dp(unk), sim_time, dt, dt_old, len(bl),
                                bl.ctypes.data_as(C.POINTER(C.c_int)))
 
+    def amr_hydro(self, unk, sim_time, dt, dt_old):
+        """The AMR step on any grid (max_level 1 included)."""
+        return lib().orc_amr_hydro(C.byref(self.p), C.byref(self.g), _dp(unk), sim_time, dt, dt_old)
+
     def compute_dt(self, unk):
         dt = C.c_double()
         loc = (C.c_int * 5)()
-        st = lib().orc_compute_dt(C.byref(self.p), C.byref(self.g), _dp(unk), C.byref(dt), loc)
+        f = lib().orc_amr_compute_dt if self.amr else lib().orc_compute_dt
+        st = f(C.byref(self.p), C.byref(self.g), _dp(unk), C.byref(dt), loc)
         return st, dt.value, tuple(loc)
 
 
@@ -84,6 +103,16 @@ def hllc(params, dirn, VL, VR):
     F = np.zeros(6)
     st = lib().orc_hllc(C.byref(params), dirn, _dp(VL), _dp(VR), _dp(F))
     return st, F
+
+
+def exact_flux(dirn, VL, VR, gamma, tol=1e-12, max_iter=50):
+    """Godunov flux of the exact solution (6 slots as hllc); (F, status, evaluations)."""
+    VL = np.ascontiguousarray(VL, dtype=np.float64)
+    VR = np.ascontiguousarray(VR, dtype=np.float64)
+    F = np.zeros(6)
+    it = C.c_int()
+    st = lib().orc_exact_flux(dirn, _dp(VL), _dp(VR), gamma, tol, max_iter, _dp(F), C.byref(it))
+    return F, st, it.value
 
 
 def star_state(dl, ul, pl, dr, ur, pr, gamma, p0=0.0, tol=1e-12, max_iter=50):

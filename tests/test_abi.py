@@ -89,6 +89,15 @@ def test_create_rejects_bad_arguments_without_touching_the_gpu():
     gd = g.desc()
     assert lib.flash_hy_create(C.byref(abi.default_params()), C.byref(gd), 0, C.byref(ctx)) == abi.ERR_UNSUPPORTED
     assert lib.flash_hy_step(None, 0.0, 1.0, 1.0, 0) == abi.ERR_BAD_ARG
+    # the learned guess belongs to the exact solver on the mixed path
+    g = UniformGrid(2, (8, 8), (2, 2))
+    gd = g.desc()
+    for kw in (dict(learned_guess=1), dict(learned_guess=1, riemann_solver=abi.RS_EXACT),
+               dict(learned_guess=1, precision=abi.PREC_MIXED), dict(riemann_solver=1)):
+        p = abi.default_params(**kw)
+        assert lib.flash_hy_create(C.byref(p), C.byref(gd), 0, C.byref(ctx)) == abi.ERR_UNSUPPORTED, kw
+    assert lib.flash_hy_set_guess_weights(None, None, 0) == abi.ERR_BAD_ARG
+    assert lib.flash_hy_harvest(None, 10, 0) == abi.ERR_BAD_ARG
 
 
 def test_grid_descriptor_and_unk_layout():

@@ -116,10 +116,10 @@ def test_learned_guess_same_result_fewer_iterations(rs):
     from flash5_b200.riemann import ExactRiemann
     r = ExactRiemann(0)                       # fresh He-initialised network
     try:
-        Str = r.generate(1, 400000)
+        Str = r.generate(1, 2000000)
         out, _, _ = r.solve(Str, learned=False)
         X, T, ns = r.make_samples(Str, out)
-        loss = r.train(X, T, ns, epochs=6, batch=4096, lr=2e-3)
+        loss = r.train(X, T, ns, epochs=8, batch=4096, lr=2e-3)
         assert np.isfinite(loss)
         S = r.generate(2, 200000)
         o0, it0, f0 = r.solve(S, learned=False)

@@ -41,9 +41,9 @@ def evolve(o, unk, tmax=None, nsteps=None, dt_cap=None):
     return t, n
 
 
-def sod_run(nblk, tmax=0.2, axis=0, nb=8):
+def sod_run(nblk, tmax=0.2, axis=0, nb=8, **pkw):
     g = UniformGrid(2, (nb, nb), (nblk, 1) if axis == 0 else (1, nblk), bc="outflow")
-    p = abi.default_params()
+    p = abi.default_params(**pkw)
     unk = setups.sod(g) if axis == 0 else setups.sod_axis(g, axis=axis)
     o = orc.Oracle(p, g)
     o.eos_init(unk)
@@ -97,11 +97,12 @@ def test_sod_x_and_y_are_symmetric():
     assert np.array_equal(vx, vy)
 
 
+@pytest.mark.parametrize("rs", [abi.RS_HLLC, abi.RS_EXACT])
 @pytest.mark.parametrize("ndim", [2, 3])
-def test_uniform_state_is_preserved(ndim):
+def test_uniform_state_is_preserved(ndim, rs):
     nb = (8, 8, 8)[:ndim]
     g = UniformGrid(ndim, nb, (2,) * ndim, bc="periodic")
-    p = abi.default_params()
+    p = abi.default_params(riemann_solver=rs)
     unk = setups.uniform(g, rho=1.3, v=(0.3, -0.2, 0.1), p=0.7)
     o = orc.Oracle(p, g)
     o.eos_init(unk)
@@ -112,11 +113,12 @@ def test_uniform_state_is_preserved(ndim):
         np.testing.assert_allclose(after[..., VAR[v]], before[..., VAR[v]], rtol=1e-13, atol=1e-14)
 
 
+@pytest.mark.parametrize("rs", [abi.RS_HLLC, abi.RS_EXACT])
 @pytest.mark.parametrize("ndim", [2, 3])
-def test_periodic_conservation(ndim):
+def test_periodic_conservation(ndim, rs):
     nb = (8, 8, 8)[:ndim]
     g = UniformGrid(ndim, nb, (2, 3, 2)[:ndim], bc="periodic")
-    p = abi.default_params(gamma=5.0 / 3.0)
+    p = abi.default_params(gamma=5.0 / 3.0, riemann_solver=rs)
     unk = setups.kelvin_helmholtz(g)
     o = orc.Oracle(p, g)
     o.eos_init(unk)
@@ -184,3 +186,30 @@ def test_exact_star_state_matches_golden():
     # the Sod p* from the shock-tube equation and from Toro's functions agree
     sod = json.load(open(os.path.join(GOLD, "sod_shocktube.json")))["cases"][0]
     assert abs(float(sod["p4"]) / float(cases[0]["pstar"]) - 1) < 1e-25
+
+
+def test_exact_solver_sod_against_exact_solution():
+    """The hydro step with exact-solver fluxes converges to the Sod solution
+    at least as well as the HLLC bound."""
+    nblk = 16
+    g, unk, t = sod_run(nblk, riemann_solver=abi.RS_EXACT)
+    nx = nblk * 8
+    x = (np.arange(nx) + 0.5) / nx
+    rs, _, _ = sod_exact.shocktube(1.0, 1.0, 0.0, 0.125, 0.1, 0.0, 1.4, 0.5, t, x)
+    l1 = np.abs(g.to_global(unk, "dens")[0] - rs[None, :]).mean()
+    assert l1 < 0.4 / nx, l1
+
+
+def test_exact_flux_vacuum_generation():
+    """Vacuum-generating data (Toro 4.6): symmetric expansion gives zero flux
+    at x/t = 0; a one-sided case samples the left fan or state."""
+    VL = np.array([1.0, -6.0, 0.0, 0.0, 0.4, 1.4, 1.4, 1.0])
+    VR = np.array([1.0, 6.0, 0.0, 0.0, 0.4, 1.4, 1.4, 1.0])
+    F, st, _ = orc.exact_flux(1, VL, VR, 1.4)
+    assert st == 0 and np.all(F == 0.0), F
+    # left state supersonic to the right: the left state itself
+    VL = np.array([1.0, 3.0, 0.5, 0.0, 0.4, 1.4, 1.4, 1.0])
+    VR = np.array([1.0, 12.0, 0.0, 0.0, 0.4, 1.4, 1.4, 1.0])
+    F, st, _ = orc.exact_flux(1, VL, VR, 1.4)
+    E = 0.4 / 0.4 + 0.5 * (9.0 + 0.25)
+    np.testing.assert_allclose(F, [3.0, 9.0 + 0.4, 1.5, 0.0, (E + 0.4) * 3.0, 0.4], rtol=1e-14)
