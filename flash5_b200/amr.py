@@ -1,0 +1,274 @@
+"""Block-structured AMR hierarchy in PARAMESH form.
+
+Every node of the refinement tree is a block of ``nb`` interior cells, as in
+PARAMESH (paramesh4/Paramesh4dev/PM4_package): a parent holds the
+restriction of its children, the leaves are the blocks Hydro advances
+(Grid_getTileIterator(LEAF), unsplit/Hydro.F90:149-229).  Level 1 is the
+complete root grid of ``nblk`` blocks per axis; a block at level l has
+block coordinates on the level-l grid of nblk * 2**(l-1) blocks per axis
+and cell size delta_1 / 2**(l-1).  Refinement keeps PARAMESH's 2:1 balance
+across faces, edges and corners (diagonals = .true., Paramesh4dev/Config:
+133-134), so every leaf touches only leaves one level up or down.
+
+Nodes are numbered level by level, Morton order inside a level; the host
+UNK array holds every node (shape (nblocks, nzt, nyt, nxt, NUNK)), like
+FLASH's unk(:,:,:,:,1:lnblocks) with parents included.
+"""
+import ctypes as C
+import itertools
+
+import numpy as np
+
+from . import abi
+from .grid import NGUARD, NUNK, VAR
+
+
+def _morton(c):
+    k = 0
+    for bit in range(16):
+        for d in range(3):
+            k |= ((c[d] >> bit) & 1) << (3 * bit + d)
+    return k
+
+
+class AmrGrid:
+    def __init__(self, ndim, nb, nblk, max_level, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), bc="outflow",
+                 nguard=NGUARD):
+        self.ndim = ndim
+        nb = tuple(nb) + (1,) * (3 - len(nb))
+        nblk = tuple(nblk) + (1,) * (3 - len(nblk))
+        self.nb = tuple(nb[d] if d < ndim else 1 for d in range(3))
+        self.nblk = tuple(nblk[d] if d < ndim else 1 for d in range(3))
+        self.max_level = int(max_level)
+        self.lo, self.hi = tuple(lo), tuple(hi)
+        if isinstance(bc, str):
+            bc = [bc] * 6
+        code = {"outflow": abi.BC_OUTFLOW, "periodic": abi.BC_PERIODIC, "reflecting": abi.BC_REFLECTING}
+        self.bc = [code[b] if isinstance(b, str) else int(b) for b in bc]
+        self.periodic = [self.bc[2 * d] == abi.BC_PERIODIC for d in range(3)]
+        self.nguard = nguard
+        self.ng = (nguard, nguard if ndim > 1 else 0, nguard if ndim > 2 else 0)
+        self.nt = tuple(self.nb[d] + 2 * self.ng[d] for d in range(3))
+        self.delta1 = tuple((self.hi[d] - self.lo[d]) / (self.nblk[d] * self.nb[d]) if d < ndim else 1.0
+                            for d in range(3))
+        self._offsets = [o for o in itertools.product((0, 1), repeat=ndim)]
+        self._leaves = {(1, (x, y, z)) for z in range(self.nblk[2]) for y in range(self.nblk[1])
+                        for x in range(self.nblk[0])}
+        self._inner = set()
+        self._finalize()
+
+    # -- tree edits ----------------------------------------------------------
+    def _extent(self, level):
+        return tuple(self.nblk[d] * (2 ** (level - 1)) if d < self.ndim else 1 for d in range(3))
+
+    def _children(self, level, c):
+        out = []
+        for o in self._offsets:
+            cc = [2 * c[d] + (o[d] if d < len(o) else 0) if d < self.ndim else 0 for d in range(3)]
+            out.append((level + 1, tuple(cc)))
+        return out
+
+    def _split(self, key):
+        self._leaves.discard(key)
+        self._inner.add(key)
+        for ch in self._children(*key):
+            self._leaves.add(ch)
+
+    def refine(self, marker):
+        """Refine every leaf below max_level for which marker(level, coords)
+        is true, then restore the 2:1 balance."""
+        for key in sorted(self._leaves):
+            lev, c = key
+            if lev < self.max_level and marker(lev, c):
+                self._split(key)
+        self._balance()
+        self._finalize()
+
+    def refine_levels(self, marker):
+        """Refine level by level (1 .. max_level-1) with the same marker."""
+        for lev in range(1, self.max_level):
+            for key in sorted(k for k in self._leaves if k[0] == lev):
+                if marker(lev, key[1]):
+                    self._split(key)
+            self._balance()
+        self._finalize()
+
+    def _neighbor(self, level, c, o):
+        ext = self._extent(level)
+        p = []
+        for d in range(3):
+            v = c[d] + (o[d] if d < self.ndim else 0)
+            if d < self.ndim and (v < 0 or v >= ext[d]):
+                if not self.periodic[d]:
+                    return None
+                v %= ext[d]
+            p.append(v)
+        return tuple(p)
+
+    def _balance(self):
+        offs = [o for o in itertools.product((-1, 0, 1), repeat=self.ndim) if any(o)]
+        changed = True
+        while changed:
+            changed = False
+            for key in sorted(self._leaves):
+                lev, c = key
+                if lev >= self.max_level:
+                    continue
+                need = False
+                for o in offs:
+                    o3 = tuple(o) + (0,) * (3 - self.ndim)
+                    p = self._neighbor(lev, c, o3)
+                    if p is None or (lev, p) not in self._inner:
+                        continue
+                    # children of the neighbour that touch this block
+                    for ch_lev, ch in self._children(lev, p):
+                        touch = True
+                        for d in range(self.ndim):
+                            co = ch[d] - 2 * p[d]
+                            if (o3[d] == 1 and co != 0) or (o3[d] == -1 and co != 1):
+                                touch = False
+                        if touch and (ch_lev, ch) in self._inner:
+                            need = True
+                            break
+                    if need:
+                        break
+                if need:
+                    self._split(key)
+                    changed = True
+
+    # -- node arrays -----------------------------------------------------------
+    def _finalize(self):
+        nodes = sorted(self._leaves | self._inner, key=lambda k: (k[0], _morton(k[1])))
+        self.node_index = {k: i for i, k in enumerate(nodes)}
+        self.nblocks = len(nodes)
+        self.levels = np.array([k[0] for k in nodes], dtype=np.int32)
+        self.coords = np.array([k[1] for k in nodes], dtype=np.int32).reshape(-1, 3)
+        self.is_leaf = np.array([k in self._leaves for k in nodes], dtype=bool)
+        self.leaf_ids = np.nonzero(self.is_leaf)[0]
+        self.parent = np.full(self.nblocks, -1, dtype=np.int32)
+        for i, (lev, c) in enumerate(nodes):
+            if lev > 1:
+                self.parent[i] = self.node_index[(lev - 1, tuple(v // 2 if d < self.ndim else 0
+                                                                 for d, v in enumerate(c)))]
+        self.max_used_level = int(self.levels.max())
+        self.delta_b = np.array([[self.delta1[d] / 2.0 ** (lv - 1) if d < self.ndim else 1.0 for d in range(3)]
+                                 for lv in self.levels])
+
+    @property
+    def nleaves(self):
+        return int(self.is_leaf.sum())
+
+    @property
+    def ncells(self):
+        """Interior cells of the leaves (the zones a step advances)."""
+        return self.nleaves * self.nb[0] * self.nb[1] * self.nb[2]
+
+    def delta(self, level):
+        return tuple(self.delta1[d] / 2.0 ** (level - 1) if d < self.ndim else 1.0 for d in range(3))
+
+    def desc(self):
+        g = abi.GridDesc()
+        g.ndim = self.ndim
+        g.nxb, g.nyb, g.nzb = self.nb
+        g.nguard = self.nguard
+        g.nblocks = self.nblocks
+        for d in range(3):
+            g.nblk_l1[d] = self.nblk[d]
+            g.domain_lo[d] = self.lo[d]
+            g.domain_hi[d] = self.hi[d]
+        for f in range(6):
+            g.bc[f] = self.bc[f]
+        g.max_level = self.max_level
+        self._keep = (np.ascontiguousarray(self.coords.reshape(-1)), np.ascontiguousarray(self.levels))
+        g.block_coords = self._keep[0].ctypes.data_as(C.POINTER(C.c_int))
+        g.block_level = self._keep[1].ctypes.data_as(C.POINTER(C.c_int))
+        return g
+
+    # -- UNK helpers (the same interface as UniformGrid) -------------------------
+    def new_unk(self):
+        return np.zeros((self.nblocks, self.nt[2], self.nt[1], self.nt[0], NUNK), dtype=np.float64)
+
+    def interior(self, unk):
+        g = self.ng
+        return unk[:, g[2]:g[2] + self.nb[2], g[1]:g[1] + self.nb[1], g[0]:g[0] + self.nb[0], :]
+
+    def cell_centers(self):
+        out = []
+        for d in range(3):
+            n = self.nb[d]
+            c = self.coords[:, d][:, None] * n + (np.arange(n) + 0.5)[None, :]
+            c = self.lo[d] + c * self.delta_b[:, d][:, None] if d < self.ndim else np.zeros_like(c, dtype=np.float64)
+            shape = [self.nblocks, 1, 1, 1]
+            shape[3 - d] = n
+            out.append(np.broadcast_to(c.reshape(shape), (self.nblocks, self.nb[2], self.nb[1], self.nb[0])))
+        return out
+
+    def cell_edges(self, d):
+        n = self.nb[d]
+        lft = self.coords[:, d][:, None] * n + np.arange(n)[None, :]
+        xl = self.lo[d] + lft * self.delta_b[:, d][:, None]
+        xr = self.lo[d] + (lft + 1) * self.delta_b[:, d][:, None]
+        shape = [self.nblocks, 1, 1, 1]
+        shape[3 - d] = n
+        full = (self.nblocks, self.nb[2], self.nb[1], self.nb[0])
+        return np.broadcast_to(xl.reshape(shape), full), np.broadcast_to(xr.reshape(shape), full)
+
+    def cell_volumes(self):
+        v = np.prod(self.delta_b[:, :self.ndim], axis=1)
+        return v
+
+    def composite(self, unk, var, level=None):
+        """One variable of the leaves on a uniform (nz, ny, nx) image at
+        `level` (default: the finest used level); coarse leaves are
+        injected (repeated), finer leaves averaged."""
+        level = self.max_used_level if level is None else level
+        ext = self._extent(level)
+        shape = tuple(ext[d] * self.nb[d] if d < self.ndim else 1 for d in (2, 1, 0))
+        out = np.zeros(shape)
+        it = self.interior(unk)[..., VAR[var]]
+        for b in self.leaf_ids:
+            lv = self.levels[b]
+            f = 2 ** (level - lv) if level >= lv else None
+            data = it[b]
+            if f is None:
+                r = 2 ** (lv - level)
+                sh = (data.shape[0] // (r if self.ndim > 2 else 1), r if self.ndim > 2 else 1,
+                      data.shape[1] // r, r, data.shape[2] // r, r)
+                data = data.reshape(sh).mean(axis=(1, 3, 5))
+                f = 1
+                scale = 1.0 / r
+            else:
+                scale = float(f)
+                for ax in range(3):
+                    if (2 - ax) < self.ndim:
+                        data = np.repeat(data, f, axis=ax)
+            o = [int(self.coords[b, d] * self.nb[d] * scale) if d < self.ndim else 0 for d in range(3)]
+            out[o[2]:o[2] + data.shape[0], o[1]:o[1] + data.shape[1], o[0]:o[0] + data.shape[2]] = data
+        return out
+
+
+def indicator_refiner(grid, field, threshold):
+    """Marker for AmrGrid.refine_levels: refine a block where the
+    dimensionless density gradient |grad rho| * dx / rho of `field` (a
+    function of cell-centre coordinates), sampled at the block's own
+    resolution with one extra ring of cells, exceeds `threshold`."""
+    def marker(level, c):
+        dx = grid.delta(level)
+        ax = []
+        for d in range(3):
+            if d < grid.ndim:
+                n = grid.nb[d]
+                ax.append(grid.lo[d] + (c[d] * n + np.arange(-1, n + 1) + 0.5) * dx[d])
+            else:
+                ax.append(np.array([0.0]))
+        Z, Y, X = np.meshgrid(ax[2], ax[1], ax[0], indexing="ij")
+        rho = field(X, Y, Z)
+        inner = tuple(slice(1, -1) if (2 - a) < grid.ndim else slice(None) for a in range(3))
+        ind = np.zeros_like(rho[inner])
+        for d in range(grid.ndim):
+            a = 2 - d
+            hi = list(inner); lo = list(inner)
+            hi[a] = slice(2, None); lo[a] = slice(None, -2)
+            ind = ind + (0.5 * (rho[tuple(hi)] - rho[tuple(lo)])) ** 2
+        return bool(np.max(np.sqrt(ind) / rho[inner]) > threshold)
+    return marker

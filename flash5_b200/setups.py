@@ -78,6 +78,29 @@ def sod_axis(grid, axis=0, gamma=1.4, rho_l=1.0, rho_r=0.125, p_l=1.0, p_r=0.1, 
     return _fill(grid, unk, rho, z, z, z, p, gamma)
 
 
+def _block_noise(grid, seed, amp):
+    """Seeded uniform noise drawn in global (z, y, x) cell order on the
+    finest level, so it does not depend on the block decomposition; a block
+    of a coarser AMR level gets the average over its footprint."""
+    L = getattr(grid, "max_used_level", 1)
+    f = 2 ** (L - 1)
+    nx, ny, nz = (grid.nblk[d] * grid.nb[d] * (f if d < grid.ndim else 1) for d in range(3))
+    rng = np.random.default_rng(seed)
+    glob = rng.uniform(-amp, amp, size=(nz, ny, nx))
+    out = np.empty((grid.nblocks, grid.nb[2], grid.nb[1], grid.nb[0]))
+    levels = getattr(grid, "levels", np.ones(grid.nblocks, dtype=np.int32))
+    for b in range(grid.nblocks):
+        r = 2 ** (L - levels[b])
+        o = [grid.coords[b, d] * grid.nb[d] * r if d < grid.ndim else 0 for d in range(3)]
+        e = [grid.nb[d] * r if d < grid.ndim else 1 for d in range(3)]
+        t = glob[o[2]:o[2] + e[2], o[1]:o[1] + e[1], o[0]:o[0] + e[0]]
+        if r > 1:
+            rz = r if grid.ndim > 2 else 1
+            t = t.reshape(grid.nb[2], rz, grid.nb[1], r, grid.nb[0], r).mean(axis=(1, 3, 5))
+        out[b] = t
+    return out
+
+
 def kelvin_helmholtz(grid, gamma=5.0 / 3.0, seed=12345, noise=1e-3):
     """3D (or 2D) Kelvin-Helmholtz shear layer with seeded noise."""
     unk = grid.new_unk()
@@ -85,14 +108,7 @@ def kelvin_helmholtz(grid, gamma=5.0 / 3.0, seed=12345, noise=1e-3):
     inner = np.abs(y - 0.5) < 0.25
     rho = np.where(inner, 2.0, 1.0)
     vx = np.where(inner, 0.5, -0.5)
-    nx, ny, nz = (grid.nblk[d] * grid.nb[d] for d in range(3))
-    rng = np.random.default_rng(seed)
-    glob = rng.uniform(-noise, noise, size=(nz, ny, nx))
-    # global (z, y, x) -> per-block (nzb, nyb, nxb) tiles in block order
-    tiles = glob.reshape(grid.nblk[2], grid.nb[2], grid.nblk[1], grid.nb[1], grid.nblk[0], grid.nb[0])
-    tiles = tiles.transpose(0, 2, 4, 1, 3, 5)
-    c = grid.coords
-    pert = tiles[c[:, 2], c[:, 1], c[:, 0]]
+    pert = _block_noise(grid, seed, noise)
     vy = 0.01 * np.sin(4.0 * np.pi * x) + pert
     vz = np.zeros_like(rho)
     p = np.full_like(rho, 2.5)

@@ -870,8 +870,7 @@ int orc_fill_guardcells(const flash_hy_params *p, const flash_hy_grid_desc *g, d
 
 /* Eos_wrapped(MODE_DENS_EI) on every block interior. */
 int orc_eos_interior(const flash_hy_params *p, const flash_hy_grid_desc *g, double *unk) {
-  int st = check_grid(g);
-  if (st) return st;
+  if (g->ndim < 2 || g->ndim > 3 || g->nguard != NGUARD) return FLASH_HY_ERR_UNSUPPORTED;
   ctx_t c; ctx_init(&c, p, g);
   size_t bsz = (size_t)c.nxt * c.nyt * c.nzt * NUNK;
   #pragma omp parallel for schedule(static)
@@ -987,4 +986,408 @@ int orc_hllc(const flash_hy_params *p, int dir, const double *VL, const double *
   ctx_t c; memset(&c, 0, sizeof c); c.p = p;
   hllc(&c, dir, VL, VR, F);
   return c.status;
+}
+
+/* ===================================================================== */
+/* AMR in PARAMESH form (max_level > 1).  Every tree node is a block of    */
+/* the descriptor (block_level, block_coords on its level's block grid);  */
+/* the leaves are advanced.  Grid semantics follow PARAMESH 4 as FLASH     */
+/* configures it with -gridinterpolation=native:                           */
+/*  * restriction: order-1 averaging of the 2^d children                   */
+/*    (amr_restrict_unk_genorder.F90, interp_mask_unk_res = 1),            */
+/*  * prolongation: linear, conserve = .false.                              */
+/*    (amr_1blk_cc_prol_linear.F90, amr_prolong_cc_fun_init.F90,           */
+/*    interp_mask_unk = 1 in gr_initParameshArrays.F90:95),                */
+/*  * both on per-volume values: per-mass variables are multiplied by DENS */
+/*    before and divided after (convertToConsvdInMeshInterp = .true.,      */
+/*    flash_convert_cc_hook.F90 / flash_unconvert_cc_hook.F90),            */
+/*  * guard cells of every node, coarse levels first: copy from the node   */
+/*    of the same level that owns the cell (leaf or parent), else          */
+/*    prolongation from the node's parent; then the EOS on leaf guard      */
+/*    cells (Grid_fillGuardCells doEos),                                   */
+/*  * flux correction with flux densities (consv_flux_densities = .true.,  */
+/*    Paramesh4dev/Config:156-158): a leaf face next to finer leaves takes */
+/*    the average of the fine face fluxes (Grid_conserveFluxes.F90:92-220),*/
+/*    all levels with one dt (unsplit/Hydro.F90:186-230).                  */
+/* ===================================================================== */
+#define AMR_MAXL 16
+typedef struct {
+  int n, L, ndim, N[3];
+  int ext[AMR_MAXL + 1][3];
+  long off[AMR_MAXL + 2];
+  int *at, *parent, *leaf;
+  const int *level, *coords;
+} amr_t;
+
+static int amr_at(const amr_t *a, int l, int x, int y, int z) {
+  if (l < 1 || l > a->L) return -1;
+  return a->at[a->off[l] + ((long)z * a->ext[l][1] + y) * a->ext[l][0] + x];
+}
+
+static void amr_free(amr_t *a) { free(a->at); free(a->parent); free(a->leaf); }
+
+/* Build the level tables and check that the nodes form a complete tree:
+ * a complete level 1, every other node's parent present, all 2^d children
+ * of a parent present. */
+static int amr_build(const flash_hy_grid_desc *g, amr_t *a) {
+  memset(a, 0, sizeof *a);
+  if (g->ndim < 2 || g->ndim > 3 || g->nguard != NGUARD) return FLASH_HY_ERR_UNSUPPORTED;
+  if (!g->block_level || !g->block_coords || g->max_level < 1 || g->max_level > AMR_MAXL) return FLASH_HY_ERR_BAD_ARG;
+  a->n = g->nblocks; a->L = g->max_level; a->ndim = g->ndim;
+  a->N[0] = g->nxb; a->N[1] = g->nyb; a->N[2] = g->ndim > 2 ? g->nzb : 1;
+  a->level = g->block_level; a->coords = g->block_coords;
+  a->off[1] = 0;
+  for (int l = 1; l <= a->L; ++l) {
+    for (int d = 0; d < 3; ++d) a->ext[l][d] = d < g->ndim ? g->nblk_l1[d] << (l - 1) : 1;
+    a->off[l + 1] = a->off[l] + (long)a->ext[l][0] * a->ext[l][1] * a->ext[l][2];
+  }
+  a->at = malloc(sizeof(int) * a->off[a->L + 1]);
+  a->parent = malloc(sizeof(int) * a->n);
+  a->leaf = malloc(sizeof(int) * a->n);
+  for (long q = 0; q < a->off[a->L + 1]; ++q) a->at[q] = -1;
+  for (int b = 0; b < a->n; ++b) {
+    int l = a->level[b];
+    const int *c = &a->coords[3 * b];
+    if (l < 1 || l > a->L) { amr_free(a); return FLASH_HY_ERR_BAD_ARG; }
+    for (int d = 0; d < 3; ++d)
+      if (c[d] < 0 || c[d] >= a->ext[l][d]) { amr_free(a); return FLASH_HY_ERR_BAD_ARG; }
+    long q = a->off[l] + ((long)c[2] * a->ext[l][1] + c[1]) * a->ext[l][0] + c[0];
+    if (a->at[q] >= 0) { amr_free(a); return FLASH_HY_ERR_BAD_ARG; }
+    a->at[q] = b;
+  }
+  for (long q = a->off[1]; q < a->off[2]; ++q) if (a->at[q] < 0) { amr_free(a); return FLASH_HY_ERR_BAD_ARG; }
+  for (int b = 0; b < a->n; ++b) {
+    int l = a->level[b];
+    const int *c = &a->coords[3 * b];
+    a->parent[b] = l > 1 ? amr_at(a, l - 1, c[0] / 2, c[1] / 2, c[2] / 2) : -1;
+    if (l > 1 && a->parent[b] < 0) { amr_free(a); return FLASH_HY_ERR_BAD_ARG; }
+    int nch = 0;
+    if (l < a->L)
+      for (int o = 0; o < (1 << g->ndim); ++o)
+        nch += amr_at(a, l + 1, 2 * c[0] + (o & 1), 2 * c[1] + ((o >> 1) & 1), g->ndim > 2 ? 2 * c[2] + (o >> 2) : 0) >= 0;
+    if (nch != 0 && nch != (1 << g->ndim)) { amr_free(a); return FLASH_HY_ERR_BAD_ARG; }
+    a->leaf[b] = nch == 0;
+  }
+  return 0;
+}
+
+static inline int is_per_mass(int v) { return v == VELX_V || v == VELY_V || v == VELZ_V || v == EINT_V || v == ENER_V; }
+
+/* Interior of parent node P = average of its children, per-volume form. */
+static void amr_restrict_node(const ctx_t *c, const amr_t *a, double *unk, int P) {
+  size_t bsz = (size_t)c->nxt * c->nyt * c->nzt * NUNK;
+  int l = a->level[P];
+  const int *pc = &a->coords[3 * P];
+  int hx = c->nxb / 2, hy = c->nyb / 2, hz = c->nzb / 2;
+  double w = c->k3 ? 0.125 : 0.25;
+  for (int k = 0; k < c->nzb; ++k)
+    for (int j = 0; j < c->nyb; ++j)
+      for (int i = 0; i < c->nxb; ++i) {
+        int ox = i >= hx, oy = j >= hy, oz = c->k3 ? k >= hz : 0;
+        int ch = amr_at(a, l + 1, 2 * pc[0] + ox, 2 * pc[1] + oy, c->k3 ? 2 * pc[2] + oz : 0);
+        int fi = 2 * (i - ox * hx), fj = 2 * (j - oy * hy), fk = c->k3 ? 2 * (k - oz * hz) : 0;
+        double s[NUNK];
+        for (int v = 0; v < NUNK; ++v) s[v] = 0.;
+        for (int kk = 0; kk <= c->k3; ++kk)
+          for (int jj = 0; jj <= 1; ++jj)
+            for (int ii = 0; ii <= 1; ++ii) {
+              const double *u = &unk[ch * bsz + cidx(c, fi + ii + NGUARD, fj + jj + NGUARD, c->k3 ? fk + kk + NGUARD : 0) * NUNK];
+              for (int v = 0; v < NUNK; ++v) s[v] = s[v] + w * (is_per_mass(v) ? u[DENS_V] * u[v] : u[v]);
+            }
+        double *d = &unk[P * bsz + cidx(c, i + NGUARD, j + NGUARD, c->k3 ? k + NGUARD : 0) * NUNK];
+        double inv = 1. / s[DENS_V];
+        for (int v = 0; v < NUNK; ++v) d[v] = is_per_mass(v) ? inv * s[v] : s[v];
+      }
+}
+
+/* One guard cell of node n (local cell li, lj, lk in [-NGUARD, N+NGUARD))
+ * from the owning node of the same level or by linear prolongation from
+ * n's parent; boundary conditions map the cell first (periodic: wrap;
+ * reflecting: mirror and flip the normal velocity; outflow: copy the edge). */
+static void amr_guard_cell(const ctx_t *c, const amr_t *a, const flash_hy_grid_desc *g, double *unk, int n,
+                           int li, int lj, int lk, double *dst) {
+  size_t bsz = (size_t)c->nxt * c->nyt * c->nzt * NUNK;
+  int l = a->level[n];
+  const int *bc = &a->coords[3 * n];
+  int loc[3] = {li, lj, lk}, gl[3], lp[3], flip[3] = {0, 0, 0};
+  for (int d = 0; d < 3; ++d) {
+    int N = a->N[d];
+    if (d >= a->ndim) { gl[d] = 0; lp[d] = 0; continue; }
+    int tot = a->ext[l][d] * N, base = bc[d] * N, gc = base + loc[d];
+    lp[d] = loc[d];
+    if (gc < 0 || gc >= tot) {
+      int side = gc < 0 ? 2 * d : 2 * d + 1;
+      if (g->bc[side] == FLASH_HY_BC_PERIODIC) gc = ((gc % tot) + tot) % tot;
+      else {
+        gc = map_axis(gc, tot, g->bc[2 * d], g->bc[2 * d + 1], &flip[d]);
+        lp[d] = gc - base;
+      }
+    }
+    gl[d] = gc;
+  }
+  int m = amr_at(a, l, gl[0] / a->N[0], gl[1] / a->N[1], a->ndim > 2 ? gl[2] / a->N[2] : 0);
+  if (m >= 0) {
+    const double *src = &unk[m * bsz + cidx(c, gl[0] % a->N[0] + NGUARD, gl[1] % a->N[1] + NGUARD,
+                                             c->k3 ? gl[2] % a->N[2] + NGUARD : 0) * NUNK];
+    memcpy(dst, src, sizeof(double) * NUNK);
+  } else {
+    /* amr_1blk_cc_prol_linear: child cell lp from the parent cells i1, i1+1
+     * per axis with weights dx, 1-dx (amr_prolong_cc_fun_init.F90) */
+    int P = a->parent[n];
+    int i1[3], dk3 = c->k3;
+    double wx[3], cx[3];
+    for (int d = 0; d < 3; ++d) {
+      if (d >= a->ndim) { i1[d] = 0; wx[d] = 1.; cx[d] = 0.; continue; }
+      int N = a->N[d], ioff = (bc[d] & 1) * (N / 2), ii = lp[d] + 1;
+      i1[d] = (ii + 2 * N) / 2 - N + ioff - 1;               /* parent-local, 0-based */
+      wx[d] = fmod(0.75 + (double)(ii + 2 * N) * .5, 1.);     /* prol_dx */
+      cx[d] = 1. - wx[d];
+    }
+    double r[2][2][2][NUNK];
+    for (int kk = 0; kk <= dk3; ++kk)
+      for (int jj = 0; jj <= 1; ++jj)
+        for (int ii = 0; ii <= 1; ++ii) {
+          const double *u = &unk[P * bsz + cidx(c, i1[0] + ii + NGUARD, i1[1] + jj + NGUARD,
+                                                  dk3 ? i1[2] + kk + NGUARD : 0) * NUNK];
+          for (int v = 0; v < NUNK; ++v) r[kk][jj][ii][v] = is_per_mass(v) ? u[DENS_V] * u[v] : u[v];
+        }
+    double val[NUNK];
+    for (int v = 0; v < NUNK; ++v) {
+      double plane0 = wx[1] * (wx[0] * r[0][0][0][v] + cx[0] * r[0][0][1][v]) +
+                      cx[1] * (wx[0] * r[0][1][0][v] + cx[0] * r[0][1][1][v]);
+      if (dk3) {
+        double plane1 = wx[1] * (wx[0] * r[1][0][0][v] + cx[0] * r[1][0][1][v]) +
+                        cx[1] * (wx[0] * r[1][1][0][v] + cx[0] * r[1][1][1][v]);
+        val[v] = wx[2] * plane0 + cx[2] * plane1;
+      } else {
+        val[v] = plane0;
+      }
+    }
+    double inv = 1. / val[DENS_V];
+    for (int v = 0; v < NUNK; ++v) dst[v] = is_per_mass(v) ? inv * val[v] : val[v];
+  }
+  if (flip[0]) dst[VELX_V] = -dst[VELX_V];
+  if (flip[1]) dst[VELY_V] = -dst[VELY_V];
+  if (flip[2]) dst[VELZ_V] = -dst[VELZ_V];
+}
+
+static void amr_fill_node_guards(const ctx_t *c, const amr_t *a, const flash_hy_grid_desc *g, double *unk, int n) {
+  size_t bsz = (size_t)c->nxt * c->nyt * c->nzt * NUNK;
+  for (int k = 0; k < c->nzt; ++k)
+    for (int j = 0; j < c->nyt; ++j)
+      for (int i = 0; i < c->nxt; ++i) {
+        int li = i - NGUARD, lj = c->k2 ? j - NGUARD : 0, lk = c->k3 ? k - NGUARD : 0;
+        if (li >= 0 && li < c->nxb && lj >= 0 && lj < c->nyb && lk >= 0 && lk < c->nzb) continue;
+        amr_guard_cell(c, a, g, unk, n, li, lj, lk, &unk[n * bsz + cidx(c, i, j, k) * NUNK]);
+      }
+}
+
+/* Restriction bottom-up, guard cells of every node coarse-to-fine, EOS on
+ * the leaves' guard cells. */
+static int amr_fill_all(const flash_hy_params *p, const flash_hy_grid_desc *g, const amr_t *a, double *unk) {
+  ctx_t c; ctx_init(&c, p, g);
+  size_t bsz = (size_t)c.nxt * c.nyt * c.nzt * NUNK;
+  for (int l = a->L - 1; l >= 1; --l) {
+    #pragma omp parallel for schedule(dynamic)
+    for (int b = 0; b < a->n; ++b)
+      if (a->level[b] == l && !a->leaf[b]) amr_restrict_node(&c, a, unk, b);
+  }
+  for (int l = 1; l <= a->L; ++l) {
+    #pragma omp parallel for schedule(dynamic)
+    for (int b = 0; b < a->n; ++b)
+      if (a->level[b] == l) amr_fill_node_guards(&c, a, g, unk, b);
+  }
+  #pragma omp parallel for schedule(dynamic)
+  for (int b = 0; b < a->n; ++b) {
+    if (!a->leaf[b]) continue;
+    for (int k = 0; k < c.nzt; ++k)
+      for (int j = 0; j < c.nyt; ++j)
+        for (int i = 0; i < c.nxt; ++i) {
+          int li = i - NGUARD, lj = c.k2 ? j - NGUARD : 0, lk = c.k3 ? k - NGUARD : 0;
+          if (li >= 0 && li < c.nxb && lj >= 0 && lj < c.nyb && lk >= 0 && lk < c.nzb) continue;
+          eos_dens_ei_cell(&c, &unk[b * bsz + cidx(&c, i, j, k) * NUNK]);
+        }
+  }
+  return 0;
+}
+
+int orc_amr_fill_guardcells(const flash_hy_params *p, const flash_hy_grid_desc *g, double *unk) {
+  amr_t a;
+  int st = amr_build(g, &a);
+  if (st) return st;
+  st = amr_fill_all(p, g, &a, unk);
+  amr_free(&a);
+  return st;
+}
+
+static void level_deltas(const flash_hy_grid_desc *g, int l, double del[3]) {
+  block_deltas(g, del);
+  for (int d = 0; d < g->ndim; ++d) del[d] = ldexp(del[d], 1 - l);
+}
+
+/* Replace leaf b's boundary face fluxes next to finer leaves by the average
+ * of the fine face fluxes (flux densities). */
+static void amr_correct_fluxes(const ctx_t *c, const amr_t *a, const flash_hy_grid_desc *g, work_t *W, int b) {
+  int l = a->level[b];
+  const int *bc = &a->coords[3 * b];
+  for (int d = 0; d < a->ndim; ++d)
+    for (int s = 0; s < 2; ++s) {
+      int pos[3] = {bc[0], bc[1], bc[2]};
+      pos[d] += s ? 1 : -1;
+      if (pos[d] < 0 || pos[d] >= a->ext[l][d]) {
+        if (g->bc[2 * d + s] != FLASH_HY_BC_PERIODIC) continue;
+        pos[d] = (pos[d] + a->ext[l][d]) % a->ext[l][d];
+      }
+      int m = amr_at(a, l, pos[0], pos[1], pos[2]);
+      if (m < 0 || a->leaf[m]) continue;                 /* same level or coarser: no correction */
+      int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;      /* tangential axes */
+      int n1 = a->N[t1], n2 = a->ndim > 2 ? a->N[t2] : 1;
+      int face = s ? a->N[d] : 0;                        /* local face index along d */
+      double w = a->ndim > 2 ? 0.25 : 0.5;
+      for (int q2 = 0; q2 < n2; ++q2)
+        for (int q1 = 0; q1 < n1; ++q1) {
+          int o[3] = {0, 0, 0};
+          o[d] = s ? 0 : 1;                              /* children of m touching b */
+          o[t1] = q1 >= n1 / 2;
+          if (a->ndim > 2) o[t2] = q2 >= n2 / 2;
+          int f = amr_at(a, l + 1, 2 * pos[0] + o[0], 2 * pos[1] + o[1], a->ndim > 2 ? 2 * pos[2] + o[2] : 0);
+          int ffa = s ? 0 : a->N[d];                     /* the fine leaf's face facing b */
+          double acc[NFLX];
+          for (int v = 0; v < NFLX; ++v) acc[v] = 0.;
+          for (int r2 = 0; r2 <= (a->ndim > 2); ++r2)
+            for (int r1 = 0; r1 <= 1; ++r1) {
+              int fl[3];
+              fl[d] = ffa;
+              fl[t1] = 2 * (q1 - o[t1] * (n1 / 2)) + r1;
+              if (a->ndim > 2) fl[t2] = 2 * (q2 - o[t2] * (n2 / 2)) + r2; else fl[2] = 0;
+              const double *F = &W[f].flux[d][cidx(c, fl[0] + NGUARD, fl[1] + NGUARD, c->k3 ? fl[2] + NGUARD : 0) * NFLX];
+              for (int v = 0; v < NFLX; ++v) acc[v] = acc[v] + w * F[v];
+            }
+          int cl[3];
+          cl[d] = face; cl[t1] = q1;
+          if (a->ndim > 2) cl[t2] = q2; else cl[2] = 0;
+          double *F = &W[b].flux[d][cidx(c, cl[0] + NGUARD, cl[1] + NGUARD, c->k3 ? cl[2] + NGUARD : 0) * NFLX];
+          for (int v = 0; v < NFLX; ++v) F[v] = acc[v];
+        }
+    }
+}
+
+/* Hydro(simTime, dt, dtOld, sweepOrder) on an AMR hierarchy: guard cells,
+ * fluxes of every leaf with its level's deltas, flux correction at
+ * fine/coarse faces, update of every leaf (unsplit/Hydro.F90:163-230, the
+ * hy_fluxCorrectPerLevel = .false. variant). */
+int orc_amr_hydro(const flash_hy_params *p, const flash_hy_grid_desc *g, double *unk,
+                  double sim_time, double dt, double dt_old) {
+  (void)sim_time; (void)dt_old;
+  if (p->order != 3) return FLASH_HY_ERR_UNSUPPORTED;
+  amr_t a;
+  int st = amr_build(g, &a);
+  if (st) return st;
+  amr_fill_all(p, g, &a, unk);
+  ctx_t c0; ctx_init(&c0, p, g);
+  size_t bsz = (size_t)c0.nxt * c0.nyt * c0.nzt * NUNK;
+  work_t *W = calloc(a.n, sizeof(work_t));
+  int status = 0;
+  #pragma omp parallel for schedule(dynamic) reduction(| : status)
+  for (int b = 0; b < a.n; ++b) {
+    if (!a.leaf[b]) continue;
+    ctx_t c; ctx_init(&c, p, g);
+    double del[3];
+    level_deltas(g, a.level[b], del);
+    work_alloc(&c, &W[b]);
+    get_riemann_state(&c, &unk[b * bsz], &W[b], dt, del);
+    get_face_flux(&c, &W[b]);
+    status |= c.status;
+  }
+  #pragma omp parallel for schedule(dynamic)
+  for (int b = 0; b < a.n; ++b)
+    if (a.leaf[b]) amr_correct_fluxes(&c0, &a, g, W, b);
+  #pragma omp parallel for schedule(dynamic) reduction(| : status)
+  for (int b = 0; b < a.n; ++b) {
+    if (!a.leaf[b]) continue;
+    ctx_t c; ctx_init(&c, p, g);
+    double del[3];
+    level_deltas(g, a.level[b], del);
+    double *U = &unk[b * bsz];
+    unsplit_update(&c, U, &W[b], dt, del);
+    energy_fix(&c, U);
+    for (int k = c.k3 ? NGUARD : 0; k < (c.k3 ? NGUARD + c.nzb : 1); ++k)
+      for (int j = c.k2 ? NGUARD : 0; j < (c.k2 ? NGUARD + c.nyb : 1); ++j)
+        for (int i = NGUARD; i < NGUARD + c.nxb; ++i) {
+          double *u = &U[cidx(&c, i, j, k) * NUNK];
+          eos_dens_ei_cell(&c, u);
+          for (int n = 0; n < NUNK; ++n) if (!isfinite(u[n]) && n != SHOK_V) c.status |= FLASH_HY_ERR_NAN;
+        }
+    status |= c.status;
+  }
+  for (int b = 0; b < a.n; ++b) if (a.leaf[b]) work_free(&W[b]);
+  free(W);
+  /* parents carry the restriction of the updated leaves */
+  ctx_t c; ctx_init(&c, p, g);
+  for (int l = a.L - 1; l >= 1; --l)
+    for (int b = 0; b < a.n; ++b)
+      if (a.level[b] == l && !a.leaf[b]) amr_restrict_node(&c, &a, unk, b);
+  amr_free(&a);
+  return status;
+}
+
+/* Hydro_computeDt over the leaves with their level's deltas, MINLOC over
+ * leaves; minloc = (i, j, k, level, block). */
+int orc_amr_compute_dt(const flash_hy_params *p, const flash_hy_grid_desc *g, const double *unk,
+                       double *dt_out, int minloc[5]) {
+  amr_t a;
+  int st = amr_build(g, &a);
+  if (st) return st;
+  ctx_t c; ctx_init(&c, p, g);
+  size_t bsz = (size_t)c.nxt * c.nyt * c.nzt * NUNK;
+  double dt_check = DBL_MAX;
+  int best[5] = {0, 0, 0, 0, -1};
+  for (int b = 0; b < a.n; ++b) {
+    if (!a.leaf[b]) continue;
+    double del[3];
+    level_deltas(g, a.level[b], del);
+    double delxinv = 1.0 / del[0], delyinv = 1.0 / del[1], delzinv = 1.0 / del[2];
+    double dt_temp = 0.;
+    int temploc[5] = {0, 0, 0, 0, 0};
+    double tempCfl = p->cfl, localCfl = p->cfl;
+    for (int k = c.k3 ? NGUARD : 0; k < (c.k3 ? NGUARD + c.nzb : 1); ++k)
+      for (int j = c.k2 ? NGUARD : 0; j < (c.k2 ? NGUARD + c.nyb : 1); ++j)
+        for (int i = NGUARD; i < NGUARD + c.nxb; ++i) {
+          const double *u = &unk[b * bsz + cidx(&c, i, j, k) * NUNK];
+          double sndspd2 = u[GAMC_V] * u[PRES_V] / u[DENS_V];
+          double dt_ltemp = (fabs(u[VELX_V] - 0.) + sqrt(sndspd2)) * delxinv;
+          if (g->ndim > 1) dt_ltemp = fmax2(dt_ltemp, (fabs(u[VELY_V] - 0.) + sqrt(sndspd2)) * delyinv);
+          if (g->ndim > 2) dt_ltemp = fmax2(dt_ltemp, (fabs(u[VELZ_V] - 0.) + sqrt(sndspd2)) * delzinv);
+          if (dt_ltemp * tempCfl > dt_temp * localCfl) {
+            dt_temp = dt_ltemp;
+            tempCfl = localCfl;
+            temploc[0] = i + 1; temploc[1] = j + 1; temploc[2] = k + 1;
+            temploc[3] = a.level[b];
+            temploc[4] = b;
+          }
+        }
+    if (dt_temp != 0.0) dt_temp = tempCfl / dt_temp;
+    else dt_temp = DBL_MAX;
+    if (dt_temp < dt_check) {
+      dt_check = dt_temp;
+      memcpy(best, temploc, sizeof best);
+    }
+  }
+  amr_free(&a);
+  *dt_out = dt_check;
+  memcpy(minloc, best, sizeof best);
+  return dt_check <= 0.0 ? FLASH_HY_ERR_NONPOS_DT : 0;
+}
+
+/* Restriction of every parent from the leaves (for initial data). */
+int orc_amr_restrict(const flash_hy_params *p, const flash_hy_grid_desc *g, double *unk) {
+  amr_t a;
+  int st = amr_build(g, &a);
+  if (st) return st;
+  ctx_t c; ctx_init(&c, p, g);
+  for (int l = a.L - 1; l >= 1; --l)
+    for (int b = 0; b < a.n; ++b)
+      if (a.level[b] == l && !a.leaf[b]) amr_restrict_node(&c, &a, unk, b);
+  amr_free(&a);
+  return 0;
 }
