@@ -272,3 +272,34 @@ def indicator_refiner(grid, field, threshold):
             ind = ind + (0.5 * (rho[tuple(hi)] - rho[tuple(lo)])) ** 2
         return bool(np.max(np.sqrt(ind) / rho[inner]) > threshold)
     return marker
+
+
+def four_quadrant_refinement_field(seed=2024, modes=12, width=0.004):
+    """Seeded smoothed density used to build the benchmark hierarchy: the
+    four-quadrant densities blended across x = 0.5 and y = 0.5 by tanh
+    profiles of the given width, times 1 + a sum of `modes` seeded Fourier
+    modes (wave numbers 1..8 per axis, amplitudes 0.02..0.06, numpy PCG64)."""
+    rng = np.random.default_rng(seed)
+    kx = rng.integers(1, 9, modes)
+    ky = rng.integers(1, 9, modes)
+    ph = rng.uniform(0, 2 * np.pi, modes)
+    am = rng.uniform(0.02, 0.06, modes)
+
+    def field(X, Y, Z):
+        sx = 0.5 * (1 + np.tanh((X - 0.5) / width))
+        sy = 0.5 * (1 + np.tanh((Y - 0.5) / width))
+        r = (1 - sx) * (1 - sy) * 0.138 + sx * (1 - sy) * 0.5323 + (1 - sx) * sy * 0.5323 + sx * sy * 1.5
+        pert = sum(am[k] * np.sin(2 * np.pi * (kx[k] * X + ky[k] * Y) + ph[k]) for k in range(modes))
+        return r * (1 + pert)
+    return field
+
+
+def four_quadrant_hierarchy(nb=16, nblk=32, max_level=4, threshold=0.0035, seed=2024, bc="outflow"):
+    """The batched AMR benchmark hierarchy: [0,1]^2, nblk^2 root blocks of
+    nb^2 cells, max_level levels, refined level by level where the
+    dimensionless density gradient of four_quadrant_refinement_field
+    exceeds `threshold` (defaults: 19,456 leaf blocks of 16^2 on levels
+    1-4, about 5.0e6 leaf zones)."""
+    g = AmrGrid(2, (nb, nb), (nblk, nblk), max_level, bc=bc)
+    g.refine_levels(indicator_refiner(g, four_quadrant_refinement_field(seed), threshold))
+    return g

@@ -8,6 +8,7 @@
 #include <vector>
 #include "../../include/flash_hy.h"
 #include "hy_launch.h"
+#include "amr_kernels.cuh"
 
 using namespace fhy;
 
@@ -53,6 +54,15 @@ struct flash_hy_ctx {
   int glaunches[2];
   int plain_steps[2];
   double *d_stepdt;
+  // AMR hierarchy (max_level > 1): node tables, level lists, guard buffers
+  int amr, nlev;
+  int *d_level, *d_leaf, *d_parent, *d_slot, *d_at;
+  int at_off[17], at_ext[17][3];
+  int *d_leaves, nleaves;
+  int *d_lev_leaves[17], lev_leaves[17];
+  int *d_lev_parents[17], lev_parents[17];
+  int nparents;
+  double *d_lh, *d_gp, *d_pe, *d_freg;
   char err[512];
 };
 
@@ -64,6 +74,8 @@ static void drop_graphs(flash_hy_ctx *c) {
 }
 
 __global__ void k_set_dt(double *d, double dt) { *d = dt; }
+
+static int amr_restrict_all(flash_hy_ctx *c);
 
 static int fail(flash_hy_ctx *c, int code, const char *fmt, const char *detail) {
   if (c) snprintf(c->err, sizeof c->err, fmt, detail ? detail : "");
@@ -121,6 +133,73 @@ static void fill_devparams(const flash_hy_ctx *c, DevParams &P) {
     P.s_in[v] = c->state[c->cur][v];
     P.s_out[v] = c->state[1 - c->cur][v];
   }
+  if (c->amr) {
+    P.blk_level = c->d_level;
+    P.leaf = c->d_leaf;
+    P.parent = c->d_parent;
+    P.slot = c->d_slot;
+    P.at = c->d_at;
+    for (int l = 0; l < 17; ++l) {
+      P.at_off[l] = c->at_off[l];
+      for (int d = 0; d < 3; ++d) P.at_ext[l][d] = c->at_ext[l][d];
+    }
+    P.lh = c->d_lh;
+    P.gp = c->d_gp;
+    P.pe = c->d_pe;
+    P.freg = c->d_freg;
+  }
+}
+
+// Level tables of an AMR hierarchy given as all its tree nodes: a complete
+// level 1, every other node's parent present, all 2^d children of a parent
+// present.  2:1 balance across faces, edges and corners is the caller's
+// contract (the guard fill and the flux register rely on it).
+static int amr_tables(const flash_hy_grid_desc *g, std::vector<int> &at, int off[17], int ext[17][3],
+                      std::vector<int> &parent, std::vector<int> &leaf) {
+  const int L = g->max_level;
+  if (L < 2 || L > 16 || !g->block_level) return FLASH_HY_ERR_BAD_ARG;
+  long tot = 0;
+  for (int l = 0; l < 17; ++l) {
+    off[l] = (int)tot;
+    for (int d = 0; d < 3; ++d) ext[l][d] = (l >= 1 && d < g->ndim) ? g->nblk_l1[d] << (l - 1) : 1;
+    if (l >= 1 && l <= L) tot += (long)ext[l][0] * ext[l][1] * ext[l][2];
+    if (tot > (1L << 30)) return FLASH_HY_ERR_UNSUPPORTED;
+  }
+  at.assign(tot, -1);
+  auto node = [&](int l, int x, int y, int z) -> int {
+    if (l < 1 || l > L || x < 0 || y < 0 || z < 0 || x >= ext[l][0] || y >= ext[l][1] || z >= ext[l][2]) return -1;
+    return at[off[l] + ((long)z * ext[l][1] + y) * ext[l][0] + x];
+  };
+  for (int b = 0; b < g->nblocks; ++b) {
+    int l = g->block_level[b];
+    const int *cc = &g->block_coords[3 * b];
+    int x = cc[0], y = g->ndim > 1 ? cc[1] : 0, z = g->ndim > 2 ? cc[2] : 0;
+    if (l < 1 || l > L || x < 0 || y < 0 || z < 0 || x >= ext[l][0] || y >= ext[l][1] || z >= ext[l][2])
+      return FLASH_HY_ERR_BAD_ARG;
+    long q = off[l] + ((long)z * ext[l][1] + y) * ext[l][0] + x;
+    if (at[q] >= 0) return FLASH_HY_ERR_BAD_ARG;
+    at[q] = b;
+  }
+  for (long q = off[1]; q < off[1] + (long)ext[1][0] * ext[1][1] * ext[1][2]; ++q)
+    if (at[q] < 0) return FLASH_HY_ERR_BAD_ARG;
+  parent.assign(g->nblocks, -1);
+  leaf.assign(g->nblocks, 0);
+  const int nch_all = 1 << g->ndim;
+  for (int b = 0; b < g->nblocks; ++b) {
+    int l = g->block_level[b];
+    const int *cc = &g->block_coords[3 * b];
+    int x = cc[0], y = g->ndim > 1 ? cc[1] : 0, z = g->ndim > 2 ? cc[2] : 0;
+    if (l > 1) {
+      parent[b] = node(l - 1, x / 2, y / 2, z / 2);
+      if (parent[b] < 0) return FLASH_HY_ERR_BAD_ARG;
+    }
+    int nch = 0;
+    for (int o = 0; o < nch_all; ++o)
+      nch += node(l + 1, 2 * x + (o & 1), g->ndim > 1 ? 2 * y + ((o >> 1) & 1) : 0, g->ndim > 2 ? 2 * z + (o >> 2) : 0) >= 0;
+    if (nch != 0 && nch != nch_all) return FLASH_HY_ERR_BAD_ARG;
+    leaf[b] = nch == 0;
+  }
+  return 0;
 }
 
 extern "C" int flash_hy_create(const flash_hy_params *params, const flash_hy_grid_desc *g, int device,
@@ -138,12 +217,26 @@ extern "C" int flash_hy_create(const flash_hy_params *params, const flash_hy_gri
   if (params->gamma <= 1.0 || params->cfl <= 0.0) return FLASH_HY_ERR_BAD_ARG;
   int nz = g->ndim > 2 ? g->nzb : 1, ny = g->ndim > 1 ? g->nyb : 1;
   if (!shape_supported(g->ndim, g->nxb, ny, nz)) return FLASH_HY_ERR_UNSUPPORTED;
-  if (g->max_level > 1) return FLASH_HY_ERR_UNSUPPORTED;
   if (g->nblocks <= 0 || !g->block_coords || g->nguard < 0) return FLASH_HY_ERR_BAD_ARG;
   int nbx = g->nblk_l1[0], nby = g->ndim > 1 ? g->nblk_l1[1] : 1, nbz = g->ndim > 2 ? g->nblk_l1[2] : 1;
-  if (nbx <= 0 || nby <= 0 || nbz <= 0 || (long)nbx * nby * nbz != g->nblocks) return FLASH_HY_ERR_BAD_ARG;
-  std::vector<int> at((size_t)nbx * nby * nbz, -1), coords(3 * (size_t)g->nblocks);
-  for (int b = 0; b < g->nblocks; ++b) {
+  const bool amr = g->max_level > 1;
+  std::vector<int> amr_at, amr_parent, amr_leaf;
+  int amr_off[17], amr_ext[17][3];
+  if (amr) {
+    if (params->precision != FLASH_HY_PREC_FP64 && params->precision != FLASH_HY_PREC_MIXED) return FLASH_HY_ERR_UNSUPPORTED;
+    if (nbx <= 0 || nby <= 0 || nbz <= 0) return FLASH_HY_ERR_BAD_ARG;
+    int rc0 = amr_tables(g, amr_at, amr_off, amr_ext, amr_parent, amr_leaf);
+    if (rc0) return rc0;
+  } else if (nbx <= 0 || nby <= 0 || nbz <= 0 || (long)nbx * nby * nbz != g->nblocks) {
+    return FLASH_HY_ERR_BAD_ARG;
+  }
+  std::vector<int> at(amr ? 0 : (size_t)nbx * nby * nbz, -1), coords(3 * (size_t)g->nblocks);
+  for (int b = 0; b < g->nblocks && amr; ++b) {
+    coords[3 * b] = g->block_coords[3 * b];
+    coords[3 * b + 1] = g->ndim > 1 ? g->block_coords[3 * b + 1] : 0;
+    coords[3 * b + 2] = g->ndim > 2 ? g->block_coords[3 * b + 2] : 0;
+  }
+  for (int b = 0; b < g->nblocks && !amr; ++b) {
     int x = g->block_coords[3 * b], y = g->ndim > 1 ? g->block_coords[3 * b + 1] : 0,
         z = g->ndim > 2 ? g->block_coords[3 * b + 2] : 0;
     if (x < 0 || x >= nbx || y < 0 || y >= nby || z < 0 || z >= nbz) return FLASH_HY_ERR_BAD_ARG;
@@ -186,11 +279,64 @@ extern "C" int flash_hy_create(const flash_hy_params *params, const flash_hy_gri
     for (int v = 0; v < 5; ++v) ALLOC(c->state[s][v], c->ncells * sizeof(double));
   ALLOC(c->acc, 5 * c->ncells * sizeof(double));
   if (g->ndim > 1) ALLOC(c->aux, (size_t)(g->ndim - 1) * 3 * c->ncells * sizeof(double));
-  {
+  if (amr) {
+    c->amr = 1;
+    c->nlev = g->max_level;
+    std::vector<int> slot(g->nblocks, -1), leaves;
+    std::vector<std::vector<int>> lev_leaves(17), lev_parents(17);
+    for (int b = 0; b < g->nblocks; ++b) {
+      int l = g->block_level[b];
+      if (amr_leaf[b]) { slot[b] = (int)leaves.size(); leaves.push_back(b); lev_leaves[l].push_back(b); }
+    }
+    int np = 0;
+    for (int b = 0; b < g->nblocks; ++b)
+      if (!amr_leaf[b]) { slot[b] = np++; lev_parents[g->block_level[b]].push_back(b); }
+    c->nleaves = (int)leaves.size();
+    c->nparents = np;
+    for (int l = 0; l < 17; ++l) {
+      c->at_off[l] = amr_off[l];
+      for (int d = 0; d < 3; ++d) c->at_ext[l][d] = amr_ext[l][d];
+    }
+    const size_t hn = (size_t)(g->nxb + 8) * (g->ndim > 1 ? ny + 8 : 1) * (g->ndim > 2 ? nz + 8 : 1);
+    const size_t nf = g->ndim == 2 ? (size_t)(g->nxb > ny ? g->nxb : ny) : (size_t)g->nxb * ny;
+    int rb = params->precision == FLASH_HY_PREC_MIXED ? 4 : 8;
+    ALLOC(c->sig, sig_bytes_per_block(g->ndim, g->nxb, ny, nz, rb) * c->nleaves);
+    ALLOC(c->d_lh, (size_t)c->nleaves * 5 * hn * sizeof(double));
+    if (np > 0) ALLOC(c->d_gp, (size_t)np * 6 * hn * sizeof(double));
+    ALLOC(c->d_pe, c->ncells * sizeof(double));
+    ALLOC(c->d_freg, (size_t)c->nleaves * 2 * g->ndim * nf * NFLX * sizeof(double));
+    ALLOC(c->d_level, g->nblocks * sizeof(int));
+    ALLOC(c->d_leaf, g->nblocks * sizeof(int));
+    ALLOC(c->d_parent, g->nblocks * sizeof(int));
+    ALLOC(c->d_slot, g->nblocks * sizeof(int));
+    ALLOC(c->d_at, amr_at.size() * sizeof(int));
+    ALLOC(c->d_leaves, leaves.size() * sizeof(int));
+    bool ok = cudaMemcpy(c->d_level, g->block_level, g->nblocks * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemcpy(c->d_leaf, amr_leaf.data(), g->nblocks * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemcpy(c->d_parent, amr_parent.data(), g->nblocks * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemcpy(c->d_slot, slot.data(), g->nblocks * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemcpy(c->d_at, amr_at.data(), amr_at.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemcpy(c->d_leaves, leaves.data(), leaves.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess;
+    for (int l = 1; l <= c->nlev && ok; ++l) {
+      c->lev_leaves[l] = (int)lev_leaves[l].size();
+      c->lev_parents[l] = (int)lev_parents[l].size();
+      if (c->lev_leaves[l]) {
+        ALLOC(c->d_lev_leaves[l], lev_leaves[l].size() * sizeof(int));
+        ok = cudaMemcpy(c->d_lev_leaves[l], lev_leaves[l].data(), lev_leaves[l].size() * sizeof(int),
+                        cudaMemcpyHostToDevice) == cudaSuccess;
+      }
+      if (ok && c->lev_parents[l]) {
+        ALLOC(c->d_lev_parents[l], lev_parents[l].size() * sizeof(int));
+        ok = cudaMemcpy(c->d_lev_parents[l], lev_parents[l].data(), lev_parents[l].size() * sizeof(int),
+                        cudaMemcpyHostToDevice) == cudaSuccess;
+      }
+    }
+    if (!ok) { rc = fail(c, FLASH_HY_ERR_CUDA, "AMR table copies%s", ""); goto bad; }
+  } else {
     int rb = params->precision == FLASH_HY_PREC_MIXED ? 4 : 8;
     ALLOC(c->sig, sig_bytes_per_block(g->ndim, g->nxb, ny, nz, rb) * g->nblocks);
   }
-  ALLOC(c->d_blk_at, at.size() * sizeof(int));
+  if (!amr) ALLOC(c->d_blk_at, at.size() * sizeof(int));
   ALLOC(c->d_blk_coord, coords.size() * sizeof(int));
   ALLOC(c->d_part, g->nblocks * sizeof(CflPart));
   ALLOC(c->d_dt, sizeof(DtInfo));
@@ -204,7 +350,7 @@ extern "C" int flash_hy_create(const flash_hy_params *params, const flash_hy_gri
       cudaMallocHost((void **)&c->h_status, sizeof(unsigned)) != cudaSuccess) {
     rc = fail(c, FLASH_HY_ERR_CUDA, "cudaMallocHost%s", ""); goto bad;
   }
-  if (cudaMemcpy(c->d_blk_at, at.data(), at.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+  if ((!amr && cudaMemcpy(c->d_blk_at, at.data(), at.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess) ||
       cudaMemcpy(c->d_blk_coord, coords.data(), coords.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemset(c->d_status, 0, sizeof(unsigned)) != cudaSuccess) {
     rc = fail(c, FLASH_HY_ERR_CUDA, "init copies%s", ""); goto bad;
@@ -227,6 +373,9 @@ extern "C" int flash_hy_destroy(flash_hy_ctx *c) {
   cudaFree(c->d_wmaster); cudaFree(c->d_mlp); cudaFree(c->d_harvest); cudaFree(c->d_harvest_n);
   drop_graphs(c);
   cudaFree(c->d_stepdt);
+  cudaFree(c->d_level); cudaFree(c->d_leaf); cudaFree(c->d_parent); cudaFree(c->d_slot); cudaFree(c->d_at);
+  cudaFree(c->d_leaves); cudaFree(c->d_lh); cudaFree(c->d_gp); cudaFree(c->d_pe); cudaFree(c->d_freg);
+  for (int l = 0; l < 17; ++l) { cudaFree(c->d_lev_leaves[l]); cudaFree(c->d_lev_parents[l]); }
   if (c->h_dt) cudaFreeHost(c->h_dt);
   if (c->h_status) cudaFreeHost(c->h_status);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -283,7 +432,7 @@ __global__ void k_pack(double *__restrict__ stage, HostLayout L, DevParams P, in
   auto put = [&](int v, double x) { if (v >= 0) stage[unk_index(L, b, hi, hj, hk, v)] = x; };
   put(L.v_dens, rho); put(L.v_velx, vx); put(L.v_vely, vy); put(L.v_velz, vz);
   put(L.v_pres, pres); put(L.v_temp, temp); put(L.v_gamc, P.gamma); put(L.v_eint, e);
-  put(L.v_ener, e + ekin); put(L.v_game, pres / (e * rho) + 1);
+  put(L.v_ener, (P.leaf && !P.leaf[b]) ? P.pe[t] : e + ekin); put(L.v_game, pres / (e * rho) + 1);
 }
 
 static int make_layout(flash_hy_ctx *c, int layout, int nunk, const flash_hy_varmap *vm, int nguard, HostLayout &L) {
@@ -345,6 +494,7 @@ extern "C" int flash_hy_download(flash_hy_ctx *c, double *unk, int layout, int n
   int owned = 0;
   for (int q = 0; q < 10; ++q) owned += (&L.v_dens)[q] >= 0;
   if (!(full && owned == nunk)) CUDA_OK(c, cudaMemcpyAsync(c->d_stage, unk, bytes, cudaMemcpyHostToDevice, c->stream));
+  if (c->amr && amr_restrict_all(c)) return fail(c, FLASH_HY_ERR_CUDA, "restriction launch%s", "");
   DevParams P;
   fill_devparams(c, P);
   k_pack<<<(unsigned)((c->ncells + 255) / 256), 256, 0, c->stream>>>((double *)c->d_stage, L, P, c->nx, c->ny, c->nz,
@@ -358,6 +508,53 @@ extern "C" int flash_hy_download(flash_hy_ctx *c, double *unk, int layout, int n
 // ---------------------------------------------------------------------------
 // step
 // ---------------------------------------------------------------------------
+// AMR: restriction (finest parents first), parent halos (coarsest first),
+// leaf guard cells; returns the number of launches, or -1 on a launch error
+template <int NDIM, int NX, int NY, int NZ>
+static int amr_guard_fill(flash_hy_ctx *c, const DevParams &P) {
+  double *const *st = c->state[c->cur];
+  int n = 0;
+  for (int l = c->nlev - 1; l >= 1; --l) {
+    if (!c->lev_parents[l]) continue;
+    k_restrict<NDIM, NX, NY, NZ><<<c->lev_parents[l], 256, 0, c->stream>>>(P, st[0], st[1], st[2], st[3], st[4],
+                                                                          c->d_lev_parents[l]);
+    ++n;
+  }
+  for (int l = 1; l < c->nlev; ++l) {
+    if (!c->lev_parents[l]) continue;
+    k_parent_halo<NDIM, NX, NY, NZ><<<c->lev_parents[l], 256, 0, c->stream>>>(P, st[0], st[1], st[2], st[3], st[4],
+                                                                             c->d_lev_parents[l]);
+    ++n;
+  }
+  k_leaf_halo<NDIM, NX, NY, NZ><<<c->nleaves, 256, 0, c->stream>>>(P, st[0], st[1], st[2], st[3], st[4], c->d_leaves);
+  ++n;
+  return cudaGetLastError() == cudaSuccess ? n : -1;
+}
+
+static int amr_prepare(flash_hy_ctx *c, const DevParams &P) {
+  if (c->ndim == 2 && c->nx == 8) return amr_guard_fill<2, 8, 8, 1>(c, P);
+  if (c->ndim == 2 && c->nx == 16) return amr_guard_fill<2, 16, 16, 1>(c, P);
+  if (c->ndim == 3) return amr_guard_fill<3, 8, 8, 8>(c, P);
+  return -1;
+}
+
+// parents = restriction of the current leaves (before a download)
+static int amr_restrict_all(flash_hy_ctx *c) {
+  DevParams P;
+  fill_devparams(c, P);
+  double *const *st = c->state[c->cur];
+  for (int l = c->nlev - 1; l >= 1; --l) {
+    if (!c->lev_parents[l]) continue;
+    if (c->ndim == 2 && c->nx == 8)
+      k_restrict<2, 8, 8, 1><<<c->lev_parents[l], 256, 0, c->stream>>>(P, st[0], st[1], st[2], st[3], st[4], c->d_lev_parents[l]);
+    else if (c->ndim == 2)
+      k_restrict<2, 16, 16, 1><<<c->lev_parents[l], 256, 0, c->stream>>>(P, st[0], st[1], st[2], st[3], st[4], c->d_lev_parents[l]);
+    else
+      k_restrict<3, 8, 8, 8><<<c->lev_parents[l], 256, 0, c->stream>>>(P, st[0], st[1], st[2], st[3], st[4], c->d_lev_parents[l]);
+  }
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
 static int enqueue_step(flash_hy_ctx *c, double dt, const int *d_list, int nlaunch, const double *dt_dev = nullptr,
                         bool set_attr = true) {
   StepArgs a;
@@ -374,6 +571,16 @@ static int enqueue_step(flash_hy_ctx *c, double dt, const int *d_list, int nlaun
   a.nlaunch = nlaunch;
   a.threads = c->threads;
   a.stream = c->stream;
+  a.nlev = 0;
+  int pre = 0;
+  if (c->amr) {
+    pre = amr_prepare(c, a.P);
+    if (pre < 0) return fail(c, FLASH_HY_ERR_CUDA, "AMR guard-cell launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    a.nlev = c->nlev;
+    a.leaves = c->d_leaves;
+    a.nleaves = c->nleaves;
+    for (int l = 0; l < 17; ++l) { a.lev_list[l] = c->d_lev_leaves[l]; a.lev_count[l] = c->lev_leaves[l]; }
+  }
   int n;
   switch (c->p.precision) {
     case FLASH_HY_PREC_FP64_FMA: n = step_fp64_fma(a, c->ndim, c->nx, c->ny, c->nz); break;
@@ -382,7 +589,7 @@ static int enqueue_step(flash_hy_ctx *c, double dt, const int *d_list, int nlaun
   }
   if (n == -1) return fail(c, FLASH_HY_ERR_UNSUPPORTED, "unsupported block shape%s", "");
   if (n < 0) return fail(c, FLASH_HY_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(cudaGetLastError()));
-  c->launches = n;
+  c->launches = n + pre;
   return 0;
 }
 
@@ -434,6 +641,7 @@ extern "C" int flash_hy_step_blocks(flash_hy_ctx *c, int blockCount, const int *
                                     double dt, double dtOld, int sweepOrder) {
   (void)timeEndAdv; (void)dtOld; (void)sweepOrder;
   if (!c || blockCount < 0 || (blockCount > 0 && !blockList)) return FLASH_HY_ERR_BAD_ARG;
+  if (c->amr) return fail(c, FLASH_HY_ERR_UNSUPPORTED, "block lists on an AMR hierarchy%s", "");
   if (!(dt > 0.0)) return fail(c, FLASH_HY_ERR_NONPOS_DT, "dt must be positive%s", "");
   for (int q = 0; q < blockCount; ++q)
     if (blockList[q] < 0 || blockList[q] >= c->nblocks) return fail(c, FLASH_HY_ERR_BAD_ARG, "block id out of range%s", "");
@@ -460,12 +668,14 @@ extern "C" int flash_hy_step_blocks(flash_hy_ctx *c, int blockCount, const int *
   return 0;
 }
 
-__global__ void k_dt_reduce(const CflPart *part, int nblocks, const int *blk_level, int ndim, DtInfo *out) {
+__global__ void k_dt_reduce(const CflPart *part, int nblocks, const int *blk_level, const int *leaf, int ndim,
+                            DtInfo *out) {
   __shared__ double sdt[1024];
   __shared__ int sb[1024];
   double best = DBL_MAX;
   int bb = 0x7fffffff;
   for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
+    if (leaf && !leaf[b]) continue;
     double d = part[b].dt;
     if (d < best || (d == best && b < bb)) { best = d; bb = b; }
   }
@@ -488,12 +698,11 @@ __global__ void k_dt_reduce(const CflPart *part, int nblocks, const int *blk_lev
       r.i = part[b].i + NG + 1;
       r.j = ndim > 1 ? part[b].j + NG + 1 : 1;
       r.k = ndim > 2 ? part[b].k + NG + 1 : 1;
-      r.level = 1;
+      r.level = blk_level ? blk_level[b] : 1;
       r.blk = b;
     } else {
       r.i = r.j = r.k = 0; r.level = 0; r.blk = -1;
     }
-    (void)blk_level;
     *out = r;
   }
 }
@@ -512,7 +721,8 @@ extern "C" int flash_hy_compute_dt(flash_hy_ctx *c, double *dt_out, int minloc_o
     if (cfl_state(a, c->ndim, c->nx, c->ny, c->nz) < 0) return fail(c, FLASH_HY_ERR_CUDA, "cfl launch%s", "");
     c->dt_valid = 1;
   }
-  k_dt_reduce<<<1, 1024, 0, c->stream>>>(c->d_part, c->nblocks, nullptr, c->ndim, c->d_dt);
+  k_dt_reduce<<<1, 1024, 0, c->stream>>>(c->d_part, c->nblocks, c->amr ? c->d_level : nullptr,
+                                         c->amr ? c->d_leaf : nullptr, c->ndim, c->d_dt);
   CUDA_OK(c, cudaGetLastError());
   CUDA_OK(c, cudaMemcpyAsync(c->h_dt, c->d_dt, sizeof(DtInfo), cudaMemcpyDeviceToHost, c->stream));
   CUDA_OK(c, cudaMemcpyAsync(c->h_status, c->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));

@@ -49,7 +49,30 @@ struct DevParams {
   unsigned harvest_mask;      // a face is kept when its hash & mask == 0
   double rs_tol;              // exact solver: relative tolerance of p*
   int rs_max_iter;
+  // AMR hierarchy (blk_level == NULL: one uniform level)
+  const int *blk_level;       // level of each node
+  const int *leaf;            // 1 for the leaves
+  const int *parent;          // parent node, -1 on level 1
+  const int *slot;            // leaf slot (guard buffer, sig scratch, flux register) / parent slot (halo)
+  const int *at;              // node by (level, block coordinates), -1 where the level is not refined
+  int at_off[17];
+  int at_ext[17][3];
+  double *lh;                 // leaf guard cells after the EOS: [slot][5][(N+8)^d]
+  double *gp;                 // parent guard-inclusive blocks: [slot][6][(N+8)^d] (rho, v, e, E)
+  double *pe;                 // parents' restricted specific total energy [node * NCB + cell]
+  double *freg;               // fine-face fluxes at fine/coarse faces: [leaf slot][2 ndim][faces][8]
 };
+
+// Cell sizes of block b: level-1 deltas scaled by 2^(1-level) (exact).
+__device__ __forceinline__ void blk_deltas(const DevParams &P, int b, double del[3]) {
+  const double s = P.blk_level ? ldexp(1.0, 1 - P.blk_level[b]) : 1.0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) del[d] = d < P.ndim ? P.del[d] * s : P.del[d];
+}
+
+__device__ __forceinline__ int at_node(const DevParams &P, int l, int x, int y, int z) {
+  return P.at[P.at_off[l] + (z * P.at_ext[l][1] + y) * P.at_ext[l][0] + x];
+}
 
 template <class R> __device__ __forceinline__ R rmax(R a, R b) { return a > b ? a : b; }
 template <class R> __device__ __forceinline__ R rmin(R a, R b) { return a < b ? a : b; }

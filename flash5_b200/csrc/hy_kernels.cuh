@@ -56,10 +56,35 @@ __device__ __forceinline__ size_t cell_src(const DevParams &P, int b, int3 bc, i
   return (size_t)sb * NCB + (size_t)(((gz % NZ) * NY + (gy % NY)) * NX + (gx % NX));
 }
 
+// Guard-inclusive box of a block (NGUARD = 4), the layout of the AMR guard
+// buffers.
+template <int NDIM, int NX, int NY, int NZ> struct Halo {
+  static constexpr int hx = NX + 8, hy = NDIM > 1 ? NY + 8 : 1, hz = NDIM > 2 ? NZ + 8 : 1;
+  static constexpr int n = hx * hy * hz;
+  __device__ static __forceinline__ int idx(int li, int lj, int lk) {
+    return ((lk + (NDIM > 2 ? 4 : 0)) * hy + (lj + (NDIM > 1 ? 4 : 0))) * hx + (li + 4);
+  }
+};
+
+template <int NDIM, int NX, int NY, int NZ>
+__device__ __forceinline__ bool is_inside(int li, int lj, int lk) {
+  return (li >= 0 && li < NX) && (NDIM < 2 || (lj >= 0 && lj < NY)) && (NDIM < 3 || (lk >= 0 && lk < NZ));
+}
+
 // Primitive slots of a cell as hy_getRiemannState sees it: interior cells
 // straight from the state, guard cells after the guard-cell EOS.
 template <int NDIM, int NX, int NY, int NZ, bool GAME = true>
 __device__ __forceinline__ void load_prim(const DevParams &P, int b, int3 bc, int li, int lj, int lk, double V[8]) {
+  if (P.lh && !is_inside<NDIM, NX, NY, NZ>(li, lj, lk)) {
+    // AMR: the leaf guard buffer, filled (and passed through the EOS) by k_leaf_halo
+    using H = Halo<NDIM, NX, NY, NZ>;
+    const double *h = P.lh + (size_t)P.slot[b] * 5 * H::n + H::idx(li, lj, lk);
+    const double rho = h[0], eg = h[4 * H::n];
+    const double p = rho * eg * P.gam1inv;
+    V[HD] = rho; V[HVX] = h[H::n]; V[HVY] = h[2 * H::n]; V[HVZ] = h[3 * H::n]; V[HP] = p;
+    V[HGC] = P.gamma; V[HGE] = GAME ? p / (eg * rho) + 1 : 0.0; V[HEI] = eg;
+    return;
+  }
   bool inside; int fx, fy, fz;
   size_t o = cell_src<NDIM, NX, NY, NZ>(P, b, bc, li, lj, lk, inside, fx, fy, fz);
   double rho = __ldg(P.s_in[0] + o), vx = __ldg(P.s_in[1] + o), vy = __ldg(P.s_in[2] + o);
@@ -83,6 +108,11 @@ __device__ __forceinline__ void load_prim(const DevParams &P, int b, int3 bc, in
 // Pressure only (flattening stencil ends).
 template <int NDIM, int NX, int NY, int NZ>
 __device__ __forceinline__ double load_pres(const DevParams &P, int b, int3 bc, int li, int lj, int lk) {
+  if (P.lh && !is_inside<NDIM, NX, NY, NZ>(li, lj, lk)) {
+    using H = Halo<NDIM, NX, NY, NZ>;
+    const double *h = P.lh + (size_t)P.slot[b] * 5 * H::n + H::idx(li, lj, lk);
+    return h[0] * h[4 * H::n] * P.gam1inv;
+  }
   bool inside; int fx, fy, fz;
   size_t o = cell_src<NDIM, NX, NY, NZ>(P, b, bc, li, lj, lk, inside, fx, fy, fz);
   double rho = __ldg(P.s_in[0] + o), e = __ldg(P.s_in[4] + o);
@@ -149,7 +179,7 @@ __global__ void __launch_bounds__(320) k_sig(const DevParams P, R *__restrict__ 
       if (d == 1) sig_dir<R, 1>(P, Vm, Vc, Vp, s, st);
       else if (d == 2) sig_dir<R, 2>(P, Vm, Vc, Vp, s, st);
       else sig_dir<R, 3>(P, Vm, Vc, Vp, s, st);
-      R *dst = SIG + ((size_t)blockIdx.x * NDIM + (d - 1)) * 6 * B::n + t;
+      R *dst = SIG + ((size_t)(P.slot ? P.slot[b] : (int)blockIdx.x) * NDIM + (d - 1)) * 6 * B::n + t;
 #pragma unroll
       for (int q = 0; q < 6; ++q) dst[(size_t)q * B::n] = s[sig_slot(q)];
     }
@@ -243,6 +273,61 @@ __device__ __forceinline__ void exact_face(const DevParams &P, const double *VL,
 }
 
 // ---------------------------------------------------------------------------
+// AMR flux register (Grid_putFluxData / Grid_conserveFluxes with flux
+// densities): a leaf whose neighbour across a DIR face is coarser stores its
+// boundary face fluxes; a leaf whose neighbour there is a parent replaces
+// its boundary face fluxes by the average of the touching fine leaves'
+// stored fluxes.  Levels are launched finest first, so the fine fluxes are
+// in place.  fidx(along, t1, t2) gives the position of a face in sF, t1/t2
+// the tangential coordinates (y, z for x faces; x, z for y; x, y for z).
+// ---------------------------------------------------------------------------
+template <int NDIM, int NX, int NY, int NZ, int DIR, class FaceIdx>
+__device__ void flux_register(const DevParams &P, int b, int3 bc, double *sF, int fstride, FaceIdx fidx) {
+  constexpr int N = DIR == 1 ? NX : (DIR == 2 ? NY : NZ);
+  constexpr int n1 = DIR == 1 ? NY : NX;
+  constexpr int n2 = NDIM > 2 ? (DIR == 3 ? NY : NZ) : 1;
+  constexpr int NF = n1 * n2;
+  constexpr int T1 = DIR == 1 ? 1 : 0, T2 = DIR == 3 ? 1 : 2;
+  const int l = P.blk_level[b];
+  for (int s = 0; s < 2; ++s) {
+    int pos[3] = {bc.x, bc.y, NDIM > 2 ? bc.z : 0};
+    pos[DIR - 1] += s ? 1 : -1;
+    const int ext = P.at_ext[l][DIR - 1];
+    if (pos[DIR - 1] < 0 || pos[DIR - 1] >= ext) {
+      if (P.bc[2 * (DIR - 1) + s] != -135) continue;          // periodic only
+      pos[DIR - 1] = (pos[DIR - 1] + ext) % ext;
+    }
+    const int m = at_node(P, l, pos[0], pos[1], pos[2]);
+    const int along = s ? N : 0;
+    if (m < 0) {
+      double *dst = P.freg + ((size_t)P.slot[b] * 2 * NDIM + 2 * (DIR - 1) + s) * NF * NFLX;
+      for (int q = threadIdx.x; q < NF * NFLX; q += blockDim.x) {
+        const int face = q / NFLX, v = q % NFLX;
+        dst[q] = sF[v * fstride + fidx(along, face % n1, face / n1)];
+      }
+    } else if (!P.leaf[m]) {
+      const double w = NDIM > 2 ? 0.25 : 0.5;
+      for (int q = threadIdx.x; q < NF * NFLX; q += blockDim.x) {
+        const int face = q / NFLX, v = q % NFLX, q1 = face % n1, q2 = face / n1;
+        int o[3] = {0, 0, 0};
+        o[DIR - 1] = s ? 0 : 1;
+        o[T1] = q1 >= n1 / 2;
+        if (NDIM > 2) o[T2] = q2 >= n2 / 2;
+        const int f = at_node(P, l + 1, 2 * pos[0] + o[0], 2 * pos[1] + o[1], NDIM > 2 ? 2 * pos[2] + o[2] : 0);
+        const double *src = P.freg + ((size_t)P.slot[f] * 2 * NDIM + 2 * (DIR - 1) + (1 - s)) * NF * NFLX;
+        double acc = 0.0;
+        for (int r2 = 0; r2 <= (NDIM > 2 ? 1 : 0); ++r2)
+          for (int r1 = 0; r1 <= 1; ++r1) {
+            const int f1 = 2 * (q1 - o[T1] * (n1 / 2)) + r1, f2 = NDIM > 2 ? 2 * (q2 - o[T2] * (n2 / 2)) + r2 : 0;
+            acc = acc + w * src[(f1 + n1 * f2) * NFLX + v];
+          }
+        sF[v * fstride + fidx(along, q1, q2)] = acc;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // k_dir: one direction of the unsplit update for one block per CTA.
 //   phase 1: face states W-/W+ of the line cells (c_DIR in [-1, N], other
 //            coordinates interior) -- PPM (hy_dataReconstOneStep.F90:485-
@@ -293,10 +378,12 @@ __global__ void __launch_bounds__(320) k_dir(const DevParams P, const R *__restr
   const int3 bc = blk_coords(P, b);
   unsigned st = 0;
   const double dt = P.dt_dev ? *P.dt_dev : P.dt;
-  const double delta = P.del[DIR - 1];
+  double del[3];
+  blk_deltas(P, b, del);
+  const double delta = del[DIR - 1];
   const R dtn = R(dt / delta);
-  const R hdtx = R(0.5 * dt / P.del[0]), hdty = R(0.5 * dt / P.del[1]), hdtz = R(0.5 * dt / P.del[2]);
-  const R *sigb = SIG + (size_t)blockIdx.x * NDIM * 6 * B::n;
+  const R hdtx = R(0.5 * dt / del[0]), hdty = R(0.5 * dt / del[1]), hdtz = R(0.5 * dt / del[2]);
+  const R *sigb = SIG + (size_t)(P.slot ? P.slot[b] : (int)blockIdx.x) * NDIM * 6 * B::n;
 
   // ---------------- phase 1: face states of the line cells ----------------
   for (int t = threadIdx.x; t < G::n; t += blockDim.x) {
@@ -353,9 +440,9 @@ __global__ void __launch_bounds__(320) k_dir(const DevParams P, const R *__restr
       // 1101-1124, 1204-1227
       constexpr int A1 = DIR == 1 ? 2 : (DIR == 2 ? 3 : 1), S1 = DIR == 1 ? 3 : (DIR == 2 ? 1 : 2);
       constexpr int A2 = DIR == 1 ? 3 : (DIR == 2 ? 1 : 2), S2 = DIR == 1 ? 2 : (DIR == 2 ? 3 : 1);
-      const double dA = P.del[A1 - 1], dB = P.del[A2 - 1];
-      const R fac = R(dt * dt / (6. * (DIR == 1 ? P.del[1] : (DIR == 2 ? P.del[2] : P.del[0])) *
-                                 (DIR == 1 ? P.del[2] : (DIR == 2 ? P.del[0] : P.del[1]))));
+      const double dA = del[A1 - 1], dB = del[A2 - 1];
+      const R fac = R(dt * dt / (6. * (DIR == 1 ? del[1] : (DIR == 2 ? del[2] : del[0])) *
+                                 (DIR == 1 ? del[2] : (DIR == 2 ? del[0] : del[1]))));
       (void)dA; (void)dB;
       R T1[8], T2[8];
       {
@@ -424,6 +511,16 @@ __global__ void __launch_bounds__(320) k_dir(const DevParams P, const R *__restr
     sF[FVOLU * G::n + t] = fv;
   }
   __syncthreads();
+  if constexpr (sizeof(R) == 8) {
+    if (P.freg) {       // AMR: fine/coarse faces
+      flux_register<NDIM, NX, NY, NZ, DIR>(P, b, bc, sF, G::n, [](int along, int t1, int t2) {
+        const int i = DIR == 1 ? along : t1, j = DIR == 1 ? t1 : (DIR == 2 ? along : t2),
+                  k = DIR == 3 ? along : (NDIM > 2 ? t2 : 0);
+        return ((k + (DIR == 3)) * G::ry + (j + (DIR == 2))) * G::rx + (i + (DIR == 1));
+      });
+      __syncthreads();
+    }
+  }
 
   // ---------------- phase 3: conservative update ----------------
   const double dtd = dt / delta;
@@ -476,14 +573,14 @@ __global__ void __launch_bounds__(320) k_dir(const DevParams P, const R *__restr
         IntEner = rho0 * e0;
         {
           const double *ax = AUX;
-          IntEner = IntEner + dt / P.del[0] * (ax[off] + pb * ax[ncells + off]);
+          IntEner = IntEner + dt / del[0] * (ax[off] + pb * ax[ncells + off]);
         }
         if (NDIM == 2) {
-          IntEner = IntEner + dt / P.del[1] * (ea + pb * eb);
+          IntEner = IntEner + dt / del[1] * (ea + pb * eb);
         } else {
           const double *ay = AUX + 3 * ncells;
-          IntEner = IntEner + dt / P.del[1] * (ay[off] + pb * ay[ncells + off]);
-          IntEner = IntEner + dt / P.del[2] * (ea + pb * eb);
+          IntEner = IntEner + dt / del[1] * (ay[off] + pb * ay[ncells + off]);
+          IntEner = IntEner + dt / del[2] * (ea + pb * eb);
         }
         IntEner = IntEner + dt * 0.;
       }
@@ -509,9 +606,9 @@ __global__ void __launch_bounds__(320) k_dir(const DevParams P, const R *__restr
       double pres = dens * e * P.gam1inv;
       double c2 = P.gamma * pres / dens;
       double cs = sqrt(c2);
-      double dtl = (fabs(vx - 0.) + cs) * (1.0 / P.del[0]);
-      if (NDIM > 1) dtl = rmax(dtl, (fabs(vy - 0.) + cs) * (1.0 / P.del[1]));
-      if (NDIM > 2) dtl = rmax(dtl, (fabs(vz - 0.) + cs) * (1.0 / P.del[2]));
+      double dtl = (fabs(vx - 0.) + cs) * (1.0 / del[0]);
+      if (NDIM > 1) dtl = rmax(dtl, (fabs(vy - 0.) + cs) * (1.0 / del[1]));
+      if (NDIM > 2) dtl = rmax(dtl, (fabs(vz - 0.) + cs) * (1.0 / del[2]));
       CflCand c; c.key = dtl * P.cfl; c.val = dtl; c.idx = loc;
       cfl_merge(cand, c);
     }
@@ -525,15 +622,21 @@ template <int NDIM, int NX, int NY, int NZ>
 __global__ void __launch_bounds__(320) k_cfl(const DevParams P, CflPart *part) {
   constexpr int NCB = NX * NY * NZ;
   const int b = blockIdx.x;
+  if (P.leaf && !P.leaf[b]) {                 // AMR parents take no part in the time step
+    if (threadIdx.x == 0) { CflPart r; r.dt = DBL_MAX; r.i = r.j = r.k = -1; r.blk = b; part[b] = r; }
+    return;
+  }
+  double del[3];
+  blk_deltas(P, b, del);
   CflCand cand; cand.key = 0.0; cand.val = 0.0; cand.idx = 0x7fffffff;
   for (int loc = threadIdx.x; loc < NCB; loc += blockDim.x) {
     size_t off = (size_t)b * NCB + loc;
     double dens = P.s_in[0][off], vx = P.s_in[1][off], vy = P.s_in[2][off], vz = P.s_in[3][off], e = P.s_in[4][off];
     double pres = dens * e * P.gam1inv;
     double cs = sqrt(P.gamma * pres / dens);
-    double dtl = (fabs(vx - 0.) + cs) * (1.0 / P.del[0]);
-    if (NDIM > 1) dtl = rmax(dtl, (fabs(vy - 0.) + cs) * (1.0 / P.del[1]));
-    if (NDIM > 2) dtl = rmax(dtl, (fabs(vz - 0.) + cs) * (1.0 / P.del[2]));
+    double dtl = (fabs(vx - 0.) + cs) * (1.0 / del[0]);
+    if (NDIM > 1) dtl = rmax(dtl, (fabs(vy - 0.) + cs) * (1.0 / del[1]));
+    if (NDIM > 2) dtl = rmax(dtl, (fabs(vz - 0.) + cs) * (1.0 / del[2]));
     CflCand c; c.key = dtl * P.cfl; c.val = dtl; c.idx = loc;
     cfl_merge(cand, c);
   }

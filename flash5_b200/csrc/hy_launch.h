@@ -16,6 +16,13 @@ struct StepArgs {
   int threads;        // threads per CTA
   cudaStream_t stream;
   bool set_attr;      // raise the kernels' dynamic shared-memory limit (not while capturing a graph)
+  // AMR (nlev > 0): k_sig over all leaves, then per direction one launch per
+  // level, finest first (the flux register needs the fine fluxes first)
+  int nlev;
+  const int *leaves;  // all leaves (device)
+  int nleaves;
+  const int *lev_list[17];  // leaves of each level (device), 1-based levels
+  int lev_count[17];
 };
 
 // Enqueue one hydro step; returns the number of kernel launches, or -1 for an

@@ -134,10 +134,12 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
   const int b = P.blk_list ? P.blk_list[blockIdx.x] : blockIdx.x;
   const int3 bc = blk_coords(P, b);
   unsigned st = 0;
-  const double dt = P.dt_dev ? *P.dt_dev : P.dt, delta = P.del[DIR - 1];
+  double del[3];
+  blk_deltas(P, b, del);
+  const double dt = P.dt_dev ? *P.dt_dev : P.dt, delta = del[DIR - 1];
   const float dtn = float(dt / delta), hdtn = 0.5f * dtn;
-  const float hdtx = float(0.5 * dt / P.del[0]), hdty = float(0.5 * dt / P.del[1]), hdtz = float(0.5 * dt / P.del[2]);
-  const float *sigb = SIG + (size_t)blockIdx.x * NDIM * 6 * B::n;
+  const float hdtx = float(0.5 * dt / del[0]), hdty = float(0.5 * dt / del[1]), hdtz = float(0.5 * dt / del[2]);
+  const float *sigb = SIG + (size_t)(P.slot ? P.slot[b] : (int)blockIdx.x) * NDIM * 6 * B::n;
 
   // ---- A: stage the primitive stencil of every line (guard cells get the EOS)
   for (int s = threadIdx.x; s < G::SA; s += NT) {
@@ -316,8 +318,8 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
     if (NDIM == 3 && P.use_ctu) {
       constexpr int A1 = DIR == 1 ? 2 : (DIR == 2 ? 3 : 1), S1 = DIR == 1 ? 3 : (DIR == 2 ? 1 : 2);
       constexpr int A2 = DIR == 1 ? 3 : (DIR == 2 ? 1 : 2), S2 = DIR == 1 ? 2 : (DIR == 2 ? 3 : 1);
-      const float fac = float(dt * dt / (6. * (DIR == 1 ? P.del[1] : (DIR == 2 ? P.del[2] : P.del[0])) *
-                                         (DIR == 1 ? P.del[2] : (DIR == 2 ? P.del[0] : P.del[1]))));
+      const float fac = float(dt * dt / (6. * (DIR == 1 ? del[1] : (DIR == 2 ? del[2] : del[0])) *
+                                         (DIR == 1 ? del[2] : (DIR == 2 ? del[0] : del[1]))));
       float T1[8], T2[8];
       {
         float sm[8], s0[8], sp[8];
@@ -522,6 +524,12 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
     for (int n = 0; n < 9; ++n) sF[n * G::SC + t] = Fr[it][n];
   }
   __syncthreads();
+  if (P.freg) {         // AMR: fine/coarse faces
+    flux_register<NDIM, NX, NY, NZ, DIR>(P, b, bc, sF, G::SC, [](int along, int t1, int t2) {
+      return G::at(along, t1 + (DIR == 1 ? NY : NX) * t2, G::LC, 1);
+    });
+    __syncthreads();
+  }
 
   // ---- E: conservative update
   const double dtd = dt / delta;
@@ -566,12 +574,12 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
           const double sy = AUX[5 * ncells + off];
           pb = (((0.5 * sx) * 0.5 + sy * 0.25) * 4.0 + sp) / 6.0;
         }
-        IntEner = rho0 * e0 + dt / P.del[0] * (AUX[off] + pb * AUX[ncells + off]);
+        IntEner = rho0 * e0 + dt / del[0] * (AUX[off] + pb * AUX[ncells + off]);
         if (NDIM == 2) {
-          IntEner += dt / P.del[1] * (ea + pb * eb);
+          IntEner += dt / del[1] * (ea + pb * eb);
         } else {
-          IntEner += dt / P.del[1] * (AUX[3 * ncells + off] + pb * AUX[4 * ncells + off]);
-          IntEner += dt / P.del[2] * (ea + pb * eb);
+          IntEner += dt / del[1] * (AUX[3 * ncells + off] + pb * AUX[4 * ncells + off]);
+          IntEner += dt / del[2] * (ea + pb * eb);
         }
       }
       double dens = fmax(U[0], P.smlrho);
@@ -590,9 +598,9 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
       if (!(isfinite(dens) && isfinite(vx) && isfinite(vy) && isfinite(vz) && isfinite(e))) st |= ST_NAN;
       double pres = dens * e * P.gam1inv;
       double cs = sqrt(P.gamma * pres * rinv);
-      double dtl = (fabs(vx) + cs) * (1.0 / P.del[0]);
-      if (NDIM > 1) dtl = fmax(dtl, (fabs(vy) + cs) * (1.0 / P.del[1]));
-      if (NDIM > 2) dtl = fmax(dtl, (fabs(vz) + cs) * (1.0 / P.del[2]));
+      double dtl = (fabs(vx) + cs) * (1.0 / del[0]);
+      if (NDIM > 1) dtl = fmax(dtl, (fabs(vy) + cs) * (1.0 / del[1]));
+      if (NDIM > 2) dtl = fmax(dtl, (fabs(vz) + cs) * (1.0 / del[2]));
       CflCand c; c.key = dtl * P.cfl; c.val = dtl; c.idx = loc;
       cfl_merge(cand, c);
     }

@@ -23,7 +23,7 @@ typedef double Real;
 namespace fhy {
 
 template <int NDIM, int NX, int NY, int NZ, int DIR, bool FIRST, bool LAST, int RS>
-static bool launch_dir(const StepArgs &a) {
+static bool launch_dir_one(const StepArgs &a) {
 #if FHY_VARIANT == 3
   using G = MxGeom<NDIM, NX, NY, NZ, DIR, RS>;
   auto kern = k_dir_mx<NDIM, NX, NY, NZ, DIR, FIRST, LAST, RS>;
@@ -40,20 +40,47 @@ static bool launch_dir(const StepArgs &a) {
   return cudaGetLastError() == cudaSuccess;
 }
 
+// one direction: a single launch, or on an AMR hierarchy one launch per
+// level, finest first
+template <int NDIM, int NX, int NY, int NZ, int DIR, bool FIRST, bool LAST, int RS>
+static bool launch_dir(const StepArgs &a) {
+  if (a.nlev == 0) return launch_dir_one<NDIM, NX, NY, NZ, DIR, FIRST, LAST, RS>(a);
+  StepArgs b = a;
+  for (int l = a.nlev; l >= 1; --l) {
+    if (a.lev_count[l] == 0) continue;
+    b.P.blk_list = a.lev_list[l];
+    b.nlaunch = a.lev_count[l];
+    if (!launch_dir_one<NDIM, NX, NY, NZ, DIR, FIRST, LAST, RS>(b)) return false;
+    b.set_attr = false;
+  }
+  return true;
+}
+
 // RS: 0 = HLLC, 1 = exact Riemann solver
 template <int NDIM, int NX, int NY, int NZ, int RS>
 static int run_rs(const StepArgs &a) {
-  k_sig<NDIM, NX, NY, NZ, Real, FHY_VARIANT><<<a.nlaunch, a.threads, 0, a.stream>>>(a.P, (Real *)a.sig);
+  if (a.nlev == 0) {
+    k_sig<NDIM, NX, NY, NZ, Real, FHY_VARIANT><<<a.nlaunch, a.threads, 0, a.stream>>>(a.P, (Real *)a.sig);
+  } else {
+    DevParams P = a.P;
+    P.blk_list = a.leaves;
+    k_sig<NDIM, NX, NY, NZ, Real, FHY_VARIANT><<<a.nleaves, a.threads, 0, a.stream>>>(P, (Real *)a.sig);
+  }
   if (cudaGetLastError() != cudaSuccess) return -2;
+  int nl = 1;
+  if (a.nlev > 0) {
+    nl = 0;
+    for (int l = 1; l <= a.nlev; ++l) nl += a.lev_count[l] > 0;
+  }
   if constexpr (NDIM == 2) {
     const bool ok =
         launch_dir<NDIM, NX, NY, NZ, 1, true, false, RS>(a) && launch_dir<NDIM, NX, NY, NZ, 2, false, true, RS>(a);
-    return ok ? 3 : -2;
+    return ok ? 1 + 2 * nl : -2;
   } else {
     const bool ok = launch_dir<NDIM, NX, NY, NZ, 1, true, false, RS>(a) &&
                     launch_dir<NDIM, NX, NY, NZ, 2, false, false, RS>(a) &&
                     launch_dir<NDIM, NX, NY, NZ, 3, false, true, RS>(a);
-    return ok ? 4 : -2;
+    return ok ? 1 + 3 * nl : -2;
   }
 }
 
