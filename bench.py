@@ -343,6 +343,111 @@ def riemann_workload(args):
     return 0
 
 
+def amr_workload(args):
+    """Batched AMR hierarchy, 2D four-quadrant Riemann problem: 4 levels,
+    about 19.5k leaf blocks of 16^2 refined where a seeded smoothed density
+    gradient is large; every level advanced in one graph-replayed step with
+    one dt, fine/coarse flux correction on.  FP64 and mixed precision."""
+    import torch
+    from flash5_b200 import abi, setups
+    from flash5_b200.amr import four_quadrant_hierarchy
+    from flash5_b200.grid import VAR
+    from flash5_b200.hydro import Hydro
+    torch.cuda.set_device(0)
+    t0 = time.perf_counter()
+    g = four_quadrant_hierarchy(nblk=args.amr_nblk)
+    unk = setups.four_quadrant(g)
+    build_s = time.perf_counter() - t0
+    zones = g.ncells
+    peak, peak_kind = measured_peaks()
+    ms, outs, dts, launches, clocks, e2e_ms, hb = {}, {}, None, {}, None, None, None
+    paths = [p for p in args.paths.split(",") if p in ("fp64", "mixed", "mixed_exact")] or ["fp64", "mixed"]
+    spec = {"fp64": (abi.PREC_FP64, abi.RS_HLLC), "mixed": (abi.PREC_MIXED, abi.RS_HLLC),
+            "mixed_exact": (abi.PREC_MIXED, abi.RS_EXACT)}
+    for name in paths:
+        pr, rsv = spec[name]
+        h = Hydro(abi.default_params(precision=pr, riemann_solver=rsv), g)
+        h.upload(unk)
+        headline = name == paths[-1]
+        sampler = ClockSampler(0) if headline else None
+        ms[name], used, launches[name] = run_device(h, args.steps, args.warmup, dts=dts, sampler=sampler)
+        if dts is None:
+            dts = used
+        if headline:
+            clocks = sampler.summary()
+        outs[name] = np.empty_like(unk)
+        h.download(outs[name])
+        if headline and not args.no_e2e:
+            pinned = torch.empty(unk.shape, dtype=torch.float64, pin_memory=True)
+            host = pinned.numpy()
+            host[...] = unk
+            e2e_ms = run_e2e(h, host, max(3, min(args.steps, 8)), 3)
+            hb = host.nbytes
+        h.close()
+    head = paths[-1]
+    leaves = g.leaf_ids
+    errs = {n: conserved_l1(outs[n][leaves], outs["fp64"][leaves], VAR) for n in outs if n != "fp64" and "fp64" in outs}
+    cpu = None if args.no_cpu else amr_cpu_baseline()
+    achieved = zones * BYTES_PER_ZONE / (ms[head] * 1e-3) / 1e9
+    levels = np.bincount(g.levels[g.is_leaf], minlength=g.max_level + 1)[1:].tolist()
+    line = {
+        "metric": METRIC, "value": zones / (ms[head] * 1e-3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms[head], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 reconstruction, f64 Riemann/update" if head.startswith("mixed") else "f64",
+        "data": "synthetic (four-quadrant states; hierarchy from a seeded smoothed density, PCG64 seed 2024)",
+        "config": {"workload": f"2D four-quadrant Riemann problem on a {g.max_level}-level AMR hierarchy, "
+                               f"{g.nleaves} leaf blocks of 16^2 + 4 guard ({levels} per level), "
+                               f"{g.nblocks - g.nleaves} parents; PPM+HLLC, CFL 0.8, one dt for all levels, "
+                               "fine/coarse flux correction, graph-replayed step",
+                   "zones_per_gpu": zones, "leaf_blocks": g.nleaves,
+                   "l2": f"inputs larger than L2 (state {g.nblocks * 256 * 40 / 1e6:.0f} MB plus guard buffers "
+                         f"{g.nleaves * 576 * 40 / 1e6:.0f} MB)", "path": head, "hierarchy_build_s": build_s},
+        "paths": {n: {"value": zones / (ms[n] * 1e-3), "ms_per_step": ms[n],
+                      **({"rel_l1_vs_fp64": errs[n]} if n in errs else {})} for n in ms},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_kind": peak_kind,
+                     "kernel": "one AMR step (restriction, halos, k_sig, per-level k_dir), 80 B/leaf zone algorithmic"},
+        "clocks": clocks, "gpu_launches": launches[head] * args.steps,
+    }
+    if "fp64" in ms and head != "fp64":
+        line["speedup_vs_fp64"] = ms["fp64"] / ms[head]
+    if e2e_ms is not None:
+        line["e2e"] = {"value": zones / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": hb,
+                       "d2h_bytes_per_step": hb, "ms_per_step": e2e_ms,
+                       "path": "flash_hy_upload + flash_hy_step + flash_hy_compute_dt + flash_hy_download, "
+                               "every node's FLASH UNK (11 vars), pinned host memory"}
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line))
+    return 0
+
+
+def amr_cpu_baseline(seconds=10.0):
+    """Oracle AMR step on a 16x16-root, 3-level four-quadrant hierarchy
+    (same refinement rule), all host threads."""
+    from flash5_b200 import abi, setups
+    from flash5_b200.amr import four_quadrant_hierarchy
+    from flash5_b200.hydro import next_dt
+    from oracle import orc
+    g = four_quadrant_hierarchy(nblk=16, max_level=3)
+    p = abi.default_params()
+    unk = setups.four_quadrant(g)
+    o = orc.Oracle(p, g)
+    o.eos_init(unk)
+    _, dt, _ = o.compute_dt(unk)
+    n, t0 = 0, time.perf_counter()
+    while n < 2 or time.perf_counter() - t0 < seconds:
+        o.hydro(unk, dt, dt, dt)
+        _, dcfl, _ = o.compute_dt(unk)
+        dt = next_dt(dcfl, dt)
+        n += 1
+    el = time.perf_counter() - t0
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
+    return {"value": g.ncells * n / el, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"2D four-quadrant AMR, 16^2 root blocks, 3 levels, {g.nleaves} leaves, {n} steps, "
+                      f"{el:.1f} s, oracle C port, OpenMP"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -352,7 +457,8 @@ def main():
     ap.add_argument("--nblk", type=int, default=32, help="blocks per axis (32 -> 256^3)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="kh", choices=["kh", "riemann"])
+    ap.add_argument("--workload", default="kh", choices=["kh", "riemann", "amr"])
+    ap.add_argument("--amr-nblk", type=int, default=32, help="root blocks per axis of the AMR hierarchy")
     ap.add_argument("--riemann-n", type=int, default=100_000_000)
     ap.add_argument("--paths", default="fp64,fp64_exact,mixed,mixed_exact,mixed_learned",
                     help="comma list of paths to time; profiling runs use one")
@@ -362,6 +468,11 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     warmup = max(3, args.warmup)
+    if args.workload == "amr" and args.impl == "ours":
+        if rank != 0:
+            return 0
+        args.warmup = warmup
+        return amr_workload(args)
     if args.workload == "riemann" and args.impl == "ours":
         if rank != 0:
             return 0
