@@ -121,6 +121,10 @@ def _set_sigs(lib):
         "flash_hy_set_guess_weights": (C.c_int, [vp, C.POINTER(C.c_float), C.c_int]),
         "flash_hy_harvest": (C.c_int, [vp, C.c_longlong, C.c_int]),
         "flash_hy_harvest_fetch": (C.c_int, [vp, vp, C.c_longlong, C.POINTER(C.c_longlong)]),
+        "flash_hy_set_owned_blocks": (C.c_int, [vp, C.c_int, ip]),
+        "flash_hy_set_exchange": (C.c_int, [vp, C.c_int, ip, C.c_int, ip]),
+        "flash_hy_pack": (C.c_int, [vp, vp]),
+        "flash_hy_unpack": (C.c_int, [vp, vp]),
     }
     for name, (res, args) in sigs.items():
         f = getattr(lib, name)

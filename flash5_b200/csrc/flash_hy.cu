@@ -63,6 +63,12 @@ struct flash_hy_ctx {
   int *d_lev_parents[17], lev_parents[17];
   int nparents;
   double *d_lh, *d_gp, *d_pe, *d_freg;
+  // a rank's share of a sharded grid: owned blocks and the ghost exchange
+  bool partial;
+  int *h_blk_at;               // host copy of the block table (partial grids)
+  int *d_owned, n_owned;       // blocks the step advances
+  int *d_owned_mask;           // 1 for owned blocks (dt reduction)
+  int *d_send, n_send, *d_recv, n_recv;  // blocks packed for / unpacked from other ranks
   char err[512];
 };
 
@@ -227,9 +233,12 @@ extern "C" int flash_hy_create(const flash_hy_params *params, const flash_hy_gri
     if (nbx <= 0 || nby <= 0 || nbz <= 0) return FLASH_HY_ERR_BAD_ARG;
     int rc0 = amr_tables(g, amr_at, amr_off, amr_ext, amr_parent, amr_leaf);
     if (rc0) return rc0;
-  } else if (nbx <= 0 || nby <= 0 || nbz <= 0 || (long)nbx * nby * nbz != g->nblocks) {
+  } else if (nbx <= 0 || nby <= 0 || nbz <= 0 || (long)nbx * nby * nbz < g->nblocks) {
     return FLASH_HY_ERR_BAD_ARG;
   }
+  // fewer blocks than positions: a rank's share of a grid (owned + ghost
+  // blocks); such a context steps only the owned blocks it is given
+  const bool partial = !amr && (long)nbx * nby * nbz > g->nblocks;
   std::vector<int> at(amr ? 0 : (size_t)nbx * nby * nbz, -1), coords(3 * (size_t)g->nblocks);
   for (int b = 0; b < g->nblocks && amr; ++b) {
     coords[3 * b] = g->block_coords[3 * b];
@@ -255,6 +264,11 @@ extern "C" int flash_hy_create(const flash_hy_params *params, const flash_hy_gri
   c->p = *params;
   c->ndim = g->ndim; c->nx = g->nxb; c->ny = ny; c->nz = nz;
   c->nblocks = g->nblocks; c->nbx = nbx; c->nby = nby; c->nbz = nbz;
+  c->partial = partial;
+  if (partial) {
+    c->h_blk_at = (int *)malloc(at.size() * sizeof(int));
+    memcpy(c->h_blk_at, at.data(), at.size() * sizeof(int));
+  }
   for (int f = 0; f < 6; ++f) c->bc[f] = f < 2 * g->ndim ? g->bc[f] : FLASH_HY_BC_OUTFLOW;
   int nb[3] = {g->nxb, ny, nz}, nbl[3] = {nbx, nby, nbz};
   for (int d = 0; d < 3; ++d)
@@ -376,6 +390,8 @@ extern "C" int flash_hy_destroy(flash_hy_ctx *c) {
   cudaFree(c->d_level); cudaFree(c->d_leaf); cudaFree(c->d_parent); cudaFree(c->d_slot); cudaFree(c->d_at);
   cudaFree(c->d_leaves); cudaFree(c->d_lh); cudaFree(c->d_gp); cudaFree(c->d_pe); cudaFree(c->d_freg);
   for (int l = 0; l < 17; ++l) { cudaFree(c->d_lev_leaves[l]); cudaFree(c->d_lev_parents[l]); }
+  cudaFree(c->d_owned); cudaFree(c->d_owned_mask); cudaFree(c->d_send); cudaFree(c->d_recv);
+  free(c->h_blk_at);
   if (c->h_dt) cudaFreeHost(c->h_dt);
   if (c->h_status) cudaFreeHost(c->h_status);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -598,8 +614,12 @@ extern "C" int flash_hy_step(flash_hy_ctx *c, double simTime, double dt, double 
   if (!c) return FLASH_HY_ERR_BAD_ARG;
   if (!(dt > 0.0)) return fail(c, FLASH_HY_ERR_NONPOS_DT, "dt must be positive%s", "");
   CUDA_OK(c, cudaSetDevice(c->device));
+  if (c->partial && c->n_owned == 0)
+    return fail(c, FLASH_HY_ERR_UNSUPPORTED, "a partial grid needs its owned blocks (flash_hy_set_owned_blocks)%s", "");
+  const int *step_list = c->n_owned ? c->d_owned : nullptr;
+  const int step_n = c->n_owned ? c->n_owned : c->nblocks;
   if (!c->use_graph) {
-    int rc = enqueue_step(c, dt, nullptr, c->nblocks);
+    int rc = enqueue_step(c, dt, step_list, step_n);
     if (rc) return rc;
   } else {
     const int q = c->cur;
@@ -608,7 +628,7 @@ extern "C" int flash_hy_step(flash_hy_ctx *c, double simTime, double dt, double 
     if (!c->gexec[q] && c->plain_steps[q] == 0) {
       // first step of this parity runs uncaptured (it also sets the kernels'
       // shared-memory attributes, which are not stream work)
-      int rc = enqueue_step(c, dt, nullptr, c->nblocks, c->d_stepdt, true);
+      int rc = enqueue_step(c, dt, step_list, step_n, c->d_stepdt, true);
       if (rc) return rc;
       c->plain_steps[q]++;
       c->launches = c->launches + 1;
@@ -616,7 +636,7 @@ extern "C" int flash_hy_step(flash_hy_ctx *c, double simTime, double dt, double 
       if (!c->gexec[q]) {
         cudaGraph_t g = nullptr;
         CUDA_OK(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-        int rc = enqueue_step(c, dt, nullptr, c->nblocks, c->d_stepdt, false);
+        int rc = enqueue_step(c, dt, step_list, step_n, c->d_stepdt, false);
         cudaError_t ec = cudaStreamEndCapture(c->stream, &g);
         if (rc) { if (g) cudaGraphDestroy(g); return rc; }
         if (ec != cudaSuccess) return fail(c, FLASH_HY_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ec));
@@ -722,7 +742,8 @@ extern "C" int flash_hy_compute_dt(flash_hy_ctx *c, double *dt_out, int minloc_o
     c->dt_valid = 1;
   }
   k_dt_reduce<<<1, 1024, 0, c->stream>>>(c->d_part, c->nblocks, c->amr ? c->d_level : nullptr,
-                                         c->amr ? c->d_leaf : nullptr, c->ndim, c->d_dt);
+                                         c->amr ? c->d_leaf : (c->n_owned ? c->d_owned_mask : nullptr), c->ndim,
+                                         c->d_dt);
   CUDA_OK(c, cudaGetLastError());
   CUDA_OK(c, cudaMemcpyAsync(c->h_dt, c->d_dt, sizeof(DtInfo), cudaMemcpyDeviceToHost, c->stream));
   CUDA_OK(c, cudaMemcpyAsync(c->h_status, c->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
@@ -811,5 +832,117 @@ extern "C" int flash_hy_harvest_fetch(flash_hy_ctx *c, double *d_states, long lo
   CUDA_OK(c, cudaMemsetAsync(c->d_harvest_n, 0, sizeof(unsigned long long), c->stream));
   CUDA_OK(c, cudaStreamSynchronize(c->stream));
   *n_out = n;
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// sharded grids: owned blocks and the ghost-block exchange
+// ---------------------------------------------------------------------------
+extern "C" int flash_hy_set_owned_blocks(flash_hy_ctx *c, int n, const int *list) {
+  if (!c || n <= 0 || !list || c->amr) return fail(c, FLASH_HY_ERR_BAD_ARG, "set_owned_blocks: %s", "bad arguments");
+  std::vector<int> mask(c->nblocks, 0);
+  for (int q = 0; q < n; ++q) {
+    if (list[q] < 0 || list[q] >= c->nblocks || mask[list[q]])
+      return fail(c, FLASH_HY_ERR_BAD_ARG, "set_owned_blocks: %s", "block out of range or repeated");
+    mask[list[q]] = 1;
+  }
+  if (c->partial) {
+    // every block an owned block reads guard cells from must be present
+    std::vector<int> coords(3 * (size_t)c->nblocks);
+    CUDA_OK(c, cudaSetDevice(c->device));
+    CUDA_OK(c, cudaMemcpy(coords.data(), c->d_blk_coord, coords.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    const int nbl[3] = {c->nbx, c->nby, c->nbz};
+    for (int q = 0; q < n; ++q) {
+      const int *cc = &coords[3 * list[q]];
+      for (int o = 0; o < 27; ++o) {
+        int off[3] = {o % 3 - 1, (o / 3) % 3 - 1, o / 9 - 1}, p[3];
+        bool ok = true;
+        for (int d = 0; d < 3; ++d) {
+          if (d >= c->ndim) { if (off[d]) ok = false; p[d] = 0; continue; }
+          p[d] = cc[d] + off[d];
+          if (p[d] < 0 || p[d] >= nbl[d]) {
+            if (c->bc[2 * d] != FLASH_HY_BC_PERIODIC) { p[d] = cc[d]; continue; }   // boundary: own cells
+            p[d] = (p[d] + nbl[d]) % nbl[d];
+          }
+        }
+        if (!ok) continue;
+        if (c->h_blk_at[((size_t)p[2] * c->nby + p[1]) * c->nbx + p[0]] < 0)
+          return fail(c, FLASH_HY_ERR_BAD_ARG, "set_owned_blocks: %s", "a neighbour of an owned block is absent");
+      }
+    }
+  }
+  CUDA_OK(c, cudaSetDevice(c->device));
+  CUDA_OK(c, cudaStreamSynchronize(c->stream));
+  cudaFree(c->d_owned); cudaFree(c->d_owned_mask);
+  c->d_owned = nullptr; c->d_owned_mask = nullptr; c->n_owned = 0;
+  CUDA_OK(c, cudaMalloc((void **)&c->d_owned, n * sizeof(int)));
+  CUDA_OK(c, cudaMalloc((void **)&c->d_owned_mask, c->nblocks * sizeof(int)));
+  CUDA_OK(c, cudaMemcpy(c->d_owned, list, n * sizeof(int), cudaMemcpyHostToDevice));
+  CUDA_OK(c, cudaMemcpy(c->d_owned_mask, mask.data(), c->nblocks * sizeof(int), cudaMemcpyHostToDevice));
+  c->n_owned = n;
+  c->dt_valid = 0;
+  drop_graphs(c);
+  return 0;
+}
+
+extern "C" int flash_hy_set_exchange(flash_hy_ctx *c, int nsend, const int *send, int nrecv, const int *recv) {
+  if (!c || nsend < 0 || nrecv < 0 || (nsend && !send) || (nrecv && !recv))
+    return fail(c, FLASH_HY_ERR_BAD_ARG, "set_exchange: %s", "bad arguments");
+  for (int q = 0; q < nsend; ++q)
+    if (send[q] < 0 || send[q] >= c->nblocks) return fail(c, FLASH_HY_ERR_BAD_ARG, "set_exchange: %s", "send block");
+  for (int q = 0; q < nrecv; ++q)
+    if (recv[q] < 0 || recv[q] >= c->nblocks) return fail(c, FLASH_HY_ERR_BAD_ARG, "set_exchange: %s", "recv block");
+  CUDA_OK(c, cudaSetDevice(c->device));
+  CUDA_OK(c, cudaStreamSynchronize(c->stream));
+  cudaFree(c->d_send); cudaFree(c->d_recv);
+  c->d_send = c->d_recv = nullptr;
+  c->n_send = c->n_recv = 0;
+  if (nsend) {
+    CUDA_OK(c, cudaMalloc((void **)&c->d_send, nsend * sizeof(int)));
+    CUDA_OK(c, cudaMemcpy(c->d_send, send, nsend * sizeof(int), cudaMemcpyHostToDevice));
+  }
+  if (nrecv) {
+    CUDA_OK(c, cudaMalloc((void **)&c->d_recv, nrecv * sizeof(int)));
+    CUDA_OK(c, cudaMemcpy(c->d_recv, recv, nrecv * sizeof(int), cudaMemcpyHostToDevice));
+  }
+  c->n_send = nsend;
+  c->n_recv = nrecv;
+  return 0;
+}
+
+// buf[i][v][cell] <-> state[v][list[i] * ncb + cell], one CTA per listed block
+__global__ void k_blocks_to_buf(const double *s0, const double *s1, const double *s2, const double *s3,
+                                const double *s4, const int *list, int ncb, double *buf) {
+  const double *st[5] = {s0, s1, s2, s3, s4};
+  const size_t b = (size_t)list[blockIdx.x];
+  double *dst = buf + (size_t)blockIdx.x * 5 * ncb;
+  for (int t = threadIdx.x; t < 5 * ncb; t += blockDim.x) dst[t] = st[t / ncb][b * ncb + t % ncb];
+}
+__global__ void k_buf_to_blocks(double *s0, double *s1, double *s2, double *s3, double *s4, const int *list, int ncb,
+                                const double *buf) {
+  double *st[5] = {s0, s1, s2, s3, s4};
+  const size_t b = (size_t)list[blockIdx.x];
+  const double *src = buf + (size_t)blockIdx.x * 5 * ncb;
+  for (int t = threadIdx.x; t < 5 * ncb; t += blockDim.x) st[t / ncb][b * ncb + t % ncb] = src[t];
+}
+
+extern "C" int flash_hy_pack(flash_hy_ctx *c, double *d_buf) {
+  if (!c || (c->n_send && !d_buf)) return FLASH_HY_ERR_BAD_ARG;
+  if (!c->n_send) return 0;
+  CUDA_OK(c, cudaSetDevice(c->device));
+  double *const *st = c->state[c->cur];
+  k_blocks_to_buf<<<c->n_send, 256, 0, c->stream>>>(st[0], st[1], st[2], st[3], st[4], c->d_send, (int)c->ncb, d_buf);
+  CUDA_OK(c, cudaGetLastError());
+  return 0;
+}
+
+extern "C" int flash_hy_unpack(flash_hy_ctx *c, const double *d_buf) {
+  if (!c || (c->n_recv && !d_buf)) return FLASH_HY_ERR_BAD_ARG;
+  if (!c->n_recv) return 0;
+  CUDA_OK(c, cudaSetDevice(c->device));
+  double *const *st = c->state[c->cur];
+  k_buf_to_blocks<<<c->n_recv, 256, 0, c->stream>>>(st[0], st[1], st[2], st[3], st[4], c->d_recv, (int)c->ncb, d_buf);
+  CUDA_OK(c, cudaGetLastError());
+  c->dt_valid = 0;
   return 0;
 }

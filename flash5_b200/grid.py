@@ -31,6 +31,7 @@ class UniformGrid:
             bc = [bc] * 6
         code = {"outflow": abi.BC_OUTFLOW, "periodic": abi.BC_PERIODIC, "reflecting": abi.BC_REFLECTING}
         self.bc = [code[b] if isinstance(b, str) else int(b) for b in bc]
+        self.bc += [abi.BC_OUTFLOW] * (6 - len(self.bc))      # faces of absent dimensions
         coords = [(bx, by, bz) for bz in range(self.nblk[2]) for by in range(self.nblk[1]) for bx in range(self.nblk[0])]
         if order == "morton":
             def key(c):

@@ -95,6 +95,25 @@ class Hydro:
     def sync(self):
         self._check(self.lib.flash_hy_sync(self.ctx))
 
+    # -- sharded grids ----------------------------------------------------
+    def set_owned_blocks(self, blocks):
+        bl = np.ascontiguousarray(blocks, dtype=np.int32)
+        self._check(self.lib.flash_hy_set_owned_blocks(self.ctx, len(bl), bl.ctypes.data_as(C.POINTER(C.c_int))))
+
+    def set_exchange(self, send, recv):
+        s = np.ascontiguousarray(send, dtype=np.int32)
+        r = np.ascontiguousarray(recv, dtype=np.int32)
+        self._check(self.lib.flash_hy_set_exchange(self.ctx, len(s), s.ctypes.data_as(C.POINTER(C.c_int)), len(r),
+                                                   r.ctypes.data_as(C.POINTER(C.c_int))))
+
+    def pack(self, buf):
+        """Enqueue the packing of the send blocks into a device buffer (a
+        CUDA tensor or a device address) on the context's stream."""
+        self._check(self.lib.flash_hy_pack(self.ctx, C.c_void_p(_addr(buf))))
+
+    def unpack(self, buf):
+        self._check(self.lib.flash_hy_unpack(self.ctx, C.c_void_p(_addr(buf))))
+
     # -- exact Riemann solver: learned guess and its training data ---------
     def set_guess_weights(self, w):
         """Attach the learned star-pressure guess (FP32 master weights, the
@@ -126,6 +145,10 @@ class Hydro:
     @property
     def last_launch_count(self):
         return self.lib.flash_hy_last_launch_count(self.ctx)
+
+
+def _addr(buf):
+    return buf.data_ptr() if hasattr(buf, "data_ptr") else int(buf)
 
 
 def next_dt(dt_cfl, dt_old, tstep_change_factor=2.0, dtmin=1e-10, dtmax=1e5):

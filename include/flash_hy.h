@@ -178,6 +178,27 @@ int flash_hy_set_guess_weights(flash_hy_ctx *ctx, const float *w, int n);
 int flash_hy_harvest(flash_hy_ctx *ctx, long long cap, int keep_log2);
 int flash_hy_harvest_fetch(flash_hy_ctx *ctx, double *d_states, long long n_max, long long *n_out);
 
+/* ---- sharded grids (one context per GPU / MPI rank) ----------------------
+ * FLASH distributes blocks over MPI ranks (PARAMESH Morton order, UG process
+ * grid) and fills guard cells from other ranks' blocks in
+ * Grid_fillGuardCells (UG gr_shiftData.F90:100-173); the dt reduction is the
+ * MPI_MINLOC of Driver_computeDt.F90:376-377.  A rank's context is created
+ * from its share of the grid: its owned blocks plus ghost blocks (copies of
+ * other ranks' blocks touching an owned block), all with global block
+ * coordinates and the global nblk_l1.  set_owned_blocks names the blocks
+ * flash_hy_step advances and flash_hy_compute_dt reduces over (local
+ * indices; every block an owned block reads guard cells from must be
+ * present); set_exchange names the local blocks packed for other ranks and
+ * those unpacked from them; pack / unpack copy the 5 state variables of
+ * those blocks (nblocks x 5 x nxb*nyb*nzb doubles, DEVICE buffers) on the
+ * context's stream.  Ghost blocks are not advanced: unpack fresh copies
+ * before every step.                                                     */
+int flash_hy_set_owned_blocks(flash_hy_ctx *ctx, int n, const int *blocks);
+int flash_hy_set_exchange(flash_hy_ctx *ctx, int nsend, const int *send_blocks, int nrecv,
+                          const int *recv_blocks);
+int flash_hy_pack(flash_hy_ctx *ctx, double *d_buf);
+int flash_hy_unpack(flash_hy_ctx *ctx, const double *d_buf);
+
 /* ---- CFL time step without any device allocation ------------------------
  * No counterpart in the reference: FLASH5's Hydro_computeDt runs on host
  * arrays.  This entry point is for callers that cannot call cudaMalloc

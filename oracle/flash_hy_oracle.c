@@ -825,7 +825,10 @@ int orc_fill_guardcells(const flash_hy_params *p, const flash_hy_grid_desc *g, d
   if (st) return st;
   ctx_t c; ctx_init(&c, p, g);
   int nbx = g->nblk_l1[0], nby = g->ndim > 1 ? g->nblk_l1[1] : 1, nbz = g->ndim > 2 ? g->nblk_l1[2] : 1;
+  /* a rank's share of a grid holds only some block positions: guard cells
+   * whose source block is absent are left as they are */
   int *owner = malloc(sizeof(int) * nbx * nby * nbz);
+  for (int q = 0; q < nbx * nby * nbz; ++q) owner[q] = -1;
   for (int b = 0; b < g->nblocks; ++b) {
     const int *bc = &g->block_coords[3 * b];
     owner[((g->ndim > 2 ? bc[2] : 0) * nby + (g->ndim > 1 ? bc[1] : 0)) * nbx + bc[0]] = b;
@@ -845,6 +848,7 @@ int orc_fill_guardcells(const flash_hy_params *p, const flash_hy_grid_desc *g, d
           int gy = c.k2 ? map_axis(bc[1] * c.nyb + lj, NY, g->bc[2], g->bc[3], &fy) : 0;
           int gz = c.k3 ? map_axis(bc[2] * c.nzb + lk, NZ, g->bc[4], g->bc[5], &fz) : 0;
           int sb = owner[((gz / c.nzb) * nby + gy / c.nyb) * nbx + gx / c.nxb];
+          if (sb < 0) continue;
           int si = gx % c.nxb + NGUARD, sj = c.k2 ? gy % c.nyb + NGUARD : 0, sk = c.k3 ? gz % c.nzb + NGUARD : 0;
           const double *src = &unk[sb * bsz + cidx(&c, si, sj, sk) * NUNK];
           double *dst = &unk[b * bsz + cidx(&c, i, j, k) * NUNK];
