@@ -43,6 +43,12 @@ sys.path.insert(0, ROOT)
 METRIC = "zone-updates/s on 1 B200: batched mixed+learned vs plain FP64, rel L1<=1e-6"
 UNIT = "zone-updates/s"
 BYTES_PER_ZONE = 80.0          # read + write of 5 FP64 state variables
+# DRAM bytes per zone-update of one step (k_sig + the three direction
+# kernels) from ncu captures of the 160^3 KH step (dram__bytes_read.sum +
+# dram__bytes_write.sum), scaled to the workload by its zone count
+# (traffic grows in proportion): HLLC 3,442 MB, exact solver 3,466 MB for
+# 4.096e6 zones
+TRAFFIC_PER_ZONE = {"mixed": 840.0, "mixed_exact": 846.0, "mixed_learned": 846.0}
 
 
 def measured_peaks():
@@ -607,7 +613,9 @@ def main():
             "paths": {n: {"value": total / (ms[n] * 1e-3), "ms_per_step": ms[n], "note": notes[n],
                           **({f"rel_l1_vs_{spec[n][3]}": errs[n]} if n in errs else {})} for n in ms},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None, "peak_kind": peak_kind,
+                         "traffic": TRAFFIC_PER_ZONE[head] * zones if head in TRAFFIC_PER_ZONE else None,
+                         "traffic_note": "DRAM bytes per step (per GPU), ncu at 160^3 scaled by zones",
+                         "peak_kind": peak_kind,
                          "kernel": "one hydro step (k_sig + k_dir x,y,z), 80 B/zone algorithmic"},
             "clocks": clocks,
             "gpu_launches": launches[head] * args.steps,
