@@ -125,6 +125,10 @@ def _set_sigs(lib):
         "flash_hy_set_exchange": (C.c_int, [vp, C.c_int, ip, C.c_int, ip]),
         "flash_hy_pack": (C.c_int, [vp, vp]),
         "flash_hy_unpack": (C.c_int, [vp, vp]),
+        "flash_hy_compute_fluxes": (C.c_int, [vp, C.c_int, ip, C.c_double, C.c_int]),
+        "flash_hy_get_fluxes": (C.c_int, [vp, C.c_int, C.c_int, dp]),
+        "flash_hy_put_fluxes": (C.c_int, [vp, C.c_int, C.c_int, dp]),
+        "flash_hy_update_solution": (C.c_int, [vp, C.c_int, ip, C.c_double]),
     }
     for name, (res, args) in sigs.items():
         f = getattr(lib, name)

@@ -69,6 +69,7 @@ struct flash_hy_ctx {
   int *d_owned, n_owned;       // blocks the step advances
   int *d_owned_mask;           // 1 for owned blocks (dt reduction)
   int *d_send, n_send, *d_recv, n_recv;  // blocks packed for / unpacked from other ranks
+  double *d_fstore;            // stored fluxes of the split step
   char err[512];
 };
 
@@ -391,6 +392,7 @@ extern "C" int flash_hy_destroy(flash_hy_ctx *c) {
   cudaFree(c->d_leaves); cudaFree(c->d_lh); cudaFree(c->d_gp); cudaFree(c->d_pe); cudaFree(c->d_freg);
   for (int l = 0; l < 17; ++l) { cudaFree(c->d_lev_leaves[l]); cudaFree(c->d_lev_parents[l]); }
   cudaFree(c->d_owned); cudaFree(c->d_owned_mask); cudaFree(c->d_send); cudaFree(c->d_recv);
+  cudaFree(c->d_fstore);
   free(c->h_blk_at);
   if (c->h_dt) cudaFreeHost(c->h_dt);
   if (c->h_status) cudaFreeHost(c->h_status);
@@ -572,11 +574,14 @@ static int amr_restrict_all(flash_hy_ctx *c) {
 }
 
 static int enqueue_step(flash_hy_ctx *c, double dt, const int *d_list, int nlaunch, const double *dt_dev = nullptr,
-                        bool set_attr = true) {
+                        bool set_attr = true, int fmode = 0) {
   StepArgs a;
   fill_devparams(c, a.P);
   a.P.dt = dt;
   a.P.dt_dev = dt_dev;
+  a.P.fmode = fmode;
+  a.P.fstore = c->d_fstore;
+  a.no_sig = fmode == 3;
   a.set_attr = set_attr;
   a.P.blk_list = d_list;
   a.sig = c->sig;
@@ -657,34 +662,133 @@ extern "C" int flash_hy_step(flash_hy_ctx *c, double simTime, double dt, double 
   return 0;
 }
 
+// device copy of a caller's block list (kept in the context)
+static int upload_list(flash_hy_ctx *c, int n, const int *list) {
+  for (int q = 0; q < n; ++q)
+    if (list[q] < 0 || list[q] >= c->nblocks) return fail(c, FLASH_HY_ERR_BAD_ARG, "block id out of range%s", "");
+  if (n > c->list_cap) {
+    cudaStreamSynchronize(c->stream);
+    cudaFree(c->d_list);
+    c->d_list = nullptr;
+    CUDA_OK(c, cudaMalloc((void **)&c->d_list, n * sizeof(int)));
+    c->list_cap = n;
+  }
+  if (n > 0) {
+    CUDA_OK(c, cudaMemcpyAsync(c->d_list, list, n * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CUDA_OK(c, cudaStreamSynchronize(c->stream));   // the list is caller memory
+  }
+  return 0;
+}
+
+// blocks outside a list keep their state in the buffer the step writes
+static int carry_state(flash_hy_ctx *c) {
+  for (int v = 0; v < 5; ++v)
+    CUDA_OK(c, cudaMemcpyAsync(c->state[1 - c->cur][v], c->state[c->cur][v], c->ncells * sizeof(double),
+                               cudaMemcpyDeviceToDevice, c->stream));
+  return 0;
+}
+
 extern "C" int flash_hy_step_blocks(flash_hy_ctx *c, int blockCount, const int *blockList, double timeEndAdv,
                                     double dt, double dtOld, int sweepOrder) {
   (void)timeEndAdv; (void)dtOld; (void)sweepOrder;
   if (!c || blockCount < 0 || (blockCount > 0 && !blockList)) return FLASH_HY_ERR_BAD_ARG;
   if (c->amr) return fail(c, FLASH_HY_ERR_UNSUPPORTED, "block lists on an AMR hierarchy%s", "");
   if (!(dt > 0.0)) return fail(c, FLASH_HY_ERR_NONPOS_DT, "dt must be positive%s", "");
-  for (int q = 0; q < blockCount; ++q)
-    if (blockList[q] < 0 || blockList[q] >= c->nblocks) return fail(c, FLASH_HY_ERR_BAD_ARG, "block id out of range%s", "");
   CUDA_OK(c, cudaSetDevice(c->device));
-  if (blockCount > c->list_cap) {
-    cudaStreamSynchronize(c->stream);
-    cudaFree(c->d_list);
-    c->d_list = nullptr;
-    CUDA_OK(c, cudaMalloc((void **)&c->d_list, blockCount * sizeof(int)));
-    c->list_cap = blockCount;
-  }
-  // blocks outside the list keep their state
-  for (int v = 0; v < 5; ++v)
-    CUDA_OK(c, cudaMemcpyAsync(c->state[1 - c->cur][v], c->state[c->cur][v], c->ncells * sizeof(double),
-                               cudaMemcpyDeviceToDevice, c->stream));
+  int rc = upload_list(c, blockCount, blockList);
+  if (rc) return rc;
+  if ((rc = carry_state(c))) return rc;
   if (blockCount > 0) {
-    CUDA_OK(c, cudaMemcpyAsync(c->d_list, blockList, blockCount * sizeof(int), cudaMemcpyHostToDevice, c->stream));
-    CUDA_OK(c, cudaStreamSynchronize(c->stream));   // blockList is caller memory
-    int rc = enqueue_step(c, dt, c->d_list, blockCount);
+    rc = enqueue_step(c, dt, c->d_list, blockCount);
     if (rc) return rc;
   }
   c->cur = 1 - c->cur;
   c->dt_valid = 0;
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// split step: fluxes, then the update (hy_computeFluxes / hy_updateSolution)
+// ---------------------------------------------------------------------------
+static int ensure_fstore(flash_hy_ctx *c) {
+  if (c->d_fstore) return 0;
+  const size_t nf = (size_t)(c->nx + 1) * c->ny * c->nz;
+  const size_t per = (size_t)NFLX * nf + c->ncb;
+  CUDA_OK(c, cudaMalloc((void **)&c->d_fstore, (size_t)c->nblocks * c->ndim * per * sizeof(double)));
+  return 0;
+}
+
+extern "C" int flash_hy_compute_fluxes(flash_hy_ctx *c, int blockCount, const int *blockList, double dt, int flags) {
+  if (!c || blockCount < 0 || (blockCount > 0 && !blockList)) return FLASH_HY_ERR_BAD_ARG;
+  if (flags != FLASH_HY_UPDATE_NONE && flags != FLASH_HY_UPDATE_ALL) return fail(c, FLASH_HY_ERR_BAD_ARG, "flags%s", "");
+  if (c->amr) return fail(c, FLASH_HY_ERR_UNSUPPORTED, "split step on an AMR hierarchy%s", "");
+  if (!(dt > 0.0)) return fail(c, FLASH_HY_ERR_NONPOS_DT, "dt must be positive%s", "");
+  CUDA_OK(c, cudaSetDevice(c->device));
+  int rc = ensure_fstore(c);
+  if (rc) return rc;
+  if ((rc = upload_list(c, blockCount, blockList))) return rc;
+  if (flags == FLASH_HY_UPDATE_ALL && (rc = carry_state(c))) return rc;
+  if (blockCount > 0) {
+    rc = enqueue_step(c, dt, c->d_list, blockCount, nullptr, true, flags == FLASH_HY_UPDATE_ALL ? 1 : 2);
+    if (rc) return rc;
+  }
+  if (flags == FLASH_HY_UPDATE_ALL) {
+    c->cur = 1 - c->cur;
+    c->dt_valid = 0;
+  }
+  return 0;
+}
+
+extern "C" int flash_hy_update_solution(flash_hy_ctx *c, int blockCount, const int *blockList, double dt) {
+  if (!c || blockCount < 0 || (blockCount > 0 && !blockList)) return FLASH_HY_ERR_BAD_ARG;
+  if (c->amr) return fail(c, FLASH_HY_ERR_UNSUPPORTED, "split step on an AMR hierarchy%s", "");
+  if (!c->d_fstore) return fail(c, FLASH_HY_ERR_BAD_ARG, "no stored fluxes (flash_hy_compute_fluxes first)%s", "");
+  if (!(dt > 0.0)) return fail(c, FLASH_HY_ERR_NONPOS_DT, "dt must be positive%s", "");
+  CUDA_OK(c, cudaSetDevice(c->device));
+  int rc = upload_list(c, blockCount, blockList);
+  if (rc) return rc;
+  if ((rc = carry_state(c))) return rc;
+  if (blockCount > 0) {
+    rc = enqueue_step(c, dt, c->d_list, blockCount, nullptr, true, 3);
+    if (rc) return rc;
+  }
+  c->cur = 1 - c->cur;
+  c->dt_valid = 0;
+  return 0;
+}
+
+static int flux_span(flash_hy_ctx *c, int blk, int dir, size_t &off, size_t &nf) {
+  if (blk < 0 || blk >= c->nblocks || dir < 1 || dir > c->ndim) return FLASH_HY_ERR_BAD_ARG;
+  if (!c->d_fstore) return FLASH_HY_ERR_BAD_ARG;
+  nf = (size_t)(c->nx + 1) * c->ny * c->nz;
+  const size_t per = (size_t)NFLX * nf + c->ncb;
+  off = ((size_t)blk * c->ndim + (dir - 1)) * per;
+  return 0;
+}
+
+extern "C" int flash_hy_get_fluxes(flash_hy_ctx *c, int blk, int dir, double *flx) {
+  if (!c || !flx) return FLASH_HY_ERR_BAD_ARG;
+  size_t off, nf;
+  if (flux_span(c, blk, dir, off, nf)) return fail(c, FLASH_HY_ERR_BAD_ARG, "get_fluxes: %s", "bad block/direction");
+  CUDA_OK(c, cudaSetDevice(c->device));
+  std::vector<double> h(NFLX * nf);
+  CUDA_OK(c, cudaMemcpyAsync(h.data(), c->d_fstore + off, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_OK(c, cudaStreamSynchronize(c->stream));
+  for (size_t f = 0; f < nf; ++f)
+    for (int v = 0; v < NFLX; ++v) flx[f * NFLX + v] = h[v * nf + f];
+  return 0;
+}
+
+extern "C" int flash_hy_put_fluxes(flash_hy_ctx *c, int blk, int dir, const double *flx) {
+  if (!c || !flx) return FLASH_HY_ERR_BAD_ARG;
+  size_t off, nf;
+  if (flux_span(c, blk, dir, off, nf)) return fail(c, FLASH_HY_ERR_BAD_ARG, "put_fluxes: %s", "bad block/direction");
+  CUDA_OK(c, cudaSetDevice(c->device));
+  std::vector<double> h(NFLX * nf);
+  for (size_t f = 0; f < nf; ++f)
+    for (int v = 0; v < NFLX; ++v) h[v * nf + f] = flx[f * NFLX + v];
+  CUDA_OK(c, cudaMemcpyAsync(c->d_fstore + off, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CUDA_OK(c, cudaStreamSynchronize(c->stream));
   return 0;
 }
 

@@ -61,6 +61,11 @@ struct DevParams {
   double *gp;                 // parent guard-inclusive blocks: [slot][6][(N+8)^d] (rho, v, e, E)
   double *pe;                 // parents' restricted specific total energy [node * NCB + cell]
   double *freg;               // fine-face fluxes at fine/coarse faces: [leaf slot][2 ndim][faces][8]
+  // split step (hy_computeFluxes with Uout disassociated, hy_updateSolution):
+  // 0 = fused step, 1 = store the fluxes and update, 2 = store the fluxes
+  // only, 3 = update from the stored fluxes
+  int fmode;
+  double *fstore;             // [block][ndim][8 x faces (FLASH flx order) + n+1/2 pressure sum per cell]
 };
 
 // Cell sizes of block b: level-1 deltas scaled by 2^(1-level) (exact).

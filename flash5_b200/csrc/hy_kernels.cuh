@@ -328,6 +328,50 @@ __device__ void flux_register(const DevParams &P, int b, int3 bc, double *sF, in
 }
 
 // ---------------------------------------------------------------------------
+// Stored fluxes of the split step: per block and direction the 8 flux
+// components at the faces in FLASH's flx(var, i, j, k) face order (the
+// DIR index runs over N+1 faces), stored component-major, then the n+1/2
+// pressure sum (N05 + P05) of every interior cell.  fidx(along, t1, t2)
+// gives a face's (or, with along in [0, N), a cell's) position in the
+// kernel's shared arrays.
+// ---------------------------------------------------------------------------
+template <int NDIM, int NX, int NY, int NZ> struct FluxStore {
+  static constexpr int NCB = NX * NY * NZ;
+  static constexpr int NF = (NX + 1) * NY * NZ;            // square blocks: the same for every direction
+  static constexpr int per_dir = NFLX * NF + NCB;
+  __device__ static __forceinline__ double *base(const DevParams &P, int b, int dir) {
+    return P.fstore + ((size_t)b * NDIM + (dir - 1)) * per_dir;
+  }
+};
+
+template <int NDIM, int NX, int NY, int NZ, int DIR>
+__device__ __forceinline__ void face_coords(int f, int &along, int &t1, int &t2) {
+  constexpr int fx = NX + (DIR == 1), fy = NY + (DIR == 2);
+  const int i = f % fx, j = (f / fx) % fy, k = f / (fx * fy);
+  along = DIR == 1 ? i : (DIR == 2 ? j : k);
+  t1 = DIR == 1 ? j : i;
+  t2 = DIR == 3 ? j : k;
+}
+
+// store: sF faces and the cell pressure sums (sp(t) for a cell position t)
+template <int NDIM, int NX, int NY, int NZ, int DIR, class T, class FaceIdx, class CellSp>
+__device__ void flux_store(const DevParams &P, int b, const T *sF, int fstride, FaceIdx fidx, CellSp sp) {
+  using FS = FluxStore<NDIM, NX, NY, NZ>;
+  double *o = FS::base(P, b, DIR);
+  for (int q = threadIdx.x; q < NFLX * FS::NF; q += blockDim.x) {
+    const int v = q / FS::NF, f = q % FS::NF;
+    int a, t1, t2;
+    face_coords<NDIM, NX, NY, NZ, DIR>(f, a, t1, t2);
+    o[q] = double(sF[v * fstride + fidx(a, t1, t2)]);
+  }
+  for (int c = threadIdx.x; c < FS::NCB; c += blockDim.x) {
+    const int i = c % NX, j = (c / NX) % NY, k = c / (NX * NY);
+    const int a = DIR == 1 ? i : (DIR == 2 ? j : k), t1 = DIR == 1 ? j : i, t2 = DIR == 3 ? j : k;
+    o[NFLX * FS::NF + c] = sp(fidx(a, t1, t2));
+  }
+}
+
+// ---------------------------------------------------------------------------
 // k_dir: one direction of the unsplit update for one block per CTA.
 //   phase 1: face states W-/W+ of the line cells (c_DIR in [-1, N], other
 //            coordinates interior) -- PPM (hy_dataReconstOneStep.F90:485-
@@ -385,6 +429,12 @@ __global__ void __launch_bounds__(320) k_dir(const DevParams P, const R *__restr
   const R hdtx = R(0.5 * dt / del[0]), hdty = R(0.5 * dt / del[1]), hdtz = R(0.5 * dt / del[2]);
   const R *sigb = SIG + (size_t)(P.slot ? P.slot[b] : (int)blockIdx.x) * NDIM * 6 * B::n;
 
+  auto fidx = [](int along, int t1, int t2) {
+    const int i = DIR == 1 ? along : t1, j = DIR == 1 ? t1 : (DIR == 2 ? along : t2),
+              k = DIR == 3 ? along : (NDIM > 2 ? t2 : 0);
+    return ((k + (DIR == 3)) * G::ry + (j + (DIR == 2))) * G::rx + (i + (DIR == 1));
+  };
+  if (P.fmode != 3) {
   // ---------------- phase 1: face states of the line cells ----------------
   for (int t = threadIdx.x; t < G::n; t += blockDim.x) {
     int i, j, k;
@@ -519,6 +569,35 @@ __global__ void __launch_bounds__(320) k_dir(const DevParams P, const R *__restr
         return ((k + (DIR == 3)) * G::ry + (j + (DIR == 2))) * G::rx + (i + (DIR == 1));
       });
       __syncthreads();
+    }
+  }
+
+  } else {
+    // replay: the stored fluxes, and the stored pressure sums in place of
+    // the face-state sum N05 + P05 of phase 3
+    using FS = FluxStore<NDIM, NX, NY, NZ>;
+    const double *src = FS::base(P, b, DIR);
+    for (int q = threadIdx.x; q < NFLX * FS::NF; q += blockDim.x) {
+      const int v = q / FS::NF, f = q % FS::NF;
+      int a, t1, t2;
+      face_coords<NDIM, NX, NY, NZ, DIR>(f, a, t1, t2);
+      sF[v * G::n + fidx(a, t1, t2)] = R(src[q]);
+    }
+    for (int c = threadIdx.x; c < FS::NCB; c += blockDim.x) {
+      const int i = c % NX, j = (c / NX) % NY, k = c / (NX * NY);
+      const int t = fidx(DIR == 1 ? i : (DIR == 2 ? j : k), DIR == 1 ? j : i, DIR == 3 ? j : k);
+      sWm[4 * G::n + t] = R(src[NFLX * FS::NF + c]);
+      sWp[4 * G::n + t] = R(0);
+    }
+    __syncthreads();
+  }
+  if (P.fmode == 1 || P.fmode == 2) {
+    flux_store<NDIM, NX, NY, NZ, DIR>(P, b, sF, G::n, fidx, [&](int t) {
+      return double(sWm[4 * G::n + t]) + double(sWp[4 * G::n + t]);
+    });
+    if (P.fmode == 2) {
+      if (st) atomicOr(P.status, st);
+      return;
     }
   }
 

@@ -18,6 +18,7 @@ struct StepArgs {
   bool set_attr;      // raise the kernels' dynamic shared-memory limit (not while capturing a graph)
   // AMR (nlev > 0): k_sig over all leaves, then per direction one launch per
   // level, finest first (the flux register needs the fine fluxes first)
+  bool no_sig;        // update from stored fluxes: the transverse-flux pass is not needed
   int nlev;
   const int *leaves;  // all leaves (device)
   int nleaves;

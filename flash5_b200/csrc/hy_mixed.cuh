@@ -141,6 +141,8 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
   const float hdtx = float(0.5 * dt / del[0]), hdty = float(0.5 * dt / del[1]), hdtz = float(0.5 * dt / del[2]);
   const float *sigb = SIG + (size_t)(P.slot ? P.slot[b] : (int)blockIdx.x) * NDIM * 6 * B::n;
 
+  auto fidx = [](int along, int t1, int t2) { return G::at(along, t1 + (DIR == 1 ? NY : NX) * t2, G::LC, 1); };
+  if (P.fmode != 3) {
   // ---- A: stage the primitive stencil of every line (guard cells get the EOS)
   for (int s = threadIdx.x; s < G::SA; s += NT) {
     int x, l, i, j, k;
@@ -529,6 +531,31 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
       return G::at(along, t1 + (DIR == 1 ? NY : NX) * t2, G::LC, 1);
     });
     __syncthreads();
+  }
+
+  } else {
+    // replay: the stored fluxes and pressure sums
+    using FS = FluxStore<NDIM, NX, NY, NZ>;
+    const double *src = FS::base(P, b, DIR);
+    for (int q = threadIdx.x; q < NFLX * FS::NF; q += NT) {
+      const int v = q / FS::NF, f = q % FS::NF;
+      int a, t1, t2;
+      face_coords<NDIM, NX, NY, NZ, DIR>(f, a, t1, t2);
+      sF[v * G::SC + fidx(a, t1, t2)] = src[q];
+    }
+    for (int c = threadIdx.x; c < FS::NCB; c += NT) {
+      const int i = c % NX, j = (c / NX) % NY, k = c / (NX * NY);
+      sF[8 * G::SC + fidx(DIR == 1 ? i : (DIR == 2 ? j : k), DIR == 1 ? j : i, DIR == 3 ? j : k)] =
+          src[NFLX * FS::NF + c];
+    }
+    __syncthreads();
+  }
+  if (P.fmode == 1 || P.fmode == 2) {
+    flux_store<NDIM, NX, NY, NZ, DIR>(P, b, sF, G::SC, fidx, [&](int t) { return sF[8 * G::SC + t]; });
+    if (P.fmode == 2) {
+      if (st) atomicOr(P.status, st);
+      return;
+    }
   }
 
   // ---- E: conservative update

@@ -59,7 +59,8 @@ static bool launch_dir(const StepArgs &a) {
 // RS: 0 = HLLC, 1 = exact Riemann solver
 template <int NDIM, int NX, int NY, int NZ, int RS>
 static int run_rs(const StepArgs &a) {
-  if (a.nlev == 0) {
+  if (a.no_sig) {
+  } else if (a.nlev == 0) {
     k_sig<NDIM, NX, NY, NZ, Real, FHY_VARIANT><<<a.nlaunch, a.threads, 0, a.stream>>>(a.P, (Real *)a.sig);
   } else {
     DevParams P = a.P;
@@ -68,6 +69,7 @@ static int run_rs(const StepArgs &a) {
   }
   if (cudaGetLastError() != cudaSuccess) return -2;
   int nl = 1;
+  const int nsig = a.no_sig ? 0 : 1;
   if (a.nlev > 0) {
     nl = 0;
     for (int l = 1; l <= a.nlev; ++l) nl += a.lev_count[l] > 0;
@@ -75,12 +77,12 @@ static int run_rs(const StepArgs &a) {
   if constexpr (NDIM == 2) {
     const bool ok =
         launch_dir<NDIM, NX, NY, NZ, 1, true, false, RS>(a) && launch_dir<NDIM, NX, NY, NZ, 2, false, true, RS>(a);
-    return ok ? 1 + 2 * nl : -2;
+    return ok ? nsig + 2 * nl : -2;
   } else {
     const bool ok = launch_dir<NDIM, NX, NY, NZ, 1, true, false, RS>(a) &&
                     launch_dir<NDIM, NX, NY, NZ, 2, false, false, RS>(a) &&
                     launch_dir<NDIM, NX, NY, NZ, 3, false, true, RS>(a);
-    return ok ? 1 + 3 * nl : -2;
+    return ok ? nsig + 3 * nl : -2;
   }
 }
 

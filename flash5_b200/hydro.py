@@ -85,6 +85,28 @@ class Hydro:
         self._check(self.lib.flash_hy_step_blocks(self.ctx, len(bl), bl.ctypes.data_as(C.POINTER(C.c_int)),
                                                   timeEndAdv, dt, dtOld, sweepOrder))
 
+    # -- split step: hy_computeFluxes / hy_updateSolution ------------------
+    def compute_fluxes(self, blockList, dt, flags=abi.UPDATE_NONE):
+        bl = np.ascontiguousarray(blockList, dtype=np.int32)
+        self._check(self.lib.flash_hy_compute_fluxes(self.ctx, len(bl), bl.ctypes.data_as(C.POINTER(C.c_int)), dt,
+                                                     flags))
+
+    def get_fluxes(self, block, dir):
+        """Fluxes of one block in direction dir (1..ndim): [faces, 8] in
+        FLASH's flx(NFLUXES, i, j, k) order."""
+        nb = self.grid.nb
+        out = np.zeros(((nb[0] + 1) * nb[1] * nb[2], 8))
+        self._check(self.lib.flash_hy_get_fluxes(self.ctx, block, dir, out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
+    def put_fluxes(self, block, dir, flx):
+        flx = np.ascontiguousarray(flx, dtype=np.float64)
+        self._check(self.lib.flash_hy_put_fluxes(self.ctx, block, dir, flx.ctypes.data_as(C.POINTER(C.c_double))))
+
+    def update_solution(self, blockList, dt):
+        bl = np.ascontiguousarray(blockList, dtype=np.int32)
+        self._check(self.lib.flash_hy_update_solution(self.ctx, len(bl), bl.ctypes.data_as(C.POINTER(C.c_int)), dt))
+
     def compute_dt(self):
         """Hydro_computeDt + the MINLOC reduction: (dt, (i, j, k, level, block))."""
         dt = C.c_double()

@@ -146,6 +146,22 @@ int flash_hy_step(flash_hy_ctx *ctx, double simTime, double dt, double dtOld,
  * indices into the descriptor's block order).                           */
 int flash_hy_step_blocks(flash_hy_ctx *ctx, int blockCount, const int *blockList,
                          double timeEndAdv, double dt, double dtOld, int sweepOrder);
+/* The step split in two, as hy_computeFluxes / hy_updateSolution
+ * (localAPI/hy_interface.F90:969,982) and unsplit/Hydro.F90:186-230 use it
+ * around a caller's own flux correction (Grid_putFluxData,
+ * Grid_conserveFluxes): compute_fluxes computes and keeps the face fluxes
+ * of the listed blocks (flags = FLASH_HY_UPDATE_NONE: Uout disassociated,
+ * the state is unchanged; FLASH_HY_UPDATE_ALL: also updates, as
+ * flash_hy_step_blocks); get/put_fluxes read or replace one block's fluxes
+ * in one direction (1..ndim) in FLASH's flux-array layout flx(NFLUXES = 8,
+ * i, j, k) over the faces (the dir index runs over nb+1 faces; host memory);
+ * update_solution applies the kept (possibly replaced) fluxes to the listed
+ * blocks.  Uniform grids only.                                           */
+int flash_hy_compute_fluxes(flash_hy_ctx *ctx, int blockCount, const int *blockList, double dt, int flags);
+int flash_hy_get_fluxes(flash_hy_ctx *ctx, int block, int dir, double *flx);
+int flash_hy_put_fluxes(flash_hy_ctx *ctx, int block, int dir, const double *flx);
+int flash_hy_update_solution(flash_hy_ctx *ctx, int blockCount, const int *blockList, double dt);
+
 /* Hydro_computeDt + the MPI_MINLOC reduction of Driver_computeDt.F90:376-377:
  * dt_out = cfl / max_cells max_d (|u_d| + c_s)/dx_d; minloc_out = (i, j, k,
  * level, block) with FLASH's 1-based guard-inclusive cell indices.      */

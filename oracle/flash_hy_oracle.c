@@ -1395,3 +1395,37 @@ int orc_amr_restrict(const flash_hy_params *p, const flash_hy_grid_desc *g, doub
   amr_free(&a);
   return 0;
 }
+
+/* Face fluxes of one block as hy_computeFluxes leaves them in the Grid's
+ * flux arrays (Uout disassociated, hy_computeFluxes.F90:156-160): for each
+ * direction d the fluxes flx(NFLUXES, i, j, k) over the faces of the block
+ * (the d index runs over nb+1 faces), written to out + d * 8 * nfaces.
+ * The guard cells of every block are filled first. */
+int orc_block_fluxes(const flash_hy_params *p, const flash_hy_grid_desc *g, double *unk, int blk, double dt,
+                     double *out) {
+  int st = orc_fill_guardcells(p, g, unk);
+  if (st) return st;
+  ctx_t c; ctx_init(&c, p, g);
+  size_t bsz = (size_t)c.nxt * c.nyt * c.nzt * NUNK;
+  double del[3];
+  block_deltas(g, del);
+  work_t w;
+  work_alloc(&c, &w);
+  get_riemann_state(&c, &unk[blk * bsz], &w, dt, del);
+  get_face_flux(&c, &w);
+  int nb[3] = {c.nxb, c.nyb, c.nzb};
+  size_t nfaces = (size_t)(c.nxb + 1) * c.nyb * c.nzb;
+  for (int d = 0; d < c.ndim; ++d) {
+    int fx = nb[0] + (d == 0), fy = nb[1] + (d == 1), fz = nb[2] + (d == 2);
+    double *o = out + (size_t)d * NFLX * nfaces;
+    for (int k = 0; k < fz; ++k)
+      for (int j = 0; j < fy; ++j)
+        for (int i = 0; i < fx; ++i) {
+          const double *F = &w.flux[d][cidx(&c, i + NGUARD, j + (c.k2 ? NGUARD : 0), k + (c.k3 ? NGUARD : 0)) * NFLX];
+          size_t f = ((size_t)k * fy + j) * fx + i;
+          for (int v = 0; v < NFLX; ++v) o[f * NFLX + v] = F[v];
+        }
+  }
+  work_free(&w);
+  return c.status;
+}

@@ -43,6 +43,7 @@ def lib():
         L.orc_amr_hydro.argtypes = [P, G, dp, C.c_double, C.c_double, C.c_double]
         L.orc_amr_compute_dt.argtypes = [P, G, dp, dp, ip]
         L.orc_amr_restrict.argtypes = [P, G, dp]
+        L.orc_block_fluxes.argtypes = [P, G, dp, C.c_int, C.c_double, dp]
         _lib = L
     return _lib
 
@@ -88,6 +89,14 @@ class Oracle:
     def amr_hydro(self, unk, sim_time, dt, dt_old):
         """The AMR step on any grid (max_level 1 included)."""
         return lib().orc_amr_hydro(C.byref(self.p), C.byref(self.g), _dp(unk), sim_time, dt, dt_old)
+
+    def block_fluxes(self, unk, blk, dt):
+        """Face fluxes of block blk, [ndim][faces][8] in FLASH's flux layout."""
+        nb = self.grid.nb
+        nf = (nb[0] + 1) * nb[1] * nb[2]
+        out = np.zeros((self.grid.ndim, nf, 8))
+        st = lib().orc_block_fluxes(C.byref(self.p), C.byref(self.g), _dp(unk), blk, dt, _dp(out))
+        return st, out
 
     def compute_dt(self, unk):
         dt = C.c_double()
