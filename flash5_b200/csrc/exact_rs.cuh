@@ -45,27 +45,59 @@ static_assert(sizeof(MlpPacked) % 16 == 0, "MlpPacked must be a multiple of 16 b
 // ---------------------------------------------------------------------------
 struct Side { double d, u, p, c; };
 
-__device__ __forceinline__ void pres_fn(double p, const Side &s, double g, double &f, double &fd) {
+// x^y for x > 0 as exp2(y log2 x): the relative error is a few ulp times
+// |y log2 x|, far below the solver's tolerance, at a fraction of the cost
+// of the correctly rounded FP64 pow
+__device__ __forceinline__ double powp(double x, double y) { return exp2(y * log2(x)); }
+
+// x^k by multiplications when k is an integer in [1, 16] (g = 5/3: the
+// fan exponents 2/(g-1) = 3, 2g/(g-1) = 5 and the guess exponent
+// 2g/(g-1) = 5), else powp
+__device__ __forceinline__ double pow_k(double x, double k) {
+  const double kn = rint(k);
+  if (fabs(k - kn) < 1e-9 && kn >= 1.0 && kn <= 16.0) {
+    double r = x;
+    for (int n = 1; n < (int)kn; ++n) r *= x;
+    return r;
+  }
+  return powp(x, k);
+}
+
+// qr = (p/pK)^((g-1)/2g) on the rarefaction branch, -1 on the shock branch
+__device__ __forceinline__ void pres_fn(double p, const Side &s, double g, double &f, double &fd, double &qr) {
   if (p <= s.p) {                                   // rarefaction, Toro eq. 4.7
     double prat = p / s.p;
     double ex = (g - 1.0) / (2.0 * g);
-    double q = pow(prat, ex);
+    double q = powp(prat, ex);
     f = 2.0 * s.c / (g - 1.0) * (q - 1.0);
     fd = q / (prat * s.d * s.c);                    // (p/pK)^(-(g+1)/2g) / (dK cK)
+    qr = q;
   } else {                                          // shock, Toro eq. 4.6
     double A = 2.0 / ((g + 1.0) * s.d);
     double B = (g - 1.0) / (g + 1.0) * s.p;
     double q = sqrt(A / (B + p));
     f = (p - s.p) * q;
     fd = (1.0 - 0.5 * (p - s.p) / (B + p)) * q;
+    qr = -1.0;
   }
 }
+__device__ __forceinline__ void pres_fn(double p, const Side &s, double g, double &f, double &fd) {
+  double qr;
+  pres_fn(p, s, g, f, fd, qr);
+}
+
+// The last pressure-function evaluation of a Newton solve: its pressure and
+// (pe/pK)^((g-1)/2g) of each side that took the rarefaction branch there
+// (-1 otherwise).  The sampling reuses these powers, carried to p* to first
+// order (p* - pe is the last Newton step, so the error is of the order of
+// its square).
+struct LastEval { double pe, qL, qR; };
 
 __device__ __forceinline__ double tr_guess(const Side &L, const Side &R, double g) {
   double z = (g - 1.0) / (2.0 * g);
   double num = L.c + R.c - 0.5 * (g - 1.0) * (R.u - L.u);
   if (num <= 0.0) return 0.0;
-  return pow(num / (L.c / pow(L.p, z) + R.c / pow(R.p, z)), 1.0 / z);
+  return pow_k(num / (L.c / powp(L.p, z) + R.c / powp(R.p, z)), 1.0 / z);
 }
 
 // vacuum generation test, Toro eq. 4.40
@@ -89,6 +121,14 @@ __device__ __forceinline__ bool strong_waves(const Side &L, const Side &R) {
   return ppv > pmin && fmax(pmax, ppv) >= 2.0 * pmin;
 }
 
+// Start of a hydro face solve: the two-rarefaction guess (the root where
+// both waves are rarefactions, within a few per cent for weak waves), with
+// the bracket probe for strong waves.
+__device__ __forceinline__ double face_start(const Side &L, const Side &R, double g, bool &probe) {
+  probe = strong_waves(L, R);
+  return tr_guess(L, R, g);
+}
+
 // Newton from p0 > 0.  With `probe`, the bracket is first located as
 // [pa, pb] = [p/4, p] with f(pb) > 0, starting from p = max(p_L, p_R) and
 // growing by 4, and a start outside it is replaced by sqrt(pa * pb) (for
@@ -104,12 +144,13 @@ __device__ __forceinline__ bool strong_waves(const Side &L, const Side &R) {
 // pressure-function evaluations (probes included), or -max_iter when not
 // converged.
 __device__ __forceinline__ int newton(const Side &L, const Side &R, double g, double p0, double tol, int max_iter,
-                                      double &pout, double &uout, bool probe = false) {
+                                      double &pout, double &uout, bool probe = false, LastEval *le = nullptr) {
   const double du = R.u - L.u;
   double pa = 0.0, pb = DBL_MAX;
   double p = p0, prev = -1.0;
-  double fl = 0., fdl = 0., fr = 0., fdr = 0., pe = p0;
+  double fl = 0., fdl = 0., fr = 0., fdr = 0., pe = p0, qL = -1.0, qR = -1.0;
   int evals = 0;
+  if (le) { le->pe = p0; le->qL = -1.0; le->qR = -1.0; }
   if (probe) {
     double q = fmax(L.p, R.p);
     for (int k = 0; k < 64 && evals < max_iter; ++k) {
@@ -122,9 +163,10 @@ __device__ __forceinline__ int newton(const Side &L, const Side &R, double g, do
     if (!(p > pa && p < pb)) p = (pa > 0.0 && pb < DBL_MAX) ? sqrt(pa * pb) : (pb < DBL_MAX ? 0.5 * pb : 4.0 * pa);
   }
   for (; evals < max_iter;) {
-    pres_fn(p, L, g, fl, fdl); pres_fn(p, R, g, fr, fdr);
+    pres_fn(p, L, g, fl, fdl, qL); pres_fn(p, R, g, fr, fdr, qR);
     ++evals;
     pe = p;
+    if (le) { le->pe = pe; le->qL = qL; le->qR = qR; }
     const double f = fl + fr + du;
     if (f == 0.0) {
       pout = p;
@@ -163,20 +205,34 @@ __device__ __forceinline__ void fan_left(const Side &L, double g, double &d, dou
   const double c = 2.0 / (g + 1.0) * (L.c + 0.5 * (g - 1.0) * L.u);
   u = c;
   const double r = c / L.c;
-  d = L.d * pow(r, 2.0 / (g - 1.0));
-  p = L.p * pow(r, 2.0 * g / (g - 1.0));
+  d = L.d * pow_k(r, 2.0 / (g - 1.0));
+  p = L.p * pow_k(r, 2.0 * g / (g - 1.0));
 }
 __device__ __forceinline__ void fan_right(const Side &R, double g, double &d, double &u, double &p) {
   const double c = 2.0 / (g + 1.0) * (R.c - 0.5 * (g - 1.0) * R.u);
   u = -c;
   const double r = c / R.c;
-  d = R.d * pow(r, 2.0 / (g - 1.0));
-  p = R.p * pow(r, 2.0 * g / (g - 1.0));
+  d = R.d * pow_k(r, 2.0 / (g - 1.0));
+  p = R.p * pow_k(r, 2.0 * g / (g - 1.0));
+}
+
+// (pr)^(1/g) from q = pr^((g-1)/2g): q^(2/(g-1)), by multiplications when
+// 2/(g-1) is an integer (g = 5/3: 3, g = 7/5: 5)
+__device__ __forceinline__ double pow_inv_gamma(double q, double pr, double g) {
+  const double k = 2.0 / (g - 1.0);
+  return fabs(k - rint(k)) < 1e-9 && k >= 1.0 && k <= 16.0 ? pow_k(q, k) : powp(pr, 1.0 / g);
+}
+
+// pr^((g-1)/2g) at pr = ps/pK: from the last evaluation when that side took
+// the rarefaction branch there, else directly
+__device__ __forceinline__ double q_at(double ps, double pK, double g, double qe, double pe) {
+  const double ex = (g - 1.0) / (2.0 * g);
+  return qe >= 0.0 ? qe * (1.0 + ex * (ps - pe) / pe) : powp(ps / pK, ex);
 }
 
 // (d, u, p) at x/t = 0 and which side supplies the transverse velocities
 __device__ __forceinline__ void sample0(const Side &L, const Side &R, double g, double ps, double us, bool vac,
-                                        double &d, double &u, double &p, bool &right) {
+                                        double &d, double &u, double &p, bool &right, const LastEval *le = nullptr) {
   if (vac) {
     const double sl = L.u + 2.0 * L.c / (g - 1.0), sr = R.u - 2.0 * R.c / (g - 1.0);
     if (0.0 <= L.u - L.c) { right = false; d = L.d; u = L.u; p = L.p; }
@@ -198,8 +254,9 @@ __device__ __forceinline__ void sample0(const Side &L, const Side &R, double g, 
       if (0.0 <= L.u - L.c) { d = L.d; u = L.u; p = L.p; }
       else {
         const double pr = ps / L.p;
-        const double cml = L.c * pow(pr, g1);
-        if (0.0 > us - cml) { d = L.d * pow(pr, 1.0 / g); u = us; p = ps; }
+        const double q = le ? q_at(ps, L.p, g, le->qL, le->pe) : powp(pr, g1);
+        const double cml = L.c * q;
+        if (0.0 > us - cml) { d = L.d * (le ? pow_inv_gamma(q, pr, g) : powp(pr, 1.0 / g)); u = us; p = ps; }
         else fan_left(L, g, d, u, p);
       }
     }
@@ -214,8 +271,9 @@ __device__ __forceinline__ void sample0(const Side &L, const Side &R, double g, 
       if (0.0 >= R.u + R.c) { d = R.d; u = R.u; p = R.p; }
       else {
         const double pr = ps / R.p;
-        const double cmr = R.c * pow(pr, g1);
-        if (0.0 <= us + cmr) { d = R.d * pow(pr, 1.0 / g); u = us; p = ps; }
+        const double q = le ? q_at(ps, R.p, g, le->qR, le->pe) : powp(pr, g1);
+        const double cmr = R.c * q;
+        if (0.0 <= us + cmr) { d = R.d * (le ? pow_inv_gamma(q, pr, g) : powp(pr, 1.0 / g)); u = us; p = ps; }
         else fan_right(R, g, d, u, p);
       }
     }
@@ -228,10 +286,11 @@ __device__ __forceinline__ void sample0(const Side &L, const Side &R, double g, 
 // normal direction (1..3).
 template <int DIR>
 __device__ __forceinline__ void godunov_flux(const double *VL, const double *VR, const Side &L, const Side &R, double g,
-                                             double ps, double us, bool vac, double F[6]) {
+                                             double ps, double us, bool vac, double F[6],
+                                             const LastEval *le = nullptr) {
   double d, u, p;
   bool right;
-  sample0(L, R, g, ps, us, vac, d, u, p, right);
+  sample0(L, R, g, ps, us, vac, d, u, p, right, le);
   double v[3];
 #pragma unroll
   for (int m = 0; m < 3; ++m) v[m] = (m == DIR - 1) ? u : (right ? VR[1 + m] : VL[1 + m]);

@@ -259,7 +259,7 @@ __device__ __forceinline__ void harvest_face(const DevParams &P, const xrs::Side
   S[3 * c + k] = R.d; S[4 * c + k] = R.u; S[5 * c + k] = R.p; S[6 * c + k] = g;
 }
 
-// Godunov flux from the exact solution with the two-rarefaction guess
+// Godunov flux from the exact solution (start: xrs::face_start)
 template <int DIR>
 __device__ __forceinline__ void exact_face(const DevParams &P, const double *VL, const double *VR, double F[6],
                                            unsigned &st) {
@@ -267,9 +267,13 @@ __device__ __forceinline__ void exact_face(const DevParams &P, const double *VL,
   const xrs::Side L = side_of(VL, DIR, g, st), R = side_of(VR, DIR, g, st);
   const bool vac = xrs::vacuum(L, R, g);
   double ps = 0.0, us = 0.5 * (L.u + R.u);
-  if (!vac && xrs::newton(L, R, g, xrs::tr_guess(L, R, g), P.rs_tol, P.rs_max_iter, ps, us, xrs::strong_waves(L, R)) < 0)
-    st |= ST_NEWTON;
-  xrs::godunov_flux<DIR>(VL, VR, L, R, g, ps, us, vac, F);
+  xrs::LastEval le;
+  if (!vac) {
+    bool probe;
+    const double p0 = xrs::face_start(L, R, g, probe);
+    if (xrs::newton(L, R, g, p0, P.rs_tol, P.rs_max_iter, ps, us, probe, &le) < 0) st |= ST_NEWTON;
+  }
+  xrs::godunov_flux<DIR>(VL, VR, L, R, g, ps, us, vac, F, vac ? nullptr : &le);
 }
 
 // ---------------------------------------------------------------------------

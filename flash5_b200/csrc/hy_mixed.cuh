@@ -451,13 +451,15 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
       sides(s, t, L, R);
       const bool vac = xrs::vacuum(L, R, g);
       double ps = 0.0, us = 0.5 * (L.u + R.u);
+      xrs::LastEval le;
       if (!vac) {
         const double q = learned ? sP0[t] : 0.0;
-        const double p0 = q < 0.0 ? -q : xrs::tr_guess(L, R, g);
-        const bool strong = xrs::strong_waves(L, R);
-        int k = xrs::newton(L, R, g, p0, P.rs_tol, q < 0.0 ? 3 : P.rs_max_iter, ps, us, q >= 0.0 && strong);
+        bool strong;
+        const double p0 = q < 0.0 ? -q : xrs::face_start(L, R, g, strong);
+        if (q < 0.0) strong = xrs::strong_waves(L, R);
+        int k = xrs::newton(L, R, g, p0, P.rs_tol, q < 0.0 ? 3 : P.rs_max_iter, ps, us, q >= 0.0 && strong, &le);
         if (k < 0 && q < 0.0)
-          k = xrs::newton(L, R, g, xrs::tr_guess(L, R, g), P.rs_tol, P.rs_max_iter, ps, us, strong);
+          k = xrs::newton(L, R, g, xrs::tr_guess(L, R, g), P.rs_tol, P.rs_max_iter, ps, us, strong, &le);
         if (k < 0) st |= ST_NEWTON;
         if (P.harvest && (q < 0.0 || (strong && !xrs::tr_exact(L, R, p0))))
           harvest_face(P, L, R, g, (unsigned)(blockIdx.x * 4 + DIR) * 2048u + (unsigned)t);
@@ -470,7 +472,7 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
         VR[n] = face(qq, false, s, t);
       }
       double F[6];
-      xrs::godunov_flux<DIR>(VL, VR, L, R, g, ps, us, vac, F);
+      xrs::godunov_flux<DIR>(VL, VR, L, R, g, ps, us, vac, F, vac ? nullptr : &le);
 #pragma unroll
       for (int n = 0; n < 6; ++n) Fr[it][n] = F[n];
       double fv = 0., fe = 0.;

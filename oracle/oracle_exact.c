@@ -20,25 +20,38 @@
  */
 #include <float.h>
 #include <math.h>
+#include <stddef.h>
 
 typedef struct { double d, u, p, c; } side_t;
 
 /* Toro eq. 4.6-4.7 and their derivatives. */
-static void pres_fn(double p, const side_t *s, double g, double *f, double *fd) {
+/* qr = (p/pK)^((g-1)/2g) on the rarefaction branch, -1 on the shock branch */
+static void pres_fn_q(double p, const side_t *s, double g, double *f, double *fd, double *qr) {
   if (p <= s->p) {                                   /* rarefaction */
     double prat = p / s->p;
     double ex = (g - 1.0) / (2.0 * g);
     double q = pow(prat, ex);
     *f = 2.0 * s->c / (g - 1.0) * (q - 1.0);
     *fd = q / (prat * s->d * s->c);                  /* (p/pK)^(-(g+1)/2g) / (dK cK) */
+    *qr = q;
   } else {                                           /* shock */
     double A = 2.0 / ((g + 1.0) * s->d);
     double B = (g - 1.0) / (g + 1.0) * s->p;
     double q = sqrt(A / (B + p));
     *f = (p - s->p) * q;
     *fd = (1.0 - 0.5 * (p - s->p) / (B + p)) * q;
+    *qr = -1.0;
   }
 }
+static void pres_fn(double p, const side_t *s, double g, double *f, double *fd) {
+  double qr;
+  pres_fn_q(p, s, g, f, fd, &qr);
+}
+
+/* The last evaluation of a Newton solve: its pressure and the rarefaction
+ * branch powers (pe/pK)^((g-1)/2g) (-1 for a shock branch), which the
+ * sampling carries to p* to first order. */
+typedef struct { double pe, qL, qR; } last_eval_t;
 
 /* Two-rarefaction guess, Toro eq. 4.46. */
 double orc_two_rarefaction_guess(double dl, double ul, double pl, double dr, double ur, double pr, double g) {
@@ -74,24 +87,16 @@ int orc_strong_waves(double dl, double ul, double pl, double dr, double ur, doub
  * below tol * p or the predicted next step of the quadratic regime,
  * |step|^3/prev^2, is below tol * p / 100.  u* uses f_L, f_R linearised
  * from the last evaluation to the returned p*. */
-int orc_star_state(double dl, double ul, double pl, double dr, double ur, double pr, double g,
-                   double p0, double tol, int max_iter, double *pstar, double *ustar, int *iters) {
-  side_t L = {dl, ul, pl, sqrt(g * pl / dl)}, R = {dr, ur, pr, sqrt(g * pr / dr)};
-  double du = ur - ul;
-  *iters = 0;
-  /* vacuum generation test, Toro eq. 4.40 */
-  if (2.0 * (L.c + R.c) / (g - 1.0) <= du) {
-    *pstar = 0.0;
-    *ustar = 0.5 * (ul + ur);
-    return 2;
-  }
-  double fl = 0., fdl = 0., fr = 0., fdr = 0.;
-  double pa = 0.0, pb = DBL_MAX;
-  int probe = p0 <= 0.0 && orc_strong_waves(dl, ul, pl, dr, ur, pr, g);
-  double p = p0 > 0.0 ? p0 : orc_two_rarefaction_guess(dl, ul, pl, dr, ur, pr, g);
+static int star_solve(const side_t *Lp, const side_t *Rp, double g, double p, int probe, double tol, int max_iter,
+                      double *pstar, double *ustar, int *iters, last_eval_t *le) {
+  side_t L = *Lp, R = *Rp;
+  double du = R.u - L.u;
+  double fl = 0., fdl = 0., fr = 0., fdr = 0., qL = -1.0, qR = -1.0;
+  double pa = 0.0, pb = DBL_MAX, pe = p, prev = -1.0;
   int evals = 0;
+  le->pe = p; le->qL = -1.0; le->qR = -1.0;
   if (probe) {
-    double q = fmax(pl, pr);
+    double q = fmax(L.p, R.p);
     for (int k = 0; k < 64 && evals < max_iter; ++k) {
       pres_fn(q, &L, g, &fl, &fdl); pres_fn(q, &R, g, &fr, &fdr);
       ++evals;
@@ -101,16 +106,17 @@ int orc_star_state(double dl, double ul, double pl, double dr, double ur, double
     }
     if (!(p > pa && p < pb)) p = (pa > 0.0 && pb < DBL_MAX) ? sqrt(pa * pb) : (pb < DBL_MAX ? 0.5 * pb : 4.0 * pa);
   }
-  double pe = p, prev = -1.0;
+  *iters = evals;
   for (; evals < max_iter;) {
-    pres_fn(p, &L, g, &fl, &fdl); pres_fn(p, &R, g, &fr, &fdr);
+    pres_fn_q(p, &L, g, &fl, &fdl, &qL); pres_fn_q(p, &R, g, &fr, &fdr, &qR);
     ++evals;
     *iters = evals;
     pe = p;
+    le->pe = pe; le->qL = qL; le->qR = qR;
     double f = fl + fr + du;
     if (f == 0.0) {
       *pstar = p;
-      *ustar = 0.5 * (ul + ur) + 0.5 * (fr - fl);
+      *ustar = 0.5 * (L.u + R.u) + 0.5 * (fr - fl);
       return 0;
     }
     if (f < 0.0) pa = p; else pb = p;
@@ -121,18 +127,40 @@ int orc_star_state(double dl, double ul, double pl, double dr, double ur, double
     if (as <= tol * p || (inside && prev > 0.0 && as < prev && as * (as / prev) * (as / prev) <= 0.01 * tol * p)) {
       *pstar = pn > 0.0 ? pn : p;
       double dp = *pstar - pe;
-      *ustar = 0.5 * (ul + ur) + 0.5 * ((fr + fdr * dp) - (fl + fdl * dp));
+      *ustar = 0.5 * (L.u + R.u) + 0.5 * ((fr + fdr * dp) - (fl + fdl * dp));
       return 0;
     }
     if (!inside) { pn = pb == DBL_MAX ? 4.0 * p : (pa > 0.0 ? sqrt(pa * pb) : 0.01 * pb); prev = -1.0; }
     else prev = as;
     p = pn;
   }
-  *iters = evals;
   *pstar = p;
   double dp = p - pe;
-  *ustar = 0.5 * (ul + ur) + 0.5 * ((fr + fdr * dp) - (fl + fdl * dp));
+  *ustar = 0.5 * (L.u + R.u) + 0.5 * ((fr + fdr * dp) - (fl + fdl * dp));
   return 1;
+}
+
+int orc_star_state(double dl, double ul, double pl, double dr, double ur, double pr, double g,
+                   double p0, double tol, int max_iter, double *pstar, double *ustar, int *iters) {
+  side_t L = {dl, ul, pl, sqrt(g * pl / dl)}, R = {dr, ur, pr, sqrt(g * pr / dr)};
+  *iters = 0;
+  /* vacuum generation test, Toro eq. 4.40 */
+  if (2.0 * (L.c + R.c) / (g - 1.0) <= ur - ul) {
+    *pstar = 0.0;
+    *ustar = 0.5 * (ul + ur);
+    return 2;
+  }
+  int probe = p0 <= 0.0 && orc_strong_waves(dl, ul, pl, dr, ur, pr, g);
+  double p = p0 > 0.0 ? p0 : orc_two_rarefaction_guess(dl, ul, pl, dr, ur, pr, g);
+  last_eval_t le;
+  return star_solve(&L, &R, g, p, probe, tol, max_iter, pstar, ustar, iters, &le);
+}
+
+/* Start of a hydro face solve: the two-rarefaction guess, with the bracket
+ * probe for strong waves. */
+static double face_start(double dl, double ul, double pl, double dr, double ur, double pr, double g, int *probe) {
+  *probe = orc_strong_waves(dl, ul, pl, dr, ur, pr, g);
+  return orc_two_rarefaction_guess(dl, ul, pl, dr, ur, pr, g);
 }
 
 /* Sample the exact solution at x/t = 0 (Toro section 4.5; vacuum
@@ -154,8 +182,24 @@ static void fan_right(const side_t *R, double g, double *d, double *u, double *p
   *p = R->p * pow(r, 2.0 * g / (g - 1.0));
 }
 
+/* pr^(1/g) from q = pr^((g-1)/2g): q^(2/(g-1)) by multiplications when
+ * 2/(g-1) is an integer (g = 5/3: 3, g = 7/5: 5) */
+static double pow_inv_gamma(double q, double pr, double g) {
+  double k = 2.0 / (g - 1.0), kn = rint(k);
+  if (fabs(k - kn) < 1e-9 && kn >= 1.0 && kn <= 16.0) {
+    double r = q;
+    for (int n = 1; n < (int)kn; ++n) r *= q;
+    return r;
+  }
+  return pow(pr, 1.0 / g);
+}
+static double q_at(double ps, double pK, double g, double qe, double pe) {
+  double ex = (g - 1.0) / (2.0 * g);
+  return qe >= 0.0 ? qe * (1.0 + ex * (ps - pe) / pe) : pow(ps / pK, ex);
+}
+
 static void sample0(const side_t *L, const side_t *R, double g, double ps, double us, int vac,
-                    double *d, double *u, double *p, int *from_right) {
+                    double *d, double *u, double *p, int *from_right, const last_eval_t *le) {
   if (vac) {
     double sl = L->u + 2.0 * L->c / (g - 1.0), sr = R->u - 2.0 * R->c / (g - 1.0);
     if (0.0 <= L->u - L->c) { *from_right = 0; *d = L->d; *u = L->u; *p = L->p; }
@@ -177,8 +221,9 @@ static void sample0(const side_t *L, const side_t *R, double g, double ps, doubl
       if (0.0 <= L->u - L->c) { *d = L->d; *u = L->u; *p = L->p; }
       else {
         double pr = ps / L->p;
-        double cml = L->c * pow(pr, g1);
-        if (0.0 > us - cml) { *d = L->d * pow(pr, 1.0 / g); *u = us; *p = ps; }
+        double q = le ? q_at(ps, L->p, g, le->qL, le->pe) : pow(pr, g1);
+        double cml = L->c * q;
+        if (0.0 > us - cml) { *d = L->d * (le ? pow_inv_gamma(q, pr, g) : pow(pr, 1.0 / g)); *u = us; *p = ps; }
         else fan_left(L, g, d, u, p);
       }
     }
@@ -193,8 +238,9 @@ static void sample0(const side_t *L, const side_t *R, double g, double ps, doubl
       if (0.0 >= R->u + R->c) { *d = R->d; *u = R->u; *p = R->p; }
       else {
         double pr = ps / R->p;
-        double cmr = R->c * pow(pr, g1);
-        if (0.0 <= us + cmr) { *d = R->d * pow(pr, 1.0 / g); *u = us; *p = ps; }
+        double q = le ? q_at(ps, R->p, g, le->qR, le->pe) : pow(pr, g1);
+        double cmr = R->c * q;
+        if (0.0 <= us + cmr) { *d = R->d * (le ? pow_inv_gamma(q, pr, g) : pow(pr, 1.0 / g)); *u = us; *p = ps; }
         else fan_right(R, g, d, u, p);
       }
     }
@@ -207,14 +253,21 @@ static void sample0(const side_t *L, const side_t *R, double g, double ps, doubl
 int orc_exact_flux(int dir, const double *VL, const double *VR, double gamma, double tol,
                    int max_iter, double F[6], int *iters) {
   int n = dir;                                       /* normal velocity slot */
-  double ps, us;
-  int st = orc_star_state(VL[0], VL[n], VL[4], VR[0], VR[n], VR[4], gamma, 0.0, tol, max_iter,
-                          &ps, &us, iters);
   side_t L = {VL[0], VL[n], VL[4], sqrt(gamma * VL[4] / VL[0])};
   side_t R = {VR[0], VR[n], VR[4], sqrt(gamma * VR[4] / VR[0])};
+  double ps = 0.0, us = 0.5 * (L.u + R.u);
+  int vac = 2.0 * (L.c + R.c) / (gamma - 1.0) <= R.u - L.u;
+  int st = 0;
+  last_eval_t le;
+  *iters = 0;
+  if (!vac) {
+    int probe;
+    double p0 = face_start(L.d, L.u, L.p, R.d, R.u, R.p, gamma, &probe);
+    st = star_solve(&L, &R, gamma, p0, probe, tol, max_iter, &ps, &us, iters, &le);
+  }
   double d, u, p;
   int fr;
-  sample0(&L, &R, gamma, ps, us, st == 2, &d, &u, &p, &fr);
+  sample0(&L, &R, gamma, ps, us, vac, &d, &u, &p, &fr, vac ? NULL : &le);
   const double *Vt = fr ? VR : VL;
   double v[3] = {Vt[1], Vt[2], Vt[3]};
   v[dir - 1] = u;
