@@ -42,63 +42,69 @@ static_assert(sizeof(MlpPacked) % 16 == 0, "MlpPacked must be a multiple of 16 b
 
 // ---------------------------------------------------------------------------
 // pressure functions, guess, Newton, star velocity
+//
+// Newton runs on w = p^z, z = (g-1)/(2g), not on p.  In w the rarefaction
+// branch of f_K (Toro eq. 4.7) is linear, f_K = 2 c_K/(g-1) (w/w_K - 1), so
+// the two-rarefaction guess (eq. 4.46) is the root of the linear part and
+// the exact root where both waves are rarefactions.  For g <= 5/3 the
+// shock branch (eq. 4.6) is convex in w, so Newton from the two-rarefaction
+// guess, which lies at or right of the root, descends monotonically; for
+// stiffer gases it is not convex near w_K and the bracket safeguards carry
+// the iteration.  p = w^(1/z) with 1/z = 2 + 2/(g-1) is an integer power
+// for g = 5/3, 7/5, 4/3, so the iteration needs no transcendental function
+// there; w_K = p_K^z is taken once per side.
 // ---------------------------------------------------------------------------
-struct Side { double d, u, p, c; };
+struct Side { double d, u, p, c, w; };              // w = p^z
 
 // x^y for x > 0 as exp2(y log2 x): the relative error is a few ulp times
 // |y log2 x|, far below the solver's tolerance, at a fraction of the cost
 // of the correctly rounded FP64 pow
 __device__ __forceinline__ double powp(double x, double y) { return exp2(y * log2(x)); }
 
-// x^k by multiplications when k is an integer in [1, 16] (g = 5/3: the
-// fan exponents 2/(g-1) = 3, 2g/(g-1) = 5 and the guess exponent
-// 2g/(g-1) = 5), else powp
+// x^k by binary powering when k is an integer in [1, 16], else powp
 __device__ __forceinline__ double pow_k(double x, double k) {
   const double kn = rint(k);
   if (fabs(k - kn) < 1e-9 && kn >= 1.0 && kn <= 16.0) {
-    double r = x;
-    for (int n = 1; n < (int)kn; ++n) r *= x;
+    int e = (int)kn;
+    double r = 1.0, b = x;
+    while (e) {
+      if (e & 1) r *= b;
+      e >>= 1;
+      if (e) b *= b;
+    }
     return r;
   }
   return powp(x, k);
 }
 
-// qr = (p/pK)^((g-1)/2g) on the rarefaction branch, -1 on the shock branch
-__device__ __forceinline__ void pres_fn(double p, const Side &s, double g, double &f, double &fd, double &qr) {
-  if (p <= s.p) {                                   // rarefaction, Toro eq. 4.7
-    double prat = p / s.p;
-    double ex = (g - 1.0) / (2.0 * g);
-    double q = powp(prat, ex);
-    f = 2.0 * s.c / (g - 1.0) * (q - 1.0);
-    fd = q / (prat * s.d * s.c);                    // (p/pK)^(-(g+1)/2g) / (dK cK)
-    qr = q;
+__device__ __forceinline__ double zexp(double g) { return (g - 1.0) / (2.0 * g); }
+__device__ __forceinline__ double p_of_w(double w, double g) { return pow_k(w, 2.0 * g / (g - 1.0)); }
+__device__ __forceinline__ Side make_side(double d, double u, double p, double c, double g) {
+  return Side{d, u, p, c, powp(p, zexp(g))};
+}
+
+// f_K(w) and df_K/dw; p = w^(1/z) is passed in
+__device__ __forceinline__ void pres_fn(double w, double p, const Side &s, double g, double &f, double &fd) {
+  if (w <= s.w) {                                   // rarefaction, Toro eq. 4.7
+    const double k = 2.0 * s.c / ((g - 1.0) * s.w);
+    f = k * (w - s.w);
+    fd = k;
   } else {                                          // shock, Toro eq. 4.6
-    double A = 2.0 / ((g + 1.0) * s.d);
-    double B = (g - 1.0) / (g + 1.0) * s.p;
-    double q = sqrt(A / (B + p));
+    const double A = 2.0 / ((g + 1.0) * s.d);
+    const double B = (g - 1.0) / (g + 1.0) * s.p;
+    const double r = 1.0 / (B + p);
+    const double q = sqrt(A * r);
     f = (p - s.p) * q;
-    fd = (1.0 - 0.5 * (p - s.p) / (B + p)) * q;
-    qr = -1.0;
+    fd = (1.0 - 0.5 * (p - s.p) * r) * q * (p / (zexp(g) * w));   // df/dp dp/dw
   }
 }
-__device__ __forceinline__ void pres_fn(double p, const Side &s, double g, double &f, double &fd) {
-  double qr;
-  pres_fn(p, s, g, f, fd, qr);
-}
 
-// The last pressure-function evaluation of a Newton solve: its pressure and
-// (pe/pK)^((g-1)/2g) of each side that took the rarefaction branch there
-// (-1 otherwise).  The sampling reuses these powers, carried to p* to first
-// order (p* - pe is the last Newton step, so the error is of the order of
-// its square).
-struct LastEval { double pe, qL, qR; };
-
-__device__ __forceinline__ double tr_guess(const Side &L, const Side &R, double g) {
-  double z = (g - 1.0) / (2.0 * g);
-  double num = L.c + R.c - 0.5 * (g - 1.0) * (R.u - L.u);
-  if (num <= 0.0) return 0.0;
-  return pow_k(num / (L.c / powp(L.p, z) + R.c / powp(R.p, z)), 1.0 / z);
+// two-rarefaction guess in w (0 where the states generate vacuum)
+__device__ __forceinline__ double tr_w(const Side &L, const Side &R, double g) {
+  const double num = L.c + R.c - 0.5 * (g - 1.0) * (R.u - L.u);
+  return num > 0.0 ? num / (L.c / L.w + R.c / R.w) : 0.0;
 }
+__device__ __forceinline__ double tr_guess(const Side &L, const Side &R, double g) { return p_of_w(tr_w(L, R, g), g); }
 
 // vacuum generation test, Toro eq. 4.40
 __device__ __forceinline__ bool vacuum(const Side &L, const Side &R, double g) {
@@ -113,88 +119,77 @@ __device__ __forceinline__ bool tr_exact(const Side &L, const Side &R, double pt
 // estimate ppv covers a factor of two or more, and ppv lies above
 // min(p_L, p_R).  Elsewhere the waves are weak or both are rarefactions
 // (ppv <= pmin; Toro section 9.5.1), and Newton from the two-rarefaction
-// guess converges in two or three evaluations: the network is consulted and
-// the bracket probed only for strong waves.
+// guess converges in one to three evaluations: the network is consulted
+// only for strong waves.
 __device__ __forceinline__ bool strong_waves(const Side &L, const Side &R) {
   const double pmin = fmin(L.p, R.p), pmax = fmax(L.p, R.p);
   const double ppv = 0.5 * (L.p + R.p) - 0.125 * (R.u - L.u) * (L.d + R.d) * (L.c + R.c);
   return ppv > pmin && fmax(pmax, ppv) >= 2.0 * pmin;
 }
 
-// Start of a hydro face solve: the two-rarefaction guess (the root where
-// both waves are rarefactions, within a few per cent for weak waves), with
-// the bracket probe for strong waves.
-__device__ __forceinline__ double face_start(const Side &L, const Side &R, double g, bool &probe) {
-  probe = strong_waves(L, R);
-  return tr_guess(L, R, g);
-}
+// The star state of a solve: p*, u* and w* = p*^z (the sampling takes the
+// rarefaction-side powers (p*/p_K)^z = w*/w_K from it).
+struct Star { double p, u, w; };
 
-// Newton from p0 > 0.  With `probe`, the bracket is first located as
-// [pa, pb] = [p/4, p] with f(pb) > 0, starting from p = max(p_L, p_R) and
-// growing by 4, and a start outside it is replaced by sqrt(pa * pb) (for
-// strong shocks the two-rarefaction guess lies far below the root, where f
-// is steep and Newton climbs slowly).  Converged when the Newton step is
-// below tol * p or, once the last two steps show the quadratic regime, when
-// the predicted next step |step|^3 / prev^2 is below tol * p / 100.  f is
-// increasing and concave, so an iterate at or left of the root stays there;
-// a step that leaves the bracket of evaluated signs is replaced by a
-// geometric bisection (both ends known), a decimation towards zero (no lower
-// end yet) or a growth by 4 (no upper end yet).  u* is f_L, f_R linearised
-// from the last evaluation to the returned p*.  Returns the number of
-// pressure-function evaluations (probes included), or -max_iter when not
-// converged.
-__device__ __forceinline__ int newton(const Side &L, const Side &R, double g, double p0, double tol, int max_iter,
-                                      double &pout, double &uout, bool probe = false, LastEval *le = nullptr) {
-  const double du = R.u - L.u;
-  double pa = 0.0, pb = DBL_MAX;
-  double p = p0, prev = -1.0;
-  double fl = 0., fdl = 0., fr = 0., fdr = 0., pe = p0, qL = -1.0, qR = -1.0;
+// Newton on f(w) = f_L + f_R + (u_R - u_L) from w0 >= 0.  Converged when
+// the step is below tol * z * w (a relative step of tol in p); once the
+// last two steps show the quadratic regime, when the predicted next step
+// |step|^3 / prev^2 is below a hundredth of that; or when the bracket
+// [wa, wb] of evaluated signs is that narrow (near vacuum, where the
+// rounding of f exceeds the tolerance on the step; the root is its
+// midpoint).  A step that leaves the bracket is replaced by its midpoint
+// (or a doubling while no upper end is known).  u* is f_L, f_R linearised
+// from the last evaluation to the returned w*.  Returns the number of
+// evaluations, or -max_iter when not converged.
+__device__ __forceinline__ int newton(const Side &L, const Side &R, double g, double w0, double tol, int max_iter,
+                                      Star &out) {
+  const double du = R.u - L.u, ztol = zexp(g) * tol;
+  double wa = 0.0, wb = DBL_MAX;
+  double w = w0, prev = -1.0, p = 0.0;
+  double fl = 0., fdl = 0., fr = 0., fdr = 0., we = w0;
   int evals = 0;
-  if (le) { le->pe = p0; le->qL = -1.0; le->qR = -1.0; }
-  if (probe) {
-    double q = fmax(L.p, R.p);
-    for (int k = 0; k < 64 && evals < max_iter; ++k) {
-      pres_fn(q, L, g, fl, fdl); pres_fn(q, R, g, fr, fdr);
-      ++evals;
-      if (fl + fr + du > 0.0) { pb = q; break; }
-      pa = q;
-      q *= 4.0;
-    }
-    if (!(p > pa && p < pb)) p = (pa > 0.0 && pb < DBL_MAX) ? sqrt(pa * pb) : (pb < DBL_MAX ? 0.5 * pb : 4.0 * pa);
-  }
   for (; evals < max_iter;) {
-    pres_fn(p, L, g, fl, fdl, qL); pres_fn(p, R, g, fr, fdr, qR);
+    p = p_of_w(w, g);
+    pres_fn(w, p, L, g, fl, fdl);
+    pres_fn(w, p, R, g, fr, fdr);
     ++evals;
-    pe = p;
-    if (le) { le->pe = pe; le->qL = qL; le->qR = qR; }
+    we = w;
     const double f = fl + fr + du;
     if (f == 0.0) {
-      pout = p;
-      uout = 0.5 * (L.u + R.u) + 0.5 * (fr - fl);
+      out.w = w; out.p = p;
+      out.u = 0.5 * (L.u + R.u) + 0.5 * (fr - fl);
       return evals;
     }
-    if (f < 0.0) pa = p; else pb = p;
+    if (f < 0.0) wa = w; else wb = w;
+    if (wb - wa <= ztol * w) {
+      out.w = 0.5 * (wa + wb);
+      out.p = p_of_w(out.w, g);
+      const double dw = out.w - we;
+      out.u = 0.5 * (L.u + R.u) + 0.5 * ((fr + fdr * dw) - (fl + fdl * dw));
+      return evals;
+    }
     const double step = f / (fdl + fdr);
-    double pn = p - step;
+    double wn = w - step;
     const double as = fabs(step);
-    const bool inside = pn > pa && pn < pb;
-    if (as <= tol * p || (inside && prev > 0.0 && as < prev && as * (as / prev) * (as / prev) <= 0.01 * tol * p)) {
-      pout = pn > 0.0 ? pn : p;
-      const double dp = pout - pe;
-      uout = 0.5 * (L.u + R.u) + 0.5 * ((fr + fdr * dp) - (fl + fdl * dp));
+    const bool inside = wn > wa && wn < wb;
+    if (as <= ztol * w || (inside && prev > 0.0 && as < prev && as * (as / prev) * (as / prev) <= 0.01 * ztol * w)) {
+      out.w = wn > 0.0 ? wn : w;
+      out.p = p_of_w(out.w, g);
+      const double dw = out.w - we;
+      out.u = 0.5 * (L.u + R.u) + 0.5 * ((fr + fdr * dw) - (fl + fdl * dw));
       return evals;
     }
     if (!inside) {
-      pn = pb == DBL_MAX ? 4.0 * p : (pa > 0.0 ? sqrt(pa * pb) : 0.01 * pb);
+      wn = wb == DBL_MAX ? 2.0 * w : 0.5 * (wa + wb);
       prev = -1.0;
     } else {
       prev = as;
     }
-    p = pn;
+    w = wn;
   }
-  pout = p;
-  const double dp = pout - pe;
-  uout = 0.5 * (L.u + R.u) + 0.5 * ((fr + fdr * dp) - (fl + fdl * dp));
+  out.w = w; out.p = p_of_w(w, g);
+  const double dw = w - we;
+  out.u = 0.5 * (L.u + R.u) + 0.5 * ((fr + fdr * dw) - (fl + fdl * dw));
   return -max_iter;
 }
 
@@ -216,23 +211,10 @@ __device__ __forceinline__ void fan_right(const Side &R, double g, double &d, do
   p = R.p * pow_k(r, 2.0 * g / (g - 1.0));
 }
 
-// (pr)^(1/g) from q = pr^((g-1)/2g): q^(2/(g-1)), by multiplications when
-// 2/(g-1) is an integer (g = 5/3: 3, g = 7/5: 5)
-__device__ __forceinline__ double pow_inv_gamma(double q, double pr, double g) {
-  const double k = 2.0 / (g - 1.0);
-  return fabs(k - rint(k)) < 1e-9 && k >= 1.0 && k <= 16.0 ? pow_k(q, k) : powp(pr, 1.0 / g);
-}
-
-// pr^((g-1)/2g) at pr = ps/pK: from the last evaluation when that side took
-// the rarefaction branch there, else directly
-__device__ __forceinline__ double q_at(double ps, double pK, double g, double qe, double pe) {
-  const double ex = (g - 1.0) / (2.0 * g);
-  return qe >= 0.0 ? qe * (1.0 + ex * (ps - pe) / pe) : powp(ps / pK, ex);
-}
-
-// (d, u, p) at x/t = 0 and which side supplies the transverse velocities
-__device__ __forceinline__ void sample0(const Side &L, const Side &R, double g, double ps, double us, bool vac,
-                                        double &d, double &u, double &p, bool &right, const LastEval *le = nullptr) {
+// (d, u, p) at x/t = 0 and which side supplies the transverse velocities;
+// behind a rarefaction (p*/p_K)^z = w*/w_K and rho*_K = rho_K (w*/w_K)^(2/(g-1))
+__device__ __forceinline__ void sample0(const Side &L, const Side &R, double g, const Star &S, bool vac,
+                                        double &d, double &u, double &p, bool &right) {
   if (vac) {
     const double sl = L.u + 2.0 * L.c / (g - 1.0), sr = R.u - 2.0 * R.c / (g - 1.0);
     if (0.0 <= L.u - L.c) { right = false; d = L.d; u = L.u; p = L.p; }
@@ -242,7 +224,8 @@ __device__ __forceinline__ void sample0(const Side &L, const Side &R, double g, 
     else { right = false; d = 0.0; u = 0.0; p = 0.0; }
     return;
   }
-  const double g1 = (g - 1.0) / (2.0 * g), g2 = (g + 1.0) / (2.0 * g), g6 = (g - 1.0) / (g + 1.0);
+  const double ps = S.p, us = S.u;
+  const double g1 = (g - 1.0) / (2.0 * g), g2 = (g + 1.0) / (2.0 * g), g6 = (g - 1.0) / (g + 1.0), k = 2.0 / (g - 1.0);
   if (0.0 <= us) {                                   // left of the contact
     right = false;
     if (ps > L.p) {                                  // left shock
@@ -253,10 +236,9 @@ __device__ __forceinline__ void sample0(const Side &L, const Side &R, double g, 
     } else {                                         // left rarefaction
       if (0.0 <= L.u - L.c) { d = L.d; u = L.u; p = L.p; }
       else {
-        const double pr = ps / L.p;
-        const double q = le ? q_at(ps, L.p, g, le->qL, le->pe) : powp(pr, g1);
+        const double q = S.w / L.w;
         const double cml = L.c * q;
-        if (0.0 > us - cml) { d = L.d * (le ? pow_inv_gamma(q, pr, g) : powp(pr, 1.0 / g)); u = us; p = ps; }
+        if (0.0 > us - cml) { d = L.d * pow_k(q, k); u = us; p = ps; }
         else fan_left(L, g, d, u, p);
       }
     }
@@ -270,10 +252,9 @@ __device__ __forceinline__ void sample0(const Side &L, const Side &R, double g, 
     } else {
       if (0.0 >= R.u + R.c) { d = R.d; u = R.u; p = R.p; }
       else {
-        const double pr = ps / R.p;
-        const double q = le ? q_at(ps, R.p, g, le->qR, le->pe) : powp(pr, g1);
+        const double q = S.w / R.w;
         const double cmr = R.c * q;
-        if (0.0 <= us + cmr) { d = R.d * (le ? pow_inv_gamma(q, pr, g) : powp(pr, 1.0 / g)); u = us; p = ps; }
+        if (0.0 <= us + cmr) { d = R.d * pow_k(q, k); u = us; p = ps; }
         else fan_right(R, g, d, u, p);
       }
     }
@@ -286,11 +267,10 @@ __device__ __forceinline__ void sample0(const Side &L, const Side &R, double g, 
 // normal direction (1..3).
 template <int DIR>
 __device__ __forceinline__ void godunov_flux(const double *VL, const double *VR, const Side &L, const Side &R, double g,
-                                             double ps, double us, bool vac, double F[6],
-                                             const LastEval *le = nullptr) {
+                                             const Star &S, bool vac, double F[6]) {
   double d, u, p;
   bool right;
-  sample0(L, R, g, ps, us, vac, d, u, p, right, le);
+  sample0(L, R, g, S, vac, d, u, p, right);
   double v[3];
 #pragma unroll
   for (int m = 0; m < 3; ++m) v[m] = (m == DIR - 1) ? u : (right ? VR[1 + m] : VL[1 + m]);

@@ -241,7 +241,7 @@ __device__ void cfl_block_reduce(CflCand c, int blk, double cfl, CflPart *part) 
 __device__ __forceinline__ xrs::Side side_of(const double *V, int n, double g, unsigned &st) {
   const double c2 = g * V[HP] / V[HD];
   if (!(c2 > 0.0)) st |= ST_NEG_SOUND;
-  return xrs::Side{V[HD], V[n], V[HP], sqrt(c2)};
+  return xrs::make_side(V[HD], V[n], V[HP], sqrt(c2), g);
 }
 
 // keep a hashed sample of the face states (two-rarefaction guess inexact) for
@@ -259,21 +259,16 @@ __device__ __forceinline__ void harvest_face(const DevParams &P, const xrs::Side
   S[3 * c + k] = R.d; S[4 * c + k] = R.u; S[5 * c + k] = R.p; S[6 * c + k] = g;
 }
 
-// Godunov flux from the exact solution (start: xrs::face_start)
+// Godunov flux from the exact solution, Newton from the two-rarefaction guess
 template <int DIR>
 __device__ __forceinline__ void exact_face(const DevParams &P, const double *VL, const double *VR, double F[6],
                                            unsigned &st) {
   const double g = P.gamma;
   const xrs::Side L = side_of(VL, DIR, g, st), R = side_of(VR, DIR, g, st);
   const bool vac = xrs::vacuum(L, R, g);
-  double ps = 0.0, us = 0.5 * (L.u + R.u);
-  xrs::LastEval le;
-  if (!vac) {
-    bool probe;
-    const double p0 = xrs::face_start(L, R, g, probe);
-    if (xrs::newton(L, R, g, p0, P.rs_tol, P.rs_max_iter, ps, us, probe, &le) < 0) st |= ST_NEWTON;
-  }
-  xrs::godunov_flux<DIR>(VL, VR, L, R, g, ps, us, vac, F, vac ? nullptr : &le);
+  xrs::Star S{0.0, 0.5 * (L.u + R.u), 0.0};
+  if (!vac && xrs::newton(L, R, g, xrs::tr_w(L, R, g), P.rs_tol, P.rs_max_iter, S) < 0) st |= ST_NEWTON;
+  xrs::godunov_flux<DIR>(VL, VR, L, R, g, S, vac, F);
 }
 
 // ---------------------------------------------------------------------------

@@ -371,10 +371,10 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
     // exact solver.  With a network attached, pass 1 evaluates its
     // tensor-core guess for the faces with strong waves (the network sits
     // over the slope scratch, dead from here on) and leaves the start value
-    // in sP0 (over the unused 1/(game-1) array; negative = network start,
-    // limited to three evaluations; 0 = two-rarefaction start); pass 2 runs
-    // Newton and the Godunov flux.  Each thread reads back only its own
-    // entries.
+    // w0 = p0^z in sP0 (over the unused 1/(game-1) array; negative = network
+    // start, limited to three evaluations; 0 = two-rarefaction start); pass
+    // 2 runs Newton and the Godunov flux.  Each thread reads back only its
+    // own entries.
     double *sP0 = sIg;
     const bool learned = P.mlp != nullptr;
     const double g = P.gamma;
@@ -382,17 +382,23 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
       return left ? Vs(qq, s - G::step) + double(sWp[qq * G::SC + t - G::step])
                   : Vs(qq, s) + double(sWm[qq * G::SC + t]);
     };
-    auto sides = [&](int s, int t, xrs::Side &L, xrs::Side &R) {
+    // the two face states; w = p^z only with `with_w` (pass 1a tests for
+    // strong waves without it)
+    auto sides = [&](int s, int t, xrs::Side &L, xrs::Side &R, bool with_w = true) {
       const double dl = face(0, true, s, t), ul = face(DIR, true, s, t), pl = face(4, true, s, t);
       const double dr = face(0, false, s, t), ur = face(DIR, false, s, t), pr = face(4, false, s, t);
       const double c2l = g * pl / dl, c2r = g * pr / dr;
       if (!(c2l > 0.0) || !(c2r > 0.0)) st |= ST_NEG_SOUND;
-      L = xrs::Side{dl, ul, pl, sqrt(c2l)};
-      R = xrs::Side{dr, ur, pr, sqrt(c2r)};
+      L = xrs::Side{dl, ul, pl, sqrt(c2l), 0.0};
+      R = xrs::Side{dr, ur, pr, sqrt(c2r), 0.0};
+      if (with_w) {
+        L.w = xrs::powp(pl, xrs::zexp(g));
+        R.w = xrs::powp(pr, xrs::zexp(g));
+      }
     };
     if (learned) {
       // pass 1a: faces with strong waves and an inexact two-rarefaction
-      // guess get sP0 = p_TR > 0, all others 0 (two-rarefaction start)
+      // guess get sP0 = w_TR > 0, all others 0 (two-rarefaction start)
       int need = 0;
 #pragma unroll
       for (int it = 0; it < NIT; ++it) {
@@ -402,11 +408,13 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
         G::dec(t, G::LC, 1, x, l);
         if (x < 0) continue;
         xrs::Side L, R;
-        sides(G::at(x, l, G::L4, 4), t, L, R);
+        sides(G::at(x, l, G::L4, 4), t, L, R, false);
         double q = 0.0;
         if (!xrs::vacuum(L, R, g) && xrs::strong_waves(L, R)) {
-          const double ptr = xrs::tr_guess(L, R, g);
-          if (!xrs::tr_exact(L, R, ptr)) q = ptr;
+          L.w = xrs::powp(L.p, xrs::zexp(g));
+          R.w = xrs::powp(R.p, xrs::zexp(g));
+          const double wtr = xrs::tr_w(L, R, g);
+          if (!xrs::tr_exact(L, R, xrs::p_of_w(wtr, g))) q = wtr;
         }
         sP0[t] = q;
         need |= q > 0.0;
@@ -426,16 +434,16 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
           const double q = (t < G::SC && x >= 0) ? sP0[t] : 0.0;
           const bool net = q > 0.0;
           if (!__any_sync(0xffffffffu, net)) continue;
-          xrs::Side L{1.0, 0.0, 1.0, 1.0}, R{1.0, 0.0, 1.0, 1.0};
+          xrs::Side L{1.0, 0.0, 1.0, 1.0, 1.0}, R{1.0, 0.0, 1.0, 1.0, 1.0};
           if (net) sides(G::at(x, l, G::L4, 4), t, L, R);
           float f[xrs::NIN];
-          if (net) xrs::features(L, R, g, q, f);
+          if (net) xrs::features(L, R, g, xrs::p_of_w(q, g), f);
           else {
 #pragma unroll
             for (int k = 0; k < xrs::NIN; ++k) f[k] = 0.f;
           }
           const float y = fminf(fmaxf(xrs::mlp_lane(*sM, f), -20.f), 20.f);
-          if (net) sP0[t] = -(q * (double)expf(y));
+          if (net) sP0[t] = -(q * (double)expf(float(xrs::zexp(g)) * y));    // (p*/p_TR)^z
         }
       }
     }
@@ -450,18 +458,14 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
       xrs::Side L, R;
       sides(s, t, L, R);
       const bool vac = xrs::vacuum(L, R, g);
-      double ps = 0.0, us = 0.5 * (L.u + R.u);
-      xrs::LastEval le;
+      xrs::Star S{0.0, 0.5 * (L.u + R.u), 0.0};
       if (!vac) {
         const double q = learned ? sP0[t] : 0.0;
-        bool strong;
-        const double p0 = q < 0.0 ? -q : xrs::face_start(L, R, g, strong);
-        if (q < 0.0) strong = xrs::strong_waves(L, R);
-        int k = xrs::newton(L, R, g, p0, P.rs_tol, q < 0.0 ? 3 : P.rs_max_iter, ps, us, q >= 0.0 && strong, &le);
-        if (k < 0 && q < 0.0)
-          k = xrs::newton(L, R, g, xrs::tr_guess(L, R, g), P.rs_tol, P.rs_max_iter, ps, us, strong, &le);
+        const double w0 = q < 0.0 ? -q : xrs::tr_w(L, R, g);
+        int k = xrs::newton(L, R, g, w0, P.rs_tol, q < 0.0 ? 3 : P.rs_max_iter, S);
+        if (k < 0 && q < 0.0) k = xrs::newton(L, R, g, xrs::tr_w(L, R, g), P.rs_tol, P.rs_max_iter, S);
         if (k < 0) st |= ST_NEWTON;
-        if (P.harvest && (q < 0.0 || (strong && !xrs::tr_exact(L, R, p0))))
+        if (P.harvest && (q < 0.0 || (xrs::strong_waves(L, R) && !xrs::tr_exact(L, R, xrs::p_of_w(w0, g)))))
           harvest_face(P, L, R, g, (unsigned)(blockIdx.x * 4 + DIR) * 2048u + (unsigned)t);
       }
       double VL[8], VR[8];
@@ -472,7 +476,7 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
         VR[n] = face(qq, false, s, t);
       }
       double F[6];
-      xrs::godunov_flux<DIR>(VL, VR, L, R, g, ps, us, vac, F, vac ? nullptr : &le);
+      xrs::godunov_flux<DIR>(VL, VR, L, R, g, S, vac, F);
 #pragma unroll
       for (int n = 0; n < 6; ++n) Fr[it][n] = F[n];
       double fv = 0., fe = 0.;
