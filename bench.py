@@ -367,6 +367,7 @@ def amr_workload(args):
     zones = g.ncells
     peak, peak_kind = measured_peaks()
     ms, outs, dts, launches, clocks, e2e_ms, hb = {}, {}, None, {}, None, None, None
+    tunings = {}
     paths = [p for p in args.paths.split(",") if p in ("fp64", "mixed", "mixed_exact")] or ["fp64", "mixed"]
     spec = {"fp64": (abi.PREC_FP64, abi.RS_HLLC), "mixed": (abi.PREC_MIXED, abi.RS_HLLC),
             "mixed_exact": (abi.PREC_MIXED, abi.RS_EXACT)}
@@ -374,6 +375,11 @@ def amr_workload(args):
         pr, rsv = spec[name]
         h = Hydro(abi.default_params(precision=pr, riemann_solver=rsv), g)
         h.upload(unk)
+        if not args.no_tune:
+            best, trials = h.autotune(dts[0] if dts is not None else h.compute_dt()[0], steps=2)
+            tunings[name] = {"best": best, "trials_ms": {"/".join(str(v) for v in t.values()): round(m, 4)
+                                                         for t, m in trials},
+                             "trial_key": "sig_threads/dir_threads/mx_threads"}
         headline = name == paths[-1]
         sampler = ClockSampler(0) if headline else None
         ms[name], used, launches[name] = run_device(h, args.steps, args.warmup, dts=dts, sampler=sampler)
@@ -381,12 +387,9 @@ def amr_workload(args):
             dts = used
         if headline:
             clocks = sampler.summary()
-        if world > 1:
-            outs[name] = h.download_owned()[0]
-        else:
-            outs[name] = np.empty_like(unk)
-            h.download(outs[name])
-        if headline and not args.no_e2e and world == 1:
+        outs[name] = np.empty_like(unk)
+        h.download(outs[name])
+        if headline and not args.no_e2e:
             pinned = torch.empty(unk.shape, dtype=torch.float64, pin_memory=True)
             host = pinned.numpy()
             host[...] = unk
@@ -412,7 +415,8 @@ def amr_workload(args):
                    "l2": f"inputs larger than L2 (state {g.nblocks * 256 * 40 / 1e6:.0f} MB plus guard buffers "
                          f"{g.nleaves * 576 * 40 / 1e6:.0f} MB)", "path": head, "hierarchy_build_s": build_s},
         "paths": {n: {"value": zones / (ms[n] * 1e-3), "ms_per_step": ms[n],
-                      **({"rel_l1_vs_fp64": errs[n]} if n in errs else {})} for n in ms},
+                      **({"rel_l1_vs_fp64": errs[n]} if n in errs else {}),
+                      **({"launch_shape": tunings[n]} if n in tunings else {})} for n in ms},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": None, "peak_kind": peak_kind,
                      "kernel": "one AMR step (restriction, halos, k_sig, per-level k_dir), 80 B/leaf zone algorithmic"},
@@ -466,6 +470,7 @@ def main():
     ap.add_argument("--nblk", type=int, default=32, help="blocks per axis (32 -> 256^3)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes (no autotuning)")
     ap.add_argument("--workload", default="kh", choices=["kh", "riemann", "amr"])
     ap.add_argument("--amr-nblk", type=int, default=32, help="root blocks per axis of the AMR hierarchy")
     ap.add_argument("--riemann-n", type=int, default=100_000_000)
@@ -541,6 +546,7 @@ def main():
             "mixed_exact": (abi.PREC_MIXED, abi.RS_EXACT, 0, "fp64_exact"),
             "mixed_learned": (abi.PREC_MIXED, abi.RS_EXACT, 1, "fp64_exact")}
     ms, outs, dts, launches, clocks, e2e_ms, hb, training = {}, {}, None, {}, None, None, None, None
+    tunings = {}
     for name in paths:
         pr, rsv, learned, _ = spec[name]
         params = abi.default_params(gamma=5.0 / 3.0, precision=pr, riemann_solver=rsv, learned_guess=learned)
@@ -557,9 +563,19 @@ def main():
             if weights is not None:
                 h.set_guess_weights(weights)
             h.upload(unk)
+        tuned = None
+        if not args.no_tune:
+            hh = h.h if world > 1 else h
+            dt0 = dts[0] if dts is not None else hh.compute_dt()[0]
+            best, trials = hh.autotune(dt0, steps=2)
+            tuned = {"best": best, "trials_ms": {"/".join(str(v) for v in t.values()): round(m, 4)
+                                                 for t, m in trials},
+                     "trial_key": "sig_threads/dir_threads/mx_threads"}
         headline = name == paths[-1]
         sampler = ClockSampler(dev) if headline else None
         ms[name], used, launches[name] = run_device(h, args.steps, warmup, dts=dts, sampler=sampler, dist=dist)
+        if tuned is not None:
+            tunings[name] = tuned
         if dts is None:
             dts = used            # later paths replay the first path's dt sequence
         if headline:
@@ -611,7 +627,8 @@ def main():
                        "zones_per_gpu": zones, "l2": f"inputs larger than L2 (state {zones * 40 / 1e6:.0f} MB)",
                        "path": head},
             "paths": {n: {"value": total / (ms[n] * 1e-3), "ms_per_step": ms[n], "note": notes[n],
-                          **({f"rel_l1_vs_{spec[n][3]}": errs[n]} if n in errs else {})} for n in ms},
+                          **({f"rel_l1_vs_{spec[n][3]}": errs[n]} if n in errs else {}),
+                          **({"launch_shape": tunings[n]} if n in tunings else {})} for n in ms},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": TRAFFIC_PER_ZONE[head] * zones if head in TRAFFIC_PER_ZONE else None,
                          "traffic_note": "DRAM bytes per step (per GPU), ncu at 160^3 scaled by zones",

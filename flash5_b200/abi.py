@@ -103,6 +103,18 @@ class GridDesc(C.Structure):
     ]
 
 
+class Tuning(C.Structure):
+    """flash_hy_tuning: threads per CTA of the transverse-flux/CFL passes,
+    the FP64 direction kernels and the mixed direction kernels."""
+    _fields_ = [("sig_threads", C.c_int), ("dir_threads", C.c_int), ("mx_threads", C.c_int)]
+
+    def as_dict(self):
+        return {"sig_threads": self.sig_threads, "dir_threads": self.dir_threads, "mx_threads": self.mx_threads}
+
+
+TUNE_MAX = 8
+
+
 def _set_sigs(lib):
     P, G, V = C.POINTER(Params), C.POINTER(GridDesc), C.POINTER(VarMap)
     dp, ip, vp = C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_void_p
@@ -129,6 +141,11 @@ def _set_sigs(lib):
         "flash_hy_get_fluxes": (C.c_int, [vp, C.c_int, C.c_int, dp]),
         "flash_hy_put_fluxes": (C.c_int, [vp, C.c_int, C.c_int, dp]),
         "flash_hy_update_solution": (C.c_int, [vp, C.c_int, ip, C.c_double]),
+        "flash_hy_get_tuning": (C.c_int, [vp, C.POINTER(Tuning)]),
+        "flash_hy_set_tuning": (C.c_int, [vp, C.POINTER(Tuning)]),
+        "flash_hy_tuning_candidates": (C.c_int, [vp, ip, ip, ip, ip, ip, ip]),
+        "flash_hy_autotune": (C.c_int, [vp, C.c_double, C.c_int, C.POINTER(Tuning), C.POINTER(Tuning),
+                                        C.POINTER(C.c_float), C.c_int, ip]),
     }
     for name, (res, args) in sigs.items():
         f = getattr(lib, name)

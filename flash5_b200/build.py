@@ -2,7 +2,8 @@
 
 ``hy_variant.cu`` is compiled once per arithmetic variant: FP64 without FMA
 contraction (the parity path), FP64 with FMA, and FP32 reconstruction with
-FP64 update.  Objects go to ``flash5_b200/_build``; the shared library is
+FP64 update (three units, one per threads-per-CTA candidate of its direction
+kernels).  Objects go to ``flash5_b200/_build``; the shared library is
 written in-tree so that it travels with the repository snapshot.
 """
 import os
@@ -21,7 +22,9 @@ COMMON = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--exp
 UNITS = [
     ("hy_fp64_exact.o", "hy_variant.cu", ["-DFHY_VARIANT=1", "--fmad=false"]),
     ("hy_fp64_fma.o", "hy_variant.cu", ["-DFHY_VARIANT=2", "--fmad=true"]),
-    ("hy_mixed.o", "hy_variant.cu", ["-DFHY_VARIANT=3", "--fmad=true"]),
+    ("hy_mixed0.o", "hy_variant.cu", ["-DFHY_VARIANT=3", "-DFHY_MXSEL=0", "--fmad=true"]),
+    ("hy_mixed1.o", "hy_variant.cu", ["-DFHY_VARIANT=3", "-DFHY_MXSEL=1", "--fmad=true"]),
+    ("hy_mixed2.o", "hy_variant.cu", ["-DFHY_VARIANT=3", "-DFHY_MXSEL=2", "--fmad=true"]),
     ("flash_hy.o", "flash_hy.cu", ["--fmad=false"]),
     ("riemann_exact.o", "riemann_exact.cu", ["--fmad=true"]),
     ("cfl_noalloc.o", "cfl_noalloc.cu", ["--fmad=false"]),

@@ -37,7 +37,9 @@ struct flash_hy_ctx {
   size_t stage_bytes;
   int dt_valid;
   int launches;
-  int threads;
+  int threads;         // threads per CTA: transverse-flux and CFL passes
+  int dir_threads;     // FP64 direction kernels
+  int mx_sel;          // mixed direction kernels: candidate 0, 1, 2
   int host_ng;         // guard layers of the caller's UNK arrays
   float *d_wmaster;    // learned guess: FP32 master weights
   void *d_mlp;         // learned guess: packed BF16 inference copy (xrs::MlpPacked)
@@ -278,6 +280,8 @@ extern "C" int flash_hy_create(const flash_hy_params *params, const flash_hy_gri
   c->ncells = c->ncb * g->nblocks;
   c->device = device;
   c->threads = g->ndim == 3 ? 320 : (g->nxb == 8 ? 96 : 288);  // line cells split evenly
+  c->dir_threads = c->threads;
+  c->mx_sel = 1;
   c->host_ng = g->nguard;
   *out = c;
   int rc = 0;
@@ -591,6 +595,8 @@ static int enqueue_step(flash_hy_ctx *c, double dt, const int *d_list, int nlaun
   a.part = c->d_part;
   a.nlaunch = nlaunch;
   a.threads = c->threads;
+  a.dir_threads = c->dir_threads;
+  a.mx_sel = c->mx_sel;
   a.stream = c->stream;
   a.nlev = 0;
   int pre = 0;
@@ -840,6 +846,8 @@ extern "C" int flash_hy_compute_dt(flash_hy_ctx *c, double *dt_out, int minloc_o
     a.part = c->d_part;
     a.nlaunch = c->nblocks;
     a.threads = c->threads;
+    a.dir_threads = c->dir_threads;
+    a.mx_sel = c->mx_sel;
     a.stream = c->stream;
     a.set_attr = true;
     if (cfl_state(a, c->ndim, c->nx, c->ny, c->nz) < 0) return fail(c, FLASH_HY_ERR_CUDA, "cfl launch%s", "");
@@ -861,6 +869,178 @@ extern "C" int flash_hy_compute_dt(flash_hy_ctx *c, double *dt_out, int minloc_o
   int st = (int)*c->h_status;
   if (!(c->h_dt->dt > 0.0)) st |= FLASH_HY_ERR_NONPOS_DT;
   return st;
+}
+
+// ---------------------------------------------------------------------------
+// launch shapes and the autotuner
+// ---------------------------------------------------------------------------
+static int thread_candidates(const flash_hy_ctx *c, int *v) {
+  if (c->ndim == 3) { const int s[] = {128, 192, 256, 320}; memcpy(v, s, sizeof(s)); return 4; }
+  if (c->nx == 8) { const int s[] = {64, 96, 128}; memcpy(v, s, sizeof(s)); return 3; }
+  const int s[] = {128, 192, 256, 288, 320};
+  memcpy(v, s, sizeof(s));
+  return 5;
+}
+static int index_of(const int *v, int n, int x) {
+  for (int q = 0; q < n; ++q)
+    if (v[q] == x) return q;
+  return -1;
+}
+
+extern "C" int flash_hy_tuning_candidates(flash_hy_ctx *c, int *sig, int *n_sig, int *dir, int *n_dir, int *mx,
+                                          int *n_mx) {
+  if (!c || !sig || !n_sig || !dir || !n_dir || !mx || !n_mx) return FLASH_HY_ERR_BAD_ARG;
+  *n_sig = thread_candidates(c, sig);
+  *n_dir = thread_candidates(c, dir);
+  *n_mx = 3;
+  for (int q = 0; q < 3; ++q) mx[q] = mx_threads_of(q, c->ndim, c->nx);
+  return 0;
+}
+
+extern "C" int flash_hy_get_tuning(flash_hy_ctx *c, flash_hy_tuning *out) {
+  if (!c || !out) return FLASH_HY_ERR_BAD_ARG;
+  out->sig_threads = c->threads;
+  out->dir_threads = c->dir_threads;
+  out->mx_threads = mx_threads_of(c->mx_sel, c->ndim, c->nx);
+  return 0;
+}
+
+extern "C" int flash_hy_set_tuning(flash_hy_ctx *c, const flash_hy_tuning *t) {
+  if (!c || !t) return FLASH_HY_ERR_BAD_ARG;
+  int cand[FLASH_HY_TUNE_MAX];
+  const int n = thread_candidates(c, cand);
+  int sel = -1;
+  for (int q = 0; q < 3; ++q)
+    if (mx_threads_of(q, c->ndim, c->nx) == t->mx_threads) sel = q;
+  if (index_of(cand, n, t->sig_threads) < 0 || index_of(cand, n, t->dir_threads) < 0 || sel < 0)
+    return fail(c, FLASH_HY_ERR_BAD_ARG, "set_tuning: %s", "not a candidate launch shape of this block shape");
+  if (t->sig_threads != c->threads || t->dir_threads != c->dir_threads || sel != c->mx_sel) {
+    CUDA_OK(c, cudaSetDevice(c->device));
+    CUDA_OK(c, cudaStreamSynchronize(c->stream));
+    drop_graphs(c);
+    c->plain_steps[0] = c->plain_steps[1] = 0;
+  }
+  c->threads = t->sig_threads;
+  c->dir_threads = t->dir_threads;
+  c->mx_sel = sel;
+  return 0;
+}
+
+extern "C" int flash_hy_autotune(flash_hy_ctx *c, double dt, int steps, flash_hy_tuning *best,
+                                 flash_hy_tuning *table, float *table_ms, int cap, int *n_trials) {
+  if (!c || !(dt > 0.0) || steps < 1 || steps > 1000 || cap < 0 || (cap > 0 && (!table || !table_ms)))
+    return FLASH_HY_ERR_BAD_ARG;
+  if (c->partial && c->n_owned == 0)
+    return fail(c, FLASH_HY_ERR_UNSUPPORTED, "a partial grid needs its owned blocks (flash_hy_set_owned_blocks)%s", "");
+  CUDA_OK(c, cudaSetDevice(c->device));
+  CUDA_OK(c, cudaStreamSynchronize(c->stream));
+  const int *step_list = c->n_owned ? c->d_owned : nullptr;
+  const int step_n = c->n_owned ? c->n_owned : c->nblocks;
+  const int cur0 = c->cur;
+  const size_t vbytes = c->ncells * sizeof(double);
+  unsigned saved_status = 0;
+  CUDA_OK(c, cudaMemcpy(&saved_status, c->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  double *keep = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = 0, nt = 0;
+  const int sig0 = c->threads, dir0 = c->dir_threads, sel0 = c->mx_sel;
+  int cand[FLASH_HY_TUNE_MAX];
+  const int ncand = thread_candidates(c, cand);
+  const bool mixed = c->p.precision == FLASH_HY_PREC_MIXED;
+  auto restore = [&]() -> cudaError_t {
+    for (int v = 0; v < 5; ++v) {
+      cudaError_t e = cudaMemcpyAsync(c->state[cur0][v], keep + (size_t)v * c->ncells, vbytes,
+                                      cudaMemcpyDeviceToDevice, c->stream);
+      if (e != cudaSuccess) return e;
+    }
+    c->cur = cur0;
+    return cudaSuccess;
+  };
+  // one trial: untimed step, then `steps` timed steps, from the kept state
+  auto trial = [&](float &ms) -> int {
+    if (restore() != cudaSuccess) return fail(c, FLASH_HY_ERR_CUDA, "autotune: %s", "state restore");
+    for (int s = 0; s <= steps; ++s) {
+      if (s == 1 && cudaEventRecord(e0, c->stream) != cudaSuccess)
+        return fail(c, FLASH_HY_ERR_CUDA, "autotune: %s", "event");
+      const int r = enqueue_step(c, dt, step_list, step_n, nullptr, true);
+      if (r) return r;
+      c->cur = 1 - c->cur;
+    }
+    if (cudaEventRecord(e1, c->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess)
+      return fail(c, FLASH_HY_ERR_CUDA, "autotune: %s", "event");
+    if (cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) return fail(c, FLASH_HY_ERR_CUDA, "autotune: %s", "event");
+    ms /= (float)steps;
+    return 0;
+  };
+  auto record = [&](float ms) {
+    if (nt < cap) {
+      table[nt].sig_threads = c->threads;
+      table[nt].dir_threads = c->dir_threads;
+      table[nt].mx_threads = mx_threads_of(c->mx_sel, c->ndim, c->nx);
+      table_ms[nt] = ms;
+    }
+    ++nt;
+  };
+  drop_graphs(c);
+  c->plain_steps[0] = c->plain_steps[1] = 0;
+  if (cudaMalloc((void **)&keep, 5 * vbytes) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(c, FLASH_HY_ERR_CUDA, "autotune: %s", "no room for the state copy");
+  }
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    rc = fail(c, FLASH_HY_ERR_CUDA, "autotune: %s", "event");
+    goto done;
+  }
+  for (int v = 0; v < 5; ++v)
+    if (cudaMemcpyAsync(keep + (size_t)v * c->ncells, c->state[cur0][v], vbytes, cudaMemcpyDeviceToDevice,
+                        c->stream) != cudaSuccess) {
+      rc = fail(c, FLASH_HY_ERR_CUDA, "autotune: %s", "state copy");
+      goto done;
+    }
+  {
+    // direction kernels first (the step's bulk), then the transverse pass
+    float best_ms = 3.4e38f;
+    int best_dir = mixed ? sel0 : dir0;
+    const int ndir = mixed ? 3 : ncand;
+    for (int q = 0; q < ndir && !rc; ++q) {
+      if (mixed) c->mx_sel = q; else c->dir_threads = cand[q];
+      float ms = 0.f;
+      rc = trial(ms);
+      if (rc) break;
+      record(ms);
+      if (ms < best_ms) { best_ms = ms; best_dir = mixed ? q : cand[q]; }
+    }
+    if (!rc) {
+      if (mixed) c->mx_sel = best_dir; else c->dir_threads = best_dir;
+      int best_sig = sig0;
+      best_ms = 3.4e38f;
+      for (int q = 0; q < ncand && !rc; ++q) {
+        c->threads = cand[q];
+        float ms = 0.f;
+        rc = trial(ms);
+        if (rc) break;
+        record(ms);
+        if (ms < best_ms) { best_ms = ms; best_sig = cand[q]; }
+      }
+      c->threads = best_sig;
+    }
+  }
+done:
+  if (keep) {
+    if (restore() != cudaSuccess && !rc) rc = fail(c, FLASH_HY_ERR_CUDA, "autotune: %s", "state restore");
+    cudaStreamSynchronize(c->stream);
+    cudaFree(keep);
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (rc) { c->threads = sig0; c->dir_threads = dir0; c->mx_sel = sel0; }
+  cudaMemcpy(c->d_status, &saved_status, sizeof(unsigned), cudaMemcpyHostToDevice);
+  c->dt_valid = 0;
+  drop_graphs(c);
+  c->plain_steps[0] = c->plain_steps[1] = 0;
+  if (n_trials) *n_trials = nt;
+  if (best) flash_hy_get_tuning(c, best);
+  return rc;
 }
 
 extern "C" int flash_hy_sync(flash_hy_ctx *c) {

@@ -13,7 +13,9 @@ struct StepArgs {
   size_t ncells;
   CflPart *part;      // per-block CFL results
   int nlaunch;        // CTAs (blocks updated)
-  int threads;        // threads per CTA
+  int threads;        // threads per CTA of the transverse-flux and CFL passes
+  int dir_threads;    // threads per CTA of the FP64 direction kernels
+  int mx_sel;         // candidate (0, 1, 2) of the mixed direction kernels' threads per CTA
   cudaStream_t stream;
   bool set_attr;      // raise the kernels' dynamic shared-memory limit (not while capturing a graph)
   // AMR (nlev > 0): k_sig over all leaves, then per direction one launch per
@@ -31,6 +33,12 @@ struct StepArgs {
 int step_fp64_exact(const StepArgs &a, int ndim, int nx, int ny, int nz);
 int step_fp64_fma(const StepArgs &a, int ndim, int nx, int ny, int nz);
 int step_mixed(const StepArgs &a, int ndim, int nx, int ny, int nz);
+int step_mixed_nt0(const StepArgs &a, int ndim, int nx, int ny, int nz);
+int step_mixed_nt1(const StepArgs &a, int ndim, int nx, int ny, int nz);
+int step_mixed_nt2(const StepArgs &a, int ndim, int nx, int ny, int nz);
+bool sig_mixed(const StepArgs &a, int ndim, int nx, int ny, int nz);
+// threads per CTA of mixed candidate `sel` for a block shape
+int mx_threads_of(int sel, int ndim, int nx);
 // CFL reduction of the stored state (one launch).
 int cfl_state(const StepArgs &a, int ndim, int nx, int ny, int nz);
 size_t sig_bytes_per_block(int ndim, int nx, int ny, int nz, int real_bytes);

@@ -107,18 +107,26 @@ struct MxGeom {
   static constexpr size_t smem_bytes() { return prim_bytes + (recon_bytes > flux_bytes ? recon_bytes : flux_bytes); }
 };
 
+// threads per CTA of k_dir_mx: three compiled candidates per block shape,
+// picked at run time (flash_hy_set_tuning / flash_hy_autotune); the middle
+// one is the default.  3D 8^3: 640 faces per direction (2 CTAs per SM by
+// shared memory); 2D 8^2: 80 faces; 2D 16^2: 288 faces.
 template <int NDIM, int NX, int NY, int NZ> struct MxThreads {
-  static constexpr int n = NDIM == 3 ? 320 : (NX == 8 ? 96 : 288);
+  static constexpr int c0 = NDIM == 3 ? 256 : (NX == 8 ? 64 : 192);
+  static constexpr int c1 = NDIM == 3 ? 320 : (NX == 8 ? 96 : 288);
+  static constexpr int c2 = NDIM == 3 ? 384 : (NX == 8 ? 128 : 320);
+  static constexpr int n = c1;
+  static constexpr int pick(int sel) { return sel == 0 ? c0 : (sel == 1 ? c1 : c2); }
 };
 
-template <int NDIM, int NX, int NY, int NZ, int DIR, bool FIRST, bool LAST, int RS>
-__global__ void __launch_bounds__(MxThreads<NDIM, NX, NY, NZ>::n, NDIM == 3 ? 2 : 1)
+template <int NDIM, int NX, int NY, int NZ, int DIR, bool FIRST, bool LAST, int RS, int NT>
+__global__ void __launch_bounds__(NT, NDIM == 3 ? 2 : 1)
 k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ ACC, double *__restrict__ AUX,
          size_t ncells, CflPart *part) {
+  static_assert(NT % 32 == 0, "threads per CTA must be a multiple of 32");
   using G = MxGeom<NDIM, NX, NY, NZ, DIR, RS>;
   using B = Box<NDIM, NX, NY, NZ>;
   constexpr int NCB = NX * NY * NZ;
-  constexpr int NT = MxThreads<NDIM, NX, NY, NZ>::n;
   constexpr int NIT = (G::SC + NT - 1) / NT;
   constexpr int v1 = Slots<DIR>::v1;
   extern __shared__ __align__(16) unsigned char smem_raw[];

@@ -1,8 +1,11 @@
 // hy_variant.cu -- instantiates the step kernels for one arithmetic variant.
-// Compiled three times (see flash5_b200/build.py):
+// Compiled once per variant (see flash5_b200/build.py):
 //   FHY_VARIANT=1  FP64, no FMA contraction (--fmad=false): the parity path
 //   FHY_VARIANT=2  FP64 with FMA contraction
-//   FHY_VARIANT=3  FP32 reconstruction / Riemann solve, FP64 update
+//   FHY_VARIANT=3  FP32 reconstruction / Riemann solve, FP64 update; compiled
+//                  once per threads-per-CTA candidate of the direction
+//                  kernels (FHY_MXSEL = 0, 1, 2), the transverse-flux pass
+//                  and the dispatcher only in unit 0
 #include "hy_launch.h"
 #include "../../include/flash_hy.h"
 #if FHY_VARIANT == 3
@@ -10,8 +13,13 @@
 #endif
 
 #if FHY_VARIANT == 3
+#ifndef FHY_MXSEL
+#define FHY_MXSEL 0
+#endif
+#define FHY_PASTE2(a, b) a##b
+#define FHY_PASTE(a, b) FHY_PASTE2(a, b)
 typedef float Real;
-#define FHY_ENTRY step_mixed
+#define FHY_ENTRY FHY_PASTE(step_mixed_nt, FHY_MXSEL)
 #elif FHY_VARIANT == 2
 typedef double Real;
 #define FHY_ENTRY step_fp64_fma
@@ -26,12 +34,13 @@ template <int NDIM, int NX, int NY, int NZ, int DIR, bool FIRST, bool LAST, int 
 static bool launch_dir_one(const StepArgs &a) {
 #if FHY_VARIANT == 3
   using G = MxGeom<NDIM, NX, NY, NZ, DIR, RS>;
-  auto kern = k_dir_mx<NDIM, NX, NY, NZ, DIR, FIRST, LAST, RS>;
-  const int threads = MxThreads<NDIM, NX, NY, NZ>::n;
+  constexpr int NT = MxThreads<NDIM, NX, NY, NZ>::pick(FHY_MXSEL);
+  auto kern = k_dir_mx<NDIM, NX, NY, NZ, DIR, FIRST, LAST, RS, NT>;
+  const int threads = NT;
 #else
   using G = DirGeom<NDIM, NX, NY, NZ, Real, DIR>;
   auto kern = k_dir<NDIM, NX, NY, NZ, Real, DIR, FIRST, LAST, FHY_VARIANT, RS>;
-  const int threads = a.threads;
+  const int threads = a.dir_threads;
 #endif
   const size_t smem = G::smem_bytes();
   if (a.set_attr && cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
@@ -56,18 +65,36 @@ static bool launch_dir(const StepArgs &a) {
   return true;
 }
 
-// RS: 0 = HLLC, 1 = exact Riemann solver
-template <int NDIM, int NX, int NY, int NZ, int RS>
-static int run_rs(const StepArgs &a) {
-  if (a.no_sig) {
-  } else if (a.nlev == 0) {
+// the transverse-flux pass (all leaves on an AMR hierarchy)
+#if FHY_VARIANT != 3 || FHY_MXSEL == 0
+template <int NDIM, int NX, int NY, int NZ>
+static bool launch_sig(const StepArgs &a) {
+  if (a.nlev == 0) {
     k_sig<NDIM, NX, NY, NZ, Real, FHY_VARIANT><<<a.nlaunch, a.threads, 0, a.stream>>>(a.P, (Real *)a.sig);
   } else {
     DevParams P = a.P;
     P.blk_list = a.leaves;
     k_sig<NDIM, NX, NY, NZ, Real, FHY_VARIANT><<<a.nleaves, a.threads, 0, a.stream>>>(P, (Real *)a.sig);
   }
-  if (cudaGetLastError() != cudaSuccess) return -2;
+  return cudaGetLastError() == cudaSuccess;
+}
+#if FHY_VARIANT == 3
+bool sig_mixed(const StepArgs &a, int ndim, int nx, int ny, int nz) {
+  if (ndim == 2 && nx == 8 && ny == 8) return launch_sig<2, 8, 8, 1>(a);
+  if (ndim == 2 && nx == 16 && ny == 16) return launch_sig<2, 16, 16, 1>(a);
+  if (ndim == 3 && nx == 8 && ny == 8 && nz == 8) return launch_sig<3, 8, 8, 8>(a);
+  return false;
+}
+#endif
+#else
+template <int NDIM, int NX, int NY, int NZ>
+static bool launch_sig(const StepArgs &a) { return sig_mixed(a, NDIM, NX, NY, NZ); }
+#endif
+
+// RS: 0 = HLLC, 1 = exact Riemann solver
+template <int NDIM, int NX, int NY, int NZ, int RS>
+static int run_rs(const StepArgs &a) {
+  if (!a.no_sig && !launch_sig<NDIM, NX, NY, NZ>(a)) return -2;
   int nl = 1;
   const int nsig = a.no_sig ? 0 : 1;
   if (a.nlev > 0) {
@@ -97,6 +124,20 @@ int FHY_ENTRY(const StepArgs &a, int ndim, int nx, int ny, int nz) {
   if (ndim == 3 && nx == 8 && ny == 8 && nz == 8) return run<3, 8, 8, 8>(a);
   return -1;
 }
+
+#if FHY_VARIANT == 3 && FHY_MXSEL == 0
+int step_mixed(const StepArgs &a, int ndim, int nx, int ny, int nz) {
+  switch (a.mx_sel) {
+    case 0: return step_mixed_nt0(a, ndim, nx, ny, nz);
+    case 2: return step_mixed_nt2(a, ndim, nx, ny, nz);
+    default: return step_mixed_nt1(a, ndim, nx, ny, nz);
+  }
+}
+int mx_threads_of(int sel, int ndim, int nx) {
+  if (ndim == 3) return MxThreads<3, 8, 8, 8>::pick(sel);
+  return nx == 8 ? MxThreads<2, 8, 8, 1>::pick(sel) : MxThreads<2, 16, 16, 1>::pick(sel);
+}
+#endif
 
 #if FHY_VARIANT == 1
 template <int NDIM, int NX, int NY, int NZ>

@@ -117,6 +117,43 @@ class Hydro:
     def sync(self):
         self._check(self.lib.flash_hy_sync(self.ctx))
 
+    # -- launch shapes ----------------------------------------------------
+    @property
+    def tuning(self):
+        """Threads per CTA of the step's kernels (dict)."""
+        t = abi.Tuning()
+        self._check(self.lib.flash_hy_get_tuning(self.ctx, C.byref(t)))
+        return t.as_dict()
+
+    @tuning.setter
+    def tuning(self, d):
+        t = abi.Tuning()
+        self._check(self.lib.flash_hy_get_tuning(self.ctx, C.byref(t)))
+        for k, v in d.items():
+            setattr(t, k, int(v))
+        self._check(self.lib.flash_hy_set_tuning(self.ctx, C.byref(t)))
+
+    def tuning_candidates(self):
+        arrs = [(C.c_int * abi.TUNE_MAX)() for _ in range(3)]
+        ns = [C.c_int() for _ in range(3)]
+        self._check(self.lib.flash_hy_tuning_candidates(self.ctx, arrs[0], C.byref(ns[0]), arrs[1], C.byref(ns[1]),
+                                                        arrs[2], C.byref(ns[2])))
+        keys = ("sig_threads", "dir_threads", "mx_threads")
+        return {k: list(a[:n.value]) for k, a, n in zip(keys, arrs, ns)}
+
+    def autotune(self, dt, steps=3):
+        """Time every candidate launch shape on this grid's state (restored
+        afterwards) and keep the fastest; returns (best, trials) with trials
+        a list of (shape, ms per step)."""
+        cap = 32
+        best = abi.Tuning()
+        table = (abi.Tuning * cap)()
+        ms = (C.c_float * cap)()
+        n = C.c_int()
+        self._check(self.lib.flash_hy_autotune(self.ctx, float(dt), int(steps), C.byref(best), table, ms, cap,
+                                               C.byref(n)))
+        return best.as_dict(), [(table[q].as_dict(), float(ms[q])) for q in range(min(n.value, cap))]
+
     # -- sharded grids ----------------------------------------------------
     def set_owned_blocks(self, blocks):
         bl = np.ascontiguousarray(blocks, dtype=np.int32)

@@ -215,6 +215,40 @@ int flash_hy_set_exchange(flash_hy_ctx *ctx, int nsend, const int *send_blocks, 
 int flash_hy_pack(flash_hy_ctx *ctx, double *d_buf);
 int flash_hy_unpack(flash_hy_ctx *ctx, const double *d_buf);
 
+/* ---- launch shapes and their autotuner ----------------------------------
+ * No FLASH5 counterpart (FLASH picks no launch shapes; its block loop is
+ * Hydro.F90:156-229).  Threads per CTA of the step's kernels: the
+ * transverse-flux and CFL passes (sig_threads), the FP64 direction kernels
+ * (dir_threads; FLASH_HY_PREC_FP64 and _FP64_FMA) and the mixed-precision
+ * direction kernels (mx_threads; FLASH_HY_PREC_MIXED, three compiled
+ * candidates per block shape).  Every face and cell is computed by one
+ * thread and the CFL reduction is order independent, so sig_threads and
+ * dir_threads leave results bit-identical; the mx_threads candidates are
+ * separately compiled FMA-contracted kernels and agree to rounding.
+ * set_tuning refuses values that are not
+ * candidates of the context's block shape (FLASH_HY_ERR_BAD_ARG);
+ * tuning_candidates lists them (arrays of FLASH_HY_TUNE_MAX entries).
+ * autotune times `steps` steps of dt, after one untimed step, for every
+ * candidate of the direction kernels and then of the transverse-flux pass
+ * (coordinate search: the two are separate launches), each trial from a
+ * copy of the current state; it restores the state, keeps the fastest
+ * shape, and writes every trial (shape, ms per step) to table / table_ms
+ * (capacity cap; *n_trials = their number).  Status bits raised by the
+ * trials are dropped; the next flash_hy_compute_dt recomputes dt from the
+ * restored state.                                                         */
+#define FLASH_HY_TUNE_MAX 8
+typedef struct {
+  int sig_threads;
+  int dir_threads;
+  int mx_threads;
+} flash_hy_tuning;
+int flash_hy_get_tuning(flash_hy_ctx *ctx, flash_hy_tuning *out);
+int flash_hy_set_tuning(flash_hy_ctx *ctx, const flash_hy_tuning *t);
+int flash_hy_tuning_candidates(flash_hy_ctx *ctx, int *sig, int *n_sig, int *dir, int *n_dir, int *mx,
+                               int *n_mx);
+int flash_hy_autotune(flash_hy_ctx *ctx, double dt, int steps, flash_hy_tuning *best, flash_hy_tuning *table,
+                      float *table_ms, int cap, int *n_trials);
+
 /* ---- CFL time step without any device allocation ------------------------
  * No counterpart in the reference: FLASH5's Hydro_computeDt runs on host
  * arrays.  This entry point is for callers that cannot call cudaMalloc
