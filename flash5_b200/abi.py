@@ -33,19 +33,34 @@ UPDATE_NONE, UPDATE_ALL = 0, 3
 
 class VarMap(C.Structure):
     _fields_ = [(n, C.c_int) for n in
-                ("dens", "eint", "ener", "gamc", "game", "pres", "temp", "velx", "vely", "velz")]
+                ("dens", "eint", "ener", "gamc", "game", "pres", "temp", "velx", "vely", "velz", "species")]
 
 
 # FLASH's alphabetical +uhd / gamma-EOS UNK ordering (1-based *_VAR).
 FLASH_UHD_VARS = ("dens", "eint", "ener", "gamc", "game", "pres", "shok", "temp", "velx", "vely", "velz")
 
 
-def flash_varmap():
+MAX_SPECIES = 16
+
+
+def flash_varmap(nsp=0):
+    """1-based *_VAR indices of FLASH's UNK; species and mass scalars (nsp of
+    them) follow the property variables (SPECIES_BEGIN = NPROP_VARS + 1)."""
     vm = VarMap()
     for i, n in enumerate(FLASH_UHD_VARS):
-        if hasattr(vm, n):
+        if hasattr(vm, n) and n != "species":
             setattr(vm, n, i + 1)
+    vm.species = len(FLASH_UHD_VARS) + 1 if nsp else 0
     return vm
+
+
+def with_species(params, grid):
+    """A copy of params carrying the grid's species / mass-scalar counts."""
+    p = Params()
+    C.memmove(C.byref(p), C.byref(params), C.sizeof(Params))
+    p.nspecies = getattr(grid, "nspecies", 0)
+    p.nmass_scalars = getattr(grid, "nmass_scalars", 0)
+    return p
 
 
 class Params(C.Structure):
@@ -58,6 +73,7 @@ class Params(C.Structure):
         ("eint_switch", C.c_double), ("smlrho", C.c_double), ("smallp", C.c_double),
         ("smalle", C.c_double), ("tiny", C.c_double), ("gamma", C.c_double),
         ("gas_constant", C.c_double), ("single_species_a", C.c_double),
+        ("nspecies", C.c_int), ("nmass_scalars", C.c_int),
     ]
 
 

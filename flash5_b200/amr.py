@@ -35,6 +35,8 @@ class AmrGrid:
     def __init__(self, ndim, nb, nblk, max_level, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), bc="outflow",
                  nguard=NGUARD):
         self.ndim = ndim
+        self.nspecies = self.nmass_scalars = 0        # species are not carried on AMR hierarchies
+        self.nunk = NUNK
         nb = tuple(nb) + (1,) * (3 - len(nb))
         nblk = tuple(nblk) + (1,) * (3 - len(nblk))
         self.nb = tuple(nb[d] if d < ndim else 1 for d in range(3))

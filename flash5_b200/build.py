@@ -28,6 +28,7 @@ UNITS = [
     ("flash_hy.o", "flash_hy.cu", ["--fmad=false"]),
     ("riemann_exact.o", "riemann_exact.cu", ["--fmad=true"]),
     ("cfl_noalloc.o", "cfl_noalloc.cu", ["--fmad=false"]),
+    ("spec.o", "spec.cu", ["--fmad=false"]),
 ]
 
 

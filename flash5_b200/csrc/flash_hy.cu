@@ -72,6 +72,12 @@ struct flash_hy_ctx {
   int *d_owned_mask;           // 1 for owned blocks (dt reduction)
   int *d_send, n_send, *d_recv, n_recv;  // blocks packed for / unpacked from other ranks
   double *d_fstore;            // stored fluxes of the split step
+  // species and mass scalars: state [2][nsp][ncells], flux-divergence
+  // accumulator, SpcSig scratch, face mass fluxes and fallback flags left
+  // by the hydro direction kernels
+  int nsp, nspec;
+  double *spec[2], *sacc, *ssig, *sp_mf;
+  unsigned char *sp_fb;
   char err[512];
 };
 
@@ -141,6 +147,14 @@ static void fill_devparams(const flash_hy_ctx *c, DevParams &P) {
   for (int v = 0; v < 5; ++v) {
     P.s_in[v] = c->state[c->cur][v];
     P.s_out[v] = c->state[1 - c->cur][v];
+  }
+  if (c->nsp > 0) {
+    P.nsp = c->nsp;
+    P.nspec = c->nspec;
+    P.sp_in = c->spec[c->cur];
+    P.sp_out = c->spec[1 - c->cur];
+    P.sp_mf = c->sp_mf;
+    P.sp_fb = c->sp_fb;
   }
   if (c->amr) {
     P.blk_level = c->d_level;
@@ -224,6 +238,10 @@ extern "C" int flash_hy_create(const flash_hy_params *params, const flash_hy_gri
       (params->riemann_solver != FLASH_HY_RS_EXACT || params->precision != FLASH_HY_PREC_MIXED))
     return FLASH_HY_ERR_UNSUPPORTED;
   if (params->gamma <= 1.0 || params->cfl <= 0.0) return FLASH_HY_ERR_BAD_ARG;
+  if (params->nspecies < 0 || params->nmass_scalars < 0 ||
+      params->nspecies + params->nmass_scalars > FLASH_HY_MAX_SPECIES)
+    return FLASH_HY_ERR_BAD_ARG;
+  if (params->nspecies + params->nmass_scalars > 0 && g->max_level > 1) return FLASH_HY_ERR_UNSUPPORTED;
   int nz = g->ndim > 2 ? g->nzb : 1, ny = g->ndim > 1 ? g->nyb : 1;
   if (!shape_supported(g->ndim, g->nxb, ny, nz)) return FLASH_HY_ERR_UNSUPPORTED;
   if (g->nblocks <= 0 || !g->block_coords || g->nguard < 0) return FLASH_HY_ERR_BAD_ARG;
@@ -283,6 +301,8 @@ extern "C" int flash_hy_create(const flash_hy_params *params, const flash_hy_gri
   c->dir_threads = c->threads;
   c->mx_sel = 1;
   c->host_ng = g->nguard;
+  c->nspec = params->nspecies;
+  c->nsp = params->nspecies + params->nmass_scalars;
   *out = c;
   int rc = 0;
 #define ALLOC(ptr, bytes)                                                           \
@@ -355,6 +375,15 @@ extern "C" int flash_hy_create(const flash_hy_params *params, const flash_hy_gri
     int rb = params->precision == FLASH_HY_PREC_MIXED ? 4 : 8;
     ALLOC(c->sig, sig_bytes_per_block(g->ndim, g->nxb, ny, nz, rb) * g->nblocks);
   }
+  if (c->nsp > 0) {
+    const size_t box = (size_t)(g->nxb + 2) * (g->ndim > 1 ? ny + 2 : 1) * (g->ndim > 2 ? nz + 2 : 1);
+    const size_t lines = (size_t)(g->nxb + 2) * (g->ndim > 1 ? ny : 1) * (g->ndim > 2 ? nz : 1);
+    for (int s = 0; s < 2; ++s) ALLOC(c->spec[s], (size_t)c->nsp * c->ncells * sizeof(double));
+    ALLOC(c->sacc, (size_t)c->nsp * c->ncells * sizeof(double));
+    ALLOC(c->ssig, (size_t)g->nblocks * g->ndim * c->nsp * box * sizeof(double));
+    ALLOC(c->sp_mf, (size_t)g->nblocks * g->ndim * lines * sizeof(double));
+    ALLOC(c->sp_fb, (size_t)g->nblocks * g->ndim * lines);
+  }
   if (!amr) ALLOC(c->d_blk_at, at.size() * sizeof(int));
   ALLOC(c->d_blk_coord, coords.size() * sizeof(int));
   ALLOC(c->d_part, g->nblocks * sizeof(CflPart));
@@ -397,6 +426,8 @@ extern "C" int flash_hy_destroy(flash_hy_ctx *c) {
   for (int l = 0; l < 17; ++l) { cudaFree(c->d_lev_leaves[l]); cudaFree(c->d_lev_parents[l]); }
   cudaFree(c->d_owned); cudaFree(c->d_owned_mask); cudaFree(c->d_send); cudaFree(c->d_recv);
   cudaFree(c->d_fstore);
+  for (int s = 0; s < 2; ++s) cudaFree(c->spec[s]);
+  cudaFree(c->sacc); cudaFree(c->ssig); cudaFree(c->sp_mf); cudaFree(c->sp_fb);
   free(c->h_blk_at);
   if (c->h_dt) cudaFreeHost(c->h_dt);
   if (c->h_status) cudaFreeHost(c->h_status);
@@ -411,6 +442,7 @@ extern "C" int flash_hy_destroy(flash_hy_ctx *c) {
 struct HostLayout {
   int layout, nunk, ng[3], nt[3];
   int v_dens, v_eint, v_ener, v_gamc, v_game, v_pres, v_temp, v_velx, v_vely, v_velz;  // 0-based, -1 absent
+  int v_spec;           // first species (0-based); species and mass scalars follow
 };
 
 __device__ __forceinline__ size_t unk_index(const HostLayout &L, int b, int i, int j, int k, int v) {
@@ -437,6 +469,7 @@ __global__ void k_unpack(const double *__restrict__ stage, HostLayout L, DevPara
     if (ener - ekin > rmax(P.smalle, P.eswitch * ekin)) eint = ener - ekin;
   }
   P.s_out[0][t] = rho; P.s_out[1][t] = vx; P.s_out[2][t] = vy; P.s_out[3][t] = vz; P.s_out[4][t] = eint;
+  for (int q = 0; q < P.nsp; ++q) P.sp_out[(size_t)q * ncells + t] = get(L.v_spec + q);
 }
 
 __global__ void k_pack(double *__restrict__ stage, HostLayout L, DevParams P, int nx, int ny, int nz, size_t ncells) {
@@ -455,6 +488,7 @@ __global__ void k_pack(double *__restrict__ stage, HostLayout L, DevParams P, in
   put(L.v_dens, rho); put(L.v_velx, vx); put(L.v_vely, vy); put(L.v_velz, vz);
   put(L.v_pres, pres); put(L.v_temp, temp); put(L.v_gamc, P.gamma); put(L.v_eint, e);
   put(L.v_ener, (P.leaf && !P.leaf[b]) ? P.pe[t] : e + ekin); put(L.v_game, pres / (e * rho) + 1);
+  for (int q = 0; q < P.nsp; ++q) put(L.v_spec + q, P.sp_in[(size_t)q * ncells + t]);
 }
 
 static int make_layout(flash_hy_ctx *c, int layout, int nunk, const flash_hy_varmap *vm, int nguard, HostLayout &L) {
@@ -473,6 +507,11 @@ static int make_layout(flash_hy_ctx *c, int layout, int nunk, const flash_hy_var
     o[q] = m[q] - 1;
   }
   if (L.v_dens < 0 || L.v_velx < 0 || (L.v_eint < 0 && L.v_ener < 0)) return FLASH_HY_ERR_BAD_ARG;
+  L.v_spec = -1;
+  if (c->nsp > 0) {
+    if (vm->species < 1 || vm->species - 1 + c->nsp > nunk) return FLASH_HY_ERR_BAD_ARG;
+    L.v_spec = vm->species - 1;
+  }
   return 0;
 }
 
@@ -496,6 +535,7 @@ extern "C" int flash_hy_upload(flash_hy_ctx *c, const double *unk, int layout, i
   DevParams P;
   fill_devparams(c, P);
   for (int v = 0; v < 5; ++v) P.s_out[v] = c->state[c->cur][v];
+  if (c->nsp > 0) P.sp_out = c->spec[c->cur];
   k_unpack<<<(unsigned)((c->ncells + 255) / 256), 256, 0, c->stream>>>((const double *)c->d_stage, L, P, c->nx, c->ny,
                                                                        c->nz, c->ncells);
   CUDA_OK(c, cudaGetLastError());
@@ -515,6 +555,7 @@ extern "C" int flash_hy_download(flash_hy_ctx *c, double *unk, int layout, int n
   // Variables we do not own (and guard cells) keep the caller's values.
   int owned = 0;
   for (int q = 0; q < 10; ++q) owned += (&L.v_dens)[q] >= 0;
+  if (L.v_spec >= 0) owned += c->nsp;
   if (!(full && owned == nunk)) CUDA_OK(c, cudaMemcpyAsync(c->d_stage, unk, bytes, cudaMemcpyHostToDevice, c->stream));
   if (c->amr && amr_restrict_all(c)) return fail(c, FLASH_HY_ERR_CUDA, "restriction launch%s", "");
   DevParams P;
@@ -616,6 +657,19 @@ static int enqueue_step(flash_hy_ctx *c, double dt, const int *d_list, int nlaun
   }
   if (n == -1) return fail(c, FLASH_HY_ERR_UNSUPPORTED, "unsupported block shape%s", "");
   if (n < 0) return fail(c, FLASH_HY_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  if (c->nsp > 0) {
+    if (fmode != 0) return fail(c, FLASH_HY_ERR_UNSUPPORTED, "species with the split step%s", "");
+    SpecArgs sa;
+    sa.P = a.P;
+    sa.ssig = c->ssig;
+    sa.sacc = c->sacc;
+    sa.ncells = c->ncells;
+    sa.nlaunch = nlaunch;
+    sa.stream = c->stream;
+    const int ns = spec_step(sa, c->ndim, c->nx, c->ny, c->nz);
+    if (ns < 0) return fail(c, FLASH_HY_ERR_CUDA, "species launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    n += ns;
+  }
   c->launches = n + pre;
   return 0;
 }
@@ -691,6 +745,9 @@ static int carry_state(flash_hy_ctx *c) {
   for (int v = 0; v < 5; ++v)
     CUDA_OK(c, cudaMemcpyAsync(c->state[1 - c->cur][v], c->state[c->cur][v], c->ncells * sizeof(double),
                                cudaMemcpyDeviceToDevice, c->stream));
+  if (c->nsp > 0)
+    CUDA_OK(c, cudaMemcpyAsync(c->spec[1 - c->cur], c->spec[c->cur], (size_t)c->nsp * c->ncells * sizeof(double),
+                               cudaMemcpyDeviceToDevice, c->stream));
   return 0;
 }
 
@@ -725,6 +782,7 @@ static int ensure_fstore(flash_hy_ctx *c) {
 }
 
 extern "C" int flash_hy_compute_fluxes(flash_hy_ctx *c, int blockCount, const int *blockList, double dt, int flags) {
+  if (c && c->nsp > 0) return fail(c, FLASH_HY_ERR_UNSUPPORTED, "species with the split step%s", "");
   if (!c || blockCount < 0 || (blockCount > 0 && !blockList)) return FLASH_HY_ERR_BAD_ARG;
   if (flags != FLASH_HY_UPDATE_NONE && flags != FLASH_HY_UPDATE_ALL) return fail(c, FLASH_HY_ERR_BAD_ARG, "flags%s", "");
   if (c->amr) return fail(c, FLASH_HY_ERR_UNSUPPORTED, "split step on an AMR hierarchy%s", "");
@@ -746,6 +804,7 @@ extern "C" int flash_hy_compute_fluxes(flash_hy_ctx *c, int blockCount, const in
 }
 
 extern "C" int flash_hy_update_solution(flash_hy_ctx *c, int blockCount, const int *blockList, double dt) {
+  if (c && c->nsp > 0) return fail(c, FLASH_HY_ERR_UNSUPPORTED, "species with the split step%s", "");
   if (!c || blockCount < 0 || (blockCount > 0 && !blockList)) return FLASH_HY_ERR_BAD_ARG;
   if (c->amr) return fail(c, FLASH_HY_ERR_UNSUPPORTED, "split step on an AMR hierarchy%s", "");
   if (!c->d_fstore) return fail(c, FLASH_HY_ERR_BAD_ARG, "no stored fluxes (flash_hy_compute_fluxes first)%s", "");
@@ -938,6 +997,7 @@ extern "C" int flash_hy_autotune(flash_hy_ctx *c, double dt, int steps, flash_hy
   const int step_n = c->n_owned ? c->n_owned : c->nblocks;
   const int cur0 = c->cur;
   const size_t vbytes = c->ncells * sizeof(double);
+  const int nkeep = 5 + c->nsp;       // state variables, then species and mass scalars
   unsigned saved_status = 0;
   CUDA_OK(c, cudaMemcpy(&saved_status, c->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost));
   double *keep = nullptr;
@@ -948,9 +1008,9 @@ extern "C" int flash_hy_autotune(flash_hy_ctx *c, double dt, int steps, flash_hy
   const int ncand = thread_candidates(c, cand);
   const bool mixed = c->p.precision == FLASH_HY_PREC_MIXED;
   auto restore = [&]() -> cudaError_t {
-    for (int v = 0; v < 5; ++v) {
-      cudaError_t e = cudaMemcpyAsync(c->state[cur0][v], keep + (size_t)v * c->ncells, vbytes,
-                                      cudaMemcpyDeviceToDevice, c->stream);
+    for (int v = 0; v < nkeep; ++v) {
+      double *dst = v < 5 ? c->state[cur0][v] : c->spec[cur0] + (size_t)(v - 5) * c->ncells;
+      cudaError_t e = cudaMemcpyAsync(dst, keep + (size_t)v * c->ncells, vbytes, cudaMemcpyDeviceToDevice, c->stream);
       if (e != cudaSuccess) return e;
     }
     c->cur = cur0;
@@ -983,7 +1043,7 @@ extern "C" int flash_hy_autotune(flash_hy_ctx *c, double dt, int steps, flash_hy
   };
   drop_graphs(c);
   c->plain_steps[0] = c->plain_steps[1] = 0;
-  if (cudaMalloc((void **)&keep, 5 * vbytes) != cudaSuccess) {
+  if (cudaMalloc((void **)&keep, nkeep * vbytes) != cudaSuccess) {
     cudaGetLastError();
     return fail(c, FLASH_HY_ERR_CUDA, "autotune: %s", "no room for the state copy");
   }
@@ -991,9 +1051,10 @@ extern "C" int flash_hy_autotune(flash_hy_ctx *c, double dt, int steps, flash_hy
     rc = fail(c, FLASH_HY_ERR_CUDA, "autotune: %s", "event");
     goto done;
   }
-  for (int v = 0; v < 5; ++v)
-    if (cudaMemcpyAsync(keep + (size_t)v * c->ncells, c->state[cur0][v], vbytes, cudaMemcpyDeviceToDevice,
-                        c->stream) != cudaSuccess) {
+  for (int v = 0; v < nkeep; ++v)
+    if (cudaMemcpyAsync(keep + (size_t)v * c->ncells,
+                        v < 5 ? c->state[cur0][v] : c->spec[cur0] + (size_t)(v - 5) * c->ncells, vbytes,
+                        cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess) {
       rc = fail(c, FLASH_HY_ERR_CUDA, "autotune: %s", "state copy");
       goto done;
     }
@@ -1195,19 +1256,31 @@ extern "C" int flash_hy_set_exchange(flash_hy_ctx *c, int nsend, const int *send
 }
 
 // buf[i][v][cell] <-> state[v][list[i] * ncb + cell], one CTA per listed block
+// one record per listed block: the 5 state variables, then the species and
+// mass scalars, ncb values each
 __global__ void k_blocks_to_buf(const double *s0, const double *s1, const double *s2, const double *s3,
-                                const double *s4, const int *list, int ncb, double *buf) {
+                                const double *s4, const double *sp, int nsp, size_t ncells, const int *list, int ncb,
+                                double *buf) {
   const double *st[5] = {s0, s1, s2, s3, s4};
   const size_t b = (size_t)list[blockIdx.x];
-  double *dst = buf + (size_t)blockIdx.x * 5 * ncb;
-  for (int t = threadIdx.x; t < 5 * ncb; t += blockDim.x) dst[t] = st[t / ncb][b * ncb + t % ncb];
+  const int nv = 5 + nsp;
+  double *dst = buf + (size_t)blockIdx.x * nv * ncb;
+  for (int t = threadIdx.x; t < nv * ncb; t += blockDim.x) {
+    const int v = t / ncb, c = t % ncb;
+    dst[t] = v < 5 ? st[v][b * ncb + c] : sp[(size_t)(v - 5) * ncells + b * ncb + c];
+  }
 }
-__global__ void k_buf_to_blocks(double *s0, double *s1, double *s2, double *s3, double *s4, const int *list, int ncb,
-                                const double *buf) {
+__global__ void k_buf_to_blocks(double *s0, double *s1, double *s2, double *s3, double *s4, double *sp, int nsp,
+                                size_t ncells, const int *list, int ncb, const double *buf) {
   double *st[5] = {s0, s1, s2, s3, s4};
   const size_t b = (size_t)list[blockIdx.x];
-  const double *src = buf + (size_t)blockIdx.x * 5 * ncb;
-  for (int t = threadIdx.x; t < 5 * ncb; t += blockDim.x) st[t / ncb][b * ncb + t % ncb] = src[t];
+  const int nv = 5 + nsp;
+  const double *src = buf + (size_t)blockIdx.x * nv * ncb;
+  for (int t = threadIdx.x; t < nv * ncb; t += blockDim.x) {
+    const int v = t / ncb, c = t % ncb;
+    if (v < 5) st[v][b * ncb + c] = src[t];
+    else sp[(size_t)(v - 5) * ncells + b * ncb + c] = src[t];
+  }
 }
 
 extern "C" int flash_hy_pack(flash_hy_ctx *c, double *d_buf) {
@@ -1215,7 +1288,8 @@ extern "C" int flash_hy_pack(flash_hy_ctx *c, double *d_buf) {
   if (!c->n_send) return 0;
   CUDA_OK(c, cudaSetDevice(c->device));
   double *const *st = c->state[c->cur];
-  k_blocks_to_buf<<<c->n_send, 256, 0, c->stream>>>(st[0], st[1], st[2], st[3], st[4], c->d_send, (int)c->ncb, d_buf);
+  k_blocks_to_buf<<<c->n_send, 256, 0, c->stream>>>(st[0], st[1], st[2], st[3], st[4], c->spec[c->cur], c->nsp,
+                                                    c->ncells, c->d_send, (int)c->ncb, d_buf);
   CUDA_OK(c, cudaGetLastError());
   return 0;
 }
@@ -1225,7 +1299,8 @@ extern "C" int flash_hy_unpack(flash_hy_ctx *c, const double *d_buf) {
   if (!c->n_recv) return 0;
   CUDA_OK(c, cudaSetDevice(c->device));
   double *const *st = c->state[c->cur];
-  k_buf_to_blocks<<<c->n_recv, 256, 0, c->stream>>>(st[0], st[1], st[2], st[3], st[4], c->d_recv, (int)c->ncb, d_buf);
+  k_buf_to_blocks<<<c->n_recv, 256, 0, c->stream>>>(st[0], st[1], st[2], st[3], st[4], c->spec[c->cur], c->nsp,
+                                                    c->ncells, c->d_recv, (int)c->ncb, d_buf);
   CUDA_OK(c, cudaGetLastError());
   c->dt_valid = 0;
   return 0;

@@ -66,6 +66,16 @@ struct DevParams {
   // only, 3 = update from the stored fluxes
   int fmode;
   double *fstore;             // [block][ndim][8 x faces (FLASH flx order) + n+1/2 pressure sum per cell]
+  // species and mass scalars (nsp > 0; the first nspec are renormalised):
+  // [nsp][ncells] block-major SoA interiors, double-buffered like s_in/s_out.
+  // The hydro direction kernels leave for them, per launch slot and
+  // direction in the line-cell order of DirGeom, the face mass flux
+  // (sp_mf) and whether the 3D CTU stage fell back to first order (sp_fb).
+  int nsp, nspec;
+  const double *sp_in;
+  double *sp_out;
+  double *sp_mf;
+  unsigned char *sp_fb;
 };
 
 // Cell sizes of block b: level-1 deltas scaled by 2^(1-level) (exact).

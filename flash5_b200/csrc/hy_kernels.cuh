@@ -401,8 +401,18 @@ struct DirGeom {
     k = NDIM > 2 ? t / (rx * ry) - (DIR == 3) : 0;
   }
   __device__ static __forceinline__ int along(int i, int j, int k) { return DIR == 1 ? i : (DIR == 2 ? j : k); }
+  // line-cell index of cell (i, j, k), the inverse of decode
+  __device__ static __forceinline__ int idx(int i, int j, int k) {
+    return ((k + (DIR == 3)) * ry + (j + (DIR == 2))) * rx + (i + (DIR == 1));
+  }
   static constexpr size_t smem_bytes() { return (size_t)n * (14 + NFLX) * sizeof(R); }
 };
+// per-slot offset of a direction's line cells in sp_mf / sp_fb
+template <int NDIM, int NX, int NY, int NZ, int DIR>
+__device__ __forceinline__ size_t sp_line_base(int slot) {
+  using L = DirGeom<NDIM, NX, NY, NZ, double, DIR>;
+  return ((size_t)slot * NDIM + (DIR - 1)) * L::n;
+}
 
 // slots stored for the face states: dens, velx, vely, velz, pres, game, eint
 __device__ __forceinline__ int wslot(int q) { return q < 5 ? q : q + 1; }
@@ -520,10 +530,12 @@ __global__ void __launch_bounds__(320) k_dir(const DevParams P, const R *__restr
         Wp[n] = Wp[n] + (T1[n] + T2[n]) * fac;
         Wm[n] = Wm[n] + (T1[n] + T2[n]) * fac;
       }
-      if (Wp[HD] <= R(0) || Wm[HD] <= R(0) || Wp[HP] <= R(0) || Wm[HP] <= R(0)) {
+      const bool fb = Wp[HD] <= R(0) || Wm[HD] <= R(0) || Wp[HP] <= R(0) || Wm[HP] <= R(0);
+      if (fb) {
 #pragma unroll
         for (int n = 0; n < 8; ++n) { Wm[n] = Vc[n]; Wp[n] = Vc[n]; }
       }
+      if (P.sp_fb) P.sp_fb[sp_line_base<NDIM, NX, NY, NZ, DIR>(blockIdx.x) + t] = fb;
     }
 #pragma unroll
     for (int q = 0; q < 7; ++q) {
@@ -558,6 +570,7 @@ __global__ void __launch_bounds__(320) k_dir(const DevParams P, const R *__restr
     }
     sF[FEINT * G::n + t] = fe;
     sF[FVOLU * G::n + t] = fv;
+    if (P.sp_mf) P.sp_mf[sp_line_base<NDIM, NX, NY, NZ, DIR>(blockIdx.x) + t] = double(F[FDENS]);
   }
   __syncthreads();
   if constexpr (sizeof(R) == 8) {

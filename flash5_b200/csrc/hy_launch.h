@@ -28,6 +28,18 @@ struct StepArgs {
   int lev_count[17];
 };
 
+// the species / mass-scalar pass after the hydro direction kernels
+struct SpecArgs {
+  DevParams P;        // the step's parameters (species buffers, mass fluxes, flags)
+  double *ssig;       // SpcSig scratch, [nlaunch][ndim][nsp][box]
+  double *sacc;       // [nsp][ncells] flux-divergence accumulator
+  size_t ncells;
+  int nlaunch;
+  cudaStream_t stream;
+};
+// launches k_spec_sig + one k_spec_dir per direction; returns their number or -2
+int spec_step(const SpecArgs &a, int ndim, int nx, int ny, int nz);
+
 // Enqueue one hydro step; returns the number of kernel launches, or -1 for an
 // unsupported block shape, or -2 for a launch error.
 int step_fp64_exact(const StepArgs &a, int ndim, int nx, int ny, int nz);

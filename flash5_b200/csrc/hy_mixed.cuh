@@ -358,10 +358,13 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
         dWp[n] += c;
         dWm[n] += c;
       }
-      if (rc + dWp[HD] <= 0. || rc + dWm[HD] <= 0. || pc + dWp[HP] <= 0. || pc + dWm[HP] <= 0.) {
+      const bool fb = rc + dWp[HD] <= 0. || rc + dWm[HD] <= 0. || pc + dWp[HP] <= 0. || pc + dWm[HP] <= 0.;
+      if (fb) {
 #pragma unroll
         for (int n = 0; n < 8; ++n) { dWm[n] = 0.f; dWp[n] = 0.f; }
       }
+      if (P.sp_fb)
+        P.sp_fb[sp_line_base<NDIM, NX, NY, NZ, DIR>(blockIdx.x) + DirGeom<NDIM, NX, NY, NZ, double, DIR>::idx(i, j, k)] = fb;
     }
 #pragma unroll
     for (int qq = 0; qq < 6; ++qq) {
@@ -545,6 +548,16 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
       return G::at(along, t1 + (DIR == 1 ? NY : NX) * t2, G::LC, 1);
     });
     __syncthreads();
+  }
+  if (P.sp_mf) {        // face mass fluxes for the species pass
+    for (int t = threadIdx.x; t < G::SC; t += NT) {
+      int x, l, i, j, k;
+      G::dec(t, G::LC, 1, x, l);
+      if (x < 0) continue;
+      G::cell(x, l, i, j, k);
+      P.sp_mf[sp_line_base<NDIM, NX, NY, NZ, DIR>(blockIdx.x) + DirGeom<NDIM, NX, NY, NZ, double, DIR>::idx(i, j, k)] =
+          sF[FDENS * G::SC + t];
+    }
   }
 
   } else {

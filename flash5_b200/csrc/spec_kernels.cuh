@@ -1,0 +1,256 @@
+// spec_kernels.cuh -- species and mass scalars of one unsplit hydro step,
+// FLASH5's hy_fullSpecMsFluxHandling path (the default, unsplit/Config:
+// 140-143).  They are passive: they read the hydro's face mass fluxes, the
+// old cell velocities and flattening, the new density and, in 3D with the
+// full CTU, where the hydro fell back to first order, and feed nothing back.
+// So they run after the hydro direction kernels, in FP64 for every
+// precision variant, compiled without FMA contraction in the expression
+// order of the CPU oracle (bit-identical to it on the FP64 hydro path).
+//
+//   k_spec_sig   SpcSig of every box cell and direction: the entropy-wave
+//                speed (the cell's normal velocity) times the upwind
+//                difference (hy_DataReconstructNormalDir_PPM.F90:360-369,
+//                hy_upwindTransverseFlux.F90:197-205 with speciesScalar)
+//   k_spec_dir   per direction: PPM face values of the line cells
+//                (hy_DataReconstructNormalDir_PPM.F90:289-301, 584-628),
+//                transverse corrections (hy_dataReconstOneStep.F90:996-1014),
+//                3D CTU cross terms or the first-order fallback
+//                (hy_getRiemannState.F90:1053-1090 and y/z analogues,
+//                fallbackToFirstOrder :1456-1475), upwind fluxes
+//                F_dens * X (hy_getFaceFlux.F90:453-467) and the flux
+//                divergence; the last direction updates
+//                X = (X rho_old + dt sum (F_L - F_R)/dx) / rho_new
+//                (updateSpeciesMassScalar, hy_unsplitUpdate.F90:1300-1318)
+//                and renormalises the species (:850-859).
+#pragma once
+#include "hy_kernels.cuh"
+
+namespace fhy {
+
+// mass fraction q of the cell providing local cell (li, lj, lk) of block b
+// (guard cells as Grid_fillGuardCells: periodic, zero gradient, mirrored
+// without sign change)
+template <int NDIM, int NX, int NY, int NZ>
+__device__ __forceinline__ double load_spec(const DevParams &P, int b, int3 bc, int li, int lj, int lk, int q,
+                                            size_t ncells) {
+  bool inside; int fx, fy, fz;
+  const size_t o = cell_src<NDIM, NX, NY, NZ>(P, b, bc, li, lj, lk, inside, fx, fy, fz);
+  return __ldg(P.sp_in + (size_t)q * ncells + o);
+}
+
+// velocity component d (0-based) of a cell, mirrored in reflecting guard cells
+template <int NDIM, int NX, int NY, int NZ>
+__device__ __forceinline__ double load_vel(const DevParams &P, int b, int3 bc, int li, int lj, int lk, int d) {
+  bool inside; int f[3];
+  const size_t o = cell_src<NDIM, NX, NY, NZ>(P, b, bc, li, lj, lk, inside, f[0], f[1], f[2]);
+  const double v = __ldg(P.s_in[1 + d] + o);
+  return f[d] ? -v : v;
+}
+
+// min / max as the CPU oracle takes them (a < b ? a : b), so that signed
+// zeros come out the same
+__device__ __forceinline__ double minmod_s(double a, double b) {     // hy_slopeLimiters.F90:56-60
+  return .5 * (copysign(1., a) + copysign(1., b)) * rmin(fabs(a), fabs(b));
+}
+
+template <int NDIM, int NX, int NY, int NZ>
+__global__ void __launch_bounds__(256) k_spec_sig(const DevParams P, double *__restrict__ SSIG, size_t ncells) {
+  using B = Box<NDIM, NX, NY, NZ>;
+  const int b = P.blk_list ? P.blk_list[blockIdx.x] : blockIdx.x;
+  const int3 bc = blk_coords(P, b);
+  for (int c = threadIdx.x; c < B::n; c += blockDim.x) {
+    const int i = c % B::bx - 1, j = NDIM > 1 ? (c / B::bx) % B::by - 1 : 0;
+    const int k = NDIM > 2 ? c / (B::bx * B::by) - 1 : 0;
+#pragma unroll
+    for (int d = 0; d < NDIM; ++d) {
+      const int di = d == 0, dj = d == 1, dk = d == 2;
+      const double lam = load_vel<NDIM, NX, NY, NZ>(P, b, bc, i, j, k, d);
+      for (int q = 0; q < P.nsp; ++q) {
+        const double sm = load_spec<NDIM, NX, NY, NZ>(P, b, bc, i - di, j - dj, k - dk, q, ncells);
+        const double s0 = load_spec<NDIM, NX, NY, NZ>(P, b, bc, i, j, k, q, ncells);
+        const double sp = load_spec<NDIM, NX, NY, NZ>(P, b, bc, i + di, j + dj, k + dk, q, ncells);
+        double g;
+        if (lam > 0.) g = s0 - sm;
+        else g = sp - s0;
+        SSIG[(((size_t)blockIdx.x * NDIM + d) * P.nsp + q) * B::n + c] = lam * g;
+      }
+    }
+  }
+}
+
+template <int NDIM, int NX, int NY, int NZ, int DIR>
+struct SpecGeom {
+  using L = DirGeom<NDIM, NX, NY, NZ, double, DIR>;
+  // shared memory: per line cell the face values of one species (left,
+  // right), the normal velocity, the flattening coefficient, the velocities
+  // along the two CTU axes and the fallback flag
+  static constexpr size_t smem_bytes() { return (size_t)L::n * (6 * sizeof(double) + 1); }
+};
+
+template <int NDIM, int NX, int NY, int NZ, int DIR, bool FIRST, bool LAST>
+__global__ void __launch_bounds__(256) k_spec_dir(const DevParams P, const double *__restrict__ SSIG,
+                                                  double *__restrict__ SACC, size_t ncells) {
+  using L = DirGeom<NDIM, NX, NY, NZ, double, DIR>;
+  using B = Box<NDIM, NX, NY, NZ>;
+  constexpr int NCB = NX * NY * NZ;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double *sSl = reinterpret_cast<double *>(smem_raw);
+  double *sSr = sSl + L::n;
+  double *sU = sSr + L::n;            // normal velocity (lambda of the entropy wave)
+  double *sFl = sU + L::n;            // flattening coefficient
+  double *sA1 = sFl + L::n;           // velocities along the CTU axes A1, A2
+  double *sA2 = sA1 + L::n;
+  unsigned char *sFb = reinterpret_cast<unsigned char *>(sA2 + L::n);
+  const int b = P.blk_list ? P.blk_list[blockIdx.x] : blockIdx.x;
+  const int3 bc = blk_coords(P, b);
+  const double dt = P.dt_dev ? *P.dt_dev : P.dt;
+  const double *del = P.del;
+  const double delta = del[DIR - 1];
+  const double hdtx = 0.5 * dt / del[0], hdty = 0.5 * dt / del[1], hdtz = 0.5 * dt / del[2];
+  constexpr int A1 = DIR == 1 ? 2 : (DIR == 2 ? 3 : 1), S1 = DIR == 1 ? 3 : (DIR == 2 ? 1 : 2);
+  constexpr int A2 = DIR == 1 ? 3 : (DIR == 2 ? 1 : 2), S2 = DIR == 1 ? 2 : (DIR == 2 ? 3 : 1);
+  const bool ctu = NDIM == 3 && P.use_ctu;
+  const size_t lb = sp_line_base<NDIM, NX, NY, NZ, DIR>(blockIdx.x);
+  const double *ssb = SSIG + (size_t)blockIdx.x * NDIM * P.nsp * B::n;
+
+  // ---- per line cell quantities shared by every species
+  for (int t = threadIdx.x; t < L::n; t += blockDim.x) {
+    int i, j, k;
+    L::decode(t, i, j, k);
+    const int di = DIR == 1, dj = DIR == 2, dk = DIR == 3;
+    sU[t] = load_vel<NDIM, NX, NY, NZ>(P, b, bc, i, j, k, DIR - 1);
+    double flat = 0.;
+    if (P.use_flattening) {
+      double p7[7], u7[7], V[8];
+#pragma unroll
+      for (int s = -3; s <= 3; ++s) {
+        if (s == -3 || s == 3) {
+          p7[s + 3] = load_pres<NDIM, NX, NY, NZ>(P, b, bc, i + s * di, j + s * dj, k + s * dk);
+          u7[s + 3] = 0.;
+        } else {
+          load_prim<NDIM, NX, NY, NZ, false>(P, b, bc, i + s * di, j + s * dj, k + s * dk, V);
+          p7[s + 3] = V[HP];
+          u7[s + 3] = V[Slots<DIR>::v1];
+        }
+      }
+      flat = flat_coeff(p7, u7);
+    }
+    sFl[t] = flat;
+    if (ctu) {
+      sA1[t] = load_vel<NDIM, NX, NY, NZ>(P, b, bc, i, j, k, A1 - 1);
+      sA2[t] = load_vel<NDIM, NX, NY, NZ>(P, b, bc, i, j, k, A2 - 1);
+      sFb[t] = P.sp_fb[lb + t];
+    }
+  }
+  __syncthreads();
+
+  const double dtn = dt / delta, hdtn = 0.5 * dtn;
+  const double fac = dt * dt / (6. * (DIR == 1 ? del[1] : (DIR == 2 ? del[2] : del[0])) *
+                                (DIR == 1 ? del[2] : (DIR == 2 ? del[0] : del[1])));
+  for (int q = 0; q < P.nsp; ++q) {
+    const double *sig = ssb + (size_t)q * B::n;           // + d * nsp * B::n for direction d
+    const size_t dstr = (size_t)P.nsp * B::n;
+    // ---- face values of the line cells
+    for (int t = threadIdx.x; t < L::n; t += blockDim.x) {
+      int i, j, k;
+      L::decode(t, i, j, k);
+      const int di = DIR == 1, dj = DIR == 2, dk = DIR == 3;
+      double S[5];
+#pragma unroll
+      for (int s = -2; s <= 2; ++s)
+        S[s + 2] = load_spec<NDIM, NX, NY, NZ>(P, b, bc, i + s * di, j + s * dj, k + s * dk, q, ncells);
+      const double Smm = S[0], Sm = S[1], Sc = S[2], Sp = S[3], Spp = S[4];
+      const double lam = sU[t];
+      double dP = minmod_s(Sp - Sc, Spp - Sp);
+      double d0 = minmod_s(Sc - Sm, Sp - Sc);
+      double dN = minmod_s(Sm - Smm, Sc - Sm);
+      double l = 0.5 * (Sc + Sm) - (d0 - dN) / 6.;
+      double r = 0.5 * (Sc + Sp) - (dP - d0) / 6.;
+      l = rmax(rmin(Sc, Sm), rmin(rmax(Sc, Sm), l));
+      r = rmax(rmin(Sc, Sp), rmin(rmax(Sc, Sp), r));
+      if ((r - Sc) * (Sc - l) <= 0.) { r = Sc; l = Sc; }
+      if (6. * (r - l) * (Sc - 0.5 * (r + l)) > (r - l) * (r - l)) l = 3. * Sc - 2. * r;
+      if (6. * (r - l) * (Sc - 0.5 * (r + l)) < -((r - l) * (r - l))) r = 3. * Sc - 2. * l;
+      d0 = r - l;
+      const double s6 = 6. * (Sc - 0.5 * (r + l));
+      const double lm = rmin(lam, 0.), lp = rmax(lam, 0.);
+      l = l - lm * hdtn * (d0 + (1. + lm * 4. / 3. * hdtn) * s6);
+      r = r - lp * hdtn * (d0 - (1. - lp * 4. / 3. * hdtn) * s6);
+      if (P.use_flattening) {
+        const double f = sFl[t];
+        l = f * Sc + (1.0 - f) * l;
+        r = f * Sc + (1.0 - f) * r;
+      }
+      // transverse corrections with SpcSig of the other directions
+      const int bi = B::idx(i, j, k);
+      if (NDIM == 2) {
+        if (DIR == 1) { const double g = sig[1 * dstr + bi]; l = l - hdty * g; r = r - hdty * g; }
+        else          { const double g = sig[0 * dstr + bi]; l = l - hdtx * g; r = r - hdtx * g; }
+      } else if (NDIM == 3) {
+        const double gx = sig[0 * dstr + bi], gy = sig[1 * dstr + bi], gz = sig[2 * dstr + bi];
+        if (DIR == 1)      { l = l - hdty * gy; r = r - hdty * gy; l = l - hdtz * gz; r = r - hdtz * gz; }
+        else if (DIR == 2) { l = l - hdtx * gx; r = r - hdtx * gx; l = l - hdtz * gz; r = r - hdtz * gz; }
+        else               { l = l - hdtx * gx - hdty * gy; r = r - hdtx * gx - hdty * gy; }
+      }
+      if (ctu) {
+        if (sFb[t]) {
+          l = Sc;
+          r = Sc;
+        } else {
+          double T[2];
+#pragma unroll
+          for (int u = 0; u < 2; ++u) {
+            const int ax = u ? A2 : A1, sd = u ? S2 : S1;
+            const double lamA = u ? sA2[t] : sA1[t];
+            const double *sg = sig + (size_t)(sd - 1) * dstr;
+            const double gm = sg[B::idx(i - (ax == 1), j - (ax == 2), k - (ax == 3))];
+            const double g0 = sg[bi];
+            const double gp = sg[B::idx(i + (ax == 1), j + (ax == 2), k + (ax == 3))];
+            const double g = lamA > 0. ? g0 - gm : gp - g0;
+            T[u] = lamA * g;
+          }
+          r = r + (T[0] + T[1]) * fac;
+          l = l + (T[0] + T[1]) * fac;
+        }
+      }
+      sSl[t] = l;
+      sSr[t] = r;
+    }
+    __syncthreads();
+    // ---- upwind fluxes at both faces of every interior cell, divergence
+    for (int t = threadIdx.x; t < L::n; t += blockDim.x) {
+      int i, j, k;
+      L::decode(t, i, j, k);
+      const int a = L::along(i, j, k);
+      if (a < 0 || a >= L::nd) continue;
+      const size_t off = (size_t)b * NCB + (size_t)((k * NY + j) * NX + i);
+      const int tr = t + L::stride;
+      const double mL = P.sp_mf[lb + t], mR = P.sp_mf[lb + tr];
+      double FL, FR;
+      if (mL < 0.) FL = mL * sSl[t];
+      else FL = mL * sSr[t - L::stride];
+      if (mR < 0.) FR = mR * sSl[tr];
+      else FR = mR * sSr[t];
+      double acc = (FL - FR) / delta;
+      if (!FIRST) acc = SACC[(size_t)q * ncells + off] + acc;
+      if (!LAST) {
+        SACC[(size_t)q * ncells + off] = acc;
+      } else {
+        const double X = P.sp_in[(size_t)q * ncells + off];
+        P.sp_out[(size_t)q * ncells + off] = (X * P.s_in[0][off] + dt * acc) / P.s_out[0][off];
+      }
+    }
+    __syncthreads();
+  }
+  // ---- species (not mass scalars) renormalised to a unit sum
+  if (LAST && P.nspec > 0) {
+    for (int c = threadIdx.x; c < NCB; c += blockDim.x) {
+      const size_t off = (size_t)b * NCB + c;
+      double sum = 0.;
+      for (int q = 0; q < P.nspec; ++q) sum = sum + P.sp_out[(size_t)q * ncells + off];
+      for (int q = 0; q < P.nspec; ++q) P.sp_out[(size_t)q * ncells + off] = P.sp_out[(size_t)q * ncells + off] / sum;
+    }
+  }
+}
+
+}  // namespace fhy

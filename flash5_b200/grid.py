@@ -5,7 +5,9 @@ with FLASH's NGUARD = 4 guard layers in the host UNK array
 (unsplit/Config:209-211).  Host UNK uses the default FLASH ordering
 unk(var, i, j, k, blk) with variables in the alphabetical +uhd/gamma-EOS
 order (bin/unitCfg.py:713-714), i.e. a C array of shape
-(nblocks, nzt, nyt, nxt, NUNK).
+(nblocks, nzt, nyt, nxt, nunk), nunk = NUNK + species + mass scalars (the
+species and mass scalars follow the property variables, as SPECIES_BEGIN ..
+MASS_SCALARS_END in Flash.h).
 """
 import ctypes as C
 import numpy as np
@@ -19,8 +21,10 @@ VAR = {n: i for i, n in enumerate(abi.FLASH_UHD_VARS)}
 
 class UniformGrid:
     def __init__(self, ndim, nb, nblk, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), bc="outflow", order="lex",
-                 nguard=NGUARD):
+                 nguard=NGUARD, nspecies=0, nmass_scalars=0):
         self.ndim = ndim
+        self.nspecies, self.nmass_scalars = int(nspecies), int(nmass_scalars)
+        self.nunk = NUNK + self.nspecies + self.nmass_scalars
         nb = tuple(nb) + (1,) * (3 - len(nb))
         nblk = tuple(nblk) + (1,) * (3 - len(nblk))
         self.nb = tuple(nb[d] if d < ndim else 1 for d in range(3))
@@ -73,7 +77,12 @@ class UniformGrid:
         return g
 
     def new_unk(self):
-        return np.zeros((self.nblocks, self.nt[2], self.nt[1], self.nt[0], NUNK), dtype=np.float64)
+        return np.zeros((self.nblocks, self.nt[2], self.nt[1], self.nt[0], self.nunk), dtype=np.float64)
+
+    @property
+    def species(self):
+        """UNK slice of the species and mass scalars."""
+        return slice(NUNK, self.nunk)
 
     def interior(self, unk):
         g = self.ng

@@ -27,6 +27,7 @@ class Hydro:
     def __init__(self, params, grid, device=0):
         self.lib = abi.load_library()
         self.device = device
+        params = abi.with_species(params, grid)
         self.params = params
         self.grid = grid
         self._gdesc = grid.desc()
@@ -38,7 +39,7 @@ class Hydro:
                 self.lib.flash_hy_destroy(self.ctx)
                 self.ctx = C.c_void_p()
             raise HydroError(st, msg)
-        self.varmap = abi.flash_varmap()
+        self.varmap = abi.flash_varmap(params.nspecies + params.nmass_scalars)
 
     # -- lifecycle -------------------------------------------------------
     def close(self):

@@ -139,3 +139,30 @@ def uniform(grid, rho=1.0, v=(0.0, 0.0, 0.0), p=1.0, gamma=1.4):
     shape = (grid.nblocks, grid.nb[2], grid.nb[1], grid.nb[0])
     f = lambda a: np.full(shape, a, dtype=np.float64)
     return _fill(grid, unk, f(rho), f(v[0]), f(v[1]), f(v[2]), f(p), gamma)
+
+
+def add_species(grid, unk, width=0.05):
+    """Fill the species and mass scalars of a grid's UNK (grid.nspecies,
+    grid.nmass_scalars): species 0 is 1 inside the band |y - 0.5| < 0.25
+    (smoothed over `width`, the dense layer of the Kelvin-Helmholtz setup),
+    further species share the rest in fixed proportions so that the species
+    sum to 1; mass scalar m is a smooth passive tracer
+    0.5 + 0.4 sin(2 pi (m + 1) x) cos(2 pi y).  Synthetic: FLASH5's
+    Simulation units define their own species."""
+    ns, nm = grid.nspecies, grid.nmass_scalars
+    if ns + nm == 0:
+        return unk
+    it = grid.interior(unk)
+    x, y, z = grid.cell_centers()
+    band = 0.5 * (np.tanh((0.25 - np.abs(y - 0.5)) / width) + 1.0)
+    base = grid.species.start
+    if ns:
+        it[..., base] = band if ns > 1 else 1.0
+        rest = 1.0 - band
+        w = np.arange(1, ns, dtype=np.float64)
+        w = w / w.sum() if ns > 1 else w
+        for s in range(1, ns):
+            it[..., base + s] = rest * w[s - 1]
+    for m in range(nm):
+        it[..., base + ns + m] = 0.5 + 0.4 * np.sin(2 * np.pi * (m + 1) * x) * np.cos(2 * np.pi * y)
+    return unk

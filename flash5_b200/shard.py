@@ -34,8 +34,10 @@ class LocalGrid(UniformGrid):
     """A rank's share of a uniform grid: owned blocks first, then ghosts,
     with global block coordinates and the global block extents."""
 
-    def __init__(self, ndim, nb, nblk, coords, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), bc="outflow", nguard=4):
-        super().__init__(ndim, nb, nblk, lo=lo, hi=hi, bc=bc, nguard=nguard)
+    def __init__(self, ndim, nb, nblk, coords, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), bc="outflow", nguard=4,
+                 nspecies=0, nmass_scalars=0):
+        super().__init__(ndim, nb, nblk, lo=lo, hi=hi, bc=bc, nguard=nguard, nspecies=nspecies,
+                         nmass_scalars=nmass_scalars)
         self.coords = np.ascontiguousarray(np.asarray(coords, dtype=np.int32).reshape(-1, 3))
         self.nblocks = len(self.coords)
         self.levels = np.ones(self.nblocks, dtype=np.int32)
@@ -110,7 +112,7 @@ class ShardPlan:
     def local_grid(self):
         gr = self.grid
         return LocalGrid(gr.ndim, gr.nb[:gr.ndim], gr.nblk[:gr.ndim], gr.coords[self.local], lo=gr.lo, hi=gr.hi,
-                         bc=gr.bc, nguard=gr.nguard)
+                         bc=gr.bc, nguard=gr.nguard, nspecies=gr.nspecies, nmass_scalars=gr.nmass_scalars)
 
     def owned_of(self, r):
         """Global ids owned by rank r, in its local (Morton) order."""
@@ -120,7 +122,7 @@ class ShardPlan:
         """The owned blocks alone (for reductions over owned blocks)."""
         gr = self.grid
         return LocalGrid(gr.ndim, gr.nb[:gr.ndim], gr.nblk[:gr.ndim], gr.coords[self.owned], lo=gr.lo, hi=gr.hi,
-                         bc=gr.bc, nguard=gr.nguard)
+                         bc=gr.bc, nguard=gr.nguard, nspecies=gr.nspecies, nmass_scalars=gr.nmass_scalars)
 
     def owned_local(self):
         return np.arange(len(self.owned), dtype=np.int32)
@@ -156,7 +158,7 @@ class ShardedHydro:
         self.h.set_owned_blocks(self.plan.owned_local())
         send, recv = self.plan.send_local(), self.plan.recv_local()
         self.h.set_exchange(send, recv)
-        per = 5 * grid.nb[0] * grid.nb[1] * grid.nb[2]
+        per = (5 + grid.nspecies + grid.nmass_scalars) * grid.nb[0] * grid.nb[1] * grid.nb[2]
         dev = torch.device("cuda", device)
         self.sbuf = torch.empty(max(1, len(send)) * per, dtype=torch.float64, device=dev)
         self.rbuf = torch.empty(max(1, len(recv)) * per, dtype=torch.float64, device=dev)

@@ -70,6 +70,9 @@ extern "C" {
  * SHOK=7 TEMP=8 VELX=9 VELY=10 VELZ=11.  0 = variable absent.           */
 typedef struct flash_hy_varmap {
   int dens, eint, ener, gamc, game, pres, temp, velx, vely, velz;
+  int species;   /* first species (SPECIES_BEGIN); the nspecies species and
+                    the nmass_scalars mass scalars are consecutive from it
+                    (SPECIES_BEGIN .. MASS_SCALARS_END); 0 when there are none */
 } flash_hy_varmap;
 
 /* ---- runtime parameters (names follow unsplit/Config:105-159) ---------- */
@@ -92,7 +95,16 @@ typedef struct flash_hy_params {
   double gamma;            /* eos_gamma                                   */
   double gas_constant;     /* eos_gasConstant (PhysicalConstants "ideal gas constant") */
   double single_species_a; /* eos_singleSpeciesA                          */
+  /* species and mass scalars advected with hy_fullSpecMsFluxHandling
+   * (the default, unsplit/Config:140-143): PPM face values, upwind fluxes
+   * F_dens * X, the conservative update and, for species only, the
+   * renormalisation to a unit sum (hy_unsplitUpdate.F90:827-859).  At most
+   * FLASH_HY_MAX_SPECIES in all.  Uniform grids only (AMR hierarchies and
+   * the split step refuse them: FLASH_HY_ERR_UNSUPPORTED). */
+  int nspecies;            /* NSPECIES                                     */
+  int nmass_scalars;       /* NMASS_SCALARS                                */
 } flash_hy_params;
+#define FLASH_HY_MAX_SPECIES 16
 
 /* ---- grid descriptor ---------------------------------------------------
  * Blocks of nxb x nyb x nzb interior cells.  FLASH keeps NGUARD=4 guard
@@ -206,7 +218,8 @@ int flash_hy_harvest_fetch(flash_hy_ctx *ctx, double *d_states, long long n_max,
  * indices; every block an owned block reads guard cells from must be
  * present); set_exchange names the local blocks packed for other ranks and
  * those unpacked from them; pack / unpack copy the 5 state variables of
- * those blocks (nblocks x 5 x nxb*nyb*nzb doubles, DEVICE buffers) on the
+ * those blocks (nblocks x (5 + nspecies + nmass_scalars) x nxb*nyb*nzb
+ * doubles: the state variables, then the species; DEVICE buffers) on the
  * context's stream.  Ghost blocks are not advanced: unpack fresh copies
  * before every step.                                                     */
 int flash_hy_set_owned_blocks(flash_hy_ctx *ctx, int n, const int *blocks);

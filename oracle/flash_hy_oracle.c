@@ -35,7 +35,11 @@
 
 /* ---- UNK variables, 0-based (DENS_VAR=1 ... VELZ_VAR=11 in Flash.h) ---- */
 enum { DENS_V = 0, EINT_V, ENER_V, GAMC_V, GAME_V, PRES_V, SHOK_V, TEMP_V,
-       VELX_V, VELY_V, VELZ_V, NUNK = 11 };
+       VELX_V, VELY_V, VELZ_V, NPROP = 11 };
+/* species and mass scalars follow the property variables (SPECIES_BEGIN =
+ * NPROP_VARS + 1 ... MASS_SCALARS_END in Flash.h); a cell holds
+ * nunk = NPROP + nspecies + nmass_scalars values */
+#define NUNK_MAX (NPROP + FLASH_HY_MAX_SPECIES)
 /* ---- primitive slots of UHD.h:374-383 (HY_DENS=1..HY_EINT=8), 0-based -- */
 enum { HD = 0, HVX, HVY, HVZ, HP, HGC, HGE, HEI, NSLOT = 9 };
 /* ---- flux slots of OnlyHydro/Config:6-13 (F01Dens..F08VOLU), 0-based --- */
@@ -49,6 +53,9 @@ typedef struct {
   int k2, k3;               /* 1 if the dimension exists (y, z)            */
   double gam1inv;           /* 1/eos_gammam1, eos_idealGamma.F90:323-326   */
   double ggprodinv;         /* 1/(eos_gammam1*R), eos_idealGamma.F90:262   */
+  int nunk;                 /* NPROP + species + mass scalars              */
+  int nsp;                  /* species + mass scalars (HY_NSPEC)           */
+  int nspec;                /* species (renormalised to a unit sum)        */
   int status;
 } ctx_t;
 
@@ -350,6 +357,11 @@ typedef struct {
   double *face[3];                        /* [cells][16]: P01..P08,N01..N08 */
   double *flux[3];                        /* [cells][8]                     */
   double *scrch;                          /* [cells][2]                     */
+  /* species and mass scalars (hy_computeFluxes.F90:222-236): face values
+   * hy_SpcL / hy_SpcR per direction, transverse terms hy_SpcSig, fluxes */
+  double *spc_l[3], *spc_r[3];            /* [cells][nsp]                   */
+  double *spc_sig;                        /* [cells][3][nsp]                */
+  double *spc_flux[3];                    /* [cells][nsp]                   */
 } work_t;
 
 static void work_alloc(const ctx_t *c, work_t *w) {
@@ -365,12 +377,78 @@ static void work_alloc(const ctx_t *c, work_t *w) {
     w->flux[d] = calloc(nc * NFLX, sizeof(double));
   }
   w->scrch = calloc(nc * 2, sizeof(double));
+  size_t ns = c->nsp > 0 ? (size_t)c->nsp : 1;
+  for (int d = 0; d < 3; ++d) {
+    w->spc_l[d] = calloc(nc * ns, sizeof(double));
+    w->spc_r[d] = calloc(nc * ns, sizeof(double));
+    w->spc_flux[d] = calloc(nc * ns, sizeof(double));
+  }
+  w->spc_sig = calloc(nc * 3 * ns, sizeof(double));
 }
 static void work_free(work_t *w) {
   free(w->flat_coeff); free(w->flat_tilde); free(w->sig); free(w->lambda);
   free(w->leig); free(w->reig);
-  for (int d = 0; d < 3; ++d) { free(w->face[d]); free(w->flux[d]); }
-  free(w->scrch);
+  for (int d = 0; d < 3; ++d) { free(w->face[d]); free(w->flux[d]); free(w->spc_l[d]); free(w->spc_r[d]); free(w->spc_flux[d]); }
+  free(w->scrch); free(w->spc_sig);
+}
+
+/* ===================================================================== */
+/* Species and mass scalars of one cell and direction: the stencil of     */
+/* hy_DataReconstructNormalDir_PPM.F90:289-301, the transverse term       */
+/* SpcSig of :360-369 (hy_upwindTransverseFlux.F90:197-205 with           */
+/* speciesScalar: the entropy eigenvalue times the upwind difference) and */
+/* the PPM face values of :584-628 (minmod slopes, monotonised parabola,  */
+/* tracing along the entropy wave, flattening).                          */
+/* ===================================================================== */
+static inline double minmod_s(double a, double b) {      /* hy_slopeLimiters.F90:56-60 */
+  return .5 * (f_sign(1., a) + f_sign(1., b)) * fmin2(fabs(a), fabs(b));
+}
+static void spc_reconst(ctx_t *c, const double *U, work_t *w, int ix, int iy, int iz, int d, double dt,
+                        double delta, int tonly, double flat) {
+  const int ns = c->nsp, nu = c->nunk;
+  const int di = d == 0, dj = d == 1, dk = d == 2;
+  const size_t cc = cidx(c, ix, iy, iz);
+  const double lam = w->lambda[(cc * 3 + d) * 5 + 2];    /* lambda0(HY_ENTROPY) */
+  const double *Sm = &U[cidx(c, ix - di, iy - dj, iz - dk) * nu + NPROP];
+  const double *Sc = &U[cc * nu + NPROP];
+  const double *Sp = &U[cidx(c, ix + di, iy + dj, iz + dk) * nu + NPROP];
+  if (c->ndim > 1) {
+    double *sig = &w->spc_sig[(cc * 3 + d) * ns];
+    for (int q = 0; q < ns; ++q) {
+      if (lam > 0.) sig[q] = Sc[q] - Sm[q];
+      else sig[q] = Sp[q] - Sc[q];
+      sig[q] = lam * sig[q];
+    }
+  }
+  if (tonly) return;
+  const double *Smm = &U[cidx(c, ix - 2 * di, iy - 2 * dj, iz - 2 * dk) * nu + NPROP];
+  const double *Spp = &U[cidx(c, ix + 2 * di, iy + 2 * dj, iz + 2 * dk) * nu + NPROP];
+  const double dtn = dt / delta, hdtn = 0.5 * dtn;      /* PPM :311-312 */
+  double *Sl = &w->spc_l[d][cc * ns], *Sr = &w->spc_r[d][cc * ns];
+  for (int q = 0; q < ns; ++q) {
+    double dP = minmod_s(Sp[q] - Sc[q], Spp[q] - Sp[q]);
+    double d0 = minmod_s(Sc[q] - Sm[q], Sp[q] - Sc[q]);
+    double dN = minmod_s(Sm[q] - Smm[q], Sc[q] - Sm[q]);
+    double l = 0.5 * (Sc[q] + Sm[q]) - (d0 - dN) / 6.;
+    double r = 0.5 * (Sc[q] + Sp[q]) - (dP - d0) / 6.;
+    l = fmax2(fmin2(Sc[q], Sm[q]), fmin2(fmax2(Sc[q], Sm[q]), l));
+    r = fmax2(fmin2(Sc[q], Sp[q]), fmin2(fmax2(Sc[q], Sp[q]), r));
+    if ((r - Sc[q]) * (Sc[q] - l) <= 0.) { r = Sc[q]; l = Sc[q]; }
+    if (6. * (r - l) * (Sc[q] - 0.5 * (r + l)) > (r - l) * (r - l)) l = 3. * Sc[q] - 2. * r;
+    if (6. * (r - l) * (Sc[q] - 0.5 * (r + l)) < -((r - l) * (r - l))) r = 3. * Sc[q] - 2. * l;
+    d0 = r - l;
+    double s6 = 6. * (Sc[q] - 0.5 * (r + l));
+    double lm = fmin2(lam, 0.), lp = fmax2(lam, 0.);
+    l = l - lm * hdtn * (d0 + (1. + lm * 4. / 3. * hdtn) * s6);
+    r = r - lp * hdtn * (d0 - (1. - lp * 4. / 3. * hdtn) * s6);
+    Sl[q] = l;
+    Sr[q] = r;
+  }
+  if (c->p->use_flattening)
+    for (int q = 0; q < ns; ++q) {
+      Sl[q] = flat * Sc[q] + (1.0 - flat) * Sl[q];
+      Sr[q] = flat * Sc[q] + (1.0 - flat) * Sr[q];
+    }
 }
 
 /* ===================================================================== */
@@ -390,13 +468,14 @@ static void data_reconst_one_step(ctx_t *c, const double *U, work_t *w, int ix, 
     memset(V5, 0, sizeof V5);
     for (int s = -kOrder; s <= kOrder; ++s) {
       int ii = ix + (d == 0 ? s : 0), jj = iy + (d == 1 ? s : 0), kk = iz + (d == 2 ? s : 0);
-      prim_of(&U[cidx(c, ii, jj, kk) * NUNK], V5[s + 2]);
+      prim_of(&U[cidx(c, ii, jj, kk) * c->nunk], V5[s + 2]);
     }
     double fc = c->p->use_flattening ? w->flat_coeff[d * (size_t)(c->nxt * c->nyt * c->nzt) + cc] : 0.;
     ppm(c, d + 1, dt, del[d], (const double (*)[NSLOT])V5, fc, trans_only[d],
         &w->lambda[(cc * 3 + d) * 5],
         (double (*)[5]) & w->leig[(cc * 3 + d) * 25], (double (*)[5]) & w->reig[(cc * 3 + d) * 25],
         Wp[d], Wn[d], &w->sig[(cc * 3 + d) * 8]);
+    if (c->nsp > 0) spc_reconst(c, U, w, ix, iy, iz, d, dt, del[d], trans_only[d], fc);
   }
   const double *sx = &w->sig[(cc * 3 + 0) * 8], *sy = &w->sig[(cc * 3 + 1) * 8], *sz = &w->sig[(cc * 3 + 2) * 8];
   /* (II) transverse contributions, :918-951 (HY_DENS:HY_END_VARS) */
@@ -416,8 +495,30 @@ static void data_reconst_one_step(ctx_t *c, const double *U, work_t *w, int ix, 
       Wp[2][n] = Wp[2][n] - hdtx * sx[n] - hdty * sy[n];
     }
   }
+  /* species transverse corrections, :996-1014 */
+  if (nd > 1 && c->nsp > 0) {
+    const int ns = c->nsp;
+    const double *gx = &w->spc_sig[(cc * 3 + 0) * ns], *gy = &w->spc_sig[(cc * 3 + 1) * ns];
+    const double *gz = &w->spc_sig[(cc * 3 + 2) * ns];
+    double *l0 = &w->spc_l[0][cc * ns], *r0 = &w->spc_r[0][cc * ns];
+    double *l1 = &w->spc_l[1][cc * ns], *r1 = &w->spc_r[1][cc * ns];
+    double *l2 = &w->spc_l[2][cc * ns], *r2 = &w->spc_r[2][cc * ns];
+    for (int q = 0; q < ns; ++q) {
+      if (!trans_only[0]) { l0[q] = l0[q] - hdty * gy[q]; r0[q] = r0[q] - hdty * gy[q]; }
+      if (!trans_only[1]) { l1[q] = l1[q] - hdtx * gx[q]; r1[q] = r1[q] - hdtx * gx[q]; }
+    }
+    if (nd > 2)
+      for (int q = 0; q < ns; ++q) {
+        if (!trans_only[0]) { l0[q] = l0[q] - hdtz * gz[q]; r0[q] = r0[q] - hdtz * gz[q]; }
+        if (!trans_only[1]) { l1[q] = l1[q] - hdtz * gz[q]; r1[q] = r1[q] - hdtz * gz[q]; }
+        if (!trans_only[2]) {
+          l2[q] = l2[q] - hdtx * gx[q] - hdty * gy[q];
+          r2[q] = r2[q] - hdtx * gx[q] - hdty * gy[q];
+        }
+      }
+  }
   /* (IV) last negativity check, :1120-1154 */
-  const double *u = &U[cc * NUNK];
+  const double *u = &U[cc * c->nunk];
   for (int d = 0; d < nd; ++d) {
     if (Wn[d][HD] < 0. || Wp[d][HD] < 0. || Wn[d][HP] < 0. || Wp[d][HP] < 0.) {
       double V[NSLOT];
@@ -446,10 +547,10 @@ static void get_riemann_state(ctx_t *c, const double *U, work_t *w, double dt, c
         for (int i = lo[0] - 2; i <= hi[0] + 2; ++i)
           for (int d = 0; d < nd; ++d) {
             int di = d == 0, dj = d == 1, dk = d == 2;
-            const double *um1 = &U[cidx(c, i - di, j - dj, k - dk) * NUNK];
-            const double *up1 = &U[cidx(c, i + di, j + dj, k + dk) * NUNK];
-            const double *um2 = &U[cidx(c, i - 2 * di, j - 2 * dj, k - 2 * dk) * NUNK];
-            const double *up2 = &U[cidx(c, i + 2 * di, j + 2 * dj, k + 2 * dk) * NUNK];
+            const double *um1 = &U[cidx(c, i - di, j - dj, k - dk) * c->nunk];
+            const double *up1 = &U[cidx(c, i + di, j + dj, k + dk) * c->nunk];
+            const double *um2 = &U[cidx(c, i - 2 * di, j - 2 * dj, k - 2 * dk) * c->nunk];
+            const double *up2 = &U[cidx(c, i + 2 * di, j + 2 * dj, k + 2 * dk) * c->nunk];
             double dp1 = (up1[PRES_V] - um1[PRES_V]);
             double dp2 = (up2[PRES_V] - um2[PRES_V]);
             double dv1 = up1[VELX_V + d] - um1[VELX_V + d];
@@ -465,7 +566,7 @@ static void get_riemann_state(ctx_t *c, const double *U, work_t *w, double dt, c
           for (int d = 0; d < nd; ++d) {
             int di = d == 0, dj = d == 1, dk = d == 2;
             size_t c0 = cidx(c, i, j, k);
-            double dp1 = U[cidx(c, i + di, j + dj, k + dk) * NUNK + PRES_V] - U[cidx(c, i - di, j - dj, k - dk) * NUNK + PRES_V];
+            double dp1 = U[cidx(c, i + di, j + dj, k + dk) * c->nunk + PRES_V] - U[cidx(c, i - di, j - dj, k - dk) * c->nunk + PRES_V];
             double t0 = w->flat_tilde[d * nc + c0];
             double fc;
             if (dp1 < 0.0) fc = fmax2(t0, w->flat_tilde[d * nc + cidx(c, i + di, j + dj, k + dk)]);
@@ -511,7 +612,7 @@ static void get_riemann_state(ctx_t *c, const double *U, work_t *w, double dt, c
         for (int i = lo[0] - 1; i <= hi[0] + 1; ++i) {
           size_t cc = cidx(c, i, j, k);
           double Vc[NSLOT];
-          prim_of(&U[cc * NUNK], Vc);
+          prim_of(&U[cc * c->nunk], Vc);
           for (int d = 0; d < 3; ++d) {
             /* d-states need the d index in [lo-1,hi+1] and the others interior */
             int ok = 1;
@@ -544,8 +645,31 @@ static void get_riemann_state(ctx_t *c, const double *U, work_t *w, double dt, c
               f[n] = f[n] + (T1[n] + T2[n]) * fac;
               f[8 + n] = f[8 + n] + (T1[n] + T2[n]) * fac;
             }
+            const int ns = c->nsp;
             if (f[HD] <= 0. || f[8 + HD] <= 0. || f[HP] <= 0. || f[8 + HP] <= 0.) {
+              /* fallbackToFirstOrder, :1456-1475: species too */
               for (int n = 0; n < 8; ++n) { f[n] = Vc[n]; f[8 + n] = Vc[n]; }
+              for (int q = 0; q < ns; ++q) {
+                w->spc_l[d][cc * ns + q] = U[cc * c->nunk + NPROP + q];
+                w->spc_r[d][cc * ns + q] = U[cc * c->nunk + NPROP + q];
+              }
+            } else if (ns > 0) {
+              /* species cross terms, :1053-1090 (and y/z analogues) */
+              for (int q = 0; q < ns; ++q) {
+                double T[2];
+                for (int t = 0; t < 2; ++t) {
+                  int ax = t ? a2 : a1, sd = t ? s2 : s1;
+                  int oi = ax == 0, oj = ax == 1, ok2 = ax == 2;
+                  double lam = w->lambda[(cc * 3 + ax) * 5 + 2];
+                  double sm = w->spc_sig[(cidx(c, i - oi, j - oj, k - ok2) * 3 + sd) * ns + q];
+                  double s0 = w->spc_sig[(cc * 3 + sd) * ns + q];
+                  double sp = w->spc_sig[(cidx(c, i + oi, j + oj, k + ok2) * 3 + sd) * ns + q];
+                  double g = lam > 0. ? s0 - sm : sp - s0;
+                  T[t] = lam * g;
+                }
+                w->spc_r[d][cc * ns + q] = w->spc_r[d][cc * ns + q] + (T[0] + T[1]) * fac;
+                w->spc_l[d][cc * ns + q] = w->spc_l[d][cc * ns + q] + (T[0] + T[1]) * fac;
+              }
             }
           }
         }
@@ -661,6 +785,14 @@ static void get_face_flux(ctx_t *c, work_t *w) {
             if (F[FDENS] > 0.) { F[FVOLU] = F[FDENS] / VL[HD]; F[FEINT] = F[FDENS] * VL[HEI]; }
             else               { F[FVOLU] = F[FDENS] / VR[HD]; F[FEINT] = F[FDENS] * VR[HEI]; }
           } else { F[FVOLU] = 0.; F[FEINT] = 0.; }
+          if (c->nsp > 0) {                                  /* :453-467 */
+            const int ns = c->nsp;
+            double *Fs2 = &w->spc_flux[d][cc * ns];
+            for (int q = 0; q < ns; ++q) {
+              if (F[FDENS] < 0.) Fs2[q] = F[FDENS] * w->spc_l[d][cc * ns + q];
+              else Fs2[q] = F[FDENS] * w->spc_r[d][cm * ns + q];
+            }
+          }
         }
     /* n+1/2 pressure average into scrch_Ptr, :551-557 and y/z analogues */
     if (c->p->use_aux_eint) {
@@ -706,9 +838,10 @@ static void unsplit_update(ctx_t *c, double *U, work_t *w, double dt, const doub
         Sphys[1] = (FL[FPRES] - FR[FPRES]) * (1.0 - fP) / dx;
         if (nd >= 2) Sphys[2] = (GL[FPRES] - GR[FPRES]) * (1.0 - fP) / dy;
         if (nd == 3) Sphys[3] = (HL[FPRES] - HR[FPRES]) * (1.0 - fP) / dz;
-        double *u = &U[cc * NUNK];
+        double *u = &U[cc * c->nunk];
         double U0[5];
         U0[0] = u[DENS_V];
+        const double densOld = u[DENS_V];                    /* Uold(HY_DENS) */
         double IntEner = 0.;
         if (p->use_aux_eint) {
           IntEner = u[DENS_V] * u[EINT_V];
@@ -736,6 +869,25 @@ static void unsplit_update(ctx_t *c, double *U, work_t *w, double dt, const doub
           IntEner = IntEner / u[DENS_V];
           u[EINT_V] = IntEner;
         }
+        if (c->nsp > 0) {          /* :827-859, updateSpeciesMassScalar :1300-1318 */
+          const int ns = c->nsp;
+          const double newDens = u[DENS_V];
+          double sumSpecies = 0.;
+          for (int q = 0; q < ns; ++q) {
+            double FLs = w->spc_flux[0][cc * ns + q], FRs = w->spc_flux[0][cidx(c, i + 1, j, k) * ns + q];
+            double GLs = w->spc_flux[1][cc * ns + q], GRs = w->spc_flux[1][cidx(c, i, j + 1, k) * ns + q];
+            double X = u[NPROP + q];
+            if (nd == 2) {
+              X = (X * densOld + dt * ((FLs - FRs) / dx + (GLs - GRs) / dy)) / newDens;
+            } else {
+              double HLs = w->spc_flux[2][cc * ns + q], HRs = w->spc_flux[2][cidx(c, i, j, k + 1) * ns + q];
+              X = (X * densOld + dt * ((FLs - FRs) / dx + (GLs - GRs) / dy + (HLs - HRs) / dz)) / newDens;
+            }
+            u[NPROP + q] = X;
+            if (q < c->nspec) sumSpecies = sumSpecies + X;
+          }
+          for (int q = 0; q < c->nspec; ++q) u[NPROP + q] = u[NPROP + q] / sumSpecies;
+        }
       }
 }
 
@@ -746,7 +898,7 @@ static void energy_fix(ctx_t *c, double *U) {
   for (int k = c->k3 ? ng : 0; k <= (c->k3 ? ng + c->nzb - 1 : 0); ++k)
     for (int j = c->k2 ? ng : 0; j <= (c->k2 ? ng + c->nyb - 1 : 0); ++j)
       for (int i = ng; i <= ng + c->nxb - 1; ++i) {
-        double *u = &U[cidx(c, i, j, k) * NUNK];
+        double *u = &U[cidx(c, i, j, k) * c->nunk];
         double ekin = 0.5 * (u[VELX_V] * u[VELX_V] + u[VELY_V] * u[VELY_V] + u[VELZ_V] * u[VELZ_V]);
         double eint = u[ENER_V] - ekin - 0.0;
         double IntEner = u[EINT_V];
@@ -808,6 +960,11 @@ static void ctx_init(ctx_t *c, const flash_hy_params *p, const flash_hy_grid_des
   c->gam1inv = 1. / gammam1;
   double ggprod = gammam1 * p->gas_constant;        /* eos_idealGamma.F90:262 */
   c->ggprodinv = 1. / ggprod;
+  int ns = p->nspecies, nm = p->nmass_scalars;
+  if (ns < 0 || nm < 0 || ns + nm > FLASH_HY_MAX_SPECIES) { ns = 0; nm = 0; c->status |= FLASH_HY_ERR_BAD_ARG; }
+  c->nspec = ns;
+  c->nsp = ns + nm;
+  c->nunk = NPROP + c->nsp;
 }
 
 static int check_grid(const flash_hy_grid_desc *g) {
@@ -833,7 +990,7 @@ int orc_fill_guardcells(const flash_hy_params *p, const flash_hy_grid_desc *g, d
     const int *bc = &g->block_coords[3 * b];
     owner[((g->ndim > 2 ? bc[2] : 0) * nby + (g->ndim > 1 ? bc[1] : 0)) * nbx + bc[0]] = b;
   }
-  size_t bsz = (size_t)c.nxt * c.nyt * c.nzt * NUNK;
+  size_t bsz = (size_t)c.nxt * c.nyt * c.nzt * c.nunk;
   int NX = nbx * c.nxb, NY = nby * c.nyb, NZ = nbz * c.nzb;
   #pragma omp parallel for schedule(dynamic)
   for (int b = 0; b < g->nblocks; ++b) {
@@ -850,9 +1007,9 @@ int orc_fill_guardcells(const flash_hy_params *p, const flash_hy_grid_desc *g, d
           int sb = owner[((gz / c.nzb) * nby + gy / c.nyb) * nbx + gx / c.nxb];
           if (sb < 0) continue;
           int si = gx % c.nxb + NGUARD, sj = c.k2 ? gy % c.nyb + NGUARD : 0, sk = c.k3 ? gz % c.nzb + NGUARD : 0;
-          const double *src = &unk[sb * bsz + cidx(&c, si, sj, sk) * NUNK];
-          double *dst = &unk[b * bsz + cidx(&c, i, j, k) * NUNK];
-          memcpy(dst, src, sizeof(double) * NUNK);
+          const double *src = &unk[sb * bsz + cidx(&c, si, sj, sk) * c.nunk];
+          double *dst = &unk[b * bsz + cidx(&c, i, j, k) * c.nunk];
+          memcpy(dst, src, sizeof(double) * c.nunk);
           if (fx) dst[VELX_V] = -dst[VELX_V];
           if (fy) dst[VELY_V] = -dst[VELY_V];
           if (fz) dst[VELZ_V] = -dst[VELZ_V];
@@ -866,7 +1023,7 @@ int orc_fill_guardcells(const flash_hy_params *p, const flash_hy_grid_desc *g, d
         for (int i = 0; i < c.nxt; ++i) {
           int li = i - NGUARD, lj = c.k2 ? j - NGUARD : 0, lk = c.k3 ? k - NGUARD : 0;
           if (li >= 0 && li < c.nxb && lj >= 0 && lj < c.nyb && lk >= 0 && lk < c.nzb) continue;
-          eos_dens_ei_cell(&c, &unk[b * bsz + cidx(&c, i, j, k) * NUNK]);
+          eos_dens_ei_cell(&c, &unk[b * bsz + cidx(&c, i, j, k) * c.nunk]);
         }
   free(owner);
   return 0;
@@ -876,13 +1033,13 @@ int orc_fill_guardcells(const flash_hy_params *p, const flash_hy_grid_desc *g, d
 int orc_eos_interior(const flash_hy_params *p, const flash_hy_grid_desc *g, double *unk) {
   if (g->ndim < 2 || g->ndim > 3 || g->nguard != NGUARD) return FLASH_HY_ERR_UNSUPPORTED;
   ctx_t c; ctx_init(&c, p, g);
-  size_t bsz = (size_t)c.nxt * c.nyt * c.nzt * NUNK;
+  size_t bsz = (size_t)c.nxt * c.nyt * c.nzt * c.nunk;
   #pragma omp parallel for schedule(static)
   for (int b = 0; b < g->nblocks; ++b)
     for (int k = c.k3 ? NGUARD : 0; k < (c.k3 ? NGUARD + c.nzb : 1); ++k)
       for (int j = c.k2 ? NGUARD : 0; j < (c.k2 ? NGUARD + c.nyb : 1); ++j)
         for (int i = NGUARD; i < NGUARD + c.nxb; ++i)
-          eos_dens_ei_cell(&c, &unk[b * bsz + cidx(&c, i, j, k) * NUNK]);
+          eos_dens_ei_cell(&c, &unk[b * bsz + cidx(&c, i, j, k) * c.nunk]);
   return 0;
 }
 
@@ -898,9 +1055,9 @@ static int compute_fluxes_block(ctx_t *c, double *U, double dt, const double del
   for (int k = c->k3 ? NGUARD : 0; k < (c->k3 ? NGUARD + c->nzb : 1); ++k)
     for (int j = c->k2 ? NGUARD : 0; j < (c->k2 ? NGUARD + c->nyb : 1); ++j)
       for (int i = NGUARD; i < NGUARD + c->nxb; ++i) {
-        double *u = &U[cidx(c, i, j, k) * NUNK];
+        double *u = &U[cidx(c, i, j, k) * c->nunk];
         eos_dens_ei_cell(c, u);
-        for (int n = 0; n < NUNK; ++n) if (!isfinite(u[n]) && n != SHOK_V) c->status |= FLASH_HY_ERR_NAN;
+        for (int n = 0; n < c->nunk; ++n) if (!isfinite(u[n]) && n != SHOK_V) c->status |= FLASH_HY_ERR_NAN;
       }
   work_free(&w);
   return c->status;
@@ -927,7 +1084,7 @@ int orc_hydro(const flash_hy_params *p, const flash_hy_grid_desc *g, double *unk
   ctx_t c0; ctx_init(&c0, p, g);
   double del[3];
   block_deltas(g, del);
-  size_t bsz = (size_t)c0.nxt * c0.nyt * c0.nzt * NUNK;
+  size_t bsz = (size_t)c0.nxt * c0.nyt * c0.nzt * c0.nunk;
   int n = block_list ? nlist : g->nblocks;
   int status = 0;
   #pragma omp parallel for schedule(dynamic) reduction(| : status)
@@ -949,7 +1106,7 @@ int orc_compute_dt(const flash_hy_params *p, const flash_hy_grid_desc *g, const 
   ctx_t c; ctx_init(&c, p, g);
   double del[3];
   block_deltas(g, del);
-  size_t bsz = (size_t)c.nxt * c.nyt * c.nzt * NUNK;
+  size_t bsz = (size_t)c.nxt * c.nyt * c.nzt * c.nunk;
   double dt_check = DBL_MAX;
   int best[5] = {0, 0, 0, 0, -1};
   double delxinv = 1.0 / del[0], delyinv = 1.0 / del[1], delzinv = 1.0 / del[2];
@@ -960,7 +1117,7 @@ int orc_compute_dt(const flash_hy_params *p, const flash_hy_grid_desc *g, const 
     for (int k = c.k3 ? NGUARD : 0; k < (c.k3 ? NGUARD + c.nzb : 1); ++k)
       for (int j = c.k2 ? NGUARD : 0; j < (c.k2 ? NGUARD + c.nyb : 1); ++j)
         for (int i = NGUARD; i < NGUARD + c.nxb; ++i) {
-          const double *u = &unk[b * bsz + cidx(&c, i, j, k) * NUNK];
+          const double *u = &unk[b * bsz + cidx(&c, i, j, k) * c.nunk];
           double sndspd2 = u[GAMC_V] * u[PRES_V] / u[DENS_V];
           double dt_ltemp = (fabs(u[VELX_V] - 0.) + sqrt(sndspd2)) * delxinv;
           if (g->ndim > 1) dt_ltemp = fmax2(dt_ltemp, (fabs(u[VELY_V] - 0.) + sqrt(sndspd2)) * delyinv);
@@ -1075,11 +1232,13 @@ static int amr_build(const flash_hy_grid_desc *g, amr_t *a) {
   return 0;
 }
 
-static inline int is_per_mass(int v) { return v == VELX_V || v == VELY_V || v == VELZ_V || v == EINT_V || v == ENER_V; }
+static inline int is_per_mass(int v) {
+  return v == VELX_V || v == VELY_V || v == VELZ_V || v == EINT_V || v == ENER_V || v >= NPROP;
+}
 
 /* Interior of parent node P = average of its children, per-volume form. */
 static void amr_restrict_node(const ctx_t *c, const amr_t *a, double *unk, int P) {
-  size_t bsz = (size_t)c->nxt * c->nyt * c->nzt * NUNK;
+  size_t bsz = (size_t)c->nxt * c->nyt * c->nzt * c->nunk;
   int l = a->level[P];
   const int *pc = &a->coords[3 * P];
   int hx = c->nxb / 2, hy = c->nyb / 2, hz = c->nzb / 2;
@@ -1090,17 +1249,17 @@ static void amr_restrict_node(const ctx_t *c, const amr_t *a, double *unk, int P
         int ox = i >= hx, oy = j >= hy, oz = c->k3 ? k >= hz : 0;
         int ch = amr_at(a, l + 1, 2 * pc[0] + ox, 2 * pc[1] + oy, c->k3 ? 2 * pc[2] + oz : 0);
         int fi = 2 * (i - ox * hx), fj = 2 * (j - oy * hy), fk = c->k3 ? 2 * (k - oz * hz) : 0;
-        double s[NUNK];
-        for (int v = 0; v < NUNK; ++v) s[v] = 0.;
+        double s[NUNK_MAX];
+        for (int v = 0; v < c->nunk; ++v) s[v] = 0.;
         for (int kk = 0; kk <= c->k3; ++kk)
           for (int jj = 0; jj <= 1; ++jj)
             for (int ii = 0; ii <= 1; ++ii) {
-              const double *u = &unk[ch * bsz + cidx(c, fi + ii + NGUARD, fj + jj + NGUARD, c->k3 ? fk + kk + NGUARD : 0) * NUNK];
-              for (int v = 0; v < NUNK; ++v) s[v] = s[v] + w * (is_per_mass(v) ? u[DENS_V] * u[v] : u[v]);
+              const double *u = &unk[ch * bsz + cidx(c, fi + ii + NGUARD, fj + jj + NGUARD, c->k3 ? fk + kk + NGUARD : 0) * c->nunk];
+              for (int v = 0; v < c->nunk; ++v) s[v] = s[v] + w * (is_per_mass(v) ? u[DENS_V] * u[v] : u[v]);
             }
-        double *d = &unk[P * bsz + cidx(c, i + NGUARD, j + NGUARD, c->k3 ? k + NGUARD : 0) * NUNK];
+        double *d = &unk[P * bsz + cidx(c, i + NGUARD, j + NGUARD, c->k3 ? k + NGUARD : 0) * c->nunk];
         double inv = 1. / s[DENS_V];
-        for (int v = 0; v < NUNK; ++v) d[v] = is_per_mass(v) ? inv * s[v] : s[v];
+        for (int v = 0; v < c->nunk; ++v) d[v] = is_per_mass(v) ? inv * s[v] : s[v];
       }
 }
 
@@ -1110,7 +1269,7 @@ static void amr_restrict_node(const ctx_t *c, const amr_t *a, double *unk, int P
  * reflecting: mirror and flip the normal velocity; outflow: copy the edge). */
 static void amr_guard_cell(const ctx_t *c, const amr_t *a, const flash_hy_grid_desc *g, double *unk, int n,
                            int li, int lj, int lk, double *dst) {
-  size_t bsz = (size_t)c->nxt * c->nyt * c->nzt * NUNK;
+  size_t bsz = (size_t)c->nxt * c->nyt * c->nzt * c->nunk;
   int l = a->level[n];
   const int *bc = &a->coords[3 * n];
   int loc[3] = {li, lj, lk}, gl[3], lp[3], flip[3] = {0, 0, 0};
@@ -1132,8 +1291,8 @@ static void amr_guard_cell(const ctx_t *c, const amr_t *a, const flash_hy_grid_d
   int m = amr_at(a, l, gl[0] / a->N[0], gl[1] / a->N[1], a->ndim > 2 ? gl[2] / a->N[2] : 0);
   if (m >= 0) {
     const double *src = &unk[m * bsz + cidx(c, gl[0] % a->N[0] + NGUARD, gl[1] % a->N[1] + NGUARD,
-                                             c->k3 ? gl[2] % a->N[2] + NGUARD : 0) * NUNK];
-    memcpy(dst, src, sizeof(double) * NUNK);
+                                             c->k3 ? gl[2] % a->N[2] + NGUARD : 0) * c->nunk];
+    memcpy(dst, src, sizeof(double) * c->nunk);
   } else {
     /* amr_1blk_cc_prol_linear: child cell lp from the parent cells i1, i1+1
      * per axis with weights dx, 1-dx (amr_prolong_cc_fun_init.F90) */
@@ -1147,16 +1306,16 @@ static void amr_guard_cell(const ctx_t *c, const amr_t *a, const flash_hy_grid_d
       wx[d] = fmod(0.75 + (double)(ii + 2 * N) * .5, 1.);     /* prol_dx */
       cx[d] = 1. - wx[d];
     }
-    double r[2][2][2][NUNK];
+    double r[2][2][2][NUNK_MAX];
     for (int kk = 0; kk <= dk3; ++kk)
       for (int jj = 0; jj <= 1; ++jj)
         for (int ii = 0; ii <= 1; ++ii) {
           const double *u = &unk[P * bsz + cidx(c, i1[0] + ii + NGUARD, i1[1] + jj + NGUARD,
-                                                  dk3 ? i1[2] + kk + NGUARD : 0) * NUNK];
-          for (int v = 0; v < NUNK; ++v) r[kk][jj][ii][v] = is_per_mass(v) ? u[DENS_V] * u[v] : u[v];
+                                                  dk3 ? i1[2] + kk + NGUARD : 0) * c->nunk];
+          for (int v = 0; v < c->nunk; ++v) r[kk][jj][ii][v] = is_per_mass(v) ? u[DENS_V] * u[v] : u[v];
         }
-    double val[NUNK];
-    for (int v = 0; v < NUNK; ++v) {
+    double val[NUNK_MAX];
+    for (int v = 0; v < c->nunk; ++v) {
       double plane0 = wx[1] * (wx[0] * r[0][0][0][v] + cx[0] * r[0][0][1][v]) +
                       cx[1] * (wx[0] * r[0][1][0][v] + cx[0] * r[0][1][1][v]);
       if (dk3) {
@@ -1168,7 +1327,7 @@ static void amr_guard_cell(const ctx_t *c, const amr_t *a, const flash_hy_grid_d
       }
     }
     double inv = 1. / val[DENS_V];
-    for (int v = 0; v < NUNK; ++v) dst[v] = is_per_mass(v) ? inv * val[v] : val[v];
+    for (int v = 0; v < c->nunk; ++v) dst[v] = is_per_mass(v) ? inv * val[v] : val[v];
   }
   if (flip[0]) dst[VELX_V] = -dst[VELX_V];
   if (flip[1]) dst[VELY_V] = -dst[VELY_V];
@@ -1176,13 +1335,13 @@ static void amr_guard_cell(const ctx_t *c, const amr_t *a, const flash_hy_grid_d
 }
 
 static void amr_fill_node_guards(const ctx_t *c, const amr_t *a, const flash_hy_grid_desc *g, double *unk, int n) {
-  size_t bsz = (size_t)c->nxt * c->nyt * c->nzt * NUNK;
+  size_t bsz = (size_t)c->nxt * c->nyt * c->nzt * c->nunk;
   for (int k = 0; k < c->nzt; ++k)
     for (int j = 0; j < c->nyt; ++j)
       for (int i = 0; i < c->nxt; ++i) {
         int li = i - NGUARD, lj = c->k2 ? j - NGUARD : 0, lk = c->k3 ? k - NGUARD : 0;
         if (li >= 0 && li < c->nxb && lj >= 0 && lj < c->nyb && lk >= 0 && lk < c->nzb) continue;
-        amr_guard_cell(c, a, g, unk, n, li, lj, lk, &unk[n * bsz + cidx(c, i, j, k) * NUNK]);
+        amr_guard_cell(c, a, g, unk, n, li, lj, lk, &unk[n * bsz + cidx(c, i, j, k) * c->nunk]);
       }
 }
 
@@ -1190,7 +1349,7 @@ static void amr_fill_node_guards(const ctx_t *c, const amr_t *a, const flash_hy_
  * the leaves' guard cells. */
 static int amr_fill_all(const flash_hy_params *p, const flash_hy_grid_desc *g, const amr_t *a, double *unk) {
   ctx_t c; ctx_init(&c, p, g);
-  size_t bsz = (size_t)c.nxt * c.nyt * c.nzt * NUNK;
+  size_t bsz = (size_t)c.nxt * c.nyt * c.nzt * c.nunk;
   for (int l = a->L - 1; l >= 1; --l) {
     #pragma omp parallel for schedule(dynamic)
     for (int b = 0; b < a->n; ++b)
@@ -1209,7 +1368,7 @@ static int amr_fill_all(const flash_hy_params *p, const flash_hy_grid_desc *g, c
         for (int i = 0; i < c.nxt; ++i) {
           int li = i - NGUARD, lj = c.k2 ? j - NGUARD : 0, lk = c.k3 ? k - NGUARD : 0;
           if (li >= 0 && li < c.nxb && lj >= 0 && lj < c.nyb && lk >= 0 && lk < c.nzb) continue;
-          eos_dens_ei_cell(&c, &unk[b * bsz + cidx(&c, i, j, k) * NUNK]);
+          eos_dens_ei_cell(&c, &unk[b * bsz + cidx(&c, i, j, k) * c.nunk]);
         }
   }
   return 0;
@@ -1289,7 +1448,7 @@ int orc_amr_hydro(const flash_hy_params *p, const flash_hy_grid_desc *g, double 
   if (st) return st;
   amr_fill_all(p, g, &a, unk);
   ctx_t c0; ctx_init(&c0, p, g);
-  size_t bsz = (size_t)c0.nxt * c0.nyt * c0.nzt * NUNK;
+  size_t bsz = (size_t)c0.nxt * c0.nyt * c0.nzt * c0.nunk;
   work_t *W = calloc(a.n, sizeof(work_t));
   int status = 0;
   #pragma omp parallel for schedule(dynamic) reduction(| : status)
@@ -1318,9 +1477,9 @@ int orc_amr_hydro(const flash_hy_params *p, const flash_hy_grid_desc *g, double 
     for (int k = c.k3 ? NGUARD : 0; k < (c.k3 ? NGUARD + c.nzb : 1); ++k)
       for (int j = c.k2 ? NGUARD : 0; j < (c.k2 ? NGUARD + c.nyb : 1); ++j)
         for (int i = NGUARD; i < NGUARD + c.nxb; ++i) {
-          double *u = &U[cidx(&c, i, j, k) * NUNK];
+          double *u = &U[cidx(&c, i, j, k) * c0.nunk];
           eos_dens_ei_cell(&c, u);
-          for (int n = 0; n < NUNK; ++n) if (!isfinite(u[n]) && n != SHOK_V) c.status |= FLASH_HY_ERR_NAN;
+          for (int n = 0; n < c0.nunk; ++n) if (!isfinite(u[n]) && n != SHOK_V) c.status |= FLASH_HY_ERR_NAN;
         }
     status |= c.status;
   }
@@ -1343,7 +1502,7 @@ int orc_amr_compute_dt(const flash_hy_params *p, const flash_hy_grid_desc *g, co
   int st = amr_build(g, &a);
   if (st) return st;
   ctx_t c; ctx_init(&c, p, g);
-  size_t bsz = (size_t)c.nxt * c.nyt * c.nzt * NUNK;
+  size_t bsz = (size_t)c.nxt * c.nyt * c.nzt * c.nunk;
   double dt_check = DBL_MAX;
   int best[5] = {0, 0, 0, 0, -1};
   for (int b = 0; b < a.n; ++b) {
@@ -1357,7 +1516,7 @@ int orc_amr_compute_dt(const flash_hy_params *p, const flash_hy_grid_desc *g, co
     for (int k = c.k3 ? NGUARD : 0; k < (c.k3 ? NGUARD + c.nzb : 1); ++k)
       for (int j = c.k2 ? NGUARD : 0; j < (c.k2 ? NGUARD + c.nyb : 1); ++j)
         for (int i = NGUARD; i < NGUARD + c.nxb; ++i) {
-          const double *u = &unk[b * bsz + cidx(&c, i, j, k) * NUNK];
+          const double *u = &unk[b * bsz + cidx(&c, i, j, k) * c.nunk];
           double sndspd2 = u[GAMC_V] * u[PRES_V] / u[DENS_V];
           double dt_ltemp = (fabs(u[VELX_V] - 0.) + sqrt(sndspd2)) * delxinv;
           if (g->ndim > 1) dt_ltemp = fmax2(dt_ltemp, (fabs(u[VELY_V] - 0.) + sqrt(sndspd2)) * delyinv);
@@ -1406,7 +1565,7 @@ int orc_block_fluxes(const flash_hy_params *p, const flash_hy_grid_desc *g, doub
   int st = orc_fill_guardcells(p, g, unk);
   if (st) return st;
   ctx_t c; ctx_init(&c, p, g);
-  size_t bsz = (size_t)c.nxt * c.nyt * c.nzt * NUNK;
+  size_t bsz = (size_t)c.nxt * c.nyt * c.nzt * c.nunk;
   double del[3];
   block_deltas(g, del);
   work_t w;

@@ -58,7 +58,8 @@ class Oracle:
     Grids with max_level > 1 (AmrGrid) use the AMR restatement."""
 
     def __init__(self, params, grid):
-        self.p = params
+        from flash5_b200 import abi
+        self.p = abi.with_species(params, grid)
         self.grid = grid
         self.g = grid.desc()
         self.amr = self.g.max_level > 1

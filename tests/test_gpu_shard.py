@@ -25,6 +25,11 @@ def kh2d():
     return g, setups.kelvin_helmholtz(g), abi.default_params(gamma=5.0 / 3.0)
 
 
+def kh3d_species():
+    g = UniformGrid(3, (8, 8, 8), (3, 3, 2), bc="periodic", nspecies=2, nmass_scalars=1)
+    return g, setups.add_species(g, setups.kelvin_helmholtz(g)), abi.default_params(gamma=5.0 / 3.0)
+
+
 def sod2d():
     g = UniformGrid(2, (8, 8), (5, 3), bc=["outflow", "outflow", "reflecting", "reflecting"])
     return g, setups.sod(g, xangle=30.0), abi.default_params()
@@ -45,7 +50,8 @@ def exchange_in_process(ranks):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("case,nranks,prec", [(kh3d, 2, abi.PREC_FP64), (kh3d, 3, abi.PREC_MIXED),
-                                              (kh2d, 3, abi.PREC_FP64), (sod2d, 3, abi.PREC_FP64)])
+                                              (kh2d, 3, abi.PREC_FP64), (sod2d, 3, abi.PREC_FP64),
+                                              (kh3d_species, 3, abi.PREC_FP64)])
 def test_sharded_contexts_match_single_context(case, nranks, prec):
     grid, unk, params = case()
     params.precision = prec
