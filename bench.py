@@ -110,11 +110,12 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def kh_workload(nblk=32, nguard=0):
+def kh_workload(nblk=32, nguard=0, nspecies=0, nmass_scalars=0):
     from flash5_b200 import abi, setups
     from flash5_b200.grid import UniformGrid
-    g = UniformGrid(3, (8, 8, 8), (nblk, nblk, nblk), bc="periodic", nguard=nguard)
-    unk = setups.kelvin_helmholtz(g)
+    g = UniformGrid(3, (8, 8, 8), (nblk, nblk, nblk), bc="periodic", nguard=nguard, nspecies=nspecies,
+                    nmass_scalars=nmass_scalars)
+    unk = setups.add_species(g, setups.kelvin_helmholtz(g))
     return g, unk, abi
 
 
@@ -285,10 +286,8 @@ def train_guess(g, unk, abi, dev, dts):
 
 
 def conserved_l1(a, b, var):
-    from oracle import sfocu
-    ca = sfocu.conserved(a, var)
-    cb = sfocu.conserved(b, var)
-    return {k: sfocu.l1_rel(ca[k], cb[k]) for k in sfocu.CONSERVED}
+    from flash5_b200.metrics import conserved_l1 as l1
+    return l1(a, b, var)
 
 
 def riemann_workload(args):
@@ -471,6 +470,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes (no autotuning)")
+    ap.add_argument("--nspecies", type=int, default=0, help="KH workload: species advected with the flow")
+    ap.add_argument("--nmass-scalars", type=int, default=0, help="KH workload: mass scalars advected with the flow")
     ap.add_argument("--workload", default="kh", choices=["kh", "riemann", "amr"])
     ap.add_argument("--amr-nblk", type=int, default=32, help="root blocks per axis of the AMR hierarchy")
     ap.add_argument("--riemann-n", type=int, default=100_000_000)
@@ -522,7 +523,7 @@ def main():
 
     from flash5_b200.hydro import Hydro
     from flash5_b200.grid import VAR
-    g, unk, abi = kh_workload(args.nblk, nguard=0)
+    g, unk, abi = kh_workload(args.nblk, nguard=0, nspecies=args.nspecies, nmass_scalars=args.nmass_scalars)
     zones = g.ncells
     peak, peak_kind = measured_peaks()
     if world > 1:
@@ -594,6 +595,13 @@ def main():
         h.close()
     head = paths[-1]
     errs = {n: conserved_l1(outs[n], outs[spec[n][3]], VAR) for n in outs if spec[n][3] in outs}
+    if g.nspecies + g.nmass_scalars:
+        from flash5_b200.metrics import l1_rel
+        for n in errs:
+            a, b = outs[n], outs[spec[n][3]]
+            for q in range(g.nspecies + g.nmass_scalars):
+                k = g.species.start + q
+                errs[n][f"rho_x{q}"] = l1_rel(a[..., 0] * a[..., k], b[..., 0] * b[..., k])
     if dist is not None:
         for n in ms:
             ms[n] = dist_max(dist, ms[n])
@@ -625,6 +633,9 @@ def main():
                                                    "point-to-point every step, NCCL dt min" if world > 1 else ""),
                        "riemann": "exact (Newton 1e-12)" if spec[head][1] == abi.RS_EXACT else "HLLC",
                        "zones_per_gpu": zones, "l2": f"inputs larger than L2 (state {zones * 40 / 1e6:.0f} MB)",
+                       **({"species": args.nspecies, "mass_scalars": args.nmass_scalars,
+                           "species_note": "dense-layer species pair and passive tracers, FP64 species pass"}
+                          if args.nspecies + args.nmass_scalars else {}),
                        "path": head},
             "paths": {n: {"value": total / (ms[n] * 1e-3), "ms_per_step": ms[n], "note": notes[n],
                           **({f"rel_l1_vs_{spec[n][3]}": errs[n]} if n in errs else {}),

@@ -76,7 +76,7 @@ struct flash_hy_ctx {
   // accumulator, SpcSig scratch, face mass fluxes and fallback flags left
   // by the hydro direction kernels
   int nsp, nspec;
-  double *spec[2], *sacc, *ssig, *sp_mf;
+  double *spec[2], *sacc, *ssig, *sp_mf, *sp_flat;
   unsigned char *sp_fb;
   char err[512];
 };
@@ -155,6 +155,7 @@ static void fill_devparams(const flash_hy_ctx *c, DevParams &P) {
     P.sp_out = c->spec[1 - c->cur];
     P.sp_mf = c->sp_mf;
     P.sp_fb = c->sp_fb;
+    P.sp_flat = c->sp_flat;
   }
   if (c->amr) {
     P.blk_level = c->d_level;
@@ -383,6 +384,7 @@ extern "C" int flash_hy_create(const flash_hy_params *params, const flash_hy_gri
     ALLOC(c->ssig, (size_t)g->nblocks * g->ndim * c->nsp * box * sizeof(double));
     ALLOC(c->sp_mf, (size_t)g->nblocks * g->ndim * lines * sizeof(double));
     ALLOC(c->sp_fb, (size_t)g->nblocks * g->ndim * lines);
+    ALLOC(c->sp_flat, (size_t)g->nblocks * g->ndim * lines * sizeof(double));
   }
   if (!amr) ALLOC(c->d_blk_at, at.size() * sizeof(int));
   ALLOC(c->d_blk_coord, coords.size() * sizeof(int));
@@ -427,7 +429,7 @@ extern "C" int flash_hy_destroy(flash_hy_ctx *c) {
   cudaFree(c->d_owned); cudaFree(c->d_owned_mask); cudaFree(c->d_send); cudaFree(c->d_recv);
   cudaFree(c->d_fstore);
   for (int s = 0; s < 2; ++s) cudaFree(c->spec[s]);
-  cudaFree(c->sacc); cudaFree(c->ssig); cudaFree(c->sp_mf); cudaFree(c->sp_fb);
+  cudaFree(c->sacc); cudaFree(c->ssig); cudaFree(c->sp_mf); cudaFree(c->sp_fb); cudaFree(c->sp_flat);
   free(c->h_blk_at);
   if (c->h_dt) cudaFreeHost(c->h_dt);
   if (c->h_status) cudaFreeHost(c->h_status);

@@ -70,12 +70,14 @@ struct DevParams {
   // [nsp][ncells] block-major SoA interiors, double-buffered like s_in/s_out.
   // The hydro direction kernels leave for them, per launch slot and
   // direction in the line-cell order of DirGeom, the face mass flux
-  // (sp_mf) and whether the 3D CTU stage fell back to first order (sp_fb).
+  // (sp_mf), whether the 3D CTU stage fell back to first order (sp_fb) and
+  // the flattening coefficient (sp_flat).
   int nsp, nspec;
   const double *sp_in;
   double *sp_out;
   double *sp_mf;
   unsigned char *sp_fb;
+  double *sp_flat;            // flattening coefficient of each line cell (same layout)
 };
 
 // Cell sizes of block b: level-1 deltas scaled by 2^(1-level) (exact).

@@ -468,6 +468,7 @@ __global__ void __launch_bounds__(320) k_dir(const DevParams P, const R *__restr
       u7[0] = R(0); u7[6] = R(0);
       flat = flat_coeff(p7, u7);
     }
+    if (P.sp_flat) P.sp_flat[sp_line_base<NDIM, NX, NY, NZ, DIR>(blockIdx.x) + t] = double(flat);
     R Wp[8], Wm[8];
     ppm_cell<R, DIR>(P, V5, flat, dtn, R(delta), Wp, Wm, st);
     const R *Vc = V5[2];

@@ -226,6 +226,9 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
       else if (dp1 == 0.) flat = t0;
       else flat = fmaxf(t0, sFlat[q - qs]);
     }
+    if (P.sp_flat)
+      P.sp_flat[sp_line_base<NDIM, NX, NY, NZ, DIR>(blockIdx.x) + DirGeom<NDIM, NX, NY, NZ, double, DIR>::idx(i, j, k)] =
+          double(flat);
     const int sl[6] = {0, 1, 2, 3, 4, 7};
     float lft[8], rgt[8], delW[8], W6[8];
 #pragma unroll

@@ -14,7 +14,8 @@ static bool launch_spec_dir(const SpecArgs &a) {
 
 template <int NDIM, int NX, int NY, int NZ>
 static int run_spec(const SpecArgs &a) {
-  k_spec_sig<NDIM, NX, NY, NZ><<<a.nlaunch, 256, 0, a.stream>>>(a.P, a.ssig, a.ncells);
+  k_spec_sig<NDIM, NX, NY, NZ><<<a.nlaunch, 256, SigGeom<NDIM, NX, NY, NZ>::smem_bytes(), a.stream>>>(a.P, a.ssig,
+                                                                                                    a.ncells);
   if (cudaGetLastError() != cudaSuccess) return -2;
   if constexpr (NDIM == 2) {
     const bool ok = launch_spec_dir<NDIM, NX, NY, NZ, 1, true, false>(a) &&

@@ -53,38 +53,91 @@ __device__ __forceinline__ double minmod_s(double a, double b) {     // hy_slope
   return .5 * (copysign(1., a) + copysign(1., b)) * rmin(fabs(a), fabs(b));
 }
 
+// Cells (N+2s)^d around a block's interior (s layers), staged in shared
+// memory so that every guard-mapped cell is loaded once.
+template <int NDIM, int NX, int NY, int NZ, int S>
+struct Ext {
+  static constexpr int ex = NX + 2 * S, ey = NDIM > 1 ? NY + 2 * S : 1, ez = NDIM > 2 ? NZ + 2 * S : 1;
+  static constexpr int n = ex * ey * ez;
+  __device__ static __forceinline__ int idx(int i, int j, int k) {
+    return ((k + (NDIM > 2 ? S : 0)) * ey + (j + (NDIM > 1 ? S : 0))) * ex + (i + S);
+  }
+  __device__ static __forceinline__ void decode(int c, int &i, int &j, int &k) {
+    i = c % ex - S;
+    j = NDIM > 1 ? (c / ex) % ey - S : 0;
+    k = NDIM > 2 ? c / (ex * ey) - S : 0;
+  }
+};
+
+template <int NDIM, int NX, int NY, int NZ>
+struct SigGeom {
+  using B = Box<NDIM, NX, NY, NZ>;
+  using E = Ext<NDIM, NX, NY, NZ, 2>;
+  // velocities of the box cells, one species on the box plus one layer
+  static constexpr size_t smem_bytes() { return ((size_t)3 * B::n + E::n) * sizeof(double); }
+};
+
 template <int NDIM, int NX, int NY, int NZ>
 __global__ void __launch_bounds__(256) k_spec_sig(const DevParams P, double *__restrict__ SSIG, size_t ncells) {
   using B = Box<NDIM, NX, NY, NZ>;
+  using E = Ext<NDIM, NX, NY, NZ, 2>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double *sV = reinterpret_cast<double *>(smem_raw);     // [3][B::n]
+  double *sX = sV + 3 * B::n;                            // [E::n]
   const int b = P.blk_list ? P.blk_list[blockIdx.x] : blockIdx.x;
   const int3 bc = blk_coords(P, b);
   for (int c = threadIdx.x; c < B::n; c += blockDim.x) {
     const int i = c % B::bx - 1, j = NDIM > 1 ? (c / B::bx) % B::by - 1 : 0;
     const int k = NDIM > 2 ? c / (B::bx * B::by) - 1 : 0;
+    bool inside; int f[3];
+    const size_t o = cell_src<NDIM, NX, NY, NZ>(P, b, bc, i, j, k, inside, f[0], f[1], f[2]);
 #pragma unroll
     for (int d = 0; d < NDIM; ++d) {
-      const int di = d == 0, dj = d == 1, dk = d == 2;
-      const double lam = load_vel<NDIM, NX, NY, NZ>(P, b, bc, i, j, k, d);
-      for (int q = 0; q < P.nsp; ++q) {
-        const double sm = load_spec<NDIM, NX, NY, NZ>(P, b, bc, i - di, j - dj, k - dk, q, ncells);
-        const double s0 = load_spec<NDIM, NX, NY, NZ>(P, b, bc, i, j, k, q, ncells);
-        const double sp = load_spec<NDIM, NX, NY, NZ>(P, b, bc, i + di, j + dj, k + dk, q, ncells);
+      const double v = __ldg(P.s_in[1 + d] + o);
+      sV[d * B::n + c] = f[d] ? -v : v;
+    }
+  }
+  for (int q = 0; q < P.nsp; ++q) {
+    for (int c = threadIdx.x; c < E::n; c += blockDim.x) {
+      int i, j, k;
+      E::decode(c, i, j, k);
+      sX[c] = load_spec<NDIM, NX, NY, NZ>(P, b, bc, i, j, k, q, ncells);
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < B::n; c += blockDim.x) {
+      const int i = c % B::bx - 1, j = NDIM > 1 ? (c / B::bx) % B::by - 1 : 0;
+      const int k = NDIM > 2 ? c / (B::bx * B::by) - 1 : 0;
+      const int e = E::idx(i, j, k);
+#pragma unroll
+      for (int d = 0; d < NDIM; ++d) {
+        const int st = d == 0 ? 1 : (d == 1 ? E::ex : E::ex * E::ey);
+        const double lam = sV[d * B::n + c];
+        const double sm = sX[e - st], s0 = sX[e], sp = sX[e + st];
         double g;
         if (lam > 0.) g = s0 - sm;
         else g = sp - s0;
         SSIG[(((size_t)blockIdx.x * NDIM + d) * P.nsp + q) * B::n + c] = lam * g;
       }
     }
+    __syncthreads();
   }
 }
 
 template <int NDIM, int NX, int NY, int NZ, int DIR>
 struct SpecGeom {
   using L = DirGeom<NDIM, NX, NY, NZ, double, DIR>;
+  // one species staged on the lines with 3 cells beyond the block along DIR
+  static constexpr int sx = DIR == 1 ? NX + 6 : NX, sy = NDIM > 1 ? (DIR == 2 ? NY + 6 : NY) : 1,
+                       sz = NDIM > 2 ? (DIR == 3 ? NZ + 6 : NZ) : 1;
+  static constexpr int ns = sx * sy * sz;
+  static constexpr int sstep = DIR == 1 ? 1 : (DIR == 2 ? sx : sx * sy);
+  __device__ static __forceinline__ int sidx(int i, int j, int k) {
+    return ((k + 3 * (DIR == 3)) * sy + (j + 3 * (DIR == 2))) * sx + (i + 3 * (DIR == 1));
+  }
   // shared memory: per line cell the face values of one species (left,
   // right), the normal velocity, the flattening coefficient, the velocities
-  // along the two CTU axes and the fallback flag
-  static constexpr size_t smem_bytes() { return (size_t)L::n * (6 * sizeof(double) + 1); }
+  // along the two CTU axes and the fallback flag; the staged species
+  static constexpr size_t smem_bytes() { return (size_t)L::n * 6 * sizeof(double) + (size_t)ns * sizeof(double) + L::n; }
 };
 
 template <int NDIM, int NX, int NY, int NZ, int DIR, bool FIRST, bool LAST>
@@ -93,6 +146,7 @@ __global__ void __launch_bounds__(256) k_spec_dir(const DevParams P, const doubl
   using L = DirGeom<NDIM, NX, NY, NZ, double, DIR>;
   using B = Box<NDIM, NX, NY, NZ>;
   constexpr int NCB = NX * NY * NZ;
+  using SG = SpecGeom<NDIM, NX, NY, NZ, DIR>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double *sSl = reinterpret_cast<double *>(smem_raw);
   double *sSr = sSl + L::n;
@@ -100,7 +154,8 @@ __global__ void __launch_bounds__(256) k_spec_dir(const DevParams P, const doubl
   double *sFl = sU + L::n;            // flattening coefficient
   double *sA1 = sFl + L::n;           // velocities along the CTU axes A1, A2
   double *sA2 = sA1 + L::n;
-  unsigned char *sFb = reinterpret_cast<unsigned char *>(sA2 + L::n);
+  double *sX = sA2 + L::n;            // the staged species
+  unsigned char *sFb = reinterpret_cast<unsigned char *>(sX + SG::ns);
   const int b = P.blk_list ? P.blk_list[blockIdx.x] : blockIdx.x;
   const int3 bc = blk_coords(P, b);
   const double dt = P.dt_dev ? *P.dt_dev : P.dt;
@@ -117,25 +172,8 @@ __global__ void __launch_bounds__(256) k_spec_dir(const DevParams P, const doubl
   for (int t = threadIdx.x; t < L::n; t += blockDim.x) {
     int i, j, k;
     L::decode(t, i, j, k);
-    const int di = DIR == 1, dj = DIR == 2, dk = DIR == 3;
     sU[t] = load_vel<NDIM, NX, NY, NZ>(P, b, bc, i, j, k, DIR - 1);
-    double flat = 0.;
-    if (P.use_flattening) {
-      double p7[7], u7[7], V[8];
-#pragma unroll
-      for (int s = -3; s <= 3; ++s) {
-        if (s == -3 || s == 3) {
-          p7[s + 3] = load_pres<NDIM, NX, NY, NZ>(P, b, bc, i + s * di, j + s * dj, k + s * dk);
-          u7[s + 3] = 0.;
-        } else {
-          load_prim<NDIM, NX, NY, NZ, false>(P, b, bc, i + s * di, j + s * dj, k + s * dk, V);
-          p7[s + 3] = V[HP];
-          u7[s + 3] = V[Slots<DIR>::v1];
-        }
-      }
-      flat = flat_coeff(p7, u7);
-    }
-    sFl[t] = flat;
+    sFl[t] = P.use_flattening ? P.sp_flat[lb + t] : 0.;   // left by the hydro direction kernel
     if (ctu) {
       sA1[t] = load_vel<NDIM, NX, NY, NZ>(P, b, bc, i, j, k, A1 - 1);
       sA2[t] = load_vel<NDIM, NX, NY, NZ>(P, b, bc, i, j, k, A2 - 1);
@@ -150,15 +188,21 @@ __global__ void __launch_bounds__(256) k_spec_dir(const DevParams P, const doubl
   for (int q = 0; q < P.nsp; ++q) {
     const double *sig = ssb + (size_t)q * B::n;           // + d * nsp * B::n for direction d
     const size_t dstr = (size_t)P.nsp * B::n;
+    // ---- stage the species on the lines, 3 cells beyond the block along DIR
+    for (int c = threadIdx.x; c < SG::ns; c += blockDim.x) {
+      const int i = c % SG::sx - 3 * (DIR == 1), j = NDIM > 1 ? (c / SG::sx) % SG::sy - 3 * (DIR == 2) : 0;
+      const int k = NDIM > 2 ? c / (SG::sx * SG::sy) - 3 * (DIR == 3) : 0;
+      sX[c] = load_spec<NDIM, NX, NY, NZ>(P, b, bc, i, j, k, q, ncells);
+    }
+    __syncthreads();
     // ---- face values of the line cells
     for (int t = threadIdx.x; t < L::n; t += blockDim.x) {
       int i, j, k;
       L::decode(t, i, j, k);
-      const int di = DIR == 1, dj = DIR == 2, dk = DIR == 3;
+      const int e = SG::sidx(i, j, k);
       double S[5];
 #pragma unroll
-      for (int s = -2; s <= 2; ++s)
-        S[s + 2] = load_spec<NDIM, NX, NY, NZ>(P, b, bc, i + s * di, j + s * dj, k + s * dk, q, ncells);
+      for (int s = -2; s <= 2; ++s) S[s + 2] = sX[e + s * SG::sstep];
       const double Smm = S[0], Sm = S[1], Sc = S[2], Sp = S[3], Spp = S[4];
       const double lam = sU[t];
       double dP = minmod_s(Sp - Sc, Spp - Sp);
