@@ -41,6 +41,8 @@ FLASH_UHD_VARS = ("dens", "eint", "ener", "gamc", "game", "pres", "shok", "temp"
 
 
 MAX_SPECIES = 16
+# refinement variables of flash_hy_estimate_error (FLASH_HY_REFVAR_*)
+REFVAR = {"dens": 1, "pres": 2, "velx": 3, "vely": 4, "velz": 5, "eint": 6}
 
 
 def flash_varmap(nsp=0):
@@ -157,6 +159,8 @@ def _set_sigs(lib):
         "flash_hy_get_fluxes": (C.c_int, [vp, C.c_int, C.c_int, dp]),
         "flash_hy_put_fluxes": (C.c_int, [vp, C.c_int, C.c_int, dp]),
         "flash_hy_update_solution": (C.c_int, [vp, C.c_int, ip, C.c_double]),
+        "flash_hy_estimate_error": (C.c_int, [vp, C.c_int, C.c_double, dp]),
+        "flash_hy_regrid": (C.c_int, [vp, vp, C.c_int, ip, ip]),
         "flash_hy_get_tuning": (C.c_int, [vp, C.POINTER(Tuning)]),
         "flash_hy_set_tuning": (C.c_int, [vp, C.POINTER(Tuning)]),
         "flash_hy_tuning_candidates": (C.c_int, [vp, ip, ip, ip, ip, ip, ip]),

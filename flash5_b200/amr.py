@@ -15,6 +15,7 @@ UNK array holds every node (shape (nblocks, nzt, nyt, nxt, NUNK)), like
 FLASH's unk(:,:,:,:,1:lnblocks) with parents included.
 """
 import ctypes as C
+import copy
 import itertools
 
 import numpy as np
@@ -305,3 +306,127 @@ def four_quadrant_hierarchy(nb=16, nblk=32, max_level=4, threshold=0.0035, seed=
     g = AmrGrid(2, (nb, nb), (nblk, nblk), max_level, bc=bc)
     g.refine_levels(indicator_refiner(g, four_quadrant_refinement_field(seed), threshold))
     return g
+
+
+# -- refinement and derefinement (Grid_markRefineDerefine, gr_updateRefinement) --
+
+def mark_refine_derefine(grid, errors, refine_cutoff, derefine_cutoff, max_refine=None):
+    """Refine / derefine flags of every node from the estimator's errors,
+    one array per refinement variable (Grid/GridMain/AMR/
+    Grid_markRefineDerefine.F90 and paramesh4/gr_markRefineDerefine.F90):
+    per variable, a leaf is marked for derefinement when it is not marked
+    for refinement or to stay and both its error and its parent's are at or
+    below the derefine cutoff; any node above the refine cutoff is marked
+    for refinement (not above max_refine); a leaf above the derefine cutoff
+    or under a parent above it stays.  Only leaves keep their marks.
+    refine_cutoff / derefine_cutoff: scalars or one value per variable."""
+    n = grid.nblocks
+    nv = len(errors)
+    rc = np.broadcast_to(np.asarray(refine_cutoff, dtype=np.float64), (nv,))
+    dc = np.broadcast_to(np.asarray(derefine_cutoff, dtype=np.float64), (nv,))
+    max_refine = grid.max_level if max_refine is None else int(max_refine)
+    refine = np.zeros(n, dtype=bool)
+    derefine = np.zeros(n, dtype=bool)
+    stay = np.zeros(n, dtype=bool)
+    leaf = grid.is_leaf
+    for v in range(nv):
+        err = np.asarray(errors[v], dtype=np.float64)
+        err_par = np.where(grid.parent >= 0, err[np.maximum(grid.parent, 0)], 0.0)
+        for b in range(n):
+            if leaf[b] and not refine[b] and not stay[b] and err[b] <= dc[v] and err_par[b] <= dc[v]:
+                derefine[b] = True
+            else:
+                derefine[b] = False
+            if err[b] > rc[v]:
+                derefine[b] = False
+                refine[b] = True
+            if (leaf[b] and err[b] > dc[v]) or err_par[b] > dc[v]:
+                stay[b] = True
+            if grid.levels[b] >= max_refine:
+                refine[b] = False
+    refine &= leaf
+    derefine &= leaf
+    return refine, derefine
+
+
+def _clone(grid):
+    g = copy.copy(grid)
+    g._leaves = set(grid._leaves)
+    g._inner = set(grid._inner)
+    return g
+
+
+def regrid(grid, refine, derefine, min_level=1):
+    """The hierarchy after the marked refinements and derefinements, with
+    PARAMESH's rules: a marked leaf below max_level is split and refinement
+    spreads to keep neighbours (diagonals included) within one level; a
+    parent's children are removed when all of them are leaves marked for
+    derefinement that were not refined, the parent is above min_level - 1
+    and no neighbour of the parent would be two levels finer.  Returns
+    (new grid, src, how): for every new node, how = 0 copies old node src,
+    1 is a new child of old leaf src (prolonged), 2 is old parent src made a
+    leaf (derefined)."""
+    old = grid
+    g = _clone(old)
+    key_of = {i: k for k, i in old.node_index.items()}
+    for b in np.nonzero(np.asarray(refine) & old.is_leaf)[0]:
+        key = key_of[int(b)]
+        if key[0] < g.max_level:
+            g._split(key)
+    g._balance()
+    # derefinement, judged on the tree after refinement: candidates are the
+    # parents all of whose children are unrefined marked leaves; a candidate
+    # is dropped while a neighbour's child touching it stays refined (is not
+    # a candidate itself), until the set no longer changes
+    offs = [o for o in itertools.product((-1, 0, 1), repeat=g.ndim) if any(o)]
+    dmark = {key_of[int(b)] for b in np.nonzero(np.asarray(derefine) & old.is_leaf)[0]}
+    cand = set()
+    for pkey in old._inner:
+        lev, pc = pkey
+        if lev >= min_level and all(k in g._leaves and k in dmark for k in g._children(lev, pc)):
+            cand.add(pkey)
+
+    def blocked(pkey):
+        lev, pc = pkey
+        for o in offs:
+            o3 = tuple(o) + (0,) * (3 - g.ndim)
+            nkey = g._neighbor(lev, pc, o3)
+            if nkey is None or (lev, nkey) not in g._inner:
+                continue
+            for ch in g._children(lev, nkey):
+                touch = all(not ((o3[d] == 1 and ch[1][d] - 2 * nkey[d] != 0) or
+                                 (o3[d] == -1 and ch[1][d] - 2 * nkey[d] != 1)) for d in range(g.ndim))
+                if touch and ch in g._inner and ch not in cand:
+                    return True
+        return False
+
+    changed = True
+    while changed:
+        changed = False
+        for pkey in sorted(cand):
+            if blocked(pkey):
+                cand.discard(pkey)
+                changed = True
+    merge = sorted(cand)
+    for pkey in merge:
+        for k in g._children(*pkey):
+            g._leaves.discard(k)
+        g._inner.discard(pkey)
+        g._leaves.add(pkey)
+    g._finalize()
+    new_key = {i: k for k, i in g.node_index.items()}
+    src = np.empty(g.nblocks, dtype=np.int32)
+    how = np.empty(g.nblocks, dtype=np.int32)
+    for q in range(g.nblocks):
+        key = new_key[q]
+        if key in old.node_index:
+            src[q] = old.node_index[key]
+            how[q] = 2 if (key in old._inner and key in g._leaves) else 0
+        else:
+            lev, c = key
+            pkey = (lev - 1, tuple(v // 2 if d < g.ndim else 0 for d, v in enumerate(c)))
+            if pkey not in old._leaves:
+                raise RuntimeError("regrid created a node two levels below the old tree")
+            src[q] = old.node_index[pkey]
+            how[q] = 1
+    return g, src, how

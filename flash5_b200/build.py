@@ -29,6 +29,7 @@ UNITS = [
     ("riemann_exact.o", "riemann_exact.cu", ["--fmad=true"]),
     ("cfl_noalloc.o", "cfl_noalloc.cu", ["--fmad=false"]),
     ("spec.o", "spec.cu", ["--fmad=false"]),
+    ("refine.o", "refine.cu", ["--fmad=false"]),
 ]
 
 

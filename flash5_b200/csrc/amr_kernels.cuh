@@ -73,6 +73,52 @@ __global__ void __launch_bounds__(256) k_restrict(DevParams P, double *st0, doub
   }
 }
 
+// Linear prolongation (amr_1blk_cc_prol_linear.F90 with the weights and
+// indices of amr_prolong_cc_fun_init.F90) of child cell lp of the node at
+// coordinates c from its parent's guard-inclusive copy gp ([6][Halo::n]:
+// rho, vx, vy, vz, e, E), in per-volume form.
+template <int NDIM, int NX, int NY, int NZ>
+__device__ __forceinline__ void prolong_linear(const double *gp, const int c[3], const int lp[3], double out[6]) {
+  using H = Halo<NDIM, NX, NY, NZ>;
+  const int Nd[3] = {NX, NY, NZ};
+  int i1[3] = {0, 0, 0};
+  double wx[3] = {1., 1., 1.}, cx[3] = {0., 0., 0.};
+#pragma unroll
+  for (int d = 0; d < NDIM; ++d) {
+    const int N = Nd[d], ioff = (c[d] & 1) * (N / 2), ii = lp[d] + 1;
+    i1[d] = (ii + 2 * N) / 2 - N + ioff - 1;
+    wx[d] = fmod(0.75 + (double)(ii + 2 * N) * .5, 1.);
+    cx[d] = 1. - wx[d];
+  }
+  double r[2][2][2][6];
+  for (int kk = 0; kk <= (NDIM > 2 ? 1 : 0); ++kk)
+    for (int jj = 0; jj <= 1; ++jj)
+      for (int ii = 0; ii <= 1; ++ii) {
+        const int h = H::idx(i1[0] + ii, i1[1] + jj, NDIM > 2 ? i1[2] + kk : 0);
+        const double rho = gp[h];
+        r[kk][jj][ii][0] = rho;
+#pragma unroll
+        for (int v = 1; v < 6; ++v) r[kk][jj][ii][v] = rho * gp[v * H::n + h];
+      }
+  double val[6];
+#pragma unroll
+  for (int v = 0; v < 6; ++v) {
+    const double plane0 = wx[1] * (wx[0] * r[0][0][0][v] + cx[0] * r[0][0][1][v]) +
+                          cx[1] * (wx[0] * r[0][1][0][v] + cx[0] * r[0][1][1][v]);
+    if (NDIM > 2) {
+      const double plane1 = wx[1] * (wx[0] * r[1][0][0][v] + cx[0] * r[1][0][1][v]) +
+                            cx[1] * (wx[0] * r[1][1][0][v] + cx[0] * r[1][1][1][v]);
+      val[v] = wx[2] * plane0 + cx[2] * plane1;
+    } else {
+      val[v] = plane0;
+    }
+  }
+  const double inv = 1. / val[0];
+  out[0] = val[0];
+#pragma unroll
+  for (int v = 1; v < 6; ++v) out[v] = inv * val[v];
+}
+
 // (rho, vx, vy, vz, e, E) of guard cell (li, lj, lk) of node n, before the EOS
 template <int NDIM, int NX, int NY, int NZ>
 __device__ void amr_guard(const DevParams &P, const double *const st[5], int n, int li, int lj, int lk, double out[6]) {
@@ -105,44 +151,7 @@ __device__ void amr_guard(const DevParams &P, const double *const st[5], int n, 
     out[5] = node_E(P, m, off, out[4], out[1], out[2], out[3]);
   } else {
     // linear prolongation from the parent's guard-inclusive copy
-    const int p = P.parent[n];
-    const double *gp = P.gp + (size_t)P.slot[p] * 6 * H::n;
-    int i1[3] = {0, 0, 0};
-    double wx[3] = {1., 1., 1.}, cx[3] = {0., 0., 0.};
-#pragma unroll
-    for (int d = 0; d < NDIM; ++d) {
-      const int N = Nd[d], ioff = (c[d] & 1) * (N / 2), ii = lp[d] + 1;
-      i1[d] = (ii + 2 * N) / 2 - N + ioff - 1;
-      wx[d] = fmod(0.75 + (double)(ii + 2 * N) * .5, 1.);
-      cx[d] = 1. - wx[d];
-    }
-    double r[2][2][2][6];
-    for (int kk = 0; kk <= (NDIM > 2 ? 1 : 0); ++kk)
-      for (int jj = 0; jj <= 1; ++jj)
-        for (int ii = 0; ii <= 1; ++ii) {
-          const int h = H::idx(i1[0] + ii, i1[1] + jj, NDIM > 2 ? i1[2] + kk : 0);
-          const double rho = gp[h];
-          r[kk][jj][ii][0] = rho;
-#pragma unroll
-          for (int v = 1; v < 6; ++v) r[kk][jj][ii][v] = rho * gp[v * H::n + h];
-        }
-    double val[6];
-#pragma unroll
-    for (int v = 0; v < 6; ++v) {
-      const double plane0 = wx[1] * (wx[0] * r[0][0][0][v] + cx[0] * r[0][0][1][v]) +
-                            cx[1] * (wx[0] * r[0][1][0][v] + cx[0] * r[0][1][1][v]);
-      if (NDIM > 2) {
-        const double plane1 = wx[1] * (wx[0] * r[1][0][0][v] + cx[0] * r[1][0][1][v]) +
-                              cx[1] * (wx[0] * r[1][1][0][v] + cx[0] * r[1][1][1][v]);
-        val[v] = wx[2] * plane0 + cx[2] * plane1;
-      } else {
-        val[v] = plane0;
-      }
-    }
-    const double inv = 1. / val[0];
-    out[0] = val[0];
-#pragma unroll
-    for (int v = 1; v < 6; ++v) out[v] = inv * val[v];
+    prolong_linear<NDIM, NX, NY, NZ>(P.gp + (size_t)P.slot[P.parent[n]] * 6 * H::n, c, lp, out);
   }
   if (flip[0]) out[1] = -out[1];
   if (flip[1]) out[2] = -out[2];

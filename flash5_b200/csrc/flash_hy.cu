@@ -78,6 +78,7 @@ struct flash_hy_ctx {
   int nsp, nspec;
   double *spec[2], *sacc, *ssig, *sp_mf, *sp_flat;
   unsigned char *sp_fb;
+  double *d_err;               // refinement criterion per block
   char err[512];
 };
 
@@ -430,6 +431,7 @@ extern "C" int flash_hy_destroy(flash_hy_ctx *c) {
   cudaFree(c->d_fstore);
   for (int s = 0; s < 2; ++s) cudaFree(c->spec[s]);
   cudaFree(c->sacc); cudaFree(c->ssig); cudaFree(c->sp_mf); cudaFree(c->sp_fb); cudaFree(c->sp_flat);
+  cudaFree(c->d_err);
   free(c->h_blk_at);
   if (c->h_dt) cudaFreeHost(c->h_dt);
   if (c->h_status) cudaFreeHost(c->h_status);
@@ -1103,6 +1105,97 @@ done:
   c->plain_steps[0] = c->plain_steps[1] = 0;
   if (n_trials) *n_trials = nt;
   if (best) flash_hy_get_tuning(c, best);
+  return rc;
+}
+
+// ---------------------------------------------------------------------------
+// refinement criterion (gr_estimateError)
+// ---------------------------------------------------------------------------
+extern "C" int flash_hy_estimate_error(flash_hy_ctx *c, int var, double refine_filter, double *err) {
+  if (!c || !err || var < FLASH_HY_REFVAR_DENS || var > FLASH_HY_REFVAR_EINT || c->ndim < 2)
+    return FLASH_HY_ERR_BAD_ARG;
+  if (c->partial && c->n_owned == 0)
+    return fail(c, FLASH_HY_ERR_UNSUPPORTED, "a partial grid needs its owned blocks (flash_hy_set_owned_blocks)%s", "");
+  CUDA_OK(c, cudaSetDevice(c->device));
+  if (!c->d_err) CUDA_OK(c, cudaMalloc((void **)&c->d_err, (size_t)c->nblocks * sizeof(double)));
+  CUDA_OK(c, cudaMemsetAsync(c->d_err, 0, (size_t)c->nblocks * sizeof(double), c->stream));
+  ErrArgs a;
+  fill_devparams(c, a.P);
+  if (c->amr && amr_prepare(c, a.P) < 0)
+    return fail(c, FLASH_HY_ERR_CUDA, "AMR guard-cell launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  a.var = var;
+  a.filter = refine_filter;
+  // a rank's share: its owned blocks only (ghost blocks lack their neighbours)
+  a.list = c->n_owned ? c->d_owned : nullptr;
+  a.n = c->n_owned ? c->n_owned : c->nblocks;
+  a.err = c->d_err;
+  a.stream = c->stream;
+  if (estimate_error(a, c->ndim, c->nx, c->ny, c->nz) < 0)
+    return fail(c, FLASH_HY_ERR_CUDA, "estimator launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  CUDA_OK(c, cudaMemcpyAsync(err, c->d_err, (size_t)c->nblocks * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_OK(c, cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// regrid: data of a new hierarchy from an old one (gr_updateRefinement)
+// ---------------------------------------------------------------------------
+extern "C" int flash_hy_regrid(flash_hy_ctx *old, flash_hy_ctx *nw, int n, const int *src, const int *how) {
+  if (!old || !nw || !src || !how || old == nw) return FLASH_HY_ERR_BAD_ARG;
+  if (!old->amr || !nw->amr || old->device != nw->device || old->ndim != nw->ndim || old->nx != nw->nx ||
+      old->ny != nw->ny || old->nz != nw->nz || n != nw->nblocks)
+    return fail(nw, FLASH_HY_ERR_BAD_ARG, "regrid: %s", "contexts of different shapes or not AMR hierarchies");
+  std::vector<int> refl, slot(n, -1), of(old->nblocks, -1);
+  std::vector<int> oleaf(old->nblocks);
+  CUDA_OK(old, cudaSetDevice(old->device));
+  CUDA_OK(old, cudaMemcpy(oleaf.data(), old->d_leaf, old->nblocks * sizeof(int), cudaMemcpyDeviceToHost));
+  for (int q = 0; q < n; ++q) {
+    if (src[q] < 0 || src[q] >= old->nblocks || how[q] < 0 || how[q] > 2 || (how[q] == 1 && !oleaf[src[q]]))
+      return fail(nw, FLASH_HY_ERR_BAD_ARG, "regrid: %s", "bad source block or kind");
+    if (how[q] == 1) {
+      if (of[src[q]] < 0) { of[src[q]] = (int)refl.size(); refl.push_back(src[q]); }
+      slot[q] = of[src[q]];
+    }
+  }
+  CUDA_OK(nw, cudaStreamSynchronize(nw->stream));
+  RegridArgs a;
+  fill_devparams(old, a.Po);
+  if (amr_prepare(old, a.Po) < 0)
+    return fail(old, FLASH_HY_ERR_CUDA, "AMR guard-cell launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  fill_devparams(nw, a.Pn);
+  for (int v = 0; v < 5; ++v) a.Pn.s_out[v] = nw->state[nw->cur][v];
+  a.nref = (int)refl.size();
+  a.nnew = n;
+  a.stream = old->stream;
+  int *d_idx = nullptr;
+  double *d_nh = nullptr;
+  const size_t hn = halo_cells(old->ndim, old->nx, old->ny, old->nz);
+  int rc = 0;
+  if (cudaMalloc((void **)&d_idx, (3 * (size_t)n + refl.size() + 1) * sizeof(int)) != cudaSuccess ||
+      (a.nref && cudaMalloc((void **)&d_nh, (size_t)a.nref * 6 * hn * sizeof(double)) != cudaSuccess)) {
+    cudaGetLastError();
+    rc = fail(nw, FLASH_HY_ERR_CUDA, "regrid: %s", "scratch allocation");
+  } else {
+    int *d_src = d_idx, *d_how = d_idx + n, *d_slot = d_idx + 2 * n, *d_refl = d_idx + 3 * n;
+    if (cudaMemcpyAsync(d_src, src, n * sizeof(int), cudaMemcpyHostToDevice, a.stream) != cudaSuccess ||
+        cudaMemcpyAsync(d_how, how, n * sizeof(int), cudaMemcpyHostToDevice, a.stream) != cudaSuccess ||
+        cudaMemcpyAsync(d_slot, slot.data(), n * sizeof(int), cudaMemcpyHostToDevice, a.stream) != cudaSuccess ||
+        (a.nref && cudaMemcpyAsync(d_refl, refl.data(), refl.size() * sizeof(int), cudaMemcpyHostToDevice,
+                                   a.stream) != cudaSuccess)) {
+      rc = fail(nw, FLASH_HY_ERR_CUDA, "regrid: %s", "index copies");
+    } else {
+      a.src = d_src; a.how = d_how; a.slot = d_slot; a.refl = d_refl; a.nh = d_nh;
+      if (regrid_fill(a, old->ndim, old->nx, old->ny, old->nz) < 0)
+        rc = fail(nw, FLASH_HY_ERR_CUDA, "regrid launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    // the copies read pageable host vectors: finish before they go away
+    if (cudaStreamSynchronize(a.stream) != cudaSuccess && !rc) rc = fail(nw, FLASH_HY_ERR_CUDA, "regrid: %s", "sync");
+  }
+  cudaFree(d_idx);
+  cudaFree(d_nh);
+  nw->dt_valid = 0;
+  drop_graphs(nw);
+  nw->plain_steps[0] = nw->plain_steps[1] = 0;
   return rc;
 }
 

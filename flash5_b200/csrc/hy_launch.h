@@ -2,6 +2,7 @@
 // variants (hy_variant.cu, compiled once per arithmetic variant).
 #pragma once
 #include "hy_kernels.cuh"
+#include "../../include/flash_hy.h"
 
 namespace fhy {
 
@@ -39,6 +40,32 @@ struct SpecArgs {
 };
 // launches k_spec_sig + one k_spec_dir per direction; returns their number or -2
 int spec_step(const SpecArgs &a, int ndim, int nx, int ny, int nz);
+
+// the refinement criterion of every listed block (all blocks without a list)
+struct ErrArgs {
+  DevParams P;
+  int var;            // FLASH_HY_REFVAR_*
+  double filter;      // refine_filter
+  const int *list;
+  int n;
+  double *err;        // device, indexed by block
+  cudaStream_t stream;
+};
+int estimate_error(const ErrArgs &a, int ndim, int nx, int ny, int nz);
+
+// data movement of a regrid from an old AMR context to a new one
+struct RegridArgs {
+  DevParams Po;            // old context after its guard fill (s_in = its state)
+  DevParams Pn;            // new context (s_out = the state to fill, pe, leaf)
+  const int *refl;         // old leaves whose children are created
+  int nref;
+  double *nh;              // [nref][6][halo] their guard-inclusive copies
+  const int *src, *how, *slot;  // per new node; slot = index into refl (how 1)
+  int nnew;
+  cudaStream_t stream;
+};
+int regrid_fill(const RegridArgs &a, int ndim, int nx, int ny, int nz);
+size_t halo_cells(int ndim, int nx, int ny, int nz);
 
 // Enqueue one hydro step; returns the number of kernel launches, or -1 for an
 // unsupported block shape, or -2 for a launch error.

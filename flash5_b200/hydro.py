@@ -118,6 +118,30 @@ class Hydro:
     def sync(self):
         self._check(self.lib.flash_hy_sync(self.ctx))
 
+    # -- refinement ---------------------------------------------------------
+    def estimate_error(self, var="dens", refine_filter=0.01):
+        """gr_estimateError: Lohner's estimator of `var` for every block
+        (numpy array indexed by block; 0 for ghost blocks of a rank's share)."""
+        err = np.zeros(self.grid.nblocks, dtype=np.float64)
+        self._check(self.lib.flash_hy_estimate_error(self.ctx, abi.REFVAR[var], float(refine_filter),
+                                                      err.ctypes.data_as(C.POINTER(C.c_double))))
+        return err
+
+    def regrid(self, new_grid, src, how):
+        """gr_updateRefinement's data movement: a new context for new_grid
+        (amr.regrid's tree) filled from this one; this context is left as it
+        was (its parents restricted)."""
+        h = Hydro(self.params, new_grid, device=self.device)
+        s = np.ascontiguousarray(src, dtype=np.int32)
+        w = np.ascontiguousarray(how, dtype=np.int32)
+        st = self.lib.flash_hy_regrid(self.ctx, h.ctx, len(s), s.ctypes.data_as(C.POINTER(C.c_int)),
+                                      w.ctypes.data_as(C.POINTER(C.c_int)))
+        if st:
+            msg = h.last_error() or self.last_error()
+            h.close()
+            raise HydroError(st, msg)
+        return h
+
     # -- launch shapes ----------------------------------------------------
     @property
     def tuning(self):

@@ -228,6 +228,38 @@ int flash_hy_set_exchange(flash_hy_ctx *ctx, int nsend, const int *send_blocks, 
 int flash_hy_pack(flash_hy_ctx *ctx, double *d_buf);
 int flash_hy_unpack(flash_hy_ctx *ctx, const double *d_buf);
 
+/* ---- refinement criterion ------------------------------------------------
+ * gr_estimateError / gr_estimateBlkError (Grid/GridMain/AMR/
+ * gr_estimateBlkError.F90, Cartesian): Lohner's normalised second-derivative
+ * estimator of one variable for every block, leaves and parents (FLASH's
+ * ACTIVE_BLKS), after the guard-cell fill with EOS that
+ * Grid_markRefineDerefine.F90 performs.  err (HOST, nblocks doubles)
+ * receives sqrt(max over the cells of num / denom) per block; HUGE where a
+ * cell has denom = 0 and num != 0.  The pressure is (gamma-1) rho e of each
+ * cell (parents: of their restricted state).  Uniform grids and AMR
+ * hierarchies.                                                          */
+#define FLASH_HY_REFVAR_DENS 1
+#define FLASH_HY_REFVAR_PRES 2
+#define FLASH_HY_REFVAR_VELX 3
+#define FLASH_HY_REFVAR_VELY 4
+#define FLASH_HY_REFVAR_VELZ 5
+#define FLASH_HY_REFVAR_EINT 6
+int flash_hy_estimate_error(flash_hy_ctx *ctx, int var, double refine_filter, double *err);
+
+/* ---- regrid --------------------------------------------------------------
+ * gr_updateRefinement (Grid/GridMain/AMR/paramesh/gr_updateRefinement.F90:
+ * 112-238) after the host has marked blocks (gr_markRefineDerefine) and
+ * built the new tree: fills the state of context new_ctx (created for the
+ * new hierarchy) from old_ctx.  For every new node q: how[q] = 0 copies old
+ * node src[q] (a kept node, or a refined leaf that becomes a parent); 2
+ * turns old parent src[q] into a leaf with its restricted data
+ * (derefinement); 1 prolongs new child q from old leaf src[q]
+ * (amr_prolong: linear prolongation in per-volume form from the old leaf
+ * with its guard cells in the old hierarchy).  Then the EOS on every leaf,
+ * as FLASH does after a grid change.  Both contexts must be AMR
+ * hierarchies of the same block shape on the same device.               */
+int flash_hy_regrid(flash_hy_ctx *old_ctx, flash_hy_ctx *new_ctx, int n, const int *src, const int *how);
+
 /* ---- launch shapes and their autotuner ----------------------------------
  * No FLASH5 counterpart (FLASH picks no launch shapes; its block loop is
  * Hydro.F90:156-229).  Threads per CTA of the step's kernels: the

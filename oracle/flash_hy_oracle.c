@@ -1588,3 +1588,215 @@ int orc_block_fluxes(const flash_hy_params *p, const flash_hy_grid_desc *g, doub
   work_free(&w);
   return c.status;
 }
+
+
+/* ===================================================================== */
+/* Refinement criterion: Lohner's estimator of gr_estimateBlkError.F90    */
+/* (Cartesian) for every block (leaves and parents, FLASH's ACTIVE_BLKS), */
+/* after the guard-cell fill of Grid_markRefineDerefine.F90 (EOS on the   */
+/* guard cells).  var: FLASH_HY_REFVAR_*; the pressure is (gamma-1) rho e */
+/* of the cell.  err[b] = sqrt(max over cells of num/denom), HUGE where   */
+/* denom vanishes with num != 0 (gr_estimateBlkError.F90 :300-315).       */
+/* ===================================================================== */
+static double refvar_of(const ctx_t *c, const double *u, int var, int eos_rule) {
+  double e = u[EINT_V];
+  if (eos_rule && (var == FLASH_HY_REFVAR_PRES || var == FLASH_HY_REFVAR_EINT)) {
+    double ekin = 0.5 * (u[VELX_V] * u[VELX_V] + u[VELY_V] * u[VELY_V] + u[VELZ_V] * u[VELZ_V]);
+    if (u[ENER_V] - ekin > fmax2(c->p->smalle, c->p->eint_switch * ekin)) e = u[ENER_V] - ekin;
+  }
+  switch (var) {
+    case FLASH_HY_REFVAR_DENS: return u[DENS_V];
+    case FLASH_HY_REFVAR_PRES: return u[DENS_V] * e * c->gam1inv;
+    case FLASH_HY_REFVAR_VELX: return u[VELX_V];
+    case FLASH_HY_REFVAR_VELY: return u[VELY_V];
+    case FLASH_HY_REFVAR_VELZ: return u[VELZ_V];
+    default: return e;
+  }
+}
+
+static double estimate_block(const ctx_t *c, const double *V, const double delta[3], const int bnd[3][2],
+                             double filter) {
+  const int nd = c->ndim;
+  double del[3] = {0., 0., 0.};
+  for (int d = 0; d < nd; ++d) del[d] = 0.5e0 / delta[d];
+  int st[3] = {1, c->nxt, c->nxt * c->nyt};
+  int bs[3] = {0, 0, 0}, be[3] = {0, 0, 0};
+  int nt[3] = {c->nxt, c->nyt, c->nzt};
+  for (int d = 0; d < nd; ++d) {
+    bs[d] = bnd[d][0] ? NGUARD : NGUARD - 2;
+    be[d] = bnd[d][1] ? nt[d] - 1 - NGUARD : nt[d] - 1 - (NGUARD - 2);
+  }
+  double err = 0.;
+  int huge = 0;
+  for (int k = bs[2]; k <= be[2]; ++k)
+    for (int j = bs[1]; j <= be[1]; ++j)
+      for (int i = bs[0]; i <= be[0]; ++i) {
+        const size_t c0 = cidx(c, i, j, k);
+        /* first derivatives delu(a), delua(a) at cell c0 + o */
+#define DU(a, o) ((V[c0 + (o) + st[a]] - V[c0 + (o) - st[a]]) * del[a])
+#define DA(a, o) ((fabs(V[c0 + (o) + st[a]]) + fabs(V[c0 + (o) - st[a]])) * del[a])
+        double d2[9], d3[9], d4[9];
+        int nk = 0;
+        /* (first-derivative axis a, second-difference axis b) in the order of :182-292 */
+        static const int A2[4][2] = {{0, 0}, {0, 1}, {1, 0}, {1, 1}};
+        static const int A3[9][2] = {{0, 0}, {0, 1}, {1, 0}, {1, 1}, {0, 2}, {1, 2}, {2, 0}, {2, 1}, {2, 2}};
+        const int (*A)[2] = nd == 3 ? A3 : A2;
+        nk = nd == 3 ? 9 : 4;
+        for (int q = 0; q < nk; ++q) {
+          int a = A[q][0], bb = A[q][1];
+          d2[q] = (DU(a, st[bb]) - DU(a, -st[bb])) * del[bb];
+          d3[q] = (fabs(DU(a, st[bb])) + fabs(DU(a, -st[bb]))) * del[bb];
+          d4[q] = (DA(a, st[bb]) + DA(a, -st[bb])) * del[bb];
+        }
+#undef DU
+#undef DA
+        double num = 0., denom = 0.;
+        for (int q = 0; q < nk; ++q) {
+          num = num + d2[q] * d2[q];
+          denom = denom + (d3[q] + (filter * d4[q])) * (d3[q] + (filter * d4[q]));
+        }
+        if (denom == 0.0 && num != 0.0) huge = 1;
+        else if (denom != 0.0) err = fmax2(err, num / denom);
+      }
+  return sqrt(huge ? DBL_MAX : err);
+}
+
+int orc_estimate_error(const flash_hy_params *p, const flash_hy_grid_desc *g, double *unk, int var, double filter,
+                       double *err) {
+  if (var < FLASH_HY_REFVAR_DENS || var > FLASH_HY_REFVAR_EINT || (g->ndim < 2)) return FLASH_HY_ERR_BAD_ARG;
+  ctx_t c; ctx_init(&c, p, g);
+  size_t bsz = (size_t)c.nxt * c.nyt * c.nzt * c.nunk;
+  const int amr = g->max_level > 1;
+  amr_t a;
+  int st = 0;
+  if (amr) {
+    if ((st = amr_build(g, &a))) return st;
+    amr_fill_all(p, g, &a, unk);
+  } else if ((st = orc_fill_guardcells(p, g, unk))) {
+    return st;
+  }
+  double del0[3];
+  block_deltas(g, del0);
+  #pragma omp parallel for schedule(dynamic)
+  for (int b = 0; b < g->nblocks; ++b) {
+    const int l = amr ? a.level[b] : 1;
+    const int parent = amr && !a.leaf[b];
+    double delta[3];
+    for (int d = 0; d < 3; ++d) delta[d] = d < g->ndim ? ldexp(del0[d], 1 - l) : 1.;
+    int bnd[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+    for (int d = 0; d < g->ndim; ++d) {
+      int ext = amr ? a.ext[l][d] : g->nblk_l1[d];
+      int cd = g->block_coords[3 * b + d];
+      bnd[d][0] = cd == 0 && g->bc[2 * d] != FLASH_HY_BC_PERIODIC;
+      bnd[d][1] = cd == ext - 1 && g->bc[2 * d + 1] != FLASH_HY_BC_PERIODIC;
+    }
+    size_t ncell = (size_t)c.nxt * c.nyt * c.nzt;
+    double *V = malloc(sizeof(double) * ncell);
+    for (int k = 0; k < c.nzt; ++k)
+      for (int j = 0; j < c.nyt; ++j)
+        for (int i = 0; i < c.nxt; ++i) {
+          int li = i - NGUARD, lj = c.k2 ? j - NGUARD : 0, lk = c.k3 ? k - NGUARD : 0;
+          int inside = li >= 0 && li < c.nxb && lj >= 0 && lj < c.nyb && lk >= 0 && lk < c.nzb;
+          V[cidx(&c, i, j, k)] = refvar_of(&c, &unk[b * bsz + cidx(&c, i, j, k) * c.nunk], var, parent && !inside);
+        }
+    err[b] = estimate_block(&c, V, delta, (const int (*)[2])bnd, filter);
+    free(V);
+  }
+  if (amr) amr_free(&a);
+  return 0;
+}
+
+
+/* ===================================================================== */
+/* Data of a regridded hierarchy (gr_updateRefinement.F90:112-238): for  */
+/* every new node, how = 0 copies old node src (kept leaves and parents; */
+/* a refined leaf keeps its data as the new parent), how = 2 turns old   */
+/* parent src into a leaf with its restricted data (derefinement), how = */
+/* 1 fills a new child of old leaf src by amr_prolong: linear            */
+/* prolongation (amr_1blk_cc_prol_linear, per-volume form) from the old  */
+/* leaf with its guard cells of the old hierarchy.  Then the EOS on      */
+/* every leaf interior (:225-238).  unk_old: guard cells are refilled.   */
+/* ===================================================================== */
+int orc_amr_regrid(const flash_hy_params *p, const flash_hy_grid_desc *g_old, double *unk_old,
+                   const flash_hy_grid_desc *g_new, double *unk_new, const int *src, const int *how) {
+  amr_t a, an;
+  int st = amr_build(g_old, &a);
+  if (st) return st;
+  if ((st = amr_build(g_new, &an))) { amr_free(&a); return st; }
+  ctx_t c; ctx_init(&c, p, g_old);
+  amr_fill_all(p, g_old, &a, unk_old);
+  const size_t ncell = (size_t)c.nxt * c.nyt * c.nzt, bsz = ncell * c.nunk;
+  int rc = 0;
+  #pragma omp parallel for schedule(dynamic)
+  for (int nb = 0; nb < g_new->nblocks; ++nb) {
+    const int o = src[nb];
+    double *dst = &unk_new[nb * bsz];
+    if (o < 0 || o >= g_old->nblocks || how[nb] < 0 || how[nb] > 2) { rc = FLASH_HY_ERR_BAD_ARG; continue; }
+    if (how[nb] != 1) {
+      memcpy(dst, &unk_old[o * bsz], sizeof(double) * bsz);
+      continue;
+    }
+    /* the old leaf o with its guard cells before the EOS */
+    double *P = malloc(sizeof(double) * bsz);
+    memcpy(P, &unk_old[o * bsz], sizeof(double) * bsz);
+    for (int k = 0; k < c.nzt; ++k)
+      for (int j = 0; j < c.nyt; ++j)
+        for (int i = 0; i < c.nxt; ++i) {
+          int li = i - NGUARD, lj = c.k2 ? j - NGUARD : 0, lk = c.k3 ? k - NGUARD : 0;
+          if (li >= 0 && li < c.nxb && lj >= 0 && lj < c.nyb && lk >= 0 && lk < c.nzb) continue;
+          amr_guard_cell(&c, &a, g_old, unk_old, o, li, lj, lk, &P[cidx(&c, i, j, k) * c.nunk]);
+        }
+    const int *cc = &g_new->block_coords[3 * nb];
+    for (int k = 0; k < c.nzb; ++k)
+      for (int j = 0; j < c.nyb; ++j)
+        for (int i = 0; i < c.nxb; ++i) {
+          int loc[3] = {i, j, k}, i1[3];
+          double wx[3], cx[3];
+          for (int d = 0; d < 3; ++d) {
+            if (d >= a.ndim) { i1[d] = 0; wx[d] = 1.; cx[d] = 0.; continue; }
+            int N = a.N[d], ioff = (cc[d] & 1) * (N / 2), ii = loc[d] + 1;
+            i1[d] = (ii + 2 * N) / 2 - N + ioff - 1;
+            wx[d] = fmod(0.75 + (double)(ii + 2 * N) * .5, 1.);
+            cx[d] = 1. - wx[d];
+          }
+          double r[2][2][2][NUNK_MAX];
+          for (int kk = 0; kk <= c.k3; ++kk)
+            for (int jj = 0; jj <= 1; ++jj)
+              for (int ii = 0; ii <= 1; ++ii) {
+                const double *u = &P[cidx(&c, i1[0] + ii + NGUARD, i1[1] + jj + NGUARD,
+                                          c.k3 ? i1[2] + kk + NGUARD : 0) * c.nunk];
+                for (int v = 0; v < c.nunk; ++v) r[kk][jj][ii][v] = is_per_mass(v) ? u[DENS_V] * u[v] : u[v];
+              }
+          double val[NUNK_MAX];
+          for (int v = 0; v < c.nunk; ++v) {
+            double plane0 = wx[1] * (wx[0] * r[0][0][0][v] + cx[0] * r[0][0][1][v]) +
+                            cx[1] * (wx[0] * r[0][1][0][v] + cx[0] * r[0][1][1][v]);
+            if (c.k3) {
+              double plane1 = wx[1] * (wx[0] * r[1][0][0][v] + cx[0] * r[1][0][1][v]) +
+                              cx[1] * (wx[0] * r[1][1][0][v] + cx[0] * r[1][1][1][v]);
+              val[v] = wx[2] * plane0 + cx[2] * plane1;
+            } else {
+              val[v] = plane0;
+            }
+          }
+          double *d = &dst[cidx(&c, i + NGUARD, j + (c.k2 ? NGUARD : 0), c.k3 ? k + NGUARD : 0) * c.nunk];
+          double inv = 1. / val[DENS_V];
+          for (int v = 0; v < c.nunk; ++v) d[v] = is_per_mass(v) ? inv * val[v] : val[v];
+        }
+    free(P);
+  }
+  if (!rc) {
+    #pragma omp parallel for schedule(dynamic)
+    for (int nb = 0; nb < g_new->nblocks; ++nb) {
+      if (!an.leaf[nb]) continue;
+      for (int k = 0; k < c.nzb; ++k)
+        for (int j = 0; j < c.nyb; ++j)
+          for (int i = 0; i < c.nxb; ++i)
+            eos_dens_ei_cell(&c, &unk_new[nb * bsz + cidx(&c, i + NGUARD, j + (c.k2 ? NGUARD : 0),
+                                                         c.k3 ? k + NGUARD : 0) * c.nunk]);
+    }
+  }
+  amr_free(&a);
+  amr_free(&an);
+  return rc;
+}

@@ -36,6 +36,8 @@ def lib():
         L.orc_hllc.argtypes = [P, C.c_int, dp, dp, dp]
         L.orc_exact_flux.argtypes = [C.c_int, dp, dp, C.c_double, C.c_double, C.c_int, dp, ip]
         L.orc_star_state.argtypes = [C.c_double] * 8 + [C.c_double, C.c_int, dp, dp, ip]
+        L.orc_estimate_error.argtypes = [C.c_void_p, C.c_void_p, dp, C.c_int, C.c_double, dp]
+        L.orc_amr_regrid.argtypes = [C.c_void_p, C.c_void_p, dp, C.c_void_p, dp, ip, ip]
         L.orc_two_rarefaction_guess.argtypes = [C.c_double] * 7
         L.orc_two_rarefaction_guess.restype = C.c_double
         L.orc_star_batch.argtypes = [C.c_long] + [dp] * 8 + [C.c_double, C.c_int, dp, dp, ip, ip]
@@ -86,6 +88,29 @@ class Oracle:
         bl = np.ascontiguousarray(blocks, dtype=np.int32)
         return lib().orc_hydro(C.byref(self.p), C.byref(self.g), _dp(unk), sim_time, dt, dt_old, len(bl),
                                bl.ctypes.data_as(C.POINTER(C.c_int)))
+
+    def estimate_error(self, unk, var="dens", refine_filter=0.01):
+        """gr_estimateError on a copy of unk (guard cells filled there)."""
+        from flash5_b200 import abi
+        u = np.ascontiguousarray(unk.copy())
+        err = np.zeros(self.grid.nblocks, dtype=np.float64)
+        st = lib().orc_estimate_error(C.byref(self.p), C.byref(self.g), _dp(u), abi.REFVAR[var],
+                                      float(refine_filter), _dp(err))
+        assert st == 0, st
+        return err
+
+    def regrid(self, unk, new_grid, src, how):
+        """gr_updateRefinement's data movement on host UNK arrays: the UNK of
+        new_grid (amr.regrid's tree) from unk (whose guard cells are
+        refilled)."""
+        out = new_grid.new_unk()
+        gn = new_grid.desc()
+        s = np.ascontiguousarray(src, dtype=np.int32)
+        w = np.ascontiguousarray(how, dtype=np.int32)
+        st = lib().orc_amr_regrid(C.byref(self.p), C.byref(self.g), _dp(unk), C.byref(gn), _dp(out),
+                                  s.ctypes.data_as(C.POINTER(C.c_int)), w.ctypes.data_as(C.POINTER(C.c_int)))
+        assert st == 0, st
+        return out
 
     def amr_hydro(self, unk, sim_time, dt, dt_old):
         """The AMR step on any grid (max_level 1 included)."""
