@@ -367,6 +367,7 @@ def amr_workload(args):
     peak, peak_kind = measured_peaks()
     ms, outs, dts, launches, clocks, e2e_ms, hb = {}, {}, None, {}, None, None, None
     tunings = {}
+    regrid_info = None
     paths = [p for p in args.paths.split(",") if p in ("fp64", "mixed", "mixed_exact")] or ["fp64", "mixed"]
     spec = {"fp64": (abi.PREC_FP64, abi.RS_HLLC), "mixed": (abi.PREC_MIXED, abi.RS_HLLC),
             "mixed_exact": (abi.PREC_MIXED, abi.RS_EXACT)}
@@ -394,6 +395,24 @@ def amr_workload(args):
             host[...] = unk
             e2e_ms = run_e2e(h, host, max(3, min(args.steps, 8)), 3)
             hb = host.nbytes
+        if headline and not args.no_regrid:
+            # one refinement cycle on the stepped state: the estimator of
+            # dens and pres on every node (device), marks and new tree
+            # (host), data of the new tree (device)
+            from flash5_b200.amr import update_refinement
+            est = []
+            for _ in range(3):
+                t0 = time.perf_counter()
+                h.estimate_error("pres", 0.01)
+                est.append(time.perf_counter() - t0)
+            tm = {}
+            h, g_new = update_refinement(h, g, ("dens", "pres"), 0.8, 0.2, 0.01, timings=tm)
+            regrid_info = {"estimate_one_var_ms": 1e3 * min(est), "nodes": g.nblocks,
+                           "cycle": {k: (round(v * 1e3, 3) if k.endswith("_s") else v) for k, v in tm.items()},
+                           "cycle_units": "ms (estimate: dens + pres on the device, mark_and_tree: host, "
+                                          "data: new context + device regrid)",
+                           "new_leaves": int(g_new.nleaves), "old_leaves": int(g.nleaves),
+                           "cutoffs": {"refine": 0.8, "derefine": 0.2, "filter": 0.01}}
         h.close()
     head = paths[-1]
     leaves = g.leaf_ids
@@ -430,6 +449,8 @@ def amr_workload(args):
                                "every node's FLASH UNK (11 vars), pinned host memory"}
     if cpu is not None:
         line["cpu_baseline"] = cpu
+    if regrid_info is not None:
+        line["refinement_cycle"] = regrid_info
     print(json.dumps(line))
     return 0
 
@@ -470,6 +491,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes (no autotuning)")
+    ap.add_argument("--no-regrid", action="store_true", help="AMR workload: skip the refinement-cycle timing")
     ap.add_argument("--nspecies", type=int, default=0, help="KH workload: species advected with the flow")
     ap.add_argument("--nmass-scalars", type=int, default=0, help="KH workload: mass scalars advected with the flow")
     ap.add_argument("--workload", default="kh", choices=["kh", "riemann", "amr"])

@@ -60,6 +60,16 @@ class AmrGrid:
         self._inner = set()
         self._finalize()
 
+    def __getattr__(self, name):
+        # key tables of a grid built from node arrays (regrid_native)
+        if name in ("node_index", "_leaves", "_inner") and "levels" in self.__dict__:
+            keys = [(int(lv), (int(c[0]), int(c[1]), int(c[2]))) for lv, c in zip(self.levels, self.coords)]
+            self.node_index = {k: i for i, k in enumerate(keys)}
+            self._leaves = {keys[i] for i in self.leaf_ids}
+            self._inner = {keys[i] for i in np.nonzero(~self.is_leaf)[0]}
+            return self.__dict__[name]
+        raise AttributeError(name)
+
     # -- tree edits ----------------------------------------------------------
     def _extent(self, level):
         return tuple(self.nblk[d] * (2 ** (level - 1)) if d < self.ndim else 1 for d in range(3))
@@ -329,21 +339,18 @@ def mark_refine_derefine(grid, errors, refine_cutoff, derefine_cutoff, max_refin
     derefine = np.zeros(n, dtype=bool)
     stay = np.zeros(n, dtype=bool)
     leaf = grid.is_leaf
+    top = grid.levels >= max_refine
     for v in range(nv):
         err = np.asarray(errors[v], dtype=np.float64)
         err_par = np.where(grid.parent >= 0, err[np.maximum(grid.parent, 0)], 0.0)
-        for b in range(n):
-            if leaf[b] and not refine[b] and not stay[b] and err[b] <= dc[v] and err_par[b] <= dc[v]:
-                derefine[b] = True
-            else:
-                derefine[b] = False
-            if err[b] > rc[v]:
-                derefine[b] = False
-                refine[b] = True
-            if (leaf[b] and err[b] > dc[v]) or err_par[b] > dc[v]:
-                stay[b] = True
-            if grid.levels[b] >= max_refine:
-                refine[b] = False
+        # the per-block rules, all blocks at once (each block's marks depend
+        # only on its own and its parent's error and its earlier marks)
+        derefine = leaf & ~refine & ~stay & (err <= dc[v]) & (err_par <= dc[v])
+        up = err > rc[v]
+        derefine &= ~up
+        refine |= up
+        stay |= (leaf & (err > dc[v])) | (err_par > dc[v])
+        refine &= ~top
     refine &= leaf
     derefine &= leaf
     return refine, derefine
@@ -354,6 +361,47 @@ def _clone(grid):
     g._leaves = set(grid._leaves)
     g._inner = set(grid._inner)
     return g
+
+
+def _grid_from_nodes(template, levels, coords, parent):
+    """An AmrGrid with the given nodes (ordered by level and Morton index)."""
+    g = copy.copy(template)
+    g.nblocks = len(levels)
+    g.levels = np.ascontiguousarray(levels, dtype=np.int32)
+    g.coords = np.ascontiguousarray(np.asarray(coords, dtype=np.int32).reshape(-1, 3))
+    g.parent = np.ascontiguousarray(parent, dtype=np.int32)
+    leaf = np.ones(g.nblocks, dtype=bool)
+    leaf[g.parent[g.parent >= 0]] = False
+    g.is_leaf = leaf
+    g.leaf_ids = np.nonzero(leaf)[0]
+    # the key tables of the Python tree code are built on first use
+    for a in ("node_index", "_leaves", "_inner"):
+        g.__dict__.pop(a, None)
+    g.max_used_level = int(g.levels.max())
+    scale = np.ldexp(1.0, 1 - g.levels.astype(np.int64))
+    g.delta_b = np.stack([g.delta1[d] * scale if d < g.ndim else np.ones(g.nblocks) for d in range(3)], axis=1)
+    return g
+
+
+def regrid_native(grid, refine, derefine, min_level=1):
+    """regrid() by the library's tree code (flash_hy_refine_tree)."""
+    lib = abi.load_library()
+    gd = grid.desc()
+    r = np.ascontiguousarray(np.asarray(refine, dtype=np.uint8))
+    d = np.ascontiguousarray(np.asarray(derefine, dtype=np.uint8))
+    cap = grid.nblocks + (2 ** grid.ndim) * int(grid.is_leaf.sum()) + 8
+    out = [np.empty(cap, dtype=np.int32) for _ in range(5)]
+    coords = np.empty(3 * cap, dtype=np.int32)
+    n = C.c_int()
+    pi = lambda a: a.ctypes.data_as(C.POINTER(C.c_int))
+    st = lib.flash_hy_refine_tree(C.byref(gd), r.ctypes.data_as(C.c_void_p), d.ctypes.data_as(C.c_void_p),
+                                  int(min_level), cap, C.byref(n), pi(out[0]), pi(coords), pi(out[1]), pi(out[2]),
+                                  pi(out[3]))
+    if st:
+        raise RuntimeError(f"flash_hy_refine_tree status {st:#x}")
+    n = n.value
+    g = _grid_from_nodes(grid, out[0][:n], coords[:3 * n], out[1][:n])
+    return g, out[2][:n].copy(), out[3][:n].copy()
 
 
 def regrid(grid, refine, derefine, min_level=1):
@@ -430,3 +478,31 @@ def regrid(grid, refine, derefine, min_level=1):
             src[q] = old.node_index[pkey]
             how[q] = 1
     return g, src, how
+
+
+def update_refinement(h, grid, refine_vars=("dens", "pres"), refine_cutoff=0.8, derefine_cutoff=0.2,
+                      refine_filter=0.01, min_level=1, timings=None):
+    """Grid_markRefineDerefine + Grid_updateRefinement on a device context:
+    the estimator of every refinement variable on the device, the marks and
+    the new tree on the host, the data of the new tree on the device.
+    Returns (context, grid): the old ones when nothing changes, else a new
+    context (the old one is closed) for the new grid.  `timings`, a dict,
+    receives the seconds of each phase."""
+    import time
+    t0 = time.perf_counter()
+    errs = [h.estimate_error(v, refine_filter) for v in refine_vars]
+    t1 = time.perf_counter()
+    refine, derefine = mark_refine_derefine(grid, errs, refine_cutoff, derefine_cutoff)
+    g2, src, how = regrid_native(grid, refine, derefine, min_level=min_level)
+    t2 = time.perf_counter()
+    changed = g2.nblocks != grid.nblocks or np.any(how != 0)
+    if changed:
+        h2 = h.regrid(g2, src, how)
+        h.close()
+        h, grid = h2, g2
+    t3 = time.perf_counter()
+    if timings is not None:
+        timings.update(estimate_s=t1 - t0, mark_and_tree_s=t2 - t1, data_s=t3 - t2,
+                       refined=int(np.count_nonzero(how == 1)), derefined=int(np.count_nonzero(how == 2)),
+                       changed=bool(changed))
+    return h, grid

@@ -30,6 +30,7 @@ UNITS = [
     ("cfl_noalloc.o", "cfl_noalloc.cu", ["--fmad=false"]),
     ("spec.o", "spec.cu", ["--fmad=false"]),
     ("refine.o", "refine.cu", ["--fmad=false"]),
+    ("tree.o", "tree.cu", []),
 ]
 
 

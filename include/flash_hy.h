@@ -260,6 +260,21 @@ int flash_hy_estimate_error(flash_hy_ctx *ctx, int var, double refine_filter, do
  * hierarchies of the same block shape on the same device.               */
 int flash_hy_regrid(flash_hy_ctx *old_ctx, flash_hy_ctx *new_ctx, int n, const int *src, const int *how);
 
+/* The tree of a regrid (PARAMESH amr_refine_derefine, restated): from the
+ * grid descriptor of an AMR hierarchy and per-node marks (refine, derefine:
+ * 0/1 bytes, leaves only), the marked leaves below max_level are split,
+ * refinement spreads until every leaf's neighbours (diagonals included) are
+ * within one level, and a parent at level >= min_level loses its children
+ * when all of them are unrefined leaves marked for derefinement and no
+ * neighbour's child touching it stays refined.  Writes the new node count
+ * to *new_n and, when it fits in cap, the new nodes ordered by level and
+ * Morton index: new_levels[n], new_coords[3n], new_parent[n] (-1 on level
+ * 1), and src / how for flash_hy_regrid.  FLASH_HY_ERR_BAD_ARG when cap is
+ * too small (*new_n says how much is needed) or the tree is incomplete. */
+int flash_hy_refine_tree(const flash_hy_grid_desc *grid, const unsigned char *refine, const unsigned char *derefine,
+                         int min_level, int cap, int *new_n, int *new_levels, int *new_coords, int *new_parent,
+                         int *src, int *how);
+
 /* ---- launch shapes and their autotuner ----------------------------------
  * No FLASH5 counterpart (FLASH picks no launch shapes; its block loop is
  * Hydro.F90:156-229).  Threads per CTA of the step's kernels: the

@@ -156,3 +156,28 @@ def test_oracle_regrid_uniform_and_linear():
     d = g2.interior(out2)[inner][..., VAR["dens"]]
     exact = 1.0 + 0.25 * x2[inner] + 0.125 * y2[inner]
     assert np.abs(d - exact).max() < 1e-13
+
+
+def _same_grid(a, b):
+    assert a.nblocks == b.nblocks
+    assert np.array_equal(a.levels, b.levels) and np.array_equal(a.coords, b.coords)
+    assert np.array_equal(a.parent, b.parent) and np.array_equal(a.is_leaf, b.is_leaf)
+    assert np.array_equal(a.delta_b, b.delta_b)
+
+
+def test_native_tree_matches_python():
+    from flash5_b200.amr import regrid_native
+    cases = [ring(), ring(bc="outflow"),
+             AmrGrid(3, (8, 8, 8), (2, 2, 2), 3, bc="periodic")]
+    f3 = lambda X, Y, Z: 1.0 + 0.8 * np.tanh(((X - 0.5) ** 2 + (Y - 0.45) ** 2 + (Z - 0.5) ** 2 - 0.06) / 0.004)
+    cases[2].refine_levels(indicator_refiner(cases[2], f3, 0.05))
+    rng = np.random.default_rng(7)
+    for g in cases:
+        for trial in range(3):
+            n = g.nblocks
+            refine = g.is_leaf & (rng.random(n) < 0.2)
+            derefine = g.is_leaf & ~refine & (rng.random(n) < 0.7)
+            a, sa, ha = regrid(g, refine, derefine)
+            b, sb, hb = regrid_native(g, refine, derefine)
+            _same_grid(a, b)
+            assert np.array_equal(sa, sb) and np.array_equal(ha, hb)
