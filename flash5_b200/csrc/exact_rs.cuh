@@ -83,19 +83,39 @@ __device__ __forceinline__ Side make_side(double d, double u, double p, double c
   return Side{d, u, p, c, powp(p, zexp(g))};
 }
 
-// f_K(w) and df_K/dw; p = w^(1/z) is passed in
-__device__ __forceinline__ void pres_fn(double w, double p, const Side &s, double g, double &f, double &fd) {
+// Constants of one side's pressure function, taken once per solve: w_K,
+// p_K, the rarefaction slope k = 2 c_K / ((g-1) w_K) and A_K, B_K of the
+// shock branch.
+struct SideK { double w, p, k, A, B; };
+__device__ __forceinline__ SideK side_k(const Side &s, double g) {
+  return SideK{s.w, s.p, 2.0 * s.c / ((g - 1.0) * s.w), 2.0 / ((g + 1.0) * s.d), (g - 1.0) / (g + 1.0) * s.p};
+}
+
+// p = w^n, n = 1/z = 2g/(g-1): unrolled for the integer exponents of
+// g = 5/3, 7/5, 4/3 (5, 7, 8), else pow_k
+struct PowN { int ni; double n; };
+__device__ __forceinline__ PowN pown_of(double g) {
+  const double n = 2.0 * g / (g - 1.0), r = rint(n);
+  return PowN{(fabs(n - r) < 1e-9 && (r == 5.0 || r == 7.0 || r == 8.0)) ? (int)r : 0, n};
+}
+__device__ __forceinline__ double pow_n(double w, const PowN &e) {
+  if (e.ni == 5) { const double w2 = w * w; return w2 * w2 * w; }
+  if (e.ni == 7) { const double w2 = w * w, w4 = w2 * w2; return w4 * w2 * w; }
+  if (e.ni == 8) { const double w2 = w * w, w4 = w2 * w2; return w4 * w4; }
+  return pow_k(w, e.n);
+}
+
+// f_K(w) and df_K/dw (Toro eqs. 4.6-4.7 with p = w^n); iw = 1/w
+__device__ __forceinline__ void pres_fn(double w, double p, double iw, const SideK &s, double n, double &f,
+                                        double &fd) {
   if (w <= s.w) {                                   // rarefaction, Toro eq. 4.7
-    const double k = 2.0 * s.c / ((g - 1.0) * s.w);
-    f = k * (w - s.w);
-    fd = k;
+    f = s.k * (w - s.w);
+    fd = s.k;
   } else {                                          // shock, Toro eq. 4.6
-    const double A = 2.0 / ((g + 1.0) * s.d);
-    const double B = (g - 1.0) / (g + 1.0) * s.p;
-    const double r = 1.0 / (B + p);
-    const double q = sqrt(A * r);
+    const double r = 1.0 / (s.B + p);
+    const double q = sqrt(s.A * r);
     f = (p - s.p) * q;
-    fd = (1.0 - 0.5 * (p - s.p) * r) * q * (p / (zexp(g) * w));   // df/dp dp/dw
+    fd = (1.0 - 0.5 * (p - s.p) * r) * q * (n * p * iw);   // df/dp dp/dw
   }
 }
 
@@ -144,14 +164,17 @@ struct Star { double p, u, w; };
 __device__ __forceinline__ int newton(const Side &L, const Side &R, double g, double w0, double tol, int max_iter,
                                       Star &out) {
   const double du = R.u - L.u, ztol = zexp(g) * tol;
+  const SideK kl = side_k(L, g), kr = side_k(R, g);
+  const PowN e = pown_of(g);
   double wa = 0.0, wb = DBL_MAX;
   double w = w0, prev = -1.0, p = 0.0;
   double fl = 0., fdl = 0., fr = 0., fdr = 0., we = w0;
   int evals = 0;
   for (; evals < max_iter;) {
-    p = p_of_w(w, g);
-    pres_fn(w, p, L, g, fl, fdl);
-    pres_fn(w, p, R, g, fr, fdr);
+    p = pow_n(w, e);
+    const double iw = 1.0 / w;
+    pres_fn(w, p, iw, kl, e.n, fl, fdl);
+    pres_fn(w, p, iw, kr, e.n, fr, fdr);
     ++evals;
     we = w;
     const double f = fl + fr + du;
@@ -163,7 +186,7 @@ __device__ __forceinline__ int newton(const Side &L, const Side &R, double g, do
     if (f < 0.0) wa = w; else wb = w;
     if (wb - wa <= ztol * w) {
       out.w = 0.5 * (wa + wb);
-      out.p = p_of_w(out.w, g);
+      out.p = pow_n(out.w, e);
       const double dw = out.w - we;
       out.u = 0.5 * (L.u + R.u) + 0.5 * ((fr + fdr * dw) - (fl + fdl * dw));
       return evals;
@@ -174,7 +197,7 @@ __device__ __forceinline__ int newton(const Side &L, const Side &R, double g, do
     const bool inside = wn > wa && wn < wb;
     if (as <= ztol * w || (inside && prev > 0.0 && as < prev && as * (as / prev) * (as / prev) <= 0.01 * ztol * w)) {
       out.w = wn > 0.0 ? wn : w;
-      out.p = p_of_w(out.w, g);
+      out.p = pow_n(out.w, e);
       const double dw = out.w - we;
       out.u = 0.5 * (L.u + R.u) + 0.5 * ((fr + fdr * dw) - (fl + fdl * dw));
       return evals;
@@ -187,7 +210,7 @@ __device__ __forceinline__ int newton(const Side &L, const Side &R, double g, do
     }
     w = wn;
   }
-  out.w = w; out.p = p_of_w(w, g);
+  out.w = w; out.p = pow_n(w, e);
   const double dw = w - we;
   out.u = 0.5 * (L.u + R.u) + 0.5 * ((fr + fdr * dw) - (fl + fdl * dw));
   return -max_iter;
