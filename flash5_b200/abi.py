@@ -82,7 +82,7 @@ class Params(C.Structure):
 def default_params(**kw):
     """Runtime parameters with FLASH5's unsplit defaults (unsplit/Config:105-159,
     HydroMain/Config:26, Eos/EosMain/Config:49-56) except order=3 (PPM) and
-    flattening on, the settings of the benchmark configurations."""
+    flattening on, as in the Sod, Kelvin-Helmholtz and four-quadrant workloads."""
     p = Params()
     p.order = 3
     p.riemann_solver = RS_HLLC

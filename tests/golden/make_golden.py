@@ -10,7 +10,7 @@
    functions (ch. 4, eqs. 4.6-4.7), solved to 50 digits by mpmath
    bisection + findroot, for a set of left/right states covering both
    shocks, both rarefactions, mixed waves, strong pressure ratios and both
-   gammas of the benchmark configurations.
+   gammas 7/5 and 5/3.
 
 Run: python tests/golden/make_golden.py
 """
