@@ -108,3 +108,20 @@ def test_mixed_close(case):
     grid, ref, out, _ = run_pair(case, precision=abi.PREC_MIXED)
     for k, l1 in momentum_normalised_l1(out, ref, grid).items():
         assert l1 <= 1e-6, (k, l1)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("opts", [
+    dict(slope_limiter=abi.LIM_MINMOD), dict(slope_limiter=abi.LIM_MC), dict(slope_limiter=abi.LIM_HYBRID),
+    dict(slope_limiter=abi.LIM_LIMITED, limited_slope_beta=1.5), dict(char_limiting=0),
+    dict(use_flattening=0), dict(use_steepening=1), dict(use_aux_eint=0), dict(use_3d_full_ctu=0),
+])
+@pytest.mark.parametrize("case", ["sod2d_rot", "kh3d"])
+def test_mixed_close_options(case, opts):
+    """The mixed path's other branches (limiters, primitive limiting,
+    steepening, no flattening, no aux eint, no 3D CTU) stay within the
+    mixed tolerance of the oracle."""
+    grid, ref, out, _ = run_pair(case, nsteps=3, precision=abi.PREC_MIXED, **opts)
+    for k, l1 in momentum_normalised_l1(out, ref, grid).items():
+        assert l1 <= 1e-6, (opts, k, l1)
+
