@@ -34,10 +34,10 @@ def _morton(c):
 
 class AmrGrid:
     def __init__(self, ndim, nb, nblk, max_level, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0), bc="outflow",
-                 nguard=NGUARD):
+                 nguard=NGUARD, nspecies=0, nmass_scalars=0):
         self.ndim = ndim
-        self.nspecies = self.nmass_scalars = 0        # species are not carried on AMR hierarchies
-        self.nunk = NUNK
+        self.nspecies, self.nmass_scalars = int(nspecies), int(nmass_scalars)
+        self.nunk = NUNK + self.nspecies + self.nmass_scalars
         nb = tuple(nb) + (1,) * (3 - len(nb))
         nblk = tuple(nblk) + (1,) * (3 - len(nblk))
         self.nb = tuple(nb[d] if d < ndim else 1 for d in range(3))
@@ -199,7 +199,12 @@ class AmrGrid:
 
     # -- UNK helpers (the same interface as UniformGrid) -------------------------
     def new_unk(self):
-        return np.zeros((self.nblocks, self.nt[2], self.nt[1], self.nt[0], NUNK), dtype=np.float64)
+        return np.zeros((self.nblocks, self.nt[2], self.nt[1], self.nt[0], self.nunk), dtype=np.float64)
+
+    @property
+    def species(self):
+        """UNK slice of the species and mass scalars."""
+        return slice(NUNK, self.nunk)
 
     def interior(self, unk):
         g = self.ng

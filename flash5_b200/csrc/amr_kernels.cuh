@@ -35,7 +35,7 @@ __device__ __forceinline__ double node_E(const DevParams &P, int m, size_t off, 
 
 template <int NDIM, int NX, int NY, int NZ>
 __global__ void __launch_bounds__(256) k_restrict(DevParams P, double *st0, double *st1, double *st2, double *st3,
-                                                  double *st4, const int *plist) {
+                                                  double *st4, const int *plist, double *sp, size_t ncells) {
   constexpr int NCB = NX * NY * NZ;
   const int b = plist[blockIdx.x];
   const int l = P.blk_level[b];
@@ -70,6 +70,17 @@ __global__ void __launch_bounds__(256) k_restrict(DevParams P, double *st0, doub
     st3[o] = inv * s[3];
     st4[o] = inv * s[4];
     P.pe[o] = inv * s[5];
+    // species and mass scalars, per-mass like the velocities
+    for (int q = 0; q < P.nsp; ++q) {
+      double x = 0.;
+      for (int kk = 0; kk <= (NDIM > 2 ? 1 : 0); ++kk)
+        for (int jj = 0; jj <= 1; ++jj)
+          for (int ii = 0; ii <= 1; ++ii) {
+            const size_t off = (size_t)ch * NCB + (size_t)(((fk + kk) * NY + (fj + jj)) * NX + (fi + ii));
+            x = x + w * (st[0][off] * sp[(size_t)q * ncells + off]);
+          }
+      sp[(size_t)q * ncells + o] = inv * x;
+    }
   }
 }
 
@@ -158,6 +169,85 @@ __device__ void amr_guard(const DevParams &P, const double *const st[5], int n, 
   if (flip[2]) out[3] = -out[3];
 }
 
+// Linear prolongation of one per-mass scalar x (a species) of child cell lp
+// from the parent's guard-inclusive density gr and x gx: the arithmetic of
+// prolong_linear on (rho, rho x).
+template <int NDIM, int NX, int NY, int NZ>
+__device__ __forceinline__ double prolong_scalar(const double *gr, const double *gx, const int c[3], const int lp[3]) {
+  using H = Halo<NDIM, NX, NY, NZ>;
+  const int Nd[3] = {NX, NY, NZ};
+  int i1[3] = {0, 0, 0};
+  double wx[3] = {1., 1., 1.}, cx[3] = {0., 0., 0.};
+#pragma unroll
+  for (int d = 0; d < NDIM; ++d) {
+    const int N = Nd[d], ioff = (c[d] & 1) * (N / 2), ii = lp[d] + 1;
+    i1[d] = (ii + 2 * N) / 2 - N + ioff - 1;
+    wx[d] = fmod(0.75 + (double)(ii + 2 * N) * .5, 1.);
+    cx[d] = 1. - wx[d];
+  }
+  double r[2][2][2][2];
+  for (int kk = 0; kk <= (NDIM > 2 ? 1 : 0); ++kk)
+    for (int jj = 0; jj <= 1; ++jj)
+      for (int ii = 0; ii <= 1; ++ii) {
+        const int h = H::idx(i1[0] + ii, i1[1] + jj, NDIM > 2 ? i1[2] + kk : 0);
+        const double rho = gr[h];
+        r[kk][jj][ii][0] = rho;
+        r[kk][jj][ii][1] = rho * gx[h];
+      }
+  double val[2];
+#pragma unroll
+  for (int v = 0; v < 2; ++v) {
+    const double plane0 = wx[1] * (wx[0] * r[0][0][0][v] + cx[0] * r[0][0][1][v]) +
+                          cx[1] * (wx[0] * r[0][1][0][v] + cx[0] * r[0][1][1][v]);
+    if (NDIM > 2) {
+      const double plane1 = wx[1] * (wx[0] * r[1][0][0][v] + cx[0] * r[1][0][1][v]) +
+                            cx[1] * (wx[0] * r[1][1][0][v] + cx[0] * r[1][1][1][v]);
+      val[v] = wx[2] * plane0 + cx[2] * plane1;
+    } else {
+      val[v] = plane0;
+    }
+  }
+  const double inv = 1. / val[0];
+  return inv * val[1];
+}
+
+// species q of guard cell (li, lj, lk) of node n: from the node of the same
+// level that owns the cell, or prolonged from n's parent (no sign change
+// at reflecting boundaries)
+template <int NDIM, int NX, int NY, int NZ>
+__device__ double amr_guard_spec(const DevParams &P, size_t ncells, int n, int li, int lj, int lk, int q) {
+  constexpr int NCB = NX * NY * NZ;
+  using H = Halo<NDIM, NX, NY, NZ>;
+  const int l = P.blk_level[n];
+  const int3 c3 = blk_coords(P, n);
+  const int c[3] = {c3.x, c3.y, c3.z}, Nd[3] = {NX, NY, NZ}, loc[3] = {li, lj, lk};
+  int gl[3] = {0, 0, 0}, lp[3] = {0, 0, 0}, flip[3] = {0, 0, 0};
+#pragma unroll
+  for (int d = 0; d < NDIM; ++d) {
+    const int tot = P.at_ext[l][d] * Nd[d], base = c[d] * Nd[d];
+    int gc = base + loc[d];
+    lp[d] = loc[d];
+    if (gc < 0 || gc >= tot) {
+      const int side = gc < 0 ? 2 * d : 2 * d + 1;
+      if (P.bc[side] == -135) {
+        gc = ((gc % tot) + tot) % tot;
+      } else {
+        gc = map_axis(gc, tot, P.bc[2 * d], P.bc[2 * d + 1], flip[d]);
+        lp[d] = gc - base;
+      }
+    }
+    gl[d] = gc;
+  }
+  const int m = at_node(P, l, gl[0] / NX, NDIM > 1 ? gl[1] / NY : 0, NDIM > 2 ? gl[2] / NZ : 0);
+  if (m >= 0) {
+    const size_t off = (size_t)m * NCB + (size_t)(((NDIM > 2 ? gl[2] % NZ : 0) * NY + (gl[1] % NY)) * NX + gl[0] % NX);
+    return P.sp_in[(size_t)q * ncells + off];
+  }
+  const int p = P.parent[n];
+  const size_t ps = (size_t)P.slot[p];
+  return prolong_scalar<NDIM, NX, NY, NZ>(P.gp + ps * 6 * H::n, P.sp_gp + (ps * P.nsp + q) * H::n, c, lp);
+}
+
 template <int NDIM, int NX, int NY, int NZ>
 __global__ void __launch_bounds__(256) k_parent_halo(DevParams P, const double *st0, const double *st1,
                                                      const double *st2, const double *st3, const double *st4,
@@ -178,6 +268,22 @@ __global__ void __launch_bounds__(256) k_parent_halo(DevParams P, const double *
     }
 #pragma unroll
     for (int q = 0; q < 6; ++q) gp[q * H::n + h] = v[q];
+  }
+  if (P.sp_gp) {
+    // species after the parent's own (rho, ...) copy: the prolongation from
+    // the grandparent reads this level's parents only through their parent
+    constexpr int NCB2 = NX * NY * NZ;
+    const size_t ncells = P.sp_ncells;
+    for (int qh = threadIdx.x; qh < P.nsp * H::n; qh += blockDim.x) {
+      const int q = qh / H::n, h = qh % H::n;
+      const int li = h % H::hx - 4, lj = NDIM > 1 ? (h / H::hx) % H::hy - 4 : 0, lk = NDIM > 2 ? h / (H::hx * H::hy) - 4 : 0;
+      double x;
+      if (is_inside<NDIM, NX, NY, NZ>(li, lj, lk))
+        x = P.sp_in[(size_t)q * ncells + (size_t)b * NCB2 + (size_t)((lk * NY + lj) * NX + li)];
+      else
+        x = amr_guard_spec<NDIM, NX, NY, NZ>(P, ncells, b, li, lj, lk, q);
+      P.sp_gp[((size_t)P.slot[b] * P.nsp + q) * H::n + h] = x;
+    }
   }
 }
 
@@ -200,6 +306,15 @@ __global__ void __launch_bounds__(256) k_leaf_halo(DevParams P, const double *st
     double eg = v[4];
     if (v[5] - ekin > rmax(P.smalle, P.eswitch * ekin)) eg = v[5] - ekin;
     lh[h] = v[0]; lh[H::n + h] = v[1]; lh[2 * H::n + h] = v[2]; lh[3 * H::n + h] = v[3]; lh[4 * H::n + h] = eg;
+  }
+  if (P.sp_lh) {
+    for (int qh = threadIdx.x; qh < P.nsp * H::n; qh += blockDim.x) {
+      const int q = qh / H::n, h = qh % H::n;
+      const int li = h % H::hx - 4, lj = NDIM > 1 ? (h / H::hx) % H::hy - 4 : 0, lk = NDIM > 2 ? h / (H::hx * H::hy) - 4 : 0;
+      if (is_inside<NDIM, NX, NY, NZ>(li, lj, lk)) continue;
+      P.sp_lh[((size_t)P.slot[b] * P.nsp + q) * H::n + h] =
+          amr_guard_spec<NDIM, NX, NY, NZ>(P, P.sp_ncells, b, li, lj, lk, q);
+    }
   }
 }
 

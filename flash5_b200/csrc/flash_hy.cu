@@ -78,6 +78,8 @@ struct flash_hy_ctx {
   int nsp, nspec;
   double *spec[2], *sacc, *ssig, *sp_mf, *sp_flat;
   unsigned char *sp_fb;
+  double *sp_lh, *sp_gp, *sp_freg;   // AMR: species guard cells, parent copies, flux register
+  size_t sp_freg_stride;
   double *d_err;               // refinement criterion per block
   char err[512];
 };
@@ -157,6 +159,13 @@ static void fill_devparams(const flash_hy_ctx *c, DevParams &P) {
     P.sp_mf = c->sp_mf;
     P.sp_fb = c->sp_fb;
     P.sp_flat = c->sp_flat;
+    P.sp_ncells = c->ncells;
+    if (c->amr) {
+      P.sp_lh = c->sp_lh;
+      P.sp_gp = c->sp_gp;
+      P.sp_freg = c->sp_freg;
+      P.sp_freg_stride = c->sp_freg_stride;
+    }
   }
   if (c->amr) {
     P.blk_level = c->d_level;
@@ -243,7 +252,6 @@ extern "C" int flash_hy_create(const flash_hy_params *params, const flash_hy_gri
   if (params->nspecies < 0 || params->nmass_scalars < 0 ||
       params->nspecies + params->nmass_scalars > FLASH_HY_MAX_SPECIES)
     return FLASH_HY_ERR_BAD_ARG;
-  if (params->nspecies + params->nmass_scalars > 0 && g->max_level > 1) return FLASH_HY_ERR_UNSUPPORTED;
   int nz = g->ndim > 2 ? g->nzb : 1, ny = g->ndim > 1 ? g->nyb : 1;
   if (!shape_supported(g->ndim, g->nxb, ny, nz)) return FLASH_HY_ERR_UNSUPPORTED;
   if (g->nblocks <= 0 || !g->block_coords || g->nguard < 0) return FLASH_HY_ERR_BAD_ARG;
@@ -378,14 +386,24 @@ extern "C" int flash_hy_create(const flash_hy_params *params, const flash_hy_gri
     ALLOC(c->sig, sig_bytes_per_block(g->ndim, g->nxb, ny, nz, rb) * g->nblocks);
   }
   if (c->nsp > 0) {
+    // per-slot scratch: a slot per block, or per leaf on an AMR hierarchy
+    const size_t nslot = amr ? (size_t)c->nleaves : (size_t)g->nblocks;
     const size_t box = (size_t)(g->nxb + 2) * (g->ndim > 1 ? ny + 2 : 1) * (g->ndim > 2 ? nz + 2 : 1);
     const size_t lines = (size_t)(g->nxb + 2) * (g->ndim > 1 ? ny : 1) * (g->ndim > 2 ? nz : 1);
     for (int s = 0; s < 2; ++s) ALLOC(c->spec[s], (size_t)c->nsp * c->ncells * sizeof(double));
     ALLOC(c->sacc, (size_t)c->nsp * c->ncells * sizeof(double));
-    ALLOC(c->ssig, (size_t)g->nblocks * g->ndim * c->nsp * box * sizeof(double));
-    ALLOC(c->sp_mf, (size_t)g->nblocks * g->ndim * lines * sizeof(double));
-    ALLOC(c->sp_fb, (size_t)g->nblocks * g->ndim * lines);
-    ALLOC(c->sp_flat, (size_t)g->nblocks * g->ndim * lines * sizeof(double));
+    ALLOC(c->ssig, nslot * g->ndim * c->nsp * box * sizeof(double));
+    ALLOC(c->sp_mf, nslot * g->ndim * lines * sizeof(double));
+    ALLOC(c->sp_fb, nslot * g->ndim * lines);
+    ALLOC(c->sp_flat, nslot * g->ndim * lines * sizeof(double));
+    if (amr) {
+      const size_t hn = (size_t)(g->nxb + 8) * (g->ndim > 1 ? ny + 8 : 1) * (g->ndim > 2 ? nz + 8 : 1);
+      const size_t nf = g->ndim == 2 ? (size_t)(g->nxb > ny ? g->nxb : ny) : (size_t)g->nxb * ny;
+      ALLOC(c->sp_lh, (size_t)c->nleaves * c->nsp * hn * sizeof(double));
+      if (c->nparents > 0) ALLOC(c->sp_gp, (size_t)c->nparents * c->nsp * hn * sizeof(double));
+      c->sp_freg_stride = (size_t)c->nleaves * 2 * g->ndim * nf;
+      ALLOC(c->sp_freg, (size_t)c->nsp * c->sp_freg_stride * sizeof(double));
+    }
   }
   if (!amr) ALLOC(c->d_blk_at, at.size() * sizeof(int));
   ALLOC(c->d_blk_coord, coords.size() * sizeof(int));
@@ -432,6 +450,7 @@ extern "C" int flash_hy_destroy(flash_hy_ctx *c) {
   for (int s = 0; s < 2; ++s) cudaFree(c->spec[s]);
   cudaFree(c->sacc); cudaFree(c->ssig); cudaFree(c->sp_mf); cudaFree(c->sp_fb); cudaFree(c->sp_flat);
   cudaFree(c->d_err);
+  cudaFree(c->sp_lh); cudaFree(c->sp_gp); cudaFree(c->sp_freg);
   free(c->h_blk_at);
   if (c->h_dt) cudaFreeHost(c->h_dt);
   if (c->h_status) cudaFreeHost(c->h_status);
@@ -584,7 +603,9 @@ static int amr_guard_fill(flash_hy_ctx *c, const DevParams &P) {
   for (int l = c->nlev - 1; l >= 1; --l) {
     if (!c->lev_parents[l]) continue;
     k_restrict<NDIM, NX, NY, NZ><<<c->lev_parents[l], 256, 0, c->stream>>>(P, st[0], st[1], st[2], st[3], st[4],
-                                                                          c->d_lev_parents[l]);
+                                                                          c->d_lev_parents[l],
+                                                                          c->nsp ? c->spec[c->cur] : nullptr,
+                                                                          c->ncells);
     ++n;
   }
   for (int l = 1; l < c->nlev; ++l) {
@@ -610,14 +631,18 @@ static int amr_restrict_all(flash_hy_ctx *c) {
   DevParams P;
   fill_devparams(c, P);
   double *const *st = c->state[c->cur];
+  double *sp = c->nsp ? c->spec[c->cur] : nullptr;
   for (int l = c->nlev - 1; l >= 1; --l) {
     if (!c->lev_parents[l]) continue;
     if (c->ndim == 2 && c->nx == 8)
-      k_restrict<2, 8, 8, 1><<<c->lev_parents[l], 256, 0, c->stream>>>(P, st[0], st[1], st[2], st[3], st[4], c->d_lev_parents[l]);
+      k_restrict<2, 8, 8, 1><<<c->lev_parents[l], 256, 0, c->stream>>>(P, st[0], st[1], st[2], st[3], st[4], c->d_lev_parents[l],
+                                                               sp, c->ncells);
     else if (c->ndim == 2)
-      k_restrict<2, 16, 16, 1><<<c->lev_parents[l], 256, 0, c->stream>>>(P, st[0], st[1], st[2], st[3], st[4], c->d_lev_parents[l]);
+      k_restrict<2, 16, 16, 1><<<c->lev_parents[l], 256, 0, c->stream>>>(P, st[0], st[1], st[2], st[3], st[4], c->d_lev_parents[l],
+                                                               sp, c->ncells);
     else
-      k_restrict<3, 8, 8, 8><<<c->lev_parents[l], 256, 0, c->stream>>>(P, st[0], st[1], st[2], st[3], st[4], c->d_lev_parents[l]);
+      k_restrict<3, 8, 8, 8><<<c->lev_parents[l], 256, 0, c->stream>>>(P, st[0], st[1], st[2], st[3], st[4], c->d_lev_parents[l],
+                                                               sp, c->ncells);
   }
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
@@ -670,6 +695,10 @@ static int enqueue_step(flash_hy_ctx *c, double dt, const int *d_list, int nlaun
     sa.ncells = c->ncells;
     sa.nlaunch = nlaunch;
     sa.stream = c->stream;
+    sa.nlev = a.nlev;
+    sa.leaves = a.leaves;
+    sa.nleaves = a.nleaves;
+    for (int l = 0; l < 17; ++l) { sa.lev_list[l] = a.lev_list[l]; sa.lev_count[l] = a.lev_count[l]; }
     const int ns = spec_step(sa, c->ndim, c->nx, c->ny, c->nz);
     if (ns < 0) return fail(c, FLASH_HY_ERR_CUDA, "species launch failed: %s", cudaGetErrorString(cudaGetLastError()));
     n += ns;
@@ -1143,7 +1172,7 @@ extern "C" int flash_hy_estimate_error(flash_hy_ctx *c, int var, double refine_f
 extern "C" int flash_hy_regrid(flash_hy_ctx *old, flash_hy_ctx *nw, int n, const int *src, const int *how) {
   if (!old || !nw || !src || !how || old == nw) return FLASH_HY_ERR_BAD_ARG;
   if (!old->amr || !nw->amr || old->device != nw->device || old->ndim != nw->ndim || old->nx != nw->nx ||
-      old->ny != nw->ny || old->nz != nw->nz || n != nw->nblocks)
+      old->ny != nw->ny || old->nz != nw->nz || n != nw->nblocks || old->nsp != nw->nsp)
     return fail(nw, FLASH_HY_ERR_BAD_ARG, "regrid: %s", "contexts of different shapes or not AMR hierarchies");
   std::vector<int> refl, slot(n, -1), of(old->nblocks, -1);
   std::vector<int> oleaf(old->nblocks);
@@ -1164,6 +1193,7 @@ extern "C" int flash_hy_regrid(flash_hy_ctx *old, flash_hy_ctx *nw, int n, const
     return fail(old, FLASH_HY_ERR_CUDA, "AMR guard-cell launch failed: %s", cudaGetErrorString(cudaGetLastError()));
   fill_devparams(nw, a.Pn);
   for (int v = 0; v < 5; ++v) a.Pn.s_out[v] = nw->state[nw->cur][v];
+  if (nw->nsp) a.Pn.sp_out = nw->spec[nw->cur];
   a.nref = (int)refl.size();
   a.nnew = n;
   a.stream = old->stream;
@@ -1172,7 +1202,7 @@ extern "C" int flash_hy_regrid(flash_hy_ctx *old, flash_hy_ctx *nw, int n, const
   const size_t hn = halo_cells(old->ndim, old->nx, old->ny, old->nz);
   int rc = 0;
   if (cudaMalloc((void **)&d_idx, (3 * (size_t)n + refl.size() + 1) * sizeof(int)) != cudaSuccess ||
-      (a.nref && cudaMalloc((void **)&d_nh, (size_t)a.nref * 6 * hn * sizeof(double)) != cudaSuccess)) {
+      (a.nref && cudaMalloc((void **)&d_nh, (size_t)a.nref * (6 + old->nsp) * hn * sizeof(double)) != cudaSuccess)) {
     cudaGetLastError();
     rc = fail(nw, FLASH_HY_ERR_CUDA, "regrid: %s", "scratch allocation");
   } else {

@@ -78,6 +78,12 @@ struct DevParams {
   double *sp_mf;
   unsigned char *sp_fb;
   double *sp_flat;            // flattening coefficient of each line cell (same layout)
+  // species on AMR hierarchies: guard cells of the leaves [leaf slot][nsp]
+  // [halo], guard-inclusive copies of the parents [parent slot][nsp][halo],
+  // the species flux register [nsp][leaf slot][2 ndim][faces]
+  double *sp_lh, *sp_gp, *sp_freg;
+  size_t sp_ncells;           // stride of the species arrays
+  size_t sp_freg_stride;      // doubles per species in sp_freg
 };
 
 // Cell sizes of block b: level-1 deltas scaled by 2^(1-level) (exact).

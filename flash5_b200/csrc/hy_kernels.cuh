@@ -280,8 +280,12 @@ __device__ __forceinline__ void exact_face(const DevParams &P, const double *VL,
 // in place.  fidx(along, t1, t2) gives the position of a face in sF, t1/t2
 // the tangential coordinates (y, z for x faces; x, z for y; x, y for z).
 // ---------------------------------------------------------------------------
+// The register of nv flux components per face: reg[(slot * 2 NDIM + face
+// side) * NF * nv + face * nv + v]; the hydro's is P.freg with the NFLX
+// fluxes, the species pass keeps one register per species.
 template <int NDIM, int NX, int NY, int NZ, int DIR, class FaceIdx>
-__device__ void flux_register(const DevParams &P, int b, int3 bc, double *sF, int fstride, FaceIdx fidx) {
+__device__ void flux_register_v(const DevParams &P, int b, int3 bc, double *sF, int fstride, FaceIdx fidx,
+                                double *reg, int nv) {
   constexpr int N = DIR == 1 ? NX : (DIR == 2 ? NY : NZ);
   constexpr int n1 = DIR == 1 ? NY : NX;
   constexpr int n2 = NDIM > 2 ? (DIR == 3 ? NY : NZ) : 1;
@@ -299,31 +303,37 @@ __device__ void flux_register(const DevParams &P, int b, int3 bc, double *sF, in
     const int m = at_node(P, l, pos[0], pos[1], pos[2]);
     const int along = s ? N : 0;
     if (m < 0) {
-      double *dst = P.freg + ((size_t)P.slot[b] * 2 * NDIM + 2 * (DIR - 1) + s) * NF * NFLX;
-      for (int q = threadIdx.x; q < NF * NFLX; q += blockDim.x) {
-        const int face = q / NFLX, v = q % NFLX;
+      double *dst = reg + ((size_t)P.slot[b] * 2 * NDIM + 2 * (DIR - 1) + s) * NF * nv;
+      for (int q = threadIdx.x; q < NF * nv; q += blockDim.x) {
+        const int face = q / nv, v = q % nv;
         dst[q] = sF[v * fstride + fidx(along, face % n1, face / n1)];
       }
     } else if (!P.leaf[m]) {
       const double w = NDIM > 2 ? 0.25 : 0.5;
-      for (int q = threadIdx.x; q < NF * NFLX; q += blockDim.x) {
-        const int face = q / NFLX, v = q % NFLX, q1 = face % n1, q2 = face / n1;
+      for (int q = threadIdx.x; q < NF * nv; q += blockDim.x) {
+        const int face = q / nv, v = q % nv, q1 = face % n1, q2 = face / n1;
         int o[3] = {0, 0, 0};
         o[DIR - 1] = s ? 0 : 1;
         o[T1] = q1 >= n1 / 2;
         if (NDIM > 2) o[T2] = q2 >= n2 / 2;
         const int f = at_node(P, l + 1, 2 * pos[0] + o[0], 2 * pos[1] + o[1], NDIM > 2 ? 2 * pos[2] + o[2] : 0);
-        const double *src = P.freg + ((size_t)P.slot[f] * 2 * NDIM + 2 * (DIR - 1) + (1 - s)) * NF * NFLX;
+        const double *src = reg + ((size_t)P.slot[f] * 2 * NDIM + 2 * (DIR - 1) + (1 - s)) * NF * nv;
         double acc = 0.0;
         for (int r2 = 0; r2 <= (NDIM > 2 ? 1 : 0); ++r2)
           for (int r1 = 0; r1 <= 1; ++r1) {
             const int f1 = 2 * (q1 - o[T1] * (n1 / 2)) + r1, f2 = NDIM > 2 ? 2 * (q2 - o[T2] * (n2 / 2)) + r2 : 0;
-            acc = acc + w * src[(f1 + n1 * f2) * NFLX + v];
+            acc = acc + w * src[(f1 + n1 * f2) * nv + v];
           }
         sF[v * fstride + fidx(along, q1, q2)] = acc;
       }
     }
   }
+}
+
+template <int NDIM, int NX, int NY, int NZ, int DIR, class FaceIdx>
+__device__ __forceinline__ void flux_register(const DevParams &P, int b, int3 bc, double *sF, int fstride,
+                                              FaceIdx fidx) {
+  flux_register_v<NDIM, NX, NY, NZ, DIR>(P, b, bc, sF, fstride, fidx, P.freg, NFLX);
 }
 
 // ---------------------------------------------------------------------------
@@ -468,7 +478,7 @@ __global__ void __launch_bounds__(320) k_dir(const DevParams P, const R *__restr
       u7[0] = R(0); u7[6] = R(0);
       flat = flat_coeff(p7, u7);
     }
-    if (P.sp_flat) P.sp_flat[sp_line_base<NDIM, NX, NY, NZ, DIR>(blockIdx.x) + t] = double(flat);
+    if (P.sp_flat) P.sp_flat[sp_line_base<NDIM, NX, NY, NZ, DIR>(P.slot ? P.slot[b] : (int)blockIdx.x) + t] = double(flat);
     R Wp[8], Wm[8];
     ppm_cell<R, DIR>(P, V5, flat, dtn, R(delta), Wp, Wm, st);
     const R *Vc = V5[2];
@@ -536,7 +546,7 @@ __global__ void __launch_bounds__(320) k_dir(const DevParams P, const R *__restr
 #pragma unroll
         for (int n = 0; n < 8; ++n) { Wm[n] = Vc[n]; Wp[n] = Vc[n]; }
       }
-      if (P.sp_fb) P.sp_fb[sp_line_base<NDIM, NX, NY, NZ, DIR>(blockIdx.x) + t] = fb;
+      if (P.sp_fb) P.sp_fb[sp_line_base<NDIM, NX, NY, NZ, DIR>(P.slot ? P.slot[b] : (int)blockIdx.x) + t] = fb;
     }
 #pragma unroll
     for (int q = 0; q < 7; ++q) {
@@ -571,7 +581,7 @@ __global__ void __launch_bounds__(320) k_dir(const DevParams P, const R *__restr
     }
     sF[FEINT * G::n + t] = fe;
     sF[FVOLU * G::n + t] = fv;
-    if (P.sp_mf) P.sp_mf[sp_line_base<NDIM, NX, NY, NZ, DIR>(blockIdx.x) + t] = double(F[FDENS]);
+    if (P.sp_mf) P.sp_mf[sp_line_base<NDIM, NX, NY, NZ, DIR>(P.slot ? P.slot[b] : (int)blockIdx.x) + t] = double(F[FDENS]);
   }
   __syncthreads();
   if constexpr (sizeof(R) == 8) {

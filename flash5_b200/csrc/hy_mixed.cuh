@@ -227,7 +227,7 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
       else flat = fmaxf(t0, sFlat[q - qs]);
     }
     if (P.sp_flat)
-      P.sp_flat[sp_line_base<NDIM, NX, NY, NZ, DIR>(blockIdx.x) + DirGeom<NDIM, NX, NY, NZ, double, DIR>::idx(i, j, k)] =
+      P.sp_flat[sp_line_base<NDIM, NX, NY, NZ, DIR>(P.slot ? P.slot[b] : (int)blockIdx.x) + DirGeom<NDIM, NX, NY, NZ, double, DIR>::idx(i, j, k)] =
           double(flat);
     const int sl[6] = {0, 1, 2, 3, 4, 7};
     float lft[8], rgt[8], delW[8], W6[8];
@@ -367,7 +367,7 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
         for (int n = 0; n < 8; ++n) { dWm[n] = 0.f; dWp[n] = 0.f; }
       }
       if (P.sp_fb)
-        P.sp_fb[sp_line_base<NDIM, NX, NY, NZ, DIR>(blockIdx.x) + DirGeom<NDIM, NX, NY, NZ, double, DIR>::idx(i, j, k)] = fb;
+        P.sp_fb[sp_line_base<NDIM, NX, NY, NZ, DIR>(P.slot ? P.slot[b] : (int)blockIdx.x) + DirGeom<NDIM, NX, NY, NZ, double, DIR>::idx(i, j, k)] = fb;
     }
 #pragma unroll
     for (int qq = 0; qq < 6; ++qq) {
@@ -558,7 +558,7 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
       G::dec(t, G::LC, 1, x, l);
       if (x < 0) continue;
       G::cell(x, l, i, j, k);
-      P.sp_mf[sp_line_base<NDIM, NX, NY, NZ, DIR>(blockIdx.x) + DirGeom<NDIM, NX, NY, NZ, double, DIR>::idx(i, j, k)] =
+      P.sp_mf[sp_line_base<NDIM, NX, NY, NZ, DIR>(P.slot ? P.slot[b] : (int)blockIdx.x) + DirGeom<NDIM, NX, NY, NZ, double, DIR>::idx(i, j, k)] =
           sF[FDENS * G::SC + t];
     }
   }

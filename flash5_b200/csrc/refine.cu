@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(256) k_node_halo(const DevParams P, const int 
   using H = Halo<NDIM, NX, NY, NZ>;
   const int b = list[blockIdx.x];
   const double *const st[5] = {P.s_in[0], P.s_in[1], P.s_in[2], P.s_in[3], P.s_in[4]};
-  double *o = out + (size_t)blockIdx.x * 6 * H::n;
+  double *o = out + (size_t)blockIdx.x * (6 + P.nsp) * H::n;
   for (int h = threadIdx.x; h < H::n; h += blockDim.x) {
     const int li = h % H::hx - 4, lj = NDIM > 1 ? (h / H::hx) % H::hy - 4 : 0;
     const int lk = NDIM > 2 ? h / (H::hx * H::hy) - 4 : 0;
@@ -157,6 +157,16 @@ __global__ void __launch_bounds__(256) k_node_halo(const DevParams P, const int 
     }
 #pragma unroll
     for (int q = 0; q < 6; ++q) o[q * H::n + h] = v[q];
+  }
+  // species and mass scalars after the six state values
+  for (int qh = threadIdx.x; qh < P.nsp * H::n; qh += blockDim.x) {
+    const int q = qh / H::n, h = qh % H::n;
+    const int li = h % H::hx - 4, lj = NDIM > 1 ? (h / H::hx) % H::hy - 4 : 0;
+    const int lk = NDIM > 2 ? h / (H::hx * H::hy) - 4 : 0;
+    o[(6 + q) * H::n + h] =
+        is_inside<NDIM, NX, NY, NZ>(li, lj, lk)
+            ? P.sp_in[(size_t)q * P.sp_ncells + (size_t)b * NCB + (size_t)((lk * NY + lj) * NX + li)]
+            : amr_guard_spec<NDIM, NX, NY, NZ>(P, P.sp_ncells, b, li, lj, lk, q);
   }
 }
 
@@ -174,9 +184,10 @@ __global__ void __launch_bounds__(256) k_regrid_fill(const RegridArgs a) {
   const int cc[3] = {c3.x, c3.y, c3.z};
   for (int c = threadIdx.x; c < NCB; c += blockDim.x) {
     double v[6];
+    const double *nh = a.nh + (size_t)(how == 1 ? a.slot[nb] : 0) * (6 + Pn.nsp) * H::n;
+    const int lp[3] = {c % NX, (c / NX) % NY, c / (NX * NY)};
     if (how == 1) {
-      const int lp[3] = {c % NX, (c / NX) % NY, c / (NX * NY)};
-      prolong_linear<NDIM, NX, NY, NZ>(a.nh + (size_t)a.slot[nb] * 6 * H::n, cc, lp, v);
+      prolong_linear<NDIM, NX, NY, NZ>(nh, cc, lp, v);
     } else {
       const size_t off = (size_t)o * NCB + c;
       v[0] = Po.s_in[0][off]; v[1] = Po.s_in[1][off]; v[2] = Po.s_in[2][off]; v[3] = Po.s_in[3][off];
@@ -193,6 +204,10 @@ __global__ void __launch_bounds__(256) k_regrid_fill(const RegridArgs a) {
     }
     Pn.s_out[0][no] = v[0]; Pn.s_out[1][no] = v[1]; Pn.s_out[2][no] = v[2]; Pn.s_out[3][no] = v[3];
     Pn.s_out[4][no] = e;
+    for (int q = 0; q < Pn.nsp; ++q)
+      Pn.sp_out[(size_t)q * Pn.sp_ncells + no] =
+          how == 1 ? prolong_scalar<NDIM, NX, NY, NZ>(nh, nh + (6 + q) * H::n, cc, lp)
+                   : Po.sp_in[(size_t)q * Po.sp_ncells + (size_t)o * NCB + c];
   }
 }
 

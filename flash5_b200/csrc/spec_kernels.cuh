@@ -33,6 +33,10 @@ namespace fhy {
 template <int NDIM, int NX, int NY, int NZ>
 __device__ __forceinline__ double load_spec(const DevParams &P, int b, int3 bc, int li, int lj, int lk, int q,
                                             size_t ncells) {
+  if (P.sp_lh && !is_inside<NDIM, NX, NY, NZ>(li, lj, lk)) {   // AMR: the leaf's species guard cells
+    using H = Halo<NDIM, NX, NY, NZ>;
+    return P.sp_lh[((size_t)P.slot[b] * P.nsp + q) * H::n + H::idx(li, lj, lk)];
+  }
   bool inside; int fx, fy, fz;
   const size_t o = cell_src<NDIM, NX, NY, NZ>(P, b, bc, li, lj, lk, inside, fx, fy, fz);
   return __ldg(P.sp_in + (size_t)q * ncells + o);
@@ -41,6 +45,10 @@ __device__ __forceinline__ double load_spec(const DevParams &P, int b, int3 bc, 
 // velocity component d (0-based) of a cell, mirrored in reflecting guard cells
 template <int NDIM, int NX, int NY, int NZ>
 __device__ __forceinline__ double load_vel(const DevParams &P, int b, int3 bc, int li, int lj, int lk, int d) {
+  if (P.lh && !is_inside<NDIM, NX, NY, NZ>(li, lj, lk)) {       // AMR: the leaf guard buffer (mirrored)
+    using H = Halo<NDIM, NX, NY, NZ>;
+    return P.lh[(size_t)P.slot[b] * 5 * H::n + (1 + d) * H::n + H::idx(li, lj, lk)];
+  }
   bool inside; int f[3];
   const size_t o = cell_src<NDIM, NX, NY, NZ>(P, b, bc, li, lj, lk, inside, f[0], f[1], f[2]);
   const double v = __ldg(P.s_in[1 + d] + o);
@@ -85,17 +93,13 @@ __global__ void __launch_bounds__(256) k_spec_sig(const DevParams P, double *__r
   double *sV = reinterpret_cast<double *>(smem_raw);     // [3][B::n]
   double *sX = sV + 3 * B::n;                            // [E::n]
   const int b = P.blk_list ? P.blk_list[blockIdx.x] : blockIdx.x;
+  const int slot = P.slot ? P.slot[b] : (int)blockIdx.x;
   const int3 bc = blk_coords(P, b);
   for (int c = threadIdx.x; c < B::n; c += blockDim.x) {
     const int i = c % B::bx - 1, j = NDIM > 1 ? (c / B::bx) % B::by - 1 : 0;
     const int k = NDIM > 2 ? c / (B::bx * B::by) - 1 : 0;
-    bool inside; int f[3];
-    const size_t o = cell_src<NDIM, NX, NY, NZ>(P, b, bc, i, j, k, inside, f[0], f[1], f[2]);
 #pragma unroll
-    for (int d = 0; d < NDIM; ++d) {
-      const double v = __ldg(P.s_in[1 + d] + o);
-      sV[d * B::n + c] = f[d] ? -v : v;
-    }
+    for (int d = 0; d < NDIM; ++d) sV[d * B::n + c] = load_vel<NDIM, NX, NY, NZ>(P, b, bc, i, j, k, d);
   }
   for (int q = 0; q < P.nsp; ++q) {
     for (int c = threadIdx.x; c < E::n; c += blockDim.x) {
@@ -116,7 +120,7 @@ __global__ void __launch_bounds__(256) k_spec_sig(const DevParams P, double *__r
         double g;
         if (lam > 0.) g = s0 - sm;
         else g = sp - s0;
-        SSIG[(((size_t)blockIdx.x * NDIM + d) * P.nsp + q) * B::n + c] = lam * g;
+        SSIG[(((size_t)slot * NDIM + d) * P.nsp + q) * B::n + c] = lam * g;
       }
     }
     __syncthreads();
@@ -136,8 +140,9 @@ struct SpecGeom {
   }
   // shared memory: per line cell the face values of one species (left,
   // right), the normal velocity, the flattening coefficient, the velocities
-  // along the two CTU axes and the fallback flag; the staged species
-  static constexpr size_t smem_bytes() { return (size_t)L::n * 6 * sizeof(double) + (size_t)ns * sizeof(double) + L::n; }
+  // along the two CTU axes, the face flux and the fallback flag; the staged
+  // species
+  static constexpr size_t smem_bytes() { return (size_t)L::n * 7 * sizeof(double) + (size_t)ns * sizeof(double) + L::n; }
 };
 
 template <int NDIM, int NX, int NY, int NZ, int DIR, bool FIRST, bool LAST>
@@ -154,19 +159,22 @@ __global__ void __launch_bounds__(256) k_spec_dir(const DevParams P, const doubl
   double *sFl = sU + L::n;            // flattening coefficient
   double *sA1 = sFl + L::n;           // velocities along the CTU axes A1, A2
   double *sA2 = sA1 + L::n;
-  double *sX = sA2 + L::n;            // the staged species
+  double *sFs = sA2 + L::n;           // species flux at the face left of each line cell
+  double *sX = sFs + L::n;            // the staged species
   unsigned char *sFb = reinterpret_cast<unsigned char *>(sX + SG::ns);
   const int b = P.blk_list ? P.blk_list[blockIdx.x] : blockIdx.x;
+  const int slot = P.slot ? P.slot[b] : (int)blockIdx.x;
   const int3 bc = blk_coords(P, b);
   const double dt = P.dt_dev ? *P.dt_dev : P.dt;
-  const double *del = P.del;
+  double del[3];
+  blk_deltas(P, b, del);                // the block's level
   const double delta = del[DIR - 1];
   const double hdtx = 0.5 * dt / del[0], hdty = 0.5 * dt / del[1], hdtz = 0.5 * dt / del[2];
   constexpr int A1 = DIR == 1 ? 2 : (DIR == 2 ? 3 : 1), S1 = DIR == 1 ? 3 : (DIR == 2 ? 1 : 2);
   constexpr int A2 = DIR == 1 ? 3 : (DIR == 2 ? 1 : 2), S2 = DIR == 1 ? 2 : (DIR == 2 ? 3 : 1);
   const bool ctu = NDIM == 3 && P.use_ctu;
-  const size_t lb = sp_line_base<NDIM, NX, NY, NZ, DIR>(blockIdx.x);
-  const double *ssb = SSIG + (size_t)blockIdx.x * NDIM * P.nsp * B::n;
+  const size_t lb = sp_line_base<NDIM, NX, NY, NZ, DIR>(slot);
+  const double *ssb = SSIG + (size_t)slot * NDIM * P.nsp * B::n;
 
   // ---- per line cell quantities shared by every species
   for (int t = threadIdx.x; t < L::n; t += blockDim.x) {
@@ -261,20 +269,34 @@ __global__ void __launch_bounds__(256) k_spec_dir(const DevParams P, const doubl
       sSr[t] = r;
     }
     __syncthreads();
-    // ---- upwind fluxes at both faces of every interior cell, divergence
+    // ---- upwind fluxes F_dens * X at the faces (the face left of line cell
+    // t for along in [0, N]); on AMR hierarchies the fine/coarse faces
+    // through the species flux register
+    for (int t = threadIdx.x; t < L::n; t += blockDim.x) {
+      int i, j, k;
+      L::decode(t, i, j, k);
+      if (L::along(i, j, k) < 0) continue;
+      const double m = P.sp_mf[lb + t];
+      if (m < 0.) sFs[t] = m * sSl[t];
+      else sFs[t] = m * sSr[t - L::stride];
+    }
+    __syncthreads();
+    if (P.sp_freg) {
+      flux_register_v<NDIM, NX, NY, NZ, DIR>(P, b, bc, sFs, 0, [](int along, int t1, int t2) {
+        const int i = DIR == 1 ? along : t1, j = DIR == 1 ? t1 : (DIR == 2 ? along : t2),
+                  k = DIR == 3 ? along : (NDIM > 2 ? t2 : 0);
+        return L::idx(i, j, k);
+      }, P.sp_freg + (size_t)q * P.sp_freg_stride, 1);
+      __syncthreads();
+    }
+    // ---- divergence
     for (int t = threadIdx.x; t < L::n; t += blockDim.x) {
       int i, j, k;
       L::decode(t, i, j, k);
       const int a = L::along(i, j, k);
       if (a < 0 || a >= L::nd) continue;
       const size_t off = (size_t)b * NCB + (size_t)((k * NY + j) * NX + i);
-      const int tr = t + L::stride;
-      const double mL = P.sp_mf[lb + t], mR = P.sp_mf[lb + tr];
-      double FL, FR;
-      if (mL < 0.) FL = mL * sSl[t];
-      else FL = mL * sSr[t - L::stride];
-      if (mR < 0.) FR = mR * sSl[tr];
-      else FR = mR * sSr[t];
+      const double FL = sFs[t], FR = sFs[t + L::stride];
       double acc = (FL - FR) / delta;
       if (!FIRST) acc = SACC[(size_t)q * ncells + off] + acc;
       if (!LAST) {

@@ -99,8 +99,10 @@ typedef struct flash_hy_params {
    * (the default, unsplit/Config:140-143): PPM face values, upwind fluxes
    * F_dens * X, the conservative update and, for species only, the
    * renormalisation to a unit sum (hy_unsplitUpdate.F90:827-859).  At most
-   * FLASH_HY_MAX_SPECIES in all.  Uniform grids only (AMR hierarchies and
-   * the split step refuse them: FLASH_HY_ERR_UNSUPPORTED). */
+   * FLASH_HY_MAX_SPECIES in all.  Uniform grids and AMR hierarchies (the
+   * species are restricted, prolonged in per-mass form into the guard cells
+   * and corrected at fine/coarse faces like the mass flux); the split step
+   * refuses them (FLASH_HY_ERR_UNSUPPORTED). */
   int nspecies;            /* NSPECIES                                     */
   int nmass_scalars;       /* NMASS_SCALARS                                */
 } flash_hy_params;

@@ -1415,22 +1415,28 @@ static void amr_correct_fluxes(const ctx_t *c, const amr_t *a, const flash_hy_gr
           if (a->ndim > 2) o[t2] = q2 >= n2 / 2;
           int f = amr_at(a, l + 1, 2 * pos[0] + o[0], 2 * pos[1] + o[1], a->ndim > 2 ? 2 * pos[2] + o[2] : 0);
           int ffa = s ? 0 : a->N[d];                     /* the fine leaf's face facing b */
-          double acc[NFLX];
-          for (int v = 0; v < NFLX; ++v) acc[v] = 0.;
+          const int ns = c->nsp;
+          double acc[NFLX + FLASH_HY_MAX_SPECIES];
+          for (int v = 0; v < NFLX + ns; ++v) acc[v] = 0.;
           for (int r2 = 0; r2 <= (a->ndim > 2); ++r2)
             for (int r1 = 0; r1 <= 1; ++r1) {
               int fl[3];
               fl[d] = ffa;
               fl[t1] = 2 * (q1 - o[t1] * (n1 / 2)) + r1;
               if (a->ndim > 2) fl[t2] = 2 * (q2 - o[t2] * (n2 / 2)) + r2; else fl[2] = 0;
-              const double *F = &W[f].flux[d][cidx(c, fl[0] + NGUARD, fl[1] + NGUARD, c->k3 ? fl[2] + NGUARD : 0) * NFLX];
+              const size_t fc = cidx(c, fl[0] + NGUARD, fl[1] + NGUARD, c->k3 ? fl[2] + NGUARD : 0);
+              const double *F = &W[f].flux[d][fc * NFLX];
               for (int v = 0; v < NFLX; ++v) acc[v] = acc[v] + w * F[v];
+              /* species and mass-scalar fluxes too (all NFLUXES components) */
+              for (int v = 0; v < ns; ++v) acc[NFLX + v] = acc[NFLX + v] + w * W[f].spc_flux[d][fc * ns + v];
             }
           int cl[3];
           cl[d] = face; cl[t1] = q1;
           if (a->ndim > 2) cl[t2] = q2; else cl[2] = 0;
-          double *F = &W[b].flux[d][cidx(c, cl[0] + NGUARD, cl[1] + NGUARD, c->k3 ? cl[2] + NGUARD : 0) * NFLX];
+          const size_t cc2 = cidx(c, cl[0] + NGUARD, cl[1] + NGUARD, c->k3 ? cl[2] + NGUARD : 0);
+          double *F = &W[b].flux[d][cc2 * NFLX];
           for (int v = 0; v < NFLX; ++v) F[v] = acc[v];
+          for (int v = 0; v < ns; ++v) W[b].spc_flux[d][cc2 * ns + v] = acc[NFLX + v];
         }
     }
 }

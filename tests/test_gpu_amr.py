@@ -20,32 +20,39 @@ from tests.test_gpu_parity import momentum_normalised_l1
 VARS = ("dens", "velx", "vely", "velz", "eint", "ener", "pres", "temp", "gamc", "game")
 
 
-def ring(ndim, nb, nblk, max_level, bc, r2=0.06, w=0.004):
+def ring(ndim, nb, nblk, max_level, bc, r2=0.06, w=0.004, **sk):
     """Hierarchy refined around a circle (sphere): leaves on several levels."""
-    g = AmrGrid(ndim, (nb,) * ndim, (nblk,) * ndim, max_level, bc=bc)
+    g = AmrGrid(ndim, (nb,) * ndim, (nblk,) * ndim, max_level, bc=bc, **sk)
     f = lambda X, Y, Z: 1.0 + 0.8 * np.tanh(((X - 0.5) ** 2 + (Y - 0.45) ** 2 + (Z - 0.5) ** 2 * (ndim > 2) - r2) / w)
     g.refine_levels(indicator_refiner(g, f, 0.05))
     return g
 
 
-def amr_case(name, **pkw):
+def amr_case(name, nspecies=0, nmass_scalars=0, **pkw):
+    sk = {"nspecies": nspecies, "nmass_scalars": nmass_scalars}
     if name == "kh2d_ring":
-        g = ring(2, 8, 8, 3, "periodic", r2=0.02, w=0.002)
-        return g, setups.kelvin_helmholtz(g), abi.default_params(gamma=5.0 / 3.0, **pkw)
-    if name == "quad2d_16":
-        g = ring(2, 16, 6, 3, "outflow", r2=0.02, w=0.003)
-        return g, setups.four_quadrant(g), abi.default_params(**pkw)
-    if name == "sod2d_reflect":
-        g = ring(2, 8, 8, 3, "reflecting", r2=0.01, w=0.002)
-        return g, setups.sod(g, xangle=30.0), abi.default_params(**pkw)
-    if name == "kh3d_ring":
-        g = ring(3, 8, 2, 3, "periodic")
-        return g, setups.kelvin_helmholtz(g), abi.default_params(gamma=5.0 / 3.0, **pkw)
-    raise KeyError(name)
+        g = ring(2, 8, 8, 3, "periodic", r2=0.02, w=0.002, **sk)
+        u, p = setups.kelvin_helmholtz(g), abi.default_params(gamma=5.0 / 3.0, **pkw)
+    elif name == "quad2d_16":
+        g = ring(2, 16, 6, 3, "outflow", r2=0.02, w=0.003, **sk)
+        u, p = setups.four_quadrant(g), abi.default_params(**pkw)
+    elif name == "sod2d_reflect":
+        g = ring(2, 8, 8, 3, "reflecting", r2=0.01, w=0.002, **sk)
+        u, p = setups.sod(g, xangle=30.0), abi.default_params(**pkw)
+    elif name == "kh3d_ring":
+        g = ring(3, 8, 2, 3, "periodic", **sk)
+        u, p = setups.kelvin_helmholtz(g), abi.default_params(gamma=5.0 / 3.0, **pkw)
+    else:
+        raise KeyError(name)
+    return g, setups.add_species(g, u), p
 
 
 def run_amr_pair(case, nsteps=4, **pkw):
     grid, unk0, params = amr_case(case, **pkw)
+    return _run_amr(grid, unk0, params, nsteps)
+
+
+def _run_amr(grid, unk0, params, nsteps):
     ref = unk0.copy()
     o = orc.Oracle(params, grid)
     o.eos_init(ref)

@@ -6,10 +6,10 @@
   block-list step;
 * the hydro variables are bit-identical with and without species;
 * mixed precision: species within 1e-6 relative L1 of the FP64 GPU run;
-* the split step and AMR hierarchies refuse species.
+* species on AMR hierarchies (restriction, guard cells, the species flux
+  register) and through a regrid equal the oracle bit for bit;
+* the split step refuses species.
 """
-import ctypes as C
-
 import numpy as np
 import pytest
 
@@ -104,7 +104,7 @@ def test_mixed_species_within_tolerance(case):
 
 
 @pytest.mark.gpu
-def test_split_step_and_amr_refuse_species():
+def test_split_step_refuses_species():
     grid, unk, params = make_case("kh3d", nspecies=1)
     h = Hydro(params, grid)
     h.upload(unk)
@@ -113,12 +113,47 @@ def test_split_step_and_amr_refuse_species():
         h.compute_fluxes([0], dt, abi.UPDATE_NONE)
     assert e.value.status & abi.ERR_UNSUPPORTED
     h.close()
-    from flash5_b200.amr import four_quadrant_hierarchy
-    ag = four_quadrant_hierarchy(nblk=4, max_level=2)
-    p = abi.default_params()
-    p.nspecies = 1
-    lib = abi.load_library()
-    ctx = C.c_void_p()
-    gd = ag.desc()
-    st = lib.flash_hy_create(C.byref(p), C.byref(gd), 0, C.byref(ctx))
-    assert st == abi.ERR_UNSUPPORTED and not ctx
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["kh2d_ring", "quad2d_16", "sod2d_reflect", "kh3d_ring"])
+def test_amr_species_match_oracle(case):
+    """Species on AMR hierarchies: restriction, guard cells (prolonged in
+    per-mass form), the species flux register at fine/coarse faces: every
+    leaf variable equal to the oracle bit for bit (FP64)."""
+    from tests.test_gpu_amr import _run_amr, amr_case, VARS
+    from flash5_b200.grid import VAR
+    grid, unk, params = amr_case(case, nspecies=2, nmass_scalars=1)
+    grid, ref, out, steps = _run_amr(grid, unk, params, 4)
+    leaves = grid.leaf_ids
+    a, b = grid.interior(out)[leaves], grid.interior(ref)[leaves]
+    sp = grid.species
+    assert np.array_equal(a[..., sp], b[..., sp]), np.abs(a[..., sp] - b[..., sp]).max()
+    for v in VARS:
+        assert np.array_equal(a[..., VAR[v]], b[..., VAR[v]]), v
+
+
+@pytest.mark.gpu
+def test_amr_species_regrid_matches_oracle():
+    from tests.test_gpu_amr import amr_case
+    from flash5_b200.amr import mark_refine_derefine, regrid_native
+    grid, unk, params = amr_case("quad2d_16", nspecies=2, nmass_scalars=1)
+    ref = unk.copy()
+    o = orc.Oracle(params, grid)
+    o.eos_init(ref)
+    h = Hydro(params, grid)
+    _steps(h, o, unk, ref, 2)
+    errs = [h.estimate_error("dens", 0.01)]
+    lv, pv = errs[0][grid.leaf_ids], errs[0][~grid.is_leaf]
+    refine, derefine = mark_refine_derefine(grid, errs, np.quantile(lv, 0.95), np.quantile(pv, 0.7))
+    g2, src, how = regrid_native(grid, refine, derefine)
+    assert np.any(how == 1) and np.any(how == 2)
+    h2 = h.regrid(g2, src, how)
+    h.close()
+    ref2 = o.regrid(ref, g2, src, how)
+    out = g2.new_unk()
+    h2.download(out)
+    h2.close()
+    leaves = g2.leaf_ids
+    a, b = g2.interior(out)[leaves], g2.interior(ref2)[leaves]
+    assert np.array_equal(a, b), np.abs(a - b).max()
