@@ -76,7 +76,7 @@ struct flash_hy_ctx {
   // accumulator, SpcSig scratch, face mass fluxes and fallback flags left
   // by the hydro direction kernels
   int nsp, nspec;
-  double *spec[2], *sacc, *ssig, *sp_mf, *sp_flat;
+  double *spec[2], *sp_mf, *sp_flat;
   unsigned char *sp_fb;
   double *sp_lh, *sp_gp, *sp_freg;   // AMR: species guard cells, parent copies, flux register
   size_t sp_freg_stride;
@@ -255,6 +255,9 @@ extern "C" int flash_hy_create(const flash_hy_params *params, const flash_hy_gri
   int nz = g->ndim > 2 ? g->nzb : 1, ny = g->ndim > 1 ? g->nyb : 1;
   if (!shape_supported(g->ndim, g->nxb, ny, nz)) return FLASH_HY_ERR_UNSUPPORTED;
   if (g->nblocks <= 0 || !g->block_coords || g->nguard < 0) return FLASH_HY_ERR_BAD_ARG;
+  // the species pass addresses the cells of one species with 31-bit offsets
+  if (params->nspecies + params->nmass_scalars > 0 && (double)g->nblocks * g->nxb * ny * nz > 2147483647.0)
+    return FLASH_HY_ERR_UNSUPPORTED;
   int nbx = g->nblk_l1[0], nby = g->ndim > 1 ? g->nblk_l1[1] : 1, nbz = g->ndim > 2 ? g->nblk_l1[2] : 1;
   const bool amr = g->max_level > 1;
   std::vector<int> amr_at, amr_parent, amr_leaf;
@@ -388,11 +391,8 @@ extern "C" int flash_hy_create(const flash_hy_params *params, const flash_hy_gri
   if (c->nsp > 0) {
     // per-slot scratch: a slot per block, or per leaf on an AMR hierarchy
     const size_t nslot = amr ? (size_t)c->nleaves : (size_t)g->nblocks;
-    const size_t box = (size_t)(g->nxb + 2) * (g->ndim > 1 ? ny + 2 : 1) * (g->ndim > 2 ? nz + 2 : 1);
     const size_t lines = (size_t)(g->nxb + 2) * (g->ndim > 1 ? ny : 1) * (g->ndim > 2 ? nz : 1);
     for (int s = 0; s < 2; ++s) ALLOC(c->spec[s], (size_t)c->nsp * c->ncells * sizeof(double));
-    ALLOC(c->sacc, (size_t)c->nsp * c->ncells * sizeof(double));
-    ALLOC(c->ssig, nslot * g->ndim * c->nsp * box * sizeof(double));
     ALLOC(c->sp_mf, nslot * g->ndim * lines * sizeof(double));
     ALLOC(c->sp_fb, nslot * g->ndim * lines);
     ALLOC(c->sp_flat, nslot * g->ndim * lines * sizeof(double));
@@ -448,7 +448,7 @@ extern "C" int flash_hy_destroy(flash_hy_ctx *c) {
   cudaFree(c->d_owned); cudaFree(c->d_owned_mask); cudaFree(c->d_send); cudaFree(c->d_recv);
   cudaFree(c->d_fstore);
   for (int s = 0; s < 2; ++s) cudaFree(c->spec[s]);
-  cudaFree(c->sacc); cudaFree(c->ssig); cudaFree(c->sp_mf); cudaFree(c->sp_fb); cudaFree(c->sp_flat);
+  cudaFree(c->sp_mf); cudaFree(c->sp_fb); cudaFree(c->sp_flat);
   cudaFree(c->d_err);
   cudaFree(c->sp_lh); cudaFree(c->sp_gp); cudaFree(c->sp_freg);
   free(c->h_blk_at);
@@ -690,14 +690,10 @@ static int enqueue_step(flash_hy_ctx *c, double dt, const int *d_list, int nlaun
     if (fmode != 0) return fail(c, FLASH_HY_ERR_UNSUPPORTED, "species with the split step%s", "");
     SpecArgs sa;
     sa.P = a.P;
-    sa.ssig = c->ssig;
-    sa.sacc = c->sacc;
     sa.ncells = c->ncells;
     sa.nlaunch = nlaunch;
     sa.stream = c->stream;
     sa.nlev = a.nlev;
-    sa.leaves = a.leaves;
-    sa.nleaves = a.nleaves;
     for (int l = 0; l < 17; ++l) { sa.lev_list[l] = a.lev_list[l]; sa.lev_count[l] = a.lev_count[l]; }
     const int ns = spec_step(sa, c->ndim, c->nx, c->ny, c->nz);
     if (ns < 0) return fail(c, FLASH_HY_ERR_CUDA, "species launch failed: %s", cudaGetErrorString(cudaGetLastError()));

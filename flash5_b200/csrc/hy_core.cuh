@@ -99,6 +99,23 @@ __device__ __forceinline__ int at_node(const DevParams &P, int l, int x, int y, 
 
 template <class R> __device__ __forceinline__ R rmax(R a, R b) { return a > b ? a : b; }
 template <class R> __device__ __forceinline__ R rmin(R a, R b) { return a < b ? a : b; }
+
+// x / b rounded to nearest, from rb = RN(1 / b) (Markstein's theorem,
+// "Computation of elementary functions on the IBM RISC System/6000
+// processor", IBM J. Res. Dev. 34 (1990): q0 = RN(x rb) is within an ulp of
+// x / b, the remainder x - q0 b is exact with an FMA, and
+// RN(q0 + (x - q0 b) rb) = RN(x / b)).  Outside the exponent range where
+// the remainder cannot underflow or the product overflow (zeros,
+// subnormals, infinities and NaN included) it divides.  Equal to x / b in
+// every bit: a CPU test checks the method on random and special operands,
+// and the FP64 GPU parity tests compare the kernels that use it with the
+// oracle's divisions.
+__device__ __forceinline__ double div_rn(double x, double b, double rb) {
+  const double q0 = x * rb;
+  const double a = fabs(q0), ax = fabs(x);
+  if (a > 0x1p-960 && a < 0x1p1000 && ax > 0x1p-960 && ax < 0x1p1000) return fma(fma(-q0, b, x), rb, q0);
+  return x / b;
+}
 __device__ __forceinline__ double rsign(double a, double b) { return copysign(fabs(a), b); }
 __device__ __forceinline__ float rsign(float a, float b) { return copysignf(fabsf(a), b); }
 __device__ __forceinline__ double rabs(double a) { return fabs(a); }

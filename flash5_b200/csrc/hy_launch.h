@@ -32,20 +32,16 @@ struct StepArgs {
 // the species / mass-scalar pass after the hydro direction kernels
 struct SpecArgs {
   DevParams P;        // the step's parameters (species buffers, mass fluxes, flags)
-  double *ssig;       // SpcSig scratch, [slot][ndim][nsp][box]
-  double *sacc;       // [nsp][ncells] flux-divergence accumulator
   size_t ncells;
   int nlaunch;
   cudaStream_t stream;
-  // AMR (nlev > 0): k_spec_sig over all leaves, the direction kernels one
-  // launch per level, finest first (the species flux register)
+  // AMR (nlev > 0): one launch per level, finest first (the species flux
+  // register)
   int nlev;
-  const int *leaves;
-  int nleaves;
   const int *lev_list[17];
   int lev_count[17];
 };
-// launches k_spec_sig + one k_spec_dir per direction; returns their number or -2
+// launches k_spec_step (once, or once per level); returns the launch count or -2
 int spec_step(const SpecArgs &a, int ndim, int nx, int ny, int nz);
 
 // the refinement criterion of every listed block (all blocks without a list)

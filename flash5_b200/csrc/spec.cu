@@ -5,46 +5,30 @@
 
 namespace fhy {
 
-template <int NDIM, int NX, int NY, int NZ, int DIR, bool FIRST, bool LAST>
-static bool launch_spec_dir(const SpecArgs &a) {
-  const size_t smem = SpecGeom<NDIM, NX, NY, NZ, DIR>::smem_bytes();
+template <int NDIM, int NX, int NY, int NZ>
+static int run_spec(const SpecArgs &a) {
+  using SS = SpecStep<NDIM, NX, NY, NZ>;
+  const size_t smem = SS::smem_bytes();
+  if (smem > 48 * 1024 &&
+      (cudaFuncSetAttribute(k_spec_step<NDIM, NX, NY, NZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+           cudaSuccess ||
+       cudaFuncSetAttribute(k_spec_step<NDIM, NX, NY, NZ>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                            cudaSharedmemCarveoutMaxShared) != cudaSuccess))
+    return -2;
   if (a.nlev == 0) {
-    k_spec_dir<NDIM, NX, NY, NZ, DIR, FIRST, LAST><<<a.nlaunch, 256, smem, a.stream>>>(a.P, a.ssig, a.sacc, a.ncells);
-    return cudaGetLastError() == cudaSuccess;
+    k_spec_step<NDIM, NX, NY, NZ><<<a.nlaunch, SS::NT, smem, a.stream>>>(a.P, a.ncells);
+    return cudaGetLastError() == cudaSuccess ? 1 : -2;
   }
   DevParams P = a.P;
+  int n = 0;
   for (int l = a.nlev; l >= 1; --l) {          // finest first: the fine species fluxes go to the register
     if (a.lev_count[l] == 0) continue;
     P.blk_list = a.lev_list[l];
-    k_spec_dir<NDIM, NX, NY, NZ, DIR, FIRST, LAST><<<a.lev_count[l], 256, smem, a.stream>>>(P, a.ssig, a.sacc,
-                                                                                         a.ncells);
-    if (cudaGetLastError() != cudaSuccess) return false;
+    k_spec_step<NDIM, NX, NY, NZ><<<a.lev_count[l], SS::NT, smem, a.stream>>>(P, a.ncells);
+    if (cudaGetLastError() != cudaSuccess) return -2;
+    ++n;
   }
-  return true;
-}
-
-template <int NDIM, int NX, int NY, int NZ>
-static int run_spec(const SpecArgs &a) {
-  DevParams P = a.P;
-  int n0 = a.nlaunch;
-  if (a.nlev > 0) { P.blk_list = a.leaves; n0 = a.nleaves; }
-  k_spec_sig<NDIM, NX, NY, NZ><<<n0, 256, SigGeom<NDIM, NX, NY, NZ>::smem_bytes(), a.stream>>>(P, a.ssig, a.ncells);
-  if (cudaGetLastError() != cudaSuccess) return -2;
-  int nl = 1;
-  if (a.nlev > 0) {
-    nl = 0;
-    for (int l = 1; l <= a.nlev; ++l) nl += a.lev_count[l] > 0;
-  }
-  if constexpr (NDIM == 2) {
-    const bool ok = launch_spec_dir<NDIM, NX, NY, NZ, 1, true, false>(a) &&
-                    launch_spec_dir<NDIM, NX, NY, NZ, 2, false, true>(a);
-    return ok ? 1 + 2 * nl : -2;
-  } else {
-    const bool ok = launch_spec_dir<NDIM, NX, NY, NZ, 1, true, false>(a) &&
-                    launch_spec_dir<NDIM, NX, NY, NZ, 2, false, false>(a) &&
-                    launch_spec_dir<NDIM, NX, NY, NZ, 3, false, true>(a);
-    return ok ? 1 + 3 * nl : -2;
-  }
+  return n;
 }
 
 int spec_step(const SpecArgs &a, int ndim, int nx, int ny, int nz) {
