@@ -72,9 +72,9 @@ struct flash_hy_ctx {
   int *d_owned_mask;           // 1 for owned blocks (dt reduction)
   int *d_send, n_send, *d_recv, n_recv;  // blocks packed for / unpacked from other ranks
   double *d_fstore;            // stored fluxes of the split step
-  // species and mass scalars: state [2][nsp][ncells], flux-divergence
-  // accumulator, SpcSig scratch, face mass fluxes and fallback flags left
-  // by the hydro direction kernels
+  double *d_sp_fstore;         // and their species fluxes
+  // species and mass scalars: state [2][nsp][ncells]; face mass fluxes,
+  // fallback flags and flattening left by the hydro direction kernels
   int nsp, nspec;
   double *spec[2], *sp_mf, *sp_flat;
   unsigned char *sp_fb;
@@ -160,6 +160,7 @@ static void fill_devparams(const flash_hy_ctx *c, DevParams &P) {
     P.sp_fb = c->sp_fb;
     P.sp_flat = c->sp_flat;
     P.sp_ncells = c->ncells;
+    P.sp_fstore = c->d_sp_fstore;
     if (c->amr) {
       P.sp_lh = c->sp_lh;
       P.sp_gp = c->sp_gp;
@@ -447,6 +448,7 @@ extern "C" int flash_hy_destroy(flash_hy_ctx *c) {
   for (int l = 0; l < 17; ++l) { cudaFree(c->d_lev_leaves[l]); cudaFree(c->d_lev_parents[l]); }
   cudaFree(c->d_owned); cudaFree(c->d_owned_mask); cudaFree(c->d_send); cudaFree(c->d_recv);
   cudaFree(c->d_fstore);
+  cudaFree(c->d_sp_fstore);
   for (int s = 0; s < 2; ++s) cudaFree(c->spec[s]);
   cudaFree(c->sp_mf); cudaFree(c->sp_fb); cudaFree(c->sp_flat);
   cudaFree(c->d_err);
@@ -687,9 +689,9 @@ static int enqueue_step(flash_hy_ctx *c, double dt, const int *d_list, int nlaun
   if (n == -1) return fail(c, FLASH_HY_ERR_UNSUPPORTED, "unsupported block shape%s", "");
   if (n < 0) return fail(c, FLASH_HY_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(cudaGetLastError()));
   if (c->nsp > 0) {
-    if (fmode != 0) return fail(c, FLASH_HY_ERR_UNSUPPORTED, "species with the split step%s", "");
     SpecArgs sa;
     sa.P = a.P;
+    sa.P.sp_fstore = c->d_sp_fstore;
     sa.ncells = c->ncells;
     sa.nlaunch = nlaunch;
     sa.stream = c->stream;
@@ -807,11 +809,12 @@ static int ensure_fstore(flash_hy_ctx *c) {
   const size_t nf = (size_t)(c->nx + 1) * c->ny * c->nz;
   const size_t per = (size_t)NFLX * nf + c->ncb;
   CUDA_OK(c, cudaMalloc((void **)&c->d_fstore, (size_t)c->nblocks * c->ndim * per * sizeof(double)));
+  if (c->nsp > 0)
+    CUDA_OK(c, cudaMalloc((void **)&c->d_sp_fstore, (size_t)c->nblocks * c->ndim * c->nsp * nf * sizeof(double)));
   return 0;
 }
 
 extern "C" int flash_hy_compute_fluxes(flash_hy_ctx *c, int blockCount, const int *blockList, double dt, int flags) {
-  if (c && c->nsp > 0) return fail(c, FLASH_HY_ERR_UNSUPPORTED, "species with the split step%s", "");
   if (!c || blockCount < 0 || (blockCount > 0 && !blockList)) return FLASH_HY_ERR_BAD_ARG;
   if (flags != FLASH_HY_UPDATE_NONE && flags != FLASH_HY_UPDATE_ALL) return fail(c, FLASH_HY_ERR_BAD_ARG, "flags%s", "");
   if (c->amr) return fail(c, FLASH_HY_ERR_UNSUPPORTED, "split step on an AMR hierarchy%s", "");
@@ -833,7 +836,6 @@ extern "C" int flash_hy_compute_fluxes(flash_hy_ctx *c, int blockCount, const in
 }
 
 extern "C" int flash_hy_update_solution(flash_hy_ctx *c, int blockCount, const int *blockList, double dt) {
-  if (c && c->nsp > 0) return fail(c, FLASH_HY_ERR_UNSUPPORTED, "species with the split step%s", "");
   if (!c || blockCount < 0 || (blockCount > 0 && !blockList)) return FLASH_HY_ERR_BAD_ARG;
   if (c->amr) return fail(c, FLASH_HY_ERR_UNSUPPORTED, "split step on an AMR hierarchy%s", "");
   if (!c->d_fstore) return fail(c, FLASH_HY_ERR_BAD_ARG, "no stored fluxes (flash_hy_compute_fluxes first)%s", "");
@@ -860,16 +862,27 @@ static int flux_span(flash_hy_ctx *c, int blk, int dir, size_t &off, size_t &nf)
   return 0;
 }
 
+// species fluxes of a block and direction in the species flux store
+static size_t sp_flux_off(const flash_hy_ctx *c, int blk, int dir, size_t nf) {
+  return ((size_t)blk * c->ndim + (dir - 1)) * c->nsp * nf;
+}
+
 extern "C" int flash_hy_get_fluxes(flash_hy_ctx *c, int blk, int dir, double *flx) {
   if (!c || !flx) return FLASH_HY_ERR_BAD_ARG;
   size_t off, nf;
   if (flux_span(c, blk, dir, off, nf)) return fail(c, FLASH_HY_ERR_BAD_ARG, "get_fluxes: %s", "bad block/direction");
   CUDA_OK(c, cudaSetDevice(c->device));
-  std::vector<double> h(NFLX * nf);
+  const int nfl = NFLX + c->nsp;
+  std::vector<double> h(NFLX * nf), hs((size_t)c->nsp * nf);
   CUDA_OK(c, cudaMemcpyAsync(h.data(), c->d_fstore + off, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (c->nsp > 0)
+    CUDA_OK(c, cudaMemcpyAsync(hs.data(), c->d_sp_fstore + sp_flux_off(c, blk, dir, nf), hs.size() * sizeof(double),
+                               cudaMemcpyDeviceToHost, c->stream));
   CUDA_OK(c, cudaStreamSynchronize(c->stream));
-  for (size_t f = 0; f < nf; ++f)
-    for (int v = 0; v < NFLX; ++v) flx[f * NFLX + v] = h[v * nf + f];
+  for (size_t f = 0; f < nf; ++f) {
+    for (int v = 0; v < NFLX; ++v) flx[f * nfl + v] = h[v * nf + f];
+    for (int q = 0; q < c->nsp; ++q) flx[f * nfl + NFLX + q] = hs[q * nf + f];
+  }
   return 0;
 }
 
@@ -878,10 +891,16 @@ extern "C" int flash_hy_put_fluxes(flash_hy_ctx *c, int blk, int dir, const doub
   size_t off, nf;
   if (flux_span(c, blk, dir, off, nf)) return fail(c, FLASH_HY_ERR_BAD_ARG, "put_fluxes: %s", "bad block/direction");
   CUDA_OK(c, cudaSetDevice(c->device));
-  std::vector<double> h(NFLX * nf);
-  for (size_t f = 0; f < nf; ++f)
-    for (int v = 0; v < NFLX; ++v) h[v * nf + f] = flx[f * NFLX + v];
+  const int nfl = NFLX + c->nsp;
+  std::vector<double> h(NFLX * nf), hs((size_t)c->nsp * nf);
+  for (size_t f = 0; f < nf; ++f) {
+    for (int v = 0; v < NFLX; ++v) h[v * nf + f] = flx[f * nfl + v];
+    for (int q = 0; q < c->nsp; ++q) hs[q * nf + f] = flx[f * nfl + NFLX + q];
+  }
   CUDA_OK(c, cudaMemcpyAsync(c->d_fstore + off, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  if (c->nsp > 0)
+    CUDA_OK(c, cudaMemcpyAsync(c->d_sp_fstore + sp_flux_off(c, blk, dir, nf), hs.data(), hs.size() * sizeof(double),
+                               cudaMemcpyHostToDevice, c->stream));
   CUDA_OK(c, cudaStreamSynchronize(c->stream));
   return 0;
 }

@@ -84,6 +84,9 @@ struct DevParams {
   double *sp_lh, *sp_gp, *sp_freg;
   size_t sp_ncells;           // stride of the species arrays
   size_t sp_freg_stride;      // doubles per species in sp_freg
+  // split step: species face fluxes F_dens * X per block, direction and
+  // species, in the face order of the hydro flux store [block][dir][nsp][faces]
+  double *sp_fstore;
 };
 
 // Cell sizes of block b: level-1 deltas scaled by 2^(1-level) (exact).

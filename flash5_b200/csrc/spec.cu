@@ -15,6 +15,10 @@ static int run_spec(const SpecArgs &a) {
        cudaFuncSetAttribute(k_spec_step<NDIM, NX, NY, NZ>, cudaFuncAttributePreferredSharedMemoryCarveout,
                             cudaSharedmemCarveoutMaxShared) != cudaSuccess))
     return -2;
+  if (a.P.fmode == 3) {                      // split step: the update from the kept fluxes (uniform grids)
+    k_spec_update<NDIM, NX, NY, NZ><<<a.nlaunch, 256, 0, a.stream>>>(a.P, a.ncells);
+    return cudaGetLastError() == cudaSuccess ? 1 : -2;
+  }
   if (a.nlev == 0) {
     k_spec_step<NDIM, NX, NY, NZ><<<a.nlaunch, SS::NT, smem, a.stream>>>(a.P, a.ncells);
     return cudaGetLastError() == cudaSuccess ? 1 : -2;

@@ -258,6 +258,12 @@ __device__ __forceinline__ void spec_dir(const DevParams &P, int b, int3 bc, int
     }, P.sp_freg + (size_t)q * P.sp_freg_stride, 1);
     __syncthreads();
   }
+  if (P.fmode == 1 || P.fmode == 2) {   // split step: keep the face fluxes
+    constexpr int fx = NX + (DIR == 1), fy = NY + (DIR == 2), NF = (NX + 1) * NY * NZ;
+    double *dst = P.sp_fstore + (((size_t)b * NDIM + (DIR - 1)) * P.nsp + q) * NF;
+    for (int f = threadIdx.x; f < NF; f += blockDim.x) dst[f] = sF[L::idx(f % fx, (f / fx) % fy, f / (fx * fy))];
+    if (P.fmode == 2) return;
+  }
   const double delta = sK[SK_DIR0 + 4 * (DIR - 1)], rdelta = sK[SK_DIR0 + 4 * (DIR - 1) + 1];
 #pragma unroll
   for (int u = 0; u < SS::CPT; ++u) {
@@ -398,6 +404,7 @@ __global__ void __launch_bounds__(SpecStep<NDIM, NX, NY, NZ>::NT, SpecStep<NDIM,
     if constexpr (NDIM > 2) spec_dir<NDIM, NX, NY, NZ, 3>(P, b, bc, slot, q, sV, sX, sF0, sK, acc);
     // the old mass fractions from the staged species; the barrier keeps the
     // next species' copies from overwriting them before every thread is done
+    if (P.fmode != 2) {
 #pragma unroll
     for (int u = 0; u < SS::CPT; ++u) {
       const int c = threadIdx.x + u * SS::NT;
@@ -406,8 +413,10 @@ __global__ void __launch_bounds__(SpecStep<NDIM, NX, NY, NZ>::NT, SpecStep<NDIM,
         P.sp_out[(size_t)q * ncells + (size_t)b * NCB + c] = (X * sRo[c] + dt * acc[u]) / sRn[c];
       }
     }
+    }
     __syncthreads();
   }
+  if (P.fmode == 2) return;                // fluxes only: the state is not updated
   // ---- species (not mass scalars) renormalised to a unit sum; each thread
   // reads back only the cells it wrote
   if (P.nspec > 0) {
@@ -416,6 +425,41 @@ __global__ void __launch_bounds__(SpecStep<NDIM, NX, NY, NZ>::NT, SpecStep<NDIM,
       const int c = threadIdx.x + u * SS::NT;
       if (c >= NCB) continue;
       const size_t off = (size_t)b * NCB + c;
+      double sum = 0.;
+      for (int q = 0; q < P.nspec; ++q) sum = sum + P.sp_out[(size_t)q * ncells + off];
+      for (int q = 0; q < P.nspec; ++q) P.sp_out[(size_t)q * ncells + off] = P.sp_out[(size_t)q * ncells + off] / sum;
+    }
+  }
+}
+
+// The species update of the split step (flash_hy_update_solution) from the
+// kept, possibly replaced face fluxes: the divergence in the x, y, z order
+// and the update of k_spec_step, then the renormalisation.
+template <int NDIM, int NX, int NY, int NZ>
+__global__ void __launch_bounds__(256) k_spec_update(const DevParams P, size_t ncells) {
+  constexpr int NCB = NX * NY * NZ, NF = (NX + 1) * NY * NZ;
+  const int b = P.blk_list ? P.blk_list[blockIdx.x] : blockIdx.x;
+  const double dt = P.dt_dev ? *P.dt_dev : P.dt;
+  double del[3];
+  blk_deltas(P, b, del);
+  const double rdel[3] = {1. / del[0], 1. / del[1], 1. / del[2]};
+  for (int c = threadIdx.x; c < NCB; c += blockDim.x) {
+    const int i = c % NX, j = (c / NX) % NY, k = c / (NX * NY);
+    const size_t off = (size_t)b * NCB + c;
+    const double ro = P.s_in[0][off], rn = P.s_out[0][off];
+    for (int q = 0; q < P.nsp; ++q) {
+      double acc = 0.;
+#pragma unroll
+      for (int d = 0; d < NDIM; ++d) {
+        const double *F = P.sp_fstore + (((size_t)b * NDIM + d) * P.nsp + q) * NF;
+        const int fx = NX + (d == 0), fy = NY + (d == 1);
+        const int fl = (k * fy + j) * fx + i, fr = fl + (d == 0 ? 1 : (d == 1 ? fx : fx * fy));
+        const double dd = div_rn(F[fl] - F[fr], del[d], rdel[d]);
+        acc = d == 0 ? dd : acc + dd;
+      }
+      P.sp_out[(size_t)q * ncells + off] = (P.sp_in[(size_t)q * ncells + off] * ro + dt * acc) / rn;
+    }
+    if (P.nspec > 0) {
       double sum = 0.;
       for (int q = 0; q < P.nspec; ++q) sum = sum + P.sp_out[(size_t)q * ncells + off];
       for (int q = 0; q < P.nspec; ++q) P.sp_out[(size_t)q * ncells + off] = P.sp_out[(size_t)q * ncells + off] / sum;

@@ -93,15 +93,21 @@ class Hydro:
                                                      flags))
 
     def get_fluxes(self, block, dir):
-        """Fluxes of one block in direction dir (1..ndim): [faces, 8] in
-        FLASH's flx(NFLUXES, i, j, k) order."""
+        """Fluxes of one block in direction dir (1..ndim): [faces, NFLUXES]
+        in FLASH's flx(NFLUXES, i, j, k) order, NFLUXES = 8 hydro fluxes +
+        the species and mass-scalar fluxes."""
         nb = self.grid.nb
-        out = np.zeros(((nb[0] + 1) * nb[1] * nb[2], 8))
+        nsp = getattr(self.grid, "nspecies", 0) + getattr(self.grid, "nmass_scalars", 0)
+        out = np.zeros(((nb[0] + 1) * nb[1] * nb[2], 8 + nsp))
         self._check(self.lib.flash_hy_get_fluxes(self.ctx, block, dir, out.ctypes.data_as(C.POINTER(C.c_double))))
         return out
 
     def put_fluxes(self, block, dir, flx):
         flx = np.ascontiguousarray(flx, dtype=np.float64)
+        nb = self.grid.nb
+        nsp = getattr(self.grid, "nspecies", 0) + getattr(self.grid, "nmass_scalars", 0)
+        if flx.shape != ((nb[0] + 1) * nb[1] * nb[2], 8 + nsp):
+            raise ValueError(f"fluxes must have shape [faces, {8 + nsp}], got {flx.shape}")
         self._check(self.lib.flash_hy_put_fluxes(self.ctx, block, dir, flx.ctypes.data_as(C.POINTER(C.c_double))))
 
     def update_solution(self, blockList, dt):

@@ -101,8 +101,8 @@ typedef struct flash_hy_params {
    * renormalisation to a unit sum (hy_unsplitUpdate.F90:827-859).  At most
    * FLASH_HY_MAX_SPECIES in all.  Uniform grids and AMR hierarchies (the
    * species are restricted, prolonged in per-mass form into the guard cells
-   * and corrected at fine/coarse faces like the mass flux); the split step
-   * refuses them (FLASH_HY_ERR_UNSUPPORTED). */
+   * and corrected at fine/coarse faces like the mass flux), in the fused
+   * and in the split step. */
   int nspecies;            /* NSPECIES                                     */
   int nmass_scalars;       /* NMASS_SCALARS                                */
 } flash_hy_params;
@@ -167,10 +167,13 @@ int flash_hy_step_blocks(flash_hy_ctx *ctx, int blockCount, const int *blockList
  * of the listed blocks (flags = FLASH_HY_UPDATE_NONE: Uout disassociated,
  * the state is unchanged; FLASH_HY_UPDATE_ALL: also updates, as
  * flash_hy_step_blocks); get/put_fluxes read or replace one block's fluxes
- * in one direction (1..ndim) in FLASH's flux-array layout flx(NFLUXES = 8,
- * i, j, k) over the faces (the dir index runs over nb+1 faces; host memory);
- * update_solution applies the kept (possibly replaced) fluxes to the listed
- * blocks.  Uniform grids only.                                           */
+ * in one direction (1..ndim) in FLASH's flux-array layout flx(NFLUXES, i,
+ * j, k) over the faces (the dir index runs over nb+1 faces; host memory),
+ * NFLUXES = 8 + nspecies + nmass_scalars: the species and mass-scalar
+ * fluxes F_dens * X follow the 8 hydro fluxes (xflux(HY_END_FLUX + isph),
+ * hy_getFaceFlux.F90:453-467); update_solution applies the kept (possibly
+ * replaced) fluxes to the listed blocks, species and mass scalars included
+ * (hy_unsplitUpdate.F90:478-491, 827-859).  Uniform grids only.          */
 int flash_hy_compute_fluxes(flash_hy_ctx *ctx, int blockCount, const int *blockList, double dt, int flags);
 int flash_hy_get_fluxes(flash_hy_ctx *ctx, int block, int dir, double *flx);
 int flash_hy_put_fluxes(flash_hy_ctx *ctx, int block, int dir, const double *flx);

@@ -1564,8 +1564,11 @@ int orc_amr_restrict(const flash_hy_params *p, const flash_hy_grid_desc *g, doub
 /* Face fluxes of one block as hy_computeFluxes leaves them in the Grid's
  * flux arrays (Uout disassociated, hy_computeFluxes.F90:156-160): for each
  * direction d the fluxes flx(NFLUXES, i, j, k) over the faces of the block
- * (the d index runs over nb+1 faces), written to out + d * 8 * nfaces.
- * The guard cells of every block are filled first. */
+ * (the d index runs over nb+1 faces), written to out + d * NFLUXES * nfaces,
+ * NFLUXES = 8 + nspecies + nmass_scalars: the species and mass-scalar
+ * fluxes F_dens * X follow the hydro fluxes (xflux(HY_END_FLUX + isph),
+ * hy_getFaceFlux.F90:453-467).  The guard cells of every block are filled
+ * first. */
 int orc_block_fluxes(const flash_hy_params *p, const flash_hy_grid_desc *g, double *unk, int blk, double dt,
                      double *out) {
   int st = orc_fill_guardcells(p, g, unk);
@@ -1580,15 +1583,18 @@ int orc_block_fluxes(const flash_hy_params *p, const flash_hy_grid_desc *g, doub
   get_face_flux(&c, &w);
   int nb[3] = {c.nxb, c.nyb, c.nzb};
   size_t nfaces = (size_t)(c.nxb + 1) * c.nyb * c.nzb;
+  const int nfl = NFLX + c.nsp;
   for (int d = 0; d < c.ndim; ++d) {
     int fx = nb[0] + (d == 0), fy = nb[1] + (d == 1), fz = nb[2] + (d == 2);
-    double *o = out + (size_t)d * NFLX * nfaces;
+    double *o = out + (size_t)d * nfl * nfaces;
     for (int k = 0; k < fz; ++k)
       for (int j = 0; j < fy; ++j)
         for (int i = 0; i < fx; ++i) {
-          const double *F = &w.flux[d][cidx(&c, i + NGUARD, j + (c.k2 ? NGUARD : 0), k + (c.k3 ? NGUARD : 0)) * NFLX];
+          const size_t cc = cidx(&c, i + NGUARD, j + (c.k2 ? NGUARD : 0), k + (c.k3 ? NGUARD : 0));
+          const double *F = &w.flux[d][cc * NFLX];
           size_t f = ((size_t)k * fy + j) * fx + i;
-          for (int v = 0; v < NFLX; ++v) o[f * NFLX + v] = F[v];
+          for (int v = 0; v < NFLX; ++v) o[f * nfl + v] = F[v];
+          for (int q = 0; q < c.nsp; ++q) o[f * nfl + NFLX + q] = w.spc_flux[d][cc * c.nsp + q];
         }
   }
   work_free(&w);

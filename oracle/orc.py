@@ -117,10 +117,12 @@ class Oracle:
         return lib().orc_amr_hydro(C.byref(self.p), C.byref(self.g), _dp(unk), sim_time, dt, dt_old)
 
     def block_fluxes(self, unk, blk, dt):
-        """Face fluxes of block blk, [ndim][faces][8] in FLASH's flux layout."""
+        """Face fluxes of block blk, [ndim][faces][NFLUXES] in FLASH's flux
+        layout (NFLUXES = 8 + species + mass scalars)."""
         nb = self.grid.nb
         nf = (nb[0] + 1) * nb[1] * nb[2]
-        out = np.zeros((self.grid.ndim, nf, 8))
+        nsp = getattr(self.grid, "nspecies", 0) + getattr(self.grid, "nmass_scalars", 0)
+        out = np.zeros((self.grid.ndim, nf, 8 + nsp))
         st = lib().orc_block_fluxes(C.byref(self.p), C.byref(self.g), _dp(unk), blk, dt, _dp(out))
         return st, out
 

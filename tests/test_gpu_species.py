@@ -8,14 +8,17 @@
 * mixed precision: species within 1e-6 relative L1 of the FP64 GPU run;
 * species on AMR hierarchies (restriction, guard cells, the species flux
   register) and through a regrid equal the oracle bit for bit;
-* the split step refuses species.
+* the split step keeps the species fluxes after the hydro fluxes in FLASH's
+  flux arrays (equal to the oracle's) and, with or without a get/put round
+  trip, updates as the fused step does; a replaced mass-scalar flux changes
+  exactly the two cells beside the face.
 """
 import numpy as np
 import pytest
 
 from flash5_b200 import abi
-from flash5_b200.grid import NUNK
-from flash5_b200.hydro import Hydro, HydroError, next_dt
+from flash5_b200.grid import NUNK, VAR
+from flash5_b200.hydro import Hydro, next_dt
 from oracle import orc
 from tests.cases import make_case
 
@@ -103,16 +106,96 @@ def test_mixed_species_within_tolerance(case):
     assert np.abs(b[..., 0] + b[..., 1] - 1.0).max() < 1e-14
 
 
+def _state(h, grid):
+    out = grid.new_unk()
+    h.download(out)
+    return grid.interior(out).copy()
+
+
 @pytest.mark.gpu
-def test_split_step_refuses_species():
-    grid, unk, params = make_case("kh3d", nspecies=1)
+@pytest.mark.parametrize("case", ["sod2d_rot", "kh3d"])
+def test_split_step_species_fluxes_match_oracle(case):
+    """compute_fluxes keeps the species fluxes F_dens * X after the 8 hydro
+    fluxes (NFLUXES = 8 + species + mass scalars), equal to the oracle's."""
+    grid, unk, params = make_case(case, nspecies=2, nmass_scalars=1)
+    ref = unk.copy()
+    o = orc.Oracle(params, grid)
+    o.eos_init(ref)
     h = Hydro(params, grid)
     h.upload(unk)
     dt, _ = h.compute_dt()
-    with pytest.raises(HydroError) as e:
-        h.compute_fluxes([0], dt, abi.UPDATE_NONE)
-    assert e.value.status & abi.ERR_UNSUPPORTED
+    blocks = [0, grid.nblocks // 2, grid.nblocks - 1]
+    h.compute_fluxes(blocks, dt, abi.UPDATE_NONE)
+    for b in blocks:
+        st, want = o.block_fluxes(ref.copy(), b, dt)
+        assert want.shape[-1] == 11
+        for d in range(grid.ndim):
+            got = h.get_fluxes(b, d + 1)
+            assert np.array_equal(got, want[d]), (b, d, np.abs(got - want[d]).max(axis=0))
     h.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case,prec", [("sod2d_rot", abi.PREC_FP64), ("kh3d", abi.PREC_FP64),
+                                       ("kh3d", abi.PREC_MIXED)])
+def test_split_step_with_species_equals_fused_step(case, prec):
+    grid, unk, params = make_case(case, nspecies=2, nmass_scalars=1, precision=prec)
+    blocks = list(range(grid.nblocks))[1::2]
+    fused, split, both = Hydro(params, grid), Hydro(params, grid), Hydro(params, grid)
+    for h in (fused, split, both):
+        h.upload(unk)
+    dt, _ = fused.compute_dt()
+    before = _state(split, grid)
+    fused.step_blocks(blocks, dt, dt, dt)
+    split.compute_fluxes(blocks, dt, abi.UPDATE_NONE)
+    assert np.array_equal(_state(split, grid), before)
+    for blk in blocks[:2]:                                      # a get/put round trip changes nothing
+        for d in range(1, grid.ndim + 1):
+            split.put_fluxes(blk, d, split.get_fluxes(blk, d))
+    split.update_solution(blocks, dt)
+    both.compute_fluxes(blocks, dt, abi.UPDATE_ALL)
+    a, b, c = _state(fused, grid), _state(split, grid), _state(both, grid)
+    sp = grid.species
+    assert np.array_equal(a[..., sp], b[..., sp]), np.abs(a[..., sp] - b[..., sp]).max()
+    assert np.array_equal(a, b) and np.array_equal(a, c)
+    with pytest.raises(ValueError):
+        split.put_fluxes(blocks[0], 1, split.get_fluxes(blocks[0], 1)[:, :8])
+    for h in (fused, split, both):
+        h.close()
+
+
+@pytest.mark.gpu
+def test_replaced_mass_scalar_flux_changes_the_two_adjacent_cells():
+    """A mass scalar (not renormalised) is linear in its fluxes: a face flux
+    raised by dF changes X of the cells beside the face by -+ dt dF/(dx rho)
+    and nothing else; the hydro variables do not move."""
+    grid, unk, params = make_case("sod2d_rot", nspecies=1, nmass_scalars=1)
+    h0, h1 = Hydro(params, grid), Hydro(params, grid)
+    for h in (h0, h1):
+        h.upload(unk)
+    dt, _ = h0.compute_dt()
+    blk = 5
+    for h in (h0, h1):
+        h.compute_fluxes([blk], dt, abi.UPDATE_NONE)
+    flx = h1.get_fluxes(blk, 1)
+    nx = grid.nb[0] + 1
+    i, j, dF = 3, 2, 1e-3
+    flx[j * nx + i, 9] += dF                                  # the mass scalar's flux at x face (i, j)
+    h1.put_fluxes(blk, 1, flx)
+    for h in (h0, h1):
+        h.update_solution([blk], dt)
+    a, b = _state(h0, grid), _state(h1, grid)
+    ms = grid.species.start + 1
+    diff = b[..., ms] - a[..., ms]
+    rho = a[..., VAR["dens"]]
+    dtdx = dt / grid.delta[0]
+    assert abs(diff[blk, 0, j, i - 1] + dtdx * dF / rho[blk, 0, j, i - 1]) <= 1e-12
+    assert abs(diff[blk, 0, j, i] - dtdx * dF / rho[blk, 0, j, i]) <= 1e-12
+    diff[blk, 0, j, i - 1] = diff[blk, 0, j, i] = 0.0
+    assert np.all(diff == 0.0)
+    assert np.array_equal(np.delete(a, ms, axis=-1), np.delete(b, ms, axis=-1))
+    for h in (h0, h1):
+        h.close()
 
 
 @pytest.mark.gpu
