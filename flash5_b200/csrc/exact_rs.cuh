@@ -147,6 +147,26 @@ __device__ __forceinline__ bool strong_waves(const Side &L, const Side &R) {
   return ppv > pmin && fmax(pmax, ppv) >= 2.0 * pmin;
 }
 
+// A single-precision screen for strong_waves on raw face states: true
+// whenever the FP64 test can be true, so that the FP64 test (with the full
+// sides) runs only on the faces that pass.  The comparisons carry margins of
+// 1e-5 relative, and the PVRS estimate a margin of 1e-5 of the magnitude of
+// its two terms (FP32 rounding of the handful of operations, cancellation
+// included, stays below 1e-6 of it); NaN, infinities and values outside
+// [1e-30, 1e30] pass, leaving the decision to the FP64 test.
+__device__ __forceinline__ bool strong_screen(double dl, double ul, double pl, double dr, double ur, double pr,
+                                              double g) {
+  const float fdl = (float)dl, fpl = (float)pl, fdr = (float)dr, fpr = (float)pr, fg = (float)g;
+  const float cl = sqrtf(fg * fpl / fdl), cr = sqrtf(fg * fpr / fdr);
+  const float pa = 0.5f * (fpl + fpr), corr = 0.125f * ((float)ur - (float)ul) * (fdl + fdr) * (cl + cr);
+  const float ppv = pa - corr, E = 1e-5f * (fabsf(pa) + fabsf(corr));
+  const float pmin = fminf(fpl, fpr), pmax = fmaxf(fpl, fpr);
+  if (!(pmin > 1e-30f && pmax < 1e30f && fminf(fdl, fdr) > 1e-30f && fmaxf(fdl, fdr) < 1e30f &&
+        fabsf(ppv) < 1e30f && E < 1e30f))
+    return true;
+  return ppv + E > pmin * (1.f - 1e-5f) && fmaxf(pmax * (1.f + 1e-5f), ppv + E) >= 2.f * pmin * (1.f - 1e-5f);
+}
+
 // The star state of a solve: p*, u* and w* = p*^z (the sampling takes the
 // rarefaction-side powers (p*/p_K)^z = w*/w_K from it).
 struct Star { double p, u, w; };

@@ -421,14 +421,19 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
         int x, l;
         G::dec(t, G::LC, 1, x, l);
         if (x < 0) continue;
-        xrs::Side L, R;
-        sides(G::at(x, l, G::L4, 4), t, L, R, false);
+        const int s4 = G::at(x, l, G::L4, 4);
         double q = 0.0;
-        if (!xrs::vacuum(L, R, g) && xrs::strong_waves(L, R)) {
-          L.w = xrs::powp(L.p, xrs::zexp(g));
-          R.w = xrs::powp(R.p, xrs::zexp(g));
-          const double wtr = xrs::tr_w(L, R, g);
-          if (!xrs::tr_exact(L, R, xrs::p_of_w(wtr, g))) q = wtr;
+        // the FP32 screen first; the FP64 sides and tests only where it passes
+        if (xrs::strong_screen(face(0, true, s4, t), face(DIR, true, s4, t), face(4, true, s4, t),
+                               face(0, false, s4, t), face(DIR, false, s4, t), face(4, false, s4, t), g)) {
+          xrs::Side L, R;
+          sides(s4, t, L, R, false);
+          if (!xrs::vacuum(L, R, g) && xrs::strong_waves(L, R)) {
+            L.w = xrs::powp(L.p, xrs::zexp(g));
+            R.w = xrs::powp(R.p, xrs::zexp(g));
+            const double wtr = xrs::tr_w(L, R, g);
+            if (!xrs::tr_exact(L, R, xrs::p_of_w(wtr, g))) q = wtr;
+          }
         }
         sP0[t] = q;
         need |= q > 0.0;
