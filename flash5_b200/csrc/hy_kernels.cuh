@@ -71,6 +71,70 @@ __device__ __forceinline__ bool is_inside(int li, int lj, int lk) {
   return (li >= 0 && li < NX) && (NDIM < 2 || (lj >= 0 && lj < NY)) && (NDIM < 3 || (lk >= 0 && lk < NZ));
 }
 
+// Cells (N+2s)^d around a block's interior (s layers), staged in shared
+// memory so that every guard-mapped cell is loaded once.
+template <int NDIM, int NX, int NY, int NZ, int S>
+struct Ext {
+  static constexpr int ex = NX + 2 * S, ey = NDIM > 1 ? NY + 2 * S : 1, ez = NDIM > 2 ? NZ + 2 * S : 1;
+  static constexpr int n = ex * ey * ez;
+  __device__ static __forceinline__ int idx(int i, int j, int k) {
+    return ((k + (NDIM > 2 ? S : 0)) * ey + (j + (NDIM > 1 ? S : 0))) * ex + (i + S);
+  }
+  __device__ static __forceinline__ void decode(int c, int &i, int &j, int &k) {
+    i = c % ex - S;
+    j = NDIM > 1 ? (c / ex) % ey - S : 0;
+    k = NDIM > 2 ? c / (ex * ey) - S : 0;
+  }
+};
+
+// asynchronous 8- and 16-byte copies from global to shared memory
+// (cp.async): a thread's copies are all in flight at once and hold no
+// registers; cp.async.wait_all makes its own copies visible to it
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// The source blocks of a block's guard cells on a uniform grid: entry
+// (cz * 3 + cy) * 3 + cx for the side (0 below, 1 inside, 2 above) of each
+// coordinate; threads 0..3^NDIM-1 write one entry each.
+template <int NDIM, int NX, int NY, int NZ>
+__device__ __forceinline__ void neighbour_table(const DevParams &P, int3 bc, int *nb) {
+  constexpr int NNB = NDIM > 2 ? 27 : 9;
+  if (threadIdx.x >= NNB) return;
+  const int t = threadIdx.x, cx = t % 3, cy = (t / 3) % 3, cz = t / 9;
+  int f;
+  const int gx = map_axis(bc.x * NX + (cx == 0 ? -1 : (cx == 1 ? 0 : NX)), P.nbx * NX, P.bc[0], P.bc[1], f);
+  const int gy = NDIM > 1 ? map_axis(bc.y * NY + (cy == 0 ? -1 : (cy == 1 ? 0 : NY)), P.nby * NY, P.bc[2], P.bc[3], f) : 0;
+  const int gz = NDIM > 2 ? map_axis(bc.z * NZ + (cz == 0 ? -1 : (cz == 1 ? 0 : NZ)), P.nbz * NZ, P.bc[4], P.bc[5], f) : 0;
+  nb[t] = P.blk_at[((gz / NZ) * P.nby + gy / NY) * P.nbx + gx / NX];
+}
+
+// Uniform grids: the cell that provides local cell (li, lj, lk), as cell_src,
+// with the source block taken from the block's neighbour table nb (the
+// source block depends only on whether each coordinate is below, inside or
+// above the block: periodic wrap, mirror and clamp stay within one block).
+template <int NDIM, int NX, int NY, int NZ>
+__device__ __forceinline__ size_t cell_src_nb(const DevParams &P, int b, int3 bc, const int *nb, int li, int lj,
+                                              int lk, int &fx, int &fy, int &fz) {
+  constexpr int NCB = NX * NY * NZ;
+  fx = fy = fz = 0;
+  if (is_inside<NDIM, NX, NY, NZ>(li, lj, lk)) return (size_t)b * NCB + (size_t)((lk * NY + lj) * NX + li);
+  const int gx = map_axis(bc.x * NX + li, P.nbx * NX, P.bc[0], P.bc[1], fx);
+  const int gy = NDIM > 1 ? map_axis(bc.y * NY + lj, P.nby * NY, P.bc[2], P.bc[3], fy) : 0;
+  const int gz = NDIM > 2 ? map_axis(bc.z * NZ + lk, P.nbz * NZ, P.bc[4], P.bc[5], fz) : 0;
+  const int cx = li < 0 ? 0 : (li < NX ? 1 : 2), cy = NDIM > 1 ? (lj < 0 ? 0 : (lj < NY ? 1 : 2)) : 0;
+  const int cz = NDIM > 2 ? (lk < 0 ? 0 : (lk < NZ ? 1 : 2)) : 0;
+  return (size_t)nb[(cz * 3 + cy) * 3 + cx] * NCB + (size_t)(((gz % NZ) * NY + (gy % NY)) * NX + (gx % NX));
+}
+
+
 // Primitive slots of a cell as hy_getRiemannState sees it: interior cells
 // straight from the state, guard cells after the guard-cell EOS.
 template <int NDIM, int NX, int NY, int NZ, bool GAME = true>
@@ -159,22 +223,103 @@ __device__ __forceinline__ int sig_slot(int q) { return q < 5 ? q : HEI; }
 // ---------------------------------------------------------------------------
 // k_sig: transverse flux "sig" of every direction for the box cells
 // (hy_DataReconstructNormalDir_PPM.F90:351-371 via hy_getRiemannState.F90:
-// 471-637, which evaluates it for every cell of [lo-1, hi+1]^d)
+// 471-637, which evaluates it for every cell of [lo-1, hi+1]^d).  The
+// primitives of the box and of one layer beyond it along each axis are
+// staged once in shared memory (cp.async through the neighbour table, then
+// the guard cells' reflections and guard-cell EOS in place, the rules of
+// load_prim); each box cell then reads its stencils from there.
 // ---------------------------------------------------------------------------
+template <int NDIM, int NX, int NY, int NZ>
+struct SigStage {
+  using E = Ext<NDIM, NX, NY, NZ, 2>;
+  static constexpr int NNB = NDIM > 2 ? 27 : 9;
+  // rho, vx, vy, vz and e (after the guard-cell EOS) of the staged cells; the neighbour table
+  static constexpr size_t smem_bytes() { return (size_t)5 * E::n * sizeof(double) + NNB * sizeof(int); }
+  // staged: at most one coordinate outside the box [-1, N]
+  __device__ static __forceinline__ bool needed(int i, int j, int k) {
+    const int c[3] = {i, j, k}, n[3] = {NX, NY, NZ};
+    int out = 0;
+#pragma unroll
+    for (int d = 0; d < NDIM; ++d) out += c[d] < -1 || c[d] > n[d];
+    return out <= 1;
+  }
+};
+
+// the primitive slots of load_prim<..., false> from the staged cell e
+__device__ __forceinline__ void staged_prim(const DevParams &P, const double *sQ, int n, int e, double V[8]) {
+  const double rho = sQ[e], eg = sQ[4 * n + e];
+  V[HD] = rho; V[HVX] = sQ[n + e]; V[HVY] = sQ[2 * n + e]; V[HVZ] = sQ[3 * n + e];
+  V[HP] = rho * eg * P.gam1inv;
+  V[HGC] = P.gamma; V[HGE] = 0.0; V[HEI] = eg;
+}
+
 template <int NDIM, int NX, int NY, int NZ, class R, int VAR>
-__global__ void __launch_bounds__(320) k_sig(const DevParams P, R *__restrict__ SIG) {
+// 3D: three CTAs per SM where shared memory allows it (FP32 sig); the FP64
+// kernel keeps two, which its registers need
+__global__ void __launch_bounds__(320, NDIM > 2 ? (sizeof(R) == 4 ? 3 : 2) : 1) k_sig(const DevParams P,
+                                                                                     R *__restrict__ SIG) {
   using B = Box<NDIM, NX, NY, NZ>;
+  using SG = SigStage<NDIM, NX, NY, NZ>;
+  using E = typename SG::E;
+  using H = Halo<NDIM, NX, NY, NZ>;
+  constexpr int NCB = NX * NY * NZ;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double *sQ = reinterpret_cast<double *>(smem_raw);     // [5][E::n]
+  int *sNb = reinterpret_cast<int *>(sQ + 5 * E::n);     // [NNB]
   const int b = P.blk_list ? P.blk_list[blockIdx.x] : blockIdx.x;
   const int3 bc = blk_coords(P, b);
+  const int slot = P.slot ? P.slot[b] : (int)blockIdx.x;
+  const bool amr = P.lh != nullptr;
+  if (!amr) neighbour_table<NDIM, NX, NY, NZ>(P, bc, sNb);
+  __syncthreads();
+  for (int c = threadIdx.x; c < E::n; c += blockDim.x) {
+    int i, j, k;
+    E::decode(c, i, j, k);
+    if (!SG::needed(i, j, k)) continue;
+    if (amr && !is_inside<NDIM, NX, NY, NZ>(i, j, k)) {     // the leaf guard buffer (after the EOS)
+      const double *h = P.lh + (size_t)slot * 5 * H::n + H::idx(i, j, k);
+#pragma unroll
+      for (int v = 0; v < 5; ++v) cp_async8(sQ + v * E::n + c, h + v * H::n);
+    } else {
+      int fx, fy, fz;
+      const size_t o = amr ? (size_t)b * NCB + (size_t)((k * NY + j) * NX + i)
+                           : cell_src_nb<NDIM, NX, NY, NZ>(P, b, bc, sNb, i, j, k, fx, fy, fz);
+#pragma unroll
+      for (int v = 0; v < 5; ++v) cp_async8(sQ + v * E::n + c, P.s_in[v] + o);
+    }
+  }
+  cp_async_wait_all();
+  if (!amr) {   // guard cells: mirrored velocities, Eos_getData.F90:80-96 on ENER = eint + ekin of the source cell
+    for (int c = threadIdx.x; c < E::n; c += blockDim.x) {
+      int i, j, k;
+      E::decode(c, i, j, k);
+      if (!SG::needed(i, j, k) || is_inside<NDIM, NX, NY, NZ>(i, j, k)) continue;
+      int f[3];
+      cell_src_nb<NDIM, NX, NY, NZ>(P, b, bc, sNb, i, j, k, f[0], f[1], f[2]);
+      double vx = sQ[E::n + c], vy = sQ[2 * E::n + c], vz = sQ[3 * E::n + c];
+      const double e = sQ[4 * E::n + c];
+      if (f[0]) vx = -vx;
+      if (f[1]) vy = -vy;
+      if (f[2]) vz = -vz;
+      double eg = e;
+      const double ekin = 0.5 * (vx * vx + vy * vy + vz * vz);
+      const double ener = e + ekin;
+      if (ener - ekin > rmax(P.smalle, P.eswitch * ekin)) eg = ener - ekin;
+      sQ[E::n + c] = vx; sQ[2 * E::n + c] = vy; sQ[3 * E::n + c] = vz; sQ[4 * E::n + c] = eg;
+    }
+  }
+  __syncthreads();
   unsigned st = 0;
   for (int t = threadIdx.x; t < B::n; t += blockDim.x) {
     int i = t % B::bx - 1, j = NDIM > 1 ? (t / B::bx) % B::by - 1 : 0, k = NDIM > 2 ? t / (B::bx * B::by) - 1 : 0;
+    const int e = E::idx(i, j, k);
     double Vc[8], Vm[8], Vp[8];
-    load_prim<NDIM, NX, NY, NZ, false>(P, b, bc, i, j, k, Vc);
+    staged_prim(P, sQ, E::n, e, Vc);
 #pragma unroll
     for (int d = 1; d <= NDIM; ++d) {
-      load_prim<NDIM, NX, NY, NZ, false>(P, b, bc, i - (d == 1), j - (d == 2), k - (d == 3), Vm);
-      load_prim<NDIM, NX, NY, NZ, false>(P, b, bc, i + (d == 1), j + (d == 2), k + (d == 3), Vp);
+      const int es = d == 1 ? 1 : (d == 2 ? E::ex : E::ex * E::ey);
+      staged_prim(P, sQ, E::n, e - es, Vm);
+      staged_prim(P, sQ, E::n, e + es, Vp);
       R s[8];
       if (d == 1) sig_dir<R, 1>(P, Vm, Vc, Vp, s, st);
       else if (d == 2) sig_dir<R, 2>(P, Vm, Vc, Vp, s, st);

@@ -69,12 +69,19 @@ static bool launch_dir(const StepArgs &a) {
 #if FHY_VARIANT != 3 || FHY_MXSEL == 0
 template <int NDIM, int NX, int NY, int NZ>
 static bool launch_sig(const StepArgs &a) {
+  auto kern = k_sig<NDIM, NX, NY, NZ, Real, FHY_VARIANT>;
+  const size_t smem = SigStage<NDIM, NX, NY, NZ>::smem_bytes();
+  if (a.set_attr && smem > 48 * 1024 &&
+      (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+       cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared) !=
+           cudaSuccess))
+    return false;
   if (a.nlev == 0) {
-    k_sig<NDIM, NX, NY, NZ, Real, FHY_VARIANT><<<a.nlaunch, a.threads, 0, a.stream>>>(a.P, (Real *)a.sig);
+    kern<<<a.nlaunch, a.threads, smem, a.stream>>>(a.P, (Real *)a.sig);
   } else {
     DevParams P = a.P;
     P.blk_list = a.leaves;
-    k_sig<NDIM, NX, NY, NZ, Real, FHY_VARIANT><<<a.nleaves, a.threads, 0, a.stream>>>(P, (Real *)a.sig);
+    kern<<<a.nleaves, a.threads, smem, a.stream>>>(P, (Real *)a.sig);
   }
   return cudaGetLastError() == cudaSuccess;
 }

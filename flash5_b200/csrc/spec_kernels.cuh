@@ -34,22 +34,6 @@ __device__ __forceinline__ double minmod_s(double a, double b) {     // hy_slope
   return .5 * (copysign(1., a) + copysign(1., b)) * rmin(fabs(a), fabs(b));
 }
 
-// Cells (N+2s)^d around a block's interior (s layers), staged in shared
-// memory so that every guard-mapped cell is loaded once.
-template <int NDIM, int NX, int NY, int NZ, int S>
-struct Ext {
-  static constexpr int ex = NX + 2 * S, ey = NDIM > 1 ? NY + 2 * S : 1, ez = NDIM > 2 ? NZ + 2 * S : 1;
-  static constexpr int n = ex * ey * ez;
-  __device__ static __forceinline__ int idx(int i, int j, int k) {
-    return ((k + (NDIM > 2 ? S : 0)) * ey + (j + (NDIM > 1 ? S : 0))) * ex + (i + S);
-  }
-  __device__ static __forceinline__ void decode(int c, int &i, int &j, int &k) {
-    i = c % ex - S;
-    j = NDIM > 1 ? (c / ex) % ey - S : 0;
-    k = NDIM > 2 ? c / (ex * ey) - S : 0;
-  }
-};
-
 // Launch shape and shared memory of k_spec_step: the velocities on the box
 // of one guard layer, one species on the cells the stencils read (the box
 // plus, along each direction, three cells beyond the block on the lines of
@@ -98,38 +82,6 @@ struct SpecStep {
     else { i = t1; j = t2; k = a; }
   }
 };
-
-// asynchronous 8- and 16-byte copies from global to shared memory
-// (cp.async): a thread's copies are all in flight at once and hold no
-// registers; cp.async.wait_all makes its own copies visible to it
-__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
-               "l"(src)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-
-// Uniform grids: the cell that provides local cell (li, lj, lk), as cell_src,
-// with the source block taken from the block's neighbour table nb (the
-// source block depends only on whether each coordinate is below, inside or
-// above the block: periodic wrap, mirror and clamp stay within one block).
-template <int NDIM, int NX, int NY, int NZ>
-__device__ __forceinline__ size_t cell_src_nb(const DevParams &P, int b, int3 bc, const int *nb, int li, int lj,
-                                              int lk, int &fx, int &fy, int &fz) {
-  constexpr int NCB = NX * NY * NZ;
-  fx = fy = fz = 0;
-  if (is_inside<NDIM, NX, NY, NZ>(li, lj, lk)) return (size_t)b * NCB + (size_t)((lk * NY + lj) * NX + li);
-  const int gx = map_axis(bc.x * NX + li, P.nbx * NX, P.bc[0], P.bc[1], fx);
-  const int gy = NDIM > 1 ? map_axis(bc.y * NY + lj, P.nby * NY, P.bc[2], P.bc[3], fy) : 0;
-  const int gz = NDIM > 2 ? map_axis(bc.z * NZ + lk, P.nbz * NZ, P.bc[4], P.bc[5], fz) : 0;
-  const int cx = li < 0 ? 0 : (li < NX ? 1 : 2), cy = NDIM > 1 ? (lj < 0 ? 0 : (lj < NY ? 1 : 2)) : 0;
-  const int cz = NDIM > 2 ? (lk < 0 ? 0 : (lk < NZ ? 1 : 2)) : 0;
-  return (size_t)nb[(cz * 3 + cy) * 3 + cx] * NCB + (size_t)(((gz % NZ) * NY + (gy % NY)) * NX + (gx % NX));
-}
 
 // CTA-wide constants of k_spec_step in shared memory (computed once per block)
 enum { SK_HDTX = 0, SK_HDTY, SK_HDTZ, SK_DIR0 };   // then per direction: delta, 1/delta, dtn/2, fac
@@ -325,14 +277,7 @@ __global__ void __launch_bounds__(SpecStep<NDIM, NX, NY, NZ>::NT, SpecStep<NDIM,
       sK[SK_DIR0 + 4 * d + 3] = dt * dt / (6. * da * db);
     }
   }
-  if (!amr && threadIdx.x < SS::NNB) {
-    const int t = threadIdx.x, cx = t % 3, cy = (t / 3) % 3, cz = t / 9;
-    int f;
-    const int gx = map_axis(bc.x * NX + (cx == 0 ? -1 : (cx == 1 ? 0 : NX)), P.nbx * NX, P.bc[0], P.bc[1], f);
-    const int gy = NDIM > 1 ? map_axis(bc.y * NY + (cy == 0 ? -1 : (cy == 1 ? 0 : NY)), P.nby * NY, P.bc[2], P.bc[3], f) : 0;
-    const int gz = NDIM > 2 ? map_axis(bc.z * NZ + (cz == 0 ? -1 : (cz == 1 ? 0 : NZ)), P.nbz * NZ, P.bc[4], P.bc[5], f) : 0;
-    sNb[t] = P.blk_at[((gz / NZ) * P.nby + gy / NY) * P.nbx + gx / NX];
-  }
+  if (!amr) neighbour_table<NDIM, NX, NY, NZ>(P, bc, sNb);
   __syncthreads();
   // ---- sources of the staged cells: offsets into a species of the state,
   // or (flagged in the sign bit) into the leaf's species guard buffer on AMR
