@@ -169,27 +169,6 @@ __device__ __forceinline__ void load_prim(const DevParams &P, int b, int3 bc, in
   V[HGC] = P.gamma; V[HGE] = GAME ? p / (eg * rho) + 1 : 0.0; V[HEI] = eg;
 }
 
-// Pressure only (flattening stencil ends).
-template <int NDIM, int NX, int NY, int NZ>
-__device__ __forceinline__ double load_pres(const DevParams &P, int b, int3 bc, int li, int lj, int lk) {
-  if (P.lh && !is_inside<NDIM, NX, NY, NZ>(li, lj, lk)) {
-    using H = Halo<NDIM, NX, NY, NZ>;
-    const double *h = P.lh + (size_t)P.slot[b] * 5 * H::n + H::idx(li, lj, lk);
-    return h[0] * h[4 * H::n] * P.gam1inv;
-  }
-  bool inside; int fx, fy, fz;
-  size_t o = cell_src<NDIM, NX, NY, NZ>(P, b, bc, li, lj, lk, inside, fx, fy, fz);
-  double rho = __ldg(P.s_in[0] + o), e = __ldg(P.s_in[4] + o);
-  double eg = e;
-  if (!inside) {
-    double vx = __ldg(P.s_in[1] + o), vy = __ldg(P.s_in[2] + o), vz = __ldg(P.s_in[3] + o);
-    double ekin = 0.5 * (vx * vx + vy * vy + vz * vz);
-    double ener = e + ekin;
-    if (ener - ekin > rmax(P.smalle, P.eswitch * ekin)) eg = ener - ekin;
-  }
-  return rho * eg * P.gam1inv;
-}
-
 template <int NDIM, int NX, int NY, int NZ> struct Box {
   static constexpr int bx = NX + 2, by = NDIM > 1 ? NY + 2 : 1, bz = NDIM > 2 ? NZ + 2 : 1;
   static constexpr int n = bx * by * bz;
@@ -229,6 +208,83 @@ __device__ __forceinline__ int sig_slot(int q) { return q < 5 ? q : HEI; }
 // the guard cells' reflections and guard-cell EOS in place, the rules of
 // load_prim); each box cell then reads its stencils from there.
 // ---------------------------------------------------------------------------
+// Stage rho, vx, vy, vz and e of the cells cell_of(c, i, j, k) selects
+// (c in [0, n)) into sQ[5][n] as load_prim sees them: cp.async copies from
+// the state (sources through the neighbour table nb; interior cells on AMR)
+// or the leaf guard buffer (AMR, after the EOS), then, by the thread that
+// issued them, the uniform grid's guard cells mirrored and passed through
+// the guard-cell EOS (Eos_getData.F90:80-96 on ENER = eint + ekin of the
+// source cell).  The caller synchronises before reading.
+template <int NDIM, int NX, int NY, int NZ, class CellOf>
+__device__ __forceinline__ void stage_prims(const DevParams &P, int b, int3 bc, int slot, const int *nb, double *sQ,
+                                            int n, CellOf cell_of) {
+  using H = Halo<NDIM, NX, NY, NZ>;
+  constexpr int NCB = NX * NY * NZ;
+  const bool amr = P.lh != nullptr;
+  for (int c = threadIdx.x; c < n; c += blockDim.x) {
+    int i, j, k;
+    if (!cell_of(c, i, j, k)) continue;
+    if (amr && !is_inside<NDIM, NX, NY, NZ>(i, j, k)) {
+      const double *h = P.lh + (size_t)slot * 5 * H::n + H::idx(i, j, k);
+#pragma unroll
+      for (int v = 0; v < 5; ++v) cp_async8(sQ + v * n + c, h + v * H::n);
+    } else {
+      int fx, fy, fz;
+      const size_t o = amr ? (size_t)b * NCB + (size_t)((k * NY + j) * NX + i)
+                           : cell_src_nb<NDIM, NX, NY, NZ>(P, b, bc, nb, i, j, k, fx, fy, fz);
+#pragma unroll
+      for (int v = 0; v < 5; ++v) cp_async8(sQ + v * n + c, P.s_in[v] + o);
+    }
+  }
+  cp_async_wait_all();
+  if (amr) return;
+  for (int c = threadIdx.x; c < n; c += blockDim.x) {
+    int i, j, k;
+    if (!cell_of(c, i, j, k) || is_inside<NDIM, NX, NY, NZ>(i, j, k)) continue;
+    int f[3];
+    cell_src_nb<NDIM, NX, NY, NZ>(P, b, bc, nb, i, j, k, f[0], f[1], f[2]);
+    double vx = sQ[n + c], vy = sQ[2 * n + c], vz = sQ[3 * n + c];
+    const double e = sQ[4 * n + c];
+    if (f[0]) vx = -vx;
+    if (f[1]) vy = -vy;
+    if (f[2]) vz = -vz;
+    double eg = e;
+    const double ekin = 0.5 * (vx * vx + vy * vy + vz * vz);
+    const double ener = e + ekin;
+    if (ener - ekin > rmax(P.smalle, P.eswitch * ekin)) eg = ener - ekin;
+    sQ[n + c] = vx; sQ[2 * n + c] = vy; sQ[3 * n + c] = vz; sQ[4 * n + c] = eg;
+  }
+}
+
+// the primitive slots of load_prim<..., GAME> from the staged cell e
+template <bool GAME = false>
+__device__ __forceinline__ void staged_prim(const DevParams &P, const double *sQ, int n, int e, double V[8]) {
+  const double rho = sQ[e], eg = sQ[4 * n + e];
+  const double p = rho * eg * P.gam1inv;
+  V[HD] = rho; V[HVX] = sQ[n + e]; V[HVY] = sQ[2 * n + e]; V[HVZ] = sQ[3 * n + e]; V[HP] = p;
+  V[HGC] = P.gamma; V[HGE] = GAME ? p / (eg * rho) + 1 : 0.0; V[HEI] = eg;
+}
+
+// The lines of interior cells along DIR with four cells beyond the block on
+// either side (the stencil of the FP64 direction kernel: PPM +-2, the
+// flattening's pressures +-3 around line cells [-1, N]), in the thread
+// order of the line cells.
+template <int NDIM, int NX, int NY, int NZ, int DIR>
+struct LineStage {
+  static constexpr int sx = DIR == 1 ? NX + 8 : NX, sy = NDIM > 1 ? (DIR == 2 ? NY + 8 : NY) : 1,
+                       sz = NDIM > 2 ? (DIR == 3 ? NZ + 8 : NZ) : 1;
+  static constexpr int n = sx * sy * sz;
+  static constexpr int step = DIR == 1 ? 1 : (DIR == 2 ? sx : sx * sy);
+  __device__ static __forceinline__ int idx(int i, int j, int k) {
+    return ((k + 4 * (DIR == 3)) * sy + (j + 4 * (DIR == 2))) * sx + (i + 4 * (DIR == 1));
+  }
+  __device__ static __forceinline__ void decode(int c, int &i, int &j, int &k) {
+    i = c % sx - 4 * (DIR == 1);
+    j = NDIM > 1 ? (c / sx) % sy - 4 * (DIR == 2) : 0;
+    k = NDIM > 2 ? c / (sx * sy) - 4 * (DIR == 3) : 0;
+  }
+};
+
 template <int NDIM, int NX, int NY, int NZ>
 struct SigStage {
   using E = Ext<NDIM, NX, NY, NZ, 2>;
@@ -244,14 +300,6 @@ struct SigStage {
     return out <= 1;
   }
 };
-
-// the primitive slots of load_prim<..., false> from the staged cell e
-__device__ __forceinline__ void staged_prim(const DevParams &P, const double *sQ, int n, int e, double V[8]) {
-  const double rho = sQ[e], eg = sQ[4 * n + e];
-  V[HD] = rho; V[HVX] = sQ[n + e]; V[HVY] = sQ[2 * n + e]; V[HVZ] = sQ[3 * n + e];
-  V[HP] = rho * eg * P.gam1inv;
-  V[HGC] = P.gamma; V[HGE] = 0.0; V[HEI] = eg;
-}
 
 template <int NDIM, int NX, int NY, int NZ, class R, int VAR>
 // 3D: three CTAs per SM where shared memory allows it (FP32 sig); the FP64
@@ -272,42 +320,10 @@ __global__ void __launch_bounds__(320, NDIM > 2 ? (sizeof(R) == 4 ? 3 : 2) : 1) 
   const bool amr = P.lh != nullptr;
   if (!amr) neighbour_table<NDIM, NX, NY, NZ>(P, bc, sNb);
   __syncthreads();
-  for (int c = threadIdx.x; c < E::n; c += blockDim.x) {
-    int i, j, k;
+  stage_prims<NDIM, NX, NY, NZ>(P, b, bc, slot, sNb, sQ, E::n, [](int c, int &i, int &j, int &k) {
     E::decode(c, i, j, k);
-    if (!SG::needed(i, j, k)) continue;
-    if (amr && !is_inside<NDIM, NX, NY, NZ>(i, j, k)) {     // the leaf guard buffer (after the EOS)
-      const double *h = P.lh + (size_t)slot * 5 * H::n + H::idx(i, j, k);
-#pragma unroll
-      for (int v = 0; v < 5; ++v) cp_async8(sQ + v * E::n + c, h + v * H::n);
-    } else {
-      int fx, fy, fz;
-      const size_t o = amr ? (size_t)b * NCB + (size_t)((k * NY + j) * NX + i)
-                           : cell_src_nb<NDIM, NX, NY, NZ>(P, b, bc, sNb, i, j, k, fx, fy, fz);
-#pragma unroll
-      for (int v = 0; v < 5; ++v) cp_async8(sQ + v * E::n + c, P.s_in[v] + o);
-    }
-  }
-  cp_async_wait_all();
-  if (!amr) {   // guard cells: mirrored velocities, Eos_getData.F90:80-96 on ENER = eint + ekin of the source cell
-    for (int c = threadIdx.x; c < E::n; c += blockDim.x) {
-      int i, j, k;
-      E::decode(c, i, j, k);
-      if (!SG::needed(i, j, k) || is_inside<NDIM, NX, NY, NZ>(i, j, k)) continue;
-      int f[3];
-      cell_src_nb<NDIM, NX, NY, NZ>(P, b, bc, sNb, i, j, k, f[0], f[1], f[2]);
-      double vx = sQ[E::n + c], vy = sQ[2 * E::n + c], vz = sQ[3 * E::n + c];
-      const double e = sQ[4 * E::n + c];
-      if (f[0]) vx = -vx;
-      if (f[1]) vy = -vy;
-      if (f[2]) vz = -vz;
-      double eg = e;
-      const double ekin = 0.5 * (vx * vx + vy * vy + vz * vz);
-      const double ener = e + ekin;
-      if (ener - ekin > rmax(P.smalle, P.eswitch * ekin)) eg = ener - ekin;
-      sQ[E::n + c] = vx; sQ[2 * E::n + c] = vy; sQ[3 * E::n + c] = vz; sQ[4 * E::n + c] = eg;
-    }
-  }
+    return SG::needed(i, j, k);
+  });
   __syncthreads();
   unsigned st = 0;
   for (int t = threadIdx.x; t < B::n; t += blockDim.x) {
@@ -599,25 +615,42 @@ __global__ void __launch_bounds__(320) k_dir(const DevParams P, const R *__restr
     return ((k + (DIR == 3)) * G::ry + (j + (DIR == 2))) * G::rx + (i + (DIR == 1));
   };
   if (P.fmode != 3) {
+  // ---------------- phase 0: the stencil of every line, staged once ---------
+  // (in the flux array, unused until phase 2: 5 (N+8) <= 8 (N+2) for N >= 8)
+  using LS = LineStage<NDIM, NX, NY, NZ, DIR>;
+  static_assert(5 * LS::n <= NFLX * G::n, "line stage fits the flux array");
+  __shared__ int sNb[NDIM > 2 ? 27 : 9];
+  double *sQ = reinterpret_cast<double *>(sF);
+  if (P.lh == nullptr) {
+    neighbour_table<NDIM, NX, NY, NZ>(P, bc, sNb);
+    __syncthreads();
+  }
+  stage_prims<NDIM, NX, NY, NZ>(P, b, bc, P.slot ? P.slot[b] : (int)blockIdx.x, sNb, sQ, LS::n,
+                                [](int c, int &i, int &j, int &k) {
+                                  LS::decode(c, i, j, k);
+                                  return true;
+                                });
+  __syncthreads();
   // ---------------- phase 1: face states of the line cells ----------------
   for (int t = threadIdx.x; t < G::n; t += blockDim.x) {
     int i, j, k;
     G::decode(t, i, j, k);
-    const int di = DIR == 1, dj = DIR == 2, dk = DIR == 3;
+    const int e0 = LS::idx(i, j, k);
     R V5[5][8];
     double Vd[8];
 #pragma unroll
     for (int s = -2; s <= 2; ++s) {
-      if (s == 0) load_prim<NDIM, NX, NY, NZ, true>(P, b, bc, i, j, k, Vd);
-      else load_prim<NDIM, NX, NY, NZ, false>(P, b, bc, i + s * di, j + s * dj, k + s * dk, Vd);
+      if (s == 0) staged_prim<true>(P, sQ, LS::n, e0, Vd);
+      else staged_prim<false>(P, sQ, LS::n, e0 + s * LS::step, Vd);
 #pragma unroll
       for (int n = 0; n < 8; ++n) V5[s + 2][n] = R(Vd[n]);
     }
     R flat = R(0);
     if (P.use_flattening) {
       R p7[7], u7[7];
-      p7[0] = R(load_pres<NDIM, NX, NY, NZ>(P, b, bc, i - 3 * di, j - 3 * dj, k - 3 * dk));
-      p7[6] = R(load_pres<NDIM, NX, NY, NZ>(P, b, bc, i + 3 * di, j + 3 * dj, k + 3 * dk));
+      const int em = e0 - 3 * LS::step, ep = e0 + 3 * LS::step;
+      p7[0] = R(sQ[em] * sQ[4 * LS::n + em] * P.gam1inv);
+      p7[6] = R(sQ[ep] * sQ[4 * LS::n + ep] * P.gam1inv);
 #pragma unroll
       for (int s = 0; s < 5; ++s) { p7[s + 1] = V5[s][HP]; u7[s + 1] = V5[s][Slots<DIR>::v1]; }
       u7[0] = R(0); u7[6] = R(0);
