@@ -148,6 +148,7 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
   const float dtn = float(dt / delta), hdtn = 0.5f * dtn;
   const float hdtx = float(0.5 * dt / del[0]), hdty = float(0.5 * dt / del[1]), hdtz = float(0.5 * dt / del[2]);
   const float *sigb = SIG + (size_t)(P.slot ? P.slot[b] : (int)blockIdx.x) * NDIM * 6 * B::n;
+  if constexpr (RS == 0) prefetch_dir_inputs<NDIM, NX, NY, NZ, DIR, FIRST, LAST>(P, b, sigb, ACC, AUX, ncells, B::n);
 
   auto fidx = [](int along, int t1, int t2) { return G::at(along, t1 + (DIR == 1 ? NY : NX) * t2, G::LC, 1); };
   if (P.fmode != 3) {
