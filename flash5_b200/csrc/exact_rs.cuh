@@ -77,24 +77,12 @@ __device__ __forceinline__ double pow_k(double x, double k) {
   return powp(x, k);
 }
 
-__device__ __forceinline__ double zexp(double g) { return (g - 1.0) / (2.0 * g); }
-__device__ __forceinline__ double p_of_w(double w, double g) { return pow_k(w, 2.0 * g / (g - 1.0)); }
-__device__ __forceinline__ Side make_side(double d, double u, double p, double c, double g) {
-  return Side{d, u, p, c, powp(p, zexp(g))};
-}
-
-// Constants of one side's pressure function, taken once per solve: w_K,
-// p_K, the rarefaction slope k = 2 c_K / ((g-1) w_K) and A_K, B_K of the
-// shock branch.
-struct SideK { double w, p, k, A, B; };
-__device__ __forceinline__ SideK side_k(const Side &s, double g) {
-  return SideK{s.w, s.p, 2.0 * s.c / ((g - 1.0) * s.w), 2.0 / ((g + 1.0) * s.d), (g - 1.0) / (g + 1.0) * s.p};
-}
+__host__ __device__ __forceinline__ double zexp(double g) { return (g - 1.0) / (2.0 * g); }
 
 // p = w^n, n = 1/z = 2g/(g-1): unrolled for the integer exponents of
 // g = 5/3, 7/5, 4/3 (5, 7, 8), else pow_k
 struct PowN { int ni; double n; };
-__device__ __forceinline__ PowN pown_of(double g) {
+__host__ __device__ __forceinline__ PowN pown_of(double g) {
   const double n = 2.0 * g / (g - 1.0), r = rint(n);
   return PowN{(fabs(n - r) < 1e-9 && (r == 5.0 || r == 7.0 || r == 8.0)) ? (int)r : 0, n};
 }
@@ -103,6 +91,42 @@ __device__ __forceinline__ double pow_n(double w, const PowN &e) {
   if (e.ni == 7) { const double w2 = w * w, w4 = w2 * w2; return w4 * w2 * w; }
   if (e.ni == 8) { const double w2 = w * w, w4 = w2 * w2; return w4 * w4; }
   return pow_k(w, e.n);
+}
+
+// Constants of the gas, taken once per context on the host where the
+// adiabatic index is uniform (the hydro kernels read them from their
+// parameter block) and per solve in the isolated solver: z = (g-1)/(2g), p = w^n, and
+// the coefficients of the pressure functions (Toro eqs. 4.6-4.7), the
+// two-rarefaction guess and the sampling (section 4.5).
+struct Gas {
+  double g, z, gm1inv, k2, a2, g6, g2, hgm1;   // 1/(g-1), 2/(g-1), 2/(g+1), (g-1)/(g+1), (g+1)/(2g), (g-1)/2
+  PowN e;
+};
+__host__ __device__ __forceinline__ Gas gas_of(double g) {
+  Gas s;
+  s.g = g;
+  s.z = zexp(g);
+  s.gm1inv = 1.0 / (g - 1.0);
+  s.k2 = 2.0 / (g - 1.0);
+  s.a2 = 2.0 / (g + 1.0);
+  s.g6 = (g - 1.0) / (g + 1.0);
+  s.g2 = (g + 1.0) / (2.0 * g);
+  s.hgm1 = 0.5 * (g - 1.0);
+  s.e = pown_of(g);
+  return s;
+}
+
+__device__ __forceinline__ double p_of_w(double w, const Gas &G) { return pow_n(w, G.e); }
+__device__ __forceinline__ Side make_side(double d, double u, double p, double c, const Gas &G) {
+  return Side{d, u, p, c, powp(p, G.z)};
+}
+
+// Constants of one side's pressure function, taken once per solve: w_K,
+// p_K, the rarefaction slope k = 2 c_K / ((g-1) w_K) and A_K, B_K of the
+// shock branch.
+struct SideK { double w, p, k, A, B; };
+__device__ __forceinline__ SideK side_k(const Side &s, const Gas &G) {
+  return SideK{s.w, s.p, G.k2 * s.c / s.w, G.a2 / s.d, G.g6 * s.p};
 }
 
 // f_K(w) and df_K/dw (Toro eqs. 4.6-4.7 with p = w^n); iw = 1/w
@@ -119,16 +143,22 @@ __device__ __forceinline__ void pres_fn(double w, double p, double iw, const Sid
   }
 }
 
-// two-rarefaction guess in w (0 where the states generate vacuum)
-__device__ __forceinline__ double tr_w(const Side &L, const Side &R, double g) {
-  const double num = L.c + R.c - 0.5 * (g - 1.0) * (R.u - L.u);
-  return num > 0.0 ? num / (L.c / L.w + R.c / R.w) : 0.0;
+// two-rarefaction guess in w (0 where the states generate vacuum), Toro
+// eq. 4.46 with c_K/w_K = k_K (g-1)/2 from the sides' rarefaction slopes
+__device__ __forceinline__ double tr_w(const Side &L, const Side &R, const SideK &kl, const SideK &kr, const Gas &G) {
+  const double num = L.c + R.c - G.hgm1 * (R.u - L.u);
+  return num > 0.0 ? num / (G.hgm1 * (kl.k + kr.k)) : 0.0;
 }
-__device__ __forceinline__ double tr_guess(const Side &L, const Side &R, double g) { return p_of_w(tr_w(L, R, g), g); }
+__device__ __forceinline__ double tr_w(const Side &L, const Side &R, const Gas &G) {
+  return tr_w(L, R, side_k(L, G), side_k(R, G), G);
+}
+__device__ __forceinline__ double tr_guess(const Side &L, const Side &R, const Gas &G) {
+  return p_of_w(tr_w(L, R, G), G);
+}
 
 // vacuum generation test, Toro eq. 4.40
-__device__ __forceinline__ bool vacuum(const Side &L, const Side &R, double g) {
-  return 2.0 * (L.c + R.c) / (g - 1.0) <= R.u - L.u;
+__device__ __forceinline__ bool vacuum(const Side &L, const Side &R, const Gas &G) {
+  return G.k2 * (L.c + R.c) <= R.u - L.u;
 }
 
 // The two-rarefaction guess is the exact root when it does not exceed
@@ -181,11 +211,10 @@ struct Star { double p, u, w; };
 // (or a doubling while no upper end is known).  u* is f_L, f_R linearised
 // from the last evaluation to the returned w*.  Returns the number of
 // evaluations, or -max_iter when not converged.
-__device__ __forceinline__ int newton(const Side &L, const Side &R, double g, double w0, double tol, int max_iter,
-                                      Star &out) {
-  const double du = R.u - L.u, ztol = zexp(g) * tol;
-  const SideK kl = side_k(L, g), kr = side_k(R, g);
-  const PowN e = pown_of(g);
+__device__ __forceinline__ int newton(const Side &L, const Side &R, const SideK &kl, const SideK &kr, const Gas &G,
+                                      double w0, double tol, int max_iter, Star &out) {
+  const double du = R.u - L.u, ztol = G.z * tol;
+  const PowN &e = G.e;
   double wa = 0.0, wb = DBL_MAX;
   double w = w0, prev = -1.0, p = 0.0;
   double fl = 0., fdl = 0., fr = 0., fdr = 0., we = w0;
@@ -239,36 +268,36 @@ __device__ __forceinline__ int newton(const Side &L, const Side &R, double g, do
 // ---------------------------------------------------------------------------
 // the exact solution at x/t = 0 (Toro 4.5; vacuum generation 4.6)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void fan_left(const Side &L, double g, double &d, double &u, double &p) {
-  const double c = 2.0 / (g + 1.0) * (L.c + 0.5 * (g - 1.0) * L.u);
+__device__ __forceinline__ void fan_left(const Side &L, const Gas &G, double &d, double &u, double &p) {
+  const double c = G.a2 * (L.c + G.hgm1 * L.u);
   u = c;
   const double r = c / L.c;
-  d = L.d * pow_k(r, 2.0 / (g - 1.0));
-  p = L.p * pow_k(r, 2.0 * g / (g - 1.0));
+  d = L.d * pow_k(r, G.k2);
+  p = L.p * pow_n(r, G.e);
 }
-__device__ __forceinline__ void fan_right(const Side &R, double g, double &d, double &u, double &p) {
-  const double c = 2.0 / (g + 1.0) * (R.c - 0.5 * (g - 1.0) * R.u);
+__device__ __forceinline__ void fan_right(const Side &R, const Gas &G, double &d, double &u, double &p) {
+  const double c = G.a2 * (R.c - G.hgm1 * R.u);
   u = -c;
   const double r = c / R.c;
-  d = R.d * pow_k(r, 2.0 / (g - 1.0));
-  p = R.p * pow_k(r, 2.0 * g / (g - 1.0));
+  d = R.d * pow_k(r, G.k2);
+  p = R.p * pow_n(r, G.e);
 }
 
 // (d, u, p) at x/t = 0 and which side supplies the transverse velocities;
 // behind a rarefaction (p*/p_K)^z = w*/w_K and rho*_K = rho_K (w*/w_K)^(2/(g-1))
-__device__ __forceinline__ void sample0(const Side &L, const Side &R, double g, const Star &S, bool vac,
+__device__ __forceinline__ void sample0(const Side &L, const Side &R, const Gas &G, const Star &S, bool vac,
                                         double &d, double &u, double &p, bool &right) {
   if (vac) {
-    const double sl = L.u + 2.0 * L.c / (g - 1.0), sr = R.u - 2.0 * R.c / (g - 1.0);
+    const double sl = L.u + G.k2 * L.c, sr = R.u - G.k2 * R.c;
     if (0.0 <= L.u - L.c) { right = false; d = L.d; u = L.u; p = L.p; }
-    else if (0.0 < sl) { right = false; fan_left(L, g, d, u, p); }
+    else if (0.0 < sl) { right = false; fan_left(L, G, d, u, p); }
     else if (0.0 >= R.u + R.c) { right = true; d = R.d; u = R.u; p = R.p; }
-    else if (0.0 > sr) { right = true; fan_right(R, g, d, u, p); }
+    else if (0.0 > sr) { right = true; fan_right(R, G, d, u, p); }
     else { right = false; d = 0.0; u = 0.0; p = 0.0; }
     return;
   }
   const double ps = S.p, us = S.u;
-  const double g1 = (g - 1.0) / (2.0 * g), g2 = (g + 1.0) / (2.0 * g), g6 = (g - 1.0) / (g + 1.0), k = 2.0 / (g - 1.0);
+  const double g1 = G.z, g2 = G.g2, g6 = G.g6, k = G.k2;
   if (0.0 <= us) {                                   // left of the contact
     right = false;
     if (ps > L.p) {                                  // left shock
@@ -282,7 +311,7 @@ __device__ __forceinline__ void sample0(const Side &L, const Side &R, double g, 
         const double q = S.w / L.w;
         const double cml = L.c * q;
         if (0.0 > us - cml) { d = L.d * pow_k(q, k); u = us; p = ps; }
-        else fan_left(L, g, d, u, p);
+        else fan_left(L, G, d, u, p);
       }
     }
   } else {                                           // right of the contact
@@ -298,7 +327,7 @@ __device__ __forceinline__ void sample0(const Side &L, const Side &R, double g, 
         const double q = S.w / R.w;
         const double cmr = R.c * q;
         if (0.0 <= us + cmr) { d = R.d * pow_k(q, k); u = us; p = ps; }
-        else fan_right(R, g, d, u, p);
+        else fan_right(R, G, d, u, p);
       }
     }
   }
@@ -309,15 +338,15 @@ __device__ __forceinline__ void sample0(const Side &L, const Side &R, double g, 
 // states in the slot order dens, velx, vely, velz, pres, ...; DIR is the
 // normal direction (1..3).
 template <int DIR>
-__device__ __forceinline__ void godunov_flux(const double *VL, const double *VR, const Side &L, const Side &R, double g,
-                                             const Star &S, bool vac, double F[6]) {
+__device__ __forceinline__ void godunov_flux(const double *VL, const double *VR, const Side &L, const Side &R,
+                                             const Gas &G, const Star &S, bool vac, double F[6]) {
   double d, u, p;
   bool right;
-  sample0(L, R, g, S, vac, d, u, p, right);
+  sample0(L, R, G, S, vac, d, u, p, right);
   double v[3];
 #pragma unroll
   for (int m = 0; m < 3; ++m) v[m] = (m == DIR - 1) ? u : (right ? VR[1 + m] : VL[1 + m]);
-  const double E = p / (g - 1.0) + 0.5 * d * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+  const double E = p * G.gm1inv + 0.5 * d * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
   F[0] = d * u;
   F[1] = F[0] * v[0]; F[2] = F[0] * v[1]; F[3] = F[0] * v[2];
   F[DIR] += p;

@@ -134,6 +134,7 @@ static void fill_devparams(const flash_hy_ctx *c, DevParams &P) {
   }
   P.lim_beta = c->p.limited_slope_beta;
   P.gamma = c->p.gamma;
+  P.gas = xrs::gas_of(c->p.gamma);
   double gammam1 = 1.0 / (c->p.gamma - 1.0);            // eos_initGamma.F90:32
   P.gam1inv = 1. / gammam1;                             // eos_idealGamma.F90:323-326
   P.ggprodinv = 1. / (gammam1 * c->p.gas_constant);     // eos_idealGamma.F90:262

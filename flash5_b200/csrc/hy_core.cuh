@@ -12,6 +12,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include "exact_rs.cuh"
 
 namespace fhy {
 
@@ -87,6 +88,8 @@ struct DevParams {
   // split step: species face fluxes F_dens * X per block, direction and
   // species, in the face order of the hydro flux store [block][dir][nsp][faces]
   double *sp_fstore;
+  // the exact Riemann solver's gas constants (xrs::gas_of(gamma), host-side)
+  xrs::Gas gas;
 };
 
 // Cell sizes of block b: level-1 deltas scaled by 2^(1-level) (exact).

@@ -426,10 +426,10 @@ __device__ void cfl_block_reduce(CflCand c, int blk, double cfl, CflPart *part) 
 // ---------------------------------------------------------------------------
 // exact Riemann face flux (no FLASH5 counterpart; Toro ch. 4, exact_rs.cuh)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ xrs::Side side_of(const double *V, int n, double g, unsigned &st) {
-  const double c2 = g * V[HP] / V[HD];
+__device__ __forceinline__ xrs::Side side_of(const double *V, int n, const xrs::Gas &G, unsigned &st) {
+  const double c2 = G.g * V[HP] / V[HD];
   if (!(c2 > 0.0)) st |= ST_NEG_SOUND;
-  return xrs::make_side(V[HD], V[n], V[HP], sqrt(c2), g);
+  return xrs::make_side(V[HD], V[n], V[HP], sqrt(c2), G);
 }
 
 // keep a hashed sample of the face states (two-rarefaction guess inexact) for
@@ -449,14 +449,16 @@ __device__ __forceinline__ void harvest_face(const DevParams &P, const xrs::Side
 
 // Godunov flux from the exact solution, Newton from the two-rarefaction guess
 template <int DIR>
-__device__ __forceinline__ void exact_face(const DevParams &P, const double *VL, const double *VR, double F[6],
-                                           unsigned &st) {
-  const double g = P.gamma;
-  const xrs::Side L = side_of(VL, DIR, g, st), R = side_of(VR, DIR, g, st);
-  const bool vac = xrs::vacuum(L, R, g);
+__device__ __forceinline__ void exact_face(const DevParams &P, const xrs::Gas &G, const double *VL, const double *VR,
+                                           double F[6], unsigned &st) {
+  const xrs::Side L = side_of(VL, DIR, G, st), R = side_of(VR, DIR, G, st);
+  const bool vac = xrs::vacuum(L, R, G);
   xrs::Star S{0.0, 0.5 * (L.u + R.u), 0.0};
-  if (!vac && xrs::newton(L, R, g, xrs::tr_w(L, R, g), P.rs_tol, P.rs_max_iter, S) < 0) st |= ST_NEWTON;
-  xrs::godunov_flux<DIR>(VL, VR, L, R, g, S, vac, F);
+  if (!vac) {
+    const xrs::SideK kl = xrs::side_k(L, G), kr = xrs::side_k(R, G);
+    if (xrs::newton(L, R, kl, kr, G, xrs::tr_w(L, R, kl, kr, G), P.rs_tol, P.rs_max_iter, S) < 0) st |= ST_NEWTON;
+  }
+  xrs::godunov_flux<DIR>(VL, VR, L, R, G, S, vac, F);
 }
 
 // ---------------------------------------------------------------------------
@@ -775,7 +777,7 @@ __global__ void __launch_bounds__(320) k_dir(const DevParams P, const R *__restr
     }
     VL[HGC] = gam; VR[HGC] = gam;
     R F[6];
-    if constexpr (RS == 1) exact_face<DIR>(P, VL, VR, F, st);
+    if constexpr (RS == 1) exact_face<DIR>(P, P.gas, VL, VR, F, st);
     else hllc<R, DIR>(P, VL, VR, F, st);
 #pragma unroll
     for (int n = 0; n < 6; ++n) sF[n * G::n + t] = F[n];

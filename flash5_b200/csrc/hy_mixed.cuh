@@ -393,6 +393,7 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
     double *sP0 = sIg;
     const bool learned = P.mlp != nullptr;
     const double g = P.gamma;
+    const xrs::Gas &gas = P.gas;             // from the parameter block
     auto face = [&](int qq, bool left, int s, int t) -> double {
       return left ? Vs(qq, s - G::step) + double(sWp[qq * G::SC + t - G::step])
                   : Vs(qq, s) + double(sWm[qq * G::SC + t]);
@@ -407,8 +408,8 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
       L = xrs::Side{dl, ul, pl, sqrt(c2l), 0.0};
       R = xrs::Side{dr, ur, pr, sqrt(c2r), 0.0};
       if (with_w) {
-        L.w = xrs::powp(pl, xrs::zexp(g));
-        R.w = xrs::powp(pr, xrs::zexp(g));
+        L.w = xrs::powp(pl, gas.z);
+        R.w = xrs::powp(pr, gas.z);
       }
     };
     if (learned) {
@@ -429,11 +430,11 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
                                face(0, false, s4, t), face(DIR, false, s4, t), face(4, false, s4, t), g)) {
           xrs::Side L, R;
           sides(s4, t, L, R, false);
-          if (!xrs::vacuum(L, R, g) && xrs::strong_waves(L, R)) {
-            L.w = xrs::powp(L.p, xrs::zexp(g));
-            R.w = xrs::powp(R.p, xrs::zexp(g));
-            const double wtr = xrs::tr_w(L, R, g);
-            if (!xrs::tr_exact(L, R, xrs::p_of_w(wtr, g))) q = wtr;
+          if (!xrs::vacuum(L, R, gas) && xrs::strong_waves(L, R)) {
+            L.w = xrs::powp(L.p, gas.z);
+            R.w = xrs::powp(R.p, gas.z);
+            const double wtr = xrs::tr_w(L, R, gas);
+            if (!xrs::tr_exact(L, R, xrs::p_of_w(wtr, gas))) q = wtr;
           }
         }
         sP0[t] = q;
@@ -457,13 +458,13 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
           xrs::Side L{1.0, 0.0, 1.0, 1.0, 1.0}, R{1.0, 0.0, 1.0, 1.0, 1.0};
           if (net) sides(G::at(x, l, G::L4, 4), t, L, R);
           float f[xrs::NIN];
-          if (net) xrs::features(L, R, g, xrs::p_of_w(q, g), f);
+          if (net) xrs::features(L, R, g, xrs::p_of_w(q, gas), f);
           else {
 #pragma unroll
             for (int k = 0; k < xrs::NIN; ++k) f[k] = 0.f;
           }
           const float y = fminf(fmaxf(xrs::mlp_lane(*sM, f), -20.f), 20.f);
-          if (net) sP0[t] = -(q * (double)expf(float(xrs::zexp(g)) * y));    // (p*/p_TR)^z
+          if (net) sP0[t] = -(q * (double)expf(float(gas.z) * y));    // (p*/p_TR)^z
         }
       }
     }
@@ -477,15 +478,16 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
       const int s = G::at(x, l, G::L4, 4);
       xrs::Side L, R;
       sides(s, t, L, R);
-      const bool vac = xrs::vacuum(L, R, g);
+      const bool vac = xrs::vacuum(L, R, gas);
       xrs::Star S{0.0, 0.5 * (L.u + R.u), 0.0};
       if (!vac) {
         const double q = learned ? sP0[t] : 0.0;
-        const double w0 = q < 0.0 ? -q : xrs::tr_w(L, R, g);
-        int k = xrs::newton(L, R, g, w0, P.rs_tol, q < 0.0 ? 3 : P.rs_max_iter, S);
-        if (k < 0 && q < 0.0) k = xrs::newton(L, R, g, xrs::tr_w(L, R, g), P.rs_tol, P.rs_max_iter, S);
+        const xrs::SideK kl = xrs::side_k(L, gas), kr = xrs::side_k(R, gas);
+        const double w0 = q < 0.0 ? -q : xrs::tr_w(L, R, kl, kr, gas);
+        int k = xrs::newton(L, R, kl, kr, gas, w0, P.rs_tol, q < 0.0 ? 3 : P.rs_max_iter, S);
+        if (k < 0 && q < 0.0) k = xrs::newton(L, R, kl, kr, gas, xrs::tr_w(L, R, kl, kr, gas), P.rs_tol, P.rs_max_iter, S);
         if (k < 0) st |= ST_NEWTON;
-        if (P.harvest && (q < 0.0 || (xrs::strong_waves(L, R) && !xrs::tr_exact(L, R, xrs::p_of_w(w0, g)))))
+        if (P.harvest && (q < 0.0 || (xrs::strong_waves(L, R) && !xrs::tr_exact(L, R, xrs::p_of_w(w0, gas)))))
           harvest_face(P, L, R, g, (unsigned)(blockIdx.x * 4 + DIR) * 2048u + (unsigned)t);
       }
       double VL[8], VR[8];
@@ -496,7 +498,7 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
         VR[n] = face(qq, false, s, t);
       }
       double F[6];
-      xrs::godunov_flux<DIR>(VL, VR, L, R, g, S, vac, F);
+      xrs::godunov_flux<DIR>(VL, VR, L, R, gas, S, vac, F);
 #pragma unroll
       for (int n = 0; n < 6; ++n) Fr[it][n] = F[n];
       double fv = 0., fe = 0.;

@@ -34,12 +34,13 @@ using namespace xrs;
 // ---------------------------------------------------------------------------
 constexpr int SOLVE_THREADS = 256;
 
-__device__ __forceinline__ void load_state(const double *__restrict__ S, long n, long i, Side &L, Side &R, double &g) {
+__device__ __forceinline__ void load_state(const double *__restrict__ S, long n, long i, Side &L, Side &R, Gas &G) {
   L.d = S[i]; L.u = S[n + i]; L.p = S[2 * n + i];
   R.d = S[3 * n + i]; R.u = S[4 * n + i]; R.p = S[5 * n + i];
-  g = S[6 * n + i];
+  const double g = S[6 * n + i];
+  G = gas_of(g);
   L.c = sqrt(g * L.p / L.d); R.c = sqrt(g * R.p / R.d);
-  L.w = powp(L.p, zexp(g)); R.w = powp(R.p, zexp(g));
+  L.w = powp(L.p, G.z); R.w = powp(R.p, G.z);
 }
 
 // learned != 0: Newton gets three evaluations from the network's guess where
@@ -65,15 +66,17 @@ k_solve(const double *__restrict__ S, long n, double *__restrict__ out, unsigned
     const long i = base + threadIdx.x;
     const bool valid = i < n;
     Side L, R;
-    double g = 1.4;
+    Gas G;
     if (valid) {
-      load_state(S, n, i, L, R, g);
+      load_state(S, n, i, L, R, G);
     } else {
+      G = gas_of(1.4);
       L.d = R.d = 1.0; L.u = R.u = 0.0; L.p = R.p = 1.0; L.c = R.c = sqrt(1.4); L.w = R.w = 1.0;
     }
-    const bool vac = vacuum(L, R, g);
-    const double wtr = vac ? 0.0 : tr_w(L, R, g);
-    const double ptr = vac ? 0.0 : p_of_w(wtr, g);
+    const SideK kl = side_k(L, G), kr = side_k(R, G);
+    const bool vac = vacuum(L, R, G);
+    const double wtr = vac ? 0.0 : tr_w(L, R, kl, kr, G);
+    const double ptr = vac ? 0.0 : p_of_w(wtr, G);
     double w0 = wtr;
     bool net = false;
     if (learned) {
@@ -82,10 +85,10 @@ k_solve(const double *__restrict__ S, long n, double *__restrict__ out, unsigned
       net = valid && !vac && !tr_exact(L, R, ptr) && strong_waves(L, R);
       if (__any_sync(0xffffffffu, net)) {
         float f[NIN];
-        if (net) features(L, R, g, ptr, f);
+        if (net) features(L, R, G.g, ptr, f);
         else for (int k = 0; k < NIN; ++k) f[k] = 0.f;
         float y = fminf(fmaxf(mlp_lane(M, f), -20.f), 20.f);
-        if (net) w0 = wtr * (double)expf(float(zexp(g)) * y);    // (p*/p_TR)^z
+        if (net) w0 = wtr * (double)expf(float(G.z) * y);    // (p*/p_TR)^z
       }
     }
     unsigned char fl = 0;
@@ -95,7 +98,7 @@ k_solve(const double *__restrict__ S, long n, double *__restrict__ out, unsigned
     if (vac) {
       fl |= 2;
     } else {
-      int k = newton(L, R, g, w0, tol, net ? 3 : max_iter, S);
+      int k = newton(L, R, kl, kr, G, w0, tol, net ? 3 : max_iter, S);
       if (k > 0) its = k;
       else if (net) pending = true;
       else { its = max_iter; fl |= 4; st |= FLASH_HY_ERR_NEWTON_NOCONV; }
@@ -129,11 +132,12 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_fallback(const double *__rest
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
     const long i = queue[q];
     Side L, R;
-    double g;
-    load_state(S, n, i, L, R, g);
+    Gas G;
+    load_state(S, n, i, L, R, G);
     Star S;
     unsigned char fl = 1;
-    int k = newton(L, R, g, tr_w(L, R, g), tol, max_iter, S);
+    const SideK kl = side_k(L, G), kr = side_k(R, G);
+    int k = newton(L, R, kl, kr, G, tr_w(L, R, kl, kr, G), tol, max_iter, S);
     int its = 3 + (k > 0 ? k : max_iter);
     if (k <= 0) { fl |= 4; st |= FLASH_HY_ERR_NEWTON_NOCONV; }
     out[i] = S.p; out[n + i] = S.u;
@@ -156,10 +160,10 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_predict(const double *__restr
     bool vac = true;
     if (i < n) {
       Side L, R;
-      double g;
-      load_state(S, n, i, L, R, g);
-      vac = vacuum(L, R, g);
-      if (!vac) features(L, R, g, tr_guess(L, R, g), f);
+      Gas G;
+      load_state(S, n, i, L, R, G);
+      vac = vacuum(L, R, G);
+      if (!vac) features(L, R, G.g, tr_guess(L, R, G), f);
     }
     const float yy = mlp_lane(M, f);
     if (i < n) y[i] = vac ? 0.f : yy;
@@ -201,17 +205,17 @@ __global__ void k_generate(uint64_t seed, long n, double *S) {
 __global__ void k_make_samples(const double *S, const double *out, long n, float *X, float *T, int *count, long cap) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
     Side L, R;
-    double g;
-    load_state(S, n, i, L, R, g);
-    if (2.0 * (L.c + R.c) / (g - 1.0) <= R.u - L.u) continue;
+    Gas G;
+    load_state(S, n, i, L, R, G);
+    if (vacuum(L, R, G)) continue;
     double ps = out[i];
     if (!(ps > 0.0)) continue;
-    double ptr = tr_guess(L, R, g);
+    double ptr = tr_guess(L, R, G);
     if (tr_exact(L, R, ptr) || !strong_waves(L, R)) continue;   // where the network is consulted
     int k = atomicAdd(count, 1);
     if (k >= cap) continue;
     float f[NIN];
-    features(L, R, g, ptr, f);
+    features(L, R, G.g, ptr, f);
     for (int q = 0; q < NIN; ++q) X[(long)k * NIN + q] = f[q];
     T[k] = float(log(ps / ptr));
   }
