@@ -92,6 +92,16 @@ __device__ __forceinline__ double pow_n(double w, const PowN &e) {
   if (e.ni == 8) { const double w2 = w * w, w4 = w2 * w2; return w4 * w4; }
   return pow_k(w, e.n);
 }
+// p = w^n and dp/dw = n w^(n-1), the latter from the same powers for the
+// integer exponents (no division)
+__device__ __forceinline__ double pow_n_d(double w, const PowN &e, double &dpdw) {
+  if (e.ni == 5) { const double w2 = w * w, w4 = w2 * w2; dpdw = 5.0 * w4; return w4 * w; }
+  if (e.ni == 7) { const double w2 = w * w, w6 = w2 * w2 * w2; dpdw = 7.0 * w6; return w6 * w; }
+  if (e.ni == 8) { const double w2 = w * w, w4 = w2 * w2, w7 = w4 * w2 * w; dpdw = 8.0 * w7; return w7 * w; }
+  const double p = pow_k(w, e.n);
+  dpdw = e.n * p / w;
+  return p;
+}
 
 // Constants of the gas, taken once per context on the host where the
 // adiabatic index is uniform (the hydro kernels read them from their
@@ -129,9 +139,8 @@ __device__ __forceinline__ SideK side_k(const Side &s, const Gas &G) {
   return SideK{s.w, s.p, G.k2 * s.c / s.w, G.a2 / s.d, G.g6 * s.p};
 }
 
-// f_K(w) and df_K/dw (Toro eqs. 4.6-4.7 with p = w^n); iw = 1/w
-__device__ __forceinline__ void pres_fn(double w, double p, double iw, const SideK &s, double n, double &f,
-                                        double &fd) {
+// f_K(w) and df_K/dw (Toro eqs. 4.6-4.7 with p = w^n, dp/dw = dpdw)
+__device__ __forceinline__ void pres_fn(double w, double p, double dpdw, const SideK &s, double &f, double &fd) {
   if (w <= s.w) {                                   // rarefaction, Toro eq. 4.7
     f = s.k * (w - s.w);
     fd = s.k;
@@ -139,7 +148,7 @@ __device__ __forceinline__ void pres_fn(double w, double p, double iw, const Sid
     const double r = 1.0 / (s.B + p);
     const double q = sqrt(s.A * r);
     f = (p - s.p) * q;
-    fd = (1.0 - 0.5 * (p - s.p) * r) * q * (n * p * iw);   // df/dp dp/dw
+    fd = (1.0 - 0.5 * (p - s.p) * r) * q * dpdw;    // df/dp dp/dw
   }
 }
 
@@ -220,10 +229,10 @@ __device__ __forceinline__ int newton(const Side &L, const Side &R, const SideK 
   double fl = 0., fdl = 0., fr = 0., fdr = 0., we = w0;
   int evals = 0;
   for (; evals < max_iter;) {
-    p = pow_n(w, e);
-    const double iw = 1.0 / w;
-    pres_fn(w, p, iw, kl, e.n, fl, fdl);
-    pres_fn(w, p, iw, kr, e.n, fr, fdr);
+    double dpdw;
+    p = pow_n_d(w, e, dpdw);
+    pres_fn(w, p, dpdw, kl, fl, fdl);
+    pres_fn(w, p, dpdw, kr, fr, fdr);
     ++evals;
     we = w;
     const double f = fl + fr + du;
