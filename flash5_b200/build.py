@@ -29,6 +29,7 @@ UNITS = [
     ("riemann_exact.o", "riemann_exact.cu", ["--fmad=true"]),
     ("cfl_noalloc.o", "cfl_noalloc.cu", ["--fmad=false"]),
     ("spec.o", "spec.cu", ["--fmad=false"]),
+    ("spec_mx.o", "spec.cu", ["-DFHY_SPEC_MIXED", "--fmad=true"]),
     ("refine.o", "refine.cu", ["--fmad=false"]),
     ("tree.o", "tree.cu", []),
 ]

@@ -692,6 +692,7 @@ static int enqueue_step(flash_hy_ctx *c, double dt, const int *d_list, int nlaun
   if (c->nsp > 0) {
     SpecArgs sa;
     sa.P = a.P;
+    sa.mixed = c->p.precision == FLASH_HY_PREC_MIXED;
     sa.P.sp_fstore = c->d_sp_fstore;
     sa.ncells = c->ncells;
     sa.nlaunch = nlaunch;

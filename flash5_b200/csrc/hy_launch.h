@@ -32,6 +32,7 @@ struct StepArgs {
 // the species / mass-scalar pass after the hydro direction kernels
 struct SpecArgs {
   DevParams P;        // the step's parameters (species buffers, mass fluxes, flags)
+  bool mixed;         // the mixed path: FP32 face values (spec_step_mx)
   size_t ncells;
   int nlaunch;
   cudaStream_t stream;
@@ -43,6 +44,7 @@ struct SpecArgs {
 };
 // launches k_spec_step (once, or once per level); returns the launch count or -2
 int spec_step(const SpecArgs &a, int ndim, int nx, int ny, int nz);
+int spec_step_mx(const SpecArgs &a, int ndim, int nx, int ny, int nz);
 
 // the refinement criterion of every listed block (all blocks without a list)
 struct ErrArgs {

@@ -191,16 +191,107 @@ __device__ __forceinline__ void spec_faces(const DevParams &P, int slot, const d
   }
 }
 
+// The mixed path's face fluxes: the face values of spec_faces in FP32 on
+// differences from the cell's mass fraction X_c (taken in FP64 and rounded:
+// the delta form of the mixed hydro reconstruction, in which X_c is the
+// origin, so 3 X_c - 2 r becomes -2 r and f X_c + (1 - f) l becomes
+// (1 - f) l), SpcSig in FP32 on FP64 differences, and the upwind flux
+// F_dens * (X_c + delta) in FP64.
+template <int NDIM, int NX, int NY, int NZ, int DIR>
+__device__ __forceinline__ void spec_faces_mx(const DevParams &P, int slot, const double *sV, const double *sX,
+                                              double *sF, const double *sK) {
+  using L = DirGeom<NDIM, NX, NY, NZ, double, DIR>;
+  using B = Box<NDIM, NX, NY, NZ>;
+  using E = Ext<NDIM, NX, NY, NZ, 3>;
+  constexpr int es = DIR == 1 ? 1 : (DIR == 2 ? E::ex : E::ex * E::ey);
+  constexpr int A1 = DIR == 1 ? 2 : (DIR == 2 ? 3 : 1), S1 = DIR == 1 ? 3 : (DIR == 2 ? 1 : 2);
+  constexpr int A2 = DIR == 1 ? 3 : (DIR == 2 ? 1 : 2), S2 = DIR == 1 ? 2 : (DIR == 2 ? 3 : 1);
+  const bool ctu = NDIM == 3 && P.use_ctu;
+  const size_t lb = sp_line_base<NDIM, NX, NY, NZ, DIR>(slot);
+  const float hdtx = float(sK[SK_HDTX]), hdty = float(sK[SK_HDTY]), hdtz = float(sK[SK_HDTZ]);
+  const float hdtn = float(sK[SK_DIR0 + 4 * (DIR - 1) + 2]), fac = float(sK[SK_DIR0 + 4 * (DIR - 1) + 3]);
+  auto sig = [&](int d, int i, int j, int k) -> float {
+    const int st = d == 0 ? 1 : (d == 1 ? E::ex : E::ex * E::ey);
+    const int e = E::idx(i, j, k);
+    const double lam = sV[d * B::n + B::idx(i, j, k)];
+    const double g = lam > 0. ? sX[e] - sX[e - st] : sX[e + st] - sX[e];
+    return float(lam) * float(g);
+  };
+  auto minmod = [](float a, float b) { return a * b > 0.f ? copysignf(fminf(fabsf(a), fabsf(b)), a) : 0.f; };
+  for (int t = threadIdx.x; t < L::n; t += blockDim.x) {
+    int i, j, k;
+    L::decode(t, i, j, k);
+    const int a = L::along(i, j, k);
+    const float flat = P.use_flattening ? float(__ldg(P.sp_flat + lb + t)) : 0.f;
+    const bool fb = ctu && __ldg(P.sp_fb + lb + t);
+    const double mL = a >= 0 ? __ldg(P.sp_mf + lb + t) : 0.;
+    const double mR = a < L::nd ? __ldg(P.sp_mf + lb + t + L::stride) : 0.;
+    const int e = E::idx(i, j, k);
+    const double Xc = sX[e];
+    const float Smm = float(sX[e - 2 * es] - Xc), Sm = float(sX[e - es] - Xc);
+    const float Sp = float(sX[e + es] - Xc), Spp = float(sX[e + 2 * es] - Xc);
+    const int bi = B::idx(i, j, k);
+    const float lam = float(sV[(DIR - 1) * B::n + bi]);
+    float dP = minmod(Sp, Spp - Sp);
+    float d0 = minmod(-Sm, Sp);
+    float dN = minmod(Sm - Smm, -Sm);
+    float l = 0.5f * Sm - (d0 - dN) * (1.f / 6.f);
+    float r = 0.5f * Sp - (dP - d0) * (1.f / 6.f);
+    l = fmaxf(fminf(0.f, Sm), fminf(fmaxf(0.f, Sm), l));
+    r = fmaxf(fminf(0.f, Sp), fminf(fmaxf(0.f, Sp), r));
+    if (r * (-l) <= 0.f) { r = 0.f; l = 0.f; }
+    if (6.f * (r - l) * (-0.5f * (r + l)) > (r - l) * (r - l)) l = -2.f * r;
+    if (6.f * (r - l) * (-0.5f * (r + l)) < -((r - l) * (r - l))) r = -2.f * l;
+    d0 = r - l;
+    const float s6 = -3.f * (r + l);
+    const float lm = fminf(lam, 0.f), lp = fmaxf(lam, 0.f);
+    l = l - lm * hdtn * (d0 + (1.f + lm * (4.f / 3.f) * hdtn) * s6);
+    r = r - lp * hdtn * (d0 - (1.f - lp * (4.f / 3.f) * hdtn) * s6);
+    if (P.use_flattening) { l = (1.f - flat) * l; r = (1.f - flat) * r; }
+    if (NDIM == 2) {
+      const float c = DIR == 1 ? hdty * sig(1, i, j, k) : hdtx * sig(0, i, j, k);
+      l -= c; r -= c;
+    } else if (NDIM == 3) {
+      const float c = DIR == 1 ? hdty * sig(1, i, j, k) + hdtz * sig(2, i, j, k)
+                               : (DIR == 2 ? hdtx * sig(0, i, j, k) + hdtz * sig(2, i, j, k)
+                                           : hdtx * sig(0, i, j, k) + hdty * sig(1, i, j, k));
+      l -= c; r -= c;
+    }
+    if (ctu) {
+      if (fb) {
+        l = 0.f;
+        r = 0.f;
+      } else {
+        float T = 0.f;
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int ax = u ? A2 : A1, sd = u ? S2 : S1;
+          const float lamA = float(sV[(ax - 1) * B::n + bi]);
+          const float gm = sig(sd - 1, i - (ax == 1), j - (ax == 2), k - (ax == 3));
+          const float g0 = sig(sd - 1, i, j, k);
+          const float gp = sig(sd - 1, i + (ax == 1), j + (ax == 2), k + (ax == 3));
+          T += lamA * (lamA > 0.f ? g0 - gm : gp - g0);
+        }
+        r += T * fac;
+        l += T * fac;
+      }
+    }
+    if (a >= 0 && mL < 0.) sF[t] = mL * (Xc + double(l));
+    if (a < L::nd && !(mR < 0.)) sF[t + L::stride] = mR * (Xc + double(r));
+  }
+}
+
 // one direction of k_spec_step: face fluxes, the species flux register at
 // fine/coarse faces (AMR), and the flux divergence added, in the x, y, z
 // order of the update, to the accumulators of the thread's interior cells
-template <int NDIM, int NX, int NY, int NZ, int DIR>
+template <int NDIM, int NX, int NY, int NZ, int DIR, bool MX>
 __device__ __forceinline__ void spec_dir(const DevParams &P, int b, int3 bc, int slot, int q, const double *sV,
                                          const double *sX, double *sF, const double *sK,
                                          double (&acc)[SpecStep<NDIM, NX, NY, NZ>::CPT]) {
   using L = DirGeom<NDIM, NX, NY, NZ, double, DIR>;
   using SS = SpecStep<NDIM, NX, NY, NZ>;
-  spec_faces<NDIM, NX, NY, NZ, DIR>(P, slot, sV, sX, sF, sK);
+  if constexpr (MX) spec_faces_mx<NDIM, NX, NY, NZ, DIR>(P, slot, sV, sX, sF, sK);
+  else spec_faces<NDIM, NX, NY, NZ, DIR>(P, slot, sV, sX, sF, sK);
   __syncthreads();
   if (P.sp_freg) {
     flux_register_v<NDIM, NX, NY, NZ, DIR>(P, b, bc, sF, 0, [](int along, int t1, int t2) {
@@ -235,7 +326,8 @@ __device__ __forceinline__ void spec_dir(const DevParams &P, int b, int3 bc, int
 // the mass scalars) are renormalised to a unit sum.  The face arrays
 // alternate between directions, so a direction's divergence and the next
 // direction's faces need no barrier between them.
-template <int NDIM, int NX, int NY, int NZ>
+// MX: the mixed path's FP32 face values (spec_faces_mx)
+template <int NDIM, int NX, int NY, int NZ, bool MX>
 __global__ void __launch_bounds__(SpecStep<NDIM, NX, NY, NZ>::NT, SpecStep<NDIM, NX, NY, NZ>::MINB) k_spec_step(const DevParams P, size_t ncells) {
   using SS = SpecStep<NDIM, NX, NY, NZ>;
   using B = Box<NDIM, NX, NY, NZ>;
@@ -344,9 +436,9 @@ __global__ void __launch_bounds__(SpecStep<NDIM, NX, NY, NZ>::NT, SpecStep<NDIM,
     cp_async_wait_all();
     __syncthreads();
     double acc[SS::CPT];
-    spec_dir<NDIM, NX, NY, NZ, 1>(P, b, bc, slot, q, sV, sX, sF0, sK, acc);
-    if constexpr (NDIM > 1) spec_dir<NDIM, NX, NY, NZ, 2>(P, b, bc, slot, q, sV, sX, sF1, sK, acc);
-    if constexpr (NDIM > 2) spec_dir<NDIM, NX, NY, NZ, 3>(P, b, bc, slot, q, sV, sX, sF0, sK, acc);
+    spec_dir<NDIM, NX, NY, NZ, 1, MX>(P, b, bc, slot, q, sV, sX, sF0, sK, acc);
+    if constexpr (NDIM > 1) spec_dir<NDIM, NX, NY, NZ, 2, MX>(P, b, bc, slot, q, sV, sX, sF1, sK, acc);
+    if constexpr (NDIM > 2) spec_dir<NDIM, NX, NY, NZ, 3, MX>(P, b, bc, slot, q, sV, sX, sF0, sK, acc);
     // the old mass fractions from the staged species; the barrier keeps the
     // next species' copies from overwriting them before every thread is done
     if (P.fmode != 2) {
@@ -355,7 +447,8 @@ __global__ void __launch_bounds__(SpecStep<NDIM, NX, NY, NZ>::NT, SpecStep<NDIM,
       const int c = threadIdx.x + u * SS::NT;
       if (c < NCB) {
         const double X = sX[E::idx(c % NX, (c / NX) % NY, c / (NX * NY))];
-        P.sp_out[(size_t)q * ncells + (size_t)b * NCB + c] = (X * sRo[c] + dt * acc[u]) / sRn[c];
+        P.sp_out[(size_t)q * ncells + (size_t)b * NCB + c] =
+            __ddiv_rn(__dadd_rn(__dmul_rn(X, sRo[c]), __dmul_rn(dt, acc[u])), sRn[c]);   // never contracted
       }
     }
     }
@@ -402,7 +495,8 @@ __global__ void __launch_bounds__(256) k_spec_update(const DevParams P, size_t n
         const double dd = div_rn(F[fl] - F[fr], del[d], rdel[d]);
         acc = d == 0 ? dd : acc + dd;
       }
-      P.sp_out[(size_t)q * ncells + off] = (P.sp_in[(size_t)q * ncells + off] * ro + dt * acc) / rn;
+      P.sp_out[(size_t)q * ncells + off] =
+          __ddiv_rn(__dadd_rn(__dmul_rn(P.sp_in[(size_t)q * ncells + off], ro), __dmul_rn(dt, acc)), rn);
     }
     if (P.nspec > 0) {
       double sum = 0.;
