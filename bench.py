@@ -656,7 +656,8 @@ def main():
                        "riemann": "exact (Newton 1e-12)" if spec[head][1] == abi.RS_EXACT else "HLLC",
                        "zones_per_gpu": zones, "l2": f"inputs larger than L2 (state {zones * 40 / 1e6:.0f} MB)",
                        **({"species": args.nspecies, "mass_scalars": args.nmass_scalars,
-                           "species_note": "dense-layer species pair and passive tracers, FP64 species pass"}
+                           "species_note": "dense-layer species pair and passive tracers; species pass in FP64 on the FP64 "
+                                           "paths, FP32 face values with FP64 fluxes and update on the mixed paths"}
                           if args.nspecies + args.nmass_scalars else {}),
                        "path": head},
             "paths": {n: {"value": total / (ms[n] * 1e-3), "ms_per_step": ms[n], "note": notes[n],
