@@ -7,7 +7,8 @@
 * the hydro variables are bit-identical with and without species;
 * mixed precision: species within 1e-6 relative L1 of the FP64 GPU run;
 * species on AMR hierarchies (restriction, guard cells, the species flux
-  register) and through a regrid equal the oracle bit for bit;
+  register) and through a regrid equal the oracle bit for bit (FP64), and
+  stay within 1e-6 relative L1 of it on the mixed path;
 * the split step keeps the species fluxes after the hydro fluxes in FLASH's
   flux arrays (equal to the oracle's) and, with or without a get/put round
   trip, updates as the fused step does; a replaced mass-scalar flux changes
@@ -240,3 +241,20 @@ def test_amr_species_regrid_matches_oracle():
     leaves = g2.leaf_ids
     a, b = g2.interior(out)[leaves], g2.interior(ref2)[leaves]
     assert np.array_equal(a, b), np.abs(a - b).max()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["kh2d_ring", "kh3d_ring"])
+def test_amr_species_mixed_close(case):
+    """The mixed path's FP32 species face values on AMR hierarchies (one
+    launch per level, species flux register): every scalar within 1e-6
+    relative L1 of the FP64 oracle on the leaves, species summing to one."""
+    from tests.test_gpu_amr import _run_amr, amr_case
+    grid, unk, params = amr_case(case, nspecies=2, nmass_scalars=1, precision=abi.PREC_MIXED)
+    grid, ref, out, _ = _run_amr(grid, unk, params, 4)
+    leaves = grid.leaf_ids
+    a, b = grid.interior(out)[leaves], grid.interior(ref)[leaves]
+    sp = grid.species
+    l1 = np.abs(a[..., sp] - b[..., sp]).sum(axis=(0, 1, 2, 3)) / np.abs(b[..., sp]).sum(axis=(0, 1, 2, 3))
+    assert np.all(l1 <= 1e-6), l1
+    assert np.abs(a[..., sp.start] + a[..., sp.start + 1] - 1.0).max() < 1e-13
