@@ -290,6 +290,11 @@ def conserved_l1(a, b, var):
     return l1(a, b, var)
 
 
+def conserved_linf(a, b, var):
+    from flash5_b200.metrics import conserved_linf as linf
+    return linf(a, b, var)
+
+
 def riemann_workload(args):
     """Isolated exact Riemann solves (1e8 interface pairs): two-rarefaction
     guess vs the learned guess trained on solver-harvested states."""
@@ -368,11 +373,12 @@ def amr_workload(args):
     ms, outs, dts, launches, clocks, e2e_ms, hb = {}, {}, None, {}, None, None, None
     tunings = {}
     regrid_info = None
-    paths = [p for p in args.paths.split(",") if p in ("fp64", "mixed", "mixed_exact")] or ["fp64", "mixed"]
-    spec = {"fp64": (abi.PREC_FP64, abi.RS_HLLC), "mixed": (abi.PREC_MIXED, abi.RS_HLLC),
-            "mixed_exact": (abi.PREC_MIXED, abi.RS_EXACT)}
+    paths = [p for p in args.paths.split(",") if p in ("fp64", "fp64_exact", "mixed", "mixed_exact")] or ["fp64", "mixed"]
+    # (precision, Riemann solver, the FP64 path the errors are measured against)
+    spec = {"fp64": (abi.PREC_FP64, abi.RS_HLLC, None), "fp64_exact": (abi.PREC_FP64, abi.RS_EXACT, None),
+            "mixed": (abi.PREC_MIXED, abi.RS_HLLC, "fp64"), "mixed_exact": (abi.PREC_MIXED, abi.RS_EXACT, "fp64_exact")}
     for name in paths:
-        pr, rsv = spec[name]
+        pr, rsv, _ = spec[name]
         h = Hydro(abi.default_params(precision=pr, riemann_solver=rsv), g)
         h.upload(unk)
         if not args.no_tune:
@@ -416,7 +422,9 @@ def amr_workload(args):
         h.close()
     head = paths[-1]
     leaves = g.leaf_ids
-    errs = {n: conserved_l1(outs[n][leaves], outs["fp64"][leaves], VAR) for n in outs if n != "fp64" and "fp64" in outs}
+    ref_of = {n: spec[n][2] for n in outs if spec[n][2] in outs}
+    errs = {n: conserved_l1(outs[n][leaves], outs[r][leaves], VAR) for n, r in ref_of.items()}
+    errs_inf = {n: conserved_linf(outs[n][leaves], outs[r][leaves], VAR) for n, r in ref_of.items()}
     cpu = None if args.no_cpu else amr_cpu_baseline()
     achieved = zones * BYTES_PER_ZONE / (ms[head] * 1e-3) / 1e9
     levels = np.bincount(g.levels[g.is_leaf], minlength=g.max_level + 1)[1:].tolist()
@@ -427,13 +435,16 @@ def amr_workload(args):
         "data": "synthetic (four-quadrant states; hierarchy from a seeded smoothed density, PCG64 seed 2024)",
         "config": {"workload": f"2D four-quadrant Riemann problem on a {g.max_level}-level AMR hierarchy, "
                                f"{g.nleaves} leaf blocks of 16^2 + 4 guard ({levels} per level), "
-                               f"{g.nblocks - g.nleaves} parents; PPM+HLLC, CFL 0.8, one dt for all levels, "
+                               f"{g.nblocks - g.nleaves} parents; PPM + "
+                               f"{'exact Riemann (Newton 1e-12)' if spec[head][1] == abi.RS_EXACT else 'HLLC'}, "
+                               "CFL 0.8, one dt for all levels, "
                                "fine/coarse flux correction, graph-replayed step",
                    "zones_per_gpu": zones, "leaf_blocks": g.nleaves,
                    "l2": f"inputs larger than L2 (state {g.nblocks * 256 * 40 / 1e6:.0f} MB plus guard buffers "
                          f"{g.nleaves * 576 * 40 / 1e6:.0f} MB)", "path": head, "hierarchy_build_s": build_s},
         "paths": {n: {"value": zones / (ms[n] * 1e-3), "ms_per_step": ms[n],
-                      **({"rel_l1_vs_fp64": errs[n]} if n in errs else {}),
+                      **({f"rel_l1_vs_{ref_of[n]}": errs[n], f"rel_linf_vs_{ref_of[n]}": errs_inf[n]}
+                         if n in errs else {}),
                       **({"launch_shape": tunings[n]} if n in tunings else {})} for n in ms},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": None, "peak_kind": peak_kind,
@@ -617,13 +628,15 @@ def main():
         h.close()
     head = paths[-1]
     errs = {n: conserved_l1(outs[n], outs[spec[n][3]], VAR) for n in outs if spec[n][3] in outs}
+    errs_inf = {n: conserved_linf(outs[n], outs[spec[n][3]], VAR) for n in errs}
     if g.nspecies + g.nmass_scalars:
-        from flash5_b200.metrics import l1_rel
+        from flash5_b200.metrics import l1_rel, mag_err
         for n in errs:
             a, b = outs[n], outs[spec[n][3]]
             for q in range(g.nspecies + g.nmass_scalars):
                 k = g.species.start + q
                 errs[n][f"rho_x{q}"] = l1_rel(a[..., 0] * a[..., k], b[..., 0] * b[..., k])
+                errs_inf[n][f"rho_x{q}"] = mag_err(a[..., 0] * a[..., k], b[..., 0] * b[..., k])
     if dist is not None:
         for n in ms:
             ms[n] = dist_max(dist, ms[n])
@@ -661,7 +674,8 @@ def main():
                           if args.nspecies + args.nmass_scalars else {}),
                        "path": head},
             "paths": {n: {"value": total / (ms[n] * 1e-3), "ms_per_step": ms[n], "note": notes[n],
-                          **({f"rel_l1_vs_{spec[n][3]}": errs[n]} if n in errs else {}),
+                          **({f"rel_l1_vs_{spec[n][3]}": errs[n], f"rel_linf_vs_{spec[n][3]}": errs_inf[n]}
+                             if n in errs else {}),
                           **({"launch_shape": tunings[n]} if n in tunings else {})} for n in ms},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": TRAFFIC_PER_ZONE[head] * zones if head in TRAFFIC_PER_ZONE else None,

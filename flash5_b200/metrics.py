@@ -32,3 +32,9 @@ def conserved_l1(a, b, var):
     """{conserved variable: L1 relative norm of a against b}."""
     ca, cb = conserved(a, var), conserved(b, var)
     return {k: l1_rel(ca[k], cb[k]) for k in CONSERVED}
+
+
+def conserved_linf(a, b, var):
+    """{conserved variable: magnitude error max|a-b| / max|b| of a against b}."""
+    ca, cb = conserved(a, var), conserved(b, var)
+    return {k: mag_err(ca[k], cb[k]) for k in CONSERVED}
