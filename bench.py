@@ -249,7 +249,7 @@ def cpu_baseline(seconds=12.0, steps=None, warmup=0):
             "sample": f"3D KH 64^3 (512 blocks of 8^3), {n} steps, {el:.1f} s, oracle C port, OpenMP"}
 
 
-def train_guess(g, unk, abi, dev, dts):
+def train_guess(g, unk, abi, dev, dts, gamma=5.0 / 3.0):
     """Learned star-pressure guess for the hydro faces: run two steps of the
     mixed exact-solver path with face-state harvesting on (the faces where
     the network is consulted: strong waves, inexact two-rarefaction guess),
@@ -260,7 +260,7 @@ def train_guess(g, unk, abi, dev, dts):
     from flash5_b200.hydro import Hydro
     from flash5_b200.riemann import ExactRiemann
     t0 = time.perf_counter()
-    h = Hydro(abi.default_params(gamma=5.0 / 3.0, precision=abi.PREC_MIXED, riemann_solver=abi.RS_EXACT), g,
+    h = Hydro(abi.default_params(gamma=gamma, precision=abi.PREC_MIXED, riemann_solver=abi.RS_EXACT), g,
               device=dev)
     h.upload(unk)
     dt, _ = h.compute_dt()
@@ -373,13 +373,20 @@ def amr_workload(args):
     ms, outs, dts, launches, clocks, e2e_ms, hb = {}, {}, None, {}, None, None, None
     tunings = {}
     regrid_info = None
-    paths = [p for p in args.paths.split(",") if p in ("fp64", "fp64_exact", "mixed", "mixed_exact")] or ["fp64", "mixed"]
-    # (precision, Riemann solver, the FP64 path the errors are measured against)
-    spec = {"fp64": (abi.PREC_FP64, abi.RS_HLLC, None), "fp64_exact": (abi.PREC_FP64, abi.RS_EXACT, None),
-            "mixed": (abi.PREC_MIXED, abi.RS_HLLC, "fp64"), "mixed_exact": (abi.PREC_MIXED, abi.RS_EXACT, "fp64_exact")}
+    paths = [p for p in args.paths.split(",") if p in ("fp64", "fp64_exact", "mixed", "mixed_exact", "mixed_learned")]
+    paths = paths or ["fp64", "mixed"]
+    # (precision, Riemann solver, the FP64 path the errors are measured against, learned guess)
+    spec = {"fp64": (abi.PREC_FP64, abi.RS_HLLC, None, 0), "fp64_exact": (abi.PREC_FP64, abi.RS_EXACT, None, 0),
+            "mixed": (abi.PREC_MIXED, abi.RS_HLLC, "fp64", 0),
+            "mixed_exact": (abi.PREC_MIXED, abi.RS_EXACT, "fp64_exact", 0),
+            "mixed_learned": (abi.PREC_MIXED, abi.RS_EXACT, "fp64_exact", 1)}
+    training = None
     for name in paths:
-        pr, rsv, _ = spec[name]
-        h = Hydro(abi.default_params(precision=pr, riemann_solver=rsv), g)
+        pr, rsv, _, learned = spec[name]
+        h = Hydro(abi.default_params(precision=pr, riemann_solver=rsv, learned_guess=learned), g)
+        if learned:
+            weights, training = train_guess(g, unk, abi, 0, dts, gamma=abi.default_params().gamma)
+            h.set_guess_weights(weights)
         h.upload(unk)
         if not args.no_tune:
             best, trials = h.autotune(dts[0] if dts is not None else h.compute_dt()[0], steps=2)
@@ -431,7 +438,9 @@ def amr_workload(args):
     line = {
         "metric": METRIC, "value": zones / (ms[head] * 1e-3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms[head], "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32 reconstruction, f64 Riemann/update" if head.startswith("mixed") else "f64",
+        "vs_baseline": None,
+        "dtype": ("f32 reconstruction, f64 Riemann/update" + (", bf16 MLP guess" if head == "mixed_learned" else ""))
+                 if head.startswith("mixed") else "f64",
         "data": "synthetic (four-quadrant states; hierarchy from a seeded smoothed density, PCG64 seed 2024)",
         "config": {"workload": f"2D four-quadrant Riemann problem on a {g.max_level}-level AMR hierarchy, "
                                f"{g.nleaves} leaf blocks of 16^2 + 4 guard ({levels} per level), "
@@ -462,6 +471,8 @@ def amr_workload(args):
         line["cpu_baseline"] = cpu
     if regrid_info is not None:
         line["refinement_cycle"] = regrid_info
+    if training is not None:
+        line["training"] = training
     print(json.dumps(line))
     return 0
 
