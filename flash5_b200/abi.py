@@ -139,6 +139,7 @@ def _set_sigs(lib):
     sigs = {
         "flash_hy_create": (C.c_int, [P, G, C.c_int, C.POINTER(vp)]),
         "flash_hy_destroy": (C.c_int, [vp]),
+        "flash_hy_release_memory": (C.c_int, [C.c_int]),
         "flash_hy_upload": (C.c_int, [vp, dp, C.c_int, C.c_int, V]),
         "flash_hy_download": (C.c_int, [vp, dp, C.c_int, C.c_int, V]),
         "flash_hy_step": (C.c_int, [vp, C.c_double, C.c_double, C.c_double, C.c_int]),

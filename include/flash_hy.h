@@ -134,6 +134,11 @@ typedef struct flash_hy_ctx flash_hy_ctx;
 int flash_hy_create(const flash_hy_params *params, const flash_hy_grid_desc *grid,
                     int device, flash_hy_ctx **ctx_out);
 int flash_hy_destroy(flash_hy_ctx *ctx);
+/* Device memory of destroyed contexts is kept per device (at most 32 GiB)
+ * and reused by later contexts, so that an AMR regrid -- a context for the
+ * new tree, the old one destroyed -- costs no cudaMalloc/cudaFree round trip.
+ * release_memory frees the kept blocks of a device (all devices: -1). */
+int flash_hy_release_memory(int device);
 
 /* Copy the caller's UNK (host memory, nunk variables per cell, guard layers
  * as grid->nguard) into the device block store and apply the gamma-law EOS
