@@ -98,6 +98,8 @@ def test_create_rejects_bad_arguments_without_touching_the_gpu():
         assert lib.flash_hy_create(C.byref(p), C.byref(gd), 0, C.byref(ctx)) == abi.ERR_UNSUPPORTED, kw
     assert lib.flash_hy_set_guess_weights(None, None, 0) == abi.ERR_BAD_ARG
     assert lib.flash_hy_harvest(None, 10, 0) == abi.ERR_BAD_ARG
+    # nothing cached yet: releasing the kept device memory touches no device
+    assert lib.flash_hy_release_memory(-1) == 0
 
 
 def test_grid_descriptor_and_unk_layout():
