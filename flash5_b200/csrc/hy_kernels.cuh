@@ -328,16 +328,14 @@ struct SigStage {
   }
 };
 
-template <int NDIM, int NX, int NY, int NZ, class R, int VAR>
 // 3D: three CTAs per SM where shared memory allows it (FP32 sig); the FP64
 // kernel keeps two, which its registers need
+template <int NDIM, int NX, int NY, int NZ, class R, int VAR>
 __global__ void __launch_bounds__(320, NDIM > 2 ? (sizeof(R) == 4 ? 3 : 2) : 1) k_sig(const DevParams P,
                                                                                      R *__restrict__ SIG) {
   using B = Box<NDIM, NX, NY, NZ>;
   using SG = SigStage<NDIM, NX, NY, NZ>;
   using E = typename SG::E;
-  using H = Halo<NDIM, NX, NY, NZ>;
-  constexpr int NCB = NX * NY * NZ;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double *sQ = reinterpret_cast<double *>(smem_raw);     // [5][E::n]
   int *sNb = reinterpret_cast<int *>(sQ + 5 * E::n);     // [NNB]
