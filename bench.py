@@ -46,9 +46,9 @@ BYTES_PER_ZONE = 80.0          # read + write of 5 FP64 state variables
 # DRAM bytes per zone-update of one step (k_sig + the three direction
 # kernels) from ncu captures of the 160^3 KH step (dram__bytes_read.sum +
 # dram__bytes_write.sum), scaled to the workload by its zone count
-# (traffic grows in proportion): HLLC 3,442 MB, exact solver 3,466 MB for
+# (traffic grows in proportion): HLLC 3,539 MB, exact solver 3,459 MB for
 # 4.096e6 zones
-TRAFFIC_PER_ZONE = {"mixed": 840.0, "mixed_exact": 846.0, "mixed_learned": 846.0}
+TRAFFIC_PER_ZONE = {"mixed": 864.0, "mixed_exact": 844.0, "mixed_learned": 844.0}
 
 
 def measured_peaks():
