@@ -427,7 +427,7 @@ def regrid(grid, refine, derefine, min_level=1):
         if key[0] < g.max_level:
             g._split(key)
     g._balance()
-    # derefinement, judged on the tree after refinement: candidates are the
+    # derefinement, decided on the tree after refinement: candidates are the
     # parents all of whose children are unrefined marked leaves; a candidate
     # is dropped while a neighbour's child touching it stays refined (is not
     # a candidate itself), until the set no longer changes
