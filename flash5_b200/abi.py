@@ -145,6 +145,8 @@ def _set_sigs(lib):
         "flash_hy_step": (C.c_int, [vp, C.c_double, C.c_double, C.c_double, C.c_int]),
         "flash_hy_step_blocks": (C.c_int, [vp, C.c_int, ip, C.c_double, C.c_double, C.c_double, C.c_int]),
         "flash_hy_compute_dt": (C.c_int, [vp, dp, ip]),
+        "flash_hy_set_mesh_me": (C.c_int, [vp, C.c_int]),
+        "flash_hy_dt_block": (C.c_int, [vp, ip]),
         "flash_hy_sync": (C.c_int, [vp]),
         "flash_hy_stream": (vp, [vp]),
         "flash_hy_last_error": (C.c_int, [vp, C.c_char_p, C.c_int]),

@@ -3,9 +3,8 @@
 //
 // Some hosts of this library cannot call cudaMalloc: a Fortran code whose
 // device memory is owned by another framework's pool allocator (so a second
-// allocator would fragment or overcommit it), a run inside an allocation
-// budget fixed at start-up, or code running while a stream is being captured
-// into a CUDA graph, where allocation calls are not permitted.  For them
+// allocator would fragment or overcommit it), or a run inside an allocation
+// budget fixed at start-up.  For them
 // flash_hy_compute_dt_noalloc computes the same time step as
 // flash_hy_compute_dt (Hydro_computeDt + the MINLOC reduction) from state
 // arrays the caller already owns, without any context and without
@@ -15,13 +14,17 @@
 // block for at most FLASH_HY_NOALLOC_MAX_BLOCKS blocks (1.5 MiB), plus one
 // result slot.  Every GPU that loads this library holds that memory until the
 // process exits.  Host code never uses the symbol itself as a device
-// address: the first call on each device (made current by the caller)
-// resolves the addresses with cudaGetSymbolAddress and caches them, so that
-// first call should come before any stream capture.  Every call overwrites
-// every entry it reads, so nothing has to be cleared between calls, but all
-// calls share the one array: calls that overlap on the GPU (different
-// streams, or threads of the same process) race and must be serialised by
-// the caller.
+// address: the first call in each CUDA context (the device's primary context,
+// or a driver-API context the caller made current) resolves the addresses
+// with cudaGetSymbolAddress and caches them under the context's unique ID
+// (cuCtxGetId), since module globals belong to a context, not to a device
+// number; that first call should come before any stream capture.  The call
+// returns dt on the host, so it synchronises the stream it is given.  Every
+// call overwrites every entry it reads, so nothing has to be cleared between
+// calls, but all calls share the one array: calls that overlap on the GPU
+// (different streams, or threads of the same process) race and must be
+// serialised by the caller.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <float.h>
 #include <mutex>
@@ -41,10 +44,45 @@ struct NoallocResult {
 static __device__ __align__(256) CflPart g_cfl_part[FLASH_HY_NOALLOC_MAX_BLOCKS];
 static __device__ __align__(256) NoallocResult g_cfl_result;
 
-constexpr int kMaxDevices = 64;
+// scratch addresses per CUDA context, keyed by the context's unique ID
+struct ScratchAddr {
+  unsigned long long ctx_id;
+  void *part, *result;
+};
+constexpr int kMaxContexts = 64;
 std::mutex g_mutex;
-void *g_part_addr[kMaxDevices];
-void *g_result_addr[kMaxDevices];
+ScratchAddr g_addr[kMaxContexts];
+int g_naddr = 0, g_next = 0;
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long *);
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+CtxGetIdFn g_ctx_get_id = nullptr;
+
+// unique ID of the calling thread's current CUDA context (binding the
+// current device's primary context first when none is current, as the
+// runtime's first call would); false when the driver cannot tell.  Called
+// with g_mutex held.
+bool current_context_id(unsigned long long *id) {
+  if (!g_ctx_get_current || !g_ctx_get_id) {
+    cudaDriverEntryPointQueryResult q1, q2;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", (void **)&g_ctx_get_current, cudaEnableDefault, &q1) !=
+            cudaSuccess || q1 != cudaDriverEntryPointSuccess ||
+        cudaGetDriverEntryPoint("cuCtxGetId", (void **)&g_ctx_get_id, cudaEnableDefault, &q2) != cudaSuccess ||
+        q2 != cudaDriverEntryPointSuccess) {
+      g_ctx_get_current = nullptr;
+      g_ctx_get_id = nullptr;
+      return false;
+    }
+  }
+  CUcontext ctx = nullptr;
+  if (g_ctx_get_current(&ctx) != CUDA_SUCCESS) return false;
+  if (!ctx) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaSetDevice(dev) != cudaSuccess) return false;
+    if (g_ctx_get_current(&ctx) != CUDA_SUCCESS || !ctx) return false;
+  }
+  return g_ctx_get_id(ctx, id) == CUDA_SUCCESS;
+}
 
 // minimum dt over the per-block results, ties to the lowest block index
 __global__ void k_noalloc_reduce(const CflPart *part, int nblocks, NoallocResult *out) {
@@ -93,21 +131,21 @@ extern "C" int flash_hy_compute_dt_noalloc(const double *d_dens, const double *d
     return FLASH_HY_ERR_BAD_ARG;
   }
   if (!(gamma > 1.0) || !(cfl > 0.0)) return FLASH_HY_ERR_BAD_ARG;
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return FLASH_HY_ERR_CUDA;
-  void *part_addr, *result_addr;
+  void *part_addr = nullptr, *result_addr = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_mutex);
-    if (!g_part_addr[dev]) {
-      // one-time set-up on this device: device addresses of the scratch
-      if (cudaGetSymbolAddress(&g_part_addr[dev], g_cfl_part) != cudaSuccess ||
-          cudaGetSymbolAddress(&g_result_addr[dev], g_cfl_result) != cudaSuccess) {
-        g_part_addr[dev] = g_result_addr[dev] = nullptr;
+    unsigned long long id = 0;
+    if (!current_context_id(&id)) return FLASH_HY_ERR_CUDA;
+    for (int q = 0; q < g_naddr; ++q)
+      if (g_addr[q].ctx_id == id) { part_addr = g_addr[q].part; result_addr = g_addr[q].result; }
+    if (!part_addr) {
+      // one-time set-up in this context: device addresses of the scratch
+      if (cudaGetSymbolAddress(&part_addr, g_cfl_part) != cudaSuccess ||
+          cudaGetSymbolAddress(&result_addr, g_cfl_result) != cudaSuccess)
         return FLASH_HY_ERR_CUDA;
-      }
+      const int slot = g_naddr < kMaxContexts ? g_naddr++ : (g_next++ % kMaxContexts);
+      g_addr[slot] = ScratchAddr{id, part_addr, result_addr};
     }
-    part_addr = g_part_addr[dev];
-    result_addr = g_result_addr[dev];
   }
   StepArgs a;
   memset(&a, 0, sizeof a);

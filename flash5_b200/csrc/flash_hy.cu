@@ -32,6 +32,9 @@ struct flash_hy_ctx {
   void *sig;
   int *d_blk_at, *d_blk_coord, *d_list;
   int list_cap;
+  int *h_list;               // 0-based copy of a caller's 1-based block list
+  int h_list_cap;
+  int mesh_me;               // hy_meshMe: the rank reported in the dt minloc
   CflPart *d_part;
   DtInfo *d_dt, *h_dt;
   unsigned *d_status, *h_status;
@@ -521,6 +524,8 @@ extern "C" int flash_hy_create(const flash_hy_params *params, const flash_hy_gri
       cudaMallocHost((void **)&c->h_status, sizeof(unsigned)) != cudaSuccess) {
     rc = fail(c, FLASH_HY_ERR_CUDA, "cudaMallocHost%s", ""); goto bad;
   }
+  c->h_dt->dt = 0.0;
+  c->h_dt->blk = -1;
   if ((!amr && cudaMemcpy(c->d_blk_at, at.data(), at.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess) ||
       cudaMemcpy(c->d_blk_coord, coords.data(), coords.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemset(c->d_status, 0, sizeof(unsigned)) != cudaSuccess) {
@@ -555,6 +560,7 @@ extern "C" int flash_hy_destroy(flash_hy_ctx *c) {
   ctx_free(c->d_err);
   ctx_free(c->sp_lh); ctx_free(c->sp_gp); ctx_free(c->sp_freg);
   free(c->h_blk_at);
+  free(c->h_list);
   if (c->h_dt) cudaFreeHost(c->h_dt);
   if (c->h_status) cudaFreeHost(c->h_status);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -855,10 +861,21 @@ extern "C" int flash_hy_step(flash_hy_ctx *c, double simTime, double dt, double 
   return 0;
 }
 
-// device copy of a caller's block list (kept in the context)
+// device copy of a caller's block list (kept in the context): FLASH's
+// 1-based block IDs (blockList(1:blockCount)), stored 0-based
 static int upload_list(flash_hy_ctx *c, int n, const int *list) {
-  for (int q = 0; q < n; ++q)
-    if (list[q] < 0 || list[q] >= c->nblocks) return fail(c, FLASH_HY_ERR_BAD_ARG, "block id out of range%s", "");
+  if (n > c->h_list_cap) {
+    int *p = (int *)realloc(c->h_list, (size_t)n * sizeof(int));
+    if (!p) return fail(c, FLASH_HY_ERR_CUDA, "host allocation of the block list%s", "");
+    c->h_list = p;
+    c->h_list_cap = n;
+  }
+  for (int q = 0; q < n; ++q) {
+    if (list[q] < 1 || list[q] > c->nblocks)
+      return fail(c, FLASH_HY_ERR_BAD_ARG, "block ID %s outside 1..nblocks (FLASH's 1-based blockList)",
+                  std::to_string(list[q]).c_str());
+    c->h_list[q] = list[q] - 1;
+  }
   if (n > c->list_cap) {
     cudaStreamSynchronize(c->stream);
     cudaFree(c->d_list);
@@ -867,8 +884,8 @@ static int upload_list(flash_hy_ctx *c, int n, const int *list) {
     c->list_cap = n;
   }
   if (n > 0) {
-    CUDA_OK(c, cudaMemcpyAsync(c->d_list, list, n * sizeof(int), cudaMemcpyHostToDevice, c->stream));
-    CUDA_OK(c, cudaStreamSynchronize(c->stream));   // the list is caller memory
+    CUDA_OK(c, cudaMemcpyAsync(c->d_list, c->h_list, n * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CUDA_OK(c, cudaStreamSynchronize(c->stream));   // h_list is reused by the next call
   }
   return 0;
 }
@@ -955,6 +972,7 @@ extern "C" int flash_hy_update_solution(flash_hy_ctx *c, int blockCount, const i
   return 0;
 }
 
+// blk: 0-based block (the entry points take FLASH's 1-based blockID)
 static int flux_span(flash_hy_ctx *c, int blk, int dir, size_t &off, size_t &nf) {
   if (blk < 0 || blk >= c->nblocks || dir < 1 || dir > c->ndim) return FLASH_HY_ERR_BAD_ARG;
   if (!c->d_fstore) return FLASH_HY_ERR_BAD_ARG;
@@ -969,8 +987,9 @@ static size_t sp_flux_off(const flash_hy_ctx *c, int blk, int dir, size_t nf) {
   return ((size_t)blk * c->ndim + (dir - 1)) * c->nsp * nf;
 }
 
-extern "C" int flash_hy_get_fluxes(flash_hy_ctx *c, int blk, int dir, double *flx) {
+extern "C" int flash_hy_get_fluxes(flash_hy_ctx *c, int blockID, int dir, double *flx) {
   if (!c || !flx) return FLASH_HY_ERR_BAD_ARG;
+  const int blk = blockID - 1;
   size_t off, nf;
   if (flux_span(c, blk, dir, off, nf)) return fail(c, FLASH_HY_ERR_BAD_ARG, "get_fluxes: %s", "bad block/direction");
   CUDA_OK(c, cudaSetDevice(c->device));
@@ -988,8 +1007,9 @@ extern "C" int flash_hy_get_fluxes(flash_hy_ctx *c, int blk, int dir, double *fl
   return 0;
 }
 
-extern "C" int flash_hy_put_fluxes(flash_hy_ctx *c, int blk, int dir, const double *flx) {
+extern "C" int flash_hy_put_fluxes(flash_hy_ctx *c, int blockID, int dir, const double *flx) {
   if (!c || !flx) return FLASH_HY_ERR_BAD_ARG;
+  const int blk = blockID - 1;
   size_t off, nf;
   if (flux_span(c, blk, dir, off, nf)) return fail(c, FLASH_HY_ERR_BAD_ARG, "put_fluxes: %s", "bad block/direction");
   CUDA_OK(c, cudaSetDevice(c->device));
@@ -1073,11 +1093,24 @@ extern "C" int flash_hy_compute_dt(flash_hy_ctx *c, double *dt_out, int minloc_o
   *dt_out = c->h_dt->dt;
   if (minloc_out) {
     minloc_out[0] = c->h_dt->i; minloc_out[1] = c->h_dt->j; minloc_out[2] = c->h_dt->k;
-    minloc_out[3] = c->h_dt->level; minloc_out[4] = c->h_dt->blk;
+    minloc_out[3] = c->h_dt->level; minloc_out[4] = c->mesh_me;
   }
   int st = (int)*c->h_status;
   if (!(c->h_dt->dt > 0.0)) st |= FLASH_HY_ERR_NONPOS_DT;
   return st;
+}
+
+extern "C" int flash_hy_set_mesh_me(flash_hy_ctx *c, int rank) {
+  if (!c || rank < 0) return FLASH_HY_ERR_BAD_ARG;
+  c->mesh_me = rank;
+  return 0;
+}
+
+extern "C" int flash_hy_dt_block(flash_hy_ctx *c, int *blockID) {
+  if (!c || !blockID) return FLASH_HY_ERR_BAD_ARG;
+  // h_dt holds the result of the last flash_hy_compute_dt (synchronised)
+  *blockID = c->h_dt->blk >= 0 ? c->h_dt->blk + 1 : 0;
+  return 0;
 }
 
 // ---------------------------------------------------------------------------

@@ -6,6 +6,9 @@ HydroMain/unsplit/Hydro.F90:6-343) and the FLASH4-style
 ``Hydro(blockCount, blockList, timeEndAdv, dt, dtOld, sweepOrder)``.
 Errors come back as ``HydroError`` with the C-ABI status bits; FLASH aborts
 the run in the same situations (Driver_abortFlash).
+
+Blocks are numbered here as numpy indexes the grid's block axis (0-based);
+the C ABI takes FLASH's 1-based block IDs, and this module converts.
 """
 import ctypes as C
 
@@ -82,13 +85,15 @@ class Hydro:
         self._check(self.lib.flash_hy_step(self.ctx, simTime, dt, dtOld, sweepOrder))
 
     def step_blocks(self, blockList, timeEndAdv, dt, dtOld, sweepOrder=0):
-        bl = np.ascontiguousarray(blockList, dtype=np.int32)
+        """FLASH4's Hydro(blockCount, blockList, ...) on the blocks of
+        blockList (0-based block indices)."""
+        bl = _flash_ids(blockList)
         self._check(self.lib.flash_hy_step_blocks(self.ctx, len(bl), bl.ctypes.data_as(C.POINTER(C.c_int)),
                                                   timeEndAdv, dt, dtOld, sweepOrder))
 
     # -- split step: hy_computeFluxes / hy_updateSolution ------------------
     def compute_fluxes(self, blockList, dt, flags=abi.UPDATE_NONE):
-        bl = np.ascontiguousarray(blockList, dtype=np.int32)
+        bl = _flash_ids(blockList)
         self._check(self.lib.flash_hy_compute_fluxes(self.ctx, len(bl), bl.ctypes.data_as(C.POINTER(C.c_int)), dt,
                                                      flags))
 
@@ -99,7 +104,8 @@ class Hydro:
         nb = self.grid.nb
         nsp = getattr(self.grid, "nspecies", 0) + getattr(self.grid, "nmass_scalars", 0)
         out = np.zeros(((nb[0] + 1) * nb[1] * nb[2], 8 + nsp))
-        self._check(self.lib.flash_hy_get_fluxes(self.ctx, block, dir, out.ctypes.data_as(C.POINTER(C.c_double))))
+        self._check(self.lib.flash_hy_get_fluxes(self.ctx, int(block) + 1, dir,
+                                                 out.ctypes.data_as(C.POINTER(C.c_double))))
         return out
 
     def put_fluxes(self, block, dir, flx):
@@ -108,18 +114,27 @@ class Hydro:
         nsp = getattr(self.grid, "nspecies", 0) + getattr(self.grid, "nmass_scalars", 0)
         if flx.shape != ((nb[0] + 1) * nb[1] * nb[2], 8 + nsp):
             raise ValueError(f"fluxes must have shape [faces, {8 + nsp}], got {flx.shape}")
-        self._check(self.lib.flash_hy_put_fluxes(self.ctx, block, dir, flx.ctypes.data_as(C.POINTER(C.c_double))))
+        self._check(self.lib.flash_hy_put_fluxes(self.ctx, int(block) + 1, dir,
+                                                 flx.ctypes.data_as(C.POINTER(C.c_double))))
 
     def update_solution(self, blockList, dt):
-        bl = np.ascontiguousarray(blockList, dtype=np.int32)
+        bl = _flash_ids(blockList)
         self._check(self.lib.flash_hy_update_solution(self.ctx, len(bl), bl.ctypes.data_as(C.POINTER(C.c_int)), dt))
 
     def compute_dt(self):
-        """Hydro_computeDt + the MINLOC reduction: (dt, (i, j, k, level, block))."""
+        """Hydro_computeDt + the MINLOC reduction: (dt, (i, j, k, level,
+        meshMe, block)) -- FLASH's dtMinLoc, then the 0-based block of the
+        limiting cell (flash_hy_dt_block)."""
         dt = C.c_double()
         loc = (C.c_int * 5)()
         self._check(self.lib.flash_hy_compute_dt(self.ctx, C.byref(dt), loc))
-        return dt.value, tuple(loc)
+        bid = C.c_int()
+        self._check(self.lib.flash_hy_dt_block(self.ctx, C.byref(bid)))
+        return dt.value, tuple(loc) + (bid.value - 1,)
+
+    def set_mesh_me(self, rank):
+        """hy_meshMe: the rank reported in the dt location."""
+        self._check(self.lib.flash_hy_set_mesh_me(self.ctx, int(rank)))
 
     def sync(self):
         self._check(self.lib.flash_hy_sync(self.ctx))
@@ -235,6 +250,11 @@ class Hydro:
     @property
     def last_launch_count(self):
         return self.lib.flash_hy_last_launch_count(self.ctx)
+
+
+def _flash_ids(blocks):
+    """FLASH's 1-based block IDs of 0-based block indices."""
+    return np.ascontiguousarray(np.asarray(blocks, dtype=np.int64) + 1, dtype=np.int32)
 
 
 def _addr(buf):

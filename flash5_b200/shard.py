@@ -155,6 +155,7 @@ class ShardedHydro:
         self.plan = ShardPlan(grid, nranks, rank)
         self.lgrid = self.plan.local_grid()
         self.h = Hydro(params, self.lgrid, device=device)
+        self.h.set_mesh_me(rank)
         self.h.set_owned_blocks(self.plan.owned_local())
         send, recv = self.plan.send_local(), self.plan.recv_local()
         self.h.set_exchange(send, recv)
@@ -210,13 +211,23 @@ class ShardedHydro:
         self.h(simTime, dt, dtOld, sweepOrder)
 
     def compute_dt(self):
-        """(dt, minloc): dt over the owned blocks, MIN over ranks with a
-        process group; minloc is this rank's (local block index)."""
+        """(dt, (i, j, k, level, meshMe, block)): dt over the owned blocks;
+        with a process group, the MPI_MINLOC of Driver_computeDt.F90:376-423
+        -- the minimum over ranks, and the location of the lowest rank that
+        holds it, broadcast from that rank.  block is the global block id."""
         dt, loc = self.h.compute_dt()
+        loc = loc[:5] + (int(self.plan.local[loc[5]]) if loc[5] >= 0 else -1,)
         if self.nranks > 1 and self.dist is not None:
-            t = self.torch.tensor([dt], dtype=self.torch.float64, device=self.torch.device("cuda", self.device))
-            self.dist.all_reduce(t, op=self.dist.ReduceOp.MIN)
-            dt = float(t.item())
+            torch, dist = self.torch, self.dist
+            dev = torch.device("cuda", self.device)
+            t = torch.tensor([dt], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MIN)
+            gdt = float(t.item())
+            w = torch.tensor([self.rank if dt == gdt else self.nranks], dtype=torch.int64, device=dev)
+            dist.all_reduce(w, op=dist.ReduceOp.MIN)
+            lt = torch.tensor(loc, dtype=torch.int64, device=dev)
+            dist.broadcast(lt, src=int(w.item()))
+            dt, loc = gdt, tuple(int(x) for x in lt.tolist())
         return dt, loc
 
     @property

@@ -161,15 +161,19 @@ int flash_hy_download(flash_hy_ctx *ctx, double *unk, int layout, int nunk,
 int flash_hy_step(flash_hy_ctx *ctx, double simTime, double dt, double dtOld,
                   int sweepOrder);
 /* FLASH4-style Hydro(blockCount, blockList, timeEndAdv, dt, dtOld,
- * sweepOrder) / hy_uhd_unsplit: update only the listed blocks (0-based
- * indices into the descriptor's block order).                           */
+ * sweepOrder) / hy_uhd_unsplit: update only the listed blocks.  blockList
+ * holds FLASH's 1-based block IDs (blockList(1:blockCount) as FLASH passes
+ * it, localAPI/hy_biermannSource.F90:9-24): block b of the descriptor is ID
+ * b + 1.  IDs outside 1..nblocks give FLASH_HY_ERR_BAD_ARG.  The same
+ * 1-based IDs are taken by compute_fluxes / update_solution (blockList) and
+ * get_fluxes / put_fluxes (blockID, as Grid_getFluxData).               */
 int flash_hy_step_blocks(flash_hy_ctx *ctx, int blockCount, const int *blockList,
                          double timeEndAdv, double dt, double dtOld, int sweepOrder);
 /* The step split in two, as hy_computeFluxes / hy_updateSolution
  * (localAPI/hy_interface.F90:969,982) and unsplit/Hydro.F90:186-230 use it
  * around a caller's own flux correction (Grid_putFluxData,
  * Grid_conserveFluxes): compute_fluxes computes and keeps the face fluxes
- * of the listed blocks (flags = FLASH_HY_UPDATE_NONE: Uout disassociated,
+ * of the listed blocks (1-based block IDs) (flags = FLASH_HY_UPDATE_NONE: Uout disassociated,
  * the state is unchanged; FLASH_HY_UPDATE_ALL: also updates, as
  * flash_hy_step_blocks); get/put_fluxes read or replace one block's fluxes
  * in one direction (1..ndim) in FLASH's flux-array layout flx(NFLUXES, i,
@@ -180,14 +184,24 @@ int flash_hy_step_blocks(flash_hy_ctx *ctx, int blockCount, const int *blockList
  * replaced) fluxes to the listed blocks, species and mass scalars included
  * (hy_unsplitUpdate.F90:478-491, 827-859).  Uniform grids only.          */
 int flash_hy_compute_fluxes(flash_hy_ctx *ctx, int blockCount, const int *blockList, double dt, int flags);
-int flash_hy_get_fluxes(flash_hy_ctx *ctx, int block, int dir, double *flx);
-int flash_hy_put_fluxes(flash_hy_ctx *ctx, int block, int dir, const double *flx);
+int flash_hy_get_fluxes(flash_hy_ctx *ctx, int blockID, int dir, double *flx);
+int flash_hy_put_fluxes(flash_hy_ctx *ctx, int blockID, int dir, const double *flx);
 int flash_hy_update_solution(flash_hy_ctx *ctx, int blockCount, const int *blockList, double dt);
 
 /* Hydro_computeDt + the MPI_MINLOC reduction of Driver_computeDt.F90:376-377:
  * dt_out = cfl / max_cells max_d (|u_d| + c_s)/dx_d; minloc_out = (i, j, k,
- * level, block) with FLASH's 1-based guard-inclusive cell indices.      */
+ * level, meshMe) as FLASH's dtMinLoc (Hydro_computeDt.F90:266-270): 1-based
+ * guard-inclusive cell indices, the block's refinement level and the rank
+ * set by flash_hy_set_mesh_me (hy_meshMe; 0 by default).  Across ranks the
+ * caller reduces as Driver_computeDt does (MINLOC, then a broadcast from the
+ * winning rank).                                                         */
 int flash_hy_compute_dt(flash_hy_ctx *ctx, double *dt_out, int minloc_out[5]);
+/* The rank this context reports in minloc_out[4] (hy_meshMe, the MPI rank
+ * of the process owning the context's blocks).                           */
+int flash_hy_set_mesh_me(flash_hy_ctx *ctx, int rank);
+/* FLASH's 1-based block ID of the cell that set the last flash_hy_compute_dt
+ * (0 when none did); FLASH's dtMinLoc does not carry it.                 */
+int flash_hy_dt_block(flash_hy_ctx *ctx, int *blockID);
 
 /* Device-side access for callers that keep the state resident. */
 int flash_hy_sync(flash_hy_ctx *ctx);
@@ -322,17 +336,20 @@ int flash_hy_autotune(flash_hy_ctx *ctx, double dt, int steps, flash_hy_tuning *
 /* ---- CFL time step without any device allocation ------------------------
  * No counterpart in the reference: FLASH5's Hydro_computeDt runs on host
  * arrays.  This entry point is for callers that cannot call cudaMalloc
- * (device memory owned by another framework's pool, a fixed allocation
- * budget, or work issued while a stream is being captured into a graph).  It
+ * (device memory owned by another framework's pool, or a fixed allocation
+ * budget set at start-up).  It
  * computes the time step of flash_hy_compute_dt from caller-owned DEVICE
  * arrays (block-major SoA: dens, velx, vely, velz, eint of the interiors,
  * nblocks x nzb x nyb x nxb each, all EOS-consistent) and writes dt and the
  * minloc (i, j, k, level, block) to HOST memory.  Its scratch is a fixed
  * file-scope device array of FLASH_HY_NOALLOC_MAX_BLOCKS entries (1.5 MiB,
  * held by every GPU that loads the library until exit); larger grids are
- * rejected with FLASH_HY_ERR_BAD_ARG.  The first call on a device resolves
- * the scratch address and should precede any stream capture.  All calls
- * share the scratch: calls that overlap on the GPU race.  stream may be NULL. */
+ * rejected with FLASH_HY_ERR_BAD_ARG.  The first call in each CUDA context
+ * (per device, or per driver-API context) resolves the scratch address and
+ * should precede any stream capture.  The result is returned on the host, so
+ * the call synchronises `stream` (NULL: the default stream).  All calls share
+ * the scratch: calls that overlap on the GPU race, and the caller serialises
+ * them.  minloc_out[4] is the 0-based block (the arrays carry no rank).  */
 #define FLASH_HY_NOALLOC_MAX_BLOCKS 65536
 int flash_hy_compute_dt_noalloc(const double *d_dens, const double *d_velx, const double *d_vely,
                                 const double *d_velz, const double *d_eint, int ndim, int nxb, int nyb, int nzb,

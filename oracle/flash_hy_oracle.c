@@ -1098,9 +1098,11 @@ int orc_hydro(const flash_hy_params *p, const flash_hy_grid_desc *g, double *unk
 
 /* Hydro_computeDt.F90:186-290 per block, then the MINLOC reduction of
  * Driver_computeDt.F90:376-377 across blocks (first block wins ties).
- * minloc = (i, j, k, level, block) with 1-based guard-inclusive indices. */
+ * minloc = (i, j, k, level, meshMe) with 1-based guard-inclusive indices and
+ * meshMe = 0 (one rank; temploc(5) = hy_meshMe, Hydro_computeDt.F90:270),
+ * then minloc[5] = the 0-based block of the minimum. */
 int orc_compute_dt(const flash_hy_params *p, const flash_hy_grid_desc *g, const double *unk,
-                   double *dt_out, int minloc[5]) {
+                   double *dt_out, int minloc[6]) {
   int st = check_grid(g);
   if (st) return st;
   ctx_t c; ctx_init(&c, p, g);
@@ -1108,11 +1110,11 @@ int orc_compute_dt(const flash_hy_params *p, const flash_hy_grid_desc *g, const 
   block_deltas(g, del);
   size_t bsz = (size_t)c.nxt * c.nyt * c.nzt * c.nunk;
   double dt_check = DBL_MAX;
-  int best[5] = {0, 0, 0, 0, -1};
+  int best[6] = {0, 0, 0, 0, 0, -1};
   double delxinv = 1.0 / del[0], delyinv = 1.0 / del[1], delzinv = 1.0 / del[2];
   for (int b = 0; b < g->nblocks; ++b) {
     double dt_temp = 0.;
-    int temploc[5] = {0, 0, 0, 0, 0};
+    int temploc[6] = {0, 0, 0, 0, 0, 0};
     double tempCfl = p->cfl, localCfl = p->cfl;
     for (int k = c.k3 ? NGUARD : 0; k < (c.k3 ? NGUARD + c.nzb : 1); ++k)
       for (int j = c.k2 ? NGUARD : 0; j < (c.k2 ? NGUARD + c.nyb : 1); ++j)
@@ -1127,7 +1129,8 @@ int orc_compute_dt(const flash_hy_params *p, const flash_hy_grid_desc *g, const 
             tempCfl = localCfl;
             temploc[0] = i + 1; temploc[1] = j + 1; temploc[2] = k + 1;
             temploc[3] = g->block_level ? g->block_level[b] : 1;
-            temploc[4] = b;
+            temploc[4] = 0;    /* hy_meshMe */
+            temploc[5] = b;
           }
         }
     if (dt_temp != 0.0) dt_temp = tempCfl / dt_temp;
@@ -1501,23 +1504,23 @@ int orc_amr_hydro(const flash_hy_params *p, const flash_hy_grid_desc *g, double 
 }
 
 /* Hydro_computeDt over the leaves with their level's deltas, MINLOC over
- * leaves; minloc = (i, j, k, level, block). */
+ * leaves; minloc = (i, j, k, level, meshMe = 0, block) as orc_compute_dt. */
 int orc_amr_compute_dt(const flash_hy_params *p, const flash_hy_grid_desc *g, const double *unk,
-                       double *dt_out, int minloc[5]) {
+                       double *dt_out, int minloc[6]) {
   amr_t a;
   int st = amr_build(g, &a);
   if (st) return st;
   ctx_t c; ctx_init(&c, p, g);
   size_t bsz = (size_t)c.nxt * c.nyt * c.nzt * c.nunk;
   double dt_check = DBL_MAX;
-  int best[5] = {0, 0, 0, 0, -1};
+  int best[6] = {0, 0, 0, 0, 0, -1};
   for (int b = 0; b < a.n; ++b) {
     if (!a.leaf[b]) continue;
     double del[3];
     level_deltas(g, a.level[b], del);
     double delxinv = 1.0 / del[0], delyinv = 1.0 / del[1], delzinv = 1.0 / del[2];
     double dt_temp = 0.;
-    int temploc[5] = {0, 0, 0, 0, 0};
+    int temploc[6] = {0, 0, 0, 0, 0, 0};
     double tempCfl = p->cfl, localCfl = p->cfl;
     for (int k = c.k3 ? NGUARD : 0; k < (c.k3 ? NGUARD + c.nzb : 1); ++k)
       for (int j = c.k2 ? NGUARD : 0; j < (c.k2 ? NGUARD + c.nyb : 1); ++j)
@@ -1532,7 +1535,8 @@ int orc_amr_compute_dt(const flash_hy_params *p, const flash_hy_grid_desc *g, co
             tempCfl = localCfl;
             temploc[0] = i + 1; temploc[1] = j + 1; temploc[2] = k + 1;
             temploc[3] = a.level[b];
-            temploc[4] = b;
+            temploc[4] = 0;    /* hy_meshMe */
+            temploc[5] = b;
           }
         }
     if (dt_temp != 0.0) dt_temp = tempCfl / dt_temp;

@@ -127,8 +127,10 @@ class Oracle:
         return st, out
 
     def compute_dt(self, unk):
+        """(status, dt, loc): loc = (i, j, k, level, meshMe, block), FLASH's
+        dtMinLoc (meshMe = 0 for one rank) and the 0-based block."""
         dt = C.c_double()
-        loc = (C.c_int * 5)()
+        loc = (C.c_int * 6)()
         f = lib().orc_amr_compute_dt if self.amr else lib().orc_compute_dt
         st = f(C.byref(self.p), C.byref(self.g), _dp(unk), C.byref(dt), loc)
         return st, dt.value, tuple(loc)

@@ -22,7 +22,8 @@ from flash5_b200 import abi, setups
 from flash5_b200.amr import AmrGrid, indicator_refiner
 from flash5_b200.grid import UniformGrid, VAR
 from flash5_b200.hydro import next_dt
-from oracle import orc, sfocu, sod_exact
+from flash5_b200 import metrics as sfocu
+from oracle import orc, sod_exact
 
 
 def ring_hierarchy(ndim=2, nb=8, nblk=4, max_level=3, bc="periodic"):

@@ -15,7 +15,7 @@ from flash5_b200.amr import AmrGrid, indicator_refiner
 from flash5_b200.grid import VAR
 from flash5_b200.hydro import Hydro, next_dt
 from oracle import orc
-from tests.test_gpu_parity import momentum_normalised_l1
+from tests.test_gpu_parity import conserved_l1
 
 VARS = ("dens", "velx", "vely", "velz", "eint", "ener", "pres", "temp", "gamc", "game")
 
@@ -100,7 +100,7 @@ def leaf_l1(grid, out, ref):
     g = G()
     leaves = grid.leaf_ids
     g.interior = lambda u: grid.interior(u)[leaves]
-    return momentum_normalised_l1(out, ref, g)
+    return conserved_l1(out, ref, g)
 
 
 @pytest.mark.gpu

@@ -20,14 +20,14 @@ from flash5_b200 import abi, setups
 from flash5_b200.grid import UniformGrid, VAR
 from flash5_b200.hydro import Hydro, next_dt
 from tests.cases import make_case
-from tests.test_gpu_parity import momentum_normalised_l1, run_pair
+from tests.test_gpu_parity import conserved_l1, run_pair
 
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("case", ["sod2d_rot", "quad2d_16", "sod2d_reflect", "kh3d", "sod3d_rot"])
 def test_exact_fp64_matches_oracle(case):
     grid, ref, out, steps = run_pair(case, riemann_solver=abi.RS_EXACT)
-    for k, l1 in momentum_normalised_l1(out, ref, grid).items():
+    for k, l1 in conserved_l1(out, ref, grid).items():
         assert l1 <= 1e-10, (k, l1)
     for dto, loco, dtg, locg in steps:
         assert abs(dtg - dto) <= 1e-10 * dto
@@ -37,7 +37,7 @@ def test_exact_fp64_matches_oracle(case):
 @pytest.mark.parametrize("case", ["sod2d_rot", "kh2d_16", "quad2d_16", "kh3d", "sod3d_rot"])
 def test_exact_mixed_close(case):
     grid, ref, out, _ = run_pair(case, riemann_solver=abi.RS_EXACT, precision=abi.PREC_MIXED)
-    for k, l1 in momentum_normalised_l1(out, ref, grid).items():
+    for k, l1 in conserved_l1(out, ref, grid).items():
         assert l1 <= 1e-6, (k, l1)
 
 
@@ -96,5 +96,5 @@ def test_learned_guess_hydro_unchanged(ndim):
     got = _run(hl, unk, 4, dt0)
     hl.sync()
     hl.close()
-    for k, l1 in momentum_normalised_l1(got, ref, grid).items():
+    for k, l1 in conserved_l1(got, ref, grid).items():
         assert l1 <= 1e-10, (k, l1)

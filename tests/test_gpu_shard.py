@@ -63,8 +63,15 @@ def test_sharded_contexts_match_single_context(case, nranks, prec):
     ranks = [ShardedHydro(params, grid, nranks, r) for r in range(nranks)]
     for s in ranks:
         s.upload(unk)
-    dt, _ = single.compute_dt()
-    assert min(s.compute_dt()[0] for s in ranks) == dt
+    dt, loc1 = single.compute_dt()
+    got = [s.compute_dt() for s in ranks]
+    assert min(g[0] for g in got) == dt
+    # each rank reports its own meshMe and the global id of its limiting block
+    for r, (dtr, locr) in enumerate(got):
+        assert locr[4] == r and ranks[r].plan.owner[locr[5]] == r
+    best = min(range(nranks), key=lambda r: (got[r][0], r))
+    if sum(g[0] == dt for g in got) == 1:
+        assert got[best][1][:4] == loc1[:4] and got[best][1][5] == loc1[5]
     t, dt_old = 0.0, dt
     for _ in range(3):
         single(t + dt, dt, dt_old)

@@ -16,7 +16,8 @@ import pytest
 from flash5_b200 import abi, setups
 from flash5_b200.grid import UniformGrid, VAR
 from flash5_b200.hydro import next_dt
-from oracle import orc, sod_exact, sfocu
+from flash5_b200 import metrics as sfocu
+from oracle import orc, sod_exact
 
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
 
