@@ -1,6 +1,6 @@
 """Benchmark of the unsplit hydro step (zone-updates/s).
 
-Workload: 3D Kelvin-Helmholtz, 256^3 cells as 32^3 blocks of 8^3 interior
+Workload: 3D Kelvin-Helmholtz, 512^3 cells as 64^3 blocks of 8^3 interior
 cells (FLASH's 4 guard layers are filled inside the kernels), gamma = 5/3,
 periodic boundaries, PPM with characteristic limiting and flattening, CFL
 0.8, the time step recomputed every step (Hydro_computeDt reduction +
@@ -18,14 +18,19 @@ Paths (all replay the dt sequence of the first):
   mixed_learned  as mixed_exact, Newton started from the tensor-core MLP
                  guess trained on this run's harvested face states
 ``value`` is the last path (by default mixed_learned, the metric's
-"batched mixed+learned") with the state resident in HBM; each path's L1
-error is measured against its FP64 reference on the same run.  ``e2e`` is
-the same metric through the C-ABI with host UNK buffers (interior-only
-FLASH UNK, 11 variables, pinned): upload, step, dt, download every step.
+"batched mixed+learned") with the state resident in HBM; each path's error
+is measured on the device against its FP64 reference on the same run.
+``e2e`` is the same metric through the C-ABI with host UNK buffers
+(interior-only FLASH UNK, 11 variables, pinned): upload, step, dt, download
+every step.  The default line also carries the batched AMR workload
+(``amr``: 2D four-quadrant hierarchy of 19,456 leaf blocks) and the
+isolated exact-Riemann workload (``riemann``: 1e8 interface pairs).
 
 ``--impl reference`` times the CPU oracle (the C restatement of the
-reference's Fortran; the Fortran itself cannot be built here) on a bounded
-64^3 sample of the same workload with all host threads.
+reference's Fortran; the Fortran itself cannot be built here) with all host
+threads on a bounded sample of the same workload: a window of 8^3 blocks
+(64^3 zones) of the 512^3 grid with its initial data, advanced with
+FLASH's own method (PPM + HLLC) from guard cells of the surrounding blocks.
 """
 import argparse
 import json
@@ -49,6 +54,20 @@ BYTES_PER_ZONE = 80.0          # read + write of 5 FP64 state variables
 # (traffic grows in proportion): HLLC 3,539 MB, exact solver 3,459 MB for
 # 4.096e6 zones
 TRAFFIC_PER_ZONE = {"mixed": 864.0, "mixed_exact": 844.0, "mixed_learned": 844.0}
+# Floating-point operations per zone-update of one step (k_sig + the three
+# direction kernels), counted by ncu on the 96^3 KH step:
+# smsp__sass_thread_inst_executed_op_{dadd,dmul,dfma,fadd,fmul,ffma}_pred_on
+# (an FMA counts two), divided by the zones; and the FP64 pipe utilisation
+# (sm__pipe_fp64_cycles_active, % of peak over the kernels' active cycles).
+FLOPS_PER_ZONE = {"fp64": {"f64": 7629, "f32": 395, "fp64_pipe_pct": 26.5},
+                  "mixed": {"f64": 1337, "f32": 3374, "fp64_pipe_pct": 9.3},
+                  "mixed_exact": {"f64": 2266, "f32": 3416, "fp64_pipe_pct": 13.8},
+                  "mixed_learned": {"f64": 2266, "f32": 3416, "fp64_pipe_pct": 13.8}}
+# nominal vector peaks of a B200 at the 1965 MHz maximum SM clock: 148 SMs x
+# 64 FP64 (128 FP32) FMA lanes x 2 flops; no measured FP64/FP32 peak exists
+# for this pool, so the compute fractions are "of nominal"
+FP64_PEAK_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12
+FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 
 
 def measured_peaks():
@@ -58,6 +77,22 @@ def measured_peaks():
             d = json.load(f)
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def pin_openmp():
+    """OpenMP settings of the CPU oracle: one thread per host core the
+    process may use, bound to cores (read when the oracle library's OpenMP
+    runtime starts, i.e. before its first parallel region)."""
+    os.environ.setdefault("OMP_NUM_THREADS", str(host_cores()))
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    os.environ.setdefault("OMP_PLACES", "cores")
 
 
 class ClockSampler:
@@ -110,13 +145,30 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def kh_workload(nblk=32, nguard=0, nspecies=0, nmass_scalars=0):
+def kh_workload(nblk=64, nguard=0, nspecies=0, nmass_scalars=0):
     from flash5_b200 import abi, setups
     from flash5_b200.grid import UniformGrid
     g = UniformGrid(3, (8, 8, 8), (nblk, nblk, nblk), bc="periodic", nguard=nguard, nspecies=nspecies,
                     nmass_scalars=nmass_scalars)
     unk = setups.add_species(g, setups.kelvin_helmholtz(g))
     return g, unk, abi
+
+
+def kh_config(args, world=1, riemann="exact (Newton 1e-12)", head="mixed_learned"):
+    """The workload description shared by both arms of the benchmark."""
+    zones = 512 * args.nblk ** 3
+    return {"workload": f"3D Kelvin-Helmholtz {8 * args.nblk}^3 as {args.nblk}^3 blocks of 8^3 (+4 guard "
+                        "filled in-kernel), gamma 5/3, periodic, PPM, CFL 0.8, dt from the CFL reduction "
+                        "every step" + (f", {world} such boxes stacked along z (periodic), blocks sharded "
+                                        "over the ranks in Morton order, ghost blocks exchanged by NCCL "
+                                        "point-to-point every step, NCCL dt min" if world > 1 else ""),
+            "riemann": riemann, "zones_per_gpu": zones,
+            "l2": f"inputs larger than L2 (state {zones * 40 / 1e6:.0f} MB)",
+            **({"species": args.nspecies, "mass_scalars": args.nmass_scalars,
+                "species_note": "dense-layer species pair and passive tracers; species pass in FP64 on the FP64 "
+                                "paths, FP32 face values with FP64 fluxes and update on the mixed paths"}
+               if args.nspecies + args.nmass_scalars else {}),
+            "path": head}
 
 
 def run_device(h, steps, warmup, dts=None, sampler=None, dist=None):
@@ -215,15 +267,69 @@ def run_e2e(h, unk_host, steps, warmup):
     return e0.elapsed_time(e1) / steps
 
 
-def cpu_baseline(seconds=12.0, steps=None, warmup=0):
-    """Oracle (C restatement of the reference) on a 64^3 sample, all threads."""
-    from flash5_b200 import abi, setups
-    from flash5_b200.grid import UniformGrid
+def device_errors(a, b):
+    """Error norms of state a against state b ([5, n] device tensors of
+    dens, velx, vely, velz, eint): per conserved variable (rho, rho u, rho v,
+    rho w, rho E) sfocu's L1 relative norm with each variable's own norm,
+    the magnitude error max|a-b| / max|b|, and the L1 norm with the momentum
+    components normalised by the momentum vector's norm sum |rho v|."""
+    import torch
+
+    def cons(s):
+        r = s[0]
+        ek = 0.5 * (s[1] * s[1] + s[2] * s[2] + s[3] * s[3])
+        return {"dens": r, "xmom": r * s[1], "ymom": r * s[2], "zmom": r * s[3], "ener": r * (s[4] + ek)}
+    ca, cb = cons(a), cons(b)
+    l1, linf, l1v = {}, {}, {}
+    mag = torch.sqrt(cb["xmom"] ** 2 + cb["ymom"] ** 2 + cb["zmom"] ** 2).sum().item()
+    for k in ca:
+        d = (ca[k] - cb[k]).abs()
+        den = cb[k].abs().sum().item()
+        l1[k] = d.sum().item() / den if den > 0 else d.sum().item()
+        mx = cb[k].abs().max().item()
+        linf[k] = d.max().item() / mx if mx > 0 else d.max().item()
+        l1v[k] = l1[k] if k in ("dens", "ener") else d.sum().item() / mag
+    return l1, linf, l1v
+
+
+# ---------------------------------------------------------------------------
+# CPU oracle legs (the checker's C restatement; only these legs run it)
+# ---------------------------------------------------------------------------
+def kh_window(nblk, w=8):
+    """A window of w^3 blocks of the nblk^3-block KH grid (straddling the
+    shear interface at y = 0.25) plus the ring of blocks around it, with the
+    full grid's initial data: (local grid, UNK, owned local indices)."""
+    from flash5_b200 import setups
+    from flash5_b200.shard import LocalGrid
+    lo = (0, max(0, nblk // 4 - w // 2), 0)
+    w = min(w, nblk)
+    own = [(lo[0] + i, lo[1] + j, lo[2] + k) for k in range(w) for j in range(w) for i in range(w)]
+    ring = set()
+    if w < nblk:
+        for (i, j, k) in own:
+            for dk in (-1, 0, 1):
+                for dj in (-1, 0, 1):
+                    for di in (-1, 0, 1):
+                        c = ((i + di) % nblk, (j + dj) % nblk, (k + dk) % nblk)
+                        ring.add(c)
+        ring -= set(own)
+    coords = own + sorted(ring)
+    g = LocalGrid(3, (8, 8, 8), (nblk, nblk, nblk), coords, bc="periodic")
+    unk = setups.kelvin_helmholtz(g)
+    return g, unk, np.arange(len(own), dtype=np.int32)
+
+
+def cpu_sample(nblk, steps=None, warmup=3, seconds=10.0):
+    """The oracle (C restatement of the reference, FLASH's method PPM + HLLC,
+    OpenMP over blocks on all host cores) advancing a 64^3-zone window of the
+    benchmark grid: per-step times after `warmup` steps, either `steps`
+    steps or as many as fit in `seconds`; the median step sets the rate."""
+    pin_openmp()
+    from flash5_b200 import abi
     from flash5_b200.hydro import next_dt
     from oracle import orc
-    g = UniformGrid(3, (8, 8, 8), (8, 8, 8), bc="periodic")
+    g, unk, owned = kh_window(nblk)
     p = abi.default_params(gamma=5.0 / 3.0)
-    unk = setups.kelvin_helmholtz(g)
     o = orc.Oracle(p, g)
     o.eos_init(unk)
     _, dt, _ = o.compute_dt(unk)
@@ -231,24 +337,63 @@ def cpu_baseline(seconds=12.0, steps=None, warmup=0):
 
     def one():
         nonlocal dt, dt_old, t
-        o.hydro(unk, t + dt, dt, dt_old)
+        o.hydro(unk, t + dt, dt, dt_old, blocks=owned)
         _, dcfl, _ = o.compute_dt(unk)
         t += dt
         dt_old, dt = dt, next_dt(dcfl, dt)
 
     for _ in range(warmup):
         one()
-    n = 0
+    times = []
     t0 = time.perf_counter()
-    while (steps is None and (n < 2 or time.perf_counter() - t0 < seconds)) or (steps is not None and n < steps):
+    while (steps is None and (len(times) < 3 or time.perf_counter() - t0 < seconds)) or \
+            (steps is not None and len(times) < steps):
+        s = time.perf_counter()
         one()
-        n += 1
-    el = time.perf_counter() - t0
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
-    return {"value": g.ncells * n / el, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"3D KH 64^3 (512 blocks of 8^3), {n} steps, {el:.1f} s, oracle C port, OpenMP"}
+        times.append(time.perf_counter() - s)
+    zones = len(owned) * 512
+    med = float(np.median(times))
+    return {"value": zones / med, "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": "port",
+            "sample": f"oracle C port (FLASH's PPM + HLLC, FP64), OpenMP on {os.environ['OMP_NUM_THREADS']} "
+                      f"cores bound close: a 64^3-zone window (512 blocks of 8^3, straddling the shear "
+                      f"interface) of the {8 * nblk}^3 grid with its initial data, guard cells from the "
+                      f"surrounding blocks; median of {len(times)} steps after {warmup} warm-up steps "
+                      f"(mean {np.mean(times) * 1e3:.1f} ms, min {np.min(times) * 1e3:.1f} ms, "
+                      f"max {np.max(times) * 1e3:.1f} ms per step)",
+            "ms_per_step_median": med * 1e3}
 
 
+def amr_cpu_baseline(seconds=10.0):
+    """Oracle AMR step on a 16x16-root, 3-level four-quadrant hierarchy
+    (same refinement rule), all host threads."""
+    pin_openmp()
+    from flash5_b200 import abi, setups
+    from flash5_b200.amr import four_quadrant_hierarchy
+    from flash5_b200.hydro import next_dt
+    from oracle import orc
+    g = four_quadrant_hierarchy(nblk=16, max_level=3)
+    p = abi.default_params()
+    unk = setups.four_quadrant(g)
+    o = orc.Oracle(p, g)
+    o.eos_init(unk)
+    _, dt, _ = o.compute_dt(unk)
+    times = []
+    t0 = time.perf_counter()
+    while len(times) < 3 or time.perf_counter() - t0 < seconds:
+        s = time.perf_counter()
+        o.hydro(unk, dt, dt, dt)
+        _, dcfl, _ = o.compute_dt(unk)
+        dt = next_dt(dcfl, dt)
+        times.append(time.perf_counter() - s)
+    med = float(np.median(times))
+    return {"value": g.ncells / med, "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": "port",
+            "sample": f"2D four-quadrant AMR, 16^2 root blocks, 3 levels, {g.nleaves} leaves, median of "
+                      f"{len(times)} steps, oracle C port, OpenMP"}
+
+
+# ---------------------------------------------------------------------------
+# learned guess
+# ---------------------------------------------------------------------------
 def train_guess(g, unk, abi, dev, dts, gamma=5.0 / 3.0):
     """Learned star-pressure guess for the hydro faces: run two steps of the
     mixed exact-solver path with face-state harvesting on (the faces where
@@ -285,23 +430,18 @@ def train_guess(g, unk, abi, dev, dts, gamma=5.0 / 3.0):
                          "solves of the 1e8-pair distribution"}
 
 
-def conserved_l1(a, b, var):
-    from flash5_b200.metrics import conserved_l1 as l1
-    return l1(a, b, var)
-
-
-def conserved_linf(a, b, var):
-    from flash5_b200.metrics import conserved_linf as linf
-    return linf(a, b, var)
-
-
-def riemann_workload(args):
+# ---------------------------------------------------------------------------
+# isolated Riemann workload
+# ---------------------------------------------------------------------------
+def riemann_run(args, n=None, steps=None, warmup=None):
     """Isolated exact Riemann solves (1e8 interface pairs): two-rarefaction
     guess vs the learned guess trained on solver-harvested states."""
     import torch
     from flash5_b200.riemann import ExactRiemann
     torch.cuda.set_device(0)
-    n = args.riemann_n
+    n = n or args.riemann_n
+    steps = steps or args.steps
+    warmup = warmup or args.warmup
     r = ExactRiemann(0)
     stream = r.stream
     # training set harvested from the solver's own solves of another seed
@@ -318,16 +458,16 @@ def riemann_workload(args):
     flg = r.empty(n, dtype=torch.uint8)
     res = {}
     for learned in (False, True):
-        for _ in range(max(1, args.warmup)):
+        for _ in range(max(1, warmup)):
             r.solve(S, learned, out=out, iters=its, flags=flg)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for _ in range(args.steps):
+        for _ in range(steps):
             r.solve(S, learned, out=out, iters=its, flags=flg)
         e1.record(stream)
         e1.synchronize()
-        ms = e0.elapsed_time(e1) / args.steps
+        ms = e0.elapsed_time(e1) / steps
         it = its.cpu().numpy()
         fl = flg.cpu().numpy()
         ok = (fl & 2) == 0
@@ -339,31 +479,37 @@ def riemann_workload(args):
     p0, p1 = res["two_rarefaction"].pop("pstar"), res["learned"].pop("pstar")
     okd = torch.tensor(ok, device=p0.device)
     rel = ((p1 - p0).abs() / p0.clamp_min(1e-300))[okd].max().item()
-    line = {"metric": "exact Riemann star-pressure solves/s (Newton to 1e-12, FP64)", "value": res["learned"]["solves_per_s"],
-            "unit": "solves/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["learned"]["ms"],
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64 Newton, bf16 MLP (f32 acc)",
-            "data": "synthetic (splitmix64 seed 20251203)",
-            "config": {"workload": f"{n:.0e} isolated interface pairs: p ratio log-uniform 1e-4..1e4, rho ratio 1e-3..1e3, "
-                                   "u uniform +-5 c, gamma in {1.4, 5/3}; MLP 8-64-64-1 BF16 on tensor cores (mma.sync)"},
-            "paths": res, "speedup_vs_two_rarefaction": res["two_rarefaction"]["ms"] / res["learned"]["ms"],
-            "max_rel_pstar_diff_learned_vs_tr": rel, "training": {"samples": ns, "epochs": 8, "final_mse": loss,
-                                                                  "seconds": train_s}}
-    print(json.dumps(line))
     r.close()
-    return 0
+    del S, out, its, flg, p0, p1
+    torch.cuda.empty_cache()
+    return {"metric": "exact Riemann star-pressure solves/s (Newton to 1e-12, FP64)",
+            "value": res["learned"]["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "steps": steps,
+            "warmup": warmup, "ms_per_step": res["learned"]["ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 Newton, bf16 MLP (f32 acc)",
+            "data": "synthetic (splitmix64 seed 20251203)",
+            "config": {"workload": f"{n:.0e} isolated interface pairs: p ratio log-uniform 1e-4..1e4, rho ratio "
+                                   "1e-3..1e3, u uniform +-5 c, gamma in {1.4, 5/3}; MLP 8-64-64-1 BF16 on tensor "
+                                   "cores (mma.sync)"},
+            "paths": res, "speedup_vs_two_rarefaction": res["two_rarefaction"]["ms"] / res["learned"]["ms"],
+            "max_rel_pstar_diff_learned_vs_tr": rel,
+            "training": {"samples": ns, "epochs": 8, "final_mse": loss, "seconds": train_s}}
 
 
-def amr_workload(args):
+# ---------------------------------------------------------------------------
+# batched AMR workload
+# ---------------------------------------------------------------------------
+def amr_run(args, paths, e2e=True, regrid=True, cpu=True, steps=None, warmup=None):
     """Batched AMR hierarchy, 2D four-quadrant Riemann problem: 4 levels,
-    about 19.5k leaf blocks of 16^2 refined where a seeded smoothed density
+    19,456 leaf blocks of 16^2 refined where a seeded smoothed density
     gradient is large; every level advanced in one graph-replayed step with
-    one dt, fine/coarse flux correction on.  FP64 and mixed precision."""
+    one dt, fine/coarse flux correction on.  Returns the JSON line."""
     import torch
     from flash5_b200 import abi, setups
     from flash5_b200.amr import four_quadrant_hierarchy
-    from flash5_b200.grid import VAR
     from flash5_b200.hydro import Hydro
     torch.cuda.set_device(0)
+    steps = steps or args.steps
+    warmup = warmup or args.warmup
     t0 = time.perf_counter()
     g = four_quadrant_hierarchy(nblk=args.amr_nblk)
     unk = setups.four_quadrant(g)
@@ -373,14 +519,16 @@ def amr_workload(args):
     ms, outs, dts, launches, clocks, e2e_ms, hb = {}, {}, None, {}, None, None, None
     tunings = {}
     regrid_info = None
-    paths = [p for p in args.paths.split(",") if p in ("fp64", "fp64_exact", "mixed", "mixed_exact", "mixed_learned")]
-    paths = paths or ["fp64", "mixed"]
     # (precision, Riemann solver, the FP64 path the errors are measured against, learned guess)
     spec = {"fp64": (abi.PREC_FP64, abi.RS_HLLC, None, 0), "fp64_exact": (abi.PREC_FP64, abi.RS_EXACT, None, 0),
             "mixed": (abi.PREC_MIXED, abi.RS_HLLC, "fp64", 0),
             "mixed_exact": (abi.PREC_MIXED, abi.RS_EXACT, "fp64_exact", 0),
             "mixed_learned": (abi.PREC_MIXED, abi.RS_EXACT, "fp64_exact", 1)}
+    paths = [p for p in paths if p in spec] or ["fp64", "mixed"]
     training = None
+    leaves = torch.tensor(g.leaf_ids, dtype=torch.long, device="cuda")
+    ncb = 16 * 16
+    lidx = (leaves[:, None] * ncb + torch.arange(ncb, device="cuda")[None, :]).reshape(-1)
     for name in paths:
         pr, rsv, _, learned = spec[name]
         h = Hydro(abi.default_params(precision=pr, riemann_solver=rsv, learned_guess=learned), g)
@@ -395,29 +543,28 @@ def amr_workload(args):
                              "trial_key": "sig_threads/dir_threads/mx_threads"}
         headline = name == paths[-1]
         sampler = ClockSampler(0) if headline else None
-        ms[name], used, launches[name] = run_device(h, args.steps, args.warmup, dts=dts, sampler=sampler)
+        ms[name], used, launches[name] = run_device(h, steps, warmup, dts=dts, sampler=sampler)
         if dts is None:
             dts = used
         if headline:
             clocks = sampler.summary()
-        outs[name] = np.empty_like(unk)
-        h.download(outs[name])
-        if headline and not args.no_e2e:
+        outs[name] = h.export_state(torch)[:, lidx]
+        if headline and e2e:
             pinned = torch.empty(unk.shape, dtype=torch.float64, pin_memory=True)
             host = pinned.numpy()
             host[...] = unk
-            e2e_ms = run_e2e(h, host, max(3, min(args.steps, 8)), 3)
+            e2e_ms = run_e2e(h, host, max(3, min(steps, 8)), 3)
             hb = host.nbytes
-        if headline and not args.no_regrid:
+        if headline and regrid:
             # one refinement cycle on the stepped state: the estimator of
             # dens and pres on every node (device), marks and new tree
             # (host), data of the new tree (device)
             from flash5_b200.amr import update_refinement
             est = []
             for _ in range(3):
-                t0 = time.perf_counter()
+                t1 = time.perf_counter()
                 h.estimate_error("pres", 0.01)
-                est.append(time.perf_counter() - t0)
+                est.append(time.perf_counter() - t1)
             tm = {}
             h, g_new = update_refinement(h, g, ("dens", "pres"), 0.8, 0.2, 0.01, timings=tm)
             regrid_info = {"estimate_one_var_ms": 1e3 * min(est), "nodes": g.nblocks,
@@ -428,16 +575,15 @@ def amr_workload(args):
                            "cutoffs": {"refine": 0.8, "derefine": 0.2, "filter": 0.01}}
         h.close()
     head = paths[-1]
-    leaves = g.leaf_ids
     ref_of = {n: spec[n][2] for n in outs if spec[n][2] in outs}
-    errs = {n: conserved_l1(outs[n][leaves], outs[r][leaves], VAR) for n, r in ref_of.items()}
-    errs_inf = {n: conserved_linf(outs[n][leaves], outs[r][leaves], VAR) for n, r in ref_of.items()}
-    cpu = None if args.no_cpu else amr_cpu_baseline()
+    errs = {n: device_errors(outs[n], outs[r]) for n, r in ref_of.items()}
+    outs.clear()
+    cpu_r = amr_cpu_baseline() if cpu else None
     achieved = zones * BYTES_PER_ZONE / (ms[head] * 1e-3) / 1e9
     levels = np.bincount(g.levels[g.is_leaf], minlength=g.max_level + 1)[1:].tolist()
     line = {
-        "metric": METRIC, "value": zones / (ms[head] * 1e-3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms[head], "higher_is_better": True, "scaling": "weak",
+        "metric": METRIC, "value": zones / (ms[head] * 1e-3), "unit": UNIT, "n_gpus": 1, "steps": steps,
+        "warmup": warmup, "ms_per_step": ms[head], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None,
         "dtype": ("f32 reconstruction, f64 Riemann/update" + (", bf16 MLP guess" if head == "mixed_learned" else ""))
                  if head.startswith("mixed") else "f64",
@@ -451,14 +597,14 @@ def amr_workload(args):
                    "zones_per_gpu": zones, "leaf_blocks": g.nleaves,
                    "l2": f"inputs larger than L2 (state {g.nblocks * 256 * 40 / 1e6:.0f} MB plus guard buffers "
                          f"{g.nleaves * 576 * 40 / 1e6:.0f} MB)", "path": head, "hierarchy_build_s": build_s},
-        "paths": {n: {"value": zones / (ms[n] * 1e-3), "ms_per_step": ms[n],
-                      **({f"rel_l1_vs_{ref_of[n]}": errs[n], f"rel_linf_vs_{ref_of[n]}": errs_inf[n]}
-                         if n in errs else {}),
+        "paths": {n: {"value": zones / (ms[n] * 1e-3), "ms_per_step": ms[n], "launches_per_step": launches[n],
+                      **({f"rel_l1_vs_{ref_of[n]}": errs[n][0], f"rel_linf_vs_{ref_of[n]}": errs[n][1],
+                          f"rel_l1_momentum_vector_vs_{ref_of[n]}": errs[n][2]} if n in errs else {}),
                       **({"launch_shape": tunings[n]} if n in tunings else {})} for n in ms},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": None, "peak_kind": peak_kind,
                      "kernel": "one AMR step (restriction, halos, k_sig, per-level k_dir), 80 B/leaf zone algorithmic"},
-        "clocks": clocks, "gpu_launches": launches[head] * args.steps,
+        "clocks": clocks, "gpu_launches": launches[head] * steps,
     }
     if "fp64" in ms and head != "fp64":
         line["speedup_vs_fp64"] = ms["fp64"] / ms[head]
@@ -467,51 +613,56 @@ def amr_workload(args):
                        "d2h_bytes_per_step": hb, "ms_per_step": e2e_ms,
                        "path": "flash_hy_upload + flash_hy_step + flash_hy_compute_dt + flash_hy_download, "
                                "every node's FLASH UNK (11 vars), pinned host memory"}
-    if cpu is not None:
-        line["cpu_baseline"] = cpu
+    if cpu_r is not None:
+        line["cpu_baseline"] = cpu_r
     if regrid_info is not None:
         line["refinement_cycle"] = regrid_info
     if training is not None:
         line["training"] = training
-    print(json.dumps(line))
-    return 0
+    torch.cuda.empty_cache()
+    return line
 
 
-def amr_cpu_baseline(seconds=10.0):
-    """Oracle AMR step on a 16x16-root, 3-level four-quadrant hierarchy
-    (same refinement rule), all host threads."""
-    from flash5_b200 import abi, setups
-    from flash5_b200.amr import four_quadrant_hierarchy
-    from flash5_b200.hydro import next_dt
-    from oracle import orc
-    g = four_quadrant_hierarchy(nblk=16, max_level=3)
-    p = abi.default_params()
-    unk = setups.four_quadrant(g)
-    o = orc.Oracle(p, g)
-    o.eos_init(unk)
-    _, dt, _ = o.compute_dt(unk)
-    n, t0 = 0, time.perf_counter()
-    while n < 2 or time.perf_counter() - t0 < seconds:
-        o.hydro(unk, dt, dt, dt)
-        _, dcfl, _ = o.compute_dt(unk)
-        dt = next_dt(dcfl, dt)
-        n += 1
-    el = time.perf_counter() - t0
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
-    return {"value": g.ncells * n / el, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"2D four-quadrant AMR, 16^2 root blocks, 3 levels, {g.nleaves} leaves, {n} steps, "
-                      f"{el:.1f} s, oracle C port, OpenMP"}
+def amr_summary(line):
+    p = line["paths"]
+    out = {"workload": line["config"]["workload"], "zones": line["config"]["zones_per_gpu"],
+           "path": line["config"]["path"], "value": line["value"], "unit": UNIT,
+           "ms_per_step": {n: round(v["ms_per_step"], 4) for n, v in p.items()},
+           "launches_per_step": {n: v["launches_per_step"] for n, v in p.items()},
+           "errors": {n: {k: v[k] for k in v if k.startswith("rel_")} for n, v in p.items()
+                      if any(k.startswith("rel_") for k in v)}}
+    if "fp64" in p:
+        out["speedup_vs_fp64"] = {n: p["fp64"]["ms_per_step"] / v["ms_per_step"] for n, v in p.items()}
+    if "fp64_exact" in p:
+        out["speedup_vs_fp64_exact"] = {n: p["fp64_exact"]["ms_per_step"] / v["ms_per_step"] for n, v in p.items()}
+    if "training" in line:
+        out["training_hydro_face_states"] = line["training"]["hydro_face_states"]
+    return out
 
 
+def riemann_summary(line):
+    p = line["paths"]
+    return {"workload": line["config"]["workload"], "unit": "solves/s",
+            "solves_per_s": {n: v["solves_per_s"] for n, v in p.items()},
+            "mean_newton_evaluations": {n: v["mean_iters"] for n, v in p.items()},
+            "fallback_frac_learned": p["learned"]["fallback_frac"],
+            "speedup_learned_vs_two_rarefaction": line["speedup_vs_two_rarefaction"],
+            "max_rel_pstar_diff_learned_vs_tr": line["max_rel_pstar_diff_learned_vs_tr"]}
+
+
+# ---------------------------------------------------------------------------
+# main
+# ---------------------------------------------------------------------------
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--nblk", type=int, default=32, help="blocks per axis (32 -> 256^3)")
+    ap.add_argument("--nblk", type=int, default=64, help="blocks per axis (64 -> 512^3)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="KH workload: skip the AMR and isolated-Riemann keys")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes (no autotuning)")
     ap.add_argument("--no-regrid", action="store_true", help="AMR workload: skip the refinement-cycle timing")
     ap.add_argument("--nspecies", type=int, default=0, help="KH workload: species advected with the flow")
@@ -527,28 +678,27 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     warmup = max(3, args.warmup)
+    args.warmup = warmup
     if args.workload == "amr" and args.impl == "ours":
         if rank != 0:
             return 0
-        args.warmup = warmup
-        return amr_workload(args)
+        print(json.dumps(amr_run(args, paths, e2e=not args.no_e2e, regrid=not args.no_regrid,
+                                 cpu=not args.no_cpu)))
+        return 0
     if args.workload == "riemann" and args.impl == "ours":
         if rank != 0:
             return 0
-        args.warmup = warmup
-        return riemann_workload(args)
+        print(json.dumps(riemann_run(args)))
+        return 0
 
     if args.impl == "reference":
         if rank != 0:
             return 0
-        r = cpu_baseline(steps=args.steps, warmup=warmup)
-        ms = 1000.0 / (r["value"] / (64 ** 3))
+        r = cpu_sample(args.nblk, steps=args.steps, warmup=warmup)
         line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-                "warmup": warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": "3D Kelvin-Helmholtz 64^3 sample (512 blocks of 8^3), periodic, PPM+HLLC, CFL 0.8",
-                           "l2": "CPU"},
-                "impl": "reference", "cpu_baseline": r,
+                "warmup": warmup, "ms_per_step": r["ms_per_step_median"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded KH noise)",
+                "config": kh_config(args, world=args.gpus), "impl": "reference", "cpu_baseline": r,
                 "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return 0
@@ -566,7 +716,6 @@ def main():
     dev = local if world > 1 else 0
 
     from flash5_b200.hydro import Hydro
-    from flash5_b200.grid import VAR
     g, unk, abi = kh_workload(args.nblk, nguard=0, nspecies=args.nspecies, nmass_scalars=args.nmass_scalars)
     zones = g.ncells
     peak, peak_kind = measured_peaks()
@@ -625,29 +774,21 @@ def main():
             dts = used            # later paths replay the first path's dt sequence
         if headline:
             clocks = sampler.summary()
-        if world > 1:
-            outs[name] = h.download_owned()[0]
-        else:
-            outs[name] = np.empty_like(unk)
-            h.download(outs[name])
+        hh = h.h if world > 1 else h
+        st = hh.export_state(torch)
+        outs[name] = st[:, :len(plan.owned) * 512] if world > 1 else st
         if headline and not args.no_e2e and world == 1:
             pinned = torch.empty(unk.shape, dtype=torch.float64, pin_memory=True)
             host = pinned.numpy()
             host[...] = unk
             e2e_ms = run_e2e(h, host, max(3, min(args.steps, 8)), 3)
             hb = host.nbytes
+            del host, pinned
         h.close()
     head = paths[-1]
-    errs = {n: conserved_l1(outs[n], outs[spec[n][3]], VAR) for n in outs if spec[n][3] in outs}
-    errs_inf = {n: conserved_linf(outs[n], outs[spec[n][3]], VAR) for n in errs}
-    if g.nspecies + g.nmass_scalars:
-        from flash5_b200.metrics import l1_rel, mag_err
-        for n in errs:
-            a, b = outs[n], outs[spec[n][3]]
-            for q in range(g.nspecies + g.nmass_scalars):
-                k = g.species.start + q
-                errs[n][f"rho_x{q}"] = l1_rel(a[..., 0] * a[..., k], b[..., 0] * b[..., k])
-                errs_inf[n][f"rho_x{q}"] = mag_err(a[..., 0] * a[..., k], b[..., 0] * b[..., k])
+    errs = {n: device_errors(outs[n], outs[spec[n][3]]) for n in outs if spec[n][3] in outs}
+    outs.clear()
+    torch.cuda.empty_cache()
     if dist is not None:
         for n in ms:
             ms[n] = dist_max(dist, ms[n])
@@ -656,7 +797,12 @@ def main():
     total = gg.ncells if world > 1 else zones
     value = total / (ms[head] * 1e-3)
     if rank == 0:
-        cpu = None if (args.no_cpu or world > 1) else cpu_baseline()
+        extra = {}
+        if world == 1 and not args.no_extra:
+            extra["amr"] = amr_summary(amr_run(args, ["fp64", "fp64_exact", "mixed", "mixed_exact", "mixed_learned"],
+                                               e2e=False, regrid=False, cpu=False))
+            extra["riemann"] = riemann_summary(riemann_run(args))
+        cpu = None if (args.no_cpu or world > 1) else cpu_sample(args.nblk)
         achieved = zones * BYTES_PER_ZONE / (ms[head] * 1e-3) / 1e9
         notes = {"fp64": "plain FP64 HLLC, no FMA contraction; bit-identical to the CPU oracle in the tests",
                  "fp64_fma": "FP64 HLLC with FMA contraction",
@@ -666,35 +812,41 @@ def main():
                  "mixed_exact": "FP32 reconstruction, FP64 exact Riemann (two-rarefaction start) and update",
                  "mixed_learned": "FP32 reconstruction, FP64 exact Riemann started from the BF16 tensor-core MLP "
                                   "guess (trained on this run's harvested face states), FP64 update"}
+        fl = FLOPS_PER_ZONE.get(head)
+        compute = None
+        if fl is not None:
+            zps = zones / (ms[head] * 1e-3)
+            compute = {"flops_per_zone": {"f64": fl["f64"], "f32": fl["f32"]},
+                       "f64_tflops": zps * fl["f64"] / 1e12, "f32_tflops": zps * fl["f32"] / 1e12,
+                       "f64_peak_tflops": FP64_PEAK_TFLOPS, "f32_peak_tflops": FP32_PEAK_TFLOPS,
+                       "f64_frac": zps * fl["f64"] / 1e12 / FP64_PEAK_TFLOPS,
+                       "f32_frac": zps * fl["f32"] / 1e12 / FP32_PEAK_TFLOPS, "peak_kind": "nominal",
+                       "fp64_pipe_pct_ncu": fl["fp64_pipe_pct"],
+                       "note": "FLOPs per zone-update counted by ncu (SASS dadd/dmul/dfma, fadd/fmul/ffma; FMA = "
+                               "2) on the 96^3 step; peaks = 148 SMs x 64 FP64 / 128 FP32 FMA lanes x 2 x "
+                               "1965 MHz"}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": warmup,
             "ms_per_step": ms[head], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 reconstruction, f64 Riemann/update" + (", bf16 MLP guess" if head == "mixed_learned" else "")
                      if head.startswith("mixed") else "f64",
             "data": "synthetic (seeded KH noise)",
-            "config": {"workload": f"3D Kelvin-Helmholtz {8 * args.nblk}^3 as {args.nblk}^3 blocks of 8^3 (+4 guard "
-                                   "filled in-kernel), gamma 5/3, periodic, PPM, CFL 0.8, dt from the CFL reduction "
-                                   "every step" + (f", {world} such boxes stacked along z (periodic), blocks sharded "
-                                                   "over the ranks in Morton order, ghost blocks exchanged by NCCL "
-                                                   "point-to-point every step, NCCL dt min" if world > 1 else ""),
-                       "riemann": "exact (Newton 1e-12)" if spec[head][1] == abi.RS_EXACT else "HLLC",
-                       "zones_per_gpu": zones, "l2": f"inputs larger than L2 (state {zones * 40 / 1e6:.0f} MB)",
-                       **({"species": args.nspecies, "mass_scalars": args.nmass_scalars,
-                           "species_note": "dense-layer species pair and passive tracers; species pass in FP64 on the FP64 "
-                                           "paths, FP32 face values with FP64 fluxes and update on the mixed paths"}
-                          if args.nspecies + args.nmass_scalars else {}),
-                       "path": head},
+            "config": kh_config(args, world=world,
+                                riemann="exact (Newton 1e-12)" if spec[head][1] == abi.RS_EXACT else "HLLC",
+                                head=head),
             "paths": {n: {"value": total / (ms[n] * 1e-3), "ms_per_step": ms[n], "note": notes[n],
-                          **({f"rel_l1_vs_{spec[n][3]}": errs[n], f"rel_linf_vs_{spec[n][3]}": errs_inf[n]}
-                             if n in errs else {}),
+                          **({f"rel_l1_vs_{spec[n][3]}": errs[n][0], f"rel_linf_vs_{spec[n][3]}": errs[n][1],
+                              f"rel_l1_momentum_vector_vs_{spec[n][3]}": errs[n][2]} if n in errs else {}),
                           **({"launch_shape": tunings[n]} if n in tunings else {})} for n in ms},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": TRAFFIC_PER_ZONE[head] * zones if head in TRAFFIC_PER_ZONE else None,
                          "traffic_note": "DRAM bytes per step (per GPU), ncu at 160^3 scaled by zones",
                          "peak_kind": peak_kind,
-                         "kernel": "one hydro step (k_sig + k_dir x,y,z), 80 B/zone algorithmic"},
+                         "kernel": "one hydro step (k_sig + k_dir x,y,z), 80 B/zone algorithmic",
+                         **({"compute": compute} if compute else {})},
             "clocks": clocks,
             "gpu_launches": launches[head] * args.steps,
+            **extra,
         }
         if training is not None:
             line["training"] = training

@@ -149,6 +149,7 @@ def _set_sigs(lib):
         "flash_hy_dt_block": (C.c_int, [vp, ip]),
         "flash_hy_sync": (C.c_int, [vp]),
         "flash_hy_stream": (vp, [vp]),
+        "flash_hy_export_state": (C.c_int, [vp, vp]),
         "flash_hy_last_error": (C.c_int, [vp, C.c_char_p, C.c_int]),
         "flash_hy_last_launch_count": (C.c_int, [vp]),
         "flash_hy_set_guess_weights": (C.c_int, [vp, C.POINTER(C.c_float), C.c_int]),

@@ -1390,6 +1390,15 @@ extern "C" int flash_hy_sync(flash_hy_ctx *c) {
 
 extern "C" void *flash_hy_stream(flash_hy_ctx *c) { return c ? (void *)c->stream : nullptr; }
 
+extern "C" int flash_hy_export_state(flash_hy_ctx *c, double *d_out) {
+  if (!c || !d_out) return FLASH_HY_ERR_BAD_ARG;
+  CUDA_OK(c, cudaSetDevice(c->device));
+  for (int v = 0; v < 5; ++v)
+    CUDA_OK(c, cudaMemcpyAsync(d_out + (size_t)v * c->ncells, c->state[c->cur][v], c->ncells * sizeof(double),
+                               cudaMemcpyDeviceToDevice, c->stream));
+  return 0;
+}
+
 extern "C" int flash_hy_last_error(flash_hy_ctx *c, char *buf, int len) {
   if (!c || !buf || len <= 0) return FLASH_HY_ERR_BAD_ARG;
   snprintf(buf, len, "%s", c->err);

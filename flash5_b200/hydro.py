@@ -139,6 +139,17 @@ class Hydro:
     def sync(self):
         self._check(self.lib.flash_hy_sync(self.ctx))
 
+    def export_state(self, torch):
+        """The device state as a [5, ncells] float64 CUDA tensor (dens, velx,
+        vely, velz, eint; blocks in descriptor order, each block's interior
+        x fastest), copied on the context's stream and synchronised."""
+        n = self.grid.nblocks * self.grid.nb[0] * self.grid.nb[1] * self.grid.nb[2]
+        out = torch.empty((5, n), dtype=torch.float64, device=torch.device("cuda", self.device))
+        torch.cuda.current_stream(out.device).synchronize()
+        self._check(self.lib.flash_hy_export_state(self.ctx, C.c_void_p(out.data_ptr())))
+        self.sync()
+        return out
+
     # -- refinement ---------------------------------------------------------
     def estimate_error(self, var="dens", refine_filter=0.01):
         """gr_estimateError: Lohner's estimator of `var` for every block

@@ -206,6 +206,11 @@ int flash_hy_dt_block(flash_hy_ctx *ctx, int *blockID);
 /* Device-side access for callers that keep the state resident. */
 int flash_hy_sync(flash_hy_ctx *ctx);
 void *flash_hy_stream(flash_hy_ctx *ctx);        /* cudaStream_t of the context */
+/* Enqueue (on the context's stream) a copy of the device state into the
+ * caller's DEVICE buffer d_out: [5][nblocks * nzb * nyb * nxb] doubles --
+ * dens, velx, vely, velz, eint of every block's interior, block-major.
+ * No FLASH counterpart (FLASH's state lives in host UNK). */
+int flash_hy_export_state(flash_hy_ctx *ctx, double *d_out);
 int flash_hy_last_error(flash_hy_ctx *ctx, char *buf, int len);
 /* Number of kernel launches issued by the last flash_hy_step call. */
 int flash_hy_last_launch_count(flash_hy_ctx *ctx);

@@ -27,6 +27,7 @@
  * FLASH unk(var,i,j,k,blk) ordering with NGUARD guard layers, variables in
  * FLASH's alphabetical order for +uhd with the gamma EOS (bin/unitCfg.py:713).
  */
+#include <malloc.h>
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -363,6 +364,19 @@ typedef struct {
   double *spc_sig;                        /* [cells][3][nsp]                */
   double *spc_flux[3];                    /* [cells][nsp]                   */
 } work_t;
+
+/* The per-block scratch above (hy_computeFluxes.F90:213-244 allocates the
+ * same per block) is a few MB per block.  Served from fresh mmap pages, its
+ * page faults cost about as much kernel time as the block's arithmetic, and
+ * whether glibc maps or reuses depends on the process's earlier allocations
+ * (its dynamic mmap threshold), so the timed CPU baseline varied 2x from one
+ * process to the next.  The oracle library therefore fixes the thresholds
+ * when it is loaded: scratch comes from the (per-thread) heaps and stays
+ * mapped. */
+__attribute__((constructor)) static void orc_malloc_setup(void) {
+  mallopt(M_MMAP_THRESHOLD, 256 << 20);
+  mallopt(M_TRIM_THRESHOLD, 1 << 30);
+}
 
 static void work_alloc(const ctx_t *c, work_t *w) {
   size_t nc = (size_t)c->nxt * c->nyt * c->nzt;
