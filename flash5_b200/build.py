@@ -19,17 +19,22 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
                  "-ccbin", "g++"]
 
+# The FP32 arithmetic of the mixed units (reconstruction, species face
+# values, the learned guess): approximate FP32 division and square root,
+# FP32 denormals flushed.  FP64 arithmetic is unaffected by these flags.
+FP32_FAST = ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"]
+
 UNITS = [
     ("hy_fp64_exact.o", "hy_variant.cu", ["-DFHY_VARIANT=1", "--fmad=false"]),
     ("hy_fp64_fma.o", "hy_variant.cu", ["-DFHY_VARIANT=2", "--fmad=true"]),
-    ("hy_mixed0.o", "hy_variant.cu", ["-DFHY_VARIANT=3", "-DFHY_MXSEL=0", "--fmad=true"]),
-    ("hy_mixed1.o", "hy_variant.cu", ["-DFHY_VARIANT=3", "-DFHY_MXSEL=1", "--fmad=true"]),
-    ("hy_mixed2.o", "hy_variant.cu", ["-DFHY_VARIANT=3", "-DFHY_MXSEL=2", "--fmad=true"]),
+    ("hy_mixed0.o", "hy_variant.cu", ["-DFHY_VARIANT=3", "-DFHY_MXSEL=0", "--fmad=true"] + FP32_FAST),
+    ("hy_mixed1.o", "hy_variant.cu", ["-DFHY_VARIANT=3", "-DFHY_MXSEL=1", "--fmad=true"] + FP32_FAST),
+    ("hy_mixed2.o", "hy_variant.cu", ["-DFHY_VARIANT=3", "-DFHY_MXSEL=2", "--fmad=true"] + FP32_FAST),
     ("flash_hy.o", "flash_hy.cu", ["--fmad=false"]),
-    ("riemann_exact.o", "riemann_exact.cu", ["--fmad=true"]),
+    ("riemann_exact.o", "riemann_exact.cu", ["--fmad=true"] + FP32_FAST),
     ("cfl_noalloc.o", "cfl_noalloc.cu", ["--fmad=false"]),
     ("spec.o", "spec.cu", ["--fmad=false"]),
-    ("spec_mx.o", "spec.cu", ["-DFHY_SPEC_MIXED", "--fmad=true"]),
+    ("spec_mx.o", "spec.cu", ["-DFHY_SPEC_MIXED", "--fmad=true"] + FP32_FAST),
     ("refine.o", "refine.cu", ["--fmad=false"]),
     ("tree.o", "tree.cu", []),
 ]
@@ -52,8 +57,12 @@ def build(verbose=False, ptxas_info=False, force=False):
         o = os.path.join(BUILD, obj)
         s = os.path.join(CSRC, src)
         objs.append(o)
-        if force or _stale(o, [s] + headers):
-            cmd = [NVCC] + COMMON + flags + (["-Xptxas", "-v"] if ptxas_info else []) + ["-c", s, "-o", o]
+        cmd = [NVCC] + COMMON + flags + (["-Xptxas", "-v"] if ptxas_info else []) + ["-c", s, "-o", o]
+        stamp = o + ".cmd"
+        same = os.path.exists(stamp) and open(stamp).read() == " ".join(cmd)
+        if force or not same or _stale(o, [s] + headers):
+            with open(stamp, "w") as f:
+                f.write(" ".join(cmd))
             if verbose:
                 print(" ".join(cmd), file=sys.stderr)
             procs.append((cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))

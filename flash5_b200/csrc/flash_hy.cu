@@ -35,6 +35,7 @@ struct flash_hy_ctx {
   int *h_list;               // 0-based copy of a caller's 1-based block list
   int h_list_cap;
   int mesh_me;               // hy_meshMe: the rank reported in the dt minloc
+  fhy::TmaLine *tma_maps;    // [2 state buffers][3 directions]: TMA staging of k_dir_mx, or NULL
   CflPart *d_part;
   DtInfo *d_dt, *h_dt;
   unsigned *d_status, *h_status;
@@ -185,6 +186,55 @@ extern "C" int flash_hy_release_memory(int device) {
   std::lock_guard<std::mutex> lk(g_mem_mu);
   release_cached_locked(device);
   return 0;
+}
+
+// Tensor maps of the mixed direction kernels' TMA staging (uniform 3D
+// grids of 8^3 blocks): for both state buffers, each variable and each
+// sweep direction, the interior box and the slab box along the direction,
+// over the block store's natural layout (dims 8, 8, 8 * nblocks; FP64).
+// cuTensorMapEncodeTiled comes from the driver through the runtime, so the
+// library needs no link-time dependency on libcuda.  Returns NULL when the
+// driver offers no encoder (the kernels then stage through load_prim).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static fhy::TmaLine *make_tma_maps(flash_hy_ctx *c) {
+  if (c->ndim != 3 || c->nx != 8 || c->ny != 8 || c->nz != 8) return nullptr;
+  static EncodeTiledFn encode = nullptr;
+  if (!encode) {
+    cudaDriverEntryPointQueryResult q;
+    void *fn = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn)
+      return nullptr;
+    encode = (EncodeTiledFn)fn;
+  }
+  void *mem = nullptr;
+  if (posix_memalign(&mem, 64, 6 * sizeof(fhy::TmaLine)) != 0) return nullptr;
+  fhy::TmaLine *m = static_cast<fhy::TmaLine *>(mem);
+  memset(m, 0, 6 * sizeof(fhy::TmaLine));
+  const cuuint64_t dims[3] = {8, 8, (cuuint64_t)c->nblocks * 8};
+  const cuuint64_t strides[2] = {8 * sizeof(double), 64 * sizeof(double)};
+  const cuuint32_t one[3] = {1, 1, 1};
+  const cuuint32_t box_in[3] = {8, 8, 8};
+  const cuuint32_t box_slab[3][3] = {{4, 8, 8}, {8, 4, 8}, {8, 8, 4}};
+  for (int par = 0; par < 2; ++par)
+    for (int d = 0; d < 3; ++d) {
+      fhy::TmaLine &t = m[par * 3 + d];
+      for (int v = 0; v < 5; ++v) {
+        if (encode(&t.intr[v], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, c->state[par][v], dims, strides, box_in, one,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS ||
+            encode(&t.slab[v], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, c->state[par][v], dims, strides, box_slab[d], one,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS) {
+          free(m);
+          return nullptr;
+        }
+      }
+      t.on = 1;
+    }
+  return m;
 }
 
 static void drop_graphs(flash_hy_ctx *c) {
@@ -436,6 +486,7 @@ extern "C" int flash_hy_create(const flash_hy_params *params, const flash_hy_gri
     for (int v = 0; v < 5; ++v) ALLOC(c->state[s][v], c->ncells * sizeof(double));
   ALLOC(c->acc, 5 * c->ncells * sizeof(double));
   if (g->ndim > 1) ALLOC(c->aux, (size_t)(g->ndim - 1) * 3 * c->ncells * sizeof(double));
+  if (!amr) c->tma_maps = make_tma_maps(c);
   if (amr) {
     c->amr = 1;
     c->nlev = g->max_level;
@@ -561,6 +612,7 @@ extern "C" int flash_hy_destroy(flash_hy_ctx *c) {
   ctx_free(c->sp_lh); ctx_free(c->sp_gp); ctx_free(c->sp_freg);
   free(c->h_blk_at);
   free(c->h_list);
+  free(c->tma_maps);
   if (c->h_dt) cudaFreeHost(c->h_dt);
   if (c->h_status) cudaFreeHost(c->h_status);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -777,6 +829,7 @@ static int enqueue_step(flash_hy_ctx *c, double dt, const int *d_list, int nlaun
   a.dir_threads = c->dir_threads;
   a.mx_sel = c->mx_sel;
   a.stream = c->stream;
+  a.tma = c->tma_maps ? c->tma_maps + 3 * c->cur : nullptr;
   a.nlev = 0;
   int pre = 0;
   if (c->amr) {
@@ -1078,6 +1131,7 @@ extern "C" int flash_hy_compute_dt(flash_hy_ctx *c, double *dt_out, int minloc_o
     a.dir_threads = c->dir_threads;
     a.mx_sel = c->mx_sel;
     a.stream = c->stream;
+    a.tma = nullptr;
     a.set_attr = true;
     if (cfl_state(a, c->ndim, c->nx, c->ny, c->nz) < 0) return fail(c, FLASH_HY_ERR_CUDA, "cfl launch%s", "");
     c->dt_valid = 1;

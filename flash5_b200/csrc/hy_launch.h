@@ -1,10 +1,21 @@
 // hy_launch.h -- interface between the C-ABI (flash_hy.cu) and the kernel
 // variants (hy_variant.cu, compiled once per arithmetic variant).
 #pragma once
+#include <cuda.h>
 #include "hy_kernels.cuh"
 #include "../../include/flash_hy.h"
 
 namespace fhy {
+
+// Tensor maps of the step's input state for the mixed direction kernels'
+// TMA staging (k_dir_mx, uniform 3D grids): per state variable the block
+// interior (box 8 x 8 x 8) and the neighbour slab along the sweep direction
+// (box 4 x 8 x 8, 8 x 4 x 8 or 8 x 8 x 4) over the natural block layout.
+struct TmaLine {
+  CUtensorMap intr[5];        // dens, velx, vely, velz, eint
+  CUtensorMap slab[5];
+  int on;                     // 0: the stencil is staged by load_prim
+};
 
 struct StepArgs {
   DevParams P;
@@ -27,6 +38,7 @@ struct StepArgs {
   int nleaves;
   const int *lev_list[17];  // leaves of each level (device), 1-based levels
   int lev_count[17];
+  const TmaLine *tma; // [3] (directions x, y, z) for the input state, or NULL
 };
 
 // the species / mass-scalar pass after the hydro direction kernels

@@ -20,6 +20,48 @@
 
 namespace fhy {
 
+// ---------------------------------------------------------------------------
+// TMA staging of the direction kernels' line stencils (uniform 3D grids).
+// Each state variable is described by tensor maps over its natural layout
+// (x fastest, then y, then z of every block: dims 8 x 8 x 8*nblocks); one
+// 3D tile copy brings a block's interior (box 8 x 8 x 8) and one a
+// neighbour's 4-cell slab along the sweep direction (box 4 x 8 x 8,
+// 8 x 4 x 8 or 8 x 8 x 4), straight into the staged layout below.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+// one bounded poll of phase `parity`; true once it has completed
+__device__ __forceinline__ bool mbar_try(unsigned long long *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.b32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// 3D tile copy global -> shared through a tensor map (no multicast)
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int c0, int c1, int c2,
+                                            unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], "
+      "[%2];\n" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
+      : "memory");
+}
+// SM cycles (about a second) a CTA waits for its tile copies before it gives
+// up (FLASH_HY_ERR_TIMEOUT)
+constexpr long long kTmaWaitCycles = 1LL << 31;
+
 // FP64 HLLC (hy_HLLC.F90:94-311) with one division per star state; igm1 =
 // 1/(game - 1) of the cell the face state belongs to.
 template <int DIR>
@@ -88,6 +130,20 @@ struct MxGeom {
     if (DIR == 1) { l = s / L; x = s % L - o; } else { l = s % C; x = s / C - o; }
   }
   static constexpr int step = DIR == 1 ? 1 : C;      // +1 along the line
+  // staged stencil (positions x in [-4, ND + 3] of line l): three regions --
+  // the slab of the neighbour below, the block's interior, the slab of the
+  // neighbour above -- each in the natural x, y, z order of the block
+  // store, so that each is one dense tile copy; along the sweep direction
+  // the regions follow one another (DIR 3: plain along-major order)
+  static constexpr int SLAB = 4 * C, LO = 0, MID = 4 * C, HI = (4 + ND) * C;
+  __device__ static __forceinline__ int sidx(int x, int l) {
+    if (DIR == 3) return (x + 4) * C + l;
+    if (DIR == 1) return x < 0 ? l * 4 + (x + 4) : (x < ND ? MID + l * ND + x : HI + l * 4 + (x - ND));
+    // DIR 2: line l = i + NX * k
+    const int i = l % NX, k = l / NX;
+    return x < 0 ? k * 4 * NX + (x + 4) * NX + i
+                 : (x < ND ? MID + (k * ND + x) * NX + i : HI + k * 4 * NX + (x - ND) * NX + i);
+  }
   __device__ static __forceinline__ void cell(int x, int l, int &i, int &j, int &k) {
     if (DIR == 1) { i = x; j = l % NY; k = l / NY; }
     else if (DIR == 2) { j = x; i = l % NX; k = l / NX; }
@@ -104,7 +160,11 @@ struct MxGeom {
       (RS == 1 && slope_bytes < sizeof(xrs::MlpPacked)) ? sizeof(xrs::MlpPacked) : slope_bytes;
   static constexpr size_t recon_bytes = wp_off + (size_t)2 * SC * 6 * 4 + (size_t)SC * 8;
   static constexpr size_t flux_bytes = (size_t)SC * 9 * 8;
-  static constexpr size_t smem_bytes() { return prim_bytes + (recon_bytes > flux_bytes ? recon_bytes : flux_bytes); }
+  // + the staging barrier and the slack that aligns the tile destinations
+  // to 128 bytes
+  static constexpr size_t smem_bytes() {
+    return prim_bytes + (recon_bytes > flux_bytes ? recon_bytes : flux_bytes) + 16 + 128;
+  }
 };
 
 // threads per CTA of k_dir_mx: three compiled candidates per block shape,
@@ -122,15 +182,17 @@ template <int NDIM, int NX, int NY, int NZ> struct MxThreads {
 template <int NDIM, int NX, int NY, int NZ, int DIR, bool FIRST, bool LAST, int RS, int NT>
 __global__ void __launch_bounds__(NT, NDIM == 3 ? 2 : 1)
 k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ ACC, double *__restrict__ AUX,
-         size_t ncells, CflPart *part) {
+         size_t ncells, CflPart *part, const __grid_constant__ TmaLine tm) {
   static_assert(NT % 32 == 0, "threads per CTA must be a multiple of 32");
   using G = MxGeom<NDIM, NX, NY, NZ, DIR, RS>;
   using B = Box<NDIM, NX, NY, NZ>;
   constexpr int NCB = NX * NY * NZ;
   constexpr int NIT = (G::SC + NT - 1) / NT;
   constexpr int v1 = Slots<DIR>::v1;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  double *sV = reinterpret_cast<double *>(smem_raw);                     // [6][SA]: rho,u,v,w,p,e
+  extern __shared__ __align__(16) unsigned char smem_dyn[];
+  unsigned char *smem_raw =
+      smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);          // tile destinations: 128-byte aligned
+  double *sV = reinterpret_cast<double *>(smem_raw);                     // [6][SA]: rho,u,v,w,p,e (sidx order)
   unsigned char *reg = smem_raw + G::prim_bytes;
   float *sFlat = reinterpret_cast<float *>(reg);                          // [SB]
   float *sDb = sFlat + G::SB;                                             // [6][SB]
@@ -153,14 +215,90 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
   auto fidx = [](int along, int t1, int t2) { return G::at(along, t1 + (DIR == 1 ? NY : NX) * t2, G::LC, 1); };
   if (P.fmode != 3) {
   // ---- A: stage the primitive stencil of every line (guard cells get the EOS)
+  // Uniform 3D grids: the block's interior and the neighbours' slabs along
+  // DIR by TMA tile copies (one thread issues 15, an mbarrier counts the
+  // bytes), then the pressure and the guard cells' EOS in place; slabs
+  // beyond a non-periodic boundary (mirror / copy rules) and all other
+  // grids through load_prim.
+  bool tma = NDIM == 3 && tm.on && P.lh == nullptr;
+  int nbs[2] = {-1, -1};          // neighbour blocks below / above along DIR (-1: load_prim)
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(smem_raw + G::smem_bytes() - 16 - 128);
+  if (tma) {
+    const int ext[3] = {P.nbx, P.nby, P.nbz};
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+      int cc[3] = {bc.x, bc.y, bc.z};
+      cc[DIR - 1] += side ? 1 : -1;
+      bool ok = true;
+      if (cc[DIR - 1] < 0 || cc[DIR - 1] >= ext[DIR - 1]) {
+        ok = P.bc[2 * (DIR - 1) + side] == FLASH_HY_BC_PERIODIC;
+        cc[DIR - 1] = (cc[DIR - 1] + ext[DIR - 1]) % ext[DIR - 1];
+      }
+      nbs[side] = ok ? P.blk_at[(cc[2] * P.nby + cc[1]) * P.nbx + cc[0]] : -1;
+    }
+    if (threadIdx.x == 0) mbar_init(bar, 1);
+    __syncthreads();                          // the barrier is initialised before anyone polls it
+    if (threadIdx.x == 0) {
+      const unsigned slab_bytes = (unsigned)G::SLAB * 8u, mid_bytes = (unsigned)(G::ND * G::C) * 8u;
+      mbar_expect_tx(bar, 5u * (mid_bytes + (nbs[0] >= 0 ? slab_bytes : 0u) + (nbs[1] >= 0 ? slab_bytes : 0u)));
+      const int q5[5] = {0, 1, 2, 3, 5};       // staged slots of dens, velx, vely, velz, eint
+#pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        double *dst = sV + q5[v] * G::SA;
+        tma_load_3d(dst + G::MID, &tm.intr[v], 0, 0, b * NZ, bar);
+        // the slab below: the neighbour's last four layers; above: its first four
+        if (nbs[0] >= 0)
+          tma_load_3d(dst + G::LO, &tm.slab[v], DIR == 1 ? NX - 4 : 0, DIR == 2 ? NY - 4 : 0,
+                      nbs[0] * NZ + (DIR == 3 ? NZ - 4 : 0), bar);
+        if (nbs[1] >= 0) tma_load_3d(dst + G::HI, &tm.slab[v], 0, 0, nbs[1] * NZ, bar);
+      }
+    }
+  }
+  // cells no tile copy covers
   for (int s = threadIdx.x; s < G::SA; s += NT) {
     int x, l, i, j, k;
     G::dec(s, G::L4, 4, x, l);
+    if (tma && (x < 0 ? nbs[0] >= 0 : (x >= G::ND ? nbs[1] >= 0 : true))) continue;
     G::cell(x, l, i, j, k);
     double V[8];
     load_prim<NDIM, NX, NY, NZ, false>(P, b, bc, i, j, k, V);
-    sV[0 * G::SA + s] = V[HD]; sV[1 * G::SA + s] = V[HVX]; sV[2 * G::SA + s] = V[HVY];
-    sV[3 * G::SA + s] = V[HVZ]; sV[4 * G::SA + s] = V[HP]; sV[5 * G::SA + s] = V[HEI];
+    const int q = G::sidx(x, l);
+    sV[0 * G::SA + q] = V[HD]; sV[1 * G::SA + q] = V[HVX]; sV[2 * G::SA + q] = V[HVY];
+    sV[3 * G::SA + q] = V[HVZ]; sV[4 * G::SA + q] = V[HP]; sV[5 * G::SA + q] = V[HEI];
+  }
+  if (tma) {
+    // bounded wait for the tile copies; a CTA that gives up flags
+    // FLASH_HY_ERR_TIMEOUT, waits (bounded) once more for its copies in
+    // flight and leaves
+    bool done = false;
+    const long long t0 = clock64();
+    while (!done && clock64() - t0 < kTmaWaitCycles) done = mbar_try(bar, 0);
+    if (__syncthreads_or(!done)) {
+      if (threadIdx.x == 0) atomicOr(P.status, (unsigned)FLASH_HY_ERR_TIMEOUT);
+      const long long t1 = clock64();
+      while (clock64() - t1 < kTmaWaitCycles && !mbar_try(bar, 0)) {
+      }
+      return;
+    }
+    // pressure of every copied cell; the guard cells' EOS first
+    // (Eos_getData.F90:80-96 on ENER = eint + ekin, as load_prim)
+    for (int s = threadIdx.x; s < G::SA; s += NT) {
+      int x, l;
+      G::dec(s, G::L4, 4, x, l);
+      const bool guard = x < 0 || x >= G::ND;
+      if (guard && nbs[x < 0 ? 0 : 1] < 0) continue;
+      const int q = G::sidx(x, l);
+      const double rho = sV[q], e = sV[5 * G::SA + q];
+      double eg = e;
+      if (guard) {
+        const double vx = sV[G::SA + q], vy = sV[2 * G::SA + q], vz = sV[3 * G::SA + q];
+        const double ekin = 0.5 * (vx * vx + vy * vy + vz * vz);
+        const double ener = e + ekin;
+        if (ener - ekin > rmax(P.smalle, P.eswitch * ekin)) eg = ener - ekin;
+        sV[5 * G::SA + q] = eg;
+      }
+      sV[4 * G::SA + q] = rho * eg * P.gam1inv;
+    }
   }
   __syncthreads();
   auto Vs = [&](int q, int s) -> double { return sV[q * G::SA + s]; };   // q: 0..5 (5 = eint)
@@ -169,29 +307,28 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
   for (int q = threadIdx.x; q < G::SB; q += NT) {
     int x, l;
     G::dec(q, G::LS, 2, x, l);
-    const int s = G::at(x, l, G::L4, 4);
+    const int s = G::sidx(x, l), sm = G::sidx(x - 1, l), sp = G::sidx(x + 1, l);
     float Vc[8], dL[5], dR[5];
 #pragma unroll
     for (int n = 0; n < 5; ++n) {
       Vc[n] = float(Vs(n, s));
-      dL[n] = float(Vs(n, s) - Vs(n, s - G::step));
-      dR[n] = float(Vs(n, s + G::step) - Vs(n, s));
+      dL[n] = float(Vs(n, s) - Vs(n, sm));
+      dR[n] = float(Vs(n, sp) - Vs(n, s));
     }
     Vc[HGC] = float(P.gamma); Vc[HGE] = 0.f; Vc[HEI] = float(Vs(5, s));
     Eig<float> e;
     eigen<float, DIR>(Vc, e, st);
     float db[8];
-    tvd_slope_d<float, DIR>(P, dL, dR, float(Vs(5, s) - Vs(5, s - G::step)), float(Vs(5, s + G::step) - Vs(5, s)), e,
-                            db);
+    tvd_slope_d<float, DIR>(P, dL, dR, float(Vs(5, s) - Vs(5, sm)), float(Vs(5, sp) - Vs(5, s)), e, db);
 #pragma unroll
     for (int n = 0; n < 5; ++n) sDb[n * G::SB + q] = db[n];
     sDb[5 * G::SB + q] = db[HEI];
     if (P.use_flattening) {
-      const int st1 = G::step, st2 = 2 * G::step;
-      float dp1 = float(Vs(4, s + st1) - Vs(4, s - st1));
-      float dp2 = float(Vs(4, s + st2) - Vs(4, s - st2));
-      float dv1 = float(Vs(v1, s + st1) - Vs(v1, s - st1));
-      float pmin = float(fmin(Vs(4, s - st1), Vs(4, s + st1)));
+      const int smm = G::sidx(x - 2, l), spp = G::sidx(x + 2, l);
+      float dp1 = float(Vs(4, sp) - Vs(4, sm));
+      float dp2 = float(Vs(4, spp) - Vs(4, smm));
+      float dv1 = float(Vs(v1, sp) - Vs(v1, sm));
+      float pmin = float(fmin(Vs(4, sm), Vs(4, sp)));
       float Sp = fabsf(dp2) > 1.e-15f ? dp1 / dp2 - 0.75f : 0.f;
       float ft = fmaxf(0.f, fminf(1.f, 10.f * Sp));
       if ((fabsf(dp1) / pmin < 1.f / 3.f) || dv1 > 0.f) ft = 0.f;
@@ -205,24 +342,24 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
     int x, l, i, j, k;
     G::dec(t, G::LC, 1, x, l);
     G::cell(x, l, i, j, k);
-    const int s = G::at(x, l, G::L4, 4), q = G::at(x, l, G::LS, 2);
+    const int s = G::sidx(x, l), sm = G::sidx(x - 1, l), sp = G::sidx(x + 1, l), q = G::at(x, l, G::LS, 2);
     const int qs = G::step;
     float Vc[8], dL[8], dR[8];
 #pragma unroll
     for (int n = 0; n < 5; ++n) {
       Vc[n] = float(Vs(n, s));
-      dL[n] = float(Vs(n, s) - Vs(n, s - G::step));
-      dR[n] = float(Vs(n, s + G::step) - Vs(n, s));
+      dL[n] = float(Vs(n, s) - Vs(n, sm));
+      dR[n] = float(Vs(n, sp) - Vs(n, s));
     }
     Vc[HGC] = float(P.gamma); Vc[HEI] = float(Vs(5, s));
-    dL[HEI] = float(Vs(5, s) - Vs(5, s - G::step));
-    dR[HEI] = float(Vs(5, s + G::step) - Vs(5, s));
+    dL[HEI] = float(Vs(5, s) - Vs(5, sm));
+    dR[HEI] = float(Vs(5, sp) - Vs(5, s));
     Eig<float> e0;
     eigen<float, DIR>(Vc, e0, st);
     float flat = 0.f;
     if (P.use_flattening) {
       float t0 = sFlat[q];
-      double dp1 = Vs(4, s + G::step) - Vs(4, s - G::step);
+      double dp1 = Vs(4, sp) - Vs(4, sm);
       if (dp1 < 0.) flat = fmaxf(t0, sFlat[q + qs]);
       else if (dp1 == 0.) flat = t0;
       else flat = fmaxf(t0, sFlat[q - qs]);
@@ -241,8 +378,8 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
     }
     if (P.use_steepening) {
       const float eta1 = 20.f, eta2 = 0.05f, epsln = 0.01f, K0 = 0.1f;
-      double rm = Vs(0, s - G::step), rp = Vs(0, s + G::step), rc = Vs(0, s);
-      double rmm = Vs(0, s - 2 * G::step), rpp = Vs(0, s + 2 * G::step);
+      double rm = Vs(0, sm), rp = Vs(0, sp), rc = Vs(0, s);
+      double rmm = Vs(0, G::sidx(x - 2, l)), rpp = Vs(0, G::sidx(x + 2, l));
       float temp1 = float(rp - rm);
       if (fabsf(temp1) > float(P.tiny)) {
         float dd = float(delta);
@@ -252,7 +389,7 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
         if (d2R * d2L >= 0.f) eta = 0.f;
         if (epsln * float(fmin(rp, rm)) - fabsf(temp1) >= 0.f) eta = 0.f;
         eta = fmaxf(0.f, fminf(1.f, eta1 * (eta - eta2)));
-        double pm = Vs(4, s - G::step), pp = Vs(4, s + G::step);
+        double pm = Vs(4, sm), pp = Vs(4, sp);
         float temp2 = float(fabs(pp - pm) / fmin(pp, pm));
         float temp3 = fabsf(temp1) / float(fmin(rp, rm));
         double game_c = Vs(4, s) / (Vs(5, s) * rc) + 1;
@@ -394,13 +531,14 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
     const bool learned = P.mlp != nullptr;
     const double g = P.gamma;
     const xrs::Gas &gas = P.gas;             // from the parameter block
-    auto face = [&](int qq, bool left, int s, int t) -> double {
-      return left ? Vs(qq, s - G::step) + double(sWp[qq * G::SC + t - G::step])
-                  : Vs(qq, s) + double(sWm[qq * G::SC + t]);
+    // s: staged index of the face's right cell, sl: of its left cell
+    auto face = [&](int qq, bool left, int2 s, int t) -> double {
+      return left ? Vs(qq, s.y) + double(sWp[qq * G::SC + t - G::step])
+                  : Vs(qq, s.x) + double(sWm[qq * G::SC + t]);
     };
     // the two face states; w = p^z only with `with_w` (pass 1a tests for
     // strong waves without it)
-    auto sides = [&](int s, int t, xrs::Side &L, xrs::Side &R, bool with_w = true) {
+    auto sides = [&](int2 s, int t, xrs::Side &L, xrs::Side &R, bool with_w = true) {
       const double dl = face(0, true, s, t), ul = face(DIR, true, s, t), pl = face(4, true, s, t);
       const double dr = face(0, false, s, t), ur = face(DIR, false, s, t), pr = face(4, false, s, t);
       const double c2l = g * pl / dl, c2r = g * pr / dr;
@@ -423,7 +561,7 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
         int x, l;
         G::dec(t, G::LC, 1, x, l);
         if (x < 0) continue;
-        const int s4 = G::at(x, l, G::L4, 4);
+        const int2 s4 = make_int2(G::sidx(x, l), G::sidx(x - 1, l));
         double q = 0.0;
         // the FP32 screen first; the FP64 sides and tests only where it passes
         if (xrs::strong_screen(face(0, true, s4, t), face(DIR, true, s4, t), face(4, true, s4, t),
@@ -456,7 +594,7 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
           const bool net = q > 0.0;
           if (!__any_sync(0xffffffffu, net)) continue;
           xrs::Side L{1.0, 0.0, 1.0, 1.0, 1.0}, R{1.0, 0.0, 1.0, 1.0, 1.0};
-          if (net) sides(G::at(x, l, G::L4, 4), t, L, R);
+          if (net) sides(make_int2(G::sidx(x, l), G::sidx(x - 1, l)), t, L, R);
           float f[xrs::NIN];
           if (net) xrs::features(L, R, g, xrs::p_of_w(q, gas), f);
           else {
@@ -475,7 +613,7 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
       int x, l;
       G::dec(t, G::LC, 1, x, l);
       if (x < 0) continue;
-      const int s = G::at(x, l, G::L4, 4);
+      const int2 s = make_int2(G::sidx(x, l), G::sidx(x - 1, l));
       xrs::Side L, R;
       sides(s, t, L, R);
       const bool vac = xrs::vacuum(L, R, gas);
@@ -508,7 +646,7 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
       }
       Fr[it][FEINT] = fe;
       Fr[it][FVOLU] = fv;
-      Fr[it][8] = (Vs(4, s) + double(sWm[4 * G::SC + t])) + (Vs(4, s) + double(sWp[4 * G::SC + t]));
+      Fr[it][8] = (Vs(4, s.x) + double(sWm[4 * G::SC + t])) + (Vs(4, s.x) + double(sWp[4 * G::SC + t]));
     }
   } else {
 #pragma unroll
@@ -518,8 +656,8 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
     int x, l;
     G::dec(t, G::LC, 1, x, l);
     if (x < 0) continue;
-    const int s = G::at(x, l, G::L4, 4);
-    const int tl = t - G::step, sL = s - G::step;
+    const int s = G::sidx(x, l);
+    const int tl = t - G::step, sL = G::sidx(x - 1, l);
     double VL[8], VR[8];
 #pragma unroll
     for (int qq = 0; qq < 6; ++qq) {

@@ -6,6 +6,7 @@
 //                  once per threads-per-CTA candidate of the direction
 //                  kernels (FHY_MXSEL = 0, 1, 2), the transverse-flux pass
 //                  and the dispatcher only in unit 0
+#include <string.h>
 #include "hy_launch.h"
 #include "../../include/flash_hy.h"
 #if FHY_VARIANT == 3
@@ -45,7 +46,14 @@ static bool launch_dir_one(const StepArgs &a) {
   const size_t smem = G::smem_bytes();
   if (a.set_attr && cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return false;
+#if FHY_VARIANT == 3
+  TmaLine tl;
+  memset(&tl, 0, sizeof tl);
+  if (NDIM == 3 && a.tma && a.nlev == 0) tl = a.tma[DIR - 1];
+  kern<<<a.nlaunch, threads, smem, a.stream>>>(a.P, (const Real *)a.sig, a.acc, a.aux, a.ncells, a.part, tl);
+#else
   kern<<<a.nlaunch, threads, smem, a.stream>>>(a.P, (const Real *)a.sig, a.acc, a.aux, a.ncells, a.part);
+#endif
   return cudaGetLastError() == cudaSuccess;
 }
 
