@@ -6,6 +6,7 @@
 #include <string.h>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 #include "../../include/flash_hy.h"
@@ -36,6 +37,7 @@ struct flash_hy_ctx {
   int h_list_cap;
   int mesh_me;               // hy_meshMe: the rank reported in the dt minloc
   fhy::TmaLine *tma_maps;    // [2 state buffers][3 directions]: TMA staging of k_dir_mx, or NULL
+  struct XferPool *xfer;     // host threads, streams and pinned slots of upload / download
   CflPart *d_part;
   DtInfo *d_dt, *h_dt;
   unsigned *d_status, *h_status;
@@ -588,6 +590,8 @@ bad:
 #undef ALLOC
 }
 
+static void xfer_free(flash_hy_ctx *c);
+
 extern "C" int flash_hy_destroy(flash_hy_ctx *c) {
   if (!c) return FLASH_HY_ERR_BAD_ARG;
   cudaSetDevice(c->device);
@@ -613,6 +617,7 @@ extern "C" int flash_hy_destroy(flash_hy_ctx *c) {
   free(c->h_blk_at);
   free(c->h_list);
   free(c->tma_maps);
+  xfer_free(c);
   if (c->h_dt) cudaFreeHost(c->h_dt);
   if (c->h_status) cudaFreeHost(c->h_status);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -622,6 +627,16 @@ extern "C" int flash_hy_destroy(flash_hy_ctx *c) {
 
 // ---------------------------------------------------------------------------
 // UNK <-> device block store
+//
+// Only the variables the device needs (upload) or owns (download) cross
+// PCIe, packed as SoA [variable][cell] over the interiors: host threads
+// gather them from the caller's UNK (either layout, with or without guard
+// cells) into pinned buffers and the copy engine moves one sub-chunk while
+// the next is gathered; downloads run the other way (device pack, copy,
+// host scatter into the owned variables only; guard cells and variables the
+// device does not own keep the caller's values).  A device kernel converts
+// between the packed copy and the state (the upload's EOS, the download's
+// Eos_putData outputs).
 // ---------------------------------------------------------------------------
 struct HostLayout {
   int layout, nunk, ng[3], nt[3];
@@ -629,50 +644,61 @@ struct HostLayout {
   int v_spec;           // first species (0-based); species and mass scalars follow
 };
 
-__device__ __forceinline__ size_t unk_index(const HostLayout &L, int b, int i, int j, int k, int v) {
+static inline size_t unk_index(const HostLayout &L, size_t b, int i, int j, int k, int v) {
   if (L.layout == FLASH_HY_LAYOUT_VAR_FASTEST)
     return ((((size_t)b * L.nt[2] + k) * L.nt[1] + j) * L.nt[0] + i) * L.nunk + v;
   return ((((size_t)b * L.nunk + v) * L.nt[2] + k) * L.nt[1] + j) * L.nt[0] + i;
 }
 
-__global__ void k_unpack(const double *__restrict__ stage, HostLayout L, DevParams P, int nx, int ny, int nz,
-                         size_t ncells) {
+// the packed variables of a transfer: UNK indices (0-based) in packed order
+struct PackList {
+  int n;
+  int unk[10 + FLASH_HY_MAX_SPECIES];
+  // positions in the packed order (-1 absent): upload dens, velx, vely, velz, eint, ener,
+  // species; download dens, velx, vely, velz, eint, pres, temp, gamc, game, ener, species
+  int at[10], spec;
+};
+
+// The packed copy is chunked SoA: chunk c holds cells [c S, c S + n_c)
+// (n_c = S but for the last chunk) as [variable][cell], one contiguous
+// copy per chunk.
+__device__ __forceinline__ size_t chunk_off(size_t t, size_t S, int nv, size_t ncells, int q) {
+  const size_t c = t / S, c0 = c * S;
+  const size_t n = ncells - c0 < S ? ncells - c0 : S;
+  return c0 * nv + (size_t)q * n + (t - c0);
+}
+
+// upload: dens, velx, vely, velz, eint, ener (as mapped), species
+__global__ void k_unpack_soa(const double *__restrict__ st, PackList pl, DevParams P, size_t ncells, size_t S) {
   size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (t >= ncells) return;
-  size_t ncb = (size_t)nx * ny * nz;
-  int b = (int)(t / ncb), loc = (int)(t % ncb);
-  int i = loc % nx, j = (loc / nx) % ny, k = loc / (nx * ny);
-  int hi = i + L.ng[0], hj = j + L.ng[1], hk = k + L.ng[2];
-  auto get = [&](int v) { return v < 0 ? 0.0 : stage[unk_index(L, b, hi, hj, hk, v)]; };
-  double rho = get(L.v_dens), vx = get(L.v_velx), vy = get(L.v_vely), vz = get(L.v_velz);
+  auto get = [&](int q) { return q < 0 ? 0.0 : st[chunk_off(t, S, pl.n, ncells, q)]; };
+  double rho = get(pl.at[0]), vx = get(pl.at[1]), vy = get(pl.at[2]), vz = get(pl.at[3]);
   // Eos_getData.F90:80-96 then MODE_DENS_EI keeps eint (Grid_initDomain's EOS)
   double ekin = 0.5 * (vx * vx + vy * vy + vz * vz);
-  double eint = L.v_eint >= 0 ? get(L.v_eint) : get(L.v_ener) - ekin;
-  if (L.v_ener >= 0) {
-    double ener = get(L.v_ener);
+  double eint = pl.at[4] >= 0 ? get(pl.at[4]) : get(pl.at[5]) - ekin;
+  if (pl.at[5] >= 0) {
+    double ener = get(pl.at[5]);
     if (ener - ekin > rmax(P.smalle, P.eswitch * ekin)) eint = ener - ekin;
   }
   P.s_out[0][t] = rho; P.s_out[1][t] = vx; P.s_out[2][t] = vy; P.s_out[3][t] = vz; P.s_out[4][t] = eint;
-  for (int q = 0; q < P.nsp; ++q) P.sp_out[(size_t)q * ncells + t] = get(L.v_spec + q);
+  for (int q = 0; q < P.nsp; ++q) P.sp_out[(size_t)q * ncells + t] = get(pl.spec + q);
 }
 
-__global__ void k_pack(double *__restrict__ stage, HostLayout L, DevParams P, int nx, int ny, int nz, size_t ncells) {
+// download: Eos_putData.F90:95-106 of the gamma law for the owned variables
+__global__ void k_pack_soa(double *__restrict__ st, PackList pl, DevParams P, int ncb, size_t ncells, size_t S) {
   size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (t >= ncells) return;
-  size_t ncb = (size_t)nx * ny * nz;
-  int b = (int)(t / ncb), loc = (int)(t % ncb);
-  int i = loc % nx, j = (loc / nx) % ny, k = loc / (nx * ny);
-  int hi = i + L.ng[0], hj = j + L.ng[1], hk = k + L.ng[2];
+  const size_t b = t / ncb;
   double rho = P.s_in[0][t], vx = P.s_in[1][t], vy = P.s_in[2][t], vz = P.s_in[3][t], e = P.s_in[4][t];
-  // Eos_putData.F90:95-106 of the gamma law
   double ekin = 0.5 * (vx * vx + vy * vy + vz * vz);
   double pres = rho * e * P.gam1inv;
   double temp = e * P.ggprodinv * P.abar;
-  auto put = [&](int v, double x) { if (v >= 0) stage[unk_index(L, b, hi, hj, hk, v)] = x; };
-  put(L.v_dens, rho); put(L.v_velx, vx); put(L.v_vely, vy); put(L.v_velz, vz);
-  put(L.v_pres, pres); put(L.v_temp, temp); put(L.v_gamc, P.gamma); put(L.v_eint, e);
-  put(L.v_ener, (P.leaf && !P.leaf[b]) ? P.pe[t] : e + ekin); put(L.v_game, pres / (e * rho) + 1);
-  for (int q = 0; q < P.nsp; ++q) put(L.v_spec + q, P.sp_in[(size_t)q * ncells + t]);
+  auto put = [&](int q, double x) { if (q >= 0) st[chunk_off(t, S, pl.n, ncells, q)] = x; };
+  put(pl.at[0], rho); put(pl.at[1], vx); put(pl.at[2], vy); put(pl.at[3], vz);
+  put(pl.at[4], e); put(pl.at[5], pres); put(pl.at[6], temp); put(pl.at[7], P.gamma);
+  put(pl.at[8], pres / (e * rho) + 1); put(pl.at[9], (P.leaf && !P.leaf[b]) ? P.pe[t] : e + ekin);
+  for (int q = 0; q < P.nsp; ++q) put(pl.spec + q, P.sp_in[(size_t)q * ncells + t]);
 }
 
 static int make_layout(flash_hy_ctx *c, int layout, int nunk, const flash_hy_varmap *vm, int nguard, HostLayout &L) {
@@ -699,6 +725,27 @@ static int make_layout(flash_hy_ctx *c, int layout, int nunk, const flash_hy_var
   return 0;
 }
 
+static PackList pack_list(const flash_hy_ctx *c, const HostLayout &L, bool upload) {
+  PackList pl;
+  pl.n = 0;
+  auto add = [&](int v) { if (v < 0) return -1; pl.unk[pl.n] = v; return pl.n++; };
+  for (int q = 0; q < 10; ++q) pl.at[q] = -1;
+  if (upload) {
+    const int vs[6] = {L.v_dens, L.v_velx, L.v_vely, L.v_velz, L.v_eint, L.v_ener};
+    for (int q = 0; q < 6; ++q) pl.at[q] = add(vs[q]);
+  } else {
+    const int vs[10] = {L.v_dens, L.v_velx, L.v_vely, L.v_velz, L.v_eint,
+                        L.v_pres, L.v_temp, L.v_gamc, L.v_game, L.v_ener};
+    for (int q = 0; q < 10; ++q) pl.at[q] = add(vs[q]);
+  }
+  pl.spec = -1;
+  for (int q = 0; q < c->nsp; ++q) {
+    const int k = add(L.v_spec + q);
+    if (q == 0) pl.spec = k;
+  }
+  return pl;
+}
+
 static int ensure_stage(flash_hy_ctx *c, size_t bytes) {
   if (c->stage_bytes >= bytes) return 0;
   if (c->d_stage) { cudaStreamSynchronize(c->stream); cudaFree(c->d_stage); c->d_stage = nullptr; c->stage_bytes = 0; }
@@ -707,22 +754,161 @@ static int ensure_stage(flash_hy_ctx *c, size_t bytes) {
   return 0;
 }
 
+// Per-context transfer workers: a stream, two pinned slots and their
+// events per host thread (created on first use, kept until destroy).
+struct XferPool {
+  int nthreads;
+  size_t slot_cells;                     // cells per sub-chunk (whole blocks)
+  size_t slot_doubles;                   // slot_cells x the most packed variables
+  cudaStream_t st[64];
+  cudaEvent_t ev[64][2], done[64];
+  double *pinned;                        // [nthreads][2][slot_doubles]
+  cudaEvent_t start;                     // recorded on the context's stream
+};
+
+static void xfer_release(XferPool *x) {
+  for (int t = 0; t < x->nthreads; ++t) {
+    if (x->st[t]) cudaStreamDestroy(x->st[t]);
+    for (int q = 0; q < 2; ++q) if (x->ev[t][q]) cudaEventDestroy(x->ev[t][q]);
+    if (x->done[t]) cudaEventDestroy(x->done[t]);
+  }
+  if (x->start) cudaEventDestroy(x->start);
+  if (x->pinned) cudaFreeHost(x->pinned);
+  free(x);
+}
+
+static int xfer_pool(flash_hy_ctx *c, XferPool *&out) {
+  if (c->xfer) { out = c->xfer; return 0; }
+  XferPool *x = (XferPool *)calloc(1, sizeof(XferPool));
+  if (!x) return fail(c, FLASH_HY_ERR_CUDA, "host allocation%s", "");
+  const size_t per_block = c->ncb;
+  const size_t blocks_per_slot = per_block >= 65536 ? 1 : 65536 / per_block;
+  x->slot_cells = blocks_per_slot * per_block;
+  x->slot_doubles = x->slot_cells * (10 + c->nsp);
+  const int hw = (int)std::thread::hardware_concurrency();
+  const size_t slots = (c->ncells + x->slot_cells - 1) / x->slot_cells;
+  int n = hw > 0 ? hw : 1;
+  if (n > 64) n = 64;
+  if ((size_t)n > slots) n = (int)slots;
+  x->nthreads = n;
+  cudaError_t e = cudaEventCreateWithFlags(&x->start, cudaEventDisableTiming);
+  for (int t = 0; t < n && e == cudaSuccess; ++t) {
+    e = cudaStreamCreateWithFlags(&x->st[t], cudaStreamNonBlocking);
+    for (int q = 0; q < 2 && e == cudaSuccess; ++q) e = cudaEventCreateWithFlags(&x->ev[t][q], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&x->done[t], cudaEventDisableTiming);
+  }
+  if (e == cudaSuccess) e = cudaMallocHost((void **)&x->pinned, (size_t)n * 2 * x->slot_doubles * sizeof(double));
+  if (e != cudaSuccess) {
+    xfer_release(x);
+    return fail(c, FLASH_HY_ERR_CUDA, "transfer buffers: %s", cudaGetErrorString(e));
+  }
+  c->xfer = x;
+  out = x;
+  return 0;
+}
+
+static void xfer_free(flash_hy_ctx *c) {
+  if (c->xfer) xfer_release(c->xfer);
+  c->xfer = nullptr;
+}
+
+// Run worker(t, first_chunk, end_chunk) on the pool's threads, the chunks
+// (slot_cells cells each, whole blocks) split evenly into contiguous ranges;
+// returns the first CUDA error any worker saw.
+template <class F>
+static cudaError_t run_workers(flash_hy_ctx *c, XferPool *x, F worker) {
+  std::vector<cudaError_t> err(x->nthreads, cudaSuccess);
+  const size_t nch = (c->ncells + x->slot_cells - 1) / x->slot_cells;
+  auto body = [&](int t) {
+    const size_t b0 = nch * t / x->nthreads, b1 = nch * (t + 1) / x->nthreads;
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e == cudaSuccess) e = worker(t, b0, b1);
+    err[t] = e;
+  };
+  if (x->nthreads == 1) {
+    body(0);
+  } else {
+    std::vector<std::thread> th;
+    th.reserve(x->nthreads);
+    for (int t = 0; t < x->nthreads; ++t) th.emplace_back(body, t);
+    for (auto &h : th) h.join();
+  }
+  for (cudaError_t e : err)
+    if (e != cudaSuccess) return e;
+  return cudaSuccess;
+}
+
+// gather (upload) or scatter (download) the packed variables of blocks
+// [b0, b1) between the caller's UNK and a pinned slot laid out [var][cell]
+static void host_gather(const flash_hy_ctx *c, const HostLayout &L, const PackList &pl, const double *unk, size_t b0,
+                        size_t b1, double *slot) {
+  const size_t n = (b1 - b0) * c->ncb;
+  size_t t = 0;
+  for (size_t b = b0; b < b1; ++b)
+    for (int k = 0; k < c->nz; ++k)
+      for (int j = 0; j < c->ny; ++j)
+        for (int i = 0; i < c->nx; ++i, ++t) {
+          const size_t base = unk_index(L, b, i + L.ng[0], j + L.ng[1], k + L.ng[2], 0);
+          const size_t vstride = L.layout == FLASH_HY_LAYOUT_VAR_FASTEST
+                                     ? 1
+                                     : (size_t)L.nt[0] * L.nt[1] * L.nt[2];
+          for (int q = 0; q < pl.n; ++q) slot[(size_t)q * n + t] = unk[base + (size_t)pl.unk[q] * vstride];
+        }
+}
+static void host_scatter(const flash_hy_ctx *c, const HostLayout &L, const PackList &pl, double *unk, size_t b0,
+                         size_t b1, const double *slot) {
+  const size_t n = (b1 - b0) * c->ncb;
+  size_t t = 0;
+  for (size_t b = b0; b < b1; ++b)
+    for (int k = 0; k < c->nz; ++k)
+      for (int j = 0; j < c->ny; ++j)
+        for (int i = 0; i < c->nx; ++i, ++t) {
+          const size_t base = unk_index(L, b, i + L.ng[0], j + L.ng[1], k + L.ng[2], 0);
+          const size_t vstride = L.layout == FLASH_HY_LAYOUT_VAR_FASTEST
+                                     ? 1
+                                     : (size_t)L.nt[0] * L.nt[1] * L.nt[2];
+          for (int q = 0; q < pl.n; ++q) unk[base + (size_t)pl.unk[q] * vstride] = slot[(size_t)q * n + t];
+        }
+}
+
 extern "C" int flash_hy_upload(flash_hy_ctx *c, const double *unk, int layout, int nunk, const flash_hy_varmap *vm) {
   if (!c || !unk) return FLASH_HY_ERR_BAD_ARG;
   HostLayout L;
   int rc = make_layout(c, layout, nunk, vm, c->host_ng, L);
   if (rc) return fail(c, rc, "bad UNK layout or variable map%s", "");
   CUDA_OK(c, cudaSetDevice(c->device));
-  size_t bytes = (size_t)c->nblocks * L.nt[0] * L.nt[1] * L.nt[2] * nunk * sizeof(double);
-  if ((rc = ensure_stage(c, bytes))) return rc;
-  CUDA_OK(c, cudaMemcpyAsync(c->d_stage, unk, bytes, cudaMemcpyHostToDevice, c->stream));
+  const PackList pl = pack_list(c, L, true);
+  if ((rc = ensure_stage(c, (size_t)(10 + c->nsp) * c->ncells * sizeof(double)))) return rc;
+  XferPool *x = nullptr;
+  if ((rc = xfer_pool(c, x))) return rc;
+  double *st = (double *)c->d_stage;
+  CUDA_OK(c, cudaEventRecord(x->start, c->stream));   // earlier users of the stage buffer
+  const size_t spb = x->slot_cells / c->ncb;           // blocks per chunk
+  cudaError_t e = run_workers(c, x, [&](int t, size_t k0, size_t k1) -> cudaError_t {
+    cudaError_t r = cudaStreamWaitEvent(x->st[t], x->start, 0);
+    int s = 0;
+    for (size_t k = k0; k < k1 && r == cudaSuccess; ++k, s ^= 1) {
+      const size_t a = k * spb, a1 = a + spb < (size_t)c->nblocks ? a + spb : (size_t)c->nblocks;
+      const size_t n = (a1 - a) * c->ncb;
+      double *slot = x->pinned + ((size_t)t * 2 + s) * x->slot_doubles;
+      r = cudaEventSynchronize(x->ev[t][s]);        // the slot's previous copy is done
+      if (r != cudaSuccess) break;
+      host_gather(c, L, pl, unk, a, a1, slot);
+      r = cudaMemcpyAsync(st + a * c->ncb * pl.n, slot, n * pl.n * sizeof(double), cudaMemcpyHostToDevice, x->st[t]);
+      if (r == cudaSuccess) r = cudaEventRecord(x->ev[t][s], x->st[t]);
+    }
+    if (r == cudaSuccess) r = cudaEventRecord(x->done[t], x->st[t]);
+    return r;
+  });
+  if (e != cudaSuccess) return fail(c, FLASH_HY_ERR_CUDA, "upload copies: %s", cudaGetErrorString(e));
+  for (int t = 0; t < x->nthreads; ++t) CUDA_OK(c, cudaStreamWaitEvent(c->stream, x->done[t], 0));
   DevParams P;
   fill_devparams(c, P);
   for (int v = 0; v < 5; ++v) P.s_out[v] = c->state[c->cur][v];
   if (c->nsp > 0) P.sp_out = c->spec[c->cur];
-  k_unpack<<<(unsigned)((c->ncells + 255) / 256), 256, 0, c->stream>>>((const double *)c->d_stage, L, P, c->nx, c->ny,
-                                                                       c->nz, c->ncells);
+  k_unpack_soa<<<(unsigned)((c->ncells + 255) / 256), 256, 0, c->stream>>>(st, pl, P, c->ncells, x->slot_cells);
   CUDA_OK(c, cudaGetLastError());
+  // the pinned slots are reused by the next transfer only after its event waits
   c->dt_valid = 0;
   return 0;
 }
@@ -733,22 +919,42 @@ extern "C" int flash_hy_download(flash_hy_ctx *c, double *unk, int layout, int n
   int rc = make_layout(c, layout, nunk, vm, c->host_ng, L);
   if (rc) return fail(c, rc, "bad UNK layout or variable map%s", "");
   CUDA_OK(c, cudaSetDevice(c->device));
-  size_t bytes = (size_t)c->nblocks * L.nt[0] * L.nt[1] * L.nt[2] * nunk * sizeof(double);
-  if ((rc = ensure_stage(c, bytes))) return rc;
-  bool full = (L.ng[0] == 0) && (L.v_dens >= 0);
-  // Variables we do not own (and guard cells) keep the caller's values.
-  int owned = 0;
-  for (int q = 0; q < 10; ++q) owned += (&L.v_dens)[q] >= 0;
-  if (L.v_spec >= 0) owned += c->nsp;
-  if (!(full && owned == nunk)) CUDA_OK(c, cudaMemcpyAsync(c->d_stage, unk, bytes, cudaMemcpyHostToDevice, c->stream));
+  const PackList pl = pack_list(c, L, false);
+  if ((rc = ensure_stage(c, (size_t)(10 + c->nsp) * c->ncells * sizeof(double)))) return rc;
+  XferPool *x = nullptr;
+  if ((rc = xfer_pool(c, x))) return rc;
   if (c->amr && amr_restrict_all(c)) return fail(c, FLASH_HY_ERR_CUDA, "restriction launch%s", "");
+  double *st = (double *)c->d_stage;
   DevParams P;
   fill_devparams(c, P);
-  k_pack<<<(unsigned)((c->ncells + 255) / 256), 256, 0, c->stream>>>((double *)c->d_stage, L, P, c->nx, c->ny, c->nz,
-                                                                     c->ncells);
+  k_pack_soa<<<(unsigned)((c->ncells + 255) / 256), 256, 0, c->stream>>>(st, pl, P, (int)c->ncb, c->ncells,
+                                                                         x->slot_cells);
   CUDA_OK(c, cudaGetLastError());
-  CUDA_OK(c, cudaMemcpyAsync(unk, c->d_stage, bytes, cudaMemcpyDeviceToHost, c->stream));
-  CUDA_OK(c, cudaStreamSynchronize(c->stream));
+  CUDA_OK(c, cudaEventRecord(x->start, c->stream));
+  const size_t spb = x->slot_cells / c->ncb;
+  const size_t nb = (size_t)c->nblocks;
+  cudaError_t e = run_workers(c, x, [&](int t, size_t k0, size_t k1) -> cudaError_t {
+    cudaError_t r = cudaStreamWaitEvent(x->st[t], x->start, 0);
+    // copy chunk k + 1 while chunk k is scattered
+    auto issue = [&](size_t k, int s) -> cudaError_t {
+      const size_t a = k * spb, a1 = a + spb < nb ? a + spb : nb, n = (a1 - a) * c->ncb;
+      double *slot = x->pinned + ((size_t)t * 2 + s) * x->slot_doubles;
+      const cudaError_t q2 = cudaMemcpyAsync(slot, st + a * c->ncb * pl.n, n * pl.n * sizeof(double),
+                                             cudaMemcpyDeviceToHost, x->st[t]);
+      return q2 == cudaSuccess ? cudaEventRecord(x->ev[t][s], x->st[t]) : q2;
+    };
+    int s = 0;
+    if (r == cudaSuccess && k0 < k1) r = issue(k0, 0);
+    for (size_t k = k0; k < k1 && r == cudaSuccess; ++k, s ^= 1) {
+      if (k + 1 < k1) r = issue(k + 1, s ^ 1);
+      if (r == cudaSuccess) r = cudaEventSynchronize(x->ev[t][s]);
+      if (r != cudaSuccess) break;
+      const size_t a = k * spb, a1 = a + spb < nb ? a + spb : nb;
+      host_scatter(c, L, pl, unk, a, a1, x->pinned + ((size_t)t * 2 + s) * x->slot_doubles);
+    }
+    return r;
+  });
+  if (e != cudaSuccess) return fail(c, FLASH_HY_ERR_CUDA, "download copies: %s", cudaGetErrorString(e));
   return 0;
 }
 
