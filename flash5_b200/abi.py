@@ -159,6 +159,7 @@ def _set_sigs(lib):
         "flash_hy_set_exchange": (C.c_int, [vp, C.c_int, ip, C.c_int, ip]),
         "flash_hy_pack": (C.c_int, [vp, vp]),
         "flash_hy_unpack": (C.c_int, [vp, vp]),
+        "flash_hy_step_phase": (C.c_int, [vp, C.c_double, C.c_double, C.c_double, C.c_int]),
         "flash_hy_compute_fluxes": (C.c_int, [vp, C.c_int, ip, C.c_double, C.c_int]),
         "flash_hy_get_fluxes": (C.c_int, [vp, C.c_int, C.c_int, dp]),
         "flash_hy_put_fluxes": (C.c_int, [vp, C.c_int, C.c_int, dp]),

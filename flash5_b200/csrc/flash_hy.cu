@@ -75,9 +75,15 @@ struct flash_hy_ctx {
   double *d_lh, *d_gp, *d_pe, *d_freg;
   // a rank's share of a sharded grid: owned blocks and the ghost exchange
   bool partial;
-  int *h_blk_at;               // host copy of the block table (partial grids)
+  int *h_blk_at;               // host copy of the block table (uniform grids)
   int *d_owned, n_owned;       // blocks the step advances
   int *d_owned_mask;           // 1 for owned blocks (dt reduction)
+  int *h_owned, *h_recv;       // host copies of the owned and received (ghost) lists
+  int n_recv_h;
+  int *d_inner, n_inner;       // owned blocks whose guard cells come from owned blocks only
+  int *d_edge, n_edge;         // the other owned blocks (they read ghost blocks)
+  int phase_pending;           // flash_hy_step_phase: phase 1 enqueued, phase 2 due
+  double phase_dt;
   int *d_send, n_send, *d_recv, n_recv;  // blocks packed for / unpacked from other ranks
   double *d_fstore;            // stored fluxes of the split step
   double *d_sp_fstore;         // and their species fluxes
@@ -456,7 +462,7 @@ extern "C" int flash_hy_create(const flash_hy_params *params, const flash_hy_gri
   c->ndim = g->ndim; c->nx = g->nxb; c->ny = ny; c->nz = nz;
   c->nblocks = g->nblocks; c->nbx = nbx; c->nby = nby; c->nbz = nbz;
   c->partial = partial;
-  if (partial) {
+  if (!amr) {
     c->h_blk_at = (int *)malloc(at.size() * sizeof(int));
     memcpy(c->h_blk_at, at.data(), at.size() * sizeof(int));
   }
@@ -608,6 +614,8 @@ extern "C" int flash_hy_destroy(flash_hy_ctx *c) {
   ctx_free(c->d_leaves); ctx_free(c->d_lh); ctx_free(c->d_gp); ctx_free(c->d_pe); ctx_free(c->d_freg);
   for (int l = 0; l < 17; ++l) { ctx_free(c->d_lev_leaves[l]); ctx_free(c->d_lev_parents[l]); }
   ctx_free(c->d_owned); ctx_free(c->d_owned_mask); ctx_free(c->d_send); ctx_free(c->d_recv);
+  ctx_free(c->d_inner); ctx_free(c->d_edge);
+  free(c->h_owned); free(c->h_recv);
   ctx_free(c->d_fstore);
   ctx_free(c->d_sp_fstore);
   for (int s = 0; s < 2; ++s) ctx_free(c->spec[s]);
@@ -1117,6 +1125,34 @@ extern "C" int flash_hy_step(flash_hy_ctx *c, double simTime, double dt, double 
   }
   c->cur = 1 - c->cur;
   c->dt_valid = 1;
+  return 0;
+}
+
+extern "C" int flash_hy_step_phase(flash_hy_ctx *c, double simTime, double dt, double dtOld, int phase) {
+  (void)simTime; (void)dtOld;
+  if (!c || (phase != 1 && phase != 2)) return FLASH_HY_ERR_BAD_ARG;
+  if (c->n_owned == 0)
+    return fail(c, FLASH_HY_ERR_UNSUPPORTED, "step_phase needs a rank's owned blocks (flash_hy_set_owned_blocks)%s", "");
+  if (!(dt > 0.0)) return fail(c, FLASH_HY_ERR_NONPOS_DT, "dt must be positive%s", "");
+  if (phase == 2 && (!c->phase_pending || dt != c->phase_dt))
+    return fail(c, FLASH_HY_ERR_BAD_ARG, "step_phase 2 must follow phase 1 with the same dt%s", "");
+  if (phase == 1 && c->phase_pending)
+    return fail(c, FLASH_HY_ERR_BAD_ARG, "step_phase 1 twice without phase 2%s", "");
+  CUDA_OK(c, cudaSetDevice(c->device));
+  const int *list = phase == 1 ? c->d_inner : c->d_edge;
+  const int n = phase == 1 ? c->n_inner : c->n_edge;
+  if (n > 0) {
+    const int rc = enqueue_step(c, dt, list, n);
+    if (rc) return rc;
+  }
+  if (phase == 1) {
+    c->phase_pending = 1;
+    c->phase_dt = dt;
+  } else {
+    c->phase_pending = 0;
+    c->cur = 1 - c->cur;
+    c->dt_valid = 1;
+  }
   return 0;
 }
 
@@ -1727,6 +1763,53 @@ extern "C" int flash_hy_harvest_fetch(flash_hy_ctx *c, double *d_states, long lo
 // ---------------------------------------------------------------------------
 // sharded grids: owned blocks and the ghost-block exchange
 // ---------------------------------------------------------------------------
+// Split the owned blocks into those whose 26 neighbours (boundary rules
+// applied) are all owned -- their step may run while the ghost blocks are in
+// transit -- and the others, which read a received ghost block.
+static int split_owned(flash_hy_ctx *c) {
+  cudaFree(c->d_inner); cudaFree(c->d_edge);
+  c->d_inner = c->d_edge = nullptr;
+  c->n_inner = c->n_edge = 0;
+  if (!c->n_owned) return 0;
+  std::vector<char> ghost(c->nblocks, 0);
+  for (int q = 0; q < c->n_recv_h; ++q) ghost[c->h_recv[q]] = 1;
+  std::vector<int> coords(3 * (size_t)c->nblocks), inner, edge;
+  CUDA_OK(c, cudaMemcpy(coords.data(), c->d_blk_coord, coords.size() * sizeof(int), cudaMemcpyDeviceToHost));
+  const int nbl[3] = {c->nbx, c->nby, c->nbz};
+  for (int q = 0; q < c->n_owned; ++q) {
+    const int b = c->h_owned[q];
+    const int *cc = &coords[3 * (size_t)b];
+    bool touches = false;
+    for (int o = 0; o < 27 && !touches; ++o) {
+      int off[3] = {o % 3 - 1, (o / 3) % 3 - 1, o / 9 - 1}, p[3];
+      bool ok = true;
+      for (int d = 0; d < 3; ++d) {
+        if (d >= c->ndim) { if (off[d]) ok = false; p[d] = 0; continue; }
+        p[d] = cc[d] + off[d];
+        if (p[d] < 0 || p[d] >= nbl[d]) {
+          if (c->bc[2 * d] != FLASH_HY_BC_PERIODIC) { p[d] = cc[d]; continue; }
+          p[d] = (p[d] + nbl[d]) % nbl[d];
+        }
+      }
+      if (!ok) continue;
+      const int nb = c->h_blk_at ? c->h_blk_at[((size_t)p[2] * c->nby + p[1]) * c->nbx + p[0]] : -1;
+      if (nb >= 0 && ghost[nb]) touches = true;
+    }
+    (touches ? edge : inner).push_back(b);
+  }
+  if (!inner.empty()) {
+    CUDA_OK(c, cudaMalloc((void **)&c->d_inner, inner.size() * sizeof(int)));
+    CUDA_OK(c, cudaMemcpy(c->d_inner, inner.data(), inner.size() * sizeof(int), cudaMemcpyHostToDevice));
+  }
+  if (!edge.empty()) {
+    CUDA_OK(c, cudaMalloc((void **)&c->d_edge, edge.size() * sizeof(int)));
+    CUDA_OK(c, cudaMemcpy(c->d_edge, edge.data(), edge.size() * sizeof(int), cudaMemcpyHostToDevice));
+  }
+  c->n_inner = (int)inner.size();
+  c->n_edge = (int)edge.size();
+  return 0;
+}
+
 extern "C" int flash_hy_set_owned_blocks(flash_hy_ctx *c, int n, const int *list) {
   if (!c || n <= 0 || !list || c->amr) return fail(c, FLASH_HY_ERR_BAD_ARG, "set_owned_blocks: %s", "bad arguments");
   std::vector<int> mask(c->nblocks, 0);
@@ -1769,9 +1852,14 @@ extern "C" int flash_hy_set_owned_blocks(flash_hy_ctx *c, int n, const int *list
   CUDA_OK(c, cudaMemcpy(c->d_owned, list, n * sizeof(int), cudaMemcpyHostToDevice));
   CUDA_OK(c, cudaMemcpy(c->d_owned_mask, mask.data(), c->nblocks * sizeof(int), cudaMemcpyHostToDevice));
   c->n_owned = n;
+  free(c->h_owned);
+  c->h_owned = (int *)malloc((size_t)n * sizeof(int));
+  if (!c->h_owned) return fail(c, FLASH_HY_ERR_CUDA, "host allocation%s", "");
+  memcpy(c->h_owned, list, (size_t)n * sizeof(int));
   c->dt_valid = 0;
+  c->phase_pending = 0;
   drop_graphs(c);
-  return 0;
+  return split_owned(c);
 }
 
 extern "C" int flash_hy_set_exchange(flash_hy_ctx *c, int nsend, const int *send, int nrecv, const int *recv) {
@@ -1796,7 +1884,13 @@ extern "C" int flash_hy_set_exchange(flash_hy_ctx *c, int nsend, const int *send
   }
   c->n_send = nsend;
   c->n_recv = nrecv;
-  return 0;
+  free(c->h_recv);
+  c->h_recv = (int *)malloc((size_t)(nrecv > 0 ? nrecv : 1) * sizeof(int));
+  if (!c->h_recv) return fail(c, FLASH_HY_ERR_CUDA, "host allocation%s", "");
+  if (nrecv) memcpy(c->h_recv, recv, (size_t)nrecv * sizeof(int));
+  c->n_recv_h = nrecv;
+  c->phase_pending = 0;
+  return split_owned(c);
 }
 
 // buf[i][v][cell] <-> state[v][list[i] * ncb + cell], one CTA per listed block

@@ -230,6 +230,11 @@ class Hydro:
     def unpack(self, buf):
         self._check(self.lib.flash_hy_unpack(self.ctx, C.c_void_p(_addr(buf))))
 
+    def step_phase(self, simTime, dt, dtOld, phase):
+        """A rank's step in two phases (1: owned blocks that read no ghost
+        block, 2: the rest, after unpack; see flash_hy_step_phase)."""
+        self._check(self.lib.flash_hy_step_phase(self.ctx, simTime, dt, dtOld, int(phase)))
+
     # -- exact Riemann solver: learned guess and its training data ---------
     def set_guess_weights(self, w):
         """Attach the learned star-pressure guess (FP32 master weights, the

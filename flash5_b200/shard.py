@@ -141,13 +141,17 @@ class ShardedHydro:
 
     The ghost blocks travel as device buffers: `pack` gathers the blocks
     other ranks need (one kernel on the context's stream), the buffers move
-    rank to rank (NCCL point-to-point sends through torch.distributed in
-    `exchange`, or any other transport through `send_views` / `recv_views`),
-    `unpack` scatters the received blocks into the ghost slots.  The step
-    then advances the owned blocks; `compute_dt` reduces dt over the owned
-    blocks and, with a process group, takes the MIN over ranks."""
+    rank to rank (NCCL point-to-point sends through torch.distributed, or
+    pinned host copies over a gloo group, or any other transport through
+    `send_views` / `recv_views`), `unpack` scatters the received blocks into
+    the ghost slots.  With a process group the step overlaps the exchange
+    (`overlap`, the default): the owned blocks that read no ghost block
+    advance while the messages are in flight (flash_hy_step_phase 1), the
+    others after the unpack (phase 2).  `compute_dt` reduces dt over the
+    owned blocks and, with a process group, does Driver_computeDt's
+    MPI_MINLOC over the ranks."""
 
-    def __init__(self, params, grid, nranks, rank, device=0, dist=None):
+    def __init__(self, params, grid, nranks, rank, device=0, dist=None, overlap=True):
         import torch
         from .hydro import Hydro
         self.torch, self.dist, self.device = torch, dist, device
@@ -177,6 +181,17 @@ class ShardedHydro:
                 self.recv_views[r] = self.rbuf[off * per:(off + k) * per]
             off += k
         self._tstream = torch.cuda.ExternalStream(self.h.stream, device=dev)
+        self.overlap = overlap
+        # gloo carries CPU tensors: the ghost buffers go through pinned host copies
+        self.host_transport = dist is not None and dist.get_backend() == "gloo"
+        self.coll_device = torch.device("cpu") if self.host_transport else dev
+        if self.host_transport:
+            self.sbuf_h = torch.empty(self.sbuf.numel(), dtype=torch.float64, pin_memory=True)
+            self.rbuf_h = torch.empty(self.rbuf.numel(), dtype=torch.float64, pin_memory=True)
+            self.send_views_h = {r: self.sbuf_h[v.storage_offset():v.storage_offset() + v.numel()]
+                                 for r, v in self.send_views.items()}
+            self.recv_views_h = {r: self.rbuf_h[v.storage_offset():v.storage_offset() + v.numel()]
+                                 for r, v in self.recv_views.items()}
 
     def upload(self, unk_global):
         """Upload this rank's blocks (owned + ghosts) taken from a global UNK
@@ -191,22 +206,52 @@ class ShardedHydro:
     def unpack(self):
         self.h.unpack(self.rbuf)
 
-    def exchange(self):
-        """Ghost exchange over the process group (NCCL point-to-point)."""
+    def post_exchange(self):
+        """Pack the blocks other ranks need and post the point-to-point
+        messages; returns the pending requests (finish_exchange completes
+        them).  NCCL: device buffers, the messages run on NCCL's stream after
+        the pack.  gloo: the packed buffer is copied to pinned host memory
+        first."""
         torch, dist = self.torch, self.dist
         self.pack()
         cur = torch.cuda.current_stream(self.device)
         cur.wait_stream(self._tstream)
-        ops = [dist.P2POp(dist.isend, v, r) for r, v in self.send_views.items()]
-        ops += [dist.P2POp(dist.irecv, v, r) for r, v in self.recv_views.items()]
-        if ops:
-            for w in dist.batch_isend_irecv(ops):
-                w.wait()
+        if self.host_transport:
+            # the copies run on torch's own stream: the pinned buffers' cached
+            # blocks must never refer to the context's stream, which dies with it
+            self.sbuf_h.copy_(self.sbuf, non_blocking=True)
+            cur.synchronize()
+            sv, rv = self.send_views_h, self.recv_views_h
+        else:
+            sv, rv = self.send_views, self.recv_views
+        ops = [dist.P2POp(dist.isend, v, r) for r, v in sv.items()]
+        ops += [dist.P2POp(dist.irecv, v, r) for r, v in rv.items()]
+        return dist.batch_isend_irecv(ops) if ops else []
+
+    def finish_exchange(self, reqs):
+        """Complete the messages and unpack the ghost blocks (ordered on the
+        context's stream after whatever it already holds)."""
+        torch = self.torch
+        for w in reqs:
+            w.wait()
+        cur = torch.cuda.current_stream(self.device)
+        if self.host_transport:
+            self.rbuf.copy_(self.rbuf_h, non_blocking=True)
         self._tstream.wait_stream(cur)
         self.unpack()
 
+    def exchange(self):
+        """Ghost exchange over the process group, blocking."""
+        self.finish_exchange(self.post_exchange())
+
     def __call__(self, simTime, dt, dtOld, sweepOrder=0):
         if self.nranks > 1 and self.dist is not None:
+            if self.overlap:
+                reqs = self.post_exchange()
+                self.h.step_phase(simTime, dt, dtOld, 1)     # blocks that read no ghost block
+                self.finish_exchange(reqs)
+                self.h.step_phase(simTime, dt, dtOld, 2)
+                return
             self.exchange()
         self.h(simTime, dt, dtOld, sweepOrder)
 
@@ -219,7 +264,7 @@ class ShardedHydro:
         loc = loc[:5] + (int(self.plan.local[loc[5]]) if loc[5] >= 0 else -1,)
         if self.nranks > 1 and self.dist is not None:
             torch, dist = self.torch, self.dist
-            dev = torch.device("cuda", self.device)
+            dev = self.coll_device
             t = torch.tensor([dt], dtype=torch.float64, device=dev)
             dist.all_reduce(t, op=dist.ReduceOp.MIN)
             gdt = float(t.item())
@@ -236,8 +281,11 @@ class ShardedHydro:
 
     @property
     def last_launch_count(self):
-        """Launches of the last step, the ghost pack and unpack included."""
-        return self.h.last_launch_count + (2 if self.nranks > 1 and self.dist is not None else 0)
+        """Launches of the last step, the ghost pack and unpack included
+        (an overlapped step launches the step's kernels once per phase)."""
+        if self.nranks > 1 and self.dist is not None:
+            return self.h.last_launch_count * (2 if self.overlap else 1) + 2
+        return self.h.last_launch_count
 
     def download_owned(self):
         """UNK of the owned blocks (local order = Morton order) and their

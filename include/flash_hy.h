@@ -256,6 +256,15 @@ int flash_hy_set_exchange(flash_hy_ctx *ctx, int nsend, const int *send_blocks, 
                           const int *recv_blocks);
 int flash_hy_pack(flash_hy_ctx *ctx, double *d_buf);
 int flash_hy_unpack(flash_hy_ctx *ctx, const double *d_buf);
+/* The step of a rank's share in two phases, so that the ghost exchange
+ * overlaps the step (gr_shiftData.F90:100-173 exchanges first, then FLASH
+ * steps): phase 1 advances the owned blocks whose guard cells all lie in
+ * owned blocks and may run while the ghost blocks are in transit; phase 2,
+ * after flash_hy_unpack, advances the other owned blocks and completes the
+ * step (the state advances, the CFL reduction covers all owned blocks).
+ * Phase 2 must follow phase 1 with the same dt.  Results equal
+ * flash_hy_step on the same share bit for bit.                          */
+int flash_hy_step_phase(flash_hy_ctx *ctx, double simTime, double dt, double dtOld, int phase);
 
 /* ---- refinement criterion ------------------------------------------------
  * gr_estimateError / gr_estimateBlkError (Grid/GridMain/AMR/
