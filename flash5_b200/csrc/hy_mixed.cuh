@@ -160,10 +160,12 @@ struct MxGeom {
       (RS == 1 && slope_bytes < sizeof(xrs::MlpPacked)) ? sizeof(xrs::MlpPacked) : slope_bytes;
   static constexpr size_t recon_bytes = wp_off + (size_t)2 * SC * 6 * 4 + (size_t)SC * 8;
   static constexpr size_t flux_bytes = (size_t)SC * 9 * 8;
-  // + the staging barrier and the slack that aligns the tile destinations
-  // to 128 bytes
+  // + the CTA's face-state ranges (learned gate, 16 warps x 6 floats), the
+  // staging barrier and the slack that aligns the tile destinations to 128
+  // bytes
+  static constexpr size_t red_bytes = 16 * 6 * 4;
   static constexpr size_t smem_bytes() {
-    return prim_bytes + (recon_bytes > flux_bytes ? recon_bytes : flux_bytes) + 16 + 128;
+    return prim_bytes + (recon_bytes > flux_bytes ? recon_bytes : flux_bytes) + red_bytes + 16 + 128;
   }
 };
 
@@ -223,6 +225,7 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
   bool tma = NDIM == 3 && tm.on && P.lh == nullptr;
   int nbs[2] = {-1, -1};          // neighbour blocks below / above along DIR (-1: load_prim)
   unsigned long long *bar = reinterpret_cast<unsigned long long *>(smem_raw + G::smem_bytes() - 16 - 128);
+  float *sRed = reinterpret_cast<float *>(smem_raw + G::smem_bytes() - 16 - 128 - G::red_bytes);
   if (tma) {
     const int ext[3] = {P.nbx, P.nby, P.nbz};
 #pragma unroll
@@ -338,6 +341,9 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
   __syncthreads();
 
   // ---- C: face states of the line cells [-1, N] as increments
+  // (exact solver with a network: the ranges of the face states' pressure,
+  // density and normal velocity over the CTA, for the learned gate's bound)
+  float rg[6] = {3.0e38f, -3.0e38f, 3.0e38f, -3.0e38f, 3.0e38f, -3.0e38f};   // p, rho, u: min, max
   for (int t = threadIdx.x; t < G::SC; t += NT) {
     int x, l, i, j, k;
     G::dec(t, G::LC, 1, x, l);
@@ -514,6 +520,29 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
     }
     // 1/(game-1) of the cell: game - 1 = p/(e rho) (Eos_putData.F90:105-106)
     sIg[t] = (Vs(5, s) * rc) / pc;
+    if (RS == 1 && P.mlp) {
+      const float fp = float(pc), fr = float(rc), fu = float(Vs(v1, s));
+      const float q6[6] = {fp + dWm[HP], fp + dWp[HP], fr + dWm[HD], fr + dWp[HD], fu + dWm[v1], fu + dWp[v1]};
+#pragma unroll
+      for (int m = 0; m < 3; ++m) {
+        rg[2 * m] = fminf(rg[2 * m], fminf(q6[2 * m], q6[2 * m + 1]));
+        rg[2 * m + 1] = fmaxf(rg[2 * m + 1], fmaxf(q6[2 * m], q6[2 * m + 1]));
+        // NaN anywhere keeps the gate open
+        if (q6[2 * m] != q6[2 * m] || q6[2 * m + 1] != q6[2 * m + 1]) rg[2 * m] = -3.0e38f;
+      }
+    }
+  }
+  if (RS == 1 && P.mlp) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+      for (int m = 0; m < 3; ++m) {
+        rg[2 * m] = fminf(rg[2 * m], __shfl_xor_sync(0xffffffffu, rg[2 * m], o));
+        rg[2 * m + 1] = fmaxf(rg[2 * m + 1], __shfl_xor_sync(0xffffffffu, rg[2 * m + 1], o));
+      }
+    if ((threadIdx.x & 31) == 0)
+#pragma unroll
+      for (int m = 0; m < 6; ++m) sRed[(threadIdx.x >> 5) * 6 + m] = rg[m];
   }
   __syncthreads();
 
@@ -528,7 +557,27 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
     // 2 runs Newton and the Godunov flux.  Each thread reads back only its
     // own entries.
     double *sP0 = sIg;
-    const bool learned = P.mlp != nullptr;
+    // The CTA-wide bound: every face has p_min >= P_lo, p_max <= P_hi and a
+    // PVRS estimate ppv <= P_hi + 0.5 (U_hi - U_lo) rho_hi c_hi with c_hi =
+    // sqrt(gamma P_hi / rho_lo); strong_waves needs max(p_max, ppv) >= 2
+    // p_min, so below 2 P_lo (a 1e-4 margin covers the FP32 rounding) no
+    // face of the CTA consults the network and the gate pass is skipped:
+    // the same decisions, and results, as testing every face.
+    bool learned = P.mlp != nullptr;
+    if (learned) {
+      float r[6] = {3.0e38f, -3.0e38f, 3.0e38f, -3.0e38f, 3.0e38f, -3.0e38f};
+      for (int w = 0; w < NT / 32; ++w)
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+          r[2 * m] = fminf(r[2 * m], sRed[w * 6 + 2 * m]);
+          r[2 * m + 1] = fmaxf(r[2 * m + 1], sRed[w * 6 + 2 * m + 1]);
+        }
+      const float chi = sqrtf(float(P.gamma) * r[1] / r[2]);
+      const float bound = r[1] + 0.5f * (r[5] - r[4]) * r[3] * chi;
+      const bool finite = r[0] > 1e-30f && r[1] < 1e30f && r[2] > 1e-30f && r[3] < 1e30f && r[4] > -1e30f &&
+                          r[5] < 1e30f && bound < 1e30f;
+      if (finite && bound < 2.f * r[0] * (1.f - 1e-4f)) learned = false;
+    }
     const double g = P.gamma;
     const xrs::Gas &gas = P.gas;             // from the parameter block
     // s: staged index of the face's right cell, sl: of its left cell
