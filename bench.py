@@ -50,19 +50,18 @@ UNIT = "zone-updates/s"
 BYTES_PER_ZONE = 80.0          # read + write of 5 FP64 state variables
 # DRAM bytes per zone-update of one step (k_sig + the three direction
 # kernels) from ncu captures of the 160^3 KH step (dram__bytes_read.sum +
-# dram__bytes_write.sum), scaled to the workload by its zone count
-# (traffic grows in proportion): HLLC 3,539 MB, exact solver 3,459 MB for
-# 4.096e6 zones
-TRAFFIC_PER_ZONE = {"mixed": 864.0, "mixed_exact": 844.0, "mixed_learned": 844.0}
+# dram__bytes_write.sum over 4.096e6 zones), scaled to the workload by its
+# zone count (traffic grows in proportion)
+TRAFFIC_PER_ZONE = {"fp64": 1248.6, "mixed": 866.7, "mixed_exact": 841.6, "mixed_learned": 841.6}
 # Floating-point operations per zone-update of one step (k_sig + the three
 # direction kernels), counted by ncu on the 96^3 KH step:
 # smsp__sass_thread_inst_executed_op_{dadd,dmul,dfma,fadd,fmul,ffma}_pred_on
 # (an FMA counts two), divided by the zones; and the FP64 pipe utilisation
 # (sm__pipe_fp64_cycles_active, % of peak over the kernels' active cycles).
 FLOPS_PER_ZONE = {"fp64": {"f64": 7629, "f32": 395, "fp64_pipe_pct": 26.5},
-                  "mixed": {"f64": 1337, "f32": 3374, "fp64_pipe_pct": 9.3},
-                  "mixed_exact": {"f64": 2266, "f32": 3416, "fp64_pipe_pct": 13.8},
-                  "mixed_learned": {"f64": 2266, "f32": 3416, "fp64_pipe_pct": 13.8}}
+                  "mixed": {"f64": 1313, "f32": 2322, "fp64_pipe_pct": 13.9},
+                  "mixed_exact": {"f64": 2243, "f32": 2368, "fp64_pipe_pct": 17.9},
+                  "mixed_learned": {"f64": 2243, "f32": 2368, "fp64_pipe_pct": 17.9}}
 # nominal vector peaks of a B200 at the 1965 MHz maximum SM clock: 148 SMs x
 # 64 FP64 (128 FP32) FMA lanes x 2 flops; no measured FP64/FP32 peak exists
 # for this pool, so the compute fractions are "of nominal"
@@ -498,7 +497,28 @@ def riemann_run(args, n=None, steps=None, warmup=None):
         res["learned" if learned else "two_rarefaction"] = {
             "solves_per_s": n / (ms * 1e-3), "ms": ms, "mean_iters": float(it[ok].mean()), "iter_hist": hist,
             "fallback_frac": float(((fl & 1) != 0)[ok].mean()), "nonconverged": int(((fl & 4) != 0).sum()),
-            "vacuum": int((~ok).sum()), "pstar": out[0].clone()}
+            "vacuum": int((~ok).sum()), "pstar": out[0].clone(), "_it": it, "_fl": fl}
+    # where the network was consulted (strong waves, inexact two-rarefaction
+    # guess): evaluations of both starts on those solves
+    cons = (res["learned"]["_fl"] & 8) != 0
+    for k in res:
+        it = res[k].pop("_it")
+        res[k].pop("_fl")
+        res[k]["mean_iters_where_consulted"] = float(it[cons].mean()) if cons.any() else None
+    consulted_frac = float(cons.mean())
+    # the network alone, dense over every pair: features + 8-64-64-1 BF16
+    # inference (what the learned start costs per consulted solve at best)
+    for _ in range(max(1, warmup)):
+        yv = r.predict(S)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        yv = r.predict(S)
+    e1.record(stream)
+    e1.synchronize()
+    predict_ms = e0.elapsed_time(e1) / steps
+    del yv
     p0, p1 = res["two_rarefaction"].pop("pstar"), res["learned"].pop("pstar")
     okd = torch.tensor(ok, device=p0.device)
     rel = ((p1 - p0).abs() / p0.clamp_min(1e-300))[okd].max().item()
@@ -514,7 +534,10 @@ def riemann_run(args, n=None, steps=None, warmup=None):
                                    "1e-3..1e3, u uniform +-5 c, gamma in {1.4, 5/3}; MLP 8-64-64-1 BF16 on tensor "
                                    "cores (mma.sync)"},
             "paths": res, "speedup_vs_two_rarefaction": res["two_rarefaction"]["ms"] / res["learned"]["ms"],
-            "max_rel_pstar_diff_learned_vs_tr": rel,
+            "max_rel_pstar_diff_learned_vs_tr": rel, "consulted_frac": consulted_frac,
+            "network_dense_ms": predict_ms,
+            "network_dense_note": "k_predict over every pair (features + tensor-core MLP, written out): the network's "
+                                  "own cost per solve, against the Newton evaluations it saves where consulted",
             "training": {"samples": ns, "epochs": 8, "final_mse": loss, "seconds": train_s}}
 
 
@@ -591,8 +614,9 @@ def amr_run(args, paths, e2e=True, regrid=True, cpu=True, steps=None, warmup=Non
             h, g_new = update_refinement(h, g, ("dens", "pres"), 0.8, 0.2, 0.01, timings=tm)
             regrid_info = {"estimate_one_var_ms": 1e3 * min(est), "nodes": g.nblocks,
                            "cycle": {k: (round(v * 1e3, 3) if k.endswith("_s") else v) for k, v in tm.items()},
-                           "cycle_units": "ms (estimate: dens + pres on the device, mark_and_tree: host, "
-                                          "data: new context + device regrid)",
+                           "cycle_units": "ms (mark_and_tree: estimator of dens + pres, marks and new tree, all on "
+                                          "the device; grid: host descriptors of the new tree; data: new context + "
+                                          "device regrid)",
                            "new_leaves": int(g_new.nleaves), "old_leaves": int(g.nleaves),
                            "cutoffs": {"refine": 0.8, "derefine": 0.2, "filter": 0.01}}
         h.close()
@@ -669,6 +693,9 @@ def riemann_summary(line):
             "solves_per_s": {n: v["solves_per_s"] for n, v in p.items()},
             "mean_newton_evaluations": {n: v["mean_iters"] for n, v in p.items()},
             "fallback_frac_learned": p["learned"]["fallback_frac"],
+            "consulted_frac": line["consulted_frac"],
+            "mean_newton_evaluations_where_consulted": {n: v["mean_iters_where_consulted"] for n, v in p.items()},
+            "network_dense_ms": line["network_dense_ms"],
             "speedup_learned_vs_two_rarefaction": line["speedup_vs_two_rarefaction"],
             "max_rel_pstar_diff_learned_vs_tr": line["max_rel_pstar_diff_learned_vs_tr"]}
 

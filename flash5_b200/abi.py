@@ -167,6 +167,8 @@ def _set_sigs(lib):
         "flash_hy_estimate_error": (C.c_int, [vp, C.c_int, C.c_double, dp]),
         "flash_hy_regrid": (C.c_int, [vp, vp, C.c_int, ip, ip]),
         "flash_hy_refine_tree": (C.c_int, [G, vp, vp, C.c_int, C.c_int, ip, ip, ip, ip, ip, ip]),
+        "flash_hy_mark_refine_tree": (C.c_int, [vp, C.c_int, ip, C.c_double, dp, dp, C.c_int, C.c_int, C.c_int, ip,
+                                                ip, ip, ip, ip, ip]),
         "flash_hy_get_tuning": (C.c_int, [vp, C.POINTER(Tuning)]),
         "flash_hy_set_tuning": (C.c_int, [vp, C.POINTER(Tuning)]),
         "flash_hy_tuning_candidates": (C.c_int, [vp, ip, ip, ip, ip, ip, ip]),

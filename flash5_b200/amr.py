@@ -488,26 +488,29 @@ def regrid(grid, refine, derefine, min_level=1):
 def update_refinement(h, grid, refine_vars=("dens", "pres"), refine_cutoff=0.8, derefine_cutoff=0.2,
                       refine_filter=0.01, min_level=1, timings=None):
     """Grid_markRefineDerefine + Grid_updateRefinement on a device context:
-    the estimator of every refinement variable on the device, the marks and
-    the new tree on the host, the data of the new tree on the device.
+    the estimator of every refinement variable, the marks and the new tree
+    on the device (flash_hy_mark_refine_tree), the new grid's descriptors on
+    the host, the data of the new tree on the device (flash_hy_regrid).
     Returns (context, grid): the old ones when nothing changes, else a new
     context (the old one is closed) for the new grid.  `timings`, a dict,
     receives the seconds of each phase."""
     import time
     t0 = time.perf_counter()
-    errs = [h.estimate_error(v, refine_filter) for v in refine_vars]
+    lev, coords, par, src, how = h.mark_refine_tree(refine_vars, refine_filter, refine_cutoff, derefine_cutoff,
+                                                    min_level=min_level)
     t1 = time.perf_counter()
-    refine, derefine = mark_refine_derefine(grid, errs, refine_cutoff, derefine_cutoff)
-    g2, src, how = regrid_native(grid, refine, derefine, min_level=min_level)
-    t2 = time.perf_counter()
-    changed = g2.nblocks != grid.nblocks or np.any(how != 0)
+    changed = len(lev) != grid.nblocks or np.any(how != 0)
     if changed:
+        g2 = _grid_from_nodes(grid, lev, coords, par)
+        t2 = time.perf_counter()
         h2 = h.regrid(g2, src, how)
         h.close()
         h, grid = h2, g2
+    else:
+        t2 = time.perf_counter()
     t3 = time.perf_counter()
     if timings is not None:
-        timings.update(estimate_s=t1 - t0, mark_and_tree_s=t2 - t1, data_s=t3 - t2,
+        timings.update(mark_and_tree_s=t1 - t0, grid_s=t2 - t1, data_s=t3 - t2,
                        refined=int(np.count_nonzero(how == 1)), derefined=int(np.count_nonzero(how == 2)),
                        changed=bool(changed))
     return h, grid

@@ -37,6 +37,7 @@ UNITS = [
     ("spec_mx.o", "spec.cu", ["-DFHY_SPEC_MIXED", "--fmad=true"] + FP32_FAST),
     ("refine.o", "refine.cu", ["--fmad=false"]),
     ("tree.o", "tree.cu", []),
+    ("tree_dev.o", "tree_dev.cu", []),
 ]
 
 

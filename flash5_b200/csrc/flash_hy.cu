@@ -1586,6 +1586,75 @@ done:
 // ---------------------------------------------------------------------------
 // refinement criterion (gr_estimateError)
 // ---------------------------------------------------------------------------
+// the estimator of one variable for every node into the device array d_out
+static int estimate_into(flash_hy_ctx *c, int var, double refine_filter, double *d_out) {
+  CUDA_OK(c, cudaMemsetAsync(d_out, 0, (size_t)c->nblocks * sizeof(double), c->stream));
+  ErrArgs a;
+  fill_devparams(c, a.P);
+  if (c->amr && amr_prepare(c, a.P) < 0)
+    return fail(c, FLASH_HY_ERR_CUDA, "AMR guard-cell launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  a.var = var;
+  a.filter = refine_filter;
+  a.list = c->n_owned ? c->d_owned : nullptr;
+  a.n = c->n_owned ? c->n_owned : c->nblocks;
+  a.err = d_out;
+  a.stream = c->stream;
+  if (estimate_error(a, c->ndim, c->nx, c->ny, c->nz) < 0)
+    return fail(c, FLASH_HY_ERR_CUDA, "estimator launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+  return 0;
+}
+
+extern "C" int flash_hy_mark_refine_tree(flash_hy_ctx *c, int nvar, const int *vars, double refine_filter,
+                                         const double *refine_cutoff, const double *derefine_cutoff, int max_refine,
+                                         int min_level, int cap, int *new_n, int *new_levels, int *new_coords,
+                                         int *new_parent, int *src, int *how) {
+  if (!c || nvar < 1 || nvar > 16 || !vars || !refine_cutoff || !derefine_cutoff || !new_n) return FLASH_HY_ERR_BAD_ARG;
+  if (!c->amr) return fail(c, FLASH_HY_ERR_UNSUPPORTED, "mark_refine_tree needs an AMR hierarchy%s", "");
+  if (c->nlev > 15) return fail(c, FLASH_HY_ERR_UNSUPPORTED, "mark_refine_tree: at most 15 levels%s", "");
+  for (int v = 0; v < nvar; ++v)
+    if (vars[v] < FLASH_HY_REFVAR_DENS || vars[v] > FLASH_HY_REFVAR_EINT) return FLASH_HY_ERR_BAD_ARG;
+  CUDA_OK(c, cudaSetDevice(c->device));
+  double *d_err = nullptr, *d_cut = nullptr;
+  int rc = 0, trc = 0;
+  if (cudaMalloc((void **)&d_err, (size_t)nvar * c->nblocks * sizeof(double)) != cudaSuccess ||
+      cudaMalloc((void **)&d_cut, 2 * (size_t)nvar * sizeof(double)) != cudaSuccess) {
+    cudaFree(d_err);
+    return fail(c, FLASH_HY_ERR_CUDA, "mark_refine_tree allocation%s", "");
+  }
+  for (int v = 0; v < nvar && !rc; ++v) rc = estimate_into(c, vars[v], refine_filter, d_err + (size_t)v * c->nblocks);
+  if (!rc) {
+    std::vector<double> cut(2 * (size_t)nvar);
+    for (int v = 0; v < nvar; ++v) { cut[v] = refine_cutoff[v]; cut[nvar + v] = derefine_cutoff[v]; }
+    if (cudaMemcpyAsync(d_cut, cut.data(), cut.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream) !=
+        cudaSuccess)
+      rc = fail(c, FLASH_HY_ERR_CUDA, "mark_refine_tree copies%s", "");
+    else {
+      TreeArgs a;
+      a.err = d_err; a.nvar = nvar; a.nblocks = c->nblocks; a.ndim = c->ndim; a.L = c->nlev;
+      a.rc = d_cut; a.dc = d_cut + nvar;
+      a.max_refine = max_refine; a.min_level = min_level;
+      a.level = c->d_level; a.coord = c->d_blk_coord; a.leaf = c->d_leaf; a.parent = c->d_parent; a.old_at = c->d_at;
+      for (int l = 0; l < 17; ++l) {
+        a.at_off[l] = c->at_off[l];
+        for (int d = 0; d < 3; ++d) a.at_ext[l][d] = c->at_ext[l][d];
+      }
+      for (int d = 0; d < 3; ++d) a.periodic[d] = d < c->ndim && c->bc[2 * d] == FLASH_HY_BC_PERIODIC;
+      a.stream = c->stream; a.cap = cap;
+      a.new_n = new_n; a.new_levels = new_levels; a.new_coords = new_coords; a.new_parent = new_parent;
+      a.src = src; a.how = how;
+      if (cap > 0 && (!new_levels || !new_coords || !new_parent || !src || !how)) trc = -4;
+      else trc = tree_update_dev(a);
+      if (trc == -2) rc = fail(c, FLASH_HY_ERR_CUDA, "mark_refine_tree: %s", cudaGetErrorString(cudaGetLastError()));
+      else if (trc == -4) rc = fail(c, FLASH_HY_ERR_BAD_ARG, "mark_refine_tree: %s", "cap too small");
+      else if (trc) rc = fail(c, FLASH_HY_ERR_UNSUPPORTED, "mark_refine_tree: %s", "the tree rules did not settle");
+    }
+  }
+  cudaStreamSynchronize(c->stream);
+  cudaFree(d_err);
+  cudaFree(d_cut);
+  return rc;
+}
+
 extern "C" int flash_hy_estimate_error(flash_hy_ctx *c, int var, double refine_filter, double *err) {
   if (!c || !err || var < FLASH_HY_REFVAR_DENS || var > FLASH_HY_REFVAR_EINT || c->ndim < 2)
     return FLASH_HY_ERR_BAD_ARG;

@@ -84,6 +84,26 @@ struct RegridArgs {
 int regrid_fill(const RegridArgs &a, int ndim, int nx, int ny, int nz);
 size_t halo_cells(int ndim, int nx, int ny, int nz);
 
+// marking and the tree of a regrid on the device (tree_dev.cu): errors of
+// nvar refinement variables [nvar][nblocks] (device), the old tree's tables
+// (device), the new node arrays (host, capacity cap).  Returns 0, -2 (CUDA),
+// -3 (a rule did not settle), -4 (cap too small; *new_n says what is needed)
+// or -5 (the tree would need a node two levels below the old tree).
+struct TreeArgs {
+  const double *err;
+  int nvar, nblocks, ndim, L;
+  const double *rc, *dc;       // per-variable cutoffs (device)
+  int max_refine, min_level;
+  const int *level, *coord, *leaf, *parent, *old_at;
+  int at_off[17];
+  int at_ext[17][3];
+  int periodic[3];
+  cudaStream_t stream;
+  int cap;
+  int *new_n, *new_levels, *new_coords, *new_parent, *src, *how;
+};
+int tree_update_dev(const TreeArgs &a);
+
 // Enqueue one hydro step; returns the number of kernel launches, or -1 for an
 // unsupported block shape, or -2 for a launch error.
 int step_fp64_exact(const StepArgs &a, int ndim, int nx, int ny, int nz);

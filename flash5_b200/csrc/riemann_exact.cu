@@ -91,7 +91,7 @@ k_solve(const double *__restrict__ S, long n, double *__restrict__ out, unsigned
         if (net) w0 = wtr * (double)expf(float(G.z) * y);    // (p*/p_TR)^z
       }
     }
-    unsigned char fl = 0;
+    unsigned char fl = net ? 8 : 0;
     int its = 0;
     bool pending = false;
     Star S{0.0, 0.5 * (L.u + R.u), 0.0};
@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS) k_fallback(const double *__rest
     Gas G;
     load_state(S, n, i, L, R, G);
     Star S;
-    unsigned char fl = 1;
+    unsigned char fl = 1 | 8;
     const SideK kl = side_k(L, G), kr = side_k(R, G);
     int k = newton(L, R, kl, kr, G, tr_w(L, R, kl, kr, G), tol, max_iter, S);
     int its = 3 + (k > 0 ? k : max_iter);

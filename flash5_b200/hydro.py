@@ -159,6 +159,29 @@ class Hydro:
                                                       err.ctypes.data_as(C.POINTER(C.c_double))))
         return err
 
+    def mark_refine_tree(self, refine_vars, refine_filter, refine_cutoff, derefine_cutoff, max_refine=None,
+                         min_level=1):
+        """Grid_markRefineDerefine and the tree of a regrid on the device
+        (flash_hy_mark_refine_tree): the estimator, FLASH's marks and
+        PARAMESH's tree rules.  Returns (levels, coords [n, 3], parent, src,
+        how) of the new tree, ordered by level and Morton index."""
+        nv = len(refine_vars)
+        vars_ = (C.c_int * nv)(*[abi.REFVAR[v] for v in refine_vars])
+        rc = (C.c_double * nv)(*np.broadcast_to(np.asarray(refine_cutoff, dtype=np.float64), (nv,)))
+        dc = (C.c_double * nv)(*np.broadcast_to(np.asarray(derefine_cutoff, dtype=np.float64), (nv,)))
+        g = self.grid
+        cap = g.nblocks + (2 ** g.ndim) * int(g.is_leaf.sum()) + 8
+        mr = g.max_level if max_refine is None else int(max_refine)
+        lev, par, src, how = (np.empty(cap, dtype=np.int32) for _ in range(4))
+        coords = np.empty(3 * cap, dtype=np.int32)
+        n = C.c_int()
+        pi = lambda a: a.ctypes.data_as(C.POINTER(C.c_int))
+        self._check(self.lib.flash_hy_mark_refine_tree(self.ctx, nv, vars_, float(refine_filter), rc, dc, mr,
+                                                       int(min_level), cap, C.byref(n), pi(lev), pi(coords), pi(par),
+                                                       pi(src), pi(how)))
+        n = n.value
+        return lev[:n].copy(), coords[:3 * n].reshape(n, 3).copy(), par[:n].copy(), src[:n].copy(), how[:n].copy()
+
     def regrid(self, new_grid, src, how):
         """gr_updateRefinement's data movement: a new context for new_grid
         (amr.regrid's tree) filled from this one; this context is left as it

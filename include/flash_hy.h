@@ -313,6 +313,24 @@ int flash_hy_refine_tree(const flash_hy_grid_desc *grid, const unsigned char *re
                          int min_level, int cap, int *new_n, int *new_levels, int *new_coords, int *new_parent,
                          int *src, int *how);
 
+/* Grid_markRefineDerefine + the tree of Grid_updateRefinement on the device:
+ * the estimator of each of the nvar variables vars[] (FLASH_HY_REFVAR_*,
+ * refine_filter as flash_hy_estimate_error), FLASH's marks with the
+ * per-variable cutoffs refine_cutoff[v] / derefine_cutoff[v] and max_refine
+ * (gr_markRefineDerefine.F90: per variable, a leaf is marked for
+ * derefinement when it is not marked to refine or stay and both its error
+ * and its parent's are at or below the derefine cutoff; any node above the
+ * refine cutoff is marked to refine, not at or above max_refine; only leaves
+ * keep their marks), then the tree rules of flash_hy_refine_tree, all as
+ * kernels over a dense table of block positions per level.  The outputs are
+ * those of flash_hy_refine_tree for the same marks, in HOST arrays (the new
+ * context is created from them): new_n, new_levels, new_coords, new_parent,
+ * src, how.  AMR hierarchies of at most 15 levels.                     */
+int flash_hy_mark_refine_tree(flash_hy_ctx *ctx, int nvar, const int *vars, double refine_filter,
+                              const double *refine_cutoff, const double *derefine_cutoff, int max_refine,
+                              int min_level, int cap, int *new_n, int *new_levels, int *new_coords, int *new_parent,
+                              int *src, int *how);
+
 /* ---- launch shapes and their autotuner ----------------------------------
  * No FLASH5 counterpart (FLASH picks no launch shapes; its block loop is
  * Hydro.F90:156-229).  Threads per CTA of the step's kernels: the
@@ -377,7 +395,8 @@ int flash_hy_compute_dt_noalloc(const double *d_dens, const double *d_velx, cons
  * DEVICE pointers.  states = SoA [7][n] of (rho_L, u_L, p_L, rho_R, u_R,
  * p_R, gamma) with u the face-normal velocity; star = SoA [2][n] (p*, u*);
  * iters[n] = Newton iterations (fallback included); flags[n]: bit 0 fell
- * back to the two-rarefaction guess, bit 1 vacuum, bit 2 not converged.  */
+ * back to the two-rarefaction guess, bit 1 vacuum, bit 2 not converged,
+ * bit 3 the network was consulted (learned solves with strong waves).   */
 typedef struct flash_hy_rsolver flash_hy_rsolver;
 int flash_hy_rsolver_create(int device, flash_hy_rsolver **out);
 int flash_hy_rsolver_destroy(flash_hy_rsolver *r);

@@ -92,3 +92,34 @@ def test_regrid_matches_oracle(case):
     a, b = g2.interior(out)[leaves], g2.interior(ref2)[leaves]
     for v in VARS:
         assert np.array_equal(a[..., VAR[v]], b[..., VAR[v]]), (v, np.abs(a[..., VAR[v]] - b[..., VAR[v]]).max())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case,rc,dc", [("kh2d_ring", 0.8, 0.2), ("quad2d_16", 0.3, 0.6), ("kh3d_ring", 0.5, 0.4),
+                                        ("sod2d_reflect", 0.05, 0.9)])
+def test_device_marks_and_tree_equal_the_host_path(case, rc, dc):
+    """flash_hy_mark_refine_tree (estimator, FLASH's marks and PARAMESH's
+    tree rules as kernels) returns the tree of the host path -- device
+    estimator, amr.mark_refine_derefine, flash_hy_refine_tree -- node for
+    node: levels, coordinates, parents, and the regrid's src / how; the
+    cutoffs are chosen so that refinement, 2:1 balance and derefinement all
+    occur."""
+    from flash5_b200.amr import regrid_native
+    grid, unk, params = _case(case)
+    h = Hydro(params, grid)
+    try:
+        h.upload(unk)
+        dt, _ = h.compute_dt()
+        for _ in range(2):
+            h(dt, dt, dt)
+        errs = [h.estimate_error(v, 0.01) for v in ("dens", "pres")]
+        r, d = mark_refine_derefine(grid, errs, rc, dc)
+        g2, src, how = regrid_native(grid, r, d)
+        lev, coords, par, src_d, how_d = h.mark_refine_tree(("dens", "pres"), 0.01, rc, dc)
+    finally:
+        h.close()
+    assert np.array_equal(lev, g2.levels)
+    assert np.array_equal(coords, g2.coords)
+    assert np.array_equal(par, g2.parent)
+    assert np.array_equal(src_d, src) and np.array_equal(how_d, how)
+    assert r.any() or d.any()
