@@ -32,6 +32,7 @@ struct flash_hy_ctx {
   double *acc, *aux;
   void *sig;
   int *d_blk_at, *d_blk_coord, *d_list;
+  int *d_blk_nbr;             // uniform grids: [nblocks][6] face neighbours
   int list_cap;
   int *h_list;               // 0-based copy of a caller's 1-based block list
   int h_list_cap;
@@ -307,6 +308,7 @@ static void fill_devparams(const flash_hy_ctx *c, DevParams &P) {
   P.cfl = c->p.cfl;
   for (int d = 0; d < 3; ++d) P.del[d] = c->del[d];
   P.blk_at = c->d_blk_at;
+  P.blk_nbr = c->d_blk_nbr;
   P.blk_coord = c->d_blk_coord;
   P.status = c->d_status;
   for (int v = 0; v < 5; ++v) {
@@ -570,6 +572,7 @@ extern "C" int flash_hy_create(const flash_hy_params *params, const flash_hy_gri
     }
   }
   if (!amr) ALLOC(c->d_blk_at, at.size() * sizeof(int));
+  if (!amr) ALLOC(c->d_blk_nbr, (size_t)g->nblocks * 6 * sizeof(int));
   ALLOC(c->d_blk_coord, coords.size() * sizeof(int));
   ALLOC(c->d_part, g->nblocks * sizeof(CflPart));
   ALLOC(c->d_dt, sizeof(DtInfo));
@@ -585,6 +588,26 @@ extern "C" int flash_hy_create(const flash_hy_params *params, const flash_hy_gri
   }
   c->h_dt->dt = 0.0;
   c->h_dt->blk = -1;
+  // face neighbours of every block, as the direction kernels look them up
+  // (periodic wrap; -1 beyond other boundaries or for a block absent from
+  // a rank's share)
+  if (!amr) {
+    std::vector<int> nbr((size_t)g->nblocks * 6, -1);
+    for (int b = 0; b < g->nblocks; ++b)
+      for (int d = 0; d < 3; ++d)
+        for (int side = 0; side < 2; ++side) {
+          int cc[3] = {coords[3 * b], coords[3 * b + 1], coords[3 * b + 2]};
+          cc[d] += side ? 1 : -1;
+          if (cc[d] < 0 || cc[d] >= nbl[d]) {
+            if (d >= g->ndim || c->bc[2 * d + side] != FLASH_HY_BC_PERIODIC) continue;
+            cc[d] = (cc[d] + nbl[d]) % nbl[d];
+          }
+          nbr[(size_t)6 * b + 2 * d + side] = at[((size_t)cc[2] * nby + cc[1]) * nbx + cc[0]];
+        }
+    if (cudaMemcpy(c->d_blk_nbr, nbr.data(), nbr.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess) {
+      rc = fail(c, FLASH_HY_ERR_CUDA, "init copies%s", ""); goto bad;
+    }
+  }
   if ((!amr && cudaMemcpy(c->d_blk_at, at.data(), at.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess) ||
       cudaMemcpy(c->d_blk_coord, coords.data(), coords.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemset(c->d_status, 0, sizeof(unsigned)) != cudaSuccess) {
@@ -605,7 +628,7 @@ extern "C" int flash_hy_destroy(flash_hy_ctx *c) {
   for (int s = 0; s < 2; ++s)
     for (int v = 0; v < 5; ++v) ctx_free(c->state[s][v]);
   ctx_free(c->acc); ctx_free(c->aux); ctx_free(c->sig);
-  ctx_free(c->d_blk_at); ctx_free(c->d_blk_coord); ctx_free(c->d_list);
+  ctx_free(c->d_blk_at); ctx_free(c->d_blk_nbr); ctx_free(c->d_blk_coord); ctx_free(c->d_list);
   ctx_free(c->d_part); ctx_free(c->d_dt); ctx_free(c->d_status); ctx_free(c->d_stage);
   ctx_free(c->d_wmaster); ctx_free(c->d_mlp); ctx_free(c->d_harvest); ctx_free(c->d_harvest_n);
   drop_graphs(c);

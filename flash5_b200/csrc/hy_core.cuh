@@ -38,6 +38,8 @@ struct DevParams {
   double dt;
   const double *dt_dev;       // when set, dt is read from device memory (graph-replayed steps)
   const int *blk_at;          // block index at block coordinates
+  const int *blk_nbr;         // uniform grids: face neighbours of each block [b][x-, x+, y-, y+, z-, z+]
+                              // (-1 beyond a non-periodic boundary or absent from the grid)
   const int *blk_coord;       // 3 ints per block
   const int *blk_list;        // optional list of blocks to update (NULL = all)
   const double *s_in[5];      // dens, velx, vely, velz, eint (block-major SoA)

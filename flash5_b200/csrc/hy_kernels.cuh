@@ -101,33 +101,6 @@ __device__ __forceinline__ void cp_async16(void *dst, const void *src) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-// L2 prefetch of [p, p + bytes) by the CTA's threads, one 128-byte line each
-__device__ __forceinline__ void prefetch_l2(const void *p, size_t bytes) {
-  const char *c = static_cast<const char *>(p);
-  for (size_t o = (size_t)threadIdx.x * 128; o < bytes; o += (size_t)blockDim.x * 128)
-    asm volatile("prefetch.global.L2 [%0];\n" ::"l"(c + o));
-}
-
-// What a direction kernel reads from global memory after its staging: the
-// sig of the other directions (face states), the accumulators of the
-// earlier directions and, in the last direction, the aux rows of the
-// earlier ones (update) -- prefetched into L2 when the kernel starts, so
-// that their first touch overlaps the staging and the slopes.  Used by the
-// mixed HLLC kernel only: on KH 256^3 it saves 0.3 ms/step there and costs
-// 0.3 ms in the mixed exact-solver kernel and 0.5 ms in the FP64 kernel.
-template <int NDIM, int NX, int NY, int NZ, int DIR, bool FIRST, bool LAST, class R>
-__device__ __forceinline__ void prefetch_dir_inputs(const DevParams &P, int b, const R *sigb, const double *ACC,
-                                                    const double *AUX, size_t ncells, int nbox) {
-  constexpr size_t NCB = (size_t)NX * NY * NZ;
-  if (P.fmode != 3)
-    for (int d = 0; d < NDIM; ++d)
-      if (d != DIR - 1) prefetch_l2(sigb + (size_t)d * 6 * nbox, (size_t)6 * nbox * sizeof(R));
-  if (!FIRST)
-    for (int n = 0; n < 5; ++n) prefetch_l2(ACC + n * ncells + (size_t)b * NCB, NCB * sizeof(double));
-  if (LAST)
-    for (int r = 0; r < 3 * (NDIM - 1); ++r) prefetch_l2(AUX + r * ncells + (size_t)b * NCB, NCB * sizeof(double));
-}
-
 // The source blocks of a block's guard cells on a uniform grid: entry
 // (cz * 3 + cy) * 3 + cx for the side (0 below, 1 inside, 2 above) of each
 // coordinate; threads 0..3^NDIM-1 write one entry each.

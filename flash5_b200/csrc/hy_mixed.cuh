@@ -50,6 +50,15 @@ __device__ __forceinline__ bool mbar_try(unsigned long long *bar, unsigned parit
   return ok != 0;
 }
 // 3D tile copy global -> shared through a tensor map (no multicast)
+// L2 prefetch of [p, p + bytes) as one bulk request (16-byte aligned,
+// bytes a multiple of 16)
+__device__ __forceinline__ void bulk_prefetch_l2(const void *p, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p), "r"(bytes) : "memory");
+}
+// fetch a tensor map into the descriptor cache ahead of its first copy
+__device__ __forceinline__ void prefetch_tensormap(const CUtensorMap *map) {
+  asm volatile("prefetch.tensormap [%0];\n" ::"l"(reinterpret_cast<unsigned long long>(map)) : "memory");
+}
 __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int c0, int c1, int c2,
                                             unsigned long long *bar) {
   asm volatile(
@@ -203,6 +212,9 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
   double *sIg = reinterpret_cast<double *>(sWm + 6 * G::SC);              // [SC] 1/(game-1)
   double *sF = reinterpret_cast<double *>(reg);                           // [9][SC] (after phase D)
 
+  static_assert((6 * B::n * 4) % 16 == 0 && (NCB * 8) % 16 == 0, "bulk prefetch sizes must be multiples of 16 bytes");
+  // the tile copies' descriptors load while the block's indices do
+  if (NDIM == 3 && tm.on && threadIdx.x < 10) prefetch_tensormap(threadIdx.x < 5 ? &tm.intr[threadIdx.x] : &tm.slab[threadIdx.x - 5]);
   const int b = P.blk_list ? P.blk_list[blockIdx.x] : blockIdx.x;
   const int3 bc = blk_coords(P, b);
   unsigned st = 0;
@@ -212,7 +224,19 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
   const float dtn = float(dt / delta), hdtn = 0.5f * dtn;
   const float hdtx = float(0.5 * dt / del[0]), hdty = float(0.5 * dt / del[1]), hdtz = float(0.5 * dt / del[2]);
   const float *sigb = SIG + (size_t)(P.slot ? P.slot[b] : (int)blockIdx.x) * NDIM * 6 * B::n;
-  if constexpr (RS == 0) prefetch_dir_inputs<NDIM, NX, NY, NZ, DIR, FIRST, LAST>(P, b, sigb, ACC, AUX, ncells, B::n);
+  // What the kernel reads from global memory after its staging -- the sig
+  // of the other directions (face states), the accumulators of the earlier
+  // directions and, in the last direction, their aux rows (update) -- is
+  // prefetched into L2 at the start, one bulk request per contiguous range
+  // (lanes of warp 0), so that the first touch overlaps the staging and the
+  // slopes.
+  if (threadIdx.x < 32) {
+    const int ln = threadIdx.x;
+    if (ln < NDIM && ln != DIR - 1 && P.fmode != 3) bulk_prefetch_l2(sigb + (size_t)ln * 6 * B::n, 6u * B::n * 4u);
+    if (!FIRST && ln >= 4 && ln < 9) bulk_prefetch_l2(ACC + (ln - 4) * ncells + (size_t)b * NCB, NCB * 8u);
+    if (LAST && ln >= 12 && ln < 12 + 3 * (NDIM - 1))
+      bulk_prefetch_l2(AUX + (ln - 12) * ncells + (size_t)b * NCB, NCB * 8u);
+  }
 
   auto fidx = [](int along, int t1, int t2) { return G::at(along, t1 + (DIR == 1 ? NY : NX) * t2, G::LC, 1); };
   if (P.fmode != 3) {
@@ -222,23 +246,15 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
   // bytes), then the pressure and the guard cells' EOS in place; slabs
   // beyond a non-periodic boundary (mirror / copy rules) and all other
   // grids through load_prim.
-  bool tma = NDIM == 3 && tm.on && P.lh == nullptr;
+  bool tma = NDIM == 3 && tm.on && P.lh == nullptr && P.blk_nbr != nullptr;
   int nbs[2] = {-1, -1};          // neighbour blocks below / above along DIR (-1: load_prim)
   unsigned long long *bar = reinterpret_cast<unsigned long long *>(smem_raw + G::smem_bytes() - 16 - 128);
   float *sRed = reinterpret_cast<float *>(smem_raw + G::smem_bytes() - 16 - 128 - G::red_bytes);
   if (tma) {
-    const int ext[3] = {P.nbx, P.nby, P.nbz};
-#pragma unroll
-    for (int side = 0; side < 2; ++side) {
-      int cc[3] = {bc.x, bc.y, bc.z};
-      cc[DIR - 1] += side ? 1 : -1;
-      bool ok = true;
-      if (cc[DIR - 1] < 0 || cc[DIR - 1] >= ext[DIR - 1]) {
-        ok = P.bc[2 * (DIR - 1) + side] == FLASH_HY_BC_PERIODIC;
-        cc[DIR - 1] = (cc[DIR - 1] + ext[DIR - 1]) % ext[DIR - 1];
-      }
-      nbs[side] = ok ? P.blk_at[(cc[2] * P.nby + cc[1]) * P.nbx + cc[0]] : -1;
-    }
+    // the neighbours from the block's face-neighbour row (one load, not
+    // dependent on the coordinates)
+    nbs[0] = P.blk_nbr[6 * b + 2 * (DIR - 1)];
+    nbs[1] = P.blk_nbr[6 * b + 2 * (DIR - 1) + 1];
     if (threadIdx.x == 0) mbar_init(bar, 1);
     __syncthreads();                          // the barrier is initialised before anyone polls it
     if (threadIdx.x == 0) {
