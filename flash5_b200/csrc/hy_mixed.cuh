@@ -671,7 +671,11 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
         }
       }
     }
-#pragma unroll
+    // One copy of the face solve, looped over the thread's faces (not
+    // unrolled: the solver and the sampling are large, and two copies of
+    // them overflow the instruction cache); the results go to the
+    // registers of face `it` by compile-time selection.
+#pragma unroll 1
     for (int it = 0; it < NIT; ++it) {
       const int t = threadIdx.x + it * NT;
       if (t >= G::SC) break;
@@ -687,8 +691,16 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
         const double q = learned ? sP0[t] : 0.0;
         const xrs::SideK kl = xrs::side_k(L, gas), kr = xrs::side_k(R, gas);
         const double w0 = q < 0.0 ? -q : xrs::tr_w(L, R, kl, kr, gas);
-        int k = xrs::newton(L, R, kl, kr, gas, w0, P.rs_tol, q < 0.0 ? 3 : P.rs_max_iter, S);
-        if (k < 0 && q < 0.0) k = xrs::newton(L, R, kl, kr, gas, xrs::tr_w(L, R, kl, kr, gas), P.rs_tol, P.rs_max_iter, S);
+        // the network's start gets three evaluations; if they do not
+        // converge, Newton restarts from the two-rarefaction guess
+        int k;
+#pragma unroll 1
+        for (int attempt = 0;; ++attempt) {
+          const bool net = attempt == 0 && q < 0.0;
+          k = xrs::newton(L, R, kl, kr, gas, attempt == 0 ? w0 : xrs::tr_w(L, R, kl, kr, gas), P.rs_tol,
+                          net ? 3 : P.rs_max_iter, S);
+          if (k >= 0 || !net) break;
+        }
         if (k < 0) st |= ST_NEWTON;
         if (P.harvest && (q < 0.0 || (xrs::strong_waves(L, R) && !xrs::tr_exact(L, R, xrs::p_of_w(w0, gas)))))
           harvest_face(P, L, R, g, (unsigned)(blockIdx.x * 4 + DIR) * 2048u + (unsigned)t);
@@ -700,18 +712,22 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
         VL[n] = face(qq, true, s, t);
         VR[n] = face(qq, false, s, t);
       }
-      double F[6];
+      double F[9];
       xrs::godunov_flux<DIR>(VL, VR, L, R, gas, S, vac, F);
-#pragma unroll
-      for (int n = 0; n < 6; ++n) Fr[it][n] = F[n];
       double fv = 0., fe = 0.;
       if (P.use_aux_eint) {
         if (F[FDENS] > 0.) { fv = F[FDENS] / VL[HD]; fe = F[FDENS] * VL[HEI]; }
         else { fv = F[FDENS] / VR[HD]; fe = F[FDENS] * VR[HEI]; }
       }
-      Fr[it][FEINT] = fe;
-      Fr[it][FVOLU] = fv;
-      Fr[it][8] = (Vs(4, s.x) + double(sWm[4 * G::SC + t])) + (Vs(4, s.x) + double(sWp[4 * G::SC + t]));
+      F[FEINT] = fe;
+      F[FVOLU] = fv;
+      F[8] = (Vs(4, s.x) + double(sWm[4 * G::SC + t])) + (Vs(4, s.x) + double(sWp[4 * G::SC + t]));
+#pragma unroll
+      for (int j = 0; j < NIT; ++j)
+        if (j == it) {
+#pragma unroll
+          for (int n = 0; n < 9; ++n) Fr[j][n] = F[n];
+        }
     }
   } else {
 #pragma unroll
