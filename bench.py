@@ -586,7 +586,7 @@ def amr_run(args, paths, e2e=True, regrid=True, cpu=True, steps=None, warmup=Non
             best, trials = h.autotune(dts[0] if dts is not None else h.compute_dt()[0], steps=2)
             tunings[name] = {"best": best, "trials_ms": {"/".join(str(v) for v in t.values()): round(m, 4)
                                                          for t, m in trials},
-                             "trial_key": "sig_threads/dir_threads/mx_threads"}
+                             "trial_key": "sig_threads/dir_threads/mx_threads/mx_runs"}
         headline = name == paths[-1]
         sampler = ClockSampler(0) if headline else None
         ms[name], used, launches[name] = run_device(h, steps, warmup, dts=dts, sampler=sampler)
@@ -814,7 +814,7 @@ def main():
             best, trials = hh.autotune(dt0, steps=2)
             tuned = {"best": best, "trials_ms": {"/".join(str(v) for v in t.values()): round(m, 4)
                                                  for t, m in trials},
-                     "trial_key": "sig_threads/dir_threads/mx_threads"}
+                     "trial_key": "sig_threads/dir_threads/mx_threads/mx_runs"}
         headline = name == paths[-1]
         sampler = ClockSampler(dev) if headline else None
         ms[name], used, launches[name] = run_device(h, args.steps, warmup, dts=dts, sampler=sampler, dist=dist)

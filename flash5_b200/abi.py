@@ -123,11 +123,13 @@ class GridDesc(C.Structure):
 
 class Tuning(C.Structure):
     """flash_hy_tuning: threads per CTA of the transverse-flux/CFL passes,
-    the FP64 direction kernels and the mixed direction kernels."""
-    _fields_ = [("sig_threads", C.c_int), ("dir_threads", C.c_int), ("mx_threads", C.c_int)]
+    the FP64 direction kernels and the mixed direction kernels, and the
+    blocks per CTA along the sweep of the mixed 3D direction kernels."""
+    _fields_ = [("sig_threads", C.c_int), ("dir_threads", C.c_int), ("mx_threads", C.c_int), ("mx_runs", C.c_int)]
 
     def as_dict(self):
-        return {"sig_threads": self.sig_threads, "dir_threads": self.dir_threads, "mx_threads": self.mx_threads}
+        return {"sig_threads": self.sig_threads, "dir_threads": self.dir_threads, "mx_threads": self.mx_threads,
+                "mx_runs": self.mx_runs}
 
 
 TUNE_MAX = 8

@@ -33,6 +33,9 @@ struct flash_hy_ctx {
   void *sig;
   int *d_blk_at, *d_blk_coord, *d_list;
   int *d_blk_nbr;             // uniform grids: [nblocks][6] face neighbours
+  fhy::TmaLine *tma_run;      // run kernels' maps (2 state buffers x 3 directions), or NULL
+  int *d_runs[3];             // per direction: [nblocks / kMxRun][kMxRun + 2]
+  void *d_cflq;               // [nblocks][kMxRun] CFL candidates of the run quarters
   int list_cap;
   int *h_list;               // 0-based copy of a caller's 1-based block list
   int h_list_cap;
@@ -49,6 +52,7 @@ struct flash_hy_ctx {
   int threads;         // threads per CTA: transverse-flux and CFL passes
   int dir_threads;     // FP64 direction kernels
   int mx_sel;          // mixed direction kernels: candidate 0, 1, 2
+  int mx_runs;         // mixed 3D direction kernels: blocks per CTA along the sweep (1 or kMxRun)
   int host_ng;         // guard layers of the caller's UNK arrays
   float *d_wmaster;    // learned guess: FP32 master weights
   void *d_mlp;         // learned guess: packed BF16 inference copy (xrs::MlpPacked)
@@ -207,7 +211,8 @@ extern "C" int flash_hy_release_memory(int device) {
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-static fhy::TmaLine *make_tma_maps(flash_hy_ctx *c) {
+static_assert(fhy::kMxRun == FLASH_HY_MX_RUN, "the run length of the header and the kernels agree");
+static fhy::TmaLine *make_tma_maps(flash_hy_ctx *c, int K = 1) {
   if (c->ndim != 3 || c->nx != 8 || c->ny != 8 || c->nz != 8) return nullptr;
   static EncodeTiledFn encode = nullptr;
   if (!encode) {
@@ -225,13 +230,16 @@ static fhy::TmaLine *make_tma_maps(flash_hy_ctx *c) {
   const cuuint64_t dims[3] = {8, 8, (cuuint64_t)c->nblocks * 8};
   const cuuint64_t strides[2] = {8 * sizeof(double), 64 * sizeof(double)};
   const cuuint32_t one[3] = {1, 1, 1};
-  const cuuint32_t box_in[3] = {8, 8, 8};
-  const cuuint32_t box_slab[3][3] = {{4, 8, 8}, {8, 4, 8}, {8, 8, 4}};
+  // runs (K > 1): 1/K of the slower transverse axis (z for the x and y
+  // sweeps, y for the z sweep)
+  const cuuint32_t q = (cuuint32_t)(8 / K);
+  const cuuint32_t box_in[3][3] = {{8, 8, q}, {8, 8, q}, {8, q, 8}};
+  const cuuint32_t box_slab[3][3] = {{4, 8, q}, {8, 4, q}, {8, q, 4}};
   for (int par = 0; par < 2; ++par)
     for (int d = 0; d < 3; ++d) {
       fhy::TmaLine &t = m[par * 3 + d];
       for (int v = 0; v < 5; ++v) {
-        if (encode(&t.intr[v], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, c->state[par][v], dims, strides, box_in, one,
+        if (encode(&t.intr[v], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, c->state[par][v], dims, strides, box_in[d], one,
                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS ||
             encode(&t.slab[v], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, c->state[par][v], dims, strides, box_slab[d], one,
@@ -478,6 +486,7 @@ extern "C" int flash_hy_create(const flash_hy_params *params, const flash_hy_gri
   c->threads = g->ndim == 3 ? 320 : (g->nxb == 8 ? 96 : 288);  // line cells split evenly
   c->dir_threads = c->threads;
   c->mx_sel = 1;
+  c->mx_runs = 1;
   c->host_ng = g->nguard;
   c->nspec = params->nspecies;
   c->nsp = params->nspecies + params->nmass_scalars;
@@ -607,6 +616,45 @@ extern "C" int flash_hy_create(const flash_hy_params *params, const flash_hy_gri
     if (cudaMemcpy(c->d_blk_nbr, nbr.data(), nbr.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess) {
       rc = fail(c, FLASH_HY_ERR_CUDA, "init copies%s", ""); goto bad;
     }
+    // runs of the mixed direction kernels: on a full grid whose block
+    // counts divide by kMxRun, every block with coordinate = 0 mod kMxRun
+    // along the sweep starts a run of kMxRun blocks (+ its neighbours below
+    // and above the run); the species pass keeps one block per CTA
+    constexpr int K = fhy::kMxRun;
+    if (c->tma_maps && !partial && c->nsp == 0 && nbx % K == 0 && nby % K == 0 && nbz % K == 0) {
+      bool ok = true;
+      for (int d = 0; d < 3 && ok; ++d) {
+        std::vector<int> runs;
+        runs.reserve((size_t)g->nblocks / K * (K + 2));
+        for (int b = 0; b < g->nblocks; ++b) {
+          if (coords[3 * b + d] % K != 0) continue;
+          int cur = b;
+          for (int m = 0; m < K; ++m) {
+            runs.push_back(cur);
+            if (m < K - 1) cur = nbr[(size_t)6 * cur + 2 * d + 1];
+            if (cur < 0) ok = false;
+          }
+          runs.push_back(nbr[(size_t)6 * b + 2 * d]);
+          runs.push_back(nbr[(size_t)6 * runs[runs.size() - 2] + 2 * d + 1]);
+          if (!ok) break;
+        }
+        if (!ok || runs.size() != (size_t)g->nblocks / K * (K + 2)) { ok = false; break; }
+        ALLOC(c->d_runs[d], runs.size() * sizeof(int));
+        if (cudaMemcpy(c->d_runs[d], runs.data(), runs.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess) {
+          rc = fail(c, FLASH_HY_ERR_CUDA, "init copies%s", ""); goto bad;
+        }
+      }
+      if (ok) {
+        ALLOC(c->d_cflq, (size_t)g->nblocks * K * sizeof(fhy::CflCand));
+        c->tma_run = make_tma_maps(c, K);
+        if (c->tma_run)
+          for (int t = 0; t < 6; ++t) {
+            c->tma_run[t].runs = c->d_runs[t % 3];
+            c->tma_run[t].cflq = c->d_cflq;
+          }
+        if (c->tma_run) c->mx_runs = K;
+      }
+    }
   }
   if ((!amr && cudaMemcpy(c->d_blk_at, at.data(), at.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess) ||
       cudaMemcpy(c->d_blk_coord, coords.data(), coords.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
@@ -648,6 +696,9 @@ extern "C" int flash_hy_destroy(flash_hy_ctx *c) {
   free(c->h_blk_at);
   free(c->h_list);
   free(c->tma_maps);
+  free(c->tma_run);
+  for (int d = 0; d < 3; ++d) ctx_free(c->d_runs[d]);
+  ctx_free(c->d_cflq);
   xfer_free(c);
   if (c->h_dt) cudaFreeHost(c->h_dt);
   if (c->h_status) cudaFreeHost(c->h_status);
@@ -1067,6 +1118,8 @@ static int enqueue_step(flash_hy_ctx *c, double dt, const int *d_list, int nlaun
   a.mx_sel = c->mx_sel;
   a.stream = c->stream;
   a.tma = c->tma_maps ? c->tma_maps + 3 * c->cur : nullptr;
+  a.tma_run = c->tma_run && c->mx_runs > 1 ? c->tma_run + 3 * c->cur : nullptr;
+  a.nblocks = c->nblocks;
   a.nlev = 0;
   int pre = 0;
   if (c->amr) {
@@ -1463,6 +1516,7 @@ extern "C" int flash_hy_get_tuning(flash_hy_ctx *c, flash_hy_tuning *out) {
   out->sig_threads = c->threads;
   out->dir_threads = c->dir_threads;
   out->mx_threads = mx_threads_of(c->mx_sel, c->ndim, c->nx);
+  out->mx_runs = c->mx_runs;
   return 0;
 }
 
@@ -1475,7 +1529,10 @@ extern "C" int flash_hy_set_tuning(flash_hy_ctx *c, const flash_hy_tuning *t) {
     if (mx_threads_of(q, c->ndim, c->nx) == t->mx_threads) sel = q;
   if (index_of(cand, n, t->sig_threads) < 0 || index_of(cand, n, t->dir_threads) < 0 || sel < 0)
     return fail(c, FLASH_HY_ERR_BAD_ARG, "set_tuning: %s", "not a candidate launch shape of this block shape");
-  if (t->sig_threads != c->threads || t->dir_threads != c->dir_threads || sel != c->mx_sel) {
+  if (t->mx_runs != 1 && !(t->mx_runs == fhy::kMxRun && c->tma_run))
+    return fail(c, FLASH_HY_ERR_BAD_ARG, "set_tuning: %s", "mx_runs is 1 or FLASH_HY_MX_RUN where runs are offered");
+  if (t->sig_threads != c->threads || t->dir_threads != c->dir_threads || sel != c->mx_sel ||
+      t->mx_runs != c->mx_runs) {
     CUDA_OK(c, cudaSetDevice(c->device));
     CUDA_OK(c, cudaStreamSynchronize(c->stream));
     drop_graphs(c);
@@ -1484,6 +1541,7 @@ extern "C" int flash_hy_set_tuning(flash_hy_ctx *c, const flash_hy_tuning *t) {
   c->threads = t->sig_threads;
   c->dir_threads = t->dir_threads;
   c->mx_sel = sel;
+  c->mx_runs = t->mx_runs;
   return 0;
 }
 
@@ -1505,7 +1563,7 @@ extern "C" int flash_hy_autotune(flash_hy_ctx *c, double dt, int steps, flash_hy
   double *keep = nullptr;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   int rc = 0, nt = 0;
-  const int sig0 = c->threads, dir0 = c->dir_threads, sel0 = c->mx_sel;
+  const int sig0 = c->threads, dir0 = c->dir_threads, sel0 = c->mx_sel, runs0 = c->mx_runs;
   int cand[FLASH_HY_TUNE_MAX];
   const int ncand = thread_candidates(c, cand);
   const bool mixed = c->p.precision == FLASH_HY_PREC_MIXED;
@@ -1539,6 +1597,7 @@ extern "C" int flash_hy_autotune(flash_hy_ctx *c, double dt, int steps, flash_hy
       table[nt].sig_threads = c->threads;
       table[nt].dir_threads = c->dir_threads;
       table[nt].mx_threads = mx_threads_of(c->mx_sel, c->ndim, c->nx);
+      table[nt].mx_runs = c->mx_runs;
       table_ms[nt] = ms;
     }
     ++nt;
@@ -1575,6 +1634,20 @@ extern "C" int flash_hy_autotune(flash_hy_ctx *c, double dt, int steps, flash_hy
     }
     if (!rc) {
       if (mixed) c->mx_sel = best_dir; else c->dir_threads = best_dir;
+      // runs of blocks along the sweep, where offered: the other setting
+      if (mixed && c->tma_run) {
+        const int other = c->mx_runs > 1 ? 1 : fhy::kMxRun;
+        const int keep_runs = c->mx_runs;
+        c->mx_runs = other;
+        float ms = 0.f;
+        rc = trial(ms);
+        if (!rc) {
+          record(ms);
+          if (!(ms < best_ms)) c->mx_runs = keep_runs;
+        }
+      }
+    }
+    if (!rc) {
       int best_sig = sig0;
       best_ms = 3.4e38f;
       for (int q = 0; q < ncand && !rc; ++q) {
@@ -1596,7 +1669,7 @@ done:
   }
   if (e0) cudaEventDestroy(e0);
   if (e1) cudaEventDestroy(e1);
-  if (rc) { c->threads = sig0; c->dir_threads = dir0; c->mx_sel = sel0; }
+  if (rc) { c->threads = sig0; c->dir_threads = dir0; c->mx_sel = sel0; c->mx_runs = runs0; }
   cudaMemcpy(c->d_status, &saved_status, sizeof(unsigned), cudaMemcpyHostToDevice);
   c->dt_valid = 0;
   drop_graphs(c);

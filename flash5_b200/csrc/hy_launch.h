@@ -7,14 +7,22 @@
 
 namespace fhy {
 
+// Blocks per run of the mixed direction kernels on full uniform 3D grids:
+// a CTA stages kMxRun blocks that follow one another along the sweep and
+// 1/kMxRun of their cross-section.
+constexpr int kMxRun = 4;
+
 // Tensor maps of the step's input state for the mixed direction kernels'
 // TMA staging (k_dir_mx, uniform 3D grids): per state variable the block
 // interior (box 8 x 8 x 8) and the neighbour slab along the sweep direction
-// (box 4 x 8 x 8, 8 x 4 x 8 or 8 x 8 x 4) over the natural block layout.
+// (box 4 x 8 x 8, 8 x 4 x 8 or 8 x 8 x 4) over the natural block layout;
+// for runs, the same boxes cut to 1/kMxRun of the slower transverse axis.
 struct TmaLine {
   CUtensorMap intr[5];        // dens, velx, vely, velz, eint
   CUtensorMap slab[5];
   int on;                     // 0: the stencil is staged by load_prim
+  const int *runs;            // runs: [nblocks / kMxRun][kMxRun + 2] blocks along the sweep, neighbours below / above
+  void *cflq;                 // runs, last direction: [nblocks][kMxRun] CflCand of the quarters
 };
 
 struct StepArgs {
@@ -39,6 +47,8 @@ struct StepArgs {
   const int *lev_list[17];  // leaves of each level (device), 1-based levels
   int lev_count[17];
   const TmaLine *tma; // [3] (directions x, y, z) for the input state, or NULL
+  const TmaLine *tma_run = nullptr;  // [3] maps of the run kernels (full uniform 3D grids), or NULL
+  int nblocks = 0;    // blocks of the grid (run kernels: the CFL merge)
 };
 
 // the species / mass-scalar pass after the hydro direction kernels

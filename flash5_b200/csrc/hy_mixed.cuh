@@ -127,10 +127,64 @@ __device__ __forceinline__ void hllc_fp64(const DevParams &P, const double *Vm, 
   for (int n = 0; n < 5; ++n) Fs[n] = F[n] + S * (UC[n] - U[n]);
 }
 
-template <int NDIM, int NX, int NY, int NZ, int DIR, int RS = 0>
+// CTA-wide merge of the threads' CFL candidates (cfl_merge: largest key,
+// first index on ties); the result is valid in thread 0.  Ends with a
+// barrier, so that it may be called again at once.
+__device__ __forceinline__ CflCand cfl_cta_merge(CflCand c) {
+  __shared__ CflCand red[32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    CflCand b;
+    b.key = __shfl_down_sync(0xffffffffu, c.key, o);
+    b.val = __shfl_down_sync(0xffffffffu, c.val, o);
+    b.idx = __shfl_down_sync(0xffffffffu, c.idx, o);
+    if (lane + o < 32) cfl_merge(c, b);
+  }
+  if (lane == 0) red[w] = c;
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int q = 1; q < (int)(blockDim.x + 31) / 32; ++q) cfl_merge(c, red[q]);
+  __syncthreads();
+  return c;
+}
+
+// Per block, the K quarter candidates of a run step merged into the block's
+// CFL result, as cfl_block_reduce writes it for a block handled whole
+// (Hydro_computeDt.F90:265-284).
+template <int NX, int NY, int K>
+__global__ void k_cfl_runs(const CflCand *cq, int nblocks, double cfl, CflPart *part) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nblocks) return;
+  CflCand a = cq[(size_t)b * K];
+#pragma unroll
+  for (int q = 1; q < K; ++q) cfl_merge(a, cq[(size_t)b * K + q]);
+  CflPart r;
+  if (a.key > 0.0) {
+    r.dt = cfl / a.val;
+    r.i = a.idx % NX; r.j = (a.idx / NX) % NY; r.k = a.idx / (NX * NY);
+  } else {
+    r.dt = DBL_MAX; r.i = r.j = r.k = -1;
+  }
+  r.blk = b;
+  part[b] = r;
+}
+
+// Lines of a CTA: the block's lines along DIR (K = 1), or, with K > 1, a
+// run of K blocks that follow one another along DIR, of which the CTA takes
+// 1/K of the cross-section (quarter q of the slower transverse axis): the
+// lines are K blocks long, so the stencil overlap along DIR (four guard
+// cells on each side, recomputed slopes and face states at the ends) is
+// paid once per run instead of once per block.
+template <int NDIM, int NX, int NY, int NZ, int DIR, int RS = 0, int K = 1>
 struct MxGeom {
-  static constexpr int ND = DIR == 1 ? NX : (DIR == 2 ? NY : NZ);
-  static constexpr int C = DIR == 1 ? NY * NZ : (DIR == 2 ? NX * NZ : NX * NY);   // lines
+  static constexpr int ND0 = DIR == 1 ? NX : (DIR == 2 ? NY : NZ);               // block extent along DIR
+  static constexpr int ND = K * ND0;                                              // line interior
+  static constexpr int T1 = DIR == 1 ? NY : NX;                                   // faster transverse axis
+  static constexpr int T2 = DIR == 3 ? NY : NZ;                                   // slower one (split by K)
+  static_assert(K == 1 || (NDIM == 3 && T2 % K == 0), "runs split the slower transverse axis");
+  static constexpr int T2Q = T2 / K;
+  static constexpr int C = T1 * T2Q;                                              // lines
   static constexpr int L4 = ND + 8, LS = ND + 4, LC = ND + 2;                      // staged, slope, line cells
   static constexpr int SA = L4 * C, SB = LS * C, SC = LC * C;
   // index of position x on line l in a space of length L with offset o
@@ -139,26 +193,37 @@ struct MxGeom {
     if (DIR == 1) { l = s / L; x = s % L - o; } else { l = s % C; x = s / C - o; }
   }
   static constexpr int step = DIR == 1 ? 1 : C;      // +1 along the line
-  // staged stencil (positions x in [-4, ND + 3] of line l): three regions --
-  // the slab of the neighbour below, the block's interior, the slab of the
+  // staged stencil (positions x in [-4, ND + 3] of line l): the slab of the
+  // neighbour below, the interior of each block of the run, the slab of the
   // neighbour above -- each in the natural x, y, z order of the block
   // store, so that each is one dense tile copy; along the sweep direction
   // the regions follow one another (DIR 3: plain along-major order)
-  static constexpr int SLAB = 4 * C, LO = 0, MID = 4 * C, HI = (4 + ND) * C;
+  static constexpr int SLAB = 4 * C, LO = 0, MID = 4 * C, HI = (4 + ND) * C, MIDB = ND0 * C;
   __device__ static __forceinline__ int sidx(int x, int l) {
     if (DIR == 3) return (x + 4) * C + l;
-    if (DIR == 1) return x < 0 ? l * 4 + (x + 4) : (x < ND ? MID + l * ND + x : HI + l * 4 + (x - ND));
+    const int m = x < 0 ? 0 : (x >= ND ? K - 1 : x / ND0), xl = x - m * ND0;
+    if (DIR == 1) return x < 0 ? l * 4 + (x + 4) : (x < ND ? MID + m * MIDB + l * ND0 + xl : HI + l * 4 + (x - ND));
     // DIR 2: line l = i + NX * k
     const int i = l % NX, k = l / NX;
     return x < 0 ? k * 4 * NX + (x + 4) * NX + i
-                 : (x < ND ? MID + (k * ND + x) * NX + i : HI + k * 4 * NX + (x - ND) * NX + i);
+                 : (x < ND ? MID + m * MIDB + (k * ND0 + xl) * NX + i : HI + k * 4 * NX + (x - ND) * NX + i);
   }
-  __device__ static __forceinline__ void cell(int x, int l, int &i, int &j, int &k) {
-    if (DIR == 1) { i = x; j = l % NY; k = l / NY; }
-    else if (DIR == 2) { j = x; i = l % NX; k = l / NX; }
-    else { k = x; i = l % NX; j = l / NX; }
+  // block of the run holding position x (the end blocks for the guard
+  // positions) and x relative to that block
+  __device__ static __forceinline__ int blk_of(int x, int &xl) {
+    const int m = x < 0 ? 0 : (x >= ND ? K - 1 : x / ND0);
+    xl = x - m * ND0;
+    return m;
+  }
+  // block-local cell of block-relative position xl on line l of quarter q
+  __device__ static __forceinline__ void cell(int xl, int l, int q, int &i, int &j, int &k) {
+    const int t1 = l % T1, t2 = l / T1 + q * T2Q;
+    if (DIR == 1) { i = xl; j = t1; k = t2; }
+    else if (DIR == 2) { j = xl; i = t1; k = t2; }
+    else { k = xl; i = t1; j = t2; }
     if (NDIM < 3) k = (DIR == 3) ? k : 0;
   }
+  __device__ static __forceinline__ void cell(int x, int l, int &i, int &j, int &k) { cell(x, l, 0, i, j, k); }
   // shared memory: staged prims (FP64), then a region used first for the
   // reconstruction scratch and then for the face fluxes
   // (with the exact solver the slope scratch, dead during the Riemann
@@ -190,12 +255,12 @@ template <int NDIM, int NX, int NY, int NZ> struct MxThreads {
   static constexpr int pick(int sel) { return sel == 0 ? c0 : (sel == 1 ? c1 : c2); }
 };
 
-template <int NDIM, int NX, int NY, int NZ, int DIR, bool FIRST, bool LAST, int RS, int NT>
+template <int NDIM, int NX, int NY, int NZ, int DIR, bool FIRST, bool LAST, int RS, int NT, int K = 1>
 __global__ void __launch_bounds__(NT, NDIM == 3 ? 2 : 1)
 k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ ACC, double *__restrict__ AUX,
          size_t ncells, CflPart *part, const __grid_constant__ TmaLine tm) {
   static_assert(NT % 32 == 0, "threads per CTA must be a multiple of 32");
-  using G = MxGeom<NDIM, NX, NY, NZ, DIR, RS>;
+  using G = MxGeom<NDIM, NX, NY, NZ, DIR, RS, K>;
   using B = Box<NDIM, NX, NY, NZ>;
   constexpr int NCB = NX * NY * NZ;
   constexpr int NIT = (G::SC + NT - 1) / NT;
@@ -215,7 +280,21 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
   static_assert((6 * B::n * 4) % 16 == 0 && (NCB * 8) % 16 == 0, "bulk prefetch sizes must be multiples of 16 bytes");
   // the tile copies' descriptors load while the block's indices do
   if (NDIM == 3 && tm.on && threadIdx.x < 10) prefetch_tensormap(threadIdx.x < 5 ? &tm.intr[threadIdx.x] : &tm.slab[threadIdx.x - 5]);
-  const int b = P.blk_list ? P.blk_list[blockIdx.x] : blockIdx.x;
+  // the CTA's blocks: one (K = 1), or run blockIdx.x / K of K blocks that
+  // follow one another along DIR (with the neighbours below and above the
+  // run), of which the CTA takes quarter qtr = blockIdx.x % K
+  int blk[K], nbs[2] = {-1, -1}, qtr = 0;
+  if constexpr (K == 1) {
+    blk[0] = P.blk_list ? P.blk_list[blockIdx.x] : blockIdx.x;
+  } else {
+    const int *run = tm.runs + (size_t)(blockIdx.x / K) * (K + 2);
+    qtr = blockIdx.x % K;
+#pragma unroll
+    for (int m = 0; m < K; ++m) blk[m] = run[m];
+    nbs[0] = run[K];
+    nbs[1] = run[K + 1];
+  }
+  const int b = blk[0];
   const int3 bc = blk_coords(P, b);
   unsigned st = 0;
   double del[3];
@@ -230,12 +309,16 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
   // prefetched into L2 at the start, one bulk request per contiguous range
   // (lanes of warp 0), so that the first touch overlaps the staging and the
   // slopes.
+  // (On a run, CTA qtr prefetches the ranges of block qtr of the run: the run's
+  // K CTAs together cover its K blocks.)
   if (threadIdx.x < 32) {
     const int ln = threadIdx.x;
-    if (ln < NDIM && ln != DIR - 1 && P.fmode != 3) bulk_prefetch_l2(sigb + (size_t)ln * 6 * B::n, 6u * B::n * 4u);
-    if (!FIRST && ln >= 4 && ln < 9) bulk_prefetch_l2(ACC + (ln - 4) * ncells + (size_t)b * NCB, NCB * 8u);
+    const int pb = K == 1 ? b : blk[qtr];
+    const float *ps = K == 1 ? sigb : SIG + (size_t)pb * NDIM * 6 * B::n;
+    if (ln < NDIM && ln != DIR - 1 && P.fmode != 3) bulk_prefetch_l2(ps + (size_t)ln * 6 * B::n, 6u * B::n * 4u);
+    if (!FIRST && ln >= 4 && ln < 9) bulk_prefetch_l2(ACC + (ln - 4) * ncells + (size_t)pb * NCB, NCB * 8u);
     if (LAST && ln >= 12 && ln < 12 + 3 * (NDIM - 1))
-      bulk_prefetch_l2(AUX + (ln - 12) * ncells + (size_t)b * NCB, NCB * 8u);
+      bulk_prefetch_l2(AUX + (ln - 12) * ncells + (size_t)pb * NCB, NCB * 8u);
   }
 
   auto fidx = [](int along, int t1, int t2) { return G::at(along, t1 + (DIR == 1 ? NY : NX) * t2, G::LC, 1); };
@@ -246,30 +329,56 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
   // bytes), then the pressure and the guard cells' EOS in place; slabs
   // beyond a non-periodic boundary (mirror / copy rules) and all other
   // grids through load_prim.
-  bool tma = NDIM == 3 && tm.on && P.lh == nullptr && P.blk_nbr != nullptr;
-  int nbs[2] = {-1, -1};          // neighbour blocks below / above along DIR (-1: load_prim)
+  bool tma = NDIM == 3 && tm.on && P.lh == nullptr && P.blk_nbr != nullptr;   // always on runs (K > 1)
   unsigned long long *bar = reinterpret_cast<unsigned long long *>(smem_raw + G::smem_bytes() - 16 - 128);
   float *sRed = reinterpret_cast<float *>(smem_raw + G::smem_bytes() - 16 - 128 - G::red_bytes);
   if (tma) {
-    // the neighbours from the block's face-neighbour row (one load, not
-    // dependent on the coordinates)
-    nbs[0] = P.blk_nbr[6 * b + 2 * (DIR - 1)];
-    nbs[1] = P.blk_nbr[6 * b + 2 * (DIR - 1) + 1];
+    // the neighbours below / above along DIR (-1: load_prim) from the
+    // block's face-neighbour row (one load, not dependent on the
+    // coordinates), or from the run's row
+    if constexpr (K == 1) {
+      nbs[0] = P.blk_nbr[6 * b + 2 * (DIR - 1)];
+      nbs[1] = P.blk_nbr[6 * b + 2 * (DIR - 1) + 1];
+    }
     if (threadIdx.x == 0) mbar_init(bar, 1);
     __syncthreads();                          // the barrier is initialised before anyone polls it
-    if (threadIdx.x == 0) {
-      const unsigned slab_bytes = (unsigned)G::SLAB * 8u, mid_bytes = (unsigned)(G::ND * G::C) * 8u;
-      mbar_expect_tx(bar, 5u * (mid_bytes + (nbs[0] >= 0 ? slab_bytes : 0u) + (nbs[1] >= 0 ? slab_bytes : 0u)));
-      const int q5[5] = {0, 1, 2, 3, 5};       // staged slots of dens, velx, vely, velz, eint
-#pragma unroll
-      for (int v = 0; v < 5; ++v) {
-        double *dst = sV + q5[v] * G::SA;
-        tma_load_3d(dst + G::MID, &tm.intr[v], 0, 0, b * NZ, bar);
-        // the slab below: the neighbour's last four layers; above: its first four
+    // copies: the interior of each block of the run (quarter qtr of its
+    // cross-section) and the slabs of the neighbours along DIR, five
+    // variables; one thread issues them (K = 1) or the lanes of warp 0
+    // issue one each
+    constexpr int NOPS = 5 * (K + 2);
+    const int q5[5] = {0, 1, 2, 3, 5};         // staged slots of dens, velx, vely, velz, eint
+    const int qo = qtr * G::T2Q;                 // quarter offset on the slower transverse axis
+    auto copy = [&](int o) {
+      const int v = o / (K + 2), r = o % (K + 2);
+      double *dst = sV + q5[v] * G::SA;
+      if (r < K) {
+        tma_load_3d(dst + G::MID + r * G::MIDB, &tm.intr[v], 0, DIR == 3 ? qo : 0, blk[r] * NZ + (DIR == 3 ? 0 : qo),
+                    bar);
+      } else if (r == K) {
+        // the slab below: the neighbour's last four layers
         if (nbs[0] >= 0)
-          tma_load_3d(dst + G::LO, &tm.slab[v], DIR == 1 ? NX - 4 : 0, DIR == 2 ? NY - 4 : 0,
-                      nbs[0] * NZ + (DIR == 3 ? NZ - 4 : 0), bar);
-        if (nbs[1] >= 0) tma_load_3d(dst + G::HI, &tm.slab[v], 0, 0, nbs[1] * NZ, bar);
+          tma_load_3d(dst + G::LO, &tm.slab[v], DIR == 1 ? NX - 4 : 0, DIR == 2 ? NY - 4 : (DIR == 3 ? qo : 0),
+                      nbs[0] * NZ + (DIR == 3 ? NZ - 4 : qo), bar);
+      } else if (nbs[1] >= 0) {
+        // the slab above: its first four
+        tma_load_3d(dst + G::HI, &tm.slab[v], 0, DIR == 3 ? qo : 0, nbs[1] * NZ + (DIR == 3 ? 0 : qo), bar);
+      }
+    };
+    const unsigned slab_bytes = (unsigned)G::SLAB * 8u, mid_bytes = (unsigned)(K * G::MIDB) * 8u;
+    if constexpr (K == 1) {
+      if (threadIdx.x == 0) {
+        mbar_expect_tx(bar, 5u * (mid_bytes + (nbs[0] >= 0 ? slab_bytes : 0u) + (nbs[1] >= 0 ? slab_bytes : 0u)));
+#pragma unroll
+        for (int o = 0; o < NOPS; ++o) copy(o);
+      }
+    } else {
+      static_assert(NOPS <= 32, "one copy per lane of warp 0");
+      if (threadIdx.x < 32) {
+        if (threadIdx.x == 0)
+          mbar_expect_tx(bar, 5u * (mid_bytes + (nbs[0] >= 0 ? slab_bytes : 0u) + (nbs[1] >= 0 ? slab_bytes : 0u)));
+        __syncwarp();
+        if (threadIdx.x < NOPS) copy(threadIdx.x);
       }
     }
   }
@@ -278,9 +387,12 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
     int x, l, i, j, k;
     G::dec(s, G::L4, 4, x, l);
     if (tma && (x < 0 ? nbs[0] >= 0 : (x >= G::ND ? nbs[1] >= 0 : true))) continue;
-    G::cell(x, l, i, j, k);
+    int xl;
+    const int m = G::blk_of(x, xl);
+    G::cell(xl, l, qtr, i, j, k);
     double V[8];
-    load_prim<NDIM, NX, NY, NZ, false>(P, b, bc, i, j, k, V);
+    if constexpr (K == 1) load_prim<NDIM, NX, NY, NZ, false>(P, b, bc, i, j, k, V);
+    else load_prim<NDIM, NX, NY, NZ, false>(P, blk[m], blk_coords(P, blk[m]), i, j, k, V);
     const int q = G::sidx(x, l);
     sV[0 * G::SA + q] = V[HD]; sV[1 * G::SA + q] = V[HVX]; sV[2 * G::SA + q] = V[HVY];
     sV[3 * G::SA + q] = V[HVZ]; sV[4 * G::SA + q] = V[HP]; sV[5 * G::SA + q] = V[HEI];
@@ -361,9 +473,11 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
   // density and normal velocity over the CTA, for the learned gate's bound)
   float rg[6] = {3.0e38f, -3.0e38f, 3.0e38f, -3.0e38f, 3.0e38f, -3.0e38f};   // p, rho, u: min, max
   for (int t = threadIdx.x; t < G::SC; t += NT) {
-    int x, l, i, j, k;
+    int x, l, i, j, k, xl;
     G::dec(t, G::LC, 1, x, l);
-    G::cell(x, l, i, j, k);
+    const int mb = G::blk_of(x, xl);             // block of the run: its sig box covers xl in [-1, N]
+    G::cell(xl, l, qtr, i, j, k);
+    const float *sigc = K == 1 ? sigb : SIG + (size_t)blk[mb] * NDIM * 6 * B::n;
     const int s = G::sidx(x, l), sm = G::sidx(x - 1, l), sp = G::sidx(x + 1, l), q = G::at(x, l, G::LS, 2);
     const int qs = G::step;
     float Vc[8], dL[8], dR[8];
@@ -386,7 +500,7 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
       else if (dp1 == 0.) flat = t0;
       else flat = fmaxf(t0, sFlat[q - qs]);
     }
-    if (P.sp_flat)
+    if (K == 1 && P.sp_flat)
       P.sp_flat[sp_line_base<NDIM, NX, NY, NZ, DIR>(P.slot ? P.slot[b] : (int)blockIdx.x) + DirGeom<NDIM, NX, NY, NZ, double, DIR>::idx(i, j, k)] =
           double(flat);
     const int sl[6] = {0, 1, 2, 3, 4, 7};
@@ -471,9 +585,9 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
     // transverse corrections
     const int bi = B::idx(i, j, k);
     float sx[8], sy[8], sz[8];
-    if (DIR != 1) load_sig(sigb + 0 * 6 * B::n + bi, B::n, sx);
-    if (NDIM > 1 && DIR != 2) load_sig(sigb + 1 * 6 * B::n + bi, B::n, sy);
-    if (NDIM > 2 && DIR != 3) load_sig(sigb + 2 * 6 * B::n + bi, B::n, sz);
+    if (DIR != 1) load_sig(sigc + 0 * 6 * B::n + bi, B::n, sx);
+    if (NDIM > 1 && DIR != 2) load_sig(sigc + 1 * 6 * B::n + bi, B::n, sy);
+    if (NDIM > 2 && DIR != 3) load_sig(sigc + 2 * 6 * B::n + bi, B::n, sz);
 #pragma unroll
     for (int qq = 0; qq < 6; ++qq) {
       int n = sl[qq];
@@ -496,7 +610,7 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
       float T1[8], T2[8];
       {
         float sm[8], s0[8], sp[8];
-        const float *base = sigb + (size_t)(S1 - 1) * 6 * B::n;
+        const float *base = sigc + (size_t)(S1 - 1) * 6 * B::n;
         load_sig(base + B::idx(i - (A1 == 1), j - (A1 == 2), k - (A1 == 3)), B::n, sm);
         load_sig(base + bi, B::n, s0);
         load_sig(base + B::idx(i + (A1 == 1), j + (A1 == 2), k + (A1 == 3)), B::n, sp);
@@ -506,7 +620,7 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
       }
       {
         float sm[8], s0[8], sp[8];
-        const float *base = sigb + (size_t)(S2 - 1) * 6 * B::n;
+        const float *base = sigc + (size_t)(S2 - 1) * 6 * B::n;
         load_sig(base + B::idx(i - (A2 == 1), j - (A2 == 2), k - (A2 == 3)), B::n, sm);
         load_sig(base + bi, B::n, s0);
         load_sig(base + B::idx(i + (A2 == 1), j + (A2 == 2), k + (A2 == 3)), B::n, sp);
@@ -526,7 +640,7 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
 #pragma unroll
         for (int n = 0; n < 8; ++n) { dWm[n] = 0.f; dWp[n] = 0.f; }
       }
-      if (P.sp_fb)
+      if (K == 1 && P.sp_fb)
         P.sp_fb[sp_line_base<NDIM, NX, NY, NZ, DIR>(P.slot ? P.slot[b] : (int)blockIdx.x) + DirGeom<NDIM, NX, NY, NZ, double, DIR>::idx(i, j, k)] = fb;
     }
 #pragma unroll
@@ -773,13 +887,13 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
     for (int n = 0; n < 9; ++n) sF[n * G::SC + t] = Fr[it][n];
   }
   __syncthreads();
-  if (P.freg) {         // AMR: fine/coarse faces
+  if (K == 1 && P.freg) {         // AMR: fine/coarse faces
     flux_register<NDIM, NX, NY, NZ, DIR>(P, b, bc, sF, G::SC, [](int along, int t1, int t2) {
       return G::at(along, t1 + (DIR == 1 ? NY : NX) * t2, G::LC, 1);
     });
     __syncthreads();
   }
-  if (P.sp_mf) {        // face mass fluxes for the species pass
+  if (K == 1 && P.sp_mf) {        // face mass fluxes for the species pass
     for (int t = threadIdx.x; t < G::SC; t += NT) {
       int x, l, i, j, k;
       G::dec(t, G::LC, 1, x, l);
@@ -807,7 +921,7 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
     }
     __syncthreads();
   }
-  if (P.fmode == 1 || P.fmode == 2) {
+  if (K == 1 && (P.fmode == 1 || P.fmode == 2)) {
     flux_store<NDIM, NX, NY, NZ, DIR>(P, b, sF, G::SC, fidx, [&](int t) { return sF[8 * G::SC + t]; });
     if (P.fmode == 2) {
       if (st) atomicOr(P.status, st);
@@ -817,14 +931,17 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
 
   // ---- E: conservative update
   const double dtd = dt / delta;
-  CflCand cand; cand.key = 0.0; cand.val = 0.0; cand.idx = 0x7fffffff;
+  CflCand cand[K];                         // per block of the run
+#pragma unroll
+  for (int m = 0; m < K; ++m) { cand[m].key = 0.0; cand[m].val = 0.0; cand[m].idx = 0x7fffffff; }
   for (int t = threadIdx.x; t < G::SC; t += NT) {
-    int x, l, i, j, k;
+    int x, l, i, j, k, xl;
     G::dec(t, G::LC, 1, x, l);
     if (x < 0 || x >= G::ND) continue;
-    G::cell(x, l, i, j, k);
+    const int mb = G::blk_of(x, xl);
+    G::cell(xl, l, qtr, i, j, k);
     const int loc = (k * NY + j) * NX + i;
-    const size_t off = (size_t)b * NCB + loc;
+    const size_t off = (size_t)(K == 1 ? b : blk[mb]) * NCB + loc;
     double FL[NFLX], FR[NFLX];
 #pragma unroll
     for (int n = 0; n < NFLX; ++n) { FL[n] = sF[n * G::SC + t]; FR[n] = sF[n * G::SC + t + G::step]; }
@@ -886,10 +1003,26 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
       if (NDIM > 1) dtl = fmax(dtl, (fabs(vy) + cs) * (1.0 / del[1]));
       if (NDIM > 2) dtl = fmax(dtl, (fabs(vz) + cs) * (1.0 / del[2]));
       CflCand c; c.key = dtl * P.cfl; c.val = dtl; c.idx = loc;
-      cfl_merge(cand, c);
+#pragma unroll
+      for (int m = 0; m < K; ++m)
+        if (m == mb) cfl_merge(cand[m], c);
     }
   }
-  if (LAST) cfl_block_reduce<NX, NY, NZ>(cand, b, P.cfl, part);
+  if constexpr (LAST) {
+    if constexpr (K == 1) {
+      cfl_block_reduce<NX, NY, NZ>(cand[0], b, P.cfl, part);
+    } else {
+      // the CTA's candidate for each block of the run; k_cfl_runs merges
+      // the K quarters of every block (the same max / first-index rule, so
+      // the result equals a reduction over the whole block)
+      CflCand *cq = static_cast<CflCand *>(tm.cflq);
+#pragma unroll
+      for (int m = 0; m < K; ++m) {
+        const CflCand r = cfl_cta_merge(cand[m]);
+        if (threadIdx.x == 0) cq[(size_t)blk[m] * K + qtr] = r;
+      }
+    }
+  }
   if (st) atomicOr(P.status, st);
 }
 

@@ -31,6 +31,13 @@ typedef double Real;
 
 namespace fhy {
 
+// the mixed direction kernels take runs of kMxRun blocks (full uniform 3D
+// grids with run maps, the plain step)
+static bool use_runs(const StepArgs &a) {
+  return FHY_VARIANT == 3 && a.tma_run && a.nlev == 0 && a.P.blk_list == nullptr && a.P.fmode == 0 &&
+         a.nlaunch == a.nblocks;
+}
+
 template <int NDIM, int NX, int NY, int NZ, int DIR, bool FIRST, bool LAST, int RS>
 static bool launch_dir_one(const StepArgs &a) {
 #if FHY_VARIANT == 3
@@ -49,6 +56,22 @@ static bool launch_dir_one(const StepArgs &a) {
 #if FHY_VARIANT == 3
   TmaLine tl;
   memset(&tl, 0, sizeof tl);
+  if constexpr (NDIM == 3) {
+    // full uniform grid: runs of kMxRun blocks along the sweep
+    if (use_runs(a)) {
+      using GR = MxGeom<NDIM, NX, NY, NZ, DIR, RS, kMxRun>;
+      auto kr = k_dir_mx<NDIM, NX, NY, NZ, DIR, FIRST, LAST, RS, NT, kMxRun>;
+      const size_t smr = GR::smem_bytes();
+      if (a.set_attr && cudaFuncSetAttribute(kr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smr) != cudaSuccess)
+        return false;
+      tl = a.tma_run[DIR - 1];
+      kr<<<a.nlaunch, threads, smr, a.stream>>>(a.P, (const Real *)a.sig, a.acc, a.aux, a.ncells, a.part, tl);
+      if (LAST)
+        k_cfl_runs<NX, NY, kMxRun><<<(a.nblocks + 255) / 256, 256, 0, a.stream>>>(
+            static_cast<const CflCand *>(tl.cflq), a.nblocks, a.P.cfl, a.part);
+      return cudaGetLastError() == cudaSuccess;
+    }
+  }
   if (NDIM == 3 && a.tma && a.nlev == 0) tl = a.tma[DIR - 1];
   kern<<<a.nlaunch, threads, smem, a.stream>>>(a.P, (const Real *)a.sig, a.acc, a.aux, a.ncells, a.part, tl);
 #else
@@ -124,7 +147,7 @@ static int run_rs(const StepArgs &a) {
     const bool ok = launch_dir<NDIM, NX, NY, NZ, 1, true, false, RS>(a) &&
                     launch_dir<NDIM, NX, NY, NZ, 2, false, false, RS>(a) &&
                     launch_dir<NDIM, NX, NY, NZ, 3, false, true, RS>(a);
-    return ok ? nsig + 3 * nl : -2;
+    return ok ? nsig + 3 * nl + (use_runs(a) ? 1 : 0) : -2;   // + the CFL merge of the runs
   }
 }
 

@@ -353,10 +353,19 @@ int flash_hy_mark_refine_tree(flash_hy_ctx *ctx, int nvar, const int *vars, doub
  * trials are dropped; the next flash_hy_compute_dt recomputes dt from the
  * restored state.                                                         */
 #define FLASH_HY_TUNE_MAX 8
+/* mx_runs: blocks a CTA of the mixed-precision 3D direction kernels
+ * stages along the sweep -- 1, or FLASH_HY_MX_RUN where the context offers
+ * runs (a full uniform grid of 8^3 blocks whose block counts divide by it,
+ * no species): the CTA then takes runs of FLASH_HY_MX_RUN blocks and
+ * 1/FLASH_HY_MX_RUN of their cross-section, which shares the stencil
+ * overlap along the sweep.  Both give the same state and dt bit for bit.
+ * The default is FLASH_HY_MX_RUN where offered; autotune tries both.    */
+#define FLASH_HY_MX_RUN 4
 typedef struct {
   int sig_threads;
   int dir_threads;
   int mx_threads;
+  int mx_runs;
 } flash_hy_tuning;
 int flash_hy_get_tuning(flash_hy_ctx *ctx, flash_hy_tuning *out);
 int flash_hy_set_tuning(flash_hy_ctx *ctx, const flash_hy_tuning *t);
