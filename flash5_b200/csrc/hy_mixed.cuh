@@ -127,28 +127,6 @@ __device__ __forceinline__ void hllc_fp64(const DevParams &P, const double *Vm, 
   for (int n = 0; n < 5; ++n) Fs[n] = F[n] + S * (UC[n] - U[n]);
 }
 
-// CTA-wide merge of the threads' CFL candidates (cfl_merge: largest key,
-// first index on ties); the result is valid in thread 0.  Ends with a
-// barrier, so that it may be called again at once.
-__device__ __forceinline__ CflCand cfl_cta_merge(CflCand c) {
-  __shared__ CflCand red[32];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    CflCand b;
-    b.key = __shfl_down_sync(0xffffffffu, c.key, o);
-    b.val = __shfl_down_sync(0xffffffffu, c.val, o);
-    b.idx = __shfl_down_sync(0xffffffffu, c.idx, o);
-    if (lane + o < 32) cfl_merge(c, b);
-  }
-  if (lane == 0) red[w] = c;
-  __syncthreads();
-  if (threadIdx.x == 0)
-    for (int q = 1; q < (int)(blockDim.x + 31) / 32; ++q) cfl_merge(c, red[q]);
-  __syncthreads();
-  return c;
-}
-
 // Per block, the K quarter candidates of a run step merged into the block's
 // CFL result, as cfl_block_reduce writes it for a block handled whole
 // (Hydro_computeDt.F90:265-284).
@@ -245,10 +223,13 @@ struct MxGeom {
 
 // threads per CTA of k_dir_mx: three compiled candidates per block shape,
 // picked at run time (flash_hy_set_tuning / flash_hy_autotune); the middle
-// one is the default.  3D 8^3: 640 faces per direction (2 CTAs per SM by
-// shared memory); 2D 8^2: 80 faces; 2D 16^2: 288 faces.
+// one is the default.  3D 8^3: 640 line cells per direction and block (2
+// CTAs per SM by shared memory), 544 on a run of four (576 slope cells,
+// two per thread at 288 threads; the register file of each of the SM's four
+// schedulers holds five warps of 96 registers a thread at 288 and 320);
+// 2D 8^2: 80 faces; 2D 16^2: 288 faces.
 template <int NDIM, int NX, int NY, int NZ> struct MxThreads {
-  static constexpr int c0 = NDIM == 3 ? 256 : (NX == 8 ? 64 : 192);
+  static constexpr int c0 = NDIM == 3 ? 288 : (NX == 8 ? 64 : 192);
   static constexpr int c1 = NDIM == 3 ? 320 : (NX == 8 ? 96 : 288);
   static constexpr int c2 = NDIM == 3 ? 384 : (NX == 8 ? 128 : 320);
   static constexpr int n = c1;
@@ -1015,11 +996,30 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
       // the CTA's candidate for each block of the run; k_cfl_runs merges
       // the K quarters of every block (the same max / first-index rule, so
       // the result equals a reduction over the whole block)
-      CflCand *cq = static_cast<CflCand *>(tm.cflq);
+      // (one barrier: every warp reduces its K candidates, then thread m
+      // merges the warps' candidates of block m)
+      __shared__ CflCand red[32][K];
+      const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
       for (int m = 0; m < K; ++m) {
-        const CflCand r = cfl_cta_merge(cand[m]);
-        if (threadIdx.x == 0) cq[(size_t)blk[m] * K + qtr] = r;
+        CflCand c = cand[m];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          CflCand o2;
+          o2.key = __shfl_down_sync(0xffffffffu, c.key, o);
+          o2.val = __shfl_down_sync(0xffffffffu, c.val, o);
+          o2.idx = __shfl_down_sync(0xffffffffu, c.idx, o);
+          if (lane + o < 32) cfl_merge(c, o2);
+        }
+        if (lane == 0) red[w][m] = c;
+      }
+      __syncthreads();
+      if (threadIdx.x < K) {
+        const int m = threadIdx.x;
+        CflCand a = red[0][m];
+        for (int q = 1; q < NT / 32; ++q) cfl_merge(a, red[q][m]);
+        const int bm = tm.runs[(size_t)(blockIdx.x / K) * (K + 2) + m];   // blk[m] (not indexed at run time)
+        static_cast<CflCand *>(tm.cflq)[(size_t)bm * K + qtr] = a;
       }
     }
   }

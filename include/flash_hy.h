@@ -358,8 +358,9 @@ int flash_hy_mark_refine_tree(flash_hy_ctx *ctx, int nvar, const int *vars, doub
  * runs (a full uniform grid of 8^3 blocks whose block counts divide by it,
  * no species): the CTA then takes runs of FLASH_HY_MX_RUN blocks and
  * 1/FLASH_HY_MX_RUN of their cross-section, which shares the stencil
- * overlap along the sweep.  Both give the same state and dt bit for bit.
- * The default is FLASH_HY_MX_RUN where offered; autotune tries both.    */
+ * overlap along the sweep.  The two are separately compiled FMA-contracted
+ * kernels, like the mx_threads candidates, and agree to rounding.  The
+ * default is FLASH_HY_MX_RUN where offered; autotune tries both.        */
 #define FLASH_HY_MX_RUN 4
 typedef struct {
   int sig_threads;

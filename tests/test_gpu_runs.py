@@ -5,11 +5,13 @@ mixed-precision direction kernels stage runs of four blocks that follow one
 another along the sweep, a quarter of their cross-section per CTA, and the
 last direction merges the quarters' CFL candidates per block (tuning
 mx_runs = 4, the default there); with mx_runs = 1 a CTA takes one block.
-Both must give the same state, bit for bit, and the same time step and
-location: each cell and face is computed by the same arithmetic, only the
-CTA that does it differs.  The step over a block list (FLASH4's
-Hydro(blockCount, blockList, ...), here listing every block) keeps one
-block per CTA too and must give the same state.  Cases: periodic
+Each cell and face is computed by the same source arithmetic either way,
+but the two are separately compiled FMA-contracted kernels, as the
+mx_threads candidates are: the time step locations must be equal, the time
+steps and every UNK variable equal to rounding (1e-13 of each variable's
+scale, floor 1).  The step over a block list (FLASH4's Hydro(blockCount,
+blockList, ...), here listing every block) takes one block per CTA through
+the same kernels as mx_runs = 1 and must match it bit for bit.  Cases: periodic
 Kelvin-Helmholtz with HLLC, and a rotated 3D Sod problem with outflow and
 reflecting boundaries (the slabs beyond them staged by the boundary rules)
 with the exact solver and a trained learned guess (strong waves at the
@@ -71,7 +73,7 @@ def test_runs_match_one_block_per_cta(case):
             t += dt
             d1, l1 = runs.compute_dt()
             d2, l2 = single.compute_dt()
-            assert d1 == d2 and tuple(l1) == tuple(l2), (d1, d2, l1, l2)
+            assert tuple(l1) == tuple(l2) and abs(d1 - d2) <= 1e-13 * d2, (d1, d2, l1, l2)
             dt_old, dt = dt, next_dt(d1, dt)
         # the run path was the one taken: the step's launches are the dt
         # store, k_sig, three direction kernels and the quarters' CFL merge
@@ -85,8 +87,9 @@ def test_runs_match_one_block_per_cta(case):
         listed.download(c)
         for v in VARS:
             x, y, z = (grid.interior(u)[..., VAR[v]] for u in (a, b, c))
-            assert np.array_equal(x, y), (v, float(np.abs(x - y).max()))
-            assert np.array_equal(x, z), (v, float(np.abs(x - z).max()))
+            lim = 1e-13 * max(float(np.abs(y).max()), 1.0)
+            assert float(np.abs(x - y).max()) <= lim, (v, float(np.abs(x - y).max()))
+            assert np.array_equal(y, z), (v, float(np.abs(y - z).max()))
     finally:
         runs.close()
         single.close()
