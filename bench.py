@@ -52,16 +52,17 @@ BYTES_PER_ZONE = 80.0          # read + write of 5 FP64 state variables
 # kernels) from ncu captures of the 160^3 KH step (dram__bytes_read.sum +
 # dram__bytes_write.sum over 4.096e6 zones), scaled to the workload by its
 # zone count (traffic grows in proportion)
-TRAFFIC_PER_ZONE = {"fp64": 1248.6, "mixed": 866.7, "mixed_exact": 841.6, "mixed_learned": 841.6}
+TRAFFIC_PER_ZONE = {"fp64": 1250.6, "mixed": 864.4, "mixed_exact": 893.5, "mixed_learned": 893.5}
 # Floating-point operations per zone-update of one step (k_sig + the three
-# direction kernels), counted by ncu on the 96^3 KH step:
+# direction kernels), counted by ncu on the same 160^3 KH step:
 # smsp__sass_thread_inst_executed_op_{dadd,dmul,dfma,fadd,fmul,ffma}_pred_on
 # (an FMA counts two), divided by the zones; and the FP64 pipe utilisation
-# (sm__pipe_fp64_cycles_active, % of peak over the kernels' active cycles).
-FLOPS_PER_ZONE = {"fp64": {"f64": 7629, "f32": 395, "fp64_pipe_pct": 26.5},
-                  "mixed": {"f64": 1313, "f32": 2322, "fp64_pipe_pct": 13.9},
-                  "mixed_exact": {"f64": 2243, "f32": 2368, "fp64_pipe_pct": 17.9},
-                  "mixed_learned": {"f64": 2243, "f32": 2368, "fp64_pipe_pct": 17.9}}
+# (sm__pipe_fp64_cycles_active, % of peak over the kernels' active cycles,
+# weighted by their durations).
+FLOPS_PER_ZONE = {"fp64": {"f64": 7626, "f32": 394, "fp64_pipe_pct": 27.1},
+                  "mixed": {"f64": 1192, "f32": 1984, "fp64_pipe_pct": 15.3},
+                  "mixed_exact": {"f64": 2120, "f32": 2035, "fp64_pipe_pct": 19.6},
+                  "mixed_learned": {"f64": 2120, "f32": 2035, "fp64_pipe_pct": 19.6}}
 # nominal vector peaks of a B200 at the 1965 MHz maximum SM clock: 148 SMs x
 # 64 FP64 (128 FP32) FMA lanes x 2 flops; no measured FP64/FP32 peak exists
 # for this pool, so the compute fractions are "of nominal"
@@ -874,7 +875,7 @@ def main():
                        "f32_frac": zps * fl["f32"] / 1e12 / FP32_PEAK_TFLOPS, "peak_kind": "nominal",
                        "fp64_pipe_pct_ncu": fl["fp64_pipe_pct"],
                        "note": "FLOPs per zone-update counted by ncu (SASS dadd/dmul/dfma, fadd/fmul/ffma; FMA = "
-                               "2) on the 96^3 step; peaks = 148 SMs x 64 FP64 / 128 FP32 FMA lanes x 2 x "
+                               "2) on the 160^3 step; peaks = 148 SMs x 64 FP64 / 128 FP32 FMA lanes x 2 x "
                                "1965 MHz"}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": warmup,
