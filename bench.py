@@ -285,7 +285,7 @@ def e2e_guard_inclusive(params, weights, dev, nblk=32, steps=3, warmup=2):
     h.close()
     zones = g.ncells
     return {"value": zones / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "zones": zones,
-            "host_unk_bytes": host.nbytes, "h2d_bytes_per_step": 6 * 8 * zones, "d2h_bytes_per_step": 10 * 8 * zones,
+            "host_unk_bytes": host.nbytes, "h2d_bytes_per_step": 6 * 8 * zones, "d2h_bytes_per_step": 5 * 8 * zones,
             "workload": f"3D Kelvin-Helmholtz {8 * nblk}^3, guard-inclusive FLASH UNK (16^3 cells per 8^3 block, "
                         "11 vars), pinned host memory, same path as the headline"}
 
@@ -907,12 +907,13 @@ def main():
         if e2e_ms is not None:
             nsp = args.nspecies + args.nmass_scalars
             line["e2e"] = {"value": total / (e2e_ms * 1e-3), "unit": UNIT,
-                           "h2d_bytes_per_step": (6 + nsp) * 8 * zones, "d2h_bytes_per_step": (10 + nsp) * 8 * zones,
+                           "h2d_bytes_per_step": (6 + nsp) * 8 * zones, "d2h_bytes_per_step": (5 + nsp) * 8 * zones,
                            "ms_per_step": e2e_ms,
                            "path": "flash_hy_upload + flash_hy_step + flash_hy_compute_dt + flash_hy_download, "
                                    "interior-only FLASH UNK (11 vars), pinned host memory; the upload packs DENS, "
-                                   "VEL*, EINT, ENER and the download the 10 owned variables (host threads gather / "
-                                   "scatter, copies pipelined by sub-chunk)"}
+                                   "VEL*, EINT, ENER, the download the 5 state variables, from which the host "
+                                   "writes the 10 owned ones (PRES, TEMP, GAMC, GAME, ENER by the gamma law; host "
+                                   "threads gather / scatter, copies pipelined by sub-chunk)"}
             if e2e_guard is not None:
                 line["e2e_guard_inclusive"] = e2e_guard
         if cpu is not None:

@@ -710,15 +710,16 @@ extern "C" int flash_hy_destroy(flash_hy_ctx *c) {
 // ---------------------------------------------------------------------------
 // UNK <-> device block store
 //
-// Only the variables the device needs (upload) or owns (download) cross
-// PCIe, packed as SoA [variable][cell] over the interiors: host threads
-// gather them from the caller's UNK (either layout, with or without guard
-// cells) into pinned buffers and the copy engine moves one sub-chunk while
-// the next is gathered; downloads run the other way (device pack, copy,
-// host scatter into the owned variables only; guard cells and variables the
-// device does not own keep the caller's values).  A device kernel converts
-// between the packed copy and the state (the upload's EOS, the download's
-// Eos_putData outputs).
+// Only the variables the device needs (upload) or the state it owns
+// (download) cross PCIe, packed as SoA [variable][cell] over the interiors:
+// host threads gather them from the caller's UNK (either layout, with or
+// without guard cells) into pinned buffers and the copy engine moves one
+// sub-chunk while the next is gathered; downloads run the other way (device
+// pack, copy, host scatter into the owned variables only; guard cells and
+// variables the device does not own keep the caller's values).  A device
+// kernel converts between the packed copy and the state (the upload's EOS;
+// on AMR hierarchies the download's Eos_putData outputs, which on uniform
+// grids the host derives from the five state variables).
 // ---------------------------------------------------------------------------
 struct HostLayout {
   int layout, nunk, ng[3], nt[3];
@@ -922,6 +923,8 @@ static cudaError_t run_workers(flash_hy_ctx *c, XferPool *x, F worker) {
 
 // gather (upload) or scatter (download) the packed variables of blocks
 // [b0, b1) between the caller's UNK and a pinned slot laid out [var][cell]
+// (non-temporal stores into the slot were measured slower: 232 vs 149 ms
+// for the 512^3 upload)
 static void host_gather(const flash_hy_ctx *c, const HostLayout &L, const PackList &pl, const double *unk, size_t b0,
                         size_t b1, double *slot) {
   const size_t n = (b1 - b0) * c->ncb;
@@ -950,6 +953,34 @@ static void host_scatter(const flash_hy_ctx *c, const HostLayout &L, const PackL
                                      ? 1
                                      : (size_t)L.nt[0] * L.nt[1] * L.nt[2];
           for (int q = 0; q < pl.n; ++q) unk[base + (size_t)pl.unk[q] * vstride] = slot[(size_t)q * n + t];
+        }
+}
+
+// Download of a uniform grid: only the five state variables (and the
+// species) cross PCIe; the host writes them and the gamma-law EOS outputs
+// of Eos_putData.F90:95-106 -- PRES, TEMP, GAMC, GAME, ENER -- with the same
+// IEEE double operations, in the same order, as k_pack_soa (bit-identical:
+// the host code has no FMA contraction).
+static void host_scatter_eos(const flash_hy_ctx *c, const HostLayout &L, const DevParams &P, double *unk, size_t b0,
+                             size_t b1, const double *slot, int nsp) {
+  const size_t n = (b1 - b0) * c->ncb;
+  const size_t vstride = L.layout == FLASH_HY_LAYOUT_VAR_FASTEST ? 1 : (size_t)L.nt[0] * L.nt[1] * L.nt[2];
+  const double gam1inv = P.gam1inv, ggprodinv = P.ggprodinv, abar = P.abar, gamma = P.gamma;
+  size_t t = 0;
+  for (size_t b = b0; b < b1; ++b)
+    for (int k = 0; k < c->nz; ++k)
+      for (int j = 0; j < c->ny; ++j)
+        for (int i = 0; i < c->nx; ++i, ++t) {
+          const size_t base = unk_index(L, b, i + L.ng[0], j + L.ng[1], k + L.ng[2], 0);
+          const double rho = slot[t], vx = slot[n + t], vy = slot[2 * n + t], vz = slot[3 * n + t],
+                       e = slot[4 * n + t];
+          const double ekin = 0.5 * (vx * vx + vy * vy + vz * vz);
+          const double pres = rho * e * gam1inv;
+          auto put = [&](int v, double val) { if (v >= 0) unk[base + (size_t)v * vstride] = val; };
+          put(L.v_dens, rho); put(L.v_velx, vx); put(L.v_vely, vy); put(L.v_velz, vz); put(L.v_eint, e);
+          put(L.v_pres, pres); put(L.v_temp, e * ggprodinv * abar); put(L.v_gamc, gamma);
+          put(L.v_game, pres / (e * rho) + 1); put(L.v_ener, e + ekin);
+          for (int q = 0; q < nsp; ++q) put(L.v_spec + q, slot[(size_t)(5 + q) * n + t]);
         }
 }
 
@@ -1001,7 +1032,16 @@ extern "C" int flash_hy_download(flash_hy_ctx *c, double *unk, int layout, int n
   int rc = make_layout(c, layout, nunk, vm, c->host_ng, L);
   if (rc) return fail(c, rc, "bad UNK layout or variable map%s", "");
   CUDA_OK(c, cudaSetDevice(c->device));
-  const PackList pl = pack_list(c, L, false);
+  // uniform grids: the five state variables and the species cross, the host
+  // derives the EOS outputs; AMR hierarchies: the ten owned variables (a
+  // parent's ENER is not eint + ekin)
+  const bool derive = !c->amr;
+  PackList pl = pack_list(c, L, false);
+  if (derive) {
+    pl.n = 5 + c->nsp;
+    for (int q = 0; q < 10; ++q) pl.at[q] = q < 5 ? q : -1;
+    pl.spec = c->nsp > 0 ? 5 : -1;
+  }
   if ((rc = ensure_stage(c, (size_t)(10 + c->nsp) * c->ncells * sizeof(double)))) return rc;
   XferPool *x = nullptr;
   if ((rc = xfer_pool(c, x))) return rc;
@@ -1032,7 +1072,9 @@ extern "C" int flash_hy_download(flash_hy_ctx *c, double *unk, int layout, int n
       if (r == cudaSuccess) r = cudaEventSynchronize(x->ev[t][s]);
       if (r != cudaSuccess) break;
       const size_t a = k * spb, a1 = a + spb < nb ? a + spb : nb;
-      host_scatter(c, L, pl, unk, a, a1, x->pinned + ((size_t)t * 2 + s) * x->slot_doubles);
+      const double *slot = x->pinned + ((size_t)t * 2 + s) * x->slot_doubles;
+      if (derive) host_scatter_eos(c, L, P, unk, a, a1, slot, c->nsp);
+      else host_scatter(c, L, pl, unk, a, a1, slot);
     }
     return r;
   });
