@@ -206,7 +206,7 @@ struct MxGeom {
   // reconstruction scratch and then for the face fluxes
   // (with the exact solver the slope scratch, dead during the Riemann
   // phase, also holds the learned-guess network, so it is at least that big)
-  static constexpr size_t prim_bytes = (size_t)6 * SA * 8;
+  static constexpr size_t prim_bytes = (size_t)5 * SA * 8;
   static constexpr size_t slope_bytes = (size_t)SB * 4 + (size_t)SB * 6 * 4;
   static constexpr size_t wp_off =
       (RS == 1 && slope_bytes < sizeof(xrs::MlpPacked)) ? sizeof(xrs::MlpPacked) : slope_bytes;
@@ -249,7 +249,7 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
   extern __shared__ __align__(16) unsigned char smem_dyn[];
   unsigned char *smem_raw =
       smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);          // tile destinations: 128-byte aligned
-  double *sV = reinterpret_cast<double *>(smem_raw);                     // [6][SA]: rho,u,v,w,p,e (sidx order)
+  double *sV = reinterpret_cast<double *>(smem_raw);                     // [5][SA]: rho,u,v,w,e (sidx order)
   unsigned char *reg = smem_raw + G::prim_bytes;
   float *sFlat = reinterpret_cast<float *>(reg);                          // [SB]
   float *sDb = sFlat + G::SB;                                             // [6][SB]
@@ -328,7 +328,7 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
     // variables; one thread issues them (K = 1) or the lanes of warp 0
     // issue one each
     constexpr int NOPS = 5 * (K + 2);
-    const int q5[5] = {0, 1, 2, 3, 5};         // staged slots of dens, velx, vely, velz, eint
+    const int q5[5] = {0, 1, 2, 3, 4};         // staged slots of dens, velx, vely, velz, eint
     const int qo = qtr * G::T2Q;                 // quarter offset on the slower transverse axis
     auto copy = [&](int o) {
       const int v = o / (K + 2), r = o % (K + 2);
@@ -376,7 +376,7 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
     else load_prim<NDIM, NX, NY, NZ, false>(P, blk[m], blk_coords(P, blk[m]), i, j, k, V);
     const int q = G::sidx(x, l);
     sV[0 * G::SA + q] = V[HD]; sV[1 * G::SA + q] = V[HVX]; sV[2 * G::SA + q] = V[HVY];
-    sV[3 * G::SA + q] = V[HVZ]; sV[4 * G::SA + q] = V[HP]; sV[5 * G::SA + q] = V[HEI];
+    sV[3 * G::SA + q] = V[HVZ]; sV[4 * G::SA + q] = V[HEI];
   }
   if (tma) {
     // bounded wait for the tile copies; a CTA that gives up flags
@@ -392,28 +392,28 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
       }
       return;
     }
-    // pressure of every copied cell; the guard cells' EOS first
-    // (Eos_getData.F90:80-96 on ENER = eint + ekin, as load_prim)
-    for (int s = threadIdx.x; s < G::SA; s += NT) {
-      int x, l;
-      G::dec(s, G::L4, 4, x, l);
-      const bool guard = x < 0 || x >= G::ND;
-      if (guard && nbs[x < 0 ? 0 : 1] < 0) continue;
+    // the copied guard cells' EOS (Eos_getData.F90:80-96 on ENER = eint +
+    // ekin, as load_prim); the pressure is not staged (Vs below)
+    for (int g = threadIdx.x; g < 8 * G::C; g += NT) {
+      const int side = g >= 4 * G::C, r = g - side * 4 * G::C;
+      if (nbs[side] < 0) continue;
+      const int x = side ? G::ND + r / G::C : r / G::C - 4, l = r % G::C;
       const int q = G::sidx(x, l);
-      const double rho = sV[q], e = sV[5 * G::SA + q];
-      double eg = e;
-      if (guard) {
-        const double vx = sV[G::SA + q], vy = sV[2 * G::SA + q], vz = sV[3 * G::SA + q];
-        const double ekin = 0.5 * (vx * vx + vy * vy + vz * vz);
-        const double ener = e + ekin;
-        if (ener - ekin > rmax(P.smalle, P.eswitch * ekin)) eg = ener - ekin;
-        sV[5 * G::SA + q] = eg;
-      }
-      sV[4 * G::SA + q] = rho * eg * P.gam1inv;
+      const double e = sV[4 * G::SA + q];
+      const double vx = sV[G::SA + q], vy = sV[2 * G::SA + q], vz = sV[3 * G::SA + q];
+      const double ekin = 0.5 * (vx * vx + vy * vy + vz * vz);
+      const double ener = e + ekin;
+      if (ener - ekin > rmax(P.smalle, P.eswitch * ekin)) sV[4 * G::SA + q] = ener - ekin;
     }
   }
   __syncthreads();
-  auto Vs = [&](int q, int s) -> double { return sV[q * G::SA + s]; };   // q: 0..5 (5 = eint)
+  // q: 0..5 = rho, u, v, w, p, e; the pressure of the gamma law from the
+  // staged rho and e, in the EOS's order (rho * e) * gam1inv
+  const double gam1inv = P.gam1inv;
+  auto Vs = [&](int q, int s) -> double {
+    if (q == 4) return sV[s] * sV[4 * G::SA + s] * gam1inv;
+    return sV[(q == 5 ? 4 : q) * G::SA + s];
+  };
 
   // ---- B: limited slopes and flattening switches of cells [-2, N+1]
   for (int q = threadIdx.x; q < G::SB; q += NT) {
