@@ -216,8 +216,15 @@ struct MxGeom {
   // staging barrier and the slack that aligns the tile destinations to 128
   // bytes
   static constexpr size_t red_bytes = 16 * 6 * 4;
+  // runs (K > 1) keep the face fluxes in their own region, so that the
+  // Riemann phase writes them as it goes (two CTAs per SM still fit); one
+  // block per CTA lays them over the reconstruction scratch and holds them
+  // in registers until that is dead
+  static constexpr bool own_flux = K > 1;
+  static constexpr size_t flux_off = own_flux ? recon_bytes : 0;
   static constexpr size_t smem_bytes() {
-    return prim_bytes + (recon_bytes > flux_bytes ? recon_bytes : flux_bytes) + red_bytes + 16 + 128;
+    return prim_bytes + (own_flux ? recon_bytes + flux_bytes : (recon_bytes > flux_bytes ? recon_bytes : flux_bytes)) +
+           red_bytes + 16 + 128;
   }
 };
 
@@ -256,7 +263,7 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
   float *sWp = reinterpret_cast<float *>(reg + G::wp_off);                // [6][SC] increments
   float *sWm = sWp + 6 * G::SC;                                           // [6][SC]
   double *sIg = reinterpret_cast<double *>(sWm + 6 * G::SC);              // [SC] 1/(game-1)
-  double *sF = reinterpret_cast<double *>(reg);                           // [9][SC] (after phase D)
+  double *sF = reinterpret_cast<double *>(reg + G::flux_off);            // [9][SC] face fluxes
 
   static_assert((6 * B::n * 4) % 16 == 0 && (NCB * 8) % 16 == 0, "bulk prefetch sizes must be multiples of 16 bytes");
   // the tile copies' descriptors load while the block's indices do
@@ -817,12 +824,17 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
       F[FEINT] = fe;
       F[FVOLU] = fv;
       F[8] = (Vs(4, s.x) + double(sWm[4 * G::SC + t])) + (Vs(4, s.x) + double(sWp[4 * G::SC + t]));
+      if constexpr (G::own_flux) {
 #pragma unroll
-      for (int j = 0; j < NIT; ++j)
-        if (j == it) {
+        for (int n = 0; n < 9; ++n) sF[n * G::SC + t] = F[n];
+      } else {
 #pragma unroll
-          for (int n = 0; n < 9; ++n) Fr[j][n] = F[n];
-        }
+        for (int j = 0; j < NIT; ++j)
+          if (j == it) {
+#pragma unroll
+            for (int n = 0; n < 9; ++n) Fr[j][n] = F[n];
+          }
+      }
     }
   } else {
 #pragma unroll
@@ -841,31 +853,38 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
       VL[n] = Vs(qq, sL) + double(sWp[qq * G::SC + tl]);
       VR[n] = Vs(qq, s) + double(sWm[qq * G::SC + t]);
     }
-    double F[6];
+    double F[9];
     hllc_fp64<DIR>(P, VL, VR, sIg[tl], sIg[t], F, st);
-#pragma unroll
-    for (int n = 0; n < 6; ++n) Fr[it][n] = F[n];
     double fv = 0., fe = 0.;
     if (P.use_aux_eint) {
       if (F[FDENS] > 0.) { fv = F[FDENS] / VL[HD]; fe = F[FDENS] * VL[HEI]; }
       else { fv = F[FDENS] / VR[HD]; fe = F[FDENS] * VR[HEI]; }
     }
-    Fr[it][FEINT] = fe;
-    Fr[it][FVOLU] = fv;
+    F[FEINT] = fe;
+    F[FVOLU] = fv;
     // N05 + P05 of this cell (n+1/2 pressure sum)
-    Fr[it][8] = (Vs(4, s) + double(sWm[4 * G::SC + t])) + (Vs(4, s) + double(sWp[4 * G::SC + t]));
+    F[8] = (Vs(4, s) + double(sWm[4 * G::SC + t])) + (Vs(4, s) + double(sWp[4 * G::SC + t]));
+#pragma unroll
+    for (int n = 0; n < 9; ++n) {
+      if constexpr (G::own_flux) sF[n * G::SC + t] = F[n];
+      else Fr[it][n] = F[n];
+    }
   }
   }
-  __syncthreads();
+  if constexpr (!G::own_flux) {
+    // the fluxes go over the reconstruction scratch once every thread is
+    // done reading it
+    __syncthreads();
 #pragma unroll
-  for (int it = 0; it < NIT; ++it) {
-    const int t = threadIdx.x + it * NT;
-    if (t >= G::SC) break;
-    int x, l;
-    G::dec(t, G::LC, 1, x, l);
-    if (x < 0) continue;
+    for (int it = 0; it < NIT; ++it) {
+      const int t = threadIdx.x + it * NT;
+      if (t >= G::SC) break;
+      int x, l;
+      G::dec(t, G::LC, 1, x, l);
+      if (x < 0) continue;
 #pragma unroll
-    for (int n = 0; n < 9; ++n) sF[n * G::SC + t] = Fr[it][n];
+      for (int n = 0; n < 9; ++n) sF[n * G::SC + t] = Fr[it][n];
+    }
   }
   __syncthreads();
   if (K == 1 && P.freg) {         // AMR: fine/coarse faces
