@@ -216,11 +216,11 @@ struct MxGeom {
   // staging barrier and the slack that aligns the tile destinations to 128
   // bytes
   static constexpr size_t red_bytes = 16 * 6 * 4;
-  // runs (K > 1) keep the face fluxes in their own region, so that the
-  // Riemann phase writes them as it goes (two CTAs per SM still fit); one
-  // block per CTA lays them over the reconstruction scratch and holds them
-  // in registers until that is dead
-  static constexpr bool own_flux = K > 1;
+  // runs (K > 1) and 2D blocks keep the face fluxes in their own region,
+  // so that the Riemann phase writes them as it goes (the CTAs per SM that
+  // the registers allow still fit); one 3D block per CTA lays them over the
+  // reconstruction scratch and holds them in registers until that is dead
+  static constexpr bool own_flux = K > 1 || NDIM == 2;
   static constexpr size_t flux_off = own_flux ? recon_bytes : 0;
   static constexpr size_t smem_bytes() {
     return prim_bytes + (own_flux ? recon_bytes + flux_bytes : (recon_bytes > flux_bytes ? recon_bytes : flux_bytes)) +
