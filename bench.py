@@ -460,7 +460,7 @@ def riemann_run(args, n=None, steps=None, warmup=None):
     """Isolated exact Riemann solves (1e8 interface pairs): two-rarefaction
     guess vs the learned guess trained on solver-harvested states."""
     import torch
-    from flash5_b200.riemann import ExactRiemann
+    from flash5_b200.riemann import INFER_TCGEN05, INFER_WARP_MMA, ExactRiemann
     torch.cuda.set_device(0)
     n = n or args.riemann_n
     steps = steps or args.steps
@@ -468,11 +468,11 @@ def riemann_run(args, n=None, steps=None, warmup=None):
     r = ExactRiemann(0)
     stream = r.stream
     # training set harvested from the solver's own solves of another seed
-    Str = r.generate(1, 2_000_000)
+    Str = r.generate(1, args.riemann_train_n)
     otr, _, _ = r.solve(Str, learned=False)
     X, T, ns = r.make_samples(Str, otr)
     t0 = time.perf_counter()
-    loss = r.train(X, T, ns, epochs=8, batch=4096, lr=2e-3)
+    loss = r.train(X, T, ns, epochs=args.riemann_epochs, batch=4096, lr=2e-3)
     train_s = time.perf_counter() - t0
     del Str, otr, X, T
     S = r.generate(20251203, n)
@@ -480,7 +480,11 @@ def riemann_run(args, n=None, steps=None, warmup=None):
     its = r.empty(n, dtype=torch.uint8)
     flg = r.empty(n, dtype=torch.uint8)
     res = {}
-    for learned in (False, True):
+    # learned: the network on the tcgen05 tensor cores (the default);
+    # learned_warp_mma: the same network per warp on mma.sync
+    for name, learned, mode in (("two_rarefaction", False, INFER_TCGEN05), ("learned", True, INFER_TCGEN05),
+                                ("learned_warp_mma", True, INFER_WARP_MMA)):
+        r.set_inference(mode)
         for _ in range(max(1, warmup)):
             r.solve(S, learned, out=out, iters=its, flags=flg)
         torch.cuda.synchronize()
@@ -495,10 +499,12 @@ def riemann_run(args, n=None, steps=None, warmup=None):
         fl = flg.cpu().numpy()
         ok = (fl & 2) == 0
         hist = np.bincount(it[ok], minlength=12)[:12].tolist()
-        res["learned" if learned else "two_rarefaction"] = {
+        res[name] = {
             "solves_per_s": n / (ms * 1e-3), "ms": ms, "mean_iters": float(it[ok].mean()), "iter_hist": hist,
             "fallback_frac": float(((fl & 1) != 0)[ok].mean()), "nonconverged": int(((fl & 4) != 0).sum()),
             "vacuum": int((~ok).sum()), "pstar": out[0].clone(), "_it": it, "_fl": fl}
+    r.set_inference(INFER_TCGEN05)
+    assert r.sync() == 0
     # where the network was consulted (strong waves, inexact two-rarefaction
     # guess): evaluations of both starts on those solves
     cons = (res["learned"]["_fl"] & 8) != 0
@@ -508,21 +514,26 @@ def riemann_run(args, n=None, steps=None, warmup=None):
         res[k]["mean_iters_where_consulted"] = float(it[cons].mean()) if cons.any() else None
     consulted_frac = float(cons.mean())
     # the network alone, dense over every pair: features + 8-64-64-1 BF16
-    # inference (what the learned start costs per consulted solve at best)
-    for _ in range(max(1, warmup)):
-        yv = r.predict(S)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(steps):
-        yv = r.predict(S)
-    e1.record(stream)
-    e1.synchronize()
-    predict_ms = e0.elapsed_time(e1) / steps
-    del yv
-    p0, p1 = res["two_rarefaction"].pop("pstar"), res["learned"].pop("pstar")
+    # inference (what the learned start costs per consulted solve at best),
+    # on the tcgen05 tensor cores and per warp on mma.sync
+    predict_ms = {}
+    for name, mode in (("tcgen05", INFER_TCGEN05), ("warp_mma", INFER_WARP_MMA)):
+        r.set_inference(mode)
+        for _ in range(max(1, warmup)):
+            yv = r.predict(S)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            yv = r.predict(S)
+        e1.record(stream)
+        e1.synchronize()
+        predict_ms[name] = e0.elapsed_time(e1) / steps
+        del yv
+    r.set_inference(INFER_TCGEN05)
+    p0, p1, p2 = (res[k].pop("pstar") for k in ("two_rarefaction", "learned", "learned_warp_mma"))
     okd = torch.tensor(ok, device=p0.device)
-    rel = ((p1 - p0).abs() / p0.clamp_min(1e-300))[okd].max().item()
+    rel = max(((p - p0).abs() / p0.clamp_min(1e-300))[okd].max().item() for p in (p1, p2))
     r.close()
     del S, out, its, flg, p0, p1
     torch.cuda.empty_cache()
@@ -532,14 +543,15 @@ def riemann_run(args, n=None, steps=None, warmup=None):
             "vs_baseline": None, "dtype": "f64 Newton, bf16 MLP (f32 acc)",
             "data": "synthetic (splitmix64 seed 20251203)",
             "config": {"workload": f"{n:.0e} isolated interface pairs: p ratio log-uniform 1e-4..1e4, rho ratio "
-                                   "1e-3..1e3, u uniform +-5 c, gamma in {1.4, 5/3}; MLP 8-64-64-1 BF16 on tensor "
-                                   "cores (mma.sync)"},
+                                   "1e-3..1e3, u uniform +-5 c, gamma in {1.4, 5/3}; MLP 8-64-64-1 BF16 on tcgen05 "
+                                   "tensor cores (TMEM accumulator, 128 interfaces per MMA tile)"},
             "paths": res, "speedup_vs_two_rarefaction": res["two_rarefaction"]["ms"] / res["learned"]["ms"],
             "max_rel_pstar_diff_learned_vs_tr": rel, "consulted_frac": consulted_frac,
             "network_dense_ms": predict_ms,
-            "network_dense_note": "k_predict over every pair (features + tensor-core MLP, written out): the network's "
-                                  "own cost per solve, against the Newton evaluations it saves where consulted",
-            "training": {"samples": ns, "epochs": 8, "final_mse": loss, "seconds": train_s}}
+            "network_dense_note": "the network over every pair (features + tensor-core MLP, written out), tcgen05 "
+                                  "and per-warp mma.sync: its own cost per solve, against the Newton evaluations it "
+                                  "saves where consulted",
+            "training": {"samples": ns, "epochs": args.riemann_epochs, "final_mse": loss, "seconds": train_s}}
 
 
 # ---------------------------------------------------------------------------
@@ -721,6 +733,9 @@ def main():
     ap.add_argument("--workload", default="kh", choices=["kh", "riemann", "amr"])
     ap.add_argument("--amr-nblk", type=int, default=32, help="root blocks per axis of the AMR hierarchy")
     ap.add_argument("--riemann-n", type=int, default=100_000_000)
+    # training set of the isolated workload's network (smaller for profiling runs)
+    ap.add_argument("--riemann-train-n", type=int, default=2_000_000)
+    ap.add_argument("--riemann-epochs", type=int, default=8)
     ap.add_argument("--paths", default="fp64,fp64_exact,mixed,mixed_exact,mixed_learned",
                     help="comma list of paths to time; profiling runs use one")
     args = ap.parse_args()

@@ -2,8 +2,10 @@
 // initial guess for the star pressure, and the hand-written training of that
 // guess (no counterpart in FLASH5, whose unsplit path only has approximate
 // solvers, hy_getFaceFlux.F90:324-372).  The solver itself (Toro ch. 4) and
-// the tensor-core network inference live in exact_rs.cuh, shared with the
-// hydro face fluxes.
+// the per-warp tensor-core network inference (mma.sync) live in
+// exact_rs.cuh, shared with the hydro face fluxes; the batched solves and
+// predictions run the network on the tcgen05 tensor cores by default
+// (k_solve_tc, primitives in tc05.cuh).
 //
 // Learned path: Newton gets three evaluations from the network's guess; if
 // that does not converge, the solve restarts from the two-rarefaction guess
@@ -21,6 +23,7 @@
 #include <string.h>
 #include "../../include/flash_hy.h"
 #include "exact_rs.cuh"
+#include "tc05.cuh"
 
 namespace rx {
 
@@ -43,12 +46,65 @@ __device__ __forceinline__ void load_state(const double *__restrict__ S, long n,
   L.w = powp(L.p, G.z); R.w = powp(R.p, G.z);
 }
 
+// the state of pair i, or a harmless placeholder for a lane past the end
+// (lanes of the last tile take part in the warp and CTA collectives)
+__device__ __forceinline__ void load_or_dummy(const double *__restrict__ S, long n, long i, bool valid, Side &L,
+                                              Side &R, Gas &G) {
+  if (valid) {
+    load_state(S, n, i, L, R, G);
+  } else {
+    G = gas_of(1.4);
+    L.d = R.d = 1.0; L.u = R.u = 0.0; L.p = R.p = 1.0; L.c = R.c = sqrt(1.4); L.w = R.w = 1.0;
+  }
+}
+
+// Newton from w0 (three evaluations where the network gave the start, else
+// max_iter) and the recording of the result; returns true where a network
+// start did not converge, so that the pair is queued for k_fallback
+__device__ __forceinline__ bool solve_store(const Side &L, const Side &R, const SideK &kl, const SideK &kr,
+                                            const Gas &G, bool vac, bool net, double w0, double tol, int max_iter,
+                                            bool valid, long i, long n, double *__restrict__ out,
+                                            unsigned char *__restrict__ iters, unsigned char *__restrict__ flags,
+                                            unsigned &st) {
+  unsigned char fl = net ? 8 : 0;
+  int its = 0;
+  bool pending = false;
+  Star S{0.0, 0.5 * (L.u + R.u), 0.0};
+  if (vac) {
+    fl |= 2;
+  } else {
+    int k = newton(L, R, kl, kr, G, w0, tol, net ? 3 : max_iter, S);
+    if (k > 0) its = k;
+    else if (net) pending = true;
+    else { its = max_iter; fl |= 4; st |= FLASH_HY_ERR_NEWTON_NOCONV; }
+  }
+  if (valid && !pending) {
+    out[i] = S.p; out[n + i] = S.u;
+    if (iters) iters[i] = (unsigned char)(its > 255 ? 255 : its);
+    if (flags) flags[i] = fl;
+  }
+  return pending;
+}
+
+// append the warp's pending lanes to the fallback queue (one atomic per warp)
+__device__ __forceinline__ void enqueue(bool pending, long i, int *queue, int *qcount) {
+  const int lane = threadIdx.x & 31;
+  const unsigned m = __ballot_sync(0xffffffffu, pending);
+  if (m) {
+    int base_q = 0;
+    if (lane == __ffs(m) - 1) base_q = atomicAdd(qcount, __popc(m));
+    base_q = __shfl_sync(0xffffffffu, base_q, __ffs(m) - 1);
+    if (pending) queue[base_q + __popc(m & ((1u << lane) - 1))] = (int)i;
+  }
+}
+
 // learned != 0: Newton gets three evaluations from the network's guess where
 // the network is consulted (strong waves, inexact two-rarefaction guess;
 // elsewhere the two-rarefaction start with the full iteration budget);
 // lanes that have not converged are appended to `queue` (warp-aggregated
 // atomics) and re-solved from the two-rarefaction guess by k_fallback, so no
-// warp waits for a fallback lane.
+// warp waits for a fallback lane.  Here the network runs per warp on
+// mma.sync (mlp_lane); k_solve_tc below is the tcgen05 form.
 // One instantiation per path, so that the two-rarefaction path does not
 // carry the network's register footprint.
 template <bool learned>
@@ -58,7 +114,6 @@ k_solve(const double *__restrict__ S, long n, double *__restrict__ out, unsigned
         int *qcount, unsigned *status) {
   __shared__ __align__(16) MlpPacked M;
   if (learned) { load_packed(M, w); __syncthreads(); }
-  const int lane = threadIdx.x & 31;
   const long stride = (long)gridDim.x * blockDim.x;
   unsigned st = 0;
   // grid-stride loop whose trip count is uniform across a warp
@@ -67,12 +122,7 @@ k_solve(const double *__restrict__ S, long n, double *__restrict__ out, unsigned
     const bool valid = i < n;
     Side L, R;
     Gas G;
-    if (valid) {
-      load_state(S, n, i, L, R, G);
-    } else {
-      G = gas_of(1.4);
-      L.d = R.d = 1.0; L.u = R.u = 0.0; L.p = R.p = 1.0; L.c = R.c = sqrt(1.4); L.w = R.w = 1.0;
-    }
+    load_or_dummy(S, n, i, valid, L, R, G);
     const SideK kl = side_k(L, G), kr = side_k(R, G);
     const bool vac = vacuum(L, R, G);
     const double wtr = vac ? 0.0 : tr_w(L, R, kl, kr, G);
@@ -91,34 +141,245 @@ k_solve(const double *__restrict__ S, long n, double *__restrict__ out, unsigned
         if (net) w0 = wtr * (double)expf(float(G.z) * y);    // (p*/p_TR)^z
       }
     }
-    unsigned char fl = net ? 8 : 0;
-    int its = 0;
-    bool pending = false;
-    Star S{0.0, 0.5 * (L.u + R.u), 0.0};
-    if (vac) {
-      fl |= 2;
-    } else {
-      int k = newton(L, R, kl, kr, G, w0, tol, net ? 3 : max_iter, S);
-      if (k > 0) its = k;
-      else if (net) pending = true;
-      else { its = max_iter; fl |= 4; st |= FLASH_HY_ERR_NEWTON_NOCONV; }
-    }
-    if (learned) {
-      const unsigned m = __ballot_sync(0xffffffffu, pending && valid);
-      if (m) {
-        int base_q = 0;
-        if (lane == __ffs(m) - 1) base_q = atomicAdd(qcount, __popc(m));
-        base_q = __shfl_sync(0xffffffffu, base_q, __ffs(m) - 1);
-        if (pending && valid) queue[base_q + __popc(m & ((1u << lane) - 1))] = (int)i;
-      }
-    }
-    if (valid && !pending) {
-      out[i] = S.p; out[n + i] = S.u;
-      if (iters) iters[i] = (unsigned char)(its > 255 ? 255 : its);
-      if (flags) flags[i] = fl;
-    }
+    const bool pending = solve_store(L, R, kl, kr, G, vac, net, w0, tol, max_iter, valid, i, n, out, iters, flags, st);
+    if (learned) enqueue(pending && valid, i, queue, qcount);
   }
   if (st) atomicOr(status, st);
+}
+
+// ---------------------------------------------------------------------------
+// The learned path with the network on the fifth-generation tensor cores.
+// A CTA of 128 threads takes tiles of 128 pairs (one per thread, grid-stride
+// over tiles).  Where any pair of the tile consults the network, thread m
+// writes row m of the tile's feature matrix to shared memory and one thread
+// issues the three layers as tcgen05.mma with the accumulator in TMEM:
+//   layer 1  [128 x 16] x [16 x 64]: K holds the 8 features, then 1, 1
+//            against the bias split into BF16 high and low parts;
+//   layer 2  [128 x 80] x [80 x 64]: K holds the 64 hidden units, then 1, 1
+//            against the bias's two parts;
+//   layer 3  [128 x 64] x [64 x 16]: N column 0 the BF16 high part of w3,
+//            column 1 its low part, y = D[m][0] + D[m][1] + b3.
+// Between the layers each thread reads its row back (tcgen05.ld), and one
+// cvt.rn.relu.bf16x2 per two units gives the BF16 operands of the next
+// layer.  The BF16 operands, FP32 accumulation and the weights are those of
+// mlp_lane; the FP32 biases and w3 enter as two BF16 parts (16 significant
+// bits) and the accumulation order differs, so the output agrees with
+// mlp_lane to that rounding.  SOLVE = false writes the network's output
+// for every pair (0 for vacuum) instead of solving.
+//
+// Waits on the MMA completions are bounded (about a second of SM clocks);
+// a CTA that gives up sets FLASH_HY_ERR_TIMEOUT, waits (bounded) for the MMA
+// in flight, frees its TMEM and leaves.
+// ---------------------------------------------------------------------------
+constexpr int TC_THREADS = 128;
+constexpr uint32_t TC_TMEM_COLS = 64;           // one 128 x 64 FP32 accumulator, reused by the three layers
+constexpr long long kTcWaitCycles = 1LL << 31;
+constexpr int kK1 = 16, kK2 = NH + 16;          // padded K of layers 1 and 2
+constexpr uint32_t kLbo = 128;                  // core matrices along K
+constexpr uint32_t kSboA1 = kK1 / 8 * 128, kSboA2 = kK2 / 8 * 128, kSboW3 = NH / 8 * 128;
+
+struct __align__(128) TcSmem {
+  uint8_t X[128 * kK2 * 2];                     // the tile's A operand: features, then hidden rows of layer 2, of layer 3
+  uint8_t W2[NH * kK2 * 2];                     // [n][k]: W2, then b2 high, b2 low
+  uint8_t W1[NH * kK1 * 2];                     // [n][k]: W1, then b1 high, b1 low
+  uint8_t W3[16 * NH * 2];                      // [n][k]: n = 0 w3 high, n = 1 w3 low, others 0
+  float b3;
+  uint32_t tmem_base;
+  int fail;
+  unsigned long long bar;
+};
+
+__device__ __forceinline__ void split_bf16(float x, __nv_bfloat16 &hi, __nv_bfloat16 &lo) {
+  hi = __float2bfloat16_rn(x);
+  lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+}
+__device__ __forceinline__ uint32_t bf16_bits(__nv_bfloat16 v) { return (uint32_t)__bfloat16_as_ushort(v); }
+// {relu(lo), relu(hi)} rounded to BF16, lo in the low half
+__device__ __forceinline__ uint32_t relu_bf16x2(float lo, float hi) {
+  uint32_t d;
+  asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;\n" : "=r"(d) : "f"(hi), "f"(lo));
+  return d;
+}
+
+template <bool SOLVE>
+__global__ void __launch_bounds__(TC_THREADS, 4)
+k_solve_tc(const double *__restrict__ S, long n, double *__restrict__ out, unsigned char *__restrict__ iters,
+           unsigned char *__restrict__ flags, const MlpPacked *__restrict__ w, double tol, int max_iter, int *queue,
+           int *qcount, unsigned *status, float *__restrict__ yout) {
+  __shared__ TcSmem sm;
+  const int t = threadIdx.x, wid = t >> 5;
+  const uint4 ones = make_uint4(0x3F803F80u, 0u, 0u, 0u);      // BF16 1.0, 1.0, then zeros
+  {
+    // weights into the canonical layouts (16-byte chunks of 8 values along K)
+    const uint4 *W1g = reinterpret_cast<const uint4 *>(&w->W1[0][0]);
+    const uint4 *W2g = reinterpret_cast<const uint4 *>(&w->W2[0][0]);
+    if (t < NH) {
+      __nv_bfloat16 h1, l1, h2, l2;
+      split_bf16(w->b1[t], h1, l1);
+      split_bf16(w->b2[t], h2, l2);
+      *reinterpret_cast<uint4 *>(sm.W1 + tc05::canon_off(t, 0, kSboA1)) = W1g[2 * t];
+      *reinterpret_cast<uint4 *>(sm.W1 + tc05::canon_off(t, 1, kSboA1)) =
+          make_uint4(bf16_bits(h1) | (bf16_bits(l1) << 16), 0u, 0u, 0u);
+      *reinterpret_cast<uint4 *>(sm.W2 + tc05::canon_off(t, 8, kSboA2)) =
+          make_uint4(bf16_bits(h2) | (bf16_bits(l2) << 16), 0u, 0u, 0u);
+      *reinterpret_cast<uint4 *>(sm.W2 + tc05::canon_off(t, 9, kSboA2)) = make_uint4(0u, 0u, 0u, 0u);
+    }
+    for (int q = t; q < NH * NH / 8; q += TC_THREADS)
+      *reinterpret_cast<uint4 *>(sm.W2 + tc05::canon_off(q >> 3, q & 7, kSboA2)) = W2g[q];
+    // W3: 16 rows x 8 chunks; thread t fills chunk t & 7 of row t >> 3
+    {
+      const int row = t >> 3, c = t & 7;
+      uint32_t v[4] = {0u, 0u, 0u, 0u};
+      if (row < 2) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          __nv_bfloat16 ha, la, hb, lb;
+          split_bf16(w->w3[8 * c + 2 * e], ha, la);
+          split_bf16(w->w3[8 * c + 2 * e + 1], hb, lb);
+          v[e] = row == 0 ? (bf16_bits(ha) | (bf16_bits(hb) << 16)) : (bf16_bits(la) | (bf16_bits(lb) << 16));
+        }
+      }
+      *reinterpret_cast<uint4 *>(sm.W3 + tc05::canon_off(row, c, kSboW3)) = make_uint4(v[0], v[1], v[2], v[3]);
+    }
+    if (t == 0) { sm.b3 = w->b3; sm.fail = 0; }
+  }
+  if (t == 0) tc05::mbar_init(&sm.bar, 1);
+  if (wid == 0) tc05::tmem_alloc(&sm.tmem_base, TC_TMEM_COLS);
+  tc05::fence_smem_to_async();
+  tc05::fence_before_sync();
+  __syncthreads();
+  tc05::fence_after_sync();
+  const uint32_t tmem = sm.tmem_base;
+  const uint32_t trow = tmem + ((uint32_t)(wid * 32) << 16);       // this warp's TMEM lanes
+  const uint32_t xs = tc05::smem_addr(sm.X);
+  const uint32_t w1s = tc05::smem_addr(sm.W1), w2s = tc05::smem_addr(sm.W2), w3s = tc05::smem_addr(sm.W3);
+  constexpr uint32_t idesc64 = tc05::idesc_bf16_f32<128, NH>(), idesc16 = tc05::idesc_bf16_f32<128, 16>();
+  uint8_t *const xrow1 = sm.X + tc05::canon_off(t, 0, kSboA1);    // this thread's row of each A operand
+  uint8_t *const xrow2 = sm.X + tc05::canon_off(t, 0, kSboA2);
+  unsigned phase = 0;
+  bool failed = false, bail = false;
+  unsigned st = 0;
+  const long ntiles = (n + TC_THREADS - 1) / TC_THREADS;
+  for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const long i = tile * TC_THREADS + t;
+    const bool valid = i < n;
+    Side L, R;
+    Gas G;
+    load_or_dummy(S, n, i, valid, L, R, G);
+    const SideK kl = side_k(L, G), kr = side_k(R, G);
+    const bool vac = vacuum(L, R, G);
+    const double wtr = vac ? 0.0 : tr_w(L, R, kl, kr, G);
+    const double ptr = vac ? 0.0 : p_of_w(wtr, G);
+    const bool net = SOLVE ? (valid && !vac && !tr_exact(L, R, ptr) && strong_waves(L, R)) : (valid && !vac);
+    float y = 0.f;
+    {
+      // layer-1 row: the features (zeros where the network is not
+      // consulted), then the bias inputs
+      float f[NIN];
+      if (net) features(L, R, G.g, ptr, f);
+      else for (int k = 0; k < NIN; ++k) f[k] = 0.f;
+      *reinterpret_cast<uint4 *>(xrow1) =
+          make_uint4(pack_bf16(f[0], f[1]), pack_bf16(f[2], f[3]), pack_bf16(f[4], f[5]), pack_bf16(f[6], f[7]));
+      *reinterpret_cast<uint4 *>(xrow1 + kLbo) = ones;
+    }
+    tc05::fence_smem_to_async();
+    tc05::fence_before_sync();
+    const bool any = __syncthreads_or(net);
+    if (sm.fail) { bail = true; break; }
+    if (any) {
+      if (t == 0) {
+        tc05::fence_after_sync();
+        tc05::mma_bf16(tmem, tc05::sdesc(xs, kLbo, kSboA1), tc05::sdesc(w1s, kLbo, kSboA1), idesc64, 0u);
+        tc05::commit(&sm.bar);
+      }
+      failed |= !tc05::mbar_wait(&sm.bar, phase, kTcWaitCycles);
+      phase ^= 1u;
+      tc05::fence_after_sync();
+      // hidden layer 1 (bias included) -> BF16 rows of layer 2, then its
+      // bias inputs and padding
+#pragma unroll
+      for (int half = 0; half < 2; ++half) {
+        uint32_t r[32];
+        tc05::ld32(trow + half * 32, r);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          *reinterpret_cast<uint4 *>(xrow2 + (half * 4 + q) * kLbo) = make_uint4(
+              relu_bf16x2(__uint_as_float(r[8 * q + 0]), __uint_as_float(r[8 * q + 1])),
+              relu_bf16x2(__uint_as_float(r[8 * q + 2]), __uint_as_float(r[8 * q + 3])),
+              relu_bf16x2(__uint_as_float(r[8 * q + 4]), __uint_as_float(r[8 * q + 5])),
+              relu_bf16x2(__uint_as_float(r[8 * q + 6]), __uint_as_float(r[8 * q + 7])));
+      }
+      *reinterpret_cast<uint4 *>(xrow2 + 8 * kLbo) = ones;
+      *reinterpret_cast<uint4 *>(xrow2 + 9 * kLbo) = make_uint4(0u, 0u, 0u, 0u);
+      tc05::fence_smem_to_async();
+      tc05::fence_before_sync();
+      if ((bail = __syncthreads_or(failed))) break;
+      if (t == 0) {
+        tc05::fence_after_sync();
+#pragma unroll
+        for (int kk = 0; kk < kK2 / 16; ++kk)
+          tc05::mma_bf16(tmem, tc05::sdesc(xs + 256u * kk, kLbo, kSboA2), tc05::sdesc(w2s + 256u * kk, kLbo, kSboA2),
+                         idesc64, kk > 0 ? 1u : 0u);
+        tc05::commit(&sm.bar);
+      }
+      failed |= !tc05::mbar_wait(&sm.bar, phase, kTcWaitCycles);
+      phase ^= 1u;
+      tc05::fence_after_sync();
+      // hidden layer 2 (bias included) -> BF16 rows of layer 3
+#pragma unroll
+      for (int half = 0; half < 2; ++half) {
+        uint32_t r[32];
+        tc05::ld32(trow + half * 32, r);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          *reinterpret_cast<uint4 *>(xrow2 + (half * 4 + q) * kLbo) = make_uint4(
+              relu_bf16x2(__uint_as_float(r[8 * q + 0]), __uint_as_float(r[8 * q + 1])),
+              relu_bf16x2(__uint_as_float(r[8 * q + 2]), __uint_as_float(r[8 * q + 3])),
+              relu_bf16x2(__uint_as_float(r[8 * q + 4]), __uint_as_float(r[8 * q + 5])),
+              relu_bf16x2(__uint_as_float(r[8 * q + 6]), __uint_as_float(r[8 * q + 7])));
+      }
+      tc05::fence_smem_to_async();
+      tc05::fence_before_sync();
+      if ((bail = __syncthreads_or(failed))) break;
+      if (t == 0) {
+        tc05::fence_after_sync();
+#pragma unroll
+        for (int kk = 0; kk < NH / 16; ++kk)
+          tc05::mma_bf16(tmem, tc05::sdesc(xs + 256u * kk, kLbo, kSboA2), tc05::sdesc(w3s + 256u * kk, kLbo, kSboW3),
+                         idesc16, kk > 0 ? 1u : 0u);
+        tc05::commit(&sm.bar);
+      }
+      if (!tc05::mbar_wait(&sm.bar, phase, kTcWaitCycles)) { failed = true; sm.fail = 1; }
+      phase ^= 1u;
+      tc05::fence_after_sync();
+      uint32_t r2[2];
+      tc05::ld2(trow, r2);
+      y = (__uint_as_float(r2[0]) + __uint_as_float(r2[1])) + sm.b3;
+      tc05::fence_before_sync();
+    }
+    if (SOLVE) {
+      double w0 = wtr;
+      if (net) w0 = wtr * (double)expf(float(G.z) * fminf(fmaxf(y, -20.f), 20.f));   // (p*/p_TR)^z
+      const bool pending = solve_store(L, R, kl, kr, G, vac, net, w0, tol, max_iter, valid, i, n, out, iters,
+                                       flags, st);
+      enqueue(pending && valid, i, queue, qcount);
+    } else if (valid) {
+      yout[i] = net ? y : 0.f;
+    }
+  }
+  if (!bail) bail = __syncthreads_or(sm.fail != 0);
+  if (bail) {
+    // the MMA of the phase that timed out may still be in flight
+    if (t == 0) st |= FLASH_HY_ERR_TIMEOUT;
+    if (failed) tc05::mbar_wait(&sm.bar, phase ^ 1u, kTcWaitCycles);
+  }
+  if (st) atomicOr(status, st);
+  tc05::fence_before_sync();
+  __syncthreads();
+  if (wid == 0) {
+    tc05::fence_after_sync();
+    tc05::tmem_free(tmem, TC_TMEM_COLS);
+  }
 }
 
 // fallback: queued solves restart from the two-rarefaction guess
@@ -387,6 +648,8 @@ struct flash_hy_rsolver {
   long qcap;
   unsigned *status;
   int step;
+  int infer;                    // FLASH_HY_INFER_TCGEN05 or FLASH_HY_INFER_WARP_MMA
+  int tc_grid;                  // resident CTAs of k_solve_tc over the device
   char err[256];
 };
 
@@ -437,7 +700,28 @@ extern "C" int flash_hy_rsolver_create(int device, flash_hy_rsolver **out) {
   cudaError_t e = cudaMemcpy(r->w, h, NPARAM * sizeof(float), cudaMemcpyHostToDevice);
   free(h);
   if (e != cudaSuccess) return FLASH_HY_ERR_CUDA;
+  // resident CTAs of the tcgen05 kernels: each holds TC_TMEM_COLS of the
+  // SM's 512 TMEM columns, so at most 512 / TC_TMEM_COLS may share an SM
+  int occ = 0, occ_p = 0, sms = 0;
+  RS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_solve_tc<true>, TC_THREADS, 0));
+  RS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_p, k_solve_tc<false>, TC_THREADS, 0));
+  RS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  occ = occ < occ_p ? occ : occ_p;
+  if (occ > (int)(512 / TC_TMEM_COLS)) occ = 512 / TC_TMEM_COLS;
+  r->tc_grid = sms * (occ > 0 ? occ : 1);
+  r->infer = FLASH_HY_INFER_TCGEN05;
   return repack(r);
+}
+
+extern "C" int flash_hy_rsolver_set_inference(flash_hy_rsolver *r, int mode) {
+  if (!r || (mode != FLASH_HY_INFER_TCGEN05 && mode != FLASH_HY_INFER_WARP_MMA)) return FLASH_HY_ERR_BAD_ARG;
+  r->infer = mode;
+  return 0;
+}
+
+static int tc_grid_for(const flash_hy_rsolver *r, long n) {
+  const long tiles = (n + TC_THREADS - 1) / TC_THREADS;
+  return (int)(tiles < r->tc_grid ? tiles : r->tc_grid);
 }
 
 extern "C" int flash_hy_rsolver_destroy(flash_hy_rsolver *r) {
@@ -473,7 +757,10 @@ extern "C" int flash_hy_rsolver_solve(flash_hy_rsolver *r, const double *d_state
     r->qcap = n;
   }
   if (learned) RS_CUDA(cudaMemsetAsync(r->qcount, 0, sizeof(int), r->stream));
-  if (learned)
+  if (learned && r->infer == FLASH_HY_INFER_TCGEN05)
+    k_solve_tc<true><<<tc_grid_for(r, n), TC_THREADS, 0, r->stream>>>(
+        d_states, n, d_star, d_iters, d_flags, r->packed, tol, max_iter, r->queue, r->qcount, r->status, nullptr);
+  else if (learned)
     k_solve<true><<<grid_for(n, SOLVE_THREADS), SOLVE_THREADS, 0, r->stream>>>(
         d_states, n, d_star, d_iters, d_flags, r->packed, tol, max_iter, r->queue, r->qcount, r->status);
   else
@@ -491,7 +778,11 @@ extern "C" int flash_hy_rsolver_solve(flash_hy_rsolver *r, const double *d_state
 extern "C" int flash_hy_rsolver_predict(flash_hy_rsolver *r, const double *d_states, long n, float *d_y) {
   if (!r || !d_states || !d_y || n <= 0) return FLASH_HY_ERR_BAD_ARG;
   RS_CUDA(cudaSetDevice(r->device));
-  k_predict<<<grid_for(n, SOLVE_THREADS), SOLVE_THREADS, 0, r->stream>>>(d_states, n, d_y, r->packed);
+  if (r->infer == FLASH_HY_INFER_TCGEN05)
+    k_solve_tc<false><<<tc_grid_for(r, n), TC_THREADS, 0, r->stream>>>(
+        d_states, n, nullptr, nullptr, nullptr, r->packed, 0.0, 0, nullptr, nullptr, r->status, d_y);
+  else
+    k_predict<<<grid_for(n, SOLVE_THREADS), SOLVE_THREADS, 0, r->stream>>>(d_states, n, d_y, r->packed);
   RS_CUDA(cudaGetLastError());
   return 0;
 }

@@ -1,8 +1,9 @@
 """Exact Riemann solver with a learned star-pressure guess (C-ABI wrapper).
 
 Device arrays are torch tensors (device memory plumbing only); the solver,
-the tensor-core network inference and the training all run in the CUDA
-library (flash5_b200/csrc/riemann_exact.cu).
+the tensor-core network inference (tcgen05 with TMEM accumulators, or
+per-warp mma.sync) and the training all run in the CUDA library
+(flash5_b200/csrc/riemann_exact.cu).
 """
 import ctypes as C
 
@@ -28,7 +29,11 @@ _SIGS = {
     "flash_hy_rsolver_set_weights": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int]),
     "flash_hy_rsolver_num_params": (C.c_int, []),
     "flash_hy_rsolver_sync": (C.c_int, [C.c_void_p]),
+    "flash_hy_rsolver_set_inference": (C.c_int, [C.c_void_p, C.c_int]),
 }
+
+INFER_TCGEN05 = 0     # network on the tcgen05 tensor cores, 128 interfaces per MMA tile (default)
+INFER_WARP_MMA = 1    # network per warp on mma.sync (the form inlined in the hydro kernels)
 
 
 def _lib():
@@ -150,6 +155,12 @@ class ExactRiemann:
     def set_weights(self, w):
         w = np.ascontiguousarray(w, dtype=np.float32)
         self._check(self.L.flash_hy_rsolver_set_weights(self.h, w.ctypes.data_as(C.POINTER(C.c_float)), self.nparam))
+
+    def set_inference(self, mode):
+        """Run the network of solve(learned=True) and predict() on the tcgen05
+        tensor cores (INFER_TCGEN05, default) or per warp on mma.sync
+        (INFER_WARP_MMA)."""
+        self._check(self.L.flash_hy_rsolver_set_inference(self.h, int(mode)))
 
     def sync(self):
         return self.L.flash_hy_rsolver_sync(self.h)

@@ -426,6 +426,17 @@ int flash_hy_rsolver_get_weights(flash_hy_rsolver *r, float *h_w, int n);
 int flash_hy_rsolver_set_weights(flash_hy_rsolver *r, const float *h_w, int n);
 int flash_hy_rsolver_num_params(void);
 int flash_hy_rsolver_sync(flash_hy_rsolver *r);
+/* Where the batched solves and predict run the network: on the tcgen05
+ * tensor cores, 128 interfaces per MMA tile with the accumulator in TMEM
+ * (FLASH_HY_INFER_TCGEN05, the default), or per warp on mma.sync
+ * (FLASH_HY_INFER_WARP_MMA, the form the hydro kernels use inline).  Both
+ * give the same converged p*; the network outputs agree to rounding (the
+ * tcgen05 form takes the FP32 biases and output weights as two BF16 parts
+ * and accumulates in another order).  Other values give
+ * FLASH_HY_ERR_BAD_ARG.                                                 */
+#define FLASH_HY_INFER_TCGEN05  0
+#define FLASH_HY_INFER_WARP_MMA 1
+int flash_hy_rsolver_set_inference(flash_hy_rsolver *r, int mode);
 
 #ifdef __cplusplus
 }

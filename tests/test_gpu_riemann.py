@@ -6,7 +6,9 @@
 * the hand-written training kernel's gradient matches the float64 analytic
   gradient of the reference MLP (which itself matches finite differences in
   tests/test_mlp_ref.py);
-* the tensor-core BF16 inference matches a BF16 numpy forward pass;
+* the tensor-core BF16 inference (tcgen05 with TMEM accumulators, the
+  default) matches a BF16 numpy forward pass, and the per-warp mma.sync form
+  to rounding, on full and partial 128-interface tiles;
 * after training on solver-harvested states, Newton from the learned guess
   gives the same p* (to 1e-11) in fewer iterations than from the
   two-rarefaction guess.
@@ -111,6 +113,38 @@ def test_tensor_core_inference_matches_bf16_reference(rs):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 129, 4096 + 37])
+def test_tcgen05_inference_matches_warp_mma(rs, n):
+    from flash5_b200.riemann import INFER_TCGEN05, INFER_WARP_MMA
+    rng = np.random.default_rng(7)
+    w = (rng.normal(size=mlp_ref.NPARAM) * 0.3).astype(np.float32)
+    rs.set_weights(w)
+    S = rs.generate(123, n)
+    try:
+        rs.set_inference(INFER_WARP_MMA)
+        yw = rs.predict(S).cpu().numpy()
+        rs.set_inference(INFER_TCGEN05)
+        yt = rs.predict(S).cpu().numpy()
+    finally:
+        rs.set_inference(INFER_TCGEN05)
+    assert rs.sync() == 0
+    assert np.all(np.isfinite(yt))
+    d = np.abs(yt - yw) / (1.0 + np.abs(yw))
+    # same BF16 operands and FP32 accumulation (the tcgen05 form takes the
+    # FP32 biases and w3 as two BF16 parts); a hidden unit's BF16 rounding
+    # can flip with the accumulation order, nothing more
+    assert d.max() <= 2e-2, d.max()
+    assert np.median(d) <= 1e-4, np.median(d)
+
+
+@pytest.mark.gpu
+def test_inference_mode_rejects_unknown_values(rs):
+    from flash5_b200.riemann import RiemannError
+    with pytest.raises(RiemannError):
+        rs.set_inference(7)
+
+
+@pytest.mark.gpu
 def test_learned_guess_same_result_fewer_iterations(rs):
     torch = rs.torch
     from flash5_b200.riemann import ExactRiemann
@@ -124,7 +158,17 @@ def test_learned_guess_same_result_fewer_iterations(rs):
         S = r.generate(2, 200000)
         o0, it0, f0 = r.solve(S, learned=False)
         o1, it1, f1 = r.solve(S, learned=True)
+        from flash5_b200.riemann import INFER_TCGEN05, INFER_WARP_MMA
+        r.set_inference(INFER_WARP_MMA)
+        o2, it2, f2 = r.solve(S, learned=True)
+        r.set_inference(INFER_TCGEN05)
         torch.cuda.synchronize()
+        assert r.sync() == 0
+        # the tcgen05 and per-warp network starts converge to the same p*
+        ok2 = (f2.cpu().numpy() & 2) == 0
+        p2 = o2[0].cpu().numpy()
+        assert np.array_equal(ok2, (f1.cpu().numpy() & 2) == 0)
+        assert (np.abs(p2[ok2] - o1[0].cpu().numpy()[ok2]) / p2[ok2]).max() <= 1e-11
         p0, p1 = o0[0].cpu().numpy(), o1[0].cpu().numpy()
         fl0, fl1 = f0.cpu().numpy(), f1.cpu().numpy()
         ok = (fl0 & 2) == 0
