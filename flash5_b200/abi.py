@@ -123,13 +123,18 @@ class GridDesc(C.Structure):
 
 class Tuning(C.Structure):
     """flash_hy_tuning: threads per CTA of the transverse-flux/CFL passes,
-    the FP64 direction kernels and the mixed direction kernels, and the
-    blocks per CTA along the sweep of the mixed 3D direction kernels."""
-    _fields_ = [("sig_threads", C.c_int), ("dir_threads", C.c_int), ("mx_threads", C.c_int), ("mx_runs", C.c_int)]
+    the FP64 direction kernels and the mixed direction kernels, the blocks
+    per CTA along the sweep of the mixed 3D direction kernels, and the sweep
+    order of the mixed path (SWEEP_XYZ or SWEEP_ZYX)."""
+    _fields_ = [("sig_threads", C.c_int), ("dir_threads", C.c_int), ("mx_threads", C.c_int), ("mx_runs", C.c_int),
+                ("mx_sweep", C.c_int)]
 
     def as_dict(self):
         return {"sig_threads": self.sig_threads, "dir_threads": self.dir_threads, "mx_threads": self.mx_threads,
-                "mx_runs": self.mx_runs}
+                "mx_runs": self.mx_runs, "mx_sweep": self.mx_sweep}
+
+
+SWEEP_XYZ, SWEEP_ZYX = 1, 2    # FLASH's constants.h values
 
 
 TUNE_MAX = 8

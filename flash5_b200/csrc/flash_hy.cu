@@ -53,6 +53,7 @@ struct flash_hy_ctx {
   int dir_threads;     // FP64 direction kernels
   int mx_sel;          // mixed direction kernels: candidate 0, 1, 2
   int mx_runs;         // mixed 3D direction kernels: blocks per CTA along the sweep (1 or kMxRun)
+  int mx_sweep;        // mixed direction kernels: FLASH_HY_SWEEP_XYZ or FLASH_HY_SWEEP_ZYX
   int host_ng;         // guard layers of the caller's UNK arrays
   float *d_wmaster;    // learned guess: FP32 master weights
   void *d_mlp;         // learned guess: packed BF16 inference copy (xrs::MlpPacked)
@@ -487,6 +488,7 @@ extern "C" int flash_hy_create(const flash_hy_params *params, const flash_hy_gri
   c->dir_threads = c->threads;
   c->mx_sel = 1;
   c->mx_runs = 1;
+  c->mx_sweep = FLASH_HY_SWEEP_XYZ;
   c->host_ng = g->nguard;
   c->nspec = params->nspecies;
   c->nsp = params->nspecies + params->nmass_scalars;
@@ -1158,6 +1160,7 @@ static int enqueue_step(flash_hy_ctx *c, double dt, const int *d_list, int nlaun
   a.threads = c->threads;
   a.dir_threads = c->dir_threads;
   a.mx_sel = c->mx_sel;
+  a.sweep = c->p.precision == FLASH_HY_PREC_MIXED && c->mx_sweep == FLASH_HY_SWEEP_ZYX ? 1 : 0;
   a.stream = c->stream;
   a.tma = c->tma_maps ? c->tma_maps + 3 * c->cur : nullptr;
   a.tma_run = c->tma_run && c->mx_runs > 1 ? c->tma_run + 3 * c->cur : nullptr;
@@ -1559,6 +1562,7 @@ extern "C" int flash_hy_get_tuning(flash_hy_ctx *c, flash_hy_tuning *out) {
   out->dir_threads = c->dir_threads;
   out->mx_threads = mx_threads_of(c->mx_sel, c->ndim, c->nx);
   out->mx_runs = c->mx_runs;
+  out->mx_sweep = c->mx_sweep;
   return 0;
 }
 
@@ -1573,8 +1577,12 @@ extern "C" int flash_hy_set_tuning(flash_hy_ctx *c, const flash_hy_tuning *t) {
     return fail(c, FLASH_HY_ERR_BAD_ARG, "set_tuning: %s", "not a candidate launch shape of this block shape");
   if (t->mx_runs != 1 && !(t->mx_runs == fhy::kMxRun && c->tma_run))
     return fail(c, FLASH_HY_ERR_BAD_ARG, "set_tuning: %s", "mx_runs is 1 or FLASH_HY_MX_RUN where runs are offered");
+  if (t->mx_sweep != FLASH_HY_SWEEP_XYZ &&
+      !(t->mx_sweep == FLASH_HY_SWEEP_ZYX && c->p.precision == FLASH_HY_PREC_MIXED))
+    return fail(c, FLASH_HY_ERR_BAD_ARG, "set_tuning: %s",
+                "mx_sweep is FLASH_HY_SWEEP_XYZ, or FLASH_HY_SWEEP_ZYX on the mixed-precision path");
   if (t->sig_threads != c->threads || t->dir_threads != c->dir_threads || sel != c->mx_sel ||
-      t->mx_runs != c->mx_runs) {
+      t->mx_runs != c->mx_runs || t->mx_sweep != c->mx_sweep) {
     CUDA_OK(c, cudaSetDevice(c->device));
     CUDA_OK(c, cudaStreamSynchronize(c->stream));
     drop_graphs(c);
@@ -1584,6 +1592,7 @@ extern "C" int flash_hy_set_tuning(flash_hy_ctx *c, const flash_hy_tuning *t) {
   c->dir_threads = t->dir_threads;
   c->mx_sel = sel;
   c->mx_runs = t->mx_runs;
+  c->mx_sweep = t->mx_sweep;
   return 0;
 }
 
@@ -1605,7 +1614,7 @@ extern "C" int flash_hy_autotune(flash_hy_ctx *c, double dt, int steps, flash_hy
   double *keep = nullptr;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   int rc = 0, nt = 0;
-  const int sig0 = c->threads, dir0 = c->dir_threads, sel0 = c->mx_sel, runs0 = c->mx_runs;
+  const int sig0 = c->threads, dir0 = c->dir_threads, sel0 = c->mx_sel, runs0 = c->mx_runs, sweep0 = c->mx_sweep;
   int cand[FLASH_HY_TUNE_MAX];
   const int ncand = thread_candidates(c, cand);
   const bool mixed = c->p.precision == FLASH_HY_PREC_MIXED;
@@ -1640,6 +1649,7 @@ extern "C" int flash_hy_autotune(flash_hy_ctx *c, double dt, int steps, flash_hy
       table[nt].dir_threads = c->dir_threads;
       table[nt].mx_threads = mx_threads_of(c->mx_sel, c->ndim, c->nx);
       table[nt].mx_runs = c->mx_runs;
+      table[nt].mx_sweep = c->mx_sweep;
       table_ms[nt] = ms;
     }
     ++nt;
@@ -1685,7 +1695,19 @@ extern "C" int flash_hy_autotune(flash_hy_ctx *c, double dt, int steps, flash_hy
         rc = trial(ms);
         if (!rc) {
           record(ms);
-          if (!(ms < best_ms)) c->mx_runs = keep_runs;
+          if (ms < best_ms) best_ms = ms;
+          else c->mx_runs = keep_runs;
+        }
+      }
+      // the other sweep order of the mixed path
+      if (mixed && !rc) {
+        const int keep_sweep = c->mx_sweep;
+        c->mx_sweep = keep_sweep == FLASH_HY_SWEEP_ZYX ? FLASH_HY_SWEEP_XYZ : FLASH_HY_SWEEP_ZYX;
+        float ms = 0.f;
+        rc = trial(ms);
+        if (!rc) {
+          record(ms);
+          if (!(ms < best_ms)) c->mx_sweep = keep_sweep;
         }
       }
     }
@@ -1711,7 +1733,7 @@ done:
   }
   if (e0) cudaEventDestroy(e0);
   if (e1) cudaEventDestroy(e1);
-  if (rc) { c->threads = sig0; c->dir_threads = dir0; c->mx_sel = sel0; c->mx_runs = runs0; }
+  if (rc) { c->threads = sig0; c->dir_threads = dir0; c->mx_sel = sel0; c->mx_runs = runs0; c->mx_sweep = sweep0; }
   cudaMemcpy(c->d_status, &saved_status, sizeof(unsigned), cudaMemcpyHostToDevice);
   c->dt_valid = 0;
   drop_graphs(c);

@@ -36,6 +36,7 @@ struct StepArgs {
   int threads;        // threads per CTA of the transverse-flux and CFL passes
   int dir_threads;    // threads per CTA of the FP64 direction kernels
   int mx_sel;         // candidate (0, 1, 2) of the mixed direction kernels' threads per CTA
+  int sweep = 0;      // mixed path: 0 = directions x, y, z; 1 = z, y, x
   cudaStream_t stream;
   bool set_attr;      // raise the kernels' dynamic shared-memory limit (not while capturing a graph)
   // AMR (nlev > 0): k_sig over all leaves, then per direction one launch per

@@ -243,7 +243,15 @@ template <int NDIM, int NX, int NY, int NZ> struct MxThreads {
   static constexpr int pick(int sel) { return sel == 0 ? c0 : (sel == 1 ? c1 : c2); }
 };
 
-template <int NDIM, int NX, int NY, int NZ, int DIR, bool FIRST, bool LAST, int RS, int NT, int K = 1>
+// Sweep order ORD of the mixed path: 0 = x, y, z (FLASH's SWEEP_XYZ), 1 =
+// z, y, x (SWEEP_ZYX).  The directions accumulate the conservative update
+// in that order; an earlier direction's internal-energy terms sit in AUX
+// slot aux_slot (its position in the order), and the last direction
+// gathers them per direction and applies the same x, y, z formula.
+template <int NDIM, int ORD>
+__host__ __device__ constexpr int aux_slot(int d) { return ORD == 0 ? d - 1 : NDIM - d; }
+
+template <int NDIM, int NX, int NY, int NZ, int DIR, bool FIRST, bool LAST, int RS, int NT, int K = 1, int ORD = 0>
 __global__ void __launch_bounds__(NT, NDIM == 3 ? 2 : 1)
 k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ ACC, double *__restrict__ AUX,
          size_t ncells, CflPart *part, const __grid_constant__ TmaLine tm) {
@@ -961,12 +969,12 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
     if (!LAST) {
 #pragma unroll
       for (int n = 0; n < 5; ++n) ACC[n * ncells + off] = U[n];
-      double *ax = AUX + (size_t)(DIR - 1) * 3 * ncells;
+      double *ax = AUX + (size_t)aux_slot<NDIM, ORD>(DIR) * 3 * ncells;
       ax[off] = ea; ax[ncells + off] = eb; ax[2 * ncells + off] = sp;
     } else {
       const double rho0 = P.s_in[0][off], e0 = P.s_in[4][off];
       double IntEner = 0.0;
-      if (P.use_aux_eint) {
+      if (P.use_aux_eint && ORD == 0) {
         double pb;
         const double sx = AUX[2 * ncells + off];
         if (NDIM == 2) {
@@ -982,6 +990,22 @@ k_dir_mx(const DevParams P, const float *__restrict__ SIG, double *__restrict__ 
           IntEner += dt / del[1] * (AUX[3 * ncells + off] + pb * AUX[4 * ncells + off]);
           IntEner += dt / del[2] * (ea + pb * eb);
         }
+      } else if (P.use_aux_eint) {
+        // the same formula for another order: each direction's (ea, eb,
+        // speed), this direction's own, the earlier ones' from their slots
+        double te[3], tb[3], ts[3];
+#pragma unroll
+        for (int d = 1; d <= NDIM; ++d) {
+          if (d == DIR) { te[d - 1] = ea; tb[d - 1] = eb; ts[d - 1] = sp; continue; }
+          const double *ad = AUX + (size_t)aux_slot<NDIM, ORD>(d) * 3 * ncells;
+          te[d - 1] = ad[off]; tb[d - 1] = ad[ncells + off]; ts[d - 1] = ad[2 * ncells + off];
+        }
+        double pb;
+        if (NDIM == 2) pb = (0.5 * ts[0]) * 0.5 + ts[1] * 0.25;
+        else pb = (((0.5 * ts[0]) * 0.5 + ts[1] * 0.25) * 4.0 + ts[2]) / 6.0;
+        IntEner = rho0 * e0 + dt / del[0] * (te[0] + pb * tb[0]);
+        IntEner += dt / del[1] * (te[1] + pb * tb[1]);
+        if (NDIM == 3) IntEner += dt / del[2] * (te[2] + pb * tb[2]);
       }
       double dens = fmax(U[0], P.smlrho);
       double rinv = 1.0 / dens;

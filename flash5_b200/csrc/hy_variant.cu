@@ -38,14 +38,17 @@ static bool use_runs(const StepArgs &a) {
          a.nlaunch == a.nblocks;
 }
 
-template <int NDIM, int NX, int NY, int NZ, int DIR, bool FIRST, bool LAST, int RS>
+// ORD: sweep order of the mixed path (0 = x, y, z; 1 = z, y, x); the FP64
+// variants always run x, y, z
+template <int NDIM, int NX, int NY, int NZ, int DIR, bool FIRST, bool LAST, int RS, int ORD = 0>
 static bool launch_dir_one(const StepArgs &a) {
 #if FHY_VARIANT == 3
   using G = MxGeom<NDIM, NX, NY, NZ, DIR, RS>;
   constexpr int NT = MxThreads<NDIM, NX, NY, NZ>::pick(FHY_MXSEL);
-  auto kern = k_dir_mx<NDIM, NX, NY, NZ, DIR, FIRST, LAST, RS, NT>;
+  auto kern = k_dir_mx<NDIM, NX, NY, NZ, DIR, FIRST, LAST, RS, NT, 1, ORD>;
   const int threads = NT;
 #else
+  static_assert(ORD == 0, "the FP64 variants sweep x, y, z");
   using G = DirGeom<NDIM, NX, NY, NZ, Real, DIR>;
   auto kern = k_dir<NDIM, NX, NY, NZ, Real, DIR, FIRST, LAST, FHY_VARIANT, RS>;
   const int threads = a.dir_threads;
@@ -60,7 +63,7 @@ static bool launch_dir_one(const StepArgs &a) {
     // full uniform grid: runs of kMxRun blocks along the sweep
     if (use_runs(a)) {
       using GR = MxGeom<NDIM, NX, NY, NZ, DIR, RS, kMxRun>;
-      auto kr = k_dir_mx<NDIM, NX, NY, NZ, DIR, FIRST, LAST, RS, NT, kMxRun>;
+      auto kr = k_dir_mx<NDIM, NX, NY, NZ, DIR, FIRST, LAST, RS, NT, kMxRun, ORD>;
       const size_t smr = GR::smem_bytes();
       if (a.set_attr && cudaFuncSetAttribute(kr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smr) != cudaSuccess)
         return false;
@@ -82,15 +85,15 @@ static bool launch_dir_one(const StepArgs &a) {
 
 // one direction: a single launch, or on an AMR hierarchy one launch per
 // level, finest first
-template <int NDIM, int NX, int NY, int NZ, int DIR, bool FIRST, bool LAST, int RS>
+template <int NDIM, int NX, int NY, int NZ, int DIR, bool FIRST, bool LAST, int RS, int ORD = 0>
 static bool launch_dir(const StepArgs &a) {
-  if (a.nlev == 0) return launch_dir_one<NDIM, NX, NY, NZ, DIR, FIRST, LAST, RS>(a);
+  if (a.nlev == 0) return launch_dir_one<NDIM, NX, NY, NZ, DIR, FIRST, LAST, RS, ORD>(a);
   StepArgs b = a;
   for (int l = a.nlev; l >= 1; --l) {
     if (a.lev_count[l] == 0) continue;
     b.P.blk_list = a.lev_list[l];
     b.nlaunch = a.lev_count[l];
-    if (!launch_dir_one<NDIM, NX, NY, NZ, DIR, FIRST, LAST, RS>(b)) return false;
+    if (!launch_dir_one<NDIM, NX, NY, NZ, DIR, FIRST, LAST, RS, ORD>(b)) return false;
     b.set_attr = false;
   }
   return true;
@@ -139,14 +142,29 @@ static int run_rs(const StepArgs &a) {
     nl = 0;
     for (int l = 1; l <= a.nlev; ++l) nl += a.lev_count[l] > 0;
   }
+  // z, y, x on the mixed path when asked (the plain step and AMR; the split
+  // step's flux modes keep x, y, z).  The middle direction of 3D has the
+  // same AUX slot in both orders, so it shares the x, y, z kernel.
+  bool ok;
+  if constexpr (FHY_VARIANT == 3) {
+    if (a.sweep == 1 && a.P.fmode == 0) {
+      if constexpr (NDIM == 2)
+        ok = launch_dir<NDIM, NX, NY, NZ, 2, true, false, RS, 1>(a) &&
+             launch_dir<NDIM, NX, NY, NZ, 1, false, true, RS, 1>(a);
+      else
+        ok = launch_dir<NDIM, NX, NY, NZ, 3, true, false, RS, 1>(a) &&
+             launch_dir<NDIM, NX, NY, NZ, 2, false, false, RS>(a) &&
+             launch_dir<NDIM, NX, NY, NZ, 1, false, true, RS, 1>(a);
+      return ok ? nsig + NDIM * nl + (NDIM == 3 && use_runs(a) ? 1 : 0) : -2;
+    }
+  }
   if constexpr (NDIM == 2) {
-    const bool ok =
-        launch_dir<NDIM, NX, NY, NZ, 1, true, false, RS>(a) && launch_dir<NDIM, NX, NY, NZ, 2, false, true, RS>(a);
+    ok = launch_dir<NDIM, NX, NY, NZ, 1, true, false, RS>(a) && launch_dir<NDIM, NX, NY, NZ, 2, false, true, RS>(a);
     return ok ? nsig + 2 * nl : -2;
   } else {
-    const bool ok = launch_dir<NDIM, NX, NY, NZ, 1, true, false, RS>(a) &&
-                    launch_dir<NDIM, NX, NY, NZ, 2, false, false, RS>(a) &&
-                    launch_dir<NDIM, NX, NY, NZ, 3, false, true, RS>(a);
+    ok = launch_dir<NDIM, NX, NY, NZ, 1, true, false, RS>(a) &&
+         launch_dir<NDIM, NX, NY, NZ, 2, false, false, RS>(a) &&
+         launch_dir<NDIM, NX, NY, NZ, 3, false, true, RS>(a);
     return ok ? nsig + 3 * nl + (use_runs(a) ? 1 : 0) : -2;   // + the CFL merge of the runs
   }
 }

@@ -345,7 +345,9 @@ int flash_hy_mark_refine_tree(flash_hy_ctx *ctx, int nvar, const int *vars, doub
  * candidates of the context's block shape (FLASH_HY_ERR_BAD_ARG);
  * tuning_candidates lists them (arrays of FLASH_HY_TUNE_MAX entries).
  * autotune times `steps` steps of dt, after one untimed step, for every
- * candidate of the direction kernels and then of the transverse-flux pass
+ * candidate of the direction kernels (then, on the mixed path, the other
+ * mx_runs setting where runs are offered and the other sweep order) and
+ * then of the transverse-flux pass
  * (coordinate search: the two are separate launches), each trial from a
  * copy of the current state; it restores the state, keeps the fastest
  * shape, and writes every trial (shape, ms per step) to table / table_ms
@@ -362,11 +364,24 @@ int flash_hy_mark_refine_tree(flash_hy_ctx *ctx, int nvar, const int *vars, doub
  * kernels, like the mx_threads candidates, and agree to rounding.  The
  * default is FLASH_HY_MX_RUN where offered; autotune tries both.        */
 #define FLASH_HY_MX_RUN 4
+/* mx_sweep: the order in which the mixed-precision direction kernels
+ * accumulate the conservative update -- FLASH_HY_SWEEP_XYZ (the default)
+ * or FLASH_HY_SWEEP_ZYX, FLASH's SWEEP_XYZ / SWEEP_ZYX values
+ * (source/Simulation/constants.h:359-360).  Each direction's face states
+ * and fluxes come from the same old state either way (the step is
+ * unsplit), so the two orders agree to rounding; the FP64 paths keep
+ * x, y, z, the order of FLASH's update expression, and accept only
+ * FLASH_HY_SWEEP_XYZ; the split step (flash_hy_compute_fluxes /
+ * flash_hy_update_solution) runs x, y, z whatever is set.  autotune tries
+ * both on the mixed path.                                               */
+#define FLASH_HY_SWEEP_XYZ 1
+#define FLASH_HY_SWEEP_ZYX 2
 typedef struct {
   int sig_threads;
   int dir_threads;
   int mx_threads;
   int mx_runs;
+  int mx_sweep;
 } flash_hy_tuning;
 int flash_hy_get_tuning(flash_hy_ctx *ctx, flash_hy_tuning *out);
 int flash_hy_set_tuning(flash_hy_ctx *ctx, const flash_hy_tuning *t);

@@ -52,6 +52,7 @@ int main(void) {
          offsetof(flash_hy_params, single_species_a), sizeof(flash_hy_grid_desc),
          offsetof(flash_hy_grid_desc, block_coords), offsetof(flash_hy_grid_desc, bc));
   printf("%zu\n", sizeof(flash_hy_varmap));
+  printf("%zu %zu\n", sizeof(flash_hy_tuning), offsetof(flash_hy_tuning, mx_sweep));
   return 0;
 }'''
     import tempfile
@@ -68,6 +69,8 @@ int main(void) {
     assert vals[4] == abi.GridDesc.block_coords.offset
     assert vals[5] == abi.GridDesc.bc.offset
     assert vals[6] == C.sizeof(abi.VarMap)
+    assert vals[7] == C.sizeof(abi.Tuning)
+    assert vals[8] == abi.Tuning.mx_sweep.offset
 
 
 def test_flash_varmap_is_alphabetical():
