@@ -24,7 +24,9 @@ is measured on the device against its FP64 reference on the same run.
 (interior-only FLASH UNK, 11 variables, pinned): upload, step, dt, download
 every step.  The default line also carries the batched AMR workload
 (``amr``: 2D four-quadrant hierarchy of 19,456 leaf blocks) and the
-isolated exact-Riemann workload (``riemann``: 1e8 interface pairs).
+isolated exact-Riemann workload (``riemann``: 1e8 interface pairs; the
+learned start with the network on the tcgen05 tensor cores and per warp on
+mma.sync, beside the two-rarefaction start).
 
 ``--impl reference`` times the CPU oracle (the C restatement of the
 reference's Fortran; the Fortran itself cannot be built here) with all host

@@ -200,7 +200,10 @@ class Hydro:
     # -- launch shapes ----------------------------------------------------
     @property
     def tuning(self):
-        """Threads per CTA of the step's kernels (dict)."""
+        """Launch shape of the step (dict): threads per CTA of the step's
+        kernels, blocks per CTA of the mixed 3D direction kernels (mx_runs)
+        and the mixed path's sweep order (mx_sweep, abi.SWEEP_XYZ or
+        abi.SWEEP_ZYX)."""
         t = abi.Tuning()
         self._check(self.lib.flash_hy_get_tuning(self.ctx, C.byref(t)))
         return t.as_dict()
