@@ -601,7 +601,7 @@ def amr_run(args, paths, e2e=True, regrid=True, cpu=True, steps=None, warmup=Non
             best, trials = h.autotune(dts[0] if dts is not None else h.compute_dt()[0], steps=2)
             tunings[name] = {"best": best, "trials_ms": {"/".join(str(v) for v in t.values()): round(m, 4)
                                                          for t, m in trials},
-                             "trial_key": "sig_threads/dir_threads/mx_threads/mx_runs"}
+                             "trial_key": "sig_threads/dir_threads/mx_threads/mx_runs/mx_sweep"}
         headline = name == paths[-1]
         sampler = ClockSampler(0) if headline else None
         ms[name], used, launches[name] = run_device(h, steps, warmup, dts=dts, sampler=sampler)
@@ -729,6 +729,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="KH workload: skip the AMR and isolated-Riemann keys")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes (no autotuning)")
+    ap.add_argument("--sweep", choices=["xyz", "zyx"], default=None,
+                    help="sweep order of the mixed paths before any tuning (the autotuner may change it)")
     ap.add_argument("--no-regrid", action="store_true", help="AMR workload: skip the refinement-cycle timing")
     ap.add_argument("--nspecies", type=int, default=0, help="KH workload: species advected with the flow")
     ap.add_argument("--nmass-scalars", type=int, default=0, help="KH workload: mass scalars advected with the flow")
@@ -826,13 +828,16 @@ def main():
                 h.set_guess_weights(weights)
             h.upload(unk)
         tuned = None
+        if args.sweep and params.precision == abi.PREC_MIXED:
+            hh = h.h if world > 1 else h
+            hh.tuning = dict(hh.tuning, mx_sweep=abi.SWEEP_ZYX if args.sweep == "zyx" else abi.SWEEP_XYZ)
         if not args.no_tune:
             hh = h.h if world > 1 else h
             dt0 = dts[0] if dts is not None else hh.compute_dt()[0]
             best, trials = hh.autotune(dt0, steps=2)
             tuned = {"best": best, "trials_ms": {"/".join(str(v) for v in t.values()): round(m, 4)
                                                  for t, m in trials},
-                     "trial_key": "sig_threads/dir_threads/mx_threads/mx_runs"}
+                     "trial_key": "sig_threads/dir_threads/mx_threads/mx_runs/mx_sweep"}
         headline = name == paths[-1]
         sampler = ClockSampler(dev) if headline else None
         ms[name], used, launches[name] = run_device(h, args.steps, warmup, dts=dts, sampler=sampler, dist=dist)
