@@ -226,8 +226,9 @@ class Hydro:
 
     def autotune(self, dt, steps=3):
         """Time every candidate launch shape on this grid's state (restored
-        afterwards) and keep the fastest; returns (best, trials) with trials
-        a list of (shape, ms per step)."""
+        afterwards) and keep the fastest: threads per CTA, then on the mixed
+        path blocks per CTA (where runs are offered) and the sweep order.
+        Returns (best, trials) with trials a list of (shape, ms per step)."""
         cap = 32
         best = abi.Tuning()
         table = (abi.Tuning * cap)()
