@@ -81,6 +81,39 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def measured_bf16_peak():
+    """Dense BF16 tensor throughput (TFLOP/s) for a kernel timed alone: the
+    measured burst figure, else the fallback."""
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        if "bf16_tflops" in d:
+            return float(d["bf16_tflops"]), "measured"
+    return 1590.0, "fallback"
+
+
+def riemann_roofline(n, solve_ms, network_ms):
+    """Rooflines of the isolated workload: the learned solve against HBM
+    (7 FP64 in, p* and u* and two flag bytes out per pair), the network
+    alone against the BF16 tensor peak (the three MMAs of a 128-row tile,
+    K and N padding included: 2 (16 x 64 + 80 x 64 + 64 x 16) FLOP per
+    row)."""
+    hbm, hbm_kind = measured_peaks()
+    tc, tc_kind = measured_bf16_peak()
+    bpp = 7 * 8 + 2 * 8 + 2
+    fpp = 2 * (16 * 64 + 80 * 64 + 64 * 16)
+    rows = -(-n // 128) * 128
+    gbs = n * bpp / (solve_ms * 1e-3) / 1e9
+    tfs = rows * fpp / (network_ms * 1e-3) / 1e12
+    return {"solve": {"bound": "issue (FP64 set-up and Newton)", "hbm_bytes_per_pair": bpp, "achieved_gbs": gbs,
+                      "peak_gbs": hbm, "frac": gbs / hbm, "peak_kind": hbm_kind},
+            "network_alone": {"tensor_flops_per_pair": fpp, "achieved_tflops": tfs, "peak_tflops": tc,
+                              "frac": tfs / tc, "peak_kind": tc_kind,
+                              "note": "tcgen05 kind::f16, BF16 operands, FP32 accumulator; the time includes "
+                                      "the per-pair FP64 set-up and features"}}
+
+
 def host_cores():
     try:
         return len(os.sched_getaffinity(0))
@@ -550,6 +583,7 @@ def riemann_run(args, n=None, steps=None, warmup=None):
             "paths": res, "speedup_vs_two_rarefaction": res["two_rarefaction"]["ms"] / res["learned"]["ms"],
             "max_rel_pstar_diff_learned_vs_tr": rel, "consulted_frac": consulted_frac,
             "network_dense_ms": predict_ms,
+            "roofline": riemann_roofline(n, res["learned"]["ms"], predict_ms["tcgen05"]),
             "network_dense_note": "the network over every pair (features + tensor-core MLP, written out), tcgen05 "
                                   "and per-warp mma.sync: its own cost per solve, against the Newton evaluations it "
                                   "saves where consulted",
@@ -711,6 +745,7 @@ def riemann_summary(line):
             "consulted_frac": line["consulted_frac"],
             "mean_newton_evaluations_where_consulted": {n: v["mean_iters_where_consulted"] for n, v in p.items()},
             "network_dense_ms": line["network_dense_ms"],
+            "roofline": line["roofline"],
             "speedup_learned_vs_two_rarefaction": line["speedup_vs_two_rarefaction"],
             "max_rel_pstar_diff_learned_vs_tr": line["max_rel_pstar_diff_learned_vs_tr"]}
 
