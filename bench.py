@@ -418,6 +418,10 @@ def cpu_sample(nblk, steps=None, warmup=3, seconds=10.0):
                       f"surrounding blocks; median of {len(times)} steps after {warmup} warm-up steps "
                       f"(mean {np.mean(times) * 1e3:.1f} ms, min {np.min(times) * 1e3:.1f} ms, "
                       f"max {np.max(times) * 1e3:.1f} ms per step)",
+            "why_window": f"at this rate one step of the whole {8 * nblk}^3 grid would take "
+                          f"{(8 * nblk) ** 3 * med / zones:.0f} s on these cores, and the run's warm-up and timed "
+                          f"steps {(8 * nblk) ** 3 * med / zones * (warmup + (steps or 3)) / 60:.0f} min; the "
+                          f"window keeps the grid's data, method and per-zone work",
             "ms_per_step_median": med * 1e3}
 
 
